@@ -1,0 +1,397 @@
+"""Benchmark of the B200 hot path (one JSON line on rank 0).
+
+Headline workload: the equi-join SELECT SUM(b.payload * p.value), COUNT(*)
+FROM probe p JOIN build b ON p.fk = b.key WHERE b.attr < 20, with a 2M-row
+build table and a 120M-row probe table per GPU (weak scaling: every rank
+joins its own probe shard against the same build table, then the partial
+SUM/COUNT are all-reduced over NCCL).  A step is the whole query: build
+append (fused filter) + table build + fused probe/aggregate + finish.
+
+`value` times it with every input resident in HBM; `e2e` times the same
+query through the C ABI from pinned host buffers (host->device copies in the
+timed region).  `roofline` is the fused probe kernel's algorithmic bytes
+(16 B per probe row) over its CUDA-event duration against the measured HBM
+copy bandwidth.  `operators` adds the lineitem-shaped fused
+filter->project->aggregate (6,001,215 rows) and the 200M-row Zipf GROUP BY.
+
+--impl reference times the CPU restatement of the engine's threaded plan
+(the reference engine itself cannot be built: its kernels are oz-lang for
+an absent compiler) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BUILD_ROWS = 2_000_000
+PROBE_ROWS = 120_000_000
+FK_DOMAIN = 2_500_000
+LINEITEM_ROWS = 6_001_215
+ZIPF_ROWS = 200_000_000
+ZIPF_DISTINCT = 20_000_000
+METRIC = "rows/s & HBM GB/s vs peak per operator; mixed-stream queries/s and p50/p99"
+
+
+def peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows: list[list[str]] = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def pinned(q, nbytes: int, dtype, count: int) -> tuple[int, np.ndarray]:
+    ptr = q.lib().qdb_gpu_host_alloc(nbytes)
+    if not ptr:
+        raise MemoryError("pinned allocation failed")
+    arr = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint8)), shape=(nbytes,)).view(dtype)[:count]
+    return ptr, arr
+
+
+class JoinWorkload:
+    def __init__(self, q, rank: int):
+        from qumirdb_b200 import queries
+        self.q = q
+        self.build_host = []
+        self.probe_host = []
+        self.ptrs = []
+        for dt, n in [(np.int64, BUILD_ROWS), (np.int64, BUILD_ROWS), (np.int32, BUILD_ROWS)]:
+            p, a = pinned(q, n * np.dtype(dt).itemsize, dt, n)
+            self.ptrs.append(p)
+            self.build_host.append(a)
+        for dt, n in [(np.int64, PROBE_ROWS), (np.int64, PROBE_ROWS)]:
+            p, a = pinned(q, n * np.dtype(dt).itemsize, dt, n)
+            self.ptrs.append(p)
+            self.probe_host.append(a)
+        # The build table is the same on every rank; the probe shard is the rank's own.
+        q.lib().qdb_gen_join(1, BUILD_ROWS, 0, FK_DOMAIN, *[a.ctypes.data for a in self.build_host], None, None)
+        tmp = [np.empty(1, np.int64), np.empty(1, np.int64), np.empty(1, np.int32)]
+        q.lib().qdb_gen_join(1000 + rank, 1, PROBE_ROWS, FK_DOMAIN, *[t.ctypes.data for t in tmp],
+                             *[a.ctypes.data for a in self.probe_host])
+        self.dev_build = q.DeviceRowSet(self.build_host)
+        self.dev_probe = q.DeviceRowSet(self.probe_host)
+        self.host_build = q.HostRowSet(self.build_host)
+        self.host_probe = q.HostRowSet(self.probe_host)
+        self.jspec, self.aspec = queries.join_sum(20)
+        self.prog = q.compile_join_aggregate(self.jspec, self.aspec)
+        self.rows = BUILD_ROWS + PROBE_ROWS
+        self.h2d = BUILD_ROWS * 20 + PROBE_ROWS * 16
+
+    def step(self, resident: bool = True) -> tuple[int, int]:
+        q = self.q
+        from qumirdb_b200 import abi
+        J = q.RowJoin(self.prog)
+        J.append(self.dev_build if resident else self.host_build)
+        J.build()
+        agg = q.Aggregate(self.prog)
+        J.probe_aggregate(agg, self.dev_probe if resident else self.host_probe)
+        out = agg.finish()
+        vals, _ = q.read_rowset(out, [abi.I64, abi.I64])
+        res = (int(vals[0][0]), int(vals[1][0]))
+        q.release(out)
+        return res
+
+
+def timed(q, fn, steps: int, warmup: int, dist=None, profile: bool = False):
+    """Device time of `steps` calls of fn on the library's stream (events)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    stream = torch.cuda.ExternalStream(q.lib().qdb_gpu_get_stream())
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    q.synchronize()
+    q.profile(profile)
+    q.profile_read()
+    launches0 = q.launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    results = [fn() for _ in range(steps)]
+    end.record(stream)
+    end.synchronize()
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end) / steps
+    launches = q.launch_count() - launches0
+    kernels = q.profile_read() if profile else []
+    q.profile(False)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, results, launches, kernels
+
+
+def kernel_avg(kernels, name):
+    ks = [(ms, units) for n, ms, units in kernels if n == name]
+    if not ks:
+        return None, None
+    return sum(k[0] for k in ks) / len(ks), sum(k[1] for k in ks) / len(ks)
+
+
+def load_traffic() -> dict:
+    p = ROOT / "profiles" / "traffic.json"
+    return json.loads(p.read_text()) if p.exists() else {}
+
+
+def lineitem_operator(q, peak):
+    from qumirdb_b200 import queries
+    n = LINEITEM_ROWS
+    cols = [np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64),
+            np.empty(n, np.uint8), np.empty(n, np.uint8), np.empty(n, np.int32)]
+    q.lib().qdb_gen_lineitem(0, n, *[c.ctypes.data for c in cols])
+    spec = queries.lineitem_agg(int(cols[6].max()) - 90)
+    prog = q.compile_aggregate(spec)
+    drs = q.DeviceRowSet(cols)
+    flush = q.DeviceBuffer(256 << 20)
+
+    def step():
+        flush_l2(q, flush)
+        agg = q.Aggregate(prog)
+        agg.add(drs)
+        out = agg.finish()
+        q.release(out)
+
+    ms, _, launches, kernels = timed(q, step, 10, 3, profile=True)
+    kms, _ = kernel_avg(kernels, "agg_update")
+    alg = n * 38
+    return {"workload": "lineitem scan-filter-aggregate, 6,001,215 rows, GROUP BY flag, status",
+            "rows_per_s": n / (ms / 1e3), "ms_per_query": ms, "kernel": "agg_update", "kernel_ms": kms,
+            "algorithmic_bytes": alg, "kernel_gbs": alg / (kms / 1e3) / 1e9 if kms else None,
+            "frac_of_measured_hbm": (alg / (kms / 1e3) / 1e9) / peak if kms else None,
+            "l2": "flushed between queries (256 MiB write)", "gpu_launches": launches / 10}
+
+
+def flush_l2(q, buf):
+    q.lib().qdb_gpu_memset(buf.ptr, 0, buf.nbytes)
+
+
+def zipf_operator(q, peak):
+    from qumirdb_b200 import queries
+    n = ZIPF_ROWS
+    cols = [np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.float64)]
+    q.lib().qdb_gen_zipf(2, n, ZIPF_DISTINCT, 1.1, *[c.ctypes.data for c in cols])
+    spec = queries.zipf_agg(expected_groups=ZIPF_DISTINCT)
+    prog = q.compile_aggregate(spec)
+    drs = q.DeviceRowSet(cols)
+    del cols
+    groups = []
+
+    def step():
+        agg = q.Aggregate(prog)
+        agg.add(drs)
+        groups.append(agg.groups)
+        out = agg.finish()
+        q.release(out)
+
+    ms, _, launches, kernels = timed(q, step, 3, 1, profile=True)
+    kms, _ = kernel_avg(kernels, "agg_update")
+    alg = n * 24
+    return {"workload": "GROUP BY key (Zipf 1.1 over 20M), 200M rows, COUNT/SUM/MIN/MAX/SUM(f64)",
+            "rows_per_s": n / (ms / 1e3), "ms_per_query": ms, "groups": groups[-1], "kernel": "agg_update",
+            "kernel_ms": kms, "algorithmic_bytes": alg,
+            "kernel_gbs": alg / (kms / 1e3) / 1e9 if kms else None,
+            "frac_of_measured_hbm": (alg / (kms / 1e3) / 1e9) / peak if kms else None,
+            "l2": "inputs larger than L2", "gpu_launches": launches / 3}
+
+
+def cpu_baseline_join(sample_probe: int, steps: int = 1) -> dict:
+    from oracle import oracle as O
+    import qumirdb_b200 as q
+    b = [np.empty(BUILD_ROWS, np.int64), np.empty(BUILD_ROWS, np.int64), np.empty(BUILD_ROWS, np.int32)]
+    p = [np.empty(sample_probe, np.int64), np.empty(sample_probe, np.int64)]
+    q.lib().qdb_gen_join(1, BUILD_ROWS, 0, FK_DOMAIN, *[x.ctypes.data for x in b], None, None)
+    tmp = [np.empty(1, np.int64), np.empty(1, np.int64), np.empty(1, np.int32)]
+    q.lib().qdb_gen_join(1000, 1, sample_probe, FK_DOMAIN, *[t.ctypes.data for t in tmp], *[x.ctypes.data for x in p])
+    threads = os.cpu_count() or 1
+    times = []
+    s = C.c_int64()
+    c = C.c_int64()
+    for _ in range(steps):
+        t = O.lib().oracle_bench_join_sum(b[0].ctypes.data, b[1].ctypes.data, b[2].ctypes.data, BUILD_ROWS, 20,
+                                          p[0].ctypes.data, p[1].ctypes.data, sample_probe, threads, C.byref(s),
+                                          C.byref(c))
+        times.append(t)
+    sec = min(times)
+    return {"value": (BUILD_ROWS + sample_probe) / sec, "unit": "rows/s", "cores": threads, "kind": "port",
+            "sample": f"build 2,000,000 rows + probe sample of {sample_probe:,} rows (of 120M), threaded "
+                      f"partitioned row-table plan of the CPU restatement", "seconds": sec}
+
+
+def reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sample = 24_000_000
+    steps = max(1, args.steps)
+    cb = cpu_baseline_join(sample, steps=args.warmup + steps)
+    line = {"metric": METRIC, "value": cb["value"], "unit": "rows/s", "n_gpus": args.gpus, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": cb["seconds"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
+            "impl": "reference",
+            "config": {"workload": "equi-join build 2M (attr<20) / probe sample, SUM(payload*value), COUNT(*)",
+                       "build_rows": BUILD_ROWS, "probe_rows": sample},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--no-operators", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    import qumirdb_b200 as q
+    q.init(local)
+    peak, peak_kind = peaks()
+
+    w = JoinWorkload(q, rank)
+
+    def query():
+        s, c = w.step(resident=True)
+        if dist is not None:
+            t = torch.tensor([s, c], device="cuda", dtype=torch.int64)
+            dist.all_reduce(t)
+            return int(t[0]), int(t[1])
+        return s, c
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms, results, launches, kernels = timed(q, query, args.steps, args.warmup, dist=dist, profile=True)
+    clocks = sampler.stop()
+    kms, kunits = kernel_avg(kernels, "join_agg_probe")
+    alg_bytes = PROBE_ROWS * 16
+    achieved = alg_bytes / (kms / 1e3) / 1e9 if kms else None
+    traffic = load_traffic().get("join_agg_probe_bytes_per_probe_row")
+
+    # End to end through the C ABI from pinned host buffers.
+    def query_e2e():
+        s, c = w.step(resident=False)
+        if dist is not None:
+            t = torch.tensor([s, c], device="cuda", dtype=torch.int64)
+            dist.all_reduce(t)
+        return s, c
+
+    ms_e2e, _, _, _ = timed(q, query_e2e, max(1, min(args.steps, 3)), 1, dist=dist)
+
+    line = {
+        "metric": METRIC,
+        "value": world * w.rows / (ms / 1e3),
+        "unit": "rows/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int64",
+        "data": "synthetic (seeded generators with the workload's shapes and distributions)",
+        "config": {"workload": "equi-join: build 2,000,000 rows (unique keys, attr<20 filter fused), probe "
+                               "120,000,000 rows per GPU (fk uniform over 1..2.5M), SUM(payload*value), COUNT(*)",
+                   "build_rows": BUILD_ROWS, "probe_rows_per_gpu": PROBE_ROWS, "parallelism": f"shard{world}",
+                   "l2": "inputs larger than L2 (1.92 GB probe stream per step)",
+                   "result": list(results[-1])},
+        "roofline": {"bound": "hbm", "kernel": "join_agg_probe", "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                     "traffic": traffic * PROBE_ROWS if traffic else None,
+                     "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": kms},
+        "e2e": {"value": world * w.rows / (ms_e2e / 1e3), "unit": "rows/s", "h2d_bytes_per_step": w.h2d,
+                "d2h_bytes_per_step": 16},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_operators:
+        try:
+            line["operators"] = {"lineitem": lineitem_operator(q, peak), "zipf": zipf_operator(q, peak)}
+        except Exception as e:  # reported, never hidden
+            line["operators_error"] = repr(e)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline_join(24_000_000)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

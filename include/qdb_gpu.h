@@ -1,0 +1,440 @@
+/*
+ * qdb_gpu.h — C ABI of the B200 (sm_100a) execution hot path of QumirDB.
+ *
+ * The engine's physical task graph calls its operator kernels through plain
+ * function pointers whose arguments are pointers, integers of at most 64 bits
+ * and bool (qdb/kernel/generated.h:28-51, TKernelSlot::Call).  Each entry
+ * point below takes a compiled program handle as its first argument and then
+ * exactly the arguments of the reference entry it replaces, so the engine's
+ * binding is a closure `[prog](args...) { return qdb_gpu_X(prog, args...); }`
+ * stored in the existing std::function dispatch members
+ * (qdb/kernel/compiler.h:207-242, :363-405, :486-596).
+ *
+ * Programs are built from plain-data descriptors that a lowering fills from
+ * TOperatorKernelSpec (qdb/kernel/spec.h:65-90) instead of from a Qumir AST.
+ * Expression evaluation selects hand-written device functors; there is no JIT.
+ *
+ * Row sets may point at host memory or at device memory (HBM).  Host columns
+ * are staged to the device on each call; device columns are used in place.
+ * Outputs are written where the program's `flags` say (QDB_OUT_DEVICE).
+ *
+ * Every entry point is re-entrant across host threads.  Device work of one
+ * table/arena state runs on the stream that was current when it was
+ * initialised (qdb_gpu_set_stream), so concurrent task states overlap.
+ *
+ * Errors: compile functions return NULL and fill `err`; dispatch entries use
+ * the reference's error conventions (documented per entry) and record a
+ * message retrievable with qdb_gpu_last_error() on the calling thread.
+ * Nothing here falls back to the CPU: a program the device kernels cannot
+ * serve is rejected at compile time.
+ */
+#ifndef QDB_GPU_H
+#define QDB_GPU_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Data ABI — layout-identical to TColumn / TRowSet (qdb/io/io.h:17-39).     */
+/* ------------------------------------------------------------------------ */
+
+typedef struct qdb_column {
+    char* Data;
+    int32_t DataBitOffset;   /* bit offset of bitmap-backed (bool) columns  */
+    const uint8_t* Mask;     /* Arrow validity bitmap; NULL = all valid     */
+    int32_t MaskBitOffset;
+    void* Offsets;           /* string offsets; NULL for fixed width        */
+    uint8_t OffsetWidth;     /* 4 (STRING), 8 (LARGE_STRING), 0 otherwise  */
+} qdb_column;
+
+typedef struct qdb_rowset {
+    qdb_column* Columns;
+    int64_t ColumnCount;
+    int64_t RowCount;
+    uint8_t* Selection;      /* NULL = every row; Selection[i]==0 skips i   */
+    uint64_t* Hash;          /* precomputed shuffle hashes, or NULL         */
+    void (*Destroy)(struct qdb_rowset*);
+    void* Private;
+    int64_t RefCount;
+} qdb_rowset;
+
+/* Value types of columns and expression results. */
+typedef enum qdb_type {
+    QDB_TYPE_INVALID = 0,
+    QDB_TYPE_BOOL = 1,        /* input: bitmap at DataBitOffset (io.h:18);
+                                 project output: one byte 0/1 per row        */
+    QDB_TYPE_I8 = 2,
+    QDB_TYPE_I16 = 3,
+    QDB_TYPE_I32 = 4,
+    QDB_TYPE_I64 = 5,
+    QDB_TYPE_U8 = 6,
+    QDB_TYPE_U16 = 7,
+    QDB_TYPE_U32 = 8,
+    QDB_TYPE_U64 = 9,
+    QDB_TYPE_F32 = 10,
+    QDB_TYPE_F64 = 11,
+    QDB_TYPE_DATE32 = 12,     /* i32 days since 1970-01-01 (qdb/plan/types/date.h:14-29) */
+    QDB_TYPE_DECIMAL64 = 13,  /* unscaled i64, precision <= 18 (qdb/plan/types/decimal.h:80-99) */
+    QDB_TYPE_DECIMAL128 = 14, /* unscaled i128 "BinInt", precision 19..38     */
+    QDB_TYPE_CHAR1 = 15       /* a string column whose values are one byte,
+                                 staged as one code byte per row             */
+} qdb_type;
+
+typedef struct qdb_column_type {
+    int32_t type;       /* qdb_type                                          */
+    int32_t precision;  /* decimals only                                     */
+    int32_t scale;      /* decimals only                                     */
+    int32_t nullable;   /* non-zero: the column may carry a validity mask    */
+} qdb_column_type;
+
+/* ------------------------------------------------------------------------ */
+/* Expressions: a flat array of nodes, operands before their users.          */
+/* Types are the lowering's annotated result types (AnnotateExprType,        */
+/* qdb/kernel/annotate_type.cpp:725-945); arithmetic follows them exactly:   */
+/*   integer ops wrap in the result width; DECIMAL +/- rescale operands to   */
+/*   the result scale; DECIMAL * multiplies unscaled values (scales add);    */
+/*   DECIMAL / integer truncates toward zero keeping the dividend's scale    */
+/*   (qdb/modules/qumirdb_runtime.cpp:703-705); comparisons align scales.   */
+/* ------------------------------------------------------------------------ */
+
+typedef enum qdb_expr_op {
+    QDB_EXPR_COLUMN = 1,      /* input column `column`                      */
+    QDB_EXPR_CONST = 2,       /* imm_lo/imm_hi (f64 bits in imm_lo)          */
+    QDB_EXPR_NULL = 3,
+    QDB_EXPR_ADD = 4,
+    QDB_EXPR_SUB = 5,
+    QDB_EXPR_MUL = 6,
+    QDB_EXPR_DIV = 7,
+    QDB_EXPR_NEG = 8,
+    QDB_EXPR_CAST = 9,        /* args[0] converted to `type`/`scale`         */
+    QDB_EXPR_EQ = 10,
+    QDB_EXPR_NE = 11,
+    QDB_EXPR_LT = 12,
+    QDB_EXPR_LE = 13,
+    QDB_EXPR_GT = 14,
+    QDB_EXPR_GE = 15,
+    QDB_EXPR_AND = 16,
+    QDB_EXPR_OR = 17,
+    QDB_EXPR_NOT = 18,
+    QDB_EXPR_BETWEEN = 19,    /* args[1] <= args[0] <= args[2]               */
+    QDB_EXPR_IN_LIST = 20,    /* args[0] IN list[0..list_len)                */
+    QDB_EXPR_CASE = 21,       /* CASE WHEN args[0] THEN args[1] ELSE args[2] */
+    QDB_EXPR_IS_NULL = 22,
+    QDB_EXPR_IS_NOT_NULL = 23,
+    QDB_EXPR_MOD = 24         /* remainder, sign of the dividend (truncating) */
+} qdb_expr_op;
+
+typedef struct qdb_expr {
+    int32_t op;         /* qdb_expr_op                                       */
+    int32_t type;       /* qdb_type of the result                            */
+    int32_t scale;      /* decimal scale of the result                       */
+    int32_t column;     /* QDB_EXPR_COLUMN: input column index               */
+    int32_t args[3];    /* operand node indices, each below this node's      */
+    int32_t list_len;   /* QDB_EXPR_IN_LIST                                  */
+    int64_t imm_lo;     /* QDB_EXPR_CONST low word                           */
+    int64_t imm_hi;     /* QDB_EXPR_CONST high word (DECIMAL128)             */
+    const int64_t* list;/* IN-list constants, in args[0]'s type and scale    */
+} qdb_expr;
+
+/* Program flags. */
+#define QDB_OUT_DEVICE 1u   /* outputs stay in device memory                 */
+
+/* ------------------------------------------------------------------------ */
+/* Aggregate: fused filter -> project -> hash aggregate.                    */
+/* ------------------------------------------------------------------------ */
+
+/* Reducers of qdb/kernel/gen.cpp:3301-3593; AVG is lowered by the planner  */
+/* into SUM and COUNT (qdb/plan/sql_lowering.cpp:799-814).                  */
+typedef enum qdb_agg_func {
+    QDB_AGG_COUNT_STAR = 1,
+    QDB_AGG_COUNT = 2,
+    QDB_AGG_SUM = 3,
+    QDB_AGG_MIN = 4,
+    QDB_AGG_MAX = 5
+} qdb_agg_func;
+
+typedef struct qdb_agg_item {
+    int32_t func;       /* qdb_agg_func                                      */
+    int32_t arg;        /* expression node, -1 for COUNT(*)                  */
+} qdb_agg_item;
+
+typedef struct qdb_aggregate_spec {
+    int32_t n_columns;
+    const qdb_column_type* columns;   /* input batch schema                 */
+    int32_t n_nodes;
+    const qdb_expr* nodes;
+    int32_t filter;                   /* predicate node, -1 for none        */
+    int32_t n_keys;
+    const int32_t* keys;              /* GROUP BY key expression nodes      */
+    int32_t n_aggs;
+    const qdb_agg_item* aggs;
+    /* Optional projection over the aggregate row (keys ++ aggregate        */
+    /* results, in that order): output column k is output_nodes[outputs[k]] */
+    /* whose COLUMN leaves index that row.  n_outputs == 0 emits the row.    */
+    int32_t n_outputs;
+    const int32_t* outputs;
+    int32_t n_output_nodes;
+    const qdb_expr* output_nodes;
+    uint32_t flags;                   /* QDB_OUT_DEVICE                     */
+    int64_t expected_groups;          /* sizing hint, 0 = unknown           */
+} qdb_aggregate_spec;
+
+/* agg_dispatch op codes (EAggregateKernelOp, qdb/kernel/compiler.h:217-230). */
+#define QDB_AGG_OP_INIT 0
+#define QDB_AGG_OP_UPDATE 1
+#define QDB_AGG_OP_INIT_ROWS 3
+#define QDB_AGG_OP_SWITCH_TO_ROWS_AT 4
+#define QDB_AGG_OP_EXPECT_ROW_GROUPS 5
+
+/* Size of the caller-owned, zero-initialised table state (HashTableSize,   */
+/* qdb/kernel/compiler.h:603).  The int64 at byte offset 72 is the group    */
+/* count (HashTable.Size), kept current after every call, as the processor   */
+/* reads it (qdb/exec/aggregate_exec.cpp:18-38, :128).                       */
+#define QDB_HASH_TABLE_SIZE 304
+
+/* ------------------------------------------------------------------------ */
+/* Row join (inner equi-join, build side fixed).                            */
+/* ------------------------------------------------------------------------ */
+
+typedef enum qdb_join_type {
+    QDB_JOIN_INNER = 0
+} qdb_join_type;
+
+typedef struct qdb_row_join_spec {
+    int32_t join_type;                 /* qdb_join_type                      */
+    int32_t build_is_left;             /* pair/output order (left, right)    */
+    int32_t n_build_columns;
+    const qdb_column_type* build_columns;
+    int32_t n_probe_columns;
+    const qdb_column_type* probe_columns;
+    int32_t n_keys;
+    const int32_t* build_keys;         /* build column per key               */
+    const int32_t* probe_keys;         /* probe column per key               */
+    int32_t n_payload;
+    const int32_t* build_payload;      /* build columns kept in the rows     */
+    /* Materialize output: column k is probe column out_column[k] when       */
+    /* out_side[k] == 0, else build payload out_column[k].                   */
+    int32_t n_out;
+    const int32_t* out_side;
+    const int32_t* out_column;
+    /* Optional build-side predicate fused into Append (-1 = none); its      */
+    /* COLUMN leaves index the build schema.                                 */
+    int32_t n_build_nodes;
+    const qdb_expr* build_nodes;
+    int32_t build_filter;
+    uint32_t flags;                    /* QDB_OUT_DEVICE                     */
+} qdb_row_join_spec;
+
+/* jr_dispatch op codes (ERowJoinKernelOp, qdb/kernel/compiler.h:363-388). */
+#define QDB_JR_OP_INIT 0
+#define QDB_JR_OP_APPEND 1
+#define QDB_JR_OP_BUILD 2
+#define QDB_JR_OP_PROBE 3
+
+/* Caller-owned zeroed state sizes (qdb/kernel/compiler.h:599-621).  The    */
+/* pair buffer's int64 at offset 0 is its pair count, read by               */
+/* TRowJoinProcessor::ProbeBatch (qdb/exec/row_join_exec.cpp:176).           */
+#define QDB_ROW_ARENA_SIZE 56
+#define QDB_ROW_TABLE_SIZE 48
+#define QDB_ROW_SCRATCH_SIZE 64
+#define QDB_PAIR_BUFFER_SIZE 24
+
+/* ------------------------------------------------------------------------ */
+/* Sort (ORDER BY over packed row ids) and top-K.                           */
+/* ------------------------------------------------------------------------ */
+
+typedef struct qdb_sort_key {
+    int32_t column;      /* key column of the store's row sets               */
+    int32_t desc;        /* default direction; the run's descs[] overrides   */
+    int32_t nulls_first; /* default; the run's nulls_firsts[] overrides      */
+    int32_t pad;
+} qdb_sort_key;
+
+typedef struct qdb_sort_spec {
+    int32_t n_columns;
+    const qdb_column_type* columns;    /* schema of every stored row set     */
+    int32_t n_keys;
+    const qdb_sort_key* keys;          /* most significant first             */
+    int32_t n_out;
+    const int32_t* out_columns;        /* materialized columns               */
+    uint32_t flags;                    /* QDB_OUT_DEVICE                     */
+} qdb_sort_spec;
+
+/* ------------------------------------------------------------------------ */
+/* Programs.                                                                */
+/* ------------------------------------------------------------------------ */
+
+typedef struct qdb_gpu_program qdb_gpu_program;
+
+/* TKernelCompiler::CompileAggregate (qdb/kernel/compiler.h:659-663).       */
+qdb_gpu_program* qdb_gpu_compile_aggregate(
+    const qdb_aggregate_spec* spec, char* err, size_t err_len);
+
+/* TKernelCompiler::CompileFilter (qdb/kernel/compiler.h:632-633).          */
+qdb_gpu_program* qdb_gpu_compile_filter(
+    int32_t n_columns, const qdb_column_type* columns,
+    int32_t n_nodes, const qdb_expr* nodes, int32_t predicate,
+    char* err, size_t err_len);
+
+/* TKernelCompiler::CompileProject (qdb/kernel/compiler.h:640-642): output   */
+/* k is node exprs[k], written as its qdb_type's storage width.              */
+qdb_gpu_program* qdb_gpu_compile_project(
+    int32_t n_columns, const qdb_column_type* columns,
+    int32_t n_nodes, const qdb_expr* nodes,
+    int32_t n_exprs, const int32_t* exprs,
+    char* err, size_t err_len);
+
+/* TKernelCompiler::CompileAggregateHash / CompileJoinHash                  */
+/* (qdb/kernel/compiler.h:691-697): rh_hash of the key columns.              */
+qdb_gpu_program* qdb_gpu_compile_hash(
+    int32_t n_columns, const qdb_column_type* columns,
+    int32_t n_keys, const int32_t* key_columns,
+    char* err, size_t err_len);
+
+/* TKernelCompiler::CompileRowJoin (qdb/kernel/compiler.h:677-679).         */
+qdb_gpu_program* qdb_gpu_compile_row_join(
+    const qdb_row_join_spec* spec, char* err, size_t err_len);
+
+/* Join fused with the aggregate downstream of it: `agg`'s input schema is   */
+/* the probe columns followed by the build payload columns.  No reference    */
+/* counterpart: it replaces the row join -> project -> aggregate chain       */
+/* (qdb/exec/row_join_exec.cpp:166-188 feeding aggregate_exec.cpp:104-117).  */
+qdb_gpu_program* qdb_gpu_compile_join_aggregate(
+    const qdb_row_join_spec* join, const qdb_aggregate_spec* agg,
+    char* err, size_t err_len);
+
+/* TKernelCompiler::CompileRadixSortComposite / CompileHeapTopK             */
+/* (qdb/kernel/compiler.h:644-653).                                          */
+qdb_gpu_program* qdb_gpu_compile_sort(
+    const qdb_sort_spec* spec, char* err, size_t err_len);
+
+void qdb_gpu_program_destroy(qdb_gpu_program* program);
+
+/* ------------------------------------------------------------------------ */
+/* Reference-shaped entry points.                                           */
+/* ------------------------------------------------------------------------ */
+
+/* agg_dispatch(ht, batch, arg, op) (qdb/kernel/compiler.h:207-230).         */
+/* Init/InitRows return 0 on failure; Update returns < 0 on failure; an op   */
+/* the kernel does not serve returns 0 and changes nothing.                  */
+int64_t qdb_gpu_agg_dispatch(const qdb_gpu_program* program, void* ht,
+                             qdb_rowset* batch, int64_t arg, int64_t op);
+
+/* agg_finish_rowset(ht, out) (qdb/kernel/compiler.h:232-242): writes every  */
+/* group into `out`, returns the group count (< 0 on failure) and destroys   */
+/* the table.  `out->Destroy` frees the output buffers.                      */
+int64_t qdb_gpu_agg_finish_rowset(const qdb_gpu_program* program, void* ht,
+                                  qdb_rowset* out);
+
+/* TFilterDispatch (qdb/kernel/compiler.h:488-495): writes rs->Selection     */
+/* (allocated by the caller, RowCount bytes) for the rows input_selection    */
+/* selects (NULL = all); NULL predicates reject.                             */
+void qdb_gpu_filter(const qdb_gpu_program* program, qdb_rowset* rs,
+                    const uint8_t* input_selection);
+
+/* TProjectDispatch (qdb/kernel/compiler.h:502-510).  `arena` is unused.     */
+void qdb_gpu_project(const qdb_gpu_program* program, qdb_rowset* in,
+                     void** out_buffers, void* arena,
+                     const uint8_t* input_selection);
+
+/* Hash dispatch (qdb/kernel/compiler.h:426-438, :513-520): one uint64 per   */
+/* selected row, equal to the engine's rh_hash of the key (gen.cpp:233-379), */
+/* so hash % P routes rows as THashShuffleTask does                          */
+/* (qdb/scheduler/tasks/runtime_adapter.cpp:1001-1003).                      */
+bool qdb_gpu_hash(const qdb_gpu_program* program, qdb_rowset* batch,
+                  uint64_t* hashes);
+
+/* jr_dispatch(arena, table, scratch, pairs, batch, op)                      */
+/* (qdb/kernel/compiler.h:390-395); returns false on failure.                */
+bool qdb_gpu_jr_dispatch(const qdb_gpu_program* program, void* arena,
+                         void* table, void* scratch, void* pairs,
+                         qdb_rowset* batch, int64_t op);
+
+/* jr_materialize(pairs, stream, start, limit, out)                          */
+/* (qdb/kernel/compiler.h:397-405): returns the rows written (<= limit).     */
+int64_t qdb_gpu_jr_materialize(const qdb_gpu_program* program, void* pairs,
+                               qdb_rowset* stream, int64_t start,
+                               int64_t limit, qdb_rowset* out);
+
+/* Probe of a fused join-aggregate program: probes `batch` against the built */
+/* arena/table and folds the joined rows into the aggregate state `ht`.      */
+/* Returns the matched pair count, < 0 on failure.                           */
+int64_t qdb_gpu_join_aggregate_probe(const qdb_gpu_program* program,
+                                     void* arena, void* table, void* ht,
+                                     qdb_rowset* batch);
+
+/* qdb_sort_run (qdb/kernel/compiler.h:522-541, compiler.cpp:1165-1218).     */
+/* With do_sort, sorts the n packed row ids (batch << 32 | row) in place by  */
+/* the keys, stable in input order; then materializes [start, start+limit)   */
+/* into `out` and returns its row count (0 at the end).  `work`/`counts`     */
+/* may be NULL: the device path keeps its own scratch.                       */
+int64_t qdb_gpu_sort_run(const qdb_gpu_program* program, qdb_rowset* store,
+                         int64_t* row_ids, int64_t* work, uint32_t* counts,
+                         int64_t n, bool* descs, bool* nulls_firsts,
+                         bool do_sort, int64_t start, int64_t limit,
+                         qdb_rowset* out);
+
+/* qdb_top_k_select (THeapTopKDispatch, qdb/kernel/compiler.h:585-596):      */
+/* keeps the first `limit` row ids of the stable order in row_ids[0..k)      */
+/* and returns k.                                                            */
+int64_t qdb_gpu_top_k_select(const qdb_gpu_program* program, qdb_rowset* store,
+                             int64_t* row_ids, int64_t size, int64_t limit);
+
+/* ------------------------------------------------------------------------ */
+/* Runtime.                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* Binds the calling thread to `device` (call once per thread). 0 = ok.      */
+int qdb_gpu_init(int device);
+/* Last error message of the calling thread ("" if none).                    */
+const char* qdb_gpu_last_error(void);
+/* cudaStream_t used by states initialised after this call on this thread;   */
+/* NULL selects the library's own stream.                                    */
+void qdb_gpu_set_stream(void* stream);
+void* qdb_gpu_get_stream(void);
+int qdb_gpu_synchronize(void);
+
+/* Device and pinned host memory for column staging (the column cache).      */
+void* qdb_gpu_alloc(size_t bytes);
+void qdb_gpu_free(void* ptr);
+void* qdb_gpu_host_alloc(size_t bytes);
+void qdb_gpu_host_free(void* ptr);
+int qdb_gpu_memcpy(void* dst, const void* src, size_t bytes);   /* async on the current stream */
+int qdb_gpu_memset(void* dst, int value, size_t bytes);
+
+/* Kernel timing: when enabled, every kernel launch of this library is       */
+/* bracketed by CUDA events on its stream.  `read` copies up to `cap`        */
+/* records (name, milliseconds) and clears the log; returns the count.       */
+typedef struct qdb_gpu_kernel_time {
+    char name[48];
+    double ms;
+    int64_t units;       /* rows (or items) the launch processed            */
+} qdb_gpu_kernel_time;
+void qdb_gpu_profile_enable(int on);
+int64_t qdb_gpu_profile_read(qdb_gpu_kernel_time* out, int64_t cap);
+/* Kernel launches of this library since the counter was last reset.         */
+int64_t qdb_gpu_launch_count(int reset);
+
+/* Seeded synthetic generators for the benchmark configurations (host, all   */
+/* cores).  Every generator is deterministic in (seed, row).                 */
+void qdb_gen_lineitem(uint64_t seed, int64_t rows, int64_t* qty, int64_t* price,
+                      int64_t* disc, int64_t* tax, uint8_t* flag, uint8_t* status,
+                      int32_t* shipdate);
+void qdb_gen_join(uint64_t seed, int64_t build_rows, int64_t probe_rows,
+                  int64_t fk_domain, int64_t* b_key, int64_t* b_payload,
+                  int32_t* b_attr, int64_t* p_fk, int64_t* p_value);
+void qdb_gen_zipf(uint64_t seed, int64_t rows, int64_t distinct, double s,
+                  int64_t* key, int64_t* a, double* x);
+void qdb_gen_sort(uint64_t seed, int64_t rows, int64_t* k1, int32_t* k2,
+                  int64_t* rowid);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QDB_GPU_H */

@@ -1,0 +1,1503 @@
+// oracle.cpp — CPU restatement of QumirDB's hot-path algorithms.
+//
+// TEST INFRASTRUCTURE ONLY: the checker of the device kernels.  Nothing in the
+// product links or loads this library.  Every routine names the reference
+// file:line whose behaviour it restates; the code is written from the
+// behaviour, not translated from the oz sources.
+#include "oracle.h"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <queue>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+using i128 = __int128;
+using u128 = unsigned __int128;
+
+struct Error : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void SetErr(char* err, size_t len, const char* msg) {
+    if (err && len) {
+        std::snprintf(err, len, "%s", msg);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Values.  Integers, dates, chars and decimals live sign-extended in `i`
+// (decimals unscaled); doubles in `f`; booleans as 0/1 in `i`.
+// ---------------------------------------------------------------------------
+struct Val {
+    i128 i = 0;
+    double f = 0.0;
+    bool null = false;
+};
+
+bool IsFloat(int t) { return t == QDB_TYPE_F32 || t == QDB_TYPE_F64; }
+bool IsDecimal(int t) { return t == QDB_TYPE_DECIMAL64 || t == QDB_TYPE_DECIMAL128; }
+bool IsUnsigned(int t) {
+    return t == QDB_TYPE_U8 || t == QDB_TYPE_U16 || t == QDB_TYPE_U32 || t == QDB_TYPE_U64;
+}
+
+int WidthBits(int t) {
+    switch (t) {
+        case QDB_TYPE_BOOL: return 1;
+        case QDB_TYPE_I8: case QDB_TYPE_U8: case QDB_TYPE_CHAR1: return 8;
+        case QDB_TYPE_I16: case QDB_TYPE_U16: return 16;
+        case QDB_TYPE_I32: case QDB_TYPE_U32: case QDB_TYPE_DATE32: case QDB_TYPE_F32: return 32;
+        case QDB_TYPE_I64: case QDB_TYPE_U64: case QDB_TYPE_DECIMAL64: case QDB_TYPE_F64: return 64;
+        case QDB_TYPE_DECIMAL128: return 128;
+    }
+    throw Error("unknown type");
+}
+
+int StorageBytes(int t) {
+    if (t == QDB_TYPE_BOOL) return 1;
+    return WidthBits(t) / 8;
+}
+
+// Wraps an integer result to its type's width, as the reference's fixed-width
+// arithmetic does (integer ops wrap; decimals wrap at 64 or 128 bits,
+// qdb/modules/qumirdb.oz:1305-1321).
+i128 Wrap(i128 v, int t) {
+    const int bits = WidthBits(t);
+    if (bits >= 128) return v;
+    const u128 mask = (u128(1) << bits) - 1;
+    u128 u = u128(v) & mask;
+    if (!IsUnsigned(t) && t != QDB_TYPE_CHAR1 && t != QDB_TYPE_BOOL) {
+        if (u >> (bits - 1)) u |= ~mask;   // sign extend
+    }
+    return i128(u);
+}
+
+i128 Pow10(int k) {
+    i128 r = 1;
+    for (int j = 0; j < k; ++j) r *= 10;
+    return r;
+}
+
+bool MaskBit(const uint8_t* mask, int64_t bit) {
+    return (mask[bit >> 3] >> (bit & 7)) & 1;
+}
+
+// Reads row `row` of a column (TColumn, qdb/io/io.h:17-24): Arrow validity
+// bits, bitmap-backed booleans at DataBitOffset, fixed-width values.
+Val ReadCell(const qdb_column& c, const qdb_column_type& t, int64_t row) {
+    Val v;
+    if (c.Mask && !MaskBit(c.Mask, c.MaskBitOffset + row)) {
+        v.null = true;
+        return v;
+    }
+    const char* d = c.Data;
+    switch (t.type) {
+        case QDB_TYPE_BOOL: v.i = MaskBit(reinterpret_cast<const uint8_t*>(d), c.DataBitOffset + row); break;
+        case QDB_TYPE_I8: v.i = reinterpret_cast<const int8_t*>(d)[row]; break;
+        case QDB_TYPE_I16: v.i = reinterpret_cast<const int16_t*>(d)[row]; break;
+        case QDB_TYPE_I32: case QDB_TYPE_DATE32: v.i = reinterpret_cast<const int32_t*>(d)[row]; break;
+        case QDB_TYPE_I64: case QDB_TYPE_DECIMAL64: v.i = reinterpret_cast<const int64_t*>(d)[row]; break;
+        case QDB_TYPE_U8: case QDB_TYPE_CHAR1: v.i = reinterpret_cast<const uint8_t*>(d)[row]; break;
+        case QDB_TYPE_U16: v.i = reinterpret_cast<const uint16_t*>(d)[row]; break;
+        case QDB_TYPE_U32: v.i = reinterpret_cast<const uint32_t*>(d)[row]; break;
+        case QDB_TYPE_U64: v.i = reinterpret_cast<const uint64_t*>(d)[row]; break;
+        case QDB_TYPE_F32: v.f = reinterpret_cast<const float*>(d)[row]; break;
+        case QDB_TYPE_F64: v.f = reinterpret_cast<const double*>(d)[row]; break;
+        case QDB_TYPE_DECIMAL128: {
+            const uint64_t* w = reinterpret_cast<const uint64_t*>(d) + 2 * row;
+            v.i = i128((u128(uint64_t(w[1])) << 64) | w[0]);
+            break;
+        }
+        default: throw Error("unsupported column type");
+    }
+    return v;
+}
+
+double ToDouble(const Val& v, int t, int scale) {
+    if (IsFloat(t)) return v.f;
+    if (IsDecimal(t)) return double(v.i) / std::pow(10.0, scale);
+    return double(v.i);
+}
+
+// ---------------------------------------------------------------------------
+// Expression evaluation under the lowering's annotated types
+// (qdb/kernel/annotate_type.cpp:725-945, qdb/modules/qumirdb.oz:1290-1330,
+// qdb/modules/qumirdb_runtime.cpp:680-735).
+// ---------------------------------------------------------------------------
+struct Expr {
+    const qdb_expr* nodes;
+    int32_t n;
+};
+
+int CmpAligned(const Val& a, int ta, int sa, const Val& b, int tb, int sb) {
+    if (IsFloat(ta) || IsFloat(tb)) {
+        const double x = ToDouble(a, ta, sa), y = ToDouble(b, tb, sb);
+        return x < y ? -1 : (x > y ? 1 : 0);
+    }
+    const int s = std::max(IsDecimal(ta) ? sa : 0, IsDecimal(tb) ? sb : 0);
+    const i128 x = a.i * Pow10(s - (IsDecimal(ta) ? sa : 0));
+    const i128 y = b.i * Pow10(s - (IsDecimal(tb) ? sb : 0));
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+// Aligns an integer/decimal operand to the result scale of +/- and CASE.
+i128 AtScale(const Val& v, int t, int s, int target) {
+    const int from = IsDecimal(t) ? s : 0;
+    if (target >= from) return v.i * Pow10(target - from);
+    return v.i / Pow10(from - target);
+}
+
+// Evaluates every node up to and including `root` for one row; `leaf(col)`
+// returns input column values.  Division by zero raises (deferred row error,
+// docs/arch/scheduler_runtime.md:174-186).
+void EvalAll(const Expr& e, int32_t root, const std::function<Val(int32_t)>& leaf,
+             std::vector<Val>& out) {
+    out.resize(root + 1);
+    for (int32_t k = 0; k <= root; ++k) {
+        const qdb_expr& n = e.nodes[k];
+        Val r;
+        auto A = [&](int j) -> const Val& { return out[n.args[j]]; };
+        auto T = [&](int j) { return e.nodes[n.args[j]].type; };
+        auto S = [&](int j) { return e.nodes[n.args[j]].scale; };
+        switch (n.op) {
+            case QDB_EXPR_COLUMN: r = leaf(n.column); break;
+            case QDB_EXPR_CONST:
+                if (IsFloat(n.type)) {
+                    std::memcpy(&r.f, &n.imm_lo, 8);
+                } else if (n.type == QDB_TYPE_DECIMAL128) {
+                    r.i = i128((u128(uint64_t(n.imm_hi)) << 64) | uint64_t(n.imm_lo));
+                } else {
+                    r.i = n.imm_lo;
+                }
+                break;
+            case QDB_EXPR_NULL: r.null = true; break;
+            case QDB_EXPR_MOD: {
+                // Operands share the result scale; the remainder takes the
+                // dividend's sign (qdb/modules/qumirdb.oz:1323-1328).
+                const Val& a = A(0); const Val& b = A(1);
+                if (a.null || b.null) { r.null = true; break; }
+                const int rs = IsDecimal(n.type) ? n.scale : 0;
+                const i128 x = AtScale(a, T(0), S(0), rs), y = AtScale(b, T(1), S(1), rs);
+                if (y == 0) throw Error("division by zero");
+                r.i = Wrap(x % y, n.type);
+                break;
+            }
+            case QDB_EXPR_ADD: case QDB_EXPR_SUB: case QDB_EXPR_MUL: case QDB_EXPR_DIV: {
+                const Val& a = A(0); const Val& b = A(1);
+                if (a.null || b.null) { r.null = true; break; }
+                if (IsFloat(n.type)) {
+                    const double x = ToDouble(a, T(0), S(0)), y = ToDouble(b, T(1), S(1));
+                    r.f = n.op == QDB_EXPR_ADD ? x + y : n.op == QDB_EXPR_SUB ? x - y
+                        : n.op == QDB_EXPR_MUL ? x * y : x / y;
+                    if (n.type == QDB_TYPE_F32) r.f = float(r.f);
+                    break;
+                }
+                if (n.op == QDB_EXPR_ADD || n.op == QDB_EXPR_SUB) {
+                    const i128 x = AtScale(a, T(0), S(0), IsDecimal(n.type) ? n.scale : 0);
+                    const i128 y = AtScale(b, T(1), S(1), IsDecimal(n.type) ? n.scale : 0);
+                    r.i = Wrap(n.op == QDB_EXPR_ADD ? i128(u128(x) + u128(y)) : i128(u128(x) - u128(y)), n.type);
+                } else if (n.op == QDB_EXPR_MUL) {
+                    // Unscaled operands multiply; the scales add up to the
+                    // result's (DecimalProductSpec, annotate_type.cpp:746-760).
+                    const int sa = IsDecimal(T(0)) ? S(0) : 0, sb = IsDecimal(T(1)) ? S(1) : 0;
+                    i128 p = i128(u128(a.i) * u128(b.i));
+                    const int rs = IsDecimal(n.type) ? n.scale : 0;
+                    if (rs > sa + sb) p = i128(u128(p) * u128(Pow10(rs - sa - sb)));
+                    r.i = Wrap(p, n.type);
+                } else {
+                    if (b.i == 0) throw Error("division by zero");
+                    // DECIMAL / integer keeps the dividend's scale
+                    // (annotate_type.cpp:908-910); DECIMAL / DECIMAL scales the
+                    // dividend to the quotient's scale first.
+                    const int sa = IsDecimal(T(0)) ? S(0) : 0, sb = IsDecimal(T(1)) ? S(1) : 0;
+                    const int rs = IsDecimal(n.type) ? n.scale : 0;
+                    const i128 x = a.i * Pow10(std::max(0, rs - sa + sb));
+                    r.i = Wrap(x / b.i, n.type);
+                }
+                break;
+            }
+            case QDB_EXPR_NEG: {
+                const Val& a = A(0);
+                if (a.null) { r.null = true; break; }
+                if (IsFloat(n.type)) r.f = -ToDouble(a, T(0), S(0));
+                else r.i = Wrap(i128(u128(0) - u128(a.i)), n.type);
+                break;
+            }
+            case QDB_EXPR_CAST: {
+                const Val& a = A(0);
+                if (a.null) { r.null = true; break; }
+                if (IsFloat(n.type)) {
+                    r.f = ToDouble(a, T(0), S(0));
+                    if (n.type == QDB_TYPE_F32) r.f = float(r.f);
+                } else if (IsFloat(T(0))) {
+                    r.i = Wrap(i128(int64_t(a.f)), n.type);
+                } else {
+                    r.i = Wrap(AtScale(a, T(0), S(0), IsDecimal(n.type) ? n.scale : 0), n.type);
+                }
+                break;
+            }
+            case QDB_EXPR_EQ: case QDB_EXPR_NE: case QDB_EXPR_LT: case QDB_EXPR_LE:
+            case QDB_EXPR_GT: case QDB_EXPR_GE: {
+                const Val& a = A(0); const Val& b = A(1);
+                if (a.null || b.null) { r.null = true; break; }
+                const int c = CmpAligned(a, T(0), S(0), b, T(1), S(1));
+                bool t = false;
+                switch (n.op) {
+                    case QDB_EXPR_EQ: t = c == 0; break;
+                    case QDB_EXPR_NE: t = c != 0; break;
+                    case QDB_EXPR_LT: t = c < 0; break;
+                    case QDB_EXPR_LE: t = c <= 0; break;
+                    case QDB_EXPR_GT: t = c > 0; break;
+                    default: t = c >= 0; break;
+                }
+                // A NaN compares false everywhere but !=.
+                if ((IsFloat(T(0)) || IsFloat(T(1))) &&
+                    (std::isnan(ToDouble(a, T(0), S(0))) || std::isnan(ToDouble(b, T(1), S(1))))) {
+                    t = n.op == QDB_EXPR_NE;
+                }
+                r.i = t;
+                break;
+            }
+            case QDB_EXPR_AND: {
+                // SQL three-valued logic (test/test_filter.cpp semantics).
+                const Val& a = A(0); const Val& b = A(1);
+                if ((!a.null && a.i == 0) || (!b.null && b.i == 0)) { r.i = 0; }
+                else if (a.null || b.null) { r.null = true; }
+                else r.i = 1;
+                break;
+            }
+            case QDB_EXPR_OR: {
+                const Val& a = A(0); const Val& b = A(1);
+                if ((!a.null && a.i) || (!b.null && b.i)) { r.i = 1; }
+                else if (a.null || b.null) { r.null = true; }
+                else r.i = 0;
+                break;
+            }
+            case QDB_EXPR_NOT: {
+                const Val& a = A(0);
+                if (a.null) r.null = true; else r.i = a.i ? 0 : 1;
+                break;
+            }
+            case QDB_EXPR_BETWEEN: {
+                const Val& a = A(0); const Val& lo = A(1); const Val& hi = A(2);
+                if (a.null || lo.null || hi.null) { r.null = true; break; }
+                r.i = CmpAligned(a, T(0), S(0), lo, T(1), S(1)) >= 0 &&
+                      CmpAligned(a, T(0), S(0), hi, T(2), S(2)) <= 0;
+                break;
+            }
+            case QDB_EXPR_IN_LIST: {
+                const Val& a = A(0);
+                if (a.null) { r.null = true; break; }
+                bool found = false;
+                for (int32_t j = 0; j < n.list_len && !found; ++j) {
+                    if (IsFloat(T(0))) {
+                        double x; std::memcpy(&x, &n.list[j], 8);
+                        found = x == a.f;
+                    } else {
+                        found = i128(n.list[j]) == a.i;
+                    }
+                }
+                r.i = found;
+                break;
+            }
+            case QDB_EXPR_CASE: {
+                const Val& c = A(0);
+                const bool take = !c.null && c.i;
+                const Val& v = take ? A(1) : A(2);
+                const int vt = take ? T(1) : T(2), vs = take ? S(1) : S(2);
+                r = v;
+                if (!v.null) {
+                    if (IsFloat(n.type)) r.f = ToDouble(v, vt, vs);
+                    else r.i = Wrap(AtScale(v, vt, vs, IsDecimal(n.type) ? n.scale : 0), n.type);
+                }
+                break;
+            }
+            case QDB_EXPR_IS_NULL: r.i = A(0).null ? 1 : 0; break;
+            case QDB_EXPR_IS_NOT_NULL: r.i = A(0).null ? 0 : 1; break;
+            default: throw Error("unsupported expression op");
+        }
+        out[k] = r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Key hashing: HashKeyValue (qdb/kernel/gen.cpp:233-379), rh_hash(i64)
+// (qdb/kernel/aggregation/key_ops_i64.oz:4-11) and qdb_string_hash_bytes for
+// short strings (qdb/modules/qumirdb_runtime.cpp:270-300).
+// ---------------------------------------------------------------------------
+uint64_t MixU64(uint64_t h) {
+    h ^= h >> 12;
+    h ^= h << 25;
+    h ^= h >> 27;
+    return h * 2685821657736338717ULL;
+}
+
+uint64_t ByteSwap(uint64_t x) { return __builtin_bswap64(x); }
+
+uint64_t StringHash(const uint8_t* d, int64_t n) {
+    const uint64_t mul0 = 11400714785074694791ULL, mul1 = 14029467366897019727ULL;
+    if (n == 0) return 1;
+    if (n <= 3) {
+        const uint32_t x = (uint32_t(n) << 24) ^ (uint32_t(d[0]) << 16) ^
+                           (uint32_t(d[n / 2]) << 8) ^ d[n - 1];
+        return ByteSwap(mul0 * x);
+    }
+    if (n <= 8) {
+        uint32_t x, y;
+        std::memcpy(&x, d + n - 4, 4);
+        std::memcpy(&y, d, 4);
+        return uint64_t(n) ^ ByteSwap(mul0 * x) ^ ByteSwap(mul1 * y);
+    }
+    if (n <= 16) {
+        uint64_t x, y;
+        std::memcpy(&x, d + n - 8, 8);
+        std::memcpy(&y, d, 8);
+        return uint64_t(n) ^ ByteSwap(mul0 * x) ^ ByteSwap(mul1 * y);
+    }
+    throw Error("strings above 16 bytes hash with XXH3; not restated");
+}
+
+// Canonical float bits: -0 -> +0, every NaN -> one quiet NaN
+// (docs/arch/aggregation.md:109-125).
+uint64_t CanonicalF64Bits(double f) {
+    if (f == 0.0) return 0;
+    if (std::isnan(f)) return 0x7ff8000000000000ULL;
+    uint64_t b; std::memcpy(&b, &f, 8);
+    return b;
+}
+
+uint64_t LeafHash(const Val& v, int t) {
+    switch (t) {
+        case QDB_TYPE_BOOL: return uint64_t(v.i != 0) * 2685821657736338717ULL;
+        case QDB_TYPE_CHAR1: { const uint8_t b = uint8_t(v.i); return StringHash(&b, 1); }
+        case QDB_TYPE_F64: return MixU64(CanonicalF64Bits(v.f));
+        case QDB_TYPE_F32: {
+            float f = float(v.f);
+            uint32_t b;
+            if (f == 0.0f) b = 0; else if (std::isnan(f)) b = 0x7fc00000u; else std::memcpy(&b, &f, 4);
+            return MixU64(b);
+        }
+        case QDB_TYPE_DECIMAL128: {
+            uint64_t lo = uint64_t(v.i), hi = uint64_t(u128(v.i) >> 64);
+            lo = MixU64(lo); hi = MixU64(hi);
+            return lo ^ (hi + 0x9e3779b97f4a7c15ULL + (lo << 6) + (lo >> 2));
+        }
+        default: {
+            const int bits = WidthBits(t);
+            const uint64_t mask = bits >= 64 ? ~0ULL : ((1ULL << bits) - 1);
+            return MixU64(uint64_t(v.i) & mask);
+        }
+    }
+}
+
+// Struct key: boost-style ordered combine of the field hashes; a NULL field
+// contributes 0 (gen.cpp:345-375).
+uint64_t StructHash(const Val* vals, const int* types, int n) {
+    uint64_t h = 0;
+    for (int j = 0; j < n; ++j) {
+        const uint64_t fh = vals[j].null ? 0 : LeafHash(vals[j], types[j]);
+        h ^= fh + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2);
+    }
+    return h;
+}
+
+bool KeyFieldEqual(const Val& a, const Val& b, int t) {
+    if (a.null || b.null) return a.null == b.null;   // NULL keys group together
+    if (IsFloat(t)) return CanonicalF64Bits(a.f) == CanonicalF64Bits(b.f);
+    return a.i == b.i;
+}
+
+// ---------------------------------------------------------------------------
+// Aggregate state and reducers (qdb/kernel/gen.cpp:3301-3593) and result
+// typing (qdb/plan/ops/aggregate.cpp:21-57).
+// ---------------------------------------------------------------------------
+struct AggState {
+    i128 acc = 0;        // integer/decimal sum, or min/max
+    double facc = 0.0;   // f64 sum/min/max
+    int64_t count = 0;   // rows (COUNT) or valid contributions
+};
+
+struct ResultType {
+    int type;
+    int scale;
+    bool nullable;
+};
+
+ResultType AggResultType(const qdb_aggregate_spec& s, const qdb_agg_item& a) {
+    if (a.func == QDB_AGG_COUNT_STAR || a.func == QDB_AGG_COUNT) return {QDB_TYPE_I64, 0, false};
+    const qdb_expr& arg = s.nodes[a.arg];
+    bool nullable = true;   // an argument is non-null only if provably so
+    if (arg.op == QDB_EXPR_COLUMN) nullable = s.columns[arg.column].nullable != 0;
+    else {
+        // Conservative: the tree is non-null when every COLUMN leaf is.
+        nullable = false;
+        std::vector<int> stack{a.arg};
+        while (!stack.empty()) {
+            const qdb_expr& e = s.nodes[stack.back()];
+            stack.pop_back();
+            if (e.op == QDB_EXPR_COLUMN && s.columns[e.column].nullable) nullable = true;
+            if (e.op == QDB_EXPR_NULL || e.op == QDB_EXPR_DIV) nullable = nullable || e.op == QDB_EXPR_NULL;
+            const int na = e.op == QDB_EXPR_BETWEEN || e.op == QDB_EXPR_CASE ? 3
+                : (e.op == QDB_EXPR_COLUMN || e.op == QDB_EXPR_CONST || e.op == QDB_EXPR_NULL) ? 0
+                : (e.op == QDB_EXPR_NEG || e.op == QDB_EXPR_CAST || e.op == QDB_EXPR_NOT ||
+                   e.op == QDB_EXPR_IN_LIST || e.op == QDB_EXPR_IS_NULL || e.op == QDB_EXPR_IS_NOT_NULL) ? 1 : 2;
+            for (int j = 0; j < na; ++j) stack.push_back(e.args[j]);
+        }
+    }
+    const int t = arg.type;
+    if (IsFloat(t)) return {QDB_TYPE_F64, 0, nullable};
+    if (a.func == QDB_AGG_SUM) {
+        if (IsDecimal(t)) return {QDB_TYPE_DECIMAL128, arg.scale, nullable};
+        if (t == QDB_TYPE_DATE32) throw Error("function sum(DATE) does not exist");
+        return {QDB_TYPE_I64, 0, nullable};
+    }
+    // MIN/MAX keep decimals; integers and dates widen to i64.
+    if (IsDecimal(t)) return {t, arg.scale, nullable};
+    return {QDB_TYPE_I64, 0, nullable};
+}
+
+void Reduce(const qdb_agg_item& a, const ResultType& rt, AggState& st, const Val& v) {
+    switch (a.func) {
+        case QDB_AGG_COUNT_STAR: ++st.count; return;
+        case QDB_AGG_COUNT: if (!v.null) ++st.count; return;
+        default: break;
+    }
+    if (v.null) return;
+    const bool first = st.count == 0;
+    if (rt.type == QDB_TYPE_F64) {
+        const double x = v.f;
+        if (a.func == QDB_AGG_SUM) st.facc = first ? x : st.facc + x;
+        else if (a.func == QDB_AGG_MIN) st.facc = first ? x : (x < st.facc ? x : st.facc);
+        else st.facc = first ? x : (x > st.facc ? x : st.facc);
+    } else {
+        const i128 x = v.i;
+        if (a.func == QDB_AGG_SUM) {
+            st.acc = first ? Wrap(x, rt.type) : Wrap(i128(u128(st.acc) + u128(x)), rt.type);
+        } else if (a.func == QDB_AGG_MIN) {
+            st.acc = first ? x : (x < st.acc ? x : st.acc);
+        } else {
+            st.acc = first ? x : (x > st.acc ? x : st.acc);
+        }
+    }
+    ++st.count;
+}
+
+// Partial-state combine of the cascade (docs/arch/aggregation.md:343-348):
+// counts add, sums add, min/max fold.
+void Combine(const qdb_agg_item& a, const ResultType& rt, AggState& into, const AggState& from) {
+    if (a.func == QDB_AGG_COUNT_STAR || a.func == QDB_AGG_COUNT) { into.count += from.count; return; }
+    if (from.count == 0) return;
+    if (into.count == 0) { into = from; return; }
+    if (rt.type == QDB_TYPE_F64) {
+        if (a.func == QDB_AGG_SUM) into.facc += from.facc;
+        else if (a.func == QDB_AGG_MIN) into.facc = from.facc < into.facc ? from.facc : into.facc;
+        else into.facc = from.facc > into.facc ? from.facc : into.facc;
+    } else {
+        if (a.func == QDB_AGG_SUM) into.acc = Wrap(i128(u128(into.acc) + u128(from.acc)), rt.type);
+        else if (a.func == QDB_AGG_MIN) into.acc = from.acc < into.acc ? from.acc : into.acc;
+        else into.acc = from.acc > into.acc ? from.acc : into.acc;
+    }
+    into.count += from.count;
+}
+
+// ---------------------------------------------------------------------------
+// Swiss group table (qdb/kernel/aggregation/swiss_group.oz:5-67,
+// robin_hood_dual_key.oz:14-288, aggregation_hashtable_generic.oz:88-177):
+// 8-slot groups of control bytes (0x80 empty, H2 = hash & 0x7F, no
+// tombstones), triangular group probing, growth before an insert would cross
+// 7/8 of the capacity, groups numbered densely in first-seen order.
+// ---------------------------------------------------------------------------
+struct SwissTable {
+    int nkeys = 0;
+    const int* key_types = nullptr;
+    int64_t capacity = 8;
+    std::vector<uint8_t> ctrl;
+    std::vector<int64_t> slot_dense;      // physical slot -> dense group id
+    std::vector<Val> group_keys;          // dense id * nkeys
+    std::vector<uint64_t> group_hash;
+
+    void Init(int n, const int* types, int64_t cap) {
+        nkeys = n;
+        key_types = types;
+        capacity = std::max<int64_t>(8, cap);
+        ctrl.assign(capacity, 0x80);
+        slot_dense.assign(capacity, -1);
+        group_keys.clear();
+        group_hash.clear();
+    }
+    int64_t Size() const { return int64_t(group_hash.size()); }
+
+    bool KeysEqual(int64_t dense, const Val* key) const {
+        for (int j = 0; j < nkeys; ++j) {
+            if (!KeyFieldEqual(group_keys[dense * nkeys + j], key[j], key_types[j])) return false;
+        }
+        return true;
+    }
+
+    // rh_lookup_or_empty_physical (robin_hood_dual_key.oz:14-52).
+    int64_t LookupOrEmpty(const Val* key, uint64_t hash, int64_t& empty_slot) const {
+        empty_slot = -1;
+        const int64_t num_groups = capacity >> 3, group_mask = num_groups - 1;
+        const uint8_t h2 = uint8_t(hash & 127);
+        int64_t g = int64_t(hash >> 7) & group_mask;
+        for (int64_t step = 0, probes = 0; probes < num_groups; ++probes) {
+            for (int s = 0; s < 8; ++s) {
+                const int64_t slot = (g << 3) + s;
+                if (ctrl[slot] == h2 && KeysEqual(slot_dense[slot], key)) return slot;
+            }
+            for (int s = 0; s < 8; ++s) {
+                if (ctrl[(g << 3) + s] & 0x80) { empty_slot = (g << 3) + s; return -1; }
+            }
+            ++step;
+            g = (g + step) & group_mask;
+        }
+        return -1;
+    }
+
+    // rh_find_empty_slot (robin_hood_dual_key.oz:96-124).
+    int64_t FindEmpty(uint64_t hash) const {
+        const int64_t num_groups = capacity >> 3, group_mask = num_groups - 1;
+        int64_t g = int64_t(hash >> 7) & group_mask;
+        for (int64_t step = 0, probes = 0; probes < num_groups; ++probes) {
+            for (int s = 0; s < 8; ++s) {
+                if (ctrl[(g << 3) + s] & 0x80) return (g << 3) + s;
+            }
+            ++step;
+            g = (g + step) & group_mask;
+        }
+        return -1;
+    }
+
+    void Rehash(int64_t new_capacity) {
+        capacity = new_capacity;
+        ctrl.assign(capacity, 0x80);
+        slot_dense.assign(capacity, -1);
+        for (int64_t d = 0; d < Size(); ++d) {
+            const int64_t slot = FindEmpty(group_hash[d]);
+            ctrl[slot] = uint8_t(group_hash[d] & 127);
+            slot_dense[slot] = d;
+        }
+    }
+
+    // aht_upsert_aggregate + aht_insert_dual (robin_hood_dual_key.oz:143-224):
+    // returns the dense group id and whether it is new.
+    int64_t Upsert(const Val* key, uint64_t hash, bool& is_new) {
+        is_new = false;
+        int64_t empty = -1;
+        const int64_t slot = LookupOrEmpty(key, hash, empty);
+        if (slot >= 0) return slot_dense[slot];
+        const int64_t dense = Size();
+        if (dense + 1 > capacity - (capacity >> 3)) {   // aht_insert_grows
+            Rehash(capacity * 2);
+            empty = FindEmpty(hash);
+        }
+        ctrl[empty] = uint8_t(hash & 127);
+        slot_dense[empty] = dense;
+        group_keys.insert(group_keys.end(), key, key + nkeys);
+        group_hash.push_back(hash);
+        is_new = true;
+        return dense;
+    }
+};
+
+// A compiled view of an aggregate spec for the oracle.
+struct AggPlan {
+    const qdb_aggregate_spec* spec;
+    Expr expr;
+    int32_t max_root = -1;
+    std::vector<int> key_types;
+    std::vector<ResultType> result_types;
+};
+
+AggPlan MakePlan(const qdb_aggregate_spec& s) {
+    AggPlan p;
+    p.spec = &s;
+    p.expr = {s.nodes, s.n_nodes};
+    p.max_root = s.filter;
+    for (int j = 0; j < s.n_keys; ++j) {
+        p.key_types.push_back(s.nodes[s.keys[j]].type);
+        p.max_root = std::max(p.max_root, s.keys[j]);
+    }
+    for (int j = 0; j < s.n_aggs; ++j) {
+        p.result_types.push_back(AggResultType(s, s.aggs[j]));
+        p.max_root = std::max(p.max_root, s.aggs[j].arg);
+    }
+    return p;
+}
+
+struct GroupSet {
+    SwissTable table;
+    std::vector<AggState> states;   // dense id * n_aggs
+};
+
+// One lane of agg_dispatch(Update) over a row range: per selected row, filter,
+// key, upsert, reducers (GenGenericAggregateDispatchAst, gen.cpp:2075-2299).
+void AggregateRows(const AggPlan& p, const qdb_rowset& b, int64_t begin, int64_t end, GroupSet& g) {
+    const qdb_aggregate_spec& s = *p.spec;
+    std::vector<Val> vals;
+    std::vector<Val> key(std::max(1, s.n_keys));
+    for (int64_t row = begin; row < end; ++row) {
+        if (b.Selection && !b.Selection[row]) continue;
+        if (p.max_root >= 0) {
+            EvalAll(p.expr, p.max_root,
+                    [&](int32_t c) { return ReadCell(b.Columns[c], s.columns[c], row); }, vals);
+        }
+        if (s.filter >= 0) {
+            const Val& f = vals[s.filter];
+            if (f.null || f.i == 0) continue;
+        }
+        for (int j = 0; j < s.n_keys; ++j) key[j] = vals[s.keys[j]];
+        const uint64_t hash = StructHash(key.data(), p.key_types.data(), s.n_keys);
+        bool is_new = false;
+        const int64_t dense = g.table.Upsert(key.data(), hash, is_new);
+        if (is_new) g.states.resize(g.states.size() + s.n_aggs);
+        for (int j = 0; j < s.n_aggs; ++j) {
+            Val v;
+            if (s.aggs[j].arg >= 0) v = vals[s.aggs[j].arg];
+            Reduce(s.aggs[j], p.result_types[j], g.states[dense * s.n_aggs + j], v);
+        }
+    }
+}
+
+Val StateValue(const ResultType& rt, const qdb_agg_item& a, const AggState& st) {
+    Val v;
+    if (a.func == QDB_AGG_COUNT_STAR || a.func == QDB_AGG_COUNT) { v.i = st.count; return v; }
+    if (st.count == 0) { v.null = true; return v; }
+    if (rt.type == QDB_TYPE_F64) v.f = st.facc; else v.i = st.acc;
+    return v;
+}
+
+// Output projection over (keys ++ aggregates) — the finalize projection of
+// the plan (AVG = sum / count, qdb/plan/sql_lowering.cpp:799-814).
+void EmitTable(const AggPlan& p, const GroupSet& g, oracle_table* out) {
+    const qdb_aggregate_spec& s = *p.spec;
+    const int64_t rows = g.table.Size();
+    std::vector<int> row_types;
+    std::vector<int> row_scales;
+    for (int j = 0; j < s.n_keys; ++j) {
+        row_types.push_back(s.nodes[s.keys[j]].type);
+        row_scales.push_back(s.nodes[s.keys[j]].scale);
+    }
+    for (int j = 0; j < s.n_aggs; ++j) {
+        row_types.push_back(p.result_types[j].type);
+        row_scales.push_back(p.result_types[j].scale);
+    }
+    const int ncols = s.n_outputs > 0 ? s.n_outputs : int(row_types.size());
+    out->rows = rows;
+    out->cols = ncols;
+    out->types = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * std::max(1, ncols)));
+    out->scales = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * std::max(1, ncols)));
+    out->cells = static_cast<int64_t*>(std::calloc(std::max<int64_t>(1, rows * ncols * 2), 8));
+    out->valid = static_cast<uint8_t*>(std::calloc(std::max<int64_t>(1, rows * ncols), 1));
+    for (int c = 0; c < ncols; ++c) {
+        if (s.n_outputs > 0) {
+            out->types[c] = s.output_nodes[s.outputs[c]].type;
+            out->scales[c] = s.output_nodes[s.outputs[c]].scale;
+        } else {
+            out->types[c] = row_types[c];
+            out->scales[c] = row_scales[c];
+        }
+    }
+    std::vector<Val> rowv(row_types.size());
+    std::vector<Val> tmp;
+    int32_t max_out = -1;
+    for (int c = 0; c < s.n_outputs; ++c) max_out = std::max(max_out, s.outputs[c]);
+    const Expr oexpr{s.output_nodes, s.n_output_nodes};
+    for (int64_t r = 0; r < rows; ++r) {
+        for (int j = 0; j < s.n_keys; ++j) rowv[j] = g.table.group_keys[r * s.n_keys + j];
+        for (int j = 0; j < s.n_aggs; ++j) {
+            rowv[s.n_keys + j] = StateValue(p.result_types[j], s.aggs[j], g.states[r * s.n_aggs + j]);
+        }
+        const Val* cellsrc = rowv.data();
+        if (s.n_outputs > 0) {
+            EvalAll(oexpr, max_out, [&](int32_t c) { return rowv[c]; }, tmp);
+        }
+        for (int c = 0; c < ncols; ++c) {
+            const Val& v = s.n_outputs > 0 ? tmp[s.outputs[c]] : cellsrc[c];
+            int64_t* cell = out->cells + (r * ncols + c) * 2;
+            out->valid[r * ncols + c] = v.null ? 0 : 1;
+            if (v.null) continue;
+            if (IsFloat(out->types[c])) std::memcpy(cell, &v.f, 8);
+            else { cell[0] = int64_t(uint64_t(v.i)); cell[1] = int64_t(uint64_t(u128(v.i) >> 64)); }
+        }
+    }
+}
+
+// Threaded plan shape (qdb/scheduler/lowering/plan_lowerer.cpp:1671 cascade,
+// qdb/exec/aggregate_exec.cpp:158-233, runtime_adapter.cpp:1001-1003): lanes
+// aggregate row ranges into partial tables, partial groups are routed by
+// hash % lanes, and each final lane combines its partition.
+void AggregateThreaded(const AggPlan& p, const qdb_rowset& b, int lanes, GroupSet& result) {
+    const qdb_aggregate_spec& s = *p.spec;
+    std::vector<GroupSet> partial(lanes);
+    std::vector<std::thread> th;
+    for (int l = 0; l < lanes; ++l) {
+        th.emplace_back([&, l] {
+            partial[l].table.Init(s.n_keys, p.key_types.data(), 8);
+            const int64_t begin = b.RowCount * l / lanes, end = b.RowCount * (l + 1) / lanes;
+            AggregateRows(p, b, begin, end, partial[l]);
+        });
+    }
+    for (auto& t : th) t.join();
+    th.clear();
+    std::vector<GroupSet> finals(lanes);
+    for (int l = 0; l < lanes; ++l) {
+        th.emplace_back([&, l] {
+            GroupSet& f = finals[l];
+            f.table.Init(s.n_keys, p.key_types.data(), 8);
+            for (int src = 0; src < lanes; ++src) {
+                const GroupSet& ps = partial[src];
+                for (int64_t d = 0; d < ps.table.Size(); ++d) {
+                    const uint64_t h = ps.table.group_hash[d];
+                    if (int(h % uint64_t(lanes)) != l) continue;
+                    bool is_new = false;
+                    const int64_t dense = f.table.Upsert(&ps.table.group_keys[d * s.n_keys], h, is_new);
+                    if (is_new) f.states.resize(f.states.size() + s.n_aggs);
+                    for (int j = 0; j < s.n_aggs; ++j) {
+                        Combine(s.aggs[j], p.result_types[j], f.states[dense * s.n_aggs + j],
+                                ps.states[d * s.n_aggs + j]);
+                    }
+                }
+            }
+        });
+    }
+    for (auto& t : th) t.join();
+    result.table.Init(s.n_keys, p.key_types.data(), 8);
+    for (int l = 0; l < lanes; ++l) {
+        const GroupSet& f = finals[l];
+        for (int64_t d = 0; d < f.table.Size(); ++d) {
+            bool is_new = false;
+            const int64_t dense = result.table.Upsert(&f.table.group_keys[d * s.n_keys], f.table.group_hash[d], is_new);
+            if (is_new) result.states.resize(result.states.size() + s.n_aggs);
+            for (int j = 0; j < s.n_aggs; ++j) {
+                Combine(s.aggs[j], p.result_types[j], result.states[dense * s.n_aggs + j],
+                        f.states[d * s.n_aggs + j]);
+            }
+        }
+    }
+}
+
+// A global aggregate (no keys) over an empty input still has its one group:
+// COUNT 0, SUM NULL (docs/arch/aggregation.md:144-164, EmptyInputGroups).
+void EnsureGlobalGroup(const AggPlan& p, GroupSet& g) {
+    if (p.spec->n_keys == 0 && g.table.Size() == 0) {
+        bool is_new = false;
+        g.table.Upsert(nullptr, StructHash(nullptr, nullptr, 0), is_new);
+        g.states.resize(p.spec->n_aggs);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Row table and row join (qdb/kernel/row_table.oz:140-295,
+// qdb/kernel/join/join_rows.oz:70-197).
+// ---------------------------------------------------------------------------
+uint64_t RtMix(uint64_t h) { return h * 0x9E3779B97F4A7C15ULL; }   // rt_mix
+uint64_t RtSalt(uint64_t h) { return (h >> 16) & 0xFFFF; }          // rt_salt
+
+struct RowTable {
+    std::vector<uint64_t> entries;   // salt << 48 | (row + 1)
+    uint64_t mask = 0;
+    int shift = 64;
+
+    // rt_init: load factor at most 1/2, at least 1024 entries.
+    void Init(int64_t rows) {
+        int64_t cap = 1024;
+        while (cap < rows * 2) cap *= 2;
+        entries.assign(cap, 0);
+        mask = uint64_t(cap - 1);
+        shift = 64 - __builtin_ctzll(uint64_t(cap));
+    }
+    // rt_seek: walk to the first entry that is empty or carries `salt`.
+    uint64_t Seek(uint64_t off, uint64_t salt, uint64_t& out_off) const {
+        uint64_t e = entries[off];
+        while (e != 0 && (e >> 48) != salt) {
+            off = (off + 1) & mask;
+            e = entries[off];
+        }
+        out_off = off;
+        return e;
+    }
+};
+
+struct JoinSide {
+    const qdb_row_join_spec* spec;
+    bool build;
+    int n_keys;
+    std::vector<int> key_cols;
+    std::vector<int> key_types;
+    const qdb_column_type* columns;
+};
+
+bool ReadKey(const JoinSide& side, const qdb_rowset& b, int64_t row, Val* key) {
+    for (int j = 0; j < side.n_keys; ++j) {
+        key[j] = ReadCell(b.Columns[side.key_cols[j]], side.columns[side.key_cols[j]], row);
+        if (key[j].null) return false;   // a NULL key matches nothing
+    }
+    return true;
+}
+
+struct BuildArena {
+    std::vector<int32_t> batch;    // arena row -> source batch
+    std::vector<int64_t> row;      // arena row -> source row
+    std::vector<Val> keys;         // arena row * n_keys
+    std::vector<uint64_t> hash;
+    std::vector<int64_t> next;     // chain of equal keys, -1 ends
+};
+
+// GenRowJoinAppendAst (qdb/kernel/join_gen.cpp:2063-2160): append the
+// selected rows with a valid key (and, fused here, that pass the build
+// predicate) in input order.
+void AppendBuild(const JoinSide& side, const qdb_rowset* build, int32_t n_build, BuildArena& a) {
+    const qdb_row_join_spec& s = *side.spec;
+    const Expr fexpr{s.build_nodes, s.n_build_nodes};
+    std::vector<Val> tmp;
+    std::vector<Val> key(side.n_keys);
+    for (int32_t bi = 0; bi < n_build; ++bi) {
+        const qdb_rowset& b = build[bi];
+        for (int64_t r = 0; r < b.RowCount; ++r) {
+            if (b.Selection && !b.Selection[r]) continue;
+            if (s.build_filter >= 0) {
+                EvalAll(fexpr, s.build_filter,
+                        [&](int32_t c) { return ReadCell(b.Columns[c], s.build_columns[c], r); }, tmp);
+                if (tmp[s.build_filter].null || tmp[s.build_filter].i == 0) continue;
+            }
+            if (!ReadKey(side, b, r, key.data())) continue;
+            a.batch.push_back(bi);
+            a.row.push_back(r);
+            a.keys.insert(a.keys.end(), key.begin(), key.end());
+            a.hash.push_back(StructHash(key.data(), side.key_types.data(), side.n_keys));
+        }
+    }
+    a.next.assign(a.row.size(), -1);
+}
+
+bool ArenaKeyEqual(const BuildArena& a, int nk, int64_t r, const Val* key, const int* types) {
+    for (int j = 0; j < nk; ++j) {
+        if (!KeyFieldEqual(a.keys[r * nk + j], key[j], types[j])) return false;
+    }
+    return true;
+}
+
+// jr_build_rows (join_rows.oz:70-113): link rows last to first so that an
+// equal-key chain lists its rows in build order.
+void BuildTable(const BuildArena& a, int nk, const int* types, RowTable& t, std::vector<int64_t>& next) {
+    const int64_t n = int64_t(a.row.size());
+    t.Init(n);
+    next.assign(n, -1);
+    for (int64_t r = n - 1; r >= 0; --r) {
+        const uint64_t h = RtMix(a.hash[r]);
+        const uint64_t salt = RtSalt(h);
+        uint64_t off = 0;
+        uint64_t e = t.Seek(h >> t.shift, salt, off);
+        while (true) {
+            if (e == 0) {
+                next[r] = -1;
+                t.entries[off] = (salt << 48) | uint64_t(r + 1);
+                break;
+            }
+            const int64_t head = int64_t(e & 0xFFFFFFFFFFFFULL) - 1;
+            if (ArenaKeyEqual(a, nk, head, &a.keys[r * nk], types)) {
+                next[r] = head;
+                t.entries[off] = (salt << 48) | uint64_t(r + 1);
+                break;
+            }
+            off = (off + 1) & t.mask;
+            e = t.Seek(off, salt, off);
+        }
+    }
+}
+
+// Probe (GenRowJoinProbeAst join_gen.cpp:2161-2270, rt_seek_all
+// row_table.oz:260-277, jr_probe_candidates join_rows.oz:146-197): a seek
+// pass over every selected valid row, then key passes; a salt collision moves
+// the row on to the next pass.  Emits (probe row, build arena row).
+template <class Emit>
+void ProbeBatch(const JoinSide& side, const BuildArena& a, const RowTable& t,
+                const std::vector<int64_t>& next, const qdb_rowset& p, Emit&& emit) {
+    const int nk = side.n_keys;
+    std::vector<int64_t> rows;
+    std::vector<Val> keys;
+    std::vector<uint64_t> salts, offsets, found;
+    std::vector<Val> key(nk);
+    for (int64_t r = 0; r < p.RowCount; ++r) {
+        if (p.Selection && !p.Selection[r]) continue;
+        if (!ReadKey(side, p, r, key.data())) continue;
+        rows.push_back(r);
+        keys.insert(keys.end(), key.begin(), key.end());
+    }
+    const int64_t count = int64_t(rows.size());
+    salts.resize(count); offsets.resize(count); found.resize(count);
+    for (int64_t j = 0; j < count; ++j) {
+        const uint64_t h = RtMix(StructHash(&keys[j * nk], side.key_types.data(), nk));
+        salts[j] = RtSalt(h);
+        found[j] = t.Seek(h >> t.shift, salts[j], offsets[j]);
+    }
+    std::vector<int64_t> work(count);
+    int64_t k = count;
+    bool first = true;
+    while (k > 0) {
+        int64_t m = 0;
+        for (int64_t q = 0; q < k; ++q) {
+            const int64_t j = first ? q : work[q];
+            const uint64_t e = found[j];
+            if (e == 0) continue;
+            const int64_t head = int64_t(e & 0xFFFFFFFFFFFFULL) - 1;
+            if (ArenaKeyEqual(a, nk, head, &keys[j * nk], side.key_types.data())) {
+                for (int64_t cur = head; cur >= 0; cur = next[cur]) emit(rows[j], cur);
+            } else {
+                offsets[j] = (offsets[j] + 1) & t.mask;
+                work[m++] = j;
+            }
+        }
+        k = m;
+        first = false;
+        for (int64_t q = 0; q < k; ++q) {   // rt_seek_work
+            const int64_t j = work[q];
+            found[j] = t.Seek(offsets[j], salts[j], offsets[j]);
+        }
+    }
+}
+
+JoinSide MakeSide(const qdb_row_join_spec& s, bool build) {
+    JoinSide side;
+    side.spec = &s;
+    side.build = build;
+    side.n_keys = s.n_keys;
+    side.columns = build ? s.build_columns : s.probe_columns;
+    for (int j = 0; j < s.n_keys; ++j) {
+        const int c = build ? s.build_keys[j] : s.probe_keys[j];
+        side.key_cols.push_back(c);
+        side.key_types.push_back(side.columns[c].type);
+    }
+    return side;
+}
+
+// ---------------------------------------------------------------------------
+// Radix sort over packed row ids (qdb/kernel/sort/radix.oz:4-123,
+// sort_rowids.oz:63-228, compiler.cpp:563-600).
+// ---------------------------------------------------------------------------
+// qumir_radix_key: order-preserving unsigned keys; PostgreSQL float order.
+uint64_t RadixKey(const Val& v, int t) {
+    switch (t) {
+        case QDB_TYPE_I8: return uint64_t(uint8_t(int8_t(v.i)) ^ 0x80u);
+        case QDB_TYPE_I16: return uint64_t(uint16_t(int16_t(v.i)) ^ 0x8000u);
+        case QDB_TYPE_I32: case QDB_TYPE_DATE32: return uint64_t(uint32_t(int32_t(v.i)) ^ 0x80000000u);
+        case QDB_TYPE_I64: case QDB_TYPE_DECIMAL64: return uint64_t(int64_t(v.i)) ^ (1ULL << 63);
+        case QDB_TYPE_U8: case QDB_TYPE_U16: case QDB_TYPE_U32: case QDB_TYPE_U64: case QDB_TYPE_CHAR1:
+        case QDB_TYPE_BOOL:
+            return uint64_t(v.i);
+        case QDB_TYPE_F64: {
+            uint64_t bits; std::memcpy(&bits, &v.f, 8);
+            const uint64_t mag = bits & 0x7fffffffffffffffULL;
+            if (mag > 0x7ff0000000000000ULL) return ~0ULL;
+            if (mag == 0) bits = 0;
+            return (bits >> 63) ? ~bits : (bits ^ (1ULL << 63));
+        }
+        case QDB_TYPE_F32: {
+            float f = float(v.f);
+            uint32_t bits; std::memcpy(&bits, &f, 4);
+            const uint32_t mag = bits & 0x7fffffffu;
+            if (mag > 0x7f800000u) return 0xffffffffULL;
+            if (mag == 0) bits = 0;
+            return uint64_t((bits >> 31) ? ~bits : (bits ^ 0x80000000u));
+        }
+    }
+    throw Error("unsupported sort key type");
+}
+
+int KeyBits(int t) {
+    if (t == QDB_TYPE_BOOL) return 8;
+    return WidthBits(t) <= 32 ? std::max(8, WidthBits(t)) : 64;
+}
+
+// sr_keyed_count_pass + sr_keyed_sort: stable LSD over 8-bit digits; a digit
+// that is the same for every key is skipped; DESC walks buckets downwards.
+void KeyedSort(std::vector<uint64_t>& keys, std::vector<int64_t>& ids, int key_bits, bool desc) {
+    const int64_t n = int64_t(keys.size());
+    std::vector<uint64_t> kout(n);
+    std::vector<int64_t> iout(n);
+    std::vector<uint64_t> counts(256);
+    for (int digit = 0; digit < key_bits; digit += 8) {
+        std::fill(counts.begin(), counts.end(), 0);
+        for (int64_t i = 0; i < n; ++i) ++counts[(keys[i] >> digit) & 255];
+        bool constant = false;
+        uint64_t offset = 0;
+        for (int i = 0; i < 256; ++i) {
+            const int bucket = desc ? 255 - i : i;
+            const uint64_t c = counts[bucket];
+            if (int64_t(c) == n) { constant = true; break; }
+            counts[bucket] = offset;
+            offset += c;
+        }
+        if (constant) continue;
+        for (int64_t i = 0; i < n; ++i) {
+            const uint64_t b = (keys[i] >> digit) & 255;
+            const uint64_t place = counts[b]++;
+            kout[place] = keys[i];
+            iout[place] = ids[i];
+        }
+        keys.swap(kout);
+        ids.swap(iout);
+    }
+}
+
+Val StoreCell(const qdb_sort_spec& s, const qdb_rowset* store, int64_t packed, int col) {
+    const int32_t batch = int32_t(packed >> 32);
+    const int32_t row = int32_t(uint32_t(packed & 0xffffffffu));
+    return ReadCell(store[batch].Columns[col], s.columns[col], row);
+}
+
+// sort_fixed_rowids(_nullable) for one key: NULL rows keep input order at
+// the chosen end, valid rows are LSD-sorted.
+void SortOneKey(const qdb_sort_spec& s, const qdb_rowset* store, std::vector<int64_t>& ids,
+                int col, bool desc, bool nulls_first) {
+    const int t = s.columns[col].type;
+    if (t == QDB_TYPE_DECIMAL128) throw Error("DECIMAL128 sort keys are not restated");
+    std::vector<uint64_t> keys;
+    std::vector<int64_t> valid_ids, null_ids;
+    for (int64_t id : ids) {
+        const Val v = StoreCell(s, store, id, col);
+        if (v.null) { null_ids.push_back(id); continue; }
+        valid_ids.push_back(id);
+        keys.push_back(RadixKey(v, t));
+    }
+    KeyedSort(keys, valid_ids, KeyBits(t), desc);
+    ids.clear();
+    if (nulls_first) { ids = null_ids; ids.insert(ids.end(), valid_ids.begin(), valid_ids.end()); }
+    else { ids = valid_ids; ids.insert(ids.end(), null_ids.begin(), null_ids.end()); }
+}
+
+// SortRowsLess (qdb/exec/sort_exec.cpp:126-293) with the packed row id as the
+// final tie break (qdb/kernel/compiler.h:135-148).
+bool RowLess(const qdb_sort_spec& s, const qdb_rowset* store, const bool* descs,
+             const bool* nulls_firsts, int64_t a, int64_t b) {
+    for (int k = 0; k < s.n_keys; ++k) {
+        const int col = s.keys[k].column;
+        const int t = s.columns[col].type;
+        const Val x = StoreCell(s, store, a, col), y = StoreCell(s, store, b, col);
+        const bool desc = descs ? descs[k] : s.keys[k].desc;
+        const bool nf = nulls_firsts ? nulls_firsts[k] : s.keys[k].nulls_first;
+        if (x.null || y.null) {
+            if (x.null && y.null) continue;
+            return x.null ? nf : !nf;
+        }
+        const uint64_t kx = RadixKey(x, t), ky = RadixKey(y, t);
+        if (kx == ky) continue;
+        return desc ? kx > ky : kx < ky;
+    }
+    return a < b;
+}
+
+void SiftDown(std::vector<int64_t>& h, int64_t size, int64_t i,
+              const std::function<bool(int64_t, int64_t)>& less) {
+    // Max-heap under `less`: the root is the last kept row of the order.
+    while (true) {
+        const int64_t l = 2 * i + 1, r = l + 1;
+        int64_t big = i;
+        if (l < size && less(h[big], h[l])) big = l;
+        if (r < size && less(h[big], h[r])) big = r;
+        if (big == i) return;
+        std::swap(h[i], h[big]);
+        i = big;
+    }
+}
+
+}  // namespace
+
+// ===========================================================================
+// C API
+// ===========================================================================
+extern "C" {
+
+void oracle_table_free(oracle_table* t) {
+    if (!t) return;
+    std::free(t->types);
+    std::free(t->scales);
+    std::free(t->cells);
+    std::free(t->valid);
+    std::memset(t, 0, sizeof(*t));
+}
+
+int oracle_aggregate(const qdb_aggregate_spec* spec, const qdb_rowset* batches, int32_t n_batches,
+                     int32_t lanes, oracle_table* out, char* err, size_t err_len) {
+    try {
+        const AggPlan p = MakePlan(*spec);
+        GroupSet g;
+        if (lanes <= 1 || n_batches != 1) {
+            g.table.Init(spec->n_keys, p.key_types.data(), 8);
+            for (int32_t b = 0; b < n_batches; ++b) AggregateRows(p, batches[b], 0, batches[b].RowCount, g);
+        } else {
+            AggregateThreaded(p, batches[0], lanes, g);
+        }
+        EnsureGlobalGroup(p, g);
+        EmitTable(p, g, out);
+        return 0;
+    } catch (const std::exception& e) {
+        SetErr(err, err_len, e.what());
+        return -1;
+    }
+}
+
+int oracle_filter(int32_t n_columns, const qdb_column_type* columns, int32_t n_nodes,
+                  const qdb_expr* nodes, int32_t predicate, const qdb_rowset* batch,
+                  uint8_t* selection, char* err, size_t err_len) {
+    (void)n_columns;
+    try {
+        const Expr e{nodes, n_nodes};
+        std::vector<Val> vals;
+        for (int64_t r = 0; r < batch->RowCount; ++r) {
+            if (batch->Selection && !batch->Selection[r]) { selection[r] = 0; continue; }
+            EvalAll(e, predicate, [&](int32_t c) { return ReadCell(batch->Columns[c], columns[c], r); }, vals);
+            selection[r] = (!vals[predicate].null && vals[predicate].i) ? 1 : 0;
+        }
+        return 0;
+    } catch (const std::exception& ex) {
+        SetErr(err, err_len, ex.what());
+        return -1;
+    }
+}
+
+int oracle_project(int32_t n_columns, const qdb_column_type* columns, int32_t n_nodes,
+                   const qdb_expr* nodes, int32_t n_exprs, const int32_t* exprs,
+                   const qdb_rowset* batch, void** out_buffers, uint8_t** out_valid,
+                   char* err, size_t err_len) {
+    (void)n_columns;
+    try {
+        const Expr e{nodes, n_nodes};
+        int32_t root = -1;
+        for (int k = 0; k < n_exprs; ++k) root = std::max(root, exprs[k]);
+        std::vector<Val> vals;
+        for (int64_t r = 0; r < batch->RowCount; ++r) {
+            if (batch->Selection && !batch->Selection[r]) continue;
+            EvalAll(e, root, [&](int32_t c) { return ReadCell(batch->Columns[c], columns[c], r); }, vals);
+            for (int k = 0; k < n_exprs; ++k) {
+                const qdb_expr& n = nodes[exprs[k]];
+                const Val& v = vals[exprs[k]];
+                if (out_valid && out_valid[k]) out_valid[k][r] = v.null ? 0 : 1;
+                char* base = static_cast<char*>(out_buffers[k]);
+                const int w = StorageBytes(n.type);
+                if (v.null) { std::memset(base + r * w, 0, w); continue; }
+                if (n.type == QDB_TYPE_F64) std::memcpy(base + r * 8, &v.f, 8);
+                else if (n.type == QDB_TYPE_F32) { const float f = float(v.f); std::memcpy(base + r * 4, &f, 4); }
+                else if (n.type == QDB_TYPE_DECIMAL128) {
+                    const uint64_t w2[2] = {uint64_t(v.i), uint64_t(u128(v.i) >> 64)};
+                    std::memcpy(base + r * 16, w2, 16);
+                } else {
+                    const uint64_t x = uint64_t(v.i);
+                    std::memcpy(base + r * w, &x, w);
+                }
+            }
+        }
+        return 0;
+    } catch (const std::exception& ex) {
+        SetErr(err, err_len, ex.what());
+        return -1;
+    }
+}
+
+int oracle_hash(int32_t n_columns, const qdb_column_type* columns, int32_t n_keys,
+                const int32_t* key_columns, const qdb_rowset* batch, uint64_t* hashes,
+                char* err, size_t err_len) {
+    (void)n_columns;
+    try {
+        std::vector<Val> key(n_keys);
+        std::vector<int> types(n_keys);
+        for (int j = 0; j < n_keys; ++j) types[j] = columns[key_columns[j]].type;
+        for (int64_t r = 0; r < batch->RowCount; ++r) {
+            if (batch->Selection && !batch->Selection[r]) continue;
+            for (int j = 0; j < n_keys; ++j) {
+                key[j] = ReadCell(batch->Columns[key_columns[j]], columns[key_columns[j]], r);
+            }
+            hashes[r] = StructHash(key.data(), types.data(), n_keys);
+        }
+        return 0;
+    } catch (const std::exception& ex) {
+        SetErr(err, err_len, ex.what());
+        return -1;
+    }
+}
+
+int64_t oracle_row_join(const qdb_row_join_spec* spec, const qdb_rowset* build, int32_t n_build,
+                        const qdb_rowset* probe, int64_t* pairs, int64_t pair_cap,
+                        char* err, size_t err_len) {
+    try {
+        const JoinSide bs = MakeSide(*spec, true), ps = MakeSide(*spec, false);
+        BuildArena a;
+        AppendBuild(bs, build, n_build, a);
+        RowTable t;
+        std::vector<int64_t> next;
+        BuildTable(a, bs.n_keys, bs.key_types.data(), t, next);
+        int64_t count = 0;
+        ProbeBatch(ps, a, t, next, *probe, [&](int64_t prow, int64_t brow) {
+            if (pairs && count < pair_cap) {
+                pairs[2 * count] = prow;
+                pairs[2 * count + 1] = brow;
+            }
+            ++count;
+        });
+        return count;
+    } catch (const std::exception& e) {
+        SetErr(err, err_len, e.what());
+        return -1;
+    }
+}
+
+int oracle_join_aggregate(const qdb_row_join_spec* join, const qdb_aggregate_spec* agg,
+                          const qdb_rowset* build, int32_t n_build, const qdb_rowset* probe,
+                          int32_t n_probe, int32_t lanes, oracle_table* out, char* err, size_t err_len) {
+    (void)lanes;
+    try {
+        const JoinSide bs = MakeSide(*join, true), ps = MakeSide(*join, false);
+        BuildArena a;
+        AppendBuild(bs, build, n_build, a);
+        RowTable t;
+        std::vector<int64_t> next;
+        BuildTable(a, bs.n_keys, bs.key_types.data(), t, next);
+        const AggPlan p = MakePlan(*agg);
+        GroupSet g;
+        g.table.Init(agg->n_keys, p.key_types.data(), 8);
+        const int np = join->n_probe_columns;
+        std::vector<Val> vals;
+        std::vector<Val> key(std::max(1, agg->n_keys));
+        for (int32_t pb = 0; pb < n_probe; ++pb) {
+            const qdb_rowset& pr = probe[pb];
+            ProbeBatch(ps, a, t, next, pr, [&](int64_t prow, int64_t brow) {
+                auto leaf = [&](int32_t c) -> Val {
+                    if (c < np) return ReadCell(pr.Columns[c], join->probe_columns[c], prow);
+                    const int bc = join->build_payload[c - np];
+                    const qdb_rowset& bb = build[a.batch[brow]];
+                    return ReadCell(bb.Columns[bc], join->build_columns[bc], a.row[brow]);
+                };
+                if (p.max_root >= 0) EvalAll(p.expr, p.max_root, leaf, vals);
+                if (agg->filter >= 0 && (vals[agg->filter].null || vals[agg->filter].i == 0)) return;
+                for (int j = 0; j < agg->n_keys; ++j) key[j] = vals[agg->keys[j]];
+                bool is_new = false;
+                const int64_t dense = g.table.Upsert(key.data(),
+                    StructHash(key.data(), p.key_types.data(), agg->n_keys), is_new);
+                if (is_new) g.states.resize(g.states.size() + agg->n_aggs);
+                for (int j = 0; j < agg->n_aggs; ++j) {
+                    Val v;
+                    if (agg->aggs[j].arg >= 0) v = vals[agg->aggs[j].arg];
+                    Reduce(agg->aggs[j], p.result_types[j], g.states[dense * agg->n_aggs + j], v);
+                }
+            });
+        }
+        EnsureGlobalGroup(p, g);
+        EmitTable(p, g, out);
+        return 0;
+    } catch (const std::exception& e) {
+        SetErr(err, err_len, e.what());
+        return -1;
+    }
+}
+
+int oracle_sort(const qdb_sort_spec* spec, const qdb_rowset* store, int64_t* row_ids, int64_t n,
+                const bool* descs, const bool* nulls_firsts, char* err, size_t err_len) {
+    try {
+        std::vector<int64_t> ids(row_ids, row_ids + n);
+        // Least significant key first (compiler.cpp:595-599).
+        for (int k = spec->n_keys - 1; k >= 0; --k) {
+            const bool desc = descs ? descs[k] : spec->keys[k].desc;
+            const bool nf = nulls_firsts ? nulls_firsts[k] : spec->keys[k].nulls_first;
+            SortOneKey(*spec, store, ids, spec->keys[k].column, desc, nf);
+        }
+        std::memcpy(row_ids, ids.data(), sizeof(int64_t) * n);
+        return 0;
+    } catch (const std::exception& e) {
+        SetErr(err, err_len, e.what());
+        return -1;
+    }
+}
+
+int64_t oracle_top_k(const qdb_sort_spec* spec, const qdb_rowset* store, int64_t* row_ids,
+                     int64_t size, int64_t limit, const bool* descs, const bool* nulls_firsts) {
+    if (size <= 0 || limit <= 0) return 0;
+    std::function<bool(int64_t, int64_t)> less = [&](int64_t a, int64_t b) {
+        return RowLess(*spec, store, descs, nulls_firsts, a, b);
+    };
+    // heap_top_k (heap.oz:156-188): heapify the first K, replace the top with
+    // every later row that precedes it, then pop the heap into order.
+    std::vector<int64_t> h(row_ids, row_ids + size);
+    const int64_t kept = std::min(limit, size);
+    for (int64_t i = kept / 2 - 1; i >= 0; --i) SiftDown(h, kept, i, less);
+    for (int64_t cur = kept; cur < size; ++cur) {
+        if (less(h[cur], h[0])) {
+            h[0] = h[cur];
+            SiftDown(h, kept, 0, less);
+        }
+    }
+    for (int64_t hs = kept; hs > 1; --hs) {
+        std::swap(h[0], h[hs - 1]);
+        SiftDown(h, hs - 1, 0, less);
+    }
+    std::memcpy(row_ids, h.data(), sizeof(int64_t) * kept);
+    return kept;
+}
+
+double oracle_bench_aggregate(const qdb_aggregate_spec* spec, const qdb_rowset* batch, int32_t threads,
+                              int64_t* groups_out) {
+    try {
+        const AggPlan p = MakePlan(*spec);
+        const auto t0 = std::chrono::steady_clock::now();
+        GroupSet g;
+        AggregateThreaded(p, *batch, std::max(1, threads), g);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (groups_out) *groups_out = g.table.Size();
+        return std::chrono::duration<double>(t1 - t0).count();
+    } catch (...) {
+        return -1.0;
+    }
+}
+
+// Threaded join plan shape (docs/arch/scheduler_runtime.md:270-289): build
+// rows partitioned by hash % P, one row table per partition, probe lanes route
+// each probe row to its partition's table.  Fused SUM(payload * value), COUNT.
+double oracle_bench_join_sum(const int64_t* b_key, const int64_t* b_payload, const int32_t* b_attr,
+                             int64_t build_rows, int32_t attr_lt, const int64_t* p_fk,
+                             const int64_t* p_value, int64_t probe_rows, int32_t threads,
+                             int64_t* sum_out, int64_t* count_out) {
+    const int P = std::max(1, threads);
+    const auto t0 = std::chrono::steady_clock::now();
+    struct Part {
+        std::vector<int64_t> key, payload;
+        std::vector<int64_t> next;
+        RowTable t;
+    };
+    std::vector<Part> parts(P);
+    std::vector<std::thread> th;
+    for (int l = 0; l < P; ++l) {
+        th.emplace_back([&, l] {
+            Part& pt = parts[l];
+            for (int64_t r = 0; r < build_rows; ++r) {
+                if (b_attr[r] >= attr_lt) continue;
+                Val v; v.i = b_key[r];
+                const int ty = QDB_TYPE_I64;
+                const uint64_t kh = StructHash(&v, &ty, 1);
+                if (int(kh % uint64_t(P)) != l) continue;
+                pt.key.push_back(b_key[r]);
+                pt.payload.push_back(b_payload[r]);
+            }
+            const int64_t n = int64_t(pt.key.size());
+            pt.t.Init(n);
+            pt.next.assign(n, -1);
+            for (int64_t r = n - 1; r >= 0; --r) {
+                Val v; v.i = pt.key[r];
+                const int ty = QDB_TYPE_I64;
+                const uint64_t h = RtMix(StructHash(&v, &ty, 1));
+                const uint64_t salt = RtSalt(h);
+                uint64_t off = 0;
+                uint64_t e = pt.t.Seek(h >> pt.t.shift, salt, off);
+                while (true) {
+                    if (e == 0) { pt.t.entries[off] = (salt << 48) | uint64_t(r + 1); break; }
+                    const int64_t head = int64_t(e & 0xFFFFFFFFFFFFULL) - 1;
+                    if (pt.key[head] == pt.key[r]) {
+                        pt.next[r] = head;
+                        pt.t.entries[off] = (salt << 48) | uint64_t(r + 1);
+                        break;
+                    }
+                    off = (off + 1) & pt.t.mask;
+                    e = pt.t.Seek(off, salt, off);
+                }
+            }
+        });
+    }
+    for (auto& t : th) t.join();
+    th.clear();
+    std::vector<int64_t> sums(P, 0), counts(P, 0);
+    for (int l = 0; l < P; ++l) {
+        th.emplace_back([&, l] {
+            int64_t sum = 0, cnt = 0;
+            const int64_t begin = probe_rows * l / P, end = probe_rows * (l + 1) / P;
+            const int ty = QDB_TYPE_I64;
+            for (int64_t r = begin; r < end; ++r) {
+                Val v; v.i = p_fk[r];
+                const uint64_t kh = StructHash(&v, &ty, 1);
+                const Part& pt = parts[kh % uint64_t(P)];
+                const uint64_t h = RtMix(kh);
+                const uint64_t salt = RtSalt(h);
+                uint64_t off = 0;
+                uint64_t e = pt.t.Seek(h >> pt.t.shift, salt, off);
+                while (e != 0) {
+                    const int64_t head = int64_t(e & 0xFFFFFFFFFFFFULL) - 1;
+                    if (pt.key[head] == p_fk[r]) {
+                        for (int64_t cur = head; cur >= 0; cur = pt.next[cur]) {
+                            sum += pt.payload[cur] * p_value[r];
+                            ++cnt;
+                        }
+                        break;
+                    }
+                    off = (off + 1) & pt.t.mask;
+                    e = pt.t.Seek(off, salt, off);
+                }
+            }
+            sums[l] = sum;
+            counts[l] = cnt;
+        });
+    }
+    for (auto& t : th) t.join();
+    const auto t1 = std::chrono::steady_clock::now();
+    int64_t sum = 0, cnt = 0;
+    for (int l = 0; l < P; ++l) { sum += sums[l]; cnt += counts[l]; }
+    if (sum_out) *sum_out = sum;
+    if (count_out) *count_out = cnt;
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// Threaded sort plan shape (BuildSortMerge plan_lowerer.cpp:2133-2211): each
+// lane LSD-sorts its range by k2 ASC then k1 DESC (pass skipping as in
+// sr_keyed_count_pass), then a heap k-way merge (TMergeProcessor::Finish,
+// sort_exec.cpp:521+) with the row id as the tie break.
+double oracle_bench_sort(const int64_t* k1, const int32_t* k2, int64_t rows, int32_t threads,
+                         int64_t* rowids_out) {
+    const int L = std::max(1, threads);
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::vector<int64_t>> runs(L);
+    std::vector<std::thread> th;
+    for (int l = 0; l < L; ++l) {
+        th.emplace_back([&, l] {
+            const int64_t begin = rows * l / L, end = rows * (l + 1) / L;
+            std::vector<int64_t> ids(end - begin);
+            std::vector<uint64_t> keys(end - begin);
+            for (int64_t i = begin; i < end; ++i) {
+                ids[i - begin] = i;
+                keys[i - begin] = uint64_t(uint32_t(k2[i]) ^ 0x80000000u);
+            }
+            KeyedSort(keys, ids, 32, false);
+            for (int64_t i = 0; i < end - begin; ++i) keys[i] = uint64_t(k1[ids[i]]) ^ (1ULL << 63);
+            KeyedSort(keys, ids, 64, true);
+            runs[l].swap(ids);
+        });
+    }
+    for (auto& t : th) t.join();
+    auto before = [&](int64_t a, int64_t b) {
+        if (k1[a] != k1[b]) return k1[a] > k1[b];
+        if (k2[a] != k2[b]) return k2[a] < k2[b];
+        return a < b;
+    };
+    using Item = std::pair<int64_t, int>;   // (row, run)
+    auto cmp = [&](const Item& x, const Item& y) { return before(y.first, x.first); };
+    std::priority_queue<Item, std::vector<Item>, decltype(cmp)> pq(cmp);
+    std::vector<size_t> pos(L, 0);
+    for (int l = 0; l < L; ++l) if (!runs[l].empty()) pq.push({runs[l][0], l});
+    int64_t o = 0;
+    while (!pq.empty()) {
+        const Item it = pq.top();
+        pq.pop();
+        if (rowids_out) rowids_out[o] = it.first;
+        ++o;
+        if (++pos[it.second] < runs[it.second].size()) pq.push({runs[it.second][pos[it.second]], it.second});
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+}  // extern "C"

@@ -1,0 +1,179 @@
+"""ctypes wrapper of the CPU oracle (oracle/oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline / reference arm as the checker and the timed CPU
+baseline; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from qumirdb_b200 import abi
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+
+_lib = None
+
+
+class OracleTable(C.Structure):
+    _fields_ = [("rows", C.c_int64), ("cols", C.c_int32), ("types", C.POINTER(C.c_int32)),
+                ("scales", C.POINTER(C.c_int32)), ("cells", C.POINTER(C.c_int64)), ("valid", C.POINTER(C.c_uint8))]
+
+
+def build() -> Path:
+    srcs = [HERE / "oracle.cpp", HERE / "oracle.h", HERE.parent / "include" / "qdb_gpu.h"]
+    if not LIB.exists() or LIB.stat().st_mtime < max(s.stat().st_mtime for s in srcs):
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(str(LIB))
+        P = C.c_void_p
+        sig = {
+            "oracle_table_free": (None, [C.POINTER(OracleTable)]),
+            "oracle_aggregate": (C.c_int, [C.POINTER(abi.AggregateSpec), C.POINTER(abi.RowSet), C.c_int32, C.c_int32,
+                                           C.POINTER(OracleTable), C.c_char_p, C.c_size_t]),
+            "oracle_filter": (C.c_int, [C.c_int32, P, C.c_int32, P, C.c_int32, C.POINTER(abi.RowSet), P, C.c_char_p,
+                                        C.c_size_t]),
+            "oracle_project": (C.c_int, [C.c_int32, P, C.c_int32, P, C.c_int32, P, C.POINTER(abi.RowSet),
+                                         C.POINTER(P), C.POINTER(P), C.c_char_p, C.c_size_t]),
+            "oracle_hash": (C.c_int, [C.c_int32, P, C.c_int32, P, C.POINTER(abi.RowSet), P, C.c_char_p, C.c_size_t]),
+            "oracle_row_join": (C.c_int64, [C.POINTER(abi.RowJoinSpec), C.POINTER(abi.RowSet), C.c_int32,
+                                            C.POINTER(abi.RowSet), P, C.c_int64, C.c_char_p, C.c_size_t]),
+            "oracle_join_aggregate": (C.c_int, [C.POINTER(abi.RowJoinSpec), C.POINTER(abi.AggregateSpec),
+                                                C.POINTER(abi.RowSet), C.c_int32, C.POINTER(abi.RowSet), C.c_int32,
+                                                C.c_int32, C.POINTER(OracleTable), C.c_char_p, C.c_size_t]),
+            "oracle_sort": (C.c_int, [C.POINTER(abi.SortSpec), C.POINTER(abi.RowSet), P, C.c_int64, P, P,
+                                      C.c_char_p, C.c_size_t]),
+            "oracle_top_k": (C.c_int64, [C.POINTER(abi.SortSpec), C.POINTER(abi.RowSet), P, C.c_int64, C.c_int64,
+                                         P, P]),
+            "oracle_bench_aggregate": (C.c_double, [C.POINTER(abi.AggregateSpec), C.POINTER(abi.RowSet), C.c_int32,
+                                                    C.POINTER(C.c_int64)]),
+            "oracle_bench_join_sum": (C.c_double, [P, P, P, C.c_int64, C.c_int32, P, P, C.c_int64, C.c_int32,
+                                                   C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+            "oracle_bench_sort": (C.c_double, [P, P, C.c_int64, C.c_int32, P]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype, fn.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+def _table_rows(t: OracleTable) -> list[list]:
+    rows = []
+    for r in range(t.rows):
+        row = []
+        for c in range(t.cols):
+            k = r * t.cols + c
+            if not t.valid[k]:
+                row.append(None)
+                continue
+            lo, hi = t.cells[2 * k], t.cells[2 * k + 1]
+            ty = t.types[c]
+            if ty in (abi.F64, abi.F32):
+                row.append(float(np.array([lo], dtype=np.int64).view(np.float64)[0]))
+            else:
+                row.append((hi << 64) | (lo & ((1 << 64) - 1)))
+        rows.append(row)
+    return rows
+
+
+def _rowsets(rowsets) -> C.Array:
+    arr = (abi.RowSet * max(1, len(rowsets)))()
+    for k, r in enumerate(rowsets):
+        arr[k] = r.rs
+    return arr
+
+
+def aggregate(spec, rowsets, lanes: int = 1) -> list[list]:
+    t = OracleTable()
+    err = C.create_string_buffer(512)
+    arr = _rowsets(rowsets)
+    if lib().oracle_aggregate(C.byref(spec.struct), arr, len(rowsets), lanes, C.byref(t), err, 512) != 0:
+        raise RuntimeError(err.value.decode())
+    try:
+        return _table_rows(t)
+    finally:
+        lib().oracle_table_free(C.byref(t))
+
+
+def join_aggregate(jspec, aspec, build_rowsets, probe_rowsets) -> list[list]:
+    t = OracleTable()
+    err = C.create_string_buffer(512)
+    b = _rowsets(build_rowsets)
+    p = _rowsets(probe_rowsets)
+    if lib().oracle_join_aggregate(C.byref(jspec.struct), C.byref(aspec.struct), b, len(build_rowsets), p,
+                                   len(probe_rowsets), 1, C.byref(t), err, 512) != 0:
+        raise RuntimeError(err.value.decode())
+    try:
+        return _table_rows(t)
+    finally:
+        lib().oracle_table_free(C.byref(t))
+
+
+def row_join(jspec, build_rowsets, probe_rowset) -> np.ndarray:
+    err = C.create_string_buffer(512)
+    b = _rowsets(build_rowsets)
+    n = lib().oracle_row_join(C.byref(jspec.struct), b, len(build_rowsets), probe_rowset.ptr, None, 0, err, 512)
+    if n < 0:
+        raise RuntimeError(err.value.decode())
+    pairs = np.zeros(max(1, 2 * n), dtype=np.int64)
+    lib().oracle_row_join(C.byref(jspec.struct), b, len(build_rowsets), probe_rowset.ptr, pairs.ctypes.data, n, err,
+                          512)
+    return pairs[: 2 * n].reshape(n, 2)
+
+
+def filter_rows(columns, eb, predicate, rowset) -> np.ndarray:
+    from qumirdb_b200 import coltypes
+    ct = coltypes(columns)
+    nodes = eb.array()
+    sel = np.zeros(max(1, rowset.rs.RowCount), dtype=np.uint8)
+    err = C.create_string_buffer(512)
+    if lib().oracle_filter(len(columns), C.cast(ct, C.c_void_p), len(eb.nodes), C.cast(nodes, C.c_void_p),
+                           predicate, rowset.ptr, sel.ctypes.data, err, 512) != 0:
+        raise RuntimeError(err.value.decode())
+    return sel[: rowset.rs.RowCount]
+
+
+def hash_rows(columns, keys, rowset) -> np.ndarray:
+    from qumirdb_b200 import coltypes, i32s
+    ct = coltypes(columns)
+    k = i32s(keys)
+    out = np.zeros(max(1, rowset.rs.RowCount), dtype=np.uint64)
+    err = C.create_string_buffer(512)
+    if lib().oracle_hash(len(columns), C.cast(ct, C.c_void_p), len(keys), C.cast(k, C.c_void_p), rowset.ptr,
+                         out.ctypes.data, err, 512) != 0:
+        raise RuntimeError(err.value.decode())
+    return out[: rowset.rs.RowCount]
+
+
+def sort(spec, store_rowsets, row_ids: np.ndarray, descs=None, nulls_firsts=None) -> np.ndarray:
+    ids = np.ascontiguousarray(row_ids, dtype=np.int64).copy()
+    store = _rowsets(store_rowsets)
+    err = C.create_string_buffer(512)
+    d = None if descs is None else np.asarray(descs, dtype=np.bool_)
+    nf = None if nulls_firsts is None else np.asarray(nulls_firsts, dtype=np.bool_)
+    if lib().oracle_sort(C.byref(spec.struct), store, ids.ctypes.data, len(ids),
+                         None if d is None else d.ctypes.data, None if nf is None else nf.ctypes.data, err, 512) != 0:
+        raise RuntimeError(err.value.decode())
+    return ids
+
+
+def top_k(spec, store_rowsets, row_ids: np.ndarray, limit: int, descs=None, nulls_firsts=None) -> np.ndarray:
+    ids = np.ascontiguousarray(row_ids, dtype=np.int64).copy()
+    store = _rowsets(store_rowsets)
+    d = None if descs is None else np.asarray(descs, dtype=np.bool_)
+    nf = None if nulls_firsts is None else np.asarray(nulls_firsts, dtype=np.bool_)
+    k = lib().oracle_top_k(C.byref(spec.struct), store, ids.ctypes.data, len(ids), limit,
+                           None if d is None else d.ctypes.data, None if nf is None else nf.ctypes.data)
+    return ids[:k]

@@ -1,0 +1,395 @@
+"""qumirdb_b200 — B200 (sm_100a) execution hot path of QumirDB behind its C ABI.
+
+Python host side: loads libqdb_gpu.so (built in-tree by qumirdb_b200/build.py),
+builds expression/operator descriptors, and drives the reference-shaped entry
+points the way the engine's processors do (TAggregateProcessor,
+qdb/exec/aggregate_exec.cpp:70-136; TRowJoinProcessor,
+qdb/exec/row_join_exec.cpp:93-220; TSortProcessor,
+qdb/exec/sort_exec.cpp:393-490).  There is no CPU execution path here: a
+missing library or a device error raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+import numpy as np
+
+from . import abi
+from .abi import *  # noqa: F401,F403
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libqdb_gpu.so"
+HEADER = _HERE.parent / "include" / "qdb_gpu.h"
+
+_lib = None
+_lock = threading.Lock()
+_initialised: set[int] = set()
+
+
+class QdbError(RuntimeError):
+    pass
+
+
+def lib() -> C.CDLL:
+    """The device library; raises if it has not been built."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                raise QdbError(f"{LIB_PATH} is missing: run qumirdb_b200/build.py (or __graft_entry__.build())")
+            _lib = abi.bind(C.CDLL(str(LIB_PATH)))
+        return _lib
+
+
+def last_error() -> str:
+    return lib().qdb_gpu_last_error().decode()
+
+
+def init(device: int = 0) -> None:
+    """Binds the calling thread to `device` (creates the CUDA context)."""
+    if lib().qdb_gpu_init(device) != 0:
+        raise QdbError(f"qdb_gpu_init({device}) failed: {last_error()}")
+    _initialised.add(threading.get_ident())
+
+
+def _ensure_init() -> None:
+    if threading.get_ident() not in _initialised:
+        init(0)
+
+
+# ---------------------------------------------------------------------------
+# Expressions.
+# ---------------------------------------------------------------------------
+class ExprBuilder:
+    """Flat expression node array (operands before their users)."""
+
+    def __init__(self) -> None:
+        self.nodes: list[tuple] = []
+        self._lists: list = []
+
+    def _add(self, op, type_, scale=0, column=0, args=(0, 0, 0), imm_lo=0, imm_hi=0, lst=None) -> int:
+        self.nodes.append((op, type_, scale, column, tuple(args) + (0,) * (3 - len(args)), imm_lo, imm_hi, lst))
+        return len(self.nodes) - 1
+
+    def col(self, c: int, type_: int, scale: int = 0) -> int:
+        return self._add(abi.COLUMN, type_, scale, column=c)
+
+    def const(self, v, type_: int, scale: int = 0) -> int:
+        if type_ in (abi.F64, abi.F32):
+            bits = int(np.array([float(v)], dtype=np.float64).view(np.int64)[0])
+            return self._add(abi.CONST, type_, scale, imm_lo=bits)
+        v = int(v)
+        lo = v & ((1 << 64) - 1)
+        hi = (v >> 64) & ((1 << 64) - 1)
+        to_s = lambda u: u - (1 << 64) if u >= (1 << 63) else u  # noqa: E731
+        return self._add(abi.CONST, type_, scale, imm_lo=to_s(lo), imm_hi=to_s(hi))
+
+    def null(self, type_: int = abi.I64) -> int:
+        return self._add(abi.NULL, type_)
+
+    def op(self, op: int, type_: int, *args: int, scale: int = 0) -> int:
+        return self._add(op, type_, scale, args=args)
+
+    def in_list(self, a: int, values, type_: int = abi.BOOL) -> int:
+        arr = (C.c_int64 * len(values))(*[int(x) for x in values])
+        self._lists.append(arr)
+        idx = self._add(abi.IN_LIST, type_, 0, args=(a,), lst=arr)
+        return idx
+
+    def array(self):
+        arr = (abi.Expr * max(1, len(self.nodes)))()
+        for k, (op, t, s, c, args, lo, hi, lst) in enumerate(self.nodes):
+            e = arr[k]
+            e.op, e.type, e.scale, e.column = op, t, s, c
+            e.args[0], e.args[1], e.args[2] = args
+            e.imm_lo, e.imm_hi = lo, hi
+            if lst is not None:
+                e.list_len = len(lst)
+                e.list = C.cast(lst, C.POINTER(C.c_int64))
+        return arr
+
+
+def coltypes(types) -> C.Array:
+    """[(type, scale, nullable)] -> qdb_column_type array."""
+    arr = (abi.ColumnType * max(1, len(types)))()
+    for k, t in enumerate(types):
+        t = (tuple(t) + (0, 0))[:3]
+        arr[k].type, arr[k].scale, arr[k].nullable = t[0], t[1], t[2]
+        arr[k].precision = 38 if t[0] == abi.DECIMAL128 else (18 if t[0] == abi.DECIMAL64 else 0)
+    return arr
+
+
+def i32s(vals) -> C.Array:
+    return (C.c_int32 * max(1, len(vals)))(*vals)
+
+
+# ---------------------------------------------------------------------------
+# Row sets.
+# ---------------------------------------------------------------------------
+def _bitmap(valid: np.ndarray) -> np.ndarray:
+    return np.packbits(valid.astype(np.uint8), bitorder="little")
+
+
+class HostRowSet:
+    """A TRowSet over host numpy columns (kept alive by this object)."""
+
+    def __init__(self, columns, masks=None, selection=None, rows=None):
+        self.arrays = [np.ascontiguousarray(c) for c in columns]
+        n = rows if rows is not None else (len(self.arrays[0]) if self.arrays else 0)
+        self.masks = [None if m is None else _bitmap(np.asarray(m, dtype=bool)) for m in (masks or [None] * len(columns))]
+        self.selection = None if selection is None else np.ascontiguousarray(selection, dtype=np.uint8)
+        self.cols = (abi.Column * max(1, len(self.arrays)))()
+        for k, a in enumerate(self.arrays):
+            self.cols[k].Data = a.ctypes.data if a.size else None
+            if self.masks[k] is not None:
+                self.cols[k].Mask = self.masks[k].ctypes.data
+        self.rs = abi.RowSet()
+        self.rs.Columns = self.cols
+        self.rs.ColumnCount = len(self.arrays)
+        self.rs.RowCount = n
+        self.rs.Selection = None if self.selection is None else self.selection.ctypes.data
+        self.rs.RefCount = 1
+
+    @property
+    def ptr(self):
+        return C.byref(self.rs)
+
+
+class DeviceBuffer:
+    def __init__(self, nbytes: int):
+        _ensure_init()
+        self.nbytes = nbytes
+        self.ptr = lib().qdb_gpu_alloc(max(16, nbytes))
+        if not self.ptr:
+            raise QdbError(f"device allocation failed: {last_error()}")
+
+    def upload(self, host: np.ndarray, stream_sync: bool = True) -> "DeviceBuffer":
+        host = np.ascontiguousarray(host)
+        if lib().qdb_gpu_memcpy(self.ptr, host.ctypes.data, host.nbytes) != 0:
+            raise QdbError(last_error())
+        if stream_sync:
+            synchronize()
+        return self
+
+    def download(self, dtype, count: int) -> np.ndarray:
+        out = np.empty(count, dtype=dtype)
+        if count and lib().qdb_gpu_memcpy(out.ctypes.data, self.ptr, out.nbytes) != 0:
+            raise QdbError(last_error())
+        synchronize()
+        return out
+
+    def free(self) -> None:
+        if self.ptr:
+            lib().qdb_gpu_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def synchronize() -> None:
+    if lib().qdb_gpu_synchronize() != 0:
+        raise QdbError(last_error())
+
+
+class DeviceRowSet:
+    """A TRowSet whose columns live in HBM (the resident column cache)."""
+
+    def __init__(self, columns, masks=None, selection=None):
+        host = HostRowSet(columns, masks, selection)
+        self.rows = host.rs.RowCount
+        self.bufs = []
+        self.cols = (abi.Column * max(1, len(host.arrays)))()
+        for k, a in enumerate(host.arrays):
+            b = DeviceBuffer(a.nbytes).upload(a, stream_sync=False)
+            self.bufs.append(b)
+            self.cols[k].Data = b.ptr
+            if host.masks[k] is not None:
+                mb = DeviceBuffer(host.masks[k].nbytes).upload(host.masks[k], stream_sync=False)
+                self.bufs.append(mb)
+                self.cols[k].Mask = mb.ptr
+        self.rs = abi.RowSet()
+        self.rs.Columns = self.cols
+        self.rs.ColumnCount = len(host.arrays)
+        self.rs.RowCount = self.rows
+        if host.selection is not None:
+            sb = DeviceBuffer(host.selection.nbytes).upload(host.selection, stream_sync=False)
+            self.bufs.append(sb)
+            self.rs.Selection = sb.ptr
+        self.rs.RefCount = 1
+        synchronize()
+
+    @property
+    def ptr(self):
+        return C.byref(self.rs)
+
+
+def read_rowset(rs: abi.RowSet, types) -> tuple[list[np.ndarray], list[np.ndarray]]:
+    """Host output row set -> (values, validity) numpy columns by qdb type."""
+    n = rs.RowCount
+    values, valid = [], []
+    for k, t in enumerate(types):
+        col = rs.Columns[k]
+        w = abi.WIDTH[t]
+        raw = np.ctypeslib.as_array(C.cast(col.Data, C.POINTER(C.c_uint8)), shape=(max(1, n * w),))[: n * w].copy()
+        if t == abi.DECIMAL128:
+            words = raw.view(np.uint64).reshape(n, 2)
+            vals = np.array([int(lo) | (int(hi) << 64) for lo, hi in words], dtype=object)
+            vals = np.array([v - (1 << 128) if v >= (1 << 127) else v for v in vals], dtype=object)
+        else:
+            dt = {abi.I8: np.int8, abi.I16: np.int16, abi.I32: np.int32, abi.I64: np.int64, abi.U8: np.uint8,
+                  abi.U16: np.uint16, abi.U32: np.uint32, abi.U64: np.uint64, abi.F32: np.float32,
+                  abi.F64: np.float64, abi.DATE32: np.int32, abi.DECIMAL64: np.int64, abi.CHAR1: np.uint8,
+                  abi.BOOL: np.uint8}[t]
+            vals = raw.view(dt)
+        values.append(vals)
+        if col.Mask:
+            bits = np.ctypeslib.as_array(C.cast(col.Mask, C.POINTER(C.c_uint8)), shape=(max(1, (n + 7) // 8),))
+            valid.append(np.unpackbits(bits, bitorder="little")[:n].astype(bool))
+        else:
+            valid.append(np.ones(n, dtype=bool))
+    return values, valid
+
+
+def release(rs: abi.RowSet) -> None:
+    if rs.Destroy:
+        rs.Destroy(C.byref(rs))
+
+
+# ---------------------------------------------------------------------------
+# Programs and processors.
+# ---------------------------------------------------------------------------
+class Program:
+    def __init__(self, handle, keep=()):
+        if not handle:
+            raise QdbError(f"compile failed: {last_error()}")
+        self.handle = handle
+        self._keep = keep
+
+    def __del__(self):
+        try:
+            if self.handle:
+                lib().qdb_gpu_program_destroy(self.handle)
+        except Exception:
+            pass
+
+
+def compile_aggregate(spec) -> Program:
+    err = C.create_string_buffer(512)
+    h = lib().qdb_gpu_compile_aggregate(C.byref(spec.struct), err, 512)
+    if not h:
+        raise QdbError(err.value.decode())
+    return Program(h, keep=(spec,))
+
+
+def compile_join_aggregate(jspec, aspec) -> Program:
+    err = C.create_string_buffer(512)
+    h = lib().qdb_gpu_compile_join_aggregate(C.byref(jspec.struct), C.byref(aspec.struct), err, 512)
+    if not h:
+        raise QdbError(err.value.decode())
+    return Program(h, keep=(jspec, aspec))
+
+
+def compile_row_join(jspec) -> Program:
+    err = C.create_string_buffer(512)
+    h = lib().qdb_gpu_compile_row_join(C.byref(jspec.struct), err, 512)
+    if not h:
+        raise QdbError(err.value.decode())
+    return Program(h, keep=(jspec,))
+
+
+class Aggregate:
+    """The engine's TAggregateProcessor over the device table."""
+
+    def __init__(self, prog: Program, initial_capacity: int = 8):
+        _ensure_init()
+        self.prog = prog
+        self.ht = (C.c_uint8 * abi.HASH_TABLE_SIZE)()
+        if lib().qdb_gpu_agg_dispatch(prog.handle, self.ht, None, initial_capacity, abi.AGG_INIT) == 0:
+            raise QdbError(f"aggregate initialization failed: {last_error()}")
+
+    @property
+    def groups(self) -> int:
+        return C.cast(self.ht, C.POINTER(C.c_int64))[9]
+
+    def add(self, rowset) -> int:
+        r = lib().qdb_gpu_agg_dispatch(self.prog.handle, self.ht, rowset.ptr, 0, abi.AGG_UPDATE)
+        if r < 0:
+            raise QdbError(f"aggregate update failed: {last_error()}")
+        return r
+
+    def finish(self) -> abi.RowSet:
+        out = abi.RowSet()
+        n = lib().qdb_gpu_agg_finish_rowset(self.prog.handle, self.ht, C.byref(out))
+        if n < 0:
+            raise QdbError(f"aggregate finish failed: {last_error()}")
+        return out
+
+
+class RowJoin:
+    """The engine's TRowJoinProcessor state: arena, table, scratch, pairs."""
+
+    def __init__(self, prog: Program):
+        _ensure_init()
+        self.prog = prog
+        self.arena = (C.c_uint8 * abi.ROW_ARENA_SIZE)()
+        self.table = (C.c_uint8 * abi.ROW_TABLE_SIZE)()
+        self.scratch = (C.c_uint8 * abi.ROW_SCRATCH_SIZE)()
+        self.pairs = (C.c_uint8 * abi.PAIR_BUFFER_SIZE)()
+        self._op(None, abi.JR_INIT)
+
+    def _op(self, batch, op) -> None:
+        ok = lib().qdb_gpu_jr_dispatch(self.prog.handle, self.arena, self.table, self.scratch, self.pairs,
+                                       None if batch is None else batch.ptr, op)
+        if not ok:
+            raise QdbError(f"jr_dispatch({op}) failed: {last_error()}")
+
+    def append(self, batch) -> None:
+        self._op(batch, abi.JR_APPEND)
+
+    def build(self) -> None:
+        self._op(None, abi.JR_BUILD)
+
+    def probe(self, batch) -> int:
+        self._op(batch, abi.JR_PROBE)
+        return self.pair_count
+
+    @property
+    def pair_count(self) -> int:
+        return C.cast(self.pairs, C.POINTER(C.c_int64))[0]
+
+    @property
+    def arena_rows(self) -> int:
+        return C.cast(self.arena, C.POINTER(C.c_int64))[5]
+
+    def materialize(self, stream, start: int, limit: int) -> tuple[int, abi.RowSet]:
+        out = abi.RowSet()
+        n = lib().qdb_gpu_jr_materialize(self.prog.handle, self.pairs, stream.ptr, start, limit, C.byref(out))
+        if n < 0:
+            raise QdbError(f"jr_materialize failed: {last_error()}")
+        return n, out
+
+    def probe_aggregate(self, agg: Aggregate, batch) -> int:
+        n = lib().qdb_gpu_join_aggregate_probe(self.prog.handle, self.arena, self.table, agg.ht, batch.ptr)
+        if n < 0:
+            raise QdbError(f"join aggregate probe failed: {last_error()}")
+        return n
+
+
+def profile(on: bool) -> None:
+    lib().qdb_gpu_profile_enable(1 if on else 0)
+
+
+def profile_read(cap: int = 4096) -> list[tuple[str, float, int]]:
+    buf = (abi.KernelTime * cap)()
+    n = lib().qdb_gpu_profile_read(buf, cap)
+    return [(buf[i].name.decode(), buf[i].ms, buf[i].units) for i in range(n)]
+
+
+def launch_count(reset: bool = False) -> int:
+    return lib().qdb_gpu_launch_count(1 if reset else 0)

@@ -1,0 +1,311 @@
+// expr.cu — row-parallel filter, project, shuffle hash, compaction and gather
+// kernels (the engine's filter / project / hash kernel contracts,
+// qdb/kernel/compiler.h:488-520), built on the functors of eval.h.
+#include <algorithm>
+
+#include "../../include/qdb_gpu.h"
+#include "common.cuh"
+#include "eval.h"
+#include "hash.h"
+#include "kernels.h"
+
+namespace qdb {
+
+namespace {
+
+struct GlobalAcc {
+    const AggPlan* P;
+    int64_t row;
+    __device__ __forceinline__ const char* Ptr(int c) const { return P->cols[c].data + row * P->cols[c].width; }
+    __device__ __forceinline__ i128 Int(int c) const {
+        const ColDesc& cd = P->cols[c];
+        if (cd.kind == LK_BOOLBIT) {
+            const int64_t bit = cd.bit_off + row;
+            return (reinterpret_cast<const uint8_t*>(cd.data)[bit >> 3] >> (bit & 7)) & 1;
+        }
+        const char* p = Ptr(c);
+        const bool u = cd.kind == LK_UNSIGNED;
+        switch (cd.width) {
+            case 1: return u ? i128(*reinterpret_cast<const uint8_t*>(p)) : i128(*reinterpret_cast<const int8_t*>(p));
+            case 2: return u ? i128(*reinterpret_cast<const uint16_t*>(p)) : i128(*reinterpret_cast<const int16_t*>(p));
+            case 4: return u ? i128(*reinterpret_cast<const uint32_t*>(p)) : i128(*reinterpret_cast<const int32_t*>(p));
+            case 8: return u ? i128(*reinterpret_cast<const uint64_t*>(p)) : i128(*reinterpret_cast<const int64_t*>(p));
+            default: {
+                const uint64_t* q = reinterpret_cast<const uint64_t*>(p);
+                return i128((u128(q[1]) << 64) | q[0]);
+            }
+        }
+    }
+    __device__ __forceinline__ double F64(int c) const {
+        const ColDesc& cd = P->cols[c];
+        if (cd.kind == LK_F64) return *reinterpret_cast<const double*>(Ptr(c));
+        if (cd.kind == LK_F32) return double(*reinterpret_cast<const float*>(Ptr(c)));
+        const i128 v = Int(c);
+        return cd.scale ? double(v) / Pow10F(cd.scale) : double(v);
+    }
+    __device__ __forceinline__ bool Null(int c) const {
+        const ColDesc& cd = P->cols[c];
+        if (!cd.mask) return false;
+        const int64_t bit = cd.mask_off + row;
+        return !((cd.mask[bit >> 3] >> (bit & 7)) & 1);
+    }
+};
+
+struct ExprLaunch {
+    AggPlan P;
+    ExprArgs A;
+};
+
+__global__ void __launch_bounds__(256) FilterKernel(const __grid_constant__ ExprLaunch L) {
+    const AggPlan& P = L.P;
+    for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < L.A.nrows;
+         r += int64_t(gridDim.x) * blockDim.x) {
+        bool pass = P.selection == nullptr || P.selection[r] != 0;
+        GlobalAcc acc{&P, r};
+        for (int j = 0; j < L.A.n_null_reject && pass; ++j) pass = !acc.Null(L.A.null_reject[j]);
+        if (pass && P.filter_kind == 1) {
+            pass = AtomsPass(P, acc);
+        } else if (pass && P.filter_kind == 2) {
+            GVal gv[kMaxGNodes];
+            uint64_t gn = 0;
+            if (!EvalGeneric(P.prog, P.filter_node, P.list, acc, gv, gn)) {
+                SetError(L.A.err, DE_DIV_ZERO);
+                pass = false;
+            } else {
+                pass = !((gn >> P.filter_node) & 1) && gv[P.filter_node].i != 0;
+            }
+        }
+        L.A.out_sel[r] = pass ? 1 : 0;
+    }
+}
+
+__device__ __forceinline__ void StoreTyped(void* base, int type, int64_t r, i128 iv, double fv) {
+    char* p = static_cast<char*>(base);
+    switch (type) {
+        case QDB_TYPE_F64: reinterpret_cast<double*>(p)[r] = fv; break;
+        case QDB_TYPE_F32: reinterpret_cast<float*>(p)[r] = float(fv); break;
+        case QDB_TYPE_DECIMAL128:
+            reinterpret_cast<uint64_t*>(p)[2 * r] = uint64_t(u128(iv));
+            reinterpret_cast<uint64_t*>(p)[2 * r + 1] = uint64_t(u128(iv) >> 64);
+            break;
+        case QDB_TYPE_I64: case QDB_TYPE_U64: case QDB_TYPE_DECIMAL64:
+            reinterpret_cast<int64_t*>(p)[r] = int64_t(iv);
+            break;
+        case QDB_TYPE_I32: case QDB_TYPE_U32: case QDB_TYPE_DATE32:
+            reinterpret_cast<int32_t*>(p)[r] = int32_t(iv);
+            break;
+        case QDB_TYPE_I16: case QDB_TYPE_U16: reinterpret_cast<int16_t*>(p)[r] = int16_t(iv); break;
+        default: reinterpret_cast<uint8_t*>(p)[r] = uint8_t(iv); break;
+    }
+}
+
+__global__ void __launch_bounds__(256) ProjectKernel(const __grid_constant__ ExprLaunch L) {
+    const AggPlan& P = L.P;
+    for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < L.A.nrows;
+         r += int64_t(gridDim.x) * blockDim.x) {
+        if (P.selection && !P.selection[r]) continue;
+        GlobalAcc acc{&P, r};
+        GVal gv[kMaxGNodes];
+        uint64_t gn = 0;
+        if (P.generic_root >= 0 && !EvalGeneric(P.prog, P.generic_root, P.list, acc, gv, gn)) {
+            SetError(L.A.err, DE_DIV_ZERO);
+            continue;
+        }
+        for (int k = 0; k < L.A.nout; ++k) {
+            i128 iv = 0;
+            double fv = 0.0;
+            const int idx = L.A.out_idx[k];
+            if (L.A.out_src[k] == VS_SOP) {
+                const SopValue& v = P.values[idx];
+                if (!SopNull(v, acc)) {
+                    if (v.kind == VK_F64) fv = SopF64(v, acc);
+                    else iv = SopInt(v, acc);
+                }
+            } else if (!((gn >> idx) & 1)) {
+                iv = gv[idx].i;
+                fv = gv[idx].f;
+                if (P.prog.nodes[idx].dom == GD_F64) iv = 0;
+            }
+            StoreTyped(L.A.out_ptr[k], L.A.out_type[k], r, iv, fv);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) HashKernel(const __grid_constant__ ExprLaunch L) {
+    const AggPlan& P = L.P;
+    for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < L.A.nrows;
+         r += int64_t(gridDim.x) * blockDim.x) {
+        if (P.selection && !P.selection[r]) continue;
+        GlobalAcc acc{&P, r};
+        uint64_t h = 0;
+        for (int j = 0; j < L.A.nhash; ++j) {
+            const int c = L.A.hash_slot[j];
+            const int t = L.A.hash_type[j];
+            uint64_t fh = 0;
+            if (!acc.Null(c)) {
+                const bool fl = t == QDB_TYPE_F32 || t == QDB_TYPE_F64;
+                fh = LeafHashOf(t, fl ? i128(0) : acc.Int(c), fl ? acc.F64(c) : 0.0);
+            }
+            h = Combine(h, fh);
+        }
+        L.A.hashes[r] = h;
+    }
+}
+
+constexpr int kCompactChunk = 4096;
+
+__global__ void __launch_bounds__(256) CountFlagsKernel(const uint8_t* flags, int64_t n, unsigned long long* counts) {
+    __shared__ unsigned cnt;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    const int64_t begin = int64_t(blockIdx.x) * kCompactChunk;
+    const int64_t end = begin + kCompactChunk < n ? begin + kCompactChunk : n;
+    unsigned local = 0;
+    for (int64_t i = begin + threadIdx.x; i < end; i += blockDim.x) local += flags[i] ? 1 : 0;
+    atomicAdd(&cnt, local);
+    __syncthreads();
+    if (threadIdx.x == 0) counts[blockIdx.x] = cnt;
+}
+
+__global__ void __launch_bounds__(256) WriteFlagsKernel(const uint8_t* flags, int64_t n,
+                                                        const unsigned long long* offsets, int64_t nblocks,
+                                                        int64_t* out, unsigned long long* d_count) {
+    __shared__ unsigned warp_cnt[8];
+    __shared__ unsigned running;
+    if (threadIdx.x == 0) running = 0;
+    __syncthreads();
+    const int64_t begin = int64_t(blockIdx.x) * kCompactChunk;
+    const int64_t end = begin + kCompactChunk < n ? begin + kCompactChunk : n;
+    const unsigned long long base = offsets[blockIdx.x];
+    for (int64_t b = begin; b < end; b += blockDim.x) {
+        const int64_t i = b + threadIdx.x;
+        const bool on = i < end && flags[i];
+        const unsigned m = __ballot_sync(kFull, on);
+        if (LaneId() == 0) warp_cnt[threadIdx.x >> 5] = __popc(m);
+        __syncthreads();
+        unsigned before = running;
+        for (int w = 0; w < int(threadIdx.x >> 5); ++w) before += warp_cnt[w];
+        before += __popc(m & ((1u << LaneId()) - 1));
+        if (on) out[base + before] = i;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned tot = 0;
+            for (int w = 0; w < 8; ++w) tot += warp_cnt[w];
+            running += tot;
+        }
+        __syncthreads();
+    }
+    if (blockIdx.x == nblocks - 1 && threadIdx.x == 0) *d_count = base + running;
+}
+
+__global__ void __launch_bounds__(256) GatherKernel(const char* src, int width, const int64_t* idx, int stride,
+                                                    int64_t n, char* out) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t j = idx[i * stride];
+        switch (width) {
+            case 1: out[i] = j < 0 ? 0 : src[j]; break;
+            case 2: reinterpret_cast<int16_t*>(out)[i] = j < 0 ? 0 : reinterpret_cast<const int16_t*>(src)[j]; break;
+            case 4: reinterpret_cast<int32_t*>(out)[i] = j < 0 ? 0 : reinterpret_cast<const int32_t*>(src)[j]; break;
+            case 8: reinterpret_cast<int64_t*>(out)[i] = j < 0 ? 0 : reinterpret_cast<const int64_t*>(src)[j]; break;
+            default: {
+                const uint64_t* s = reinterpret_cast<const uint64_t*>(src);
+                uint64_t* o = reinterpret_cast<uint64_t*>(out);
+                o[2 * i] = j < 0 ? 0 : s[2 * j];
+                o[2 * i + 1] = j < 0 ? 0 : s[2 * j + 1];
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) GatherValidityKernel(const uint8_t* mask, int64_t mask_off, const int64_t* idx,
+                                                            int stride, int64_t n, uint32_t* out, int64_t out_off) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t j = idx[i * stride];
+        bool valid = j >= 0;
+        if (valid && mask) {
+            const int64_t bit = mask_off + j;
+            valid = (mask[bit >> 3] >> (bit & 7)) & 1;
+        }
+        const int64_t o = out_off + i;
+        if (valid) atomicOr(&out[o >> 5], 1u << (o & 31));
+    }
+}
+
+int Blocks(int64_t n, int threads) {
+    return int(std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, int64_t(DeviceSMs()) * 16)));
+}
+
+ExprLaunch* ThreadLaunch() {
+    static thread_local ExprLaunch* p = nullptr;
+    if (!p) p = new ExprLaunch();
+    return p;
+}
+
+}  // namespace
+
+void FilterRows(const ExprArgs& a, cudaStream_t s) {
+    if (a.nrows == 0) return;
+    ExprLaunch& L = *ThreadLaunch();
+    L.P = *a.plan;
+    L.A = a;
+    ProfileBegin(s, "filter", a.nrows);
+    FilterKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(L);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+void ProjectRows(const ExprArgs& a, cudaStream_t s) {
+    if (a.nrows == 0) return;
+    ExprLaunch& L = *ThreadLaunch();
+    L.P = *a.plan;
+    L.A = a;
+    ProfileBegin(s, "project", a.nrows);
+    ProjectKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(L);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+void HashRows(const ExprArgs& a, cudaStream_t s) {
+    if (a.nrows == 0) return;
+    ExprLaunch& L = *ThreadLaunch();
+    L.P = *a.plan;
+    L.A = a;
+    ProfileBegin(s, "hash", a.nrows);
+    HashKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(L);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+size_t CompactScratch(int64_t n) {
+    return size_t((n + kCompactChunk - 1) / kCompactChunk + 1) * sizeof(unsigned long long);
+}
+
+void CompactFlags(const uint8_t* flags, int64_t n, int64_t* out_idx, unsigned long long* d_count, void* scratch,
+                  cudaStream_t s) {
+    if (n == 0) {
+        cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s);
+        return;
+    }
+    const int64_t nb = (n + kCompactChunk - 1) / kCompactChunk;
+    auto* counts = static_cast<unsigned long long*>(scratch);
+    CountFlagsKernel<<<int(nb), 256, 0, s>>>(flags, n, counts);
+    ExclusiveScanU64(counts, nb, s);
+    WriteFlagsKernel<<<int(nb), 256, 0, s>>>(flags, n, counts, nb, out_idx, d_count);
+    CountLaunch(2);
+}
+
+void GatherColumn(const char* src, int width, const int64_t* idx, int idx_stride, int64_t n, char* out,
+                  cudaStream_t s) {
+    if (n == 0) return;
+    GatherKernel<<<Blocks(n, 256), 256, 0, s>>>(src, width, idx, idx_stride, n, out);
+    CountLaunch();
+}
+
+void GatherValidity(const uint8_t* mask, int64_t mask_off, const int64_t* idx, int idx_stride, int64_t n,
+                    uint32_t* out_words, int64_t out_bit_off, cudaStream_t s) {
+    if (n == 0) return;
+    GatherValidityKernel<<<Blocks(n, 256), 256, 0, s>>>(mask, mask_off, idx, idx_stride, n, out_words, out_bit_off);
+    CountLaunch();
+}
+
+}  // namespace qdb

@@ -1,0 +1,612 @@
+// join_rt.cpp — row join entries of the C ABI: jr_dispatch (Init / Append /
+// Build / Probe), jr_materialize and the fused join-aggregate probe.
+//
+// The caller-owned state buffers keep the engine's layouts where the engine
+// reads them (qdb/exec/row_join_exec.h:63-101): arena.Rows (offset 40),
+// table.Capacity (8) / Rows (32) / Keys (40), pairs.Count (0).  Word 0 of the
+// arena and table buffers holds this library's device state.
+#include <algorithm>
+#include <cstring>
+
+#include "runtime.h"
+
+namespace qdb {
+
+namespace {
+
+constexpr uint32_t kArenaMagic = 0x5144414a;   // 'QDAJ'
+constexpr uint32_t kTableMagic = 0x5144544a;   // 'QDTJ'
+
+struct ArenaCol {
+    char* data = nullptr;        // device, capacity rows
+    uint32_t* valid = nullptr;   // device bitmap (capacity bits), or nullptr
+    int width = 0;
+    int type = 0;
+};
+
+// Build rows in append order: the key columns, then the payload columns.
+struct ArenaState {
+    uint32_t magic = kArenaMagic;
+    cudaStream_t s = nullptr;
+    int64_t rows = 0;
+    int64_t capacity = 0;
+    std::vector<ArenaCol> keys;
+    std::vector<ArenaCol> payload;
+};
+
+struct TableState {
+    uint32_t magic = kTableMagic;
+    cudaStream_t s = nullptr;
+    uint64_t* entries = nullptr;
+    int64_t capacity = 0;
+    int64_t* special = nullptr;
+    unsigned long long* nspecial_d = nullptr;
+    int64_t nspecial = 0;
+    JTableDev dev() const {
+        JTableDev j;
+        j.entries = entries;
+        j.mask = uint64_t(capacity - 1);
+        j.special_rows = special;
+        j.nspecial = nspecial;
+        return j;
+    }
+};
+
+constexpr uint32_t kPairMagic = 0x51445050;   // 'QDPP'
+
+// The engine reads only PairBuffer.Count; Data points at this host record of
+// the device pairs and of the arena their build rows index.
+struct PairState {
+    uint32_t magic = kPairMagic;
+    int64_t* dev = nullptr;        // (probe row, arena row) pairs
+    int64_t cap = 0;
+    ArenaState* arena = nullptr;
+    cudaStream_t s = nullptr;
+};
+
+struct PairBuf {
+    int64_t count;
+    int64_t capacity;
+    PairState* state;
+};
+
+ArenaState* ArenaOf(void* arena) {
+    auto* a = *static_cast<ArenaState**>(arena);
+    return (a && a->magic == kArenaMagic) ? a : nullptr;
+}
+
+TableState* TableOf(void* table) {
+    auto* t = *static_cast<TableState**>(table);
+    return (t && t->magic == kTableMagic) ? t : nullptr;
+}
+
+int Width(int type) { return StorageWidth(type); }
+
+bool IsFloat(int t) { return t == QDB_TYPE_F32 || t == QDB_TYPE_F64; }
+bool IsSigned(int t) {
+    return t != QDB_TYPE_U8 && t != QDB_TYPE_U16 && t != QDB_TYPE_U32 && t != QDB_TYPE_U64 && t != QDB_TYPE_CHAR1;
+}
+
+// Packs up to four key columns into one word.  Both sides must agree on the
+// key types (the planner casts join keys to a common type).
+JoinKeyPlan MakeKeyPlan(const std::vector<qdb_column_type>& bcols, const std::vector<int>& bkeys,
+                        const std::vector<qdb_column_type>& pcols, const std::vector<int>& pkeys) {
+    JoinKeyPlan k;
+    const int n = int(bkeys.size());
+    if (n < 1 || n > 4) throw LowerError("row join needs 1..4 key columns");
+    k.n = n;
+    int shift = 0;
+    for (int j = 0; j < n; ++j) {
+        const int bt = bcols.at(bkeys[j]).type, pt = pcols.at(pkeys[j]).type;
+        if (bt == QDB_TYPE_BOOL || pt == QDB_TYPE_BOOL || bt == QDB_TYPE_DECIMAL128 || pt == QDB_TYPE_DECIMAL128) {
+            throw LowerError("boolean and DECIMAL128 join keys are not served");
+        }
+        if (IsFloat(bt) != IsFloat(pt)) throw LowerError("join keys mix float and integer types");
+        if ((bt == QDB_TYPE_DECIMAL64) != (pt == QDB_TYPE_DECIMAL64) ||
+            (bt == QDB_TYPE_DECIMAL64 && bcols[bkeys[j]].scale != pcols[pkeys[j]].scale)) {
+            throw LowerError("decimal join keys must share a scale");
+        }
+        k.is_float[j] = IsFloat(bt) ? 1 : 0;
+        const int bits = n == 1 ? 64 : std::max(InfoOf(bt).key_bits, InfoOf(pt).key_bits);
+        if (n > 1 && InfoOf(bt).key_bits != InfoOf(pt).key_bits) {
+            throw LowerError("multi-column join keys must have equal widths on both sides");
+        }
+        k.bits[j] = uint8_t(bits);
+        k.shift[j] = uint8_t(shift);
+        shift += bits;
+    }
+    if (shift > 64) throw LowerError("join key wider than 64 bits is not served");
+    k.full64 = (n == 1 && !k.is_float[0]) || shift >= 64 ? 1 : 0;
+    return k;
+}
+
+bool GrowArena(ArenaState* a, int64_t need) {
+    if (need <= a->capacity) return true;
+    int64_t cap = std::max<int64_t>(1024, a->capacity);
+    while (cap < need) cap *= 2;
+    auto grow = [&](ArenaCol& c) -> bool {
+        char* d = static_cast<char*>(DevAlloc(size_t(cap) * c.width, a->s));
+        if (!d) return false;
+        if (c.data) cudaMemcpyAsync(d, c.data, size_t(a->rows) * c.width, cudaMemcpyDeviceToDevice, a->s);
+        DevFree(c.data, a->s);
+        c.data = d;
+        if (c.valid || c.type < 0) {
+            uint32_t* v = static_cast<uint32_t*>(DevAlloc(size_t((cap + 31) / 32) * 4, a->s));
+            if (!v) return false;
+            cudaMemsetAsync(v, 0, size_t((cap + 31) / 32) * 4, a->s);
+            if (c.valid) cudaMemcpyAsync(v, c.valid, size_t((a->rows + 31) / 32) * 4, cudaMemcpyDeviceToDevice, a->s);
+            DevFree(c.valid, a->s);
+            c.valid = v;
+            if (c.type < 0) c.type = -c.type;
+        }
+        return true;
+    };
+    for (auto& c : a->keys) {
+        if (!grow(c)) return false;
+    }
+    for (auto& c : a->payload) {
+        if (!grow(c)) return false;
+    }
+    a->capacity = cap;
+    return true;
+}
+
+void DestroyArena(ArenaState* a) {
+    for (auto& c : a->keys) {
+        DevFree(c.data, a->s);
+        DevFree(c.valid, a->s);
+    }
+    for (auto& c : a->payload) {
+        DevFree(c.data, a->s);
+        DevFree(c.valid, a->s);
+    }
+    cudaStreamSynchronize(a->s);
+    a->magic = 0;
+    delete a;
+}
+
+void DestroyTable(TableState* t) {
+    DevFree(t->entries, t->s);
+    DevFree(t->special, t->s);
+    DevFree(t->nspecial_d, t->s);
+    cudaStreamSynchronize(t->s);
+    t->magic = 0;
+    delete t;
+}
+
+// Append: selected rows that pass the build predicate and have valid keys,
+// in input order (GenRowJoinAppendAst, qdb/kernel/join_gen.cpp:2063-2160).
+bool Append(const qdb_gpu_program* prog, ArenaState* a, qdb_rowset* batch) {
+    const JoinProgram& J = prog->join;
+    const int64_t n = batch->RowCount;
+    if (n == 0) return true;
+    cudaStream_t s = a->s;
+    Staging stg(s);
+    AggPlan plan = J.build_filter.plan;
+    if (!ResolveColumns(plan, J.build_filter.cols, J.build_columns.data(), batch, stg)) return false;
+    uint8_t* flags = static_cast<uint8_t*>(DevAlloc(size_t(n), s));
+    int64_t* idx = static_cast<int64_t*>(DevAlloc(size_t(n) * 8, s));
+    unsigned long long* dcount = static_cast<unsigned long long*>(DevAlloc(8, s));
+    void* scratch = DevAlloc(CompactScratch(n), s);
+    int* derr = static_cast<int*>(DevAlloc(sizeof(int), s));
+    if (!flags || !idx || !dcount || !scratch || !derr) return false;
+    cudaMemsetAsync(derr, 0, sizeof(int), s);
+    ExprArgs ea;
+    ea.plan = &plan;
+    ea.nrows = n;
+    ea.out_sel = flags;
+    ea.err = derr;
+    ea.n_null_reject = int(J.build_keys.size());
+    for (size_t j = 0; j < J.build_keys.size(); ++j) {
+        ea.null_reject[j] = uint8_t(J.build_filter.cols.slot_of[J.build_keys[j]]);
+    }
+    FilterRows(ea, s);
+    CompactFlags(flags, n, idx, dcount, scratch, s);
+    unsigned long long selected = 0;
+    int herr = 0;
+    cudaMemcpyAsync(&selected, dcount, 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (!CudaOk(cudaStreamSynchronize(s), "row join append")) return false;
+    bool ok = herr == 0;
+    if (!ok) SetErr("row join append: device error %d", herr);
+    if (ok && selected > 0) {
+        ok = GrowArena(a, a->rows + int64_t(selected));
+        auto gather = [&](ArenaCol& c, int input) {
+            const ColDesc& cd = plan.cols[J.build_filter.cols.slot_of[input]];
+            GatherColumn(cd.data, c.width, idx, 1, int64_t(selected), c.data + a->rows * c.width, s);
+            if (c.valid) GatherValidity(cd.mask, cd.mask_off, idx, 1, int64_t(selected), c.valid, a->rows, s);
+        };
+        for (size_t j = 0; ok && j < J.build_keys.size(); ++j) gather(a->keys[j], J.build_keys[j]);
+        for (size_t j = 0; ok && j < J.payload.size(); ++j) gather(a->payload[j], J.payload[j]);
+        a->rows += int64_t(selected);
+    }
+    DevFree(flags, s);
+    DevFree(idx, s);
+    DevFree(dcount, s);
+    DevFree(scratch, s);
+    DevFree(derr, s);
+    return ok;
+}
+
+bool Build(const qdb_gpu_program* prog, ArenaState* a, void* table) {
+    const JoinProgram& J = prog->join;
+    TableState* old = TableOf(table);
+    if (old) DestroyTable(old);
+    auto* t = new TableState();
+    t->s = a->s;
+    int64_t cap = 1024;
+    while (cap < a->rows * 2) cap *= 2;
+    t->capacity = cap;
+    t->entries = static_cast<uint64_t*>(DevAlloc(size_t(cap) * 16, t->s));
+    t->special = static_cast<int64_t*>(DevAlloc(size_t(std::max<int64_t>(a->rows, 1)) * 8, t->s));
+    t->nspecial_d = static_cast<unsigned long long*>(DevAlloc(8, t->s));
+    if (!t->entries || !t->special || !t->nspecial_d) {
+        DestroyTable(t);
+        return false;
+    }
+    cudaMemsetAsync(t->nspecial_d, 0, 8, t->s);
+    JoinInitTable(t->entries, cap, t->s);
+    JoinBuildArgs b;
+    std::memset(&b, 0, sizeof(b));
+    for (size_t j = 0; j < J.build_keys.size(); ++j) {
+        const int ty = J.build_columns[J.build_keys[j]].type;
+        b.key_data[j] = a->keys[j].data;
+        b.key_mask[j] = nullptr;   // the arena only holds rows with valid keys
+        b.key_width[j] = uint8_t(Width(ty));
+        b.key_signed[j] = IsSigned(ty) ? 1 : 0;
+    }
+    b.jkey = J.build_jk;
+    b.nrows = a->rows;
+    b.entries = t->entries;
+    b.mask = uint64_t(cap - 1);
+    b.special_rows = t->special;
+    b.nspecial = t->nspecial_d;
+    b.row_base = 0;
+    JoinBuild(b, t->s);
+    unsigned long long ns = 0;
+    cudaMemcpyAsync(&ns, t->nspecial_d, 8, cudaMemcpyDeviceToHost, t->s);
+    if (!CudaOk(cudaStreamSynchronize(t->s), "row join build")) {
+        DestroyTable(t);
+        return false;
+    }
+    t->nspecial = int64_t(ns);
+    *static_cast<TableState**>(table) = t;
+    int64_t* w = static_cast<int64_t*>(table);
+    w[1] = cap;        // Capacity
+    w[4] = a->rows;    // Rows
+    w[5] = a->rows;    // Keys (rows indexed)
+    return true;
+}
+
+// Resolves the probe key columns of a batch into JoinProbeArgs.
+bool ProbeKeyArgs(const JoinProgram& J, qdb_rowset* batch, Staging& stg, JoinProbeArgs& p) {
+    const int64_t n = batch->RowCount;
+    for (size_t j = 0; j < J.probe_keys.size(); ++j) {
+        const int input = J.probe_keys[j];
+        if (input >= batch->ColumnCount) {
+            SetErr("probe batch has too few columns");
+            return false;
+        }
+        const int ty = J.probe_columns[input].type;
+        const qdb_column& c = batch->Columns[input];
+        p.key_data[j] = static_cast<const char*>(stg.Device(c.Data, size_t(n) * Width(ty)));
+        p.key_width[j] = uint8_t(Width(ty));
+        p.key_signed[j] = IsSigned(ty) ? 1 : 0;
+        if (c.Mask) {
+            p.key_mask[j] = static_cast<const uint8_t*>(stg.Device(c.Mask, size_t((c.MaskBitOffset + n + 7) / 8)));
+            p.key_mask_off[j] = c.MaskBitOffset;
+        }
+    }
+    p.selection = batch->Selection ? static_cast<const uint8_t*>(stg.Device(batch->Selection, size_t(n))) : nullptr;
+    return true;
+}
+
+bool Probe(const qdb_gpu_program* prog, ArenaState* a, TableState* t, PairBuf* pairs, qdb_rowset* batch) {
+    const JoinProgram& J = prog->join;
+    const int64_t n = batch->RowCount;
+    cudaStream_t s = a->s;
+    Staging stg(s);
+    JoinProbeArgs p;
+    std::memset(&p, 0, sizeof(p));
+    if (!ProbeKeyArgs(J, batch, stg, p)) return false;
+    p.jkey = J.probe_jk;
+    p.jt = t->dev();
+    p.nrows = n;
+    if (!pairs->state || pairs->state->magic != kPairMagic) {
+        pairs->state = new PairState();
+        pairs->state->s = s;
+    }
+    PairState* ps = pairs->state;
+    ps->arena = a;
+    unsigned long long* dn = static_cast<unsigned long long*>(DevAlloc(8, s));
+    int64_t want = std::max<int64_t>(n, 1024);
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        if (ps->cap < want) {
+            DevFree(ps->dev, s);
+            ps->cap = want;
+            ps->dev = static_cast<int64_t*>(DevAlloc(size_t(ps->cap) * 16, s));
+            if (!ps->dev) return false;
+        }
+        cudaMemsetAsync(dn, 0, 8, s);
+        p.pairs = ps->dev;
+        p.pair_cap = ps->cap;
+        p.npairs = dn;
+        JoinProbePairs(p, s);
+        unsigned long long cnt = 0;
+        cudaMemcpyAsync(&cnt, dn, 8, cudaMemcpyDeviceToHost, s);
+        if (!CudaOk(cudaStreamSynchronize(s), "row join probe")) return false;
+        pairs->count = int64_t(cnt);
+        pairs->capacity = ps->cap;
+        if (pairs->count <= ps->cap) break;
+        want = pairs->count;   // too small: size it to the count and probe again
+    }
+    DevFree(dn, s);
+    return true;
+}
+
+}  // namespace
+
+}  // namespace qdb
+
+using namespace qdb;
+
+extern "C" {
+
+qdb_gpu_program* qdb_gpu_compile_row_join(const qdb_row_join_spec* spec, char* err, size_t err_len) {
+    try {
+        if (spec->join_type != QDB_JOIN_INNER) throw LowerError("only inner row joins are served");
+        auto* p = new qdb_gpu_program();
+        p->kind = PK_JOIN;
+        p->flags = spec->flags;
+        JoinProgram& J = p->join;
+        J.build_is_left = spec->build_is_left;
+        J.build_columns.assign(spec->build_columns, spec->build_columns + spec->n_build_columns);
+        J.probe_columns.assign(spec->probe_columns, spec->probe_columns + spec->n_probe_columns);
+        J.build_keys.assign(spec->build_keys, spec->build_keys + spec->n_keys);
+        J.probe_keys.assign(spec->probe_keys, spec->probe_keys + spec->n_keys);
+        J.payload.assign(spec->build_payload, spec->build_payload + spec->n_payload);
+        J.out_side.assign(spec->out_side, spec->out_side + spec->n_out);
+        J.out_column.assign(spec->out_column, spec->out_column + spec->n_out);
+        for (int c : J.build_keys) {
+            if (c < 0 || c >= spec->n_build_columns) throw LowerError("build key column out of range");
+        }
+        for (int c : J.probe_keys) {
+            if (c < 0 || c >= spec->n_probe_columns) throw LowerError("probe key column out of range");
+        }
+        for (int c : J.payload) {
+            if (c < 0 || c >= spec->n_build_columns) throw LowerError("payload column out of range");
+        }
+        for (size_t k = 0; k < J.out_side.size(); ++k) {
+            const int lim = J.out_side[k] == 0 ? spec->n_probe_columns : spec->n_payload;
+            if (J.out_column[k] < 0 || J.out_column[k] >= lim) throw LowerError("output column out of range");
+        }
+        J.build_jk = MakeKeyPlan(J.build_columns, J.build_keys, J.probe_columns, J.probe_keys);
+        J.probe_jk = J.build_jk;
+        // The build predicate program also maps every key and payload column
+        // so that Append can gather them.
+        std::vector<qdb_expr> nodes(spec->build_nodes, spec->build_nodes + spec->n_build_nodes);
+        int predicate = spec->build_filter;
+        if (predicate < 0) {
+            // A constant-true predicate: 1 = 1.
+            qdb_expr one;
+            std::memset(&one, 0, sizeof(one));
+            one.op = QDB_EXPR_CONST;
+            one.type = QDB_TYPE_I64;
+            one.imm_lo = 1;
+            nodes.push_back(one);
+            qdb_expr eq;
+            std::memset(&eq, 0, sizeof(eq));
+            eq.op = QDB_EXPR_EQ;
+            eq.type = QDB_TYPE_BOOL;
+            eq.args[0] = int(nodes.size()) - 1;
+            eq.args[1] = int(nodes.size()) - 1;
+            nodes.push_back(eq);
+            predicate = int(nodes.size()) - 1;
+        }
+        J.build_filter = LowerFilter(spec->n_build_columns, spec->build_columns, int(nodes.size()), nodes.data(),
+                                     predicate);
+        J.has_build_filter = spec->build_filter >= 0;
+        // Map key and payload columns into the filter plan's slots.
+        {
+            std::vector<int> need(J.build_keys);
+            need.insert(need.end(), J.payload.begin(), J.payload.end());
+            for (int c : need) {
+                if (J.build_filter.cols.slot_of[c] >= 0) continue;
+                const int slot = int(J.build_filter.cols.input_of.size());
+                if (slot >= kMaxCols) throw LowerError("too many build columns");
+                J.build_filter.cols.slot_of[c] = slot;
+                J.build_filter.cols.input_of.push_back(c);
+                ColDesc& cd = J.build_filter.plan.cols[slot];
+                std::memset(&cd, 0, sizeof(cd));
+                const TypeInfo ti = InfoOf(J.build_columns[c].type);
+                cd.width = ti.width;
+                cd.kind = ti.load;
+                cd.nullable = J.build_columns[c].nullable ? 1 : 0;
+                cd.scale = J.build_columns[c].type == QDB_TYPE_DECIMAL64 || J.build_columns[c].type == QDB_TYPE_DECIMAL128
+                               ? J.build_columns[c].scale : 0;
+                J.build_filter.plan.ncols = slot + 1;
+            }
+        }
+        return p;
+    } catch (const std::exception& e) {
+        if (err && err_len) std::snprintf(err, err_len, "%s", e.what());
+        t_error = e.what();
+        return nullptr;
+    }
+}
+
+qdb_gpu_program* qdb_gpu_compile_join_aggregate(const qdb_row_join_spec* join, const qdb_aggregate_spec* agg,
+                                                char* err, size_t err_len) {
+    qdb_gpu_program* p = qdb_gpu_compile_row_join(join, err, err_len);
+    if (!p) return nullptr;
+    try {
+        if (agg->n_columns != join->n_probe_columns + join->n_payload) {
+            throw LowerError("aggregate input must be the probe columns followed by the payload columns");
+        }
+        p->kind = PK_JOIN_AGG;
+        p->flags = agg->flags;
+        p->expected_groups = agg->expected_groups;
+        p->columns.assign(agg->columns, agg->columns + agg->n_columns);
+        std::vector<int> first(join->probe_keys, join->probe_keys + join->n_keys);
+        p->agg = LowerAggregate(*agg, join->n_probe_columns, first);
+        p->agg.plan.key_words = std::max(1, p->agg.plan.key_words);
+        p->join.agg_jk = p->join.probe_jk;
+        for (int j = 0; j < join->n_keys; ++j) p->join.agg_jk.col[j] = uint8_t(p->agg.cols.slot_of[join->probe_keys[j]]);
+        return p;
+    } catch (const std::exception& e) {
+        if (err && err_len) std::snprintf(err, err_len, "%s", e.what());
+        t_error = e.what();
+        delete p;
+        return nullptr;
+    }
+}
+
+bool qdb_gpu_jr_dispatch(const qdb_gpu_program* prog, void* arena, void* table, void* scratch, void* pairs,
+                         qdb_rowset* batch, int64_t op) {
+    (void)scratch;
+    t_error.clear();
+    if (!prog || (prog->kind != PK_JOIN && prog->kind != PK_JOIN_AGG) || !arena) {
+        SetErr("jr_dispatch: not a row join program");
+        return false;
+    }
+    const JoinProgram& J = prog->join;
+    switch (op) {
+        case QDB_JR_OP_INIT: {
+            if (ArenaOf(arena)) DestroyArena(ArenaOf(arena));
+            auto* a = new ArenaState();
+            a->s = CurStream();
+            for (int c : J.build_keys) {
+                ArenaCol col;
+                col.type = J.build_columns[c].type;
+                col.width = Width(col.type);
+                a->keys.push_back(col);
+            }
+            for (int c : J.payload) {
+                ArenaCol col;
+                col.type = J.build_columns[c].nullable ? -J.build_columns[c].type : J.build_columns[c].type;
+                col.width = Width(J.build_columns[c].type);
+                a->payload.push_back(col);
+            }
+            *static_cast<ArenaState**>(arena) = a;
+            static_cast<int64_t*>(arena)[5] = 0;
+            return GrowArena(a, 1024);
+        }
+        case QDB_JR_OP_APPEND: {
+            ArenaState* a = ArenaOf(arena);
+            if (!a || !batch) {
+                SetErr("jr_dispatch(Append) before Init");
+                return false;
+            }
+            if (!Append(prog, a, batch)) return false;
+            static_cast<int64_t*>(arena)[5] = a->rows;
+            return true;
+        }
+        case QDB_JR_OP_BUILD: {
+            ArenaState* a = ArenaOf(arena);
+            if (!a || !table) {
+                SetErr("jr_dispatch(Build) before Init");
+                return false;
+            }
+            return Build(prog, a, table);
+        }
+        case QDB_JR_OP_PROBE: {
+            ArenaState* a = ArenaOf(arena);
+            TableState* t = table ? TableOf(table) : nullptr;
+            if (!a || !t || !pairs || !batch) {
+                SetErr("jr_dispatch(Probe) before Build");
+                return false;
+            }
+            return Probe(prog, a, t, static_cast<PairBuf*>(pairs), batch);
+        }
+        default:
+            SetErr("jr_dispatch: op %lld is not served", (long long)op);
+            return false;
+    }
+}
+
+int64_t qdb_gpu_jr_materialize(const qdb_gpu_program* prog, void* pairs_v, qdb_rowset* stream, int64_t start,
+                               int64_t limit, qdb_rowset* out) {
+    t_error.clear();
+    if (!prog || !pairs_v || !out || (prog->kind != PK_JOIN && prog->kind != PK_JOIN_AGG)) {
+        SetErr("jr_materialize: bad arguments");
+        return -1;
+    }
+    auto* pairs = static_cast<PairBuf*>(pairs_v);
+    const JoinProgram& J = prog->join;
+    const int64_t n = std::max<int64_t>(0, std::min(limit, pairs->count - start));
+    if (n == 0) return 0;
+    cudaStream_t s = CurStream();
+    PairState* ps = pairs->state;
+    if (!ps || ps->magic != kPairMagic || !ps->arena || !stream) {
+        SetErr("jr_materialize: the pair buffer holds no probe result");
+        return -1;
+    }
+    ArenaState* a = ps->arena;
+    Staging stg(s);
+    std::vector<int> types;
+    for (size_t k = 0; k < J.out_side.size(); ++k) {
+        types.push_back(J.out_side[k] == 0 ? J.probe_columns[J.out_column[k]].type
+                                           : J.build_columns[J.payload[J.out_column[k]]].type);
+    }
+    std::vector<AggOutputCol> cols;
+    if (!AllocOutputCols(types, n, true, cols)) {
+        SetErr("jr_materialize: allocation failed");
+        return -1;
+    }
+    const int64_t* base = ps->dev + 2 * start;
+    for (size_t k = 0; k < J.out_side.size(); ++k) {
+        const int w = Width(types[k]);
+        if (J.out_side[k] == 0) {
+            const qdb_column& c = stream->Columns[J.out_column[k]];
+            const char* d = static_cast<const char*>(stg.Device(c.Data, size_t(stream->RowCount) * w));
+            GatherColumn(d, w, base, 2, n, cols[k].data, s);
+            const uint8_t* m = c.Mask ? static_cast<const uint8_t*>(stg.Device(
+                                            c.Mask, size_t((c.MaskBitOffset + stream->RowCount + 7) / 8)))
+                                      : nullptr;
+            GatherValidity(m, c.MaskBitOffset, base, 2, n, cols[k].valid, 0, s);
+        } else {
+            const ArenaCol& ac = a->payload[J.out_column[k]];
+            GatherColumn(ac.data, w, base + 1, 2, n, cols[k].data, s);
+            GatherValidity(reinterpret_cast<const uint8_t*>(ac.valid), 0, base + 1, 2, n, cols[k].valid, 0, s);
+        }
+    }
+    if (!EmitRowset(cols, types, n, (prog->flags & QDB_OUT_DEVICE) != 0, s, out)) return -1;
+    return n;
+}
+
+int64_t qdb_gpu_join_aggregate_probe(const qdb_gpu_program* prog, void* arena, void* table, void* ht,
+                                     qdb_rowset* batch) {
+    t_error.clear();
+    if (!prog || prog->kind != PK_JOIN_AGG || !arena || !table || !ht || !batch) {
+        SetErr("join_aggregate_probe: bad arguments");
+        return -1;
+    }
+    ArenaState* a = ArenaOf(arena);
+    TableState* t = TableOf(table);
+    AggTableState* st = AggStateOf(ht);
+    if (!a || !t || !st) {
+        SetErr("join_aggregate_probe: arena, table and aggregate state must be initialised and built");
+        return -1;
+    }
+    const JoinProgram& J = prog->join;
+    AggPlan plan = prog->agg.plan;
+    Staging stg(CurStream());
+    if (!ResolveColumns(plan, prog->agg.cols, prog->columns.data(), batch, stg)) return -1;
+    const int np = int(J.probe_columns.size());
+    for (int slot = 0; slot < plan.ncols; ++slot) {
+        ColDesc& cd = plan.cols[slot];
+        if (!cd.build) continue;
+        const ArenaCol& ac = a->payload[prog->agg.cols.input_of[slot] - np];
+        cd.data = ac.data;
+        cd.mask = reinterpret_cast<const uint8_t*>(ac.valid);
+        cd.mask_off = 0;
+        cd.bit_off = 0;
+    }
+    const int64_t before = AggStateMatched(st);
+    const JTableDev jt = t->dev();
+    if (!AggRun(st, plan, batch->RowCount, &J.agg_jk, &jt)) return -1;
+    AggMirrorHeader(ht, st, prog->agg.plan);
+    return AggStateMatched(st) - before;
+}
+
+}  // extern "C"

@@ -1,0 +1,180 @@
+// kernels.h — host-side launchers of the device kernels (implemented in the
+// .cu files), called by the runtime that serves the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "plan.h"
+
+namespace qdb {
+
+constexpr uint64_t kEmptyKey = ~0ull;
+
+// Device-resident counters of one table state.
+struct AggCounters {
+    unsigned long long new_groups;
+    unsigned long long deferred;
+    unsigned long long spilled;
+    unsigned long long matched;     // fused join: joined rows folded in
+    int error;
+    int pad;
+};
+
+// Global open-addressing group table in HBM: capacity slots plus one slot for
+// the one-word key that equals kEmptyKey.  Slot = [status?][key][states].
+struct GTableDev {
+    uint64_t* slots = nullptr;
+    int64_t capacity = 0;          // power of two
+    int32_t slot_words = 0;
+    int32_t key_off = 0;           // 1 when the slot leads with a status word
+    int32_t state_off = 0;
+    int32_t wide = 0;              // multi-word keys claimed by status word
+};
+
+// Packed equi-join key over up to four columns (one word).
+struct JoinKeyPlan {
+    int32_t n = 0;
+    int32_t full64 = 0;            // the packed key may equal kEmptyKey
+    uint8_t col[4] = {};           // plan column slots (probe) / input columns (build)
+    uint8_t bits[4] = {};
+    uint8_t shift[4] = {};
+    uint8_t is_float[4] = {};
+};
+
+// Built join table: 2 words per slot (packed key, build row), EMPTY key =
+// kEmptyKey; rows whose key equals kEmptyKey are listed separately.
+struct JTableDev {
+    const uint64_t* entries = nullptr;
+    uint64_t mask = 0;
+    const int64_t* special_rows = nullptr;
+    int64_t nspecial = 0;
+};
+
+struct AggUpdateArgs {
+    const AggPlan* plan = nullptr;
+    int64_t nrows = 0;
+    const int64_t* index = nullptr;   // index mode: (row, build row) pairs
+    int64_t nindex = 0;
+    GTableDev table;
+    AggCounters* counters = nullptr;
+    int64_t* deferred = nullptr;       // (row, build row) pairs
+    int64_t deferred_cap = 0;
+    uint64_t* spill = nullptr;
+    int64_t spill_cap = 0;
+    int32_t smem_slots = 0;            // 0 disables the shared-memory tier
+    bool join = false;
+    JoinKeyPlan jkey;
+    JTableDev jt;
+};
+
+struct AggOutputCol {
+    int32_t type;
+    char* data;           // device, rows * width
+    int32_t* offsets;     // CHAR1 outputs: rows + 1 i32 string offsets
+    uint32_t* valid;      // validity bitmap (words) or nullptr
+};
+
+// Launch geometry chosen per device.
+int DeviceSMs();
+size_t MaxSmemOptin();
+
+void AggInitTable(const AggPlan& p, const GTableDev& t, cudaStream_t s);
+// Returns the shared-memory slots actually used by the launch.
+void AggUpdate(const AggUpdateArgs& a, cudaStream_t s);
+void AggRehash(const AggPlan& p, const GTableDev& from, const GTableDev& to, AggCounters* c,
+               cudaStream_t s);
+void AggMergeSpill(const AggPlan& p, const uint64_t* spill, int64_t n, const GTableDev& t,
+                   AggCounters* c, cudaStream_t s);
+// Writes every group of `t` into `cols`; `scratch` holds >= AggFinalizeScratch
+// bytes.  `out` describes the output projection (see lower.h OutputPlan).
+struct OutputPlan;
+size_t AggFinalizeScratch(const GTableDev& t);
+void AggFinalize(const AggPlan& p, const OutputPlan& out, const GTableDev& t, AggOutputCol* cols,
+                 int ncols, int64_t groups, void* scratch, int* err, cudaStream_t s);
+
+// ---- join ----
+struct JoinBuildArgs {
+    // Build columns (device): key columns per JoinKeyPlan.col (input index).
+    const char* key_data[4];
+    const uint8_t* key_mask[4];
+    int64_t key_mask_off[4];
+    uint8_t key_width[4];
+    uint8_t key_signed[4];
+    JoinKeyPlan jkey;
+    int64_t nrows;
+    uint64_t* entries;      // capacity * 2 words
+    uint64_t mask;
+    int64_t* special_rows;
+    unsigned long long* nspecial;
+    int64_t row_base;       // arena row of build row 0
+};
+void JoinInitTable(uint64_t* entries, int64_t capacity, cudaStream_t s);
+void JoinBuild(const JoinBuildArgs& a, cudaStream_t s);
+
+struct JoinProbeArgs {
+    const char* key_data[4];
+    const uint8_t* key_mask[4];
+    int64_t key_mask_off[4];
+    uint8_t key_width[4];
+    uint8_t key_signed[4];
+    const uint8_t* selection;
+    JoinKeyPlan jkey;
+    JTableDev jt;
+    int64_t nrows;
+    int64_t* pairs;          // (probe row, build row)
+    int64_t pair_cap;
+    unsigned long long* npairs;
+    int* err;
+};
+void JoinProbePairs(const JoinProbeArgs& a, cudaStream_t s);
+
+// Gathers rows: out[i] = src[idx[i]] for `width`-byte values (idx < 0 -> 0).
+void GatherColumn(const char* src, int width, const int64_t* idx, int idx_stride, int64_t n, char* out,
+                  cudaStream_t s);
+// Sets bit (out_bit_off + i) of out_words (pre-zeroed) for every valid
+// gathered row i.
+void GatherValidity(const uint8_t* mask, int64_t mask_off, const int64_t* idx, int idx_stride, int64_t n,
+                    uint32_t* out_words, int64_t out_bit_off, cudaStream_t s);
+
+// In-place exclusive scan of n counters (one block; n up to a few million).
+void ExclusiveScanU64(unsigned long long* counts, int64_t n, cudaStream_t s);
+
+// ---- filter / project / hash over one row set ----
+struct ExprArgs {
+    const AggPlan* plan = nullptr;   // filter and value sections, columns resolved
+    int64_t nrows = 0;
+    // Filter: writes out_sel[r] (selected input rows that pass); also rows
+    // whose `null_reject` slots are NULL fail (join keys).
+    uint8_t* out_sel = nullptr;
+    int32_t n_null_reject = 0;
+    uint8_t null_reject[4] = {};
+    // Project: output k = value (src, idx) stored with type out_type[k].
+    int32_t nout = 0;
+    uint8_t out_src[kMaxCols] = {};
+    uint8_t out_idx[kMaxCols] = {};
+    int32_t out_type[kMaxCols] = {};
+    void* out_ptr[kMaxCols] = {};
+    // Hash: struct rh_hash over key slots with their qdb types.
+    int32_t nhash = 0;
+    uint8_t hash_slot[kMaxKeyParts] = {};
+    int32_t hash_type[kMaxKeyParts] = {};
+    uint64_t* hashes = nullptr;
+    int* err = nullptr;
+};
+void FilterRows(const ExprArgs& a, cudaStream_t s);
+void ProjectRows(const ExprArgs& a, cudaStream_t s);
+void HashRows(const ExprArgs& a, cudaStream_t s);
+// Indices (ascending) of the rows with flags[r] != 0; returns nothing on the
+// host: the count lands in *d_count (device).  `scratch` >= CompactScratch(n).
+size_t CompactScratch(int64_t n);
+void CompactFlags(const uint8_t* flags, int64_t n, int64_t* out_idx, unsigned long long* d_count, void* scratch,
+                  cudaStream_t s);
+
+// Kernel timing hooks (runtime.cpp).
+void ProfileBegin(cudaStream_t s, const char* name, int64_t units);
+void ProfileEnd(cudaStream_t s);
+void CountLaunch(int n = 1);
+
+}  // namespace qdb

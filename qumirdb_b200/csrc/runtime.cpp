@@ -1,0 +1,890 @@
+// runtime.cpp — the C ABI of include/qdb_gpu.h: programs, per-task device
+// states behind the engine's caller-owned state buffers, staging of row sets
+// into device memory, the table growth / replay loop, kernel timing.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/qdb_gpu.h"
+#include "kernels.h"
+#include "lower.h"
+#include "runtime.h"
+
+namespace qdb {
+
+// ---------------------------------------------------------------------------
+// Errors, streams, memory.
+// ---------------------------------------------------------------------------
+thread_local std::string t_error;
+
+void SetErr(const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    t_error = buf;
+}
+
+bool CudaOk(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    SetErr("%s: %s", what, cudaGetErrorString(e));
+    return false;
+}
+
+namespace {
+
+std::mutex g_mu;
+cudaStream_t g_lib_stream = nullptr;
+thread_local cudaStream_t t_stream = nullptr;
+thread_local bool t_stream_set = false;
+std::atomic<int64_t> g_launches{0};
+
+// Kernel timing.
+struct ProfRec {
+    std::string name;
+    int64_t units;
+    cudaEvent_t a;
+    cudaEvent_t b;
+};
+std::mutex g_prof_mu;
+std::vector<ProfRec> g_prof;
+std::atomic<bool> g_prof_on{false};
+thread_local int64_t t_prof_open = -1;
+
+}  // namespace
+
+cudaStream_t CurStream() {
+    if (t_stream_set) return t_stream;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_lib_stream) {
+        cudaStreamCreateWithFlags(&g_lib_stream, cudaStreamNonBlocking);
+        cudaMemPool_t pool;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t threshold = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+        }
+    }
+    return g_lib_stream;
+}
+
+void ProfileBegin(cudaStream_t s, const char* name, int64_t units) {
+    if (!g_prof_on.load(std::memory_order_relaxed)) return;
+    ProfRec r;
+    r.name = name;
+    r.units = units;
+    cudaEventCreate(&r.a);
+    cudaEventCreate(&r.b);
+    cudaEventRecord(r.a, s);
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_prof.push_back(r);
+    t_prof_open = int64_t(g_prof.size()) - 1;
+}
+
+void ProfileEnd(cudaStream_t s) {
+    if (t_prof_open < 0) return;
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    if (t_prof_open < int64_t(g_prof.size())) cudaEventRecord(g_prof[t_prof_open].b, s);
+    t_prof_open = -1;
+}
+
+void CountLaunch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void* DevAlloc(size_t bytes, cudaStream_t s) {
+    void* p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (cudaMallocAsync(&p, bytes, s) != cudaSuccess) {
+        cudaGetLastError();
+        SetErr("device allocation of %zu bytes failed", bytes);
+        return nullptr;
+    }
+    return p;
+}
+
+void DevFree(void* p, cudaStream_t s) {
+    if (p) cudaFreeAsync(p, s);
+}
+
+bool IsDevicePtr(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Device copy of `bytes` at `p` (host or device); adds owned buffers to st.
+const void* Staging::Device(const void* p, size_t bytes) {
+    if (!p) return nullptr;
+    if (IsDevicePtr(p)) return p;
+    void* d = DevAlloc(bytes, s);
+    if (!d) return nullptr;
+    cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, s);
+    owned.push_back(d);
+    return d;
+}
+
+Staging::~Staging() {
+    for (void* p : owned) DevFree(p, s);
+}
+
+// Resolves the plan's probe/scan column slots against a row set.
+bool ResolveColumns(AggPlan& P, const ColumnMap& cm, const qdb_column_type* types, const qdb_rowset* rs,
+                    Staging& st) {
+    const int64_t n = rs->RowCount;
+    for (int slot = 0; slot < P.ncols; ++slot) {
+        ColDesc& cd = P.cols[slot];
+        if (cd.build) continue;
+        const int input = cm.input_of[slot];
+        if (input >= rs->ColumnCount) {
+            SetErr("row set has %lld columns, the program reads column %d", (long long)rs->ColumnCount, input);
+            return false;
+        }
+        const qdb_column& c = rs->Columns[input];
+        const int t = types[input].type;
+        if (t == QDB_TYPE_BOOL) {
+            const size_t bytes = size_t((c.DataBitOffset + n + 7) / 8);
+            cd.data = static_cast<const char*>(st.Device(c.Data, bytes));
+            cd.bit_off = c.DataBitOffset;
+        } else {
+            cd.data = static_cast<const char*>(st.Device(c.Data, size_t(n) * cd.width));
+        }
+        if (n > 0 && !cd.data) {
+            if (t_error.empty()) SetErr("column %d has no data", input);
+            return false;
+        }
+        cd.mask = nullptr;
+        cd.mask_off = 0;
+        if (c.Mask) {
+            cd.mask = static_cast<const uint8_t*>(st.Device(c.Mask, size_t((c.MaskBitOffset + n + 7) / 8)));
+            cd.mask_off = c.MaskBitOffset;
+        }
+    }
+    P.selection = rs->Selection ? static_cast<const uint8_t*>(st.Device(rs->Selection, size_t(n))) : nullptr;
+    P.has_selection = P.selection != nullptr;
+    return true;
+}
+
+// Offsets every scan column of a resolved plan by `begin` rows.
+AggPlan OffsetPlan(const AggPlan& P, int64_t begin) {
+    AggPlan q = P;
+    for (int slot = 0; slot < q.ncols; ++slot) {
+        ColDesc& cd = q.cols[slot];
+        if (cd.build) continue;
+        if (cd.kind == LK_BOOLBIT) cd.bit_off += begin;
+        else cd.data += begin * cd.width;
+        if (cd.mask) cd.mask_off += begin;
+    }
+    if (q.selection) q.selection += begin;
+    return q;
+}
+
+int64_t NextPow2(int64_t v) {
+    int64_t p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// Aggregate table state.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kAggMagic = 0x51444741;   // 'QDGA'
+constexpr int64_t kChunkRows = int64_t(64) << 20;
+
+struct AggTableState {
+    uint32_t magic = kAggMagic;
+    cudaStream_t s = nullptr;
+    GTableDev t;
+    AggCounters* dc = nullptr;      // device counters
+    AggCounters* hc = nullptr;      // pinned host mirror
+    int64_t groups = 0;
+    int64_t expected = 0;
+    int64_t* deferred[2] = {nullptr, nullptr};
+    int64_t deferred_cap = 0;
+    uint64_t* spill = nullptr;
+    int64_t spill_cap = 0;
+    int smem_slots = 2048;
+    int64_t matched = 0;
+};
+
+namespace {
+
+int SlotWords(const AggPlan& p, bool wide) {
+    int w = (wide ? 1 + p.key_words : 1) + p.state_words;
+    if (w <= 16) {
+        int q = 1;
+        while (q < w) q <<= 1;
+        return q;
+    }
+    return (w + 1) & ~1;
+}
+
+bool AllocTable(const AggPlan& p, int64_t capacity, cudaStream_t s, GTableDev& t) {
+    t.wide = p.key_words > 1 ? 1 : 0;
+    t.capacity = capacity;
+    t.slot_words = SlotWords(p, t.wide);
+    t.key_off = t.wide ? 1 : 0;
+    t.state_off = t.wide ? 1 + p.key_words : 1;
+    t.slots = static_cast<uint64_t*>(DevAlloc(size_t(capacity + 1) * t.slot_words * 8, s));
+    if (!t.slots) return false;
+    AggInitTable(p, t, s);
+    return true;
+}
+
+AggTableState* StateOf(void* ht) {
+    AggTableState* st = *static_cast<AggTableState**>(ht);
+    if (!st || st->magic != kAggMagic) return nullptr;
+    return st;
+}
+
+void MirrorHeader(void* ht, const AggTableState* st, const AggPlan& p) {
+    int64_t* w = static_cast<int64_t*>(ht);
+    w[8] = st ? st->t.capacity : 0;     // Capacity
+    w[9] = st ? st->groups : 0;         // Size
+    w[10] = p.naggs;                    // NumAggs
+    w[11] = p.nkeyparts;                // NumKeys
+    w[12] = p.key_words * 8;            // KeySize
+}
+
+bool ReadCounters(AggTableState* st) {
+    cudaMemcpyAsync(st->hc, st->dc, sizeof(AggCounters), cudaMemcpyDeviceToHost, st->s);
+    if (!CudaOk(cudaStreamSynchronize(st->s), "aggregate update")) return false;
+    if (st->hc->error) {
+        SetErr("aggregate kernel reported device error %d", st->hc->error);
+        return false;
+    }
+    return true;
+}
+
+void ResetCounters(AggTableState* st) { cudaMemsetAsync(st->dc, 0, sizeof(AggCounters), st->s); }
+
+bool Grow(AggTableState* st, const AggPlan& p, int64_t min_groups) {
+    int64_t cap = st->t.capacity;
+    while (cap < 2 * min_groups) cap <<= 1;
+    if (cap == st->t.capacity) cap <<= 1;
+    GTableDev nt;
+    if (!AllocTable(p, cap, st->s, nt)) return false;
+    AggRehash(p, st->t, nt, st->dc, st->s);
+    DevFree(st->t.slots, st->s);
+    st->t = nt;
+    return true;
+}
+
+bool EnsureBuffers(AggTableState* st, const AggPlan& p, int64_t rows) {
+    const int64_t need = std::min<int64_t>(std::max<int64_t>(rows, 1), kChunkRows);
+    if (st->deferred_cap < need) {
+        for (int j = 0; j < 2; ++j) {
+            DevFree(st->deferred[j], st->s);
+            st->deferred[j] = static_cast<int64_t*>(DevAlloc(size_t(need) * 16, st->s));
+            if (!st->deferred[j]) return false;
+        }
+        st->deferred_cap = need;
+    }
+    const int64_t spill = int64_t(DeviceSMs()) * st->smem_slots;
+    if (st->spill_cap < spill) {
+        DevFree(st->spill, st->s);
+        st->spill = static_cast<uint64_t*>(DevAlloc(size_t(spill) * (1 + p.state_words) * 8, st->s));
+        if (!st->spill) return false;
+        st->spill_cap = spill;
+    }
+    return true;
+}
+
+}  // namespace
+
+AggTableState* AggStateCreate(const AggPlan& p, int64_t capacity_hint, int64_t expected, cudaStream_t s) {
+    auto* st = new AggTableState();
+    st->s = s;
+    st->expected = expected;
+    int64_t cap = std::max<int64_t>(1024, NextPow2(std::max<int64_t>(capacity_hint, 1)));
+    if (expected > 0) cap = std::max(cap, NextPow2(expected * 2));
+    if (cudaMallocHost(&st->hc, sizeof(AggCounters)) != cudaSuccess) {
+        delete st;
+        SetErr("pinned allocation failed");
+        return nullptr;
+    }
+    st->dc = static_cast<AggCounters*>(DevAlloc(sizeof(AggCounters), s));
+    if (!st->dc || !AllocTable(p, cap, s, st->t)) {
+        cudaFreeHost(st->hc);
+        delete st;
+        return nullptr;
+    }
+    ResetCounters(st);
+    // A keyless aggregate has its group before any row arrives.
+    if (p.nkeyparts == 0) {
+        uint64_t zero = 0;
+        const int64_t slot = int64_t(Fmix64(0) & uint64_t(cap - 1));
+        cudaMemcpyAsync(st->t.slots + slot * st->t.slot_words + st->t.key_off, &zero, 8, cudaMemcpyHostToDevice, s);
+        cudaStreamSynchronize(s);
+        st->groups = 1;
+    }
+    return st;
+}
+
+int64_t AggStateGroups(const AggTableState* st) { return st ? st->groups : 0; }
+int64_t AggStateMatched(const AggTableState* st) { return st ? st->matched : 0; }
+AggTableState* AggStateOf(void* ht) { return StateOf(ht); }
+void AggMirrorHeader(void* ht, const AggTableState* st, const AggPlan& p) { MirrorHeader(ht, st, p); }
+
+void AggStateDestroy(AggTableState* st) {
+    if (!st) return;
+    DevFree(st->t.slots, st->s);
+    DevFree(st->dc, st->s);
+    DevFree(st->deferred[0], st->s);
+    DevFree(st->deferred[1], st->s);
+    DevFree(st->spill, st->s);
+    cudaStreamSynchronize(st->s);
+    cudaFreeHost(st->hc);
+    st->magic = 0;
+    delete st;
+}
+
+// Runs the fused kernel over `rows` rows of a resolved plan, then replays
+// deferred rows and spilled entries after growing the table.
+bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyPlan* jk, const JTableDev* jt) {
+    if (!EnsureBuffers(st, plan, rows)) return false;
+    for (int64_t begin = 0; begin < rows || (rows == 0 && begin == 0); begin += kChunkRows) {
+        const int64_t n = std::min<int64_t>(kChunkRows, rows - begin);
+        if (n <= 0) break;
+        const AggPlan chunk = OffsetPlan(plan, begin);
+        AggUpdateArgs a;
+        a.plan = &chunk;
+        a.nrows = n;
+        a.table = st->t;
+        a.counters = st->dc;
+        a.deferred = st->deferred[0];
+        a.deferred_cap = st->deferred_cap;
+        a.spill = st->spill;
+        a.spill_cap = st->spill_cap;
+        a.smem_slots = st->smem_slots;
+        if (jk) {
+            a.join = true;
+            a.jkey = *jk;
+            a.jt = *jt;
+        }
+        ResetCounters(st);
+        AggUpdate(a, st->s);
+        if (!ReadCounters(st)) return false;
+        st->groups += int64_t(st->hc->new_groups);
+        st->matched += int64_t(st->hc->matched);
+        int64_t ndef = int64_t(st->hc->deferred);
+        int64_t nspill = int64_t(st->hc->spilled);
+        int cur = 0;
+        for (int round = 0; (ndef > 0 || nspill > 0); ++round) {
+            if (round > 16) {
+                SetErr("aggregate replay did not converge");
+                return false;
+            }
+            if (!Grow(st, plan, st->groups + ndef + nspill)) return false;
+            ResetCounters(st);
+            AggMergeSpill(plan, st->spill, nspill, st->t, st->dc, st->s);
+            // Replay deferred rows into the grown table; new deferrals go to the other buffer.
+            AggUpdateArgs r = a;
+            r.table = st->t;
+            r.index = st->deferred[cur];
+            r.nindex = ndef;
+            r.deferred = st->deferred[cur ^ 1];
+            r.join = jk != nullptr;
+            AggUpdate(r, st->s);
+            cur ^= 1;
+            if (!ReadCounters(st)) return false;
+            st->groups += int64_t(st->hc->new_groups);
+            ndef = int64_t(st->hc->deferred);
+            nspill = int64_t(st->hc->spilled);
+        }
+        if (st->groups * 2 > st->t.capacity) {
+            if (!Grow(st, plan, st->groups)) return false;
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Output row sets.
+// ---------------------------------------------------------------------------
+struct OwnedRowset {
+    std::vector<void*> host;
+    std::vector<void*> dev;
+    std::vector<qdb_column> cols;
+};
+
+void DestroyOwned(qdb_rowset* rs) {
+    if (!rs || !rs->Private) return;
+    auto* o = static_cast<OwnedRowset*>(rs->Private);
+    for (void* p : o->host) std::free(p);
+    for (void* p : o->dev) cudaFree(p);
+    delete o;
+    rs->Private = nullptr;
+    rs->Columns = nullptr;
+}
+
+// Moves device output columns into `out` (copying to host unless on_device).
+bool EmitRowset(std::vector<AggOutputCol>& cols, const std::vector<int>& types, int64_t rows, bool on_device,
+                cudaStream_t s, qdb_rowset* out) {
+    auto* o = new OwnedRowset();
+    o->cols.resize(cols.size());
+    if (!CudaOk(cudaStreamSynchronize(s), "output")) {
+        delete o;
+        return false;
+    }
+    for (size_t k = 0; k < cols.size(); ++k) {
+        qdb_column& c = o->cols[k];
+        std::memset(&c, 0, sizeof(c));
+        const size_t w = size_t(StorageWidth(types[k]));
+        const size_t dbytes = std::max<size_t>(1, size_t(rows) * w);
+        const size_t mbytes = size_t((rows + 31) / 32) * 4;
+        if (on_device) {
+            c.Data = cols[k].data;
+            o->dev.push_back(cols[k].data);
+            if (cols[k].valid) {
+                c.Mask = reinterpret_cast<const uint8_t*>(cols[k].valid);
+                o->dev.push_back(cols[k].valid);
+            }
+            if (cols[k].offsets) {
+                c.Offsets = cols[k].offsets;
+                c.OffsetWidth = 4;
+                o->dev.push_back(cols[k].offsets);
+            }
+        } else {
+            void* h = std::malloc(dbytes);
+            cudaMemcpy(h, cols[k].data, size_t(rows) * w, cudaMemcpyDeviceToHost);
+            c.Data = static_cast<char*>(h);
+            o->host.push_back(h);
+            cudaFree(cols[k].data);
+            if (cols[k].valid) {
+                void* m = std::malloc(std::max<size_t>(4, mbytes));
+                cudaMemcpy(m, cols[k].valid, mbytes, cudaMemcpyDeviceToHost);
+                c.Mask = static_cast<const uint8_t*>(m);
+                o->host.push_back(m);
+                cudaFree(cols[k].valid);
+            }
+            if (cols[k].offsets) {
+                void* off = std::malloc(size_t(rows + 1) * 4);
+                cudaMemcpy(off, cols[k].offsets, size_t(rows + 1) * 4, cudaMemcpyDeviceToHost);
+                c.Offsets = off;
+                c.OffsetWidth = 4;
+                o->host.push_back(off);
+                cudaFree(cols[k].offsets);
+            }
+        }
+    }
+    std::memset(out, 0, sizeof(*out));
+    out->Columns = o->cols.data();
+    out->ColumnCount = int64_t(cols.size());
+    out->RowCount = rows;
+    out->Destroy = DestroyOwned;
+    out->Private = o;
+    out->RefCount = 1;
+    return true;
+}
+
+bool AllocOutputCols(const std::vector<int>& types, int64_t rows, bool with_valid, std::vector<AggOutputCol>& cols) {
+    cols.resize(types.size());
+    for (size_t k = 0; k < types.size(); ++k) {
+        AggOutputCol& c = cols[k];
+        std::memset(&c, 0, sizeof(c));
+        c.type = types[k];
+        const size_t w = size_t(StorageWidth(types[k]));
+        if (cudaMalloc(&c.data, std::max<size_t>(16, size_t(rows) * w)) != cudaSuccess) return false;
+        if (with_valid) {
+            const size_t mb = std::max<size_t>(4, size_t((rows + 31) / 32) * 4);
+            if (cudaMalloc(&c.valid, mb) != cudaSuccess) return false;
+            cudaMemset(c.valid, 0, mb);
+        }
+        if (types[k] == QDB_TYPE_CHAR1) {
+            if (cudaMalloc(&c.offsets, size_t(rows + 1) * 4) != cudaSuccess) return false;
+            cudaMemset(c.offsets, 0, 4);
+        }
+    }
+    return true;
+}
+
+int64_t AggFinish(AggTableState* st, const AggLowering& lw, uint32_t flags, qdb_rowset* out) {
+    const int64_t groups = st->groups;
+    std::vector<int> types;
+    for (int k = 0; k < lw.out.n; ++k) types.push_back(lw.out.out_type[k]);
+    std::vector<AggOutputCol> cols;
+    if (!AllocOutputCols(types, groups, true, cols)) {
+        SetErr("output allocation failed");
+        return -1;
+    }
+    void* scratch = DevAlloc(AggFinalizeScratch(st->t), st->s);
+    if (!scratch) return -1;
+    ResetCounters(st);
+    AggFinalize(lw.plan, lw.out, st->t, cols.data(), int(cols.size()), groups, scratch, &st->dc->error, st->s);
+    DevFree(scratch, st->s);
+    if (!ReadCounters(st)) return -1;
+    if (!EmitRowset(cols, types, groups, (flags & QDB_OUT_DEVICE) != 0, st->s, out)) return -1;
+    return groups;
+}
+
+}  // namespace qdb
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace qdb;
+
+namespace {
+
+void Fill(char* err, size_t len, const char* msg) {
+    if (err && len) std::snprintf(err, len, "%s", msg);
+    t_error = msg;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qdb_gpu_init(int device) {
+    if (!CudaOk(cudaSetDevice(device), "cudaSetDevice")) return -1;
+    if (!CudaOk(cudaFree(nullptr), "context")) return -1;
+    CurStream();
+    return 0;
+}
+
+const char* qdb_gpu_last_error(void) { return t_error.c_str(); }
+
+void qdb_gpu_set_stream(void* stream) {
+    t_stream = static_cast<cudaStream_t>(stream);
+    t_stream_set = stream != nullptr;
+}
+
+void* qdb_gpu_get_stream(void) { return CurStream(); }
+
+int qdb_gpu_synchronize(void) { return CudaOk(cudaStreamSynchronize(CurStream()), "synchronize") ? 0 : -1; }
+
+void* qdb_gpu_alloc(size_t bytes) {
+    void* p = nullptr;
+    if (!CudaOk(cudaMalloc(&p, std::max<size_t>(bytes, 16)), "cudaMalloc")) return nullptr;
+    return p;
+}
+
+void qdb_gpu_free(void* ptr) {
+    if (ptr) cudaFree(ptr);
+}
+
+void* qdb_gpu_host_alloc(size_t bytes) {
+    void* p = nullptr;
+    if (!CudaOk(cudaMallocHost(&p, std::max<size_t>(bytes, 16)), "cudaMallocHost")) return nullptr;
+    return p;
+}
+
+void qdb_gpu_host_free(void* ptr) {
+    if (ptr) cudaFreeHost(ptr);
+}
+
+int qdb_gpu_memcpy(void* dst, const void* src, size_t bytes) {
+    return CudaOk(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, CurStream()), "memcpy") ? 0 : -1;
+}
+
+int qdb_gpu_memset(void* dst, int value, size_t bytes) {
+    return CudaOk(cudaMemsetAsync(dst, value, bytes, CurStream()), "memset") ? 0 : -1;
+}
+
+void qdb_gpu_profile_enable(int on) { g_prof_on.store(on != 0); }
+
+int64_t qdb_gpu_profile_read(qdb_gpu_kernel_time* out, int64_t cap) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    int64_t n = 0;
+    for (auto& r : g_prof) {
+        cudaEventSynchronize(r.b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        if (out && n < cap) {
+            std::snprintf(out[n].name, sizeof(out[n].name), "%s", r.name.c_str());
+            out[n].ms = ms;
+            out[n].units = r.units;
+        }
+        ++n;
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    g_prof.clear();
+    return std::min(n, cap);
+}
+
+int64_t qdb_gpu_launch_count(int reset) {
+    return reset ? g_launches.exchange(0) : g_launches.load();
+}
+
+qdb_gpu_program* qdb_gpu_compile_aggregate(const qdb_aggregate_spec* spec, char* err, size_t err_len) {
+    try {
+        auto* p = new qdb_gpu_program();
+        p->kind = PK_AGG;
+        p->flags = spec->flags;
+        p->columns.assign(spec->columns, spec->columns + spec->n_columns);
+        p->agg = LowerAggregate(*spec);
+        p->agg.plan.key_words = std::max(1, p->agg.plan.key_words);
+        p->expected_groups = spec->expected_groups;
+        return p;
+    } catch (const std::exception& e) {
+        Fill(err, err_len, e.what());
+        return nullptr;
+    }
+}
+
+qdb_gpu_program* qdb_gpu_compile_filter(int32_t n_columns, const qdb_column_type* columns, int32_t n_nodes,
+                                        const qdb_expr* nodes, int32_t predicate, char* err, size_t err_len) {
+    try {
+        auto* p = new qdb_gpu_program();
+        p->kind = PK_FILTER;
+        p->columns.assign(columns, columns + n_columns);
+        p->expr = LowerFilter(n_columns, columns, n_nodes, nodes, predicate);
+        return p;
+    } catch (const std::exception& e) {
+        Fill(err, err_len, e.what());
+        return nullptr;
+    }
+}
+
+qdb_gpu_program* qdb_gpu_compile_project(int32_t n_columns, const qdb_column_type* columns, int32_t n_nodes,
+                                         const qdb_expr* nodes, int32_t n_exprs, const int32_t* exprs, char* err,
+                                         size_t err_len) {
+    try {
+        if (n_exprs > kMaxCols) throw LowerError("too many projections for one device plan");
+        auto* p = new qdb_gpu_program();
+        p->kind = PK_PROJECT;
+        p->columns.assign(columns, columns + n_columns);
+        p->expr = LowerProject(n_columns, columns, n_nodes, nodes, n_exprs, exprs);
+        return p;
+    } catch (const std::exception& e) {
+        Fill(err, err_len, e.what());
+        return nullptr;
+    }
+}
+
+qdb_gpu_program* qdb_gpu_compile_hash(int32_t n_columns, const qdb_column_type* columns, int32_t n_keys,
+                                      const int32_t* key_columns, char* err, size_t err_len) {
+    try {
+        if (n_keys < 1 || n_keys > kMaxKeyParts) throw LowerError("hash needs 1..6 key columns");
+        std::vector<qdb_expr> nodes(n_keys);
+        std::vector<int32_t> exprs(n_keys);
+        for (int j = 0; j < n_keys; ++j) {
+            if (key_columns[j] < 0 || key_columns[j] >= n_columns) throw LowerError("key column out of range");
+            const qdb_column_type& ct = columns[key_columns[j]];
+            if (ct.nullable) throw LowerError("nullable shuffle keys are not served");
+            if (ct.type == QDB_TYPE_BOOL) throw LowerError("boolean shuffle keys are not served");
+            std::memset(&nodes[j], 0, sizeof(qdb_expr));
+            nodes[j].op = QDB_EXPR_COLUMN;
+            nodes[j].type = ct.type;
+            nodes[j].scale = ct.scale;
+            nodes[j].column = key_columns[j];
+            exprs[j] = j;
+        }
+        auto* p = new qdb_gpu_program();
+        p->kind = PK_HASH;
+        p->columns.assign(columns, columns + n_columns);
+        p->expr = LowerProject(n_columns, columns, n_keys, nodes.data(), n_keys, exprs.data());
+        for (int j = 0; j < n_keys; ++j) {
+            p->expr.value_idx[j] = p->expr.cols.slot_of[key_columns[j]];
+            p->expr.out_types[j] = columns[key_columns[j]].type;
+        }
+        return p;
+    } catch (const std::exception& e) {
+        Fill(err, err_len, e.what());
+        return nullptr;
+    }
+}
+
+void qdb_gpu_program_destroy(qdb_gpu_program* program) { delete program; }
+
+int64_t qdb_gpu_agg_dispatch(const qdb_gpu_program* prog, void* ht, qdb_rowset* batch, int64_t arg, int64_t op) {
+    t_error.clear();
+    if (!prog || (prog->kind != PK_AGG && prog->kind != PK_JOIN_AGG) || !ht) {
+        SetErr("agg_dispatch: not an aggregate program");
+        return op == QDB_AGG_OP_UPDATE ? -1 : 0;
+    }
+    const AggLowering& lw = prog->agg;
+    cudaStream_t s = CurStream();
+    switch (op) {
+        case QDB_AGG_OP_INIT:
+        case QDB_AGG_OP_INIT_ROWS: {
+            if (StateOf(ht)) AggStateDestroy(StateOf(ht));
+            const int64_t hint = op == QDB_AGG_OP_INIT ? arg : arg * 2;
+            AggTableState* st = AggStateCreate(lw.plan, hint, prog->expected_groups, s);
+            *static_cast<AggTableState**>(ht) = st;
+            if (!st) return 0;
+            MirrorHeader(ht, st, lw.plan);
+            return 1;
+        }
+        case QDB_AGG_OP_SWITCH_TO_ROWS_AT:
+            // The device table already keeps key and states in one row slot.
+            return StateOf(ht) ? 1 : 0;
+        case QDB_AGG_OP_EXPECT_ROW_GROUPS: {
+            AggTableState* st = StateOf(ht);
+            if (!st) return 0;
+            st->expected = std::max<int64_t>(st->expected, arg);
+            if (arg * 2 > st->t.capacity && !Grow(st, lw.plan, arg)) return 0;
+            MirrorHeader(ht, st, lw.plan);
+            return 1;
+        }
+        case QDB_AGG_OP_UPDATE: {
+            AggTableState* st = StateOf(ht);
+            if (!st) {
+                SetErr("agg_dispatch(Update) before Init");
+                return -1;
+            }
+            if (prog->kind != PK_AGG) {
+                SetErr("a fused join-aggregate is updated through qdb_gpu_join_aggregate_probe");
+                return -1;
+            }
+            if (!batch) return st->groups;
+            AggPlan plan = lw.plan;
+            Staging stg(st->s);
+            if (!ResolveColumns(plan, lw.cols, prog->columns.data(), batch, stg)) return -1;
+            if (!AggRun(st, plan, batch->RowCount, nullptr, nullptr)) return -1;
+            MirrorHeader(ht, st, lw.plan);
+            return st->groups;
+        }
+        default:
+            return 0;
+    }
+}
+
+int64_t qdb_gpu_agg_finish_rowset(const qdb_gpu_program* prog, void* ht, qdb_rowset* out) {
+    t_error.clear();
+    if (!prog || !ht || !out) {
+        SetErr("agg_finish_rowset: bad arguments");
+        return -1;
+    }
+    AggTableState* st = StateOf(ht);
+    if (!st) {
+        SetErr("agg_finish_rowset before Init");
+        return -1;
+    }
+    const int64_t n = AggFinish(st, prog->agg, prog->flags, out);
+    AggStateDestroy(st);
+    std::memset(ht, 0, QDB_HASH_TABLE_SIZE);
+    return n;
+}
+
+void qdb_gpu_filter(const qdb_gpu_program* prog, qdb_rowset* rs, const uint8_t* input_selection) {
+    t_error.clear();
+    if (!prog || prog->kind != PK_FILTER || !rs || !rs->Selection) {
+        SetErr("filter: bad arguments (the caller owns rs->Selection)");
+        return;
+    }
+    cudaStream_t s = CurStream();
+    AggPlan plan = prog->expr.plan;
+    Staging stg(s);
+    qdb_rowset view = *rs;
+    view.Selection = const_cast<uint8_t*>(input_selection);
+    if (!ResolveColumns(plan, prog->expr.cols, prog->columns.data(), &view, stg)) return;
+    const bool dev_out = IsDevicePtr(rs->Selection);
+    uint8_t* out = dev_out ? rs->Selection : static_cast<uint8_t*>(DevAlloc(size_t(rs->RowCount), s));
+    int* derr = static_cast<int*>(DevAlloc(sizeof(int), s));
+    cudaMemsetAsync(derr, 0, sizeof(int), s);
+    ExprArgs a;
+    a.plan = &plan;
+    a.nrows = rs->RowCount;
+    a.out_sel = out;
+    a.err = derr;
+    FilterRows(a, s);
+    int herr = 0;
+    cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (!dev_out) cudaMemcpyAsync(rs->Selection, out, size_t(rs->RowCount), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    if (herr) SetErr("filter: device error %d", herr);
+    if (!dev_out) DevFree(out, s);
+    DevFree(derr, s);
+}
+
+void qdb_gpu_project(const qdb_gpu_program* prog, qdb_rowset* in, void** out_buffers, void* arena,
+                     const uint8_t* input_selection) {
+    (void)arena;
+    t_error.clear();
+    if (!prog || prog->kind != PK_PROJECT || !in || !out_buffers) {
+        SetErr("project: bad arguments");
+        return;
+    }
+    cudaStream_t s = CurStream();
+    AggPlan plan = prog->expr.plan;
+    Staging stg(s);
+    qdb_rowset view = *in;
+    view.Selection = const_cast<uint8_t*>(input_selection);
+    if (!ResolveColumns(plan, prog->expr.cols, prog->columns.data(), &view, stg)) return;
+    const int nout = int(prog->expr.out_types.size());
+    ExprArgs a;
+    a.plan = &plan;
+    a.nrows = in->RowCount;
+    a.nout = nout;
+    std::vector<void*> dev(nout, nullptr);
+    std::vector<bool> staged(nout, false);
+    for (int k = 0; k < nout; ++k) {
+        a.out_src[k] = uint8_t(prog->expr.value_src[k]);
+        a.out_idx[k] = uint8_t(prog->expr.value_idx[k]);
+        a.out_type[k] = prog->expr.out_types[k];
+        if (IsDevicePtr(out_buffers[k])) {
+            dev[k] = out_buffers[k];
+        } else {
+            dev[k] = DevAlloc(size_t(in->RowCount) * StorageWidth(a.out_type[k]), s);
+            staged[k] = true;
+        }
+        a.out_ptr[k] = dev[k];
+    }
+    int* derr = static_cast<int*>(DevAlloc(sizeof(int), s));
+    cudaMemsetAsync(derr, 0, sizeof(int), s);
+    a.err = derr;
+    ProjectRows(a, s);
+    int herr = 0;
+    cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s);
+    for (int k = 0; k < nout; ++k) {
+        if (staged[k]) {
+            cudaMemcpyAsync(out_buffers[k], dev[k], size_t(in->RowCount) * StorageWidth(a.out_type[k]),
+                            cudaMemcpyDeviceToHost, s);
+        }
+    }
+    cudaStreamSynchronize(s);
+    if (herr) SetErr("project: device error %d", herr);
+    for (int k = 0; k < nout; ++k) {
+        if (staged[k]) DevFree(dev[k], s);
+    }
+    DevFree(derr, s);
+}
+
+bool qdb_gpu_hash(const qdb_gpu_program* prog, qdb_rowset* batch, uint64_t* hashes) {
+    t_error.clear();
+    if (!prog || prog->kind != PK_HASH || !batch || !hashes) {
+        SetErr("hash: bad arguments");
+        return false;
+    }
+    cudaStream_t s = CurStream();
+    AggPlan plan = prog->expr.plan;
+    Staging stg(s);
+    if (!ResolveColumns(plan, prog->expr.cols, prog->columns.data(), batch, stg)) return false;
+    ExprArgs a;
+    a.plan = &plan;
+    a.nrows = batch->RowCount;
+    a.nhash = int(prog->expr.out_types.size());
+    for (int j = 0; j < a.nhash; ++j) {
+        a.hash_slot[j] = uint8_t(prog->expr.value_idx[j]);
+        a.hash_type[j] = prog->expr.out_types[j];
+    }
+    const bool dev_out = IsDevicePtr(hashes);
+    uint64_t* out = dev_out ? hashes : static_cast<uint64_t*>(DevAlloc(size_t(batch->RowCount) * 8, s));
+    if (!dev_out && batch->Selection) {
+        cudaMemcpyAsync(out, hashes, size_t(batch->RowCount) * 8, cudaMemcpyHostToDevice, s);
+    }
+    a.hashes = out;
+    HashRows(a, s);
+    if (!dev_out) cudaMemcpyAsync(hashes, out, size_t(batch->RowCount) * 8, cudaMemcpyDeviceToHost, s);
+    const bool ok = CudaOk(cudaStreamSynchronize(s), "hash");
+    if (!dev_out) DevFree(out, s);
+    return ok;
+}
+
+}  // extern "C"

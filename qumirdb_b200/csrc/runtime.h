@@ -1,0 +1,88 @@
+// runtime.h — host runtime shared by the C ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/qdb_gpu.h"
+#include "kernels.h"
+#include "lower.h"
+
+namespace qdb {
+
+extern thread_local std::string t_error;
+void SetErr(const char* fmt, ...);
+bool CudaOk(cudaError_t e, const char* what);
+cudaStream_t CurStream();
+void* DevAlloc(size_t bytes, cudaStream_t s);
+void DevFree(void* p, cudaStream_t s);
+bool IsDevicePtr(const void* p);
+int64_t NextPow2(int64_t v);
+
+// Device copies of host buffers for the duration of one call.
+struct Staging {
+    explicit Staging(cudaStream_t st) : s(st) {}
+    ~Staging();
+    const void* Device(const void* p, size_t bytes);
+    cudaStream_t s;
+    std::vector<void*> owned;
+};
+
+bool ResolveColumns(AggPlan& P, const ColumnMap& cm, const qdb_column_type* types, const qdb_rowset* rs,
+                    Staging& st);
+AggPlan OffsetPlan(const AggPlan& P, int64_t begin);
+
+struct AggTableState;
+AggTableState* AggStateCreate(const AggPlan& p, int64_t capacity_hint, int64_t expected, cudaStream_t s);
+void AggStateDestroy(AggTableState* st);
+bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyPlan* jk, const JTableDev* jt);
+int64_t AggFinish(AggTableState* st, const AggLowering& lw, uint32_t flags, qdb_rowset* out);
+int64_t AggStateGroups(const AggTableState* st);
+int64_t AggStateMatched(const AggTableState* st);
+AggTableState* AggStateOf(void* ht);
+void AggMirrorHeader(void* ht, const AggTableState* st, const AggPlan& p);
+
+bool AllocOutputCols(const std::vector<int>& types, int64_t rows, bool with_valid, std::vector<AggOutputCol>& cols);
+bool EmitRowset(std::vector<AggOutputCol>& cols, const std::vector<int>& types, int64_t rows, bool on_device,
+                cudaStream_t s, qdb_rowset* out);
+
+struct JoinProgram {
+    int32_t build_is_left = 0;
+    std::vector<qdb_column_type> build_columns;
+    std::vector<qdb_column_type> probe_columns;
+    std::vector<int> build_keys;
+    std::vector<int> probe_keys;
+    std::vector<int> payload;
+    std::vector<int> out_side;
+    std::vector<int> out_column;
+    bool has_build_filter = false;
+    ExprLowering build_filter;        // over the build schema (filter + key NULL rejection)
+    JoinKeyPlan build_jk;             // col = build input column
+    JoinKeyPlan probe_jk;             // col = probe input column
+    JoinKeyPlan agg_jk;               // col = fused plan slot of the probe key
+};
+
+struct SortProgram {
+    std::vector<qdb_column_type> columns;
+    std::vector<qdb_sort_key> keys;
+    std::vector<int> out_columns;
+};
+
+}  // namespace qdb
+
+struct qdb_gpu_program {
+    int kind = 0;
+    uint32_t flags = 0;
+    int64_t expected_groups = 0;
+    std::vector<qdb_column_type> columns;     // scan / probe / aggregate input schema
+    qdb::AggLowering agg;
+    qdb::ExprLowering expr;
+    qdb::JoinProgram join;
+    qdb::SortProgram sort;
+};
+
+namespace qdb {
+enum ProgramKind { PK_AGG = 1, PK_FILTER, PK_PROJECT, PK_HASH, PK_JOIN, PK_JOIN_AGG, PK_SORT };
+}
