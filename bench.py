@@ -179,11 +179,13 @@ def timed(q, fn, steps: int, warmup: int, dist=None, profile: bool = False):
     return ms, results, launches, kernels
 
 
-def kernel_avg(kernels, name):
+def kernel_avg(kernels, name, steps: int = 1):
+    """Per-step device time of every launch of `name` (summed over the step's
+    launches) and the units they processed per step."""
     ks = [(ms, units) for n, ms, units in kernels if n == name]
     if not ks:
         return None, None
-    return sum(k[0] for k in ks) / len(ks), sum(k[1] for k in ks) / len(ks)
+    return sum(k[0] for k in ks) / steps, sum(k[1] for k in ks) / steps
 
 
 def load_traffic() -> dict:
@@ -192,12 +194,12 @@ def load_traffic() -> dict:
 
 
 def lineitem_operator(q, peak):
-    from qumirdb_b200 import queries
+    from qumirdb_b200 import abi, queries
     n = LINEITEM_ROWS
     cols = [np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64),
             np.empty(n, np.uint8), np.empty(n, np.uint8), np.empty(n, np.int32)]
     q.lib().qdb_gen_lineitem(0, n, *[c.ctypes.data for c in cols])
-    spec = queries.lineitem_agg(int(cols[6].max()) - 90)
+    spec = queries.lineitem_agg(int(cols[6].max()) - 90, flags=abi.OUT_DEVICE)
     prog = q.compile_aggregate(spec)
     drs = q.DeviceRowSet(cols)
     flush = q.DeviceBuffer(256 << 20)
@@ -210,7 +212,7 @@ def lineitem_operator(q, peak):
         q.release(out)
 
     ms, _, launches, kernels = timed(q, step, 10, 3, profile=True)
-    kms, _ = kernel_avg(kernels, "agg_update")
+    kms, _ = kernel_avg(kernels, "agg_update", 10)
     alg = n * 38
     return {"workload": "lineitem scan-filter-aggregate, 6,001,215 rows, GROUP BY flag, status",
             "rows_per_s": n / (ms / 1e3), "ms_per_query": ms, "kernel": "agg_update", "kernel_ms": kms,
@@ -224,11 +226,11 @@ def flush_l2(q, buf):
 
 
 def zipf_operator(q, peak):
-    from qumirdb_b200 import queries
+    from qumirdb_b200 import abi, queries
     n = ZIPF_ROWS
     cols = [np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.float64)]
     q.lib().qdb_gen_zipf(2, n, ZIPF_DISTINCT, 1.1, *[c.ctypes.data for c in cols])
-    spec = queries.zipf_agg(expected_groups=ZIPF_DISTINCT)
+    spec = queries.zipf_agg(expected_groups=ZIPF_DISTINCT, flags=abi.OUT_DEVICE)
     prog = q.compile_aggregate(spec)
     drs = q.DeviceRowSet(cols)
     del cols
@@ -242,7 +244,7 @@ def zipf_operator(q, peak):
         q.release(out)
 
     ms, _, launches, kernels = timed(q, step, 3, 1, profile=True)
-    kms, _ = kernel_avg(kernels, "agg_update")
+    kms, _ = kernel_avg(kernels, "agg_update", 3)
     alg = n * 24
     return {"workload": "GROUP BY key (Zipf 1.1 over 20M), 200M rows, COUNT/SUM/MIN/MAX/SUM(f64)",
             "rows_per_s": n / (ms / 1e3), "ms_per_query": ms, "groups": groups[-1], "kernel": "agg_update",
@@ -336,7 +338,7 @@ def main() -> None:
     sampler.start()
     ms, results, launches, kernels = timed(q, query, args.steps, args.warmup, dist=dist, profile=True)
     clocks = sampler.stop()
-    kms, kunits = kernel_avg(kernels, "join_agg_probe")
+    kms, kunits = kernel_avg(kernels, "join_agg_probe", args.steps)
     alg_bytes = PROBE_ROWS * 16
     achieved = alg_bytes / (kms / 1e3) / 1e9 if kms else None
     traffic = load_traffic().get("join_agg_probe_bytes_per_probe_row")

@@ -1,21 +1,29 @@
 // agg.cu — fused filter -> project -> hash aggregate for sm_100a.
 //
 // One persistent CTA per SM streams row tiles of every referenced column
-// into shared memory with 1-D bulk copies (cp.async.bulk, completion on an
-// mbarrier; several stages in flight), evaluates the predicate, group key and
-// aggregate arguments per row from shared memory, and folds rows into
-//   (1) a per-CTA shared-memory group table (low cardinality, and the hot
-//       head of a skewed key distribution), after a warp-level
-//       pre-aggregation (__match_any_sync + butterfly reduction) when a warp
-//       holds few distinct groups, and
-//   (2) a global open-addressing table in HBM (one cache-line-sized slot per
-//       group: key + state words; CAS key claim, atomic state updates).
-// At the end each CTA merges its shared table into the global one.  A row
-// whose global probe exceeds the probe bound is deferred (row id to a list)
-// and a shared entry that cannot be merged is spilled; the host grows the
-// table and replays both, so no row is ever lost or double counted.
+// into shared memory with 1-D bulk copies (cp.async.bulk completing on an
+// mbarrier, three stages in flight; warps release a stage through a second
+// mbarrier, so no block-wide barrier sits between tiles).  Each lane takes
+// one row at a time and evaluates the predicate, the group key and every
+// aggregate input from shared memory, then folds the row into
+//   (1) lane-private accumulators in shared memory for the first four
+//       groups the CTA meets (no atomics, no bank conflicts: word w of
+//       group g of thread t lives at ((g * W + w) * blockDim + t)) — the
+//       low-cardinality and keyless case,
+//   (2) a per-CTA shared-memory group table updated with shared atomics,
+//   (3) a global open-addressing table in HBM (one slot per group holding
+//       key and state words; CAS key claim, atomic state updates) — the
+//       high-cardinality case.
+// At the end a CTA reduces (1) into (2) and merges (2) into (3).  A row whose
+// global probe exceeds the probe bound is deferred (row id to a list) and a
+// shared entry that cannot be merged is spilled; the host grows the table and
+// replays both, so no row is lost or counted twice.
 //
-// Semantics match the engine's reducers (qdb/kernel/gen.cpp:3301-3593): i64
+// The fused join variant probes a built join table (32-byte entries: key,
+// arena row, first payload word) for several probe rows per lane at once and
+// folds every joined row the same way.
+//
+// Semantics are the engine's reducers (qdb/kernel/gen.cpp:3301-3593): i64
 // sums wrap, decimal sums are exact i128, COUNT counts non-NULL inputs, MIN /
 // MAX fold non-NULL inputs, f64 sums are IEEE additions in device order.
 #include <algorithm>
@@ -30,7 +38,8 @@
 namespace qdb {
 
 constexpr int kAggThreads = 512;
-constexpr int kWarpAggMax = 4;     // leader-loop pre-aggregation up to this many groups per warp
+constexpr int kPrivGroups = 4;     // groups per CTA folded into lane-private accumulators
+constexpr int kProbeRows = 4;      // fused join: probe rows in flight per lane
 constexpr int kMaxProbe = 256;     // global table probe bound before a row is deferred
 
 __device__ __forceinline__ int64_t Min64(int64_t a, int64_t b) { return a < b ? a : b; }
@@ -51,12 +60,15 @@ struct AggLaunch {
     int32_t sel_off;          // selection tile offset inside a stage (-1: not staged)
     int32_t smem_slots;
     int32_t smem_limit;
-    int32_t off_bars;
-    int32_t off_bases;
+    int32_t off_bars;         // full barriers, then empty barriers
+    int32_t off_misc;
     int32_t off_skeys;
     int32_t off_sst;
-    int32_t off_misc;
+    int32_t off_gid;
+    int32_t off_pacc;
     int32_t any_staged;
+    int32_t priv;
+    int32_t inline_slot;      // fused join: plan slot served by the entry's payload word (-1 none)
     GTableDev T;
     uint64_t cap_mask;
     AggCounters* counters;
@@ -74,18 +86,21 @@ struct AggLaunch {
 // ---------------------------------------------------------------------------
 struct RowAcc {
     const AggPlan* P;
-    const char* const* base;  // tile base per column slot (smem or global), or nullptr
-    int r;                    // row inside the tile
-    int64_t arow;             // row inside the launch range
-    int64_t brow;             // matched build row (fused join)
+    const unsigned char* stage;   // staged tile of this row, or nullptr (global columns)
+    int r;                        // row inside the tile
+    int64_t arow;                 // row inside the launch range
+    int64_t brow;                 // matched build row (fused join)
+    int inl_slot;                 // slot whose value is `inl` (fused join), -1 none
+    uint64_t inl;
 
     __device__ __forceinline__ const char* Ptr(int c) const {
         const ColDesc& cd = P->cols[c];
         if (cd.build) return cd.data + brow * cd.width;
-        if (base) return base[c] + int64_t(r) * cd.width;
+        if (stage && cd.stage) return reinterpret_cast<const char*>(stage + cd.smem_off) + int64_t(r) * cd.width;
         return cd.data + arow * cd.width;
     }
     __device__ __forceinline__ i128 Int(int c) const {
+        if (c == inl_slot) return i128(int64_t(inl));
         const ColDesc& cd = P->cols[c];
         if (cd.kind == LK_BOOLBIT) {
             const int64_t bit = cd.bit_off + (cd.build ? brow : arow);
@@ -106,6 +121,10 @@ struct RowAcc {
     }
     __device__ __forceinline__ double F64(int c) const {
         const ColDesc& cd = P->cols[c];
+        if (c == inl_slot) {
+            if (cd.kind == LK_F64) return __longlong_as_double((long long)inl);
+            return cd.scale ? double(int64_t(inl)) / Pow10F(cd.scale) : double(int64_t(inl));
+        }
         if (cd.kind == LK_F64) return *reinterpret_cast<const double*>(Ptr(c));
         if (cd.kind == LK_F32) return double(*reinterpret_cast<const float*>(Ptr(c)));
         const i128 v = Int(c);
@@ -148,8 +167,8 @@ __device__ __forceinline__ Contrib StateInput(const AggPlan& P, const StateDesc&
     double fv = 0.0;
     if (sd.src == VS_SOP) {
         const SopValue& v = P.values[sd.idx];
-        null = SopNull(v, acc);
-        if (!null) {
+        null = v.null_cols != 0 && SopNull(v, acc);
+        if (!null && sd.kind != ST_COUNT) {
             if (v.kind == VK_F64) fv = SopF64(v, acc);
             else iv = SopInt(v, acc);
         }
@@ -210,6 +229,27 @@ __device__ __forceinline__ void ApplyState(uint64_t* w, uint64_t* w_hi, uint8_t 
         case ST_MAX_I64: atomicMax(reinterpret_cast<long long*>(w), (long long)lo); break;
         case ST_MIN_F64: atomicMin(u, (unsigned long long)lo); break;
         case ST_MAX_F64: atomicMax(u, (unsigned long long)lo); break;
+    }
+}
+
+// Plain fold into a lane-private accumulator (w_hi: the high word).
+__device__ __forceinline__ void PrivFold(uint64_t* w, uint64_t* w_hi, uint8_t kind, uint64_t lo, uint64_t hi,
+                                         double f) {
+    switch (kind) {
+        case ST_COUNT:
+        case ST_SUM_I64: *w += lo; break;
+        case ST_SUM_I128: {
+            const uint64_t o = *w;
+            const uint64_t n = o + lo;
+            *w = n;
+            *w_hi += hi + (n < o ? 1ull : 0ull);
+            break;
+        }
+        case ST_SUM_F64: *reinterpret_cast<double*>(w) += f; break;
+        case ST_MIN_I64: if ((long long)lo < (long long)*w) *w = lo; break;
+        case ST_MAX_I64: if ((long long)lo > (long long)*w) *w = lo; break;
+        case ST_MIN_F64: if (lo < *w) *w = lo; break;
+        case ST_MAX_F64: if (lo > *w) *w = lo; break;
     }
 }
 
@@ -313,15 +353,20 @@ __device__ __forceinline__ void Defer(const AggLaunch& L, int64_t arow, int64_t 
 }
 
 // ---------------------------------------------------------------------------
-// Shared-memory tier (one-word keys).
+// Shared-memory tier (one-word keys) with the lane-private group directory.
 // ---------------------------------------------------------------------------
 struct SmemTable {
     uint64_t* keys;       // S keys (kEmptyKey = free)
     uint64_t* st;         // state word w of slot i at st[w * S + i]
+    int* gid;             // slot -> lane-private group (-2 pending, -1 none)
+    int* gid_slot;        // lane-private group -> slot
     unsigned* count;      // keys inserted
     unsigned* fresh;      // global groups this CTA created
+    unsigned* ngid;       // lane-private groups handed out
+    uint64_t* pacc;       // lane-private accumulators
     int S;
     int limit;
+    int priv;
 
     __device__ __forceinline__ int Find(uint64_t key) const {
         uint32_t i = uint32_t(Fmix64(key)) & uint32_t(S - 1);
@@ -333,6 +378,15 @@ struct SmemTable {
                 const uint64_t old = atomicCAS(reinterpret_cast<unsigned long long*>(&keys[i]), kEmptyKey, key);
                 if (old == kEmptyKey) {
                     atomicAdd(count, 1u);
+                    int g = -1;
+                    if (priv) {
+                        const unsigned k = atomicAdd(ngid, 1u);
+                        if (k < unsigned(kPrivGroups)) {
+                            g = int(k);
+                            gid_slot[k] = int(i);
+                        }
+                    }
+                    *reinterpret_cast<volatile int*>(&gid[i]) = g;
                     return int(i);
                 }
                 if (old == key) return int(i);
@@ -343,31 +397,65 @@ struct SmemTable {
     }
 };
 
+__device__ __forceinline__ unsigned char* DynSmem() {
+    extern __shared__ __align__(128) unsigned char qdb_dyn_smem[];
+    return qdb_dyn_smem;
+}
+
+// The shared-memory tier of this CTA, located by the launch's offsets.
+__device__ __forceinline__ SmemTable MakeSmem(const AggLaunch& L, bool wide, bool priv) {
+    unsigned char* smem = DynSmem();
+    unsigned* misc = reinterpret_cast<unsigned*>(smem + L.off_misc);
+    SmemTable sm;
+    sm.keys = reinterpret_cast<uint64_t*>(smem + L.off_skeys);
+    sm.st = reinterpret_cast<uint64_t*>(smem + L.off_sst);
+    sm.gid = reinterpret_cast<int*>(smem + L.off_gid);
+    sm.gid_slot = reinterpret_cast<int*>(misc + 8);
+    sm.count = misc;
+    sm.fresh = misc + 1;
+    sm.ngid = misc + 2;
+    sm.pacc = reinterpret_cast<uint64_t*>(smem + L.off_pacc);
+    sm.S = wide ? 0 : L.smem_slots;
+    sm.limit = L.smem_limit;
+    sm.priv = priv;
+    return sm;
+}
+
 // ---------------------------------------------------------------------------
-// Per-row (per-warp) fold of one joined/scanned row.  Warp-uniform.
+// Per-lane fold of one (joined) row that is selected.  Kept out of line: one
+// copy serves every call site, so the kernel stays inside the instruction
+// cache.
 // ---------------------------------------------------------------------------
-template <bool WIDE, bool GEN>
-__device__ __forceinline__ void FoldRow(const AggLaunch& L, const SmemTable& sm, bool act, const RowAcc& acc) {
+template <bool WIDE, bool GEN, bool PRIV>
+__device__ __noinline__ void FoldRow(const AggLaunch& L, RowAcc acc) {
+    const SmemTable sm = MakeSmem(L, WIDE, PRIV);
     const AggPlan& P = L.P;
     GVal gv[GEN ? kMaxGNodes : 1];
     uint64_t gn = 0;
-    if (GEN && act && P.generic_root >= 0) {
+    if (GEN && P.generic_root >= 0) {
         if (!EvalGeneric(P.prog, P.generic_root, P.list, acc, gv, gn)) {
             SetError(&L.counters->error, DE_DIV_ZERO);
-            act = false;
+            return;
         }
     }
-    if (act && P.filter_kind == 1) act = AtomsPass(P, acc);
-    else if (GEN && act && P.filter_kind == 2) act = !((gn >> P.filter_node) & 1) && gv[P.filter_node].i != 0;
+    if (P.filter_kind == 1) {
+        if (!AtomsPass(P, acc)) return;
+    } else if (GEN && P.filter_kind == 2) {
+        if (((gn >> P.filter_node) & 1) || gv[P.filter_node].i == 0) return;
+    }
 
     int slot = -1;
+    int g = -1;
     int64_t gslot = -1;
     if (!WIDE) {
         uint64_t key = 0;
-        if (act) key = PackKey1(P, acc, gv, gn);
-        const bool special = act && P.key_full64 && key == kEmptyKey;
-        if (act && sm.S > 0 && !special) slot = sm.Find(key);
-        if (act && slot < 0) {
+        if (P.nkeyparts) key = PackKey1(P, acc, gv, gn);
+        const bool special = P.key_full64 && key == kEmptyKey;
+        if (sm.S > 0 && !special) {
+            slot = sm.Find(key);
+            if (PRIV && slot >= 0) g = *reinterpret_cast<volatile int*>(&sm.gid[slot]);
+        }
+        if (slot < 0) {
             if (special) {
                 gslot = L.T.capacity;
                 unsigned long long* flag = reinterpret_cast<unsigned long long*>(
@@ -382,72 +470,36 @@ __device__ __forceinline__ void FoldRow(const AggLaunch& L, const SmemTable& sm,
             }
             if (gslot < 0) {
                 Defer(L, acc.arow, acc.brow);
-                act = false;
+                return;
             }
         }
     } else {
-        if (act) {
-            uint64_t kw[kMaxKeyWords];
-            PackKey(P, acc, gv, gn, kw);
-            int is_new = 0;
-            gslot = GlobalFindW(L.T, L.cap_mask, kw, P.key_words, is_new, &L.counters->error);
-            if (is_new) atomicAdd(sm.fresh, 1u);
-            if (gslot == -1) Defer(L, acc.arow, acc.brow);
-            if (gslot < 0) act = false;
-        }
+        uint64_t kw[kMaxKeyWords];
+        PackKey(P, acc, gv, gn, kw);
+        int is_new = 0;
+        gslot = GlobalFindW(L.T, L.cap_mask, kw, P.key_words, is_new, &L.counters->error);
+        if (is_new) atomicAdd(sm.fresh, 1u);
+        if (gslot == -1) Defer(L, acc.arow, acc.brow);
+        if (gslot < 0) return;
     }
 
-    const unsigned actmask = __ballot_sync(kFull, act);
-    if (actmask == 0) return;
-    const int grp = (act && slot >= 0) ? slot : -1;
-    const unsigned peers = __match_any_sync(kFull, grp);
-    const bool leader = grp >= 0 && LaneId() == __ffs(peers) - 1;
-    const unsigned leaders = __ballot_sync(kFull, leader);
-    const int nlead = __popc(leaders);
-    const bool wagg = nlead > 0 && nlead <= kWarpAggMax;
+    const int bd = blockDim.x;
     uint64_t* gbase = gslot >= 0 ? L.T.slots + gslot * L.T.slot_words + L.T.state_off : nullptr;
-
     for (int s = 0; s < P.nstates; ++s) {
         const StateDesc sd = P.states[s];
-        Contrib c{0, 0, 0.0, false};
-        if (act) c = StateInput(P, sd, acc, gv, gn);
-        if (wagg) {
-            unsigned lm = leaders;
-            while (lm) {
-                const int ld = __ffs(lm) - 1;
-                lm &= lm - 1;
-                const int lslot = __shfl_sync(kFull, slot, ld);
-                Contrib r = c;
-                WarpReduceState(sd.kind, act && c.has && slot == lslot, r);
-                const bool any = sd.kind == ST_SUM_F64 ? r.f != 0.0 : !IsIdentity(sd.kind, r.lo, r.hi);
-                if (LaneId() == ld && any) {
-                    uint64_t* w = sm.st + int64_t(sd.word) * sm.S + lslot;
-                    ApplyState(w, w + sm.S, sd.kind, r.lo, r.hi, r.f);
-                }
-            }
-        } else if (act && slot >= 0 && c.has) {
+        const Contrib c = StateInput(P, sd, acc, gv, gn);
+        if (!c.has) continue;
+        if (PRIV && g >= 0) {
+            uint64_t* w = sm.pacc + (int64_t(g) * P.state_words + sd.word) * bd + threadIdx.x;
+            PrivFold(w, w + bd, sd.kind, c.lo, c.hi, c.f);
+        } else if (slot >= 0) {
             uint64_t* w = sm.st + int64_t(sd.word) * sm.S + slot;
             ApplyState(w, w + sm.S, sd.kind, c.lo, c.hi, c.f);
-        }
-        if (act && gslot >= 0 && c.has) {
+        } else {
             uint64_t* w = gbase + sd.word;
             ApplyState(w, w + 1, sd.kind, c.lo, c.hi, c.f);
         }
     }
-}
-
-// Probes the join table for the first match at or after slot `i`.
-__device__ __forceinline__ int64_t JoinNext(const JTableDev& jt, uint64_t key, uint64_t i, int64_t& brow) {
-    for (int64_t p = 0; p <= int64_t(jt.mask); ++p) {
-        const uint64_t k = jt.entries[2 * i];
-        if (k == kEmptyKey) return -1;
-        if (k == key) {
-            brow = int64_t(jt.entries[2 * i + 1]);
-            return int64_t(i);
-        }
-        i = (i + 1) & jt.mask;
-    }
-    return -1;
 }
 
 __device__ __forceinline__ uint64_t PackJoinKey(const JoinKeyPlan& jk, const RowAcc& a, bool& null) {
@@ -472,68 +524,77 @@ __device__ __forceinline__ uint64_t PackJoinKey(const JoinKeyPlan& jk, const Row
     return k;
 }
 
-// Folds every joined row of probe row `acc` (fused join-aggregate).
-template <bool WIDE, bool GEN>
-__device__ __forceinline__ void FoldProbeRow(const AggLaunch& L, const SmemTable& sm, bool act, RowAcc acc) {
-    bool null = false;
-    uint64_t key = 0;
-    if (act) key = PackJoinKey(L.jk, acc, null);
-    act = act && !null;
-    int64_t pos = -1;
-    int64_t special_i = -1;
-    const bool special = act && L.jk.full64 && key == kEmptyKey;
-    if (act && !special) pos = JoinNext(L.jt, key, Fmix64(key) & L.jt.mask, acc.brow);
-    if (special && L.jt.nspecial > 0) {
-        special_i = 0;
-        acc.brow = L.jt.special_rows[0];
-    }
+// Folds every joined row of one probe row whose first probed entry is `e`
+// (key, row) at slot `i`.
+template <bool WIDE, bool GEN, bool PRIV>
+__device__ __forceinline__ unsigned FoldMatches(const AggLaunch& L, RowAcc acc, uint64_t key, uint64_t i,
+                                                ulonglong2 e) {
     unsigned matched = 0;
-    while (__any_sync(kFull, pos >= 0 || special_i >= 0)) {
-        const bool has = pos >= 0 || special_i >= 0;
-        FoldRow<WIDE, GEN>(L, sm, has, acc);
-        matched += has ? 1u : 0u;
-        if (pos >= 0) {
-            pos = JoinNext(L.jt, key, (uint64_t(pos) + 1) & L.jt.mask, acc.brow);
-        } else if (special_i >= 0) {
-            ++special_i;
-            if (special_i < L.jt.nspecial) acc.brow = L.jt.special_rows[special_i];
-            else special_i = -1;
+    for (int64_t p = 0; p <= int64_t(L.jt.mask); ++p) {
+        if (e.x == kEmptyKey) break;
+        if (e.x == key) {
+            acc.brow = int64_t(e.y);
+            if (acc.inl_slot >= 0) acc.inl = L.jt.entries[4 * i + 2];
+            FoldRow<WIDE, GEN, PRIV>(L, acc);
+            ++matched;
         }
+        i = (i + 1) & L.jt.mask;
+        e = *reinterpret_cast<const ulonglong2*>(&L.jt.entries[4 * i]);
     }
-    const unsigned total = __reduce_add_sync(kFull, matched);
-    if (LaneId() == 0 && total) atomicAdd(&L.counters->matched, (unsigned long long)total);
+    return matched;
 }
 
-template <bool WIDE, bool JOIN, bool GEN>
+template <bool WIDE, bool JOIN, bool GEN, bool PRIV>
 __global__ void __launch_bounds__(kAggThreads, 1) AggUpdateKernel(const __grid_constant__ AggLaunch L) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.off_bars);
-    const char** sbase = reinterpret_cast<const char**>(smem + L.off_bases);
+    unsigned char* smem = DynSmem();
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.off_bars);
+    uint64_t* empty = full + L.stages;
     unsigned* misc = reinterpret_cast<unsigned*>(smem + L.off_misc);
-    SmemTable sm;
-    sm.keys = reinterpret_cast<uint64_t*>(smem + L.off_skeys);
-    sm.st = reinterpret_cast<uint64_t*>(smem + L.off_sst);
-    sm.count = misc;
-    sm.fresh = misc + 1;
-    sm.S = WIDE ? 0 : L.smem_slots;
-    sm.limit = L.smem_limit;
+    const SmemTable sm = MakeSmem(L, WIDE, PRIV);
     const AggPlan& P = L.P;
     const int tid = threadIdx.x;
+    const int bd = blockDim.x;
+    const int nwarps = bd >> 5;
 
     if (tid == 0) {
         misc[0] = 0;
         misc[1] = 0;
         misc[2] = 0;
-        for (int s = 0; s < L.stages; ++s) MbarInit(&bars[s], 1);
+        misc[3] = 0;   // matched rows (fused join)
+        misc[4] = 0;   // abort flag
+        for (int s = 0; s < L.stages; ++s) {
+            MbarInit(&full[s], 1);
+            MbarInit(&empty[s], nwarps);
+        }
         FenceBarrierInit();
     }
-    for (int i = tid; i < sm.S; i += blockDim.x) {
+    for (int i = tid; i < sm.S; i += bd) {
         sm.keys[i] = kEmptyKey;
+        sm.gid[i] = -1;
         for (int s = 0; s < P.nstates; ++s) {
             const StateDesc sd = P.states[s];
             sm.st[int64_t(sd.word) * sm.S + i] = StateIdentity(sd.kind);
             if (sd.kind == ST_SUM_I128) sm.st[int64_t(sd.word + 1) * sm.S + i] = 0;
         }
+    }
+    if (PRIV) {
+        for (int g = 0; g < kPrivGroups; ++g) {
+            for (int s = 0; s < P.nstates; ++s) {
+                const StateDesc sd = P.states[s];
+                sm.pacc[(int64_t(g) * P.state_words + sd.word) * bd + tid] = StateIdentity(sd.kind);
+                if (sd.kind == ST_SUM_I128) sm.pacc[(int64_t(g) * P.state_words + sd.word + 1) * bd + tid] = 0;
+            }
+        }
+    }
+    __syncthreads();
+    if (PRIV && P.nkeyparts == 0 && tid == 0 && sm.S > 0) {
+        // A keyless aggregate has one group: key 0, lane-private group 0.
+        const int i = int(uint32_t(Fmix64(0)) & uint32_t(sm.S - 1));
+        sm.keys[i] = 0;
+        sm.gid[i] = 0;
+        sm.gid_slot[0] = i;
+        misc[0] = 1;
+        misc[2] = 1;
     }
     __syncthreads();
 
@@ -543,13 +604,13 @@ __global__ void __launch_bounds__(kAggThreads, 1) AggUpdateKernel(const __grid_c
     auto issue = [&](int64_t t, int s) {
         unsigned char* st = smem + int64_t(s) * L.stage_bytes;
         FenceProxyAsync();
-        MbarArriveExpectTx(&bars[s], uint32_t(L.stage_bytes));
+        MbarArriveExpectTx(&full[s], uint32_t(L.stage_bytes));
         for (int c = 0; c < P.ncols; ++c) {
             const ColDesc& cd = P.cols[c];
             if (!cd.stage) continue;
-            BulkG2S(st + cd.smem_off, cd.data + t * T * cd.width, uint32_t(T * cd.width), &bars[s]);
+            BulkG2S(st + cd.smem_off, cd.data + t * T * cd.width, uint32_t(T * cd.width), &full[s]);
         }
-        if (L.sel_off >= 0) BulkG2S(st + L.sel_off, P.selection + t * T, uint32_t(T), &bars[s]);
+        if (L.sel_off >= 0) BulkG2S(st + L.sel_off, P.selection + t * T, uint32_t(T), &full[s]);
     };
 
     if (tid == 0) {
@@ -559,67 +620,153 @@ __global__ void __launch_bounds__(kAggThreads, 1) AggUpdateKernel(const __grid_c
         }
     }
 
+    unsigned matched = 0;
     bool aborted = false;
     for (int64_t k = 0;; ++k) {
         const int64_t t = blockIdx.x + k * gridDim.x;
         if (t >= ntiles) break;
         const int s = int(k % L.stages);
-        const bool full = tile_full(t);
+        const uint32_t phase = uint32_t((k / L.stages) & 1);
+        const bool full_tile = tile_full(t);
         const int64_t row0 = t * T;
-        if (tid == 0) {
-            unsigned char* st = smem + int64_t(s) * L.stage_bytes;
-            for (int c = 0; c < P.ncols; ++c) {
-                const ColDesc& cd = P.cols[c];
-                sbase[c] = (full && cd.stage) ? reinterpret_cast<const char*>(st + cd.smem_off)
-                                              : cd.data + row0 * cd.width;
-            }
-            sbase[kMaxCols] = P.selection == nullptr ? nullptr
-                              : (full && L.sel_off >= 0) ? reinterpret_cast<const char*>(st + L.sel_off)
-                                                         : reinterpret_cast<const char*>(P.selection + row0);
+        const unsigned char* stage = full_tile ? smem + int64_t(s) * L.stage_bytes : nullptr;
+        if (full_tile && !MbarWaitBounded(&full[s], phase)) {
+            SetError(&L.counters->error, DE_WAIT_TIMEOUT);
+            aborted = true;
         }
-        __syncthreads();
-        if (full) {
-            if (!MbarWaitBounded(&bars[s], uint32_t((k / L.stages) & 1))) {
-                SetError(&L.counters->error, DE_WAIT_TIMEOUT);
-                aborted = true;
+        if (!aborted) {
+            const int nrows = int(Min64(T, L.nrows - row0));
+            const uint8_t* sel = P.selection == nullptr ? nullptr
+                                 : (stage && L.sel_off >= 0) ? stage + L.sel_off : P.selection + row0;
+            // Row accessor: staged columns come from the stage, the others
+            // (unaligned or tail tiles) from global memory.
+            RowAcc acc{&P, stage, 0, 0, 0, L.inline_slot, 0};
+            if (!JOIN) {
+                for (int r = tid; r < nrows; r += bd) {
+                    if (sel && !sel[r]) continue;
+                    acc.r = r;
+                    acc.arow = row0 + r;
+                    FoldRow<WIDE, GEN, PRIV>(L, acc);
+                }
+            } else {
+                for (int rb = tid; rb < nrows; rb += bd * kProbeRows) {
+                    uint64_t key[kProbeRows];
+                    uint64_t slot[kProbeRows];
+                    ulonglong2 e[kProbeRows];
+                    bool ok[kProbeRows];
+#pragma unroll
+                    for (int j = 0; j < kProbeRows; ++j) {
+                        const int r = rb + j * bd;
+                        ok[j] = r < nrows && (!sel || sel[r]);
+                        bool null = false;
+                        key[j] = 0;
+                        if (ok[j]) {
+                            acc.r = r;
+                            acc.arow = row0 + r;
+                            key[j] = PackJoinKey(L.jk, acc, null);
+                        }
+                        ok[j] = ok[j] && !null && !(L.jk.full64 && key[j] == kEmptyKey);
+                        slot[j] = Fmix64(key[j]) & L.jt.mask;
+                        e[j] = make_ulonglong2(kEmptyKey, 0);
+                        if (ok[j]) e[j] = *reinterpret_cast<const ulonglong2*>(&L.jt.entries[4 * slot[j]]);
+                    }
+#pragma unroll 1
+                    for (int j = 0; j < kProbeRows; ++j) {
+                        const int r = rb + j * bd;
+                        if (r >= nrows) continue;
+                        acc.r = r;
+                        acc.arow = row0 + r;
+                        if (ok[j]) matched += FoldMatches<WIDE, GEN, PRIV>(L, acc, key[j], slot[j], e[j]);
+                        // Keys equal to the empty marker live in a side list.
+                        if (L.jk.full64 && L.jt.nspecial > 0 && (!sel || sel[r])) {
+                            bool null = false;
+                            const uint64_t k2 = PackJoinKey(L.jk, acc, null);
+                            if (!null && k2 == kEmptyKey) {
+                                for (int64_t q = 0; q < L.jt.nspecial; ++q) {
+                                    acc.brow = L.jt.special_rows[2 * q];
+                                    if (acc.inl_slot >= 0) acc.inl = uint64_t(L.jt.special_rows[2 * q + 1]);
+                                    FoldRow<WIDE, GEN, PRIV>(L, acc);
+                                    ++matched;
+                                }
+                            }
+                        }
+                    }
+                }
             }
         }
-        if (__syncthreads_or(aborted)) {
+        // Release the stage; the producer refills it once every warp is done
+        // with it, so warps run up to `stages` tiles apart without a
+        // block-wide barrier.
+        __syncwarp();
+        if ((tid & 31) == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(SmemAddr(&empty[s])) : "memory");
+        if (aborted) *reinterpret_cast<volatile unsigned*>(&misc[4]) = 1;
+        if (*reinterpret_cast<volatile unsigned*>(&misc[4])) {
             aborted = true;
             break;
         }
-        const int nrows = int(Min64(T, L.nrows - row0));
-        const uint8_t* sel = reinterpret_cast<const uint8_t*>(sbase[kMaxCols]);
-        for (int rb = (tid & ~31); rb < T; rb += blockDim.x) {
-            const int r = rb + LaneId();
-            bool act = r < nrows;
-            if (act && sel) act = sel[r] != 0;
-            RowAcc acc{&P, sbase, r, row0 + r, 0};
-            if (JOIN) FoldProbeRow<WIDE, GEN>(L, sm, act, acc);
-            else FoldRow<WIDE, GEN>(L, sm, act, acc);
-        }
-        __syncthreads();
         if (tid == 0) {
             const int64_t nt = t + int64_t(L.stages) * gridDim.x;
-            if (nt < ntiles && tile_full(nt)) issue(nt, s);
+            if (nt < ntiles && tile_full(nt)) {
+                if (!MbarWaitBounded(&empty[s], phase)) {
+                    SetError(&L.counters->error, DE_WAIT_TIMEOUT);
+                    *reinterpret_cast<volatile unsigned*>(&misc[4]) = 1;
+                } else {
+                    issue(nt, s);
+                }
+            }
         }
     }
-    if (aborted) {
+    __syncthreads();
+    if (aborted || *reinterpret_cast<volatile unsigned*>(&misc[4])) {
         // Let copies already issued land before the CTA's memory goes away.
         if (tid == 0) {
-            for (int s = 0; s < L.stages; ++s) {
-                const long long start = clock64();
-                while (clock64() - start < 1000000) {
-                }
+            const long long start = clock64();
+            while (clock64() - start < 2000000) {
             }
         }
         __syncthreads();
         return;
     }
+    if (JOIN && matched) atomicAdd(&misc[3], matched);
 
-    // Merge the shared table into the global table.
+    // Lane-private accumulators -> shared table (one warp per group state).
     __syncthreads();
-    for (int i = tid; i < sm.S; i += blockDim.x) {
+    if (PRIV) {
+        const int ng = int(min(*reinterpret_cast<volatile unsigned*>(sm.ngid), unsigned(kPrivGroups)));
+        for (int item = tid >> 5; item < ng * P.nstates; item += nwarps) {
+            const int g = item / P.nstates;
+            const StateDesc sd = P.states[item % P.nstates];
+            Contrib c{StateIdentity(sd.kind), 0, 0.0, true};
+            for (int t2 = tid & 31; t2 < bd; t2 += 32) {
+                const uint64_t* w = sm.pacc + (int64_t(g) * P.state_words + sd.word) * bd + t2;
+                const uint64_t lo = w[0];
+                switch (sd.kind) {
+                    case ST_COUNT: case ST_SUM_I64: c.lo += lo; break;
+                    case ST_SUM_I128: {
+                        const uint64_t n = c.lo + lo;
+                        c.hi += w[bd] + (n < c.lo ? 1ull : 0ull);
+                        c.lo = n;
+                        break;
+                    }
+                    case ST_SUM_F64: c.f += __longlong_as_double((long long)lo); break;
+                    case ST_MIN_I64: if ((long long)lo < (long long)c.lo) c.lo = lo; break;
+                    case ST_MAX_I64: if ((long long)lo > (long long)c.lo) c.lo = lo; break;
+                    case ST_MIN_F64: if (lo < c.lo) c.lo = lo; break;
+                    case ST_MAX_F64: if (lo > c.lo) c.lo = lo; break;
+                }
+            }
+            WarpReduceState(sd.kind, true, c);
+            const bool any = sd.kind == ST_SUM_F64 ? c.f != 0.0 : !IsIdentity(sd.kind, c.lo, c.hi);
+            if ((tid & 31) == 0 && any) {
+                uint64_t* w = sm.st + int64_t(sd.word) * sm.S + sm.gid_slot[g];
+                ApplyState(w, w + sm.S, sd.kind, c.lo, c.hi, c.f);
+            }
+        }
+        __syncthreads();
+    }
+
+    // Shared table -> global table.
+    for (int i = tid; i < sm.S; i += bd) {
         const uint64_t key = sm.keys[i];
         if (key == kEmptyKey) continue;
         int is_new = 0;
@@ -648,23 +795,22 @@ __global__ void __launch_bounds__(kAggThreads, 1) AggUpdateKernel(const __grid_c
         }
     }
     __syncthreads();
-    if (tid == 0 && sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
+    if (tid == 0) {
+        if (sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
+        if (JOIN && misc[3]) atomicAdd(&L.counters->matched, (unsigned long long)misc[3]);
+    }
 }
 
 // Index mode: rows named by (row, build row) pairs, global table only.
 template <bool WIDE>
 __global__ void __launch_bounds__(256) AggIndexKernel(const __grid_constant__ AggLaunch L) {
-    __shared__ unsigned misc[4];
+    unsigned* misc = reinterpret_cast<unsigned*>(DynSmem() + L.off_misc);
     if (threadIdx.x == 0) misc[1] = 0;
     __syncthreads();
-    SmemTable sm{nullptr, nullptr, misc, misc + 1, 0, 0};
-    const int64_t warps = int64_t(gridDim.x) * (blockDim.x / 32);
-    const int64_t wid = int64_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
-    for (int64_t b = wid * 32; b < L.nindex; b += warps * 32) {
-        const int64_t i = b + LaneId();
-        const bool act = i < L.nindex;
-        RowAcc acc{&L.P, nullptr, 0, act ? L.index[2 * i] : 0, act ? L.index[2 * i + 1] : 0};
-        FoldRow<WIDE, true>(L, sm, act, acc);
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < L.nindex;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        RowAcc acc{&L.P, nullptr, 0, L.index[2 * i], L.index[2 * i + 1], -1, 0};
+        FoldRow<WIDE, true, false>(L, acc);
     }
     __syncthreads();
     if (threadIdx.x == 0 && misc[1]) atomicAdd(&L.counters->new_groups, (unsigned long long)misc[1]);
@@ -1024,21 +1170,25 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
     L.join = a.join;
     L.jk = a.jkey;
     L.jt = a.jt;
+    L.inline_slot = a.join ? a.inline_slot : -1;
     const bool wide = a.table.wide != 0;
 
     if (a.index) {
         if (a.nindex == 0) return;
         const int blocks = int(std::min<int64_t>((a.nindex + 255) / 256, int64_t(g_sms) * 8));
+        // The index kernel keeps only its counters in shared memory.
+        L.off_misc = 0;
+        L.smem_slots = 0;
         ProfileBegin(s, "agg_update_index", a.nindex);
-        if (wide) AggIndexKernel<true><<<blocks, 256, 0, s>>>(L);
-        else AggIndexKernel<false><<<blocks, 256, 0, s>>>(L);
+        if (wide) AggIndexKernel<true><<<blocks, 256, 64, s>>>(L);
+        else AggIndexKernel<false><<<blocks, 256, 64, s>>>(L);
         ProfileEnd(s);
         CountLaunch();
         return;
     }
     if (a.nrows == 0) return;
 
-    // Tile geometry: bulk-stage every aligned, non-build column.
+    // Stage every aligned scan column (not build-side ones) through shared memory.
     int bytes_per_row = 0;
     bool any = false;
     for (int c = 0; c < L.P.ncols; ++c) {
@@ -1055,43 +1205,60 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
         bytes_per_row += 1;
         any = true;
     }
-    int T = 1024;
-    if (bytes_per_row > 0) {
-        const int target = 40 * 1024;
-        T = 256;
-        while (T * 2 * bytes_per_row <= target && T < 4096) T *= 2;
-    }
-    L.tile_rows = T;
-    L.stages = 3;
-    int off = 0;
-    for (int c = 0; c < L.P.ncols; ++c) {
-        ColDesc& cd = L.P.cols[c];
-        if (!cd.stage) continue;
-        cd.smem_off = off;
-        off += int(Align(int64_t(T) * cd.width, 16));
-    }
-    L.sel_off = -1;
-    if (sel_staged) {
-        L.sel_off = off;
-        off += int(Align(T, 16));
-    }
-    L.stage_bytes = off;
-    L.any_staged = any ? 1 : 0;
-    if (!any) L.stages = 1;
-    L.off_bars = int(Align(int64_t(L.stages) * L.stage_bytes, 16));
-    L.off_bases = L.off_bars + 8 * L.stages;
-    L.off_bases = int(Align(L.off_bases, 16));
-    L.off_misc = L.off_bases + 8 * (kMaxCols + 1);
-    L.off_skeys = int(Align(L.off_misc + 16, 128));
-    const size_t budget = g_smem_optin - 1024;
     const int sw = L.P.state_words;
-    int S = wide ? 0 : a.smem_slots;
-    while (S > 0 && size_t(L.off_skeys) + size_t(S) * (1 + sw) * 8 > budget) S >>= 1;
-    if (S < 32) S = 0;
+    const size_t budget = g_smem_optin - 1024;
+    bool priv = a.priv && !wide;
+    int S = wide ? 0 : (priv ? 64 : a.smem_slots);
+    const size_t pacc_bytes = size_t(kPrivGroups) * sw * kAggThreads * 8;
+    auto layout = [&](int T, int stages, int S_) -> size_t {
+        int off = 0;
+        for (int c = 0; c < L.P.ncols; ++c) {
+            ColDesc& cd = L.P.cols[c];
+            if (!cd.stage) continue;
+            cd.smem_off = off;
+            off += int(Align(int64_t(T) * cd.width, 16));
+        }
+        L.sel_off = -1;
+        if (sel_staged) {
+            L.sel_off = off;
+            off += int(Align(T, 16));
+        }
+        L.stage_bytes = off;
+        L.stages = any ? stages : 1;
+        L.tile_rows = T;
+        L.off_bars = int(Align(int64_t(L.stages) * L.stage_bytes, 16));
+        L.off_misc = L.off_bars + 16 * L.stages;
+        L.off_skeys = int(Align(L.off_misc + 64, 128));
+        L.off_sst = L.off_skeys + S_ * 8;
+        L.off_gid = L.off_sst + S_ * sw * 8;
+        L.off_pacc = int(Align(L.off_gid + S_ * 4, 16));
+        return size_t(L.off_pacc) + (priv ? pacc_bytes : 0);
+    };
+    int T = 1024, stages = 3;
+    if (bytes_per_row > 0) {
+        T = 256;
+        while (T * 2 * bytes_per_row <= 40 * 1024 && T < 4096) T *= 2;
+    }
+    // Shrink tiles, then stages, then the private accumulators, until it fits.
+    for (;;) {
+        if (layout(T, stages, S) <= budget) break;
+        if (priv && S > 64) { S >>= 1; continue; }
+        if (!priv && S > 256) { S >>= 1; continue; }
+        if (T > 256) { T >>= 1; continue; }
+        if (stages > 2) { stages--; continue; }
+        if (priv) { priv = false; S = a.smem_slots; T = 1024; stages = 3; continue; }
+        if (S > 0) { S >>= 1; if (S < 32) S = 0; continue; }
+        break;
+    }
+    if (!priv && !wide) {
+        // Grow the shared table into whatever shared memory is left.
+        while (S > 0 && S < a.smem_slots && layout(T, stages, S * 2) <= budget) S *= 2;
+    }
+    const size_t smem_bytes = layout(T, stages, S);
     L.smem_slots = S;
     L.smem_limit = S / 2;
-    L.off_sst = L.off_skeys + S * 8;
-    const size_t smem_bytes = size_t(L.off_sst) + size_t(S) * sw * 8;
+    L.priv = priv;
+    L.any_staged = any ? 1 : 0;
 
     const int64_t ntiles = (a.nrows + T - 1) / T;
     const int grid = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, g_sms)));
@@ -1102,16 +1269,20 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
         SetSmem(kernel, smem_bytes);
         kernel<<<grid, kAggThreads, smem_bytes, s>>>(L);
     };
-    const int variant = (wide ? 4 : 0) | (a.join ? 2 : 0) | (gen ? 1 : 0);
+    const int variant = (wide ? 8 : 0) | (a.join ? 4 : 0) | (gen ? 2 : 0) | (priv ? 1 : 0);
     switch (variant) {
-        case 0: launch(AggUpdateKernel<false, false, false>); break;
-        case 1: launch(AggUpdateKernel<false, false, true>); break;
-        case 2: launch(AggUpdateKernel<false, true, false>); break;
-        case 3: launch(AggUpdateKernel<false, true, true>); break;
-        case 4: launch(AggUpdateKernel<true, false, false>); break;
-        case 5: launch(AggUpdateKernel<true, false, true>); break;
-        case 6: launch(AggUpdateKernel<true, true, false>); break;
-        default: launch(AggUpdateKernel<true, true, true>); break;
+        case 0: launch(AggUpdateKernel<false, false, false, false>); break;
+        case 1: launch(AggUpdateKernel<false, false, false, true>); break;
+        case 2: launch(AggUpdateKernel<false, false, true, false>); break;
+        case 3: launch(AggUpdateKernel<false, false, true, true>); break;
+        case 4: launch(AggUpdateKernel<false, true, false, false>); break;
+        case 5: launch(AggUpdateKernel<false, true, false, true>); break;
+        case 6: launch(AggUpdateKernel<false, true, true, false>); break;
+        case 7: launch(AggUpdateKernel<false, true, true, true>); break;
+        case 8: case 9: launch(AggUpdateKernel<true, false, false, false>); break;
+        case 10: case 11: launch(AggUpdateKernel<true, false, true, false>); break;
+        case 12: case 13: launch(AggUpdateKernel<true, true, false, false>); break;
+        default: launch(AggUpdateKernel<true, true, true, false>); break;
     }
     ProfileEnd(s);
     CountLaunch();

@@ -223,8 +223,8 @@ QDB_HD inline int GCmp(const GNode& na, const GVal& a, const GNode& nb, const GV
 // Evaluates nodes [0, root].  Returns false on a row error (division by
 // zero); `nulls` gets one bit per node.
 template <class Acc>
-QDB_HD inline bool EvalGeneric(const GProg& g, int root, const int64_t* list, const Acc& acc,
-                               GVal* v, uint64_t& nulls) {
+QDB_HD QDB_NOINLINE bool EvalGeneric(const GProg& g, int root, const int64_t* list, const Acc& acc,
+                                     GVal* v, uint64_t& nulls) {
     nulls = 0;
     for (int k = 0; k <= root; ++k) {
         const GNode& n = g.nodes[k];

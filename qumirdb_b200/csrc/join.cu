@@ -62,8 +62,8 @@ __device__ __forceinline__ uint64_t PackKeyCols(const A& a, int64_t r, bool& nul
 
 __global__ void JoinInitKernel(uint64_t* entries, int64_t capacity) {
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < capacity; i += int64_t(gridDim.x) * blockDim.x) {
-        entries[2 * i] = kEmptyKey;
-        entries[2 * i + 1] = 0;
+        reinterpret_cast<ulonglong2*>(entries)[2 * i] = make_ulonglong2(kEmptyKey, 0);
+        reinterpret_cast<ulonglong2*>(entries)[2 * i + 1] = make_ulonglong2(0, 0);
     }
 }
 
@@ -72,17 +72,20 @@ __global__ void __launch_bounds__(256) JoinBuildKernel(const __grid_constant__ J
         bool null = false;
         const uint64_t key = PackKeyCols(a, r, null);
         if (null) continue;
+        const uint64_t pay = a.pay0 ? uint64_t(a.pay0[r]) : 0;
         if (a.jkey.full64 && key == kEmptyKey) {
             const unsigned long long k = atomicAdd(a.nspecial, 1ull);
-            a.special_rows[k] = a.row_base + r;
+            a.special_rows[2 * k] = a.row_base + r;
+            a.special_rows[2 * k + 1] = int64_t(pay);
             continue;
         }
         uint64_t i = Fmix64(key) & a.mask;
         for (uint64_t p = 0; p <= a.mask; ++p) {
-            auto* kp = reinterpret_cast<unsigned long long*>(&a.entries[2 * i]);
+            auto* kp = reinterpret_cast<unsigned long long*>(&a.entries[4 * i]);
             if (*reinterpret_cast<volatile unsigned long long*>(kp) == kEmptyKey &&
                 atomicCAS(kp, kEmptyKey, key) == kEmptyKey) {
-                a.entries[2 * i + 1] = uint64_t(a.row_base + r);
+                a.entries[4 * i + 1] = uint64_t(a.row_base + r);
+                a.entries[4 * i + 2] = pay;
                 break;
             }
             i = (i + 1) & a.mask;
@@ -109,23 +112,23 @@ __global__ void __launch_bounds__(256) JoinProbePairsKernel(const __grid_constan
             int64_t brow = -1;
             if (act && !special) {
                 while (probes <= int64_t(a.jt.mask)) {
-                    const uint64_t k = a.jt.entries[2 * i];
+                    const ulonglong2 e = *reinterpret_cast<const ulonglong2*>(&a.jt.entries[4 * i]);
                     ++probes;
-                    if (k == kEmptyKey) {
+                    if (e.x == kEmptyKey) {
                         act = false;
                         break;
                     }
                     const uint64_t here = i;
                     i = (i + 1) & a.jt.mask;
-                    if (k == key) {
-                        brow = int64_t(a.jt.entries[2 * here + 1]);
+                    if (e.x == key) {
+                        brow = int64_t(e.y);
                         pos = int64_t(here);
                         break;
                     }
                 }
                 if (probes > int64_t(a.jt.mask)) act = false;
             } else if (special) {
-                if (sp < a.jt.nspecial) brow = a.jt.special_rows[sp++];
+                if (sp < a.jt.nspecial) brow = a.jt.special_rows[2 * sp++];
                 else act = false;
             }
             const bool emit = brow >= 0;

@@ -237,8 +237,8 @@ bool Build(const qdb_gpu_program* prog, ArenaState* a, void* table) {
     int64_t cap = 1024;
     while (cap < a->rows * 2) cap *= 2;
     t->capacity = cap;
-    t->entries = static_cast<uint64_t*>(DevAlloc(size_t(cap) * 16, t->s));
-    t->special = static_cast<int64_t*>(DevAlloc(size_t(std::max<int64_t>(a->rows, 1)) * 8, t->s));
+    t->entries = static_cast<uint64_t*>(DevAlloc(size_t(cap) * 32, t->s));
+    t->special = static_cast<int64_t*>(DevAlloc(size_t(std::max<int64_t>(a->rows, 1)) * 16, t->s));
     t->nspecial_d = static_cast<unsigned long long*>(DevAlloc(8, t->s));
     if (!t->entries || !t->special || !t->nspecial_d) {
         DestroyTable(t);
@@ -257,6 +257,10 @@ bool Build(const qdb_gpu_program* prog, ArenaState* a, void* table) {
     }
     b.jkey = J.build_jk;
     b.nrows = a->rows;
+    // The first 8-byte payload column rides in the entry: a probe reads one
+    // 32-byte sector for key, row and that value.
+    b.pay0 = (!a->payload.empty() && a->payload[0].width == 8) ? reinterpret_cast<const int64_t*>(a->payload[0].data)
+                                                                : nullptr;
     b.entries = t->entries;
     b.mask = uint64_t(cap - 1);
     b.special_rows = t->special;
@@ -602,9 +606,15 @@ int64_t qdb_gpu_join_aggregate_probe(const qdb_gpu_program* prog, void* arena, v
         cd.mask_off = 0;
         cd.bit_off = 0;
     }
+    // The slot of the first payload column reads the entry's payload word.
+    int inline_slot = -1;
+    if (!J.payload.empty() && a->payload[0].width == 8) {
+        const int s0 = prog->agg.cols.slot_of[np];
+        if (s0 >= 0 && (plan.cols[s0].kind == LK_SIGNED || plan.cols[s0].kind == LK_F64)) inline_slot = s0;
+    }
     const int64_t before = AggStateMatched(st);
     const JTableDev jt = t->dev();
-    if (!AggRun(st, plan, batch->RowCount, &J.agg_jk, &jt)) return -1;
+    if (!AggRun(st, plan, batch->RowCount, &J.agg_jk, &jt, inline_slot)) return -1;
     AggMirrorHeader(ht, st, prog->agg.plan);
     return AggStateMatched(st) - before;
 }

@@ -43,8 +43,9 @@ struct JoinKeyPlan {
     uint8_t is_float[4] = {};
 };
 
-// Built join table: 2 words per slot (packed key, build row), EMPTY key =
-// kEmptyKey; rows whose key equals kEmptyKey are listed separately.
+// Built join table: 4 words (32 bytes, one sector) per slot: packed key,
+// arena row, first payload word, unused; EMPTY key = kEmptyKey.  Rows whose
+// key equals kEmptyKey are listed separately as (arena row, payload word).
 struct JTableDev {
     const uint64_t* entries = nullptr;
     uint64_t mask = 0;
@@ -64,6 +65,8 @@ struct AggUpdateArgs {
     uint64_t* spill = nullptr;
     int64_t spill_cap = 0;
     int32_t smem_slots = 0;            // 0 disables the shared-memory tier
+    bool priv = false;                 // lane-private accumulators for the first groups
+    int32_t inline_slot = -1;          // fused join: slot served by the entry's payload word
     bool join = false;
     JoinKeyPlan jkey;
     JTableDev jt;
@@ -104,7 +107,8 @@ struct JoinBuildArgs {
     uint8_t key_signed[4];
     JoinKeyPlan jkey;
     int64_t nrows;
-    uint64_t* entries;      // capacity * 2 words
+    const int64_t* pay0;    // first 8-byte payload column (stored in the entry) or nullptr
+    uint64_t* entries;      // capacity * 4 words
     uint64_t mask;
     int64_t* special_rows;
     unsigned long long* nspecial;

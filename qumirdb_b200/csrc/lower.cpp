@@ -719,6 +719,15 @@ AggLowering LowerAggregate(const qdb_aggregate_spec& s, int probe_cols, const st
     if (s.n_aggs > kMaxAggs) throw LowerError("too many aggregates for one device table");
     int words = 0;
     auto add_state = [&](uint8_t kind, uint8_t src, uint8_t idx) -> int {
+        // A COUNT over a value that is never NULL is COUNT(*): share one word.
+        if (kind == ST_COUNT && src == VS_SOP && p.values[idx].null_cols == 0) {
+            src = VS_NONE;
+            idx = 0;
+        }
+        for (int s = 0; s < p.nstates; ++s) {
+            const StateDesc& o = p.states[s];
+            if (o.kind == kind && o.src == src && o.idx == idx && (kind == ST_COUNT || src != VS_NONE)) return s;
+        }
         if (p.nstates >= kMaxStates) throw LowerError("too many aggregate states");
         StateDesc& st = p.states[p.nstates];
         st.kind = kind;

@@ -6,8 +6,10 @@
 
 #if defined(__CUDACC__)
 #define QDB_HD __host__ __device__
+#define QDB_NOINLINE __noinline__
 #else
 #define QDB_HD
+#define QDB_NOINLINE
 #endif
 
 namespace qdb {

@@ -222,13 +222,9 @@ struct AggTableState {
 
 namespace {
 
+// Slots are 16-byte aligned; a 48-byte slot still spans two 32-byte sectors.
 int SlotWords(const AggPlan& p, bool wide) {
-    int w = (wide ? 1 + p.key_words : 1) + p.state_words;
-    if (w <= 16) {
-        int q = 1;
-        while (q < w) q <<= 1;
-        return q;
-    }
+    const int w = (wide ? 1 + p.key_words : 1) + p.state_words;
     return (w + 1) & ~1;
 }
 
@@ -310,7 +306,7 @@ AggTableState* AggStateCreate(const AggPlan& p, int64_t capacity_hint, int64_t e
     st->s = s;
     st->expected = expected;
     int64_t cap = std::max<int64_t>(1024, NextPow2(std::max<int64_t>(capacity_hint, 1)));
-    if (expected > 0) cap = std::max(cap, NextPow2(expected * 2));
+    if (expected > 0) cap = std::max(cap, NextPow2(expected + expected / 2));
     if (cudaMallocHost(&st->hc, sizeof(AggCounters)) != cudaSuccess) {
         delete st;
         SetErr("pinned allocation failed");
@@ -354,8 +350,12 @@ void AggStateDestroy(AggTableState* st) {
 
 // Runs the fused kernel over `rows` rows of a resolved plan, then replays
 // deferred rows and spilled entries after growing the table.
-bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyPlan* jk, const JTableDev* jt) {
+bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyPlan* jk, const JTableDev* jt,
+            int inline_slot) {
     if (!EnsureBuffers(st, plan, rows)) return false;
+    // Few expected groups (or none): fold the first groups of each CTA into
+    // lane-private accumulators.
+    const bool priv = plan.nkeyparts == 0 || (st->expected > 0 && st->expected <= 64);
     for (int64_t begin = 0; begin < rows || (rows == 0 && begin == 0); begin += kChunkRows) {
         const int64_t n = std::min<int64_t>(kChunkRows, rows - begin);
         if (n <= 0) break;
@@ -370,10 +370,12 @@ bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyP
         a.spill = st->spill;
         a.spill_cap = st->spill_cap;
         a.smem_slots = st->smem_slots;
+        a.priv = priv;
         if (jk) {
             a.join = true;
             a.jkey = *jk;
             a.jt = *jt;
+            a.inline_slot = inline_slot;
         }
         ResetCounters(st);
         AggUpdate(a, st->s);

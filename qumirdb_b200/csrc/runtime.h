@@ -37,7 +37,8 @@ AggPlan OffsetPlan(const AggPlan& P, int64_t begin);
 struct AggTableState;
 AggTableState* AggStateCreate(const AggPlan& p, int64_t capacity_hint, int64_t expected, cudaStream_t s);
 void AggStateDestroy(AggTableState* st);
-bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyPlan* jk, const JTableDev* jt);
+bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyPlan* jk, const JTableDev* jt,
+            int inline_slot = -1);
 int64_t AggFinish(AggTableState* st, const AggLowering& lw, uint32_t flags, qdb_rowset* out);
 int64_t AggStateGroups(const AggTableState* st);
 int64_t AggStateMatched(const AggTableState* st);
