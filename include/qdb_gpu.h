@@ -386,6 +386,38 @@ int64_t qdb_gpu_top_k_select(const qdb_gpu_program* program, qdb_rowset* store,
                              int64_t* row_ids, int64_t size, int64_t limit);
 
 /* ------------------------------------------------------------------------ */
+/* Aggregation without device allocation.                                   */
+/* ------------------------------------------------------------------------ */
+
+/* No counterpart in the reference: an addition for embedders that cannot     */
+/* allocate device memory while a query runs — an engine that hands the GPU   */
+/* a fixed memory budget up front, a caller recording work into a CUDA graph, */
+/* or a process whose device allocator belongs to another runtime.           */
+/*                                                                           */
+/* Runs one whole aggregate of an aggregate program (table set-up, the fused  */
+/* filter -> project -> aggregate over `batch`, finalize) and writes the      */
+/* groups into the caller's output columns.  Every column, mask and the       */
+/* selection of `batch` must already be in device memory (nothing is copied), */
+/* and out_columns[k].Data must be a device buffer of out_capacity values of  */
+/* output column k (Mask, when set, a device bitmap of out_capacity bits;     */
+/* Offsets, when set on a one-byte string column, out_capacity + 1 int32).   */
+/* Returns the group count, or -1 (see qdb_gpu_last_error) when an input is   */
+/* not in device memory, the groups exceed out_capacity, or the state does    */
+/* not fit the scratch.                                                       */
+/*                                                                           */
+/* Table, counters and finalize scratch live in one file-scope device array   */
+/* of QDB_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds      */
+/* until the process exits; it fits one-word group keys and at most 2^19     */
+/* groups (fewer for wide aggregate states).  The first call on a device      */
+/* looks up that array's device address, so make it before any stream        */
+/* capture.  Calls share the array: each clears what it uses, and calls whose */
+/* work overlaps on the GPU race and must be serialised by the caller.  It    */
+/* runs on the stream set by qdb_gpu_set_stream.                              */
+#define QDB_NOALLOC_SCRATCH_BYTES (16u << 20)
+int64_t qdb_gpu_agg_run_noalloc(const qdb_gpu_program* program, const qdb_rowset* batch,
+                                qdb_column* out_columns, int64_t out_capacity);
+
+/* ------------------------------------------------------------------------ */
 /* Runtime.                                                                  */
 /* ------------------------------------------------------------------------ */
 

@@ -29,6 +29,8 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "common.cuh"
 #include "eval.h"
@@ -1352,6 +1354,143 @@ void AggFinalize(const AggPlan& p, const OutputPlan& out, const GTableDev& t, Ag
     FinWriteKernel<<<int(blocks), kFinThreads, 0, s>>>(L);
     ProfileEnd(s);
     CountLaunch(3);
+}
+
+// ---------------------------------------------------------------------------
+// Aggregation without device allocation.
+//
+// Some embedders cannot allocate device memory while a query runs: an engine
+// that hands the GPU a fixed memory budget up front, a caller recording work
+// into a CUDA graph, or a process whose allocator belongs to another runtime.
+// For them one whole aggregate (table init, fused update, finalize) runs in
+// this file-scope scratch array instead of cudaMalloc'd buffers.  Every GPU
+// that loads the library holds it until the process exits.  All calls share
+// it and it keeps the last call's contents, so each call clears the counters
+// and the table it uses; two calls whose work overlaps on the GPU (different
+// streams, or different host threads) race on it and must be serialised by
+// the caller.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device (the host-side symbol is only a stand-in for it).
+void* NoAllocScratch(std::string& err) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        err = "no current CUDA device";
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            err = std::string("cudaGetSymbolAddress of the scratch array failed: ") + cudaGetErrorString(e);
+            return nullptr;
+        }
+        g_noalloc_addr[dev] = p;
+    }
+    return g_noalloc_addr[dev];
+}
+
+}  // namespace
+
+int64_t AggRunNoAlloc(const AggPlan& plan, const OutputPlan& out, int64_t nrows, AggOutputCol* cols, int ncols,
+                      int64_t out_capacity, bool priv, cudaStream_t s, std::string& err) {
+    EnsureDeviceInfo();
+    unsigned char* base = static_cast<unsigned char*>(NoAllocScratch(err));
+    if (!base) return -1;
+    if (plan.key_words > 1) {
+        err = "the no-allocation aggregate serves one-word group keys only";
+        return -1;
+    }
+    // Scratch layout: counters | finalize block counts | spill | table.
+    const int sw = plan.state_words;
+    const int slot_words = (1 + sw + 1) & ~1;
+    const int S = priv ? 64 : 256;
+    const int64_t spill_cap = int64_t(g_sms) * S;
+    const size_t counters_bytes = 256;
+    const size_t spill_bytes = size_t(spill_cap) * (1 + sw) * 8;
+    int64_t cap = int64_t(1) << 20;
+    auto table_bytes = [&](int64_t c) { return size_t(c + 1) * slot_words * 8; };
+    auto fin_bytes = [&](int64_t c) { return size_t((c + 1 + kFinChunk - 1) / kFinChunk) * 8; };
+    while (cap > 1024 && counters_bytes + fin_bytes(cap) + spill_bytes + table_bytes(cap) > kNoAllocScratchBytes) {
+        cap >>= 1;
+    }
+    if (counters_bytes + fin_bytes(cap) + spill_bytes + table_bytes(cap) > kNoAllocScratchBytes) {
+        err = "aggregate state too wide for the no-allocation scratch of " +
+              std::to_string(kNoAllocScratchBytes) + " bytes";
+        return -1;
+    }
+    auto* counters = reinterpret_cast<AggCounters*>(base);
+    auto* block_counts = reinterpret_cast<unsigned long long*>(base + counters_bytes);
+    auto* spill = reinterpret_cast<uint64_t*>(base + counters_bytes + fin_bytes(cap));
+    GTableDev t;
+    t.slots = reinterpret_cast<uint64_t*>(base + counters_bytes + fin_bytes(cap) + spill_bytes);
+    t.capacity = cap;
+    t.slot_words = slot_words;
+    t.key_off = 0;
+    t.state_off = 1;
+    t.wide = 0;
+
+    cudaMemsetAsync(counters, 0, sizeof(AggCounters), s);
+    AggInitTable(plan, t, s);
+    int64_t groups = 0;
+    if (plan.nkeyparts == 0) {
+        // The keyless group exists before any row: key 0 at its home slot.
+        const int64_t slot = int64_t(Fmix64(0) & uint64_t(cap - 1));
+        cudaMemsetAsync(t.slots + slot * t.slot_words + t.key_off, 0, 8, s);
+        groups = 1;
+    }
+    AggUpdateArgs a;
+    a.plan = &plan;
+    a.nrows = nrows;
+    a.table = t;
+    a.counters = counters;
+    a.deferred = nullptr;   // a row that does not fit is an error here, not a replay
+    a.deferred_cap = 0;
+    a.spill = spill;
+    a.spill_cap = spill_cap;
+    a.smem_slots = S;
+    a.priv = priv;
+    AggUpdate(a, s);
+    AggCounters hc;
+    cudaMemcpyAsync(&hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+        err = std::string("no-allocation aggregate: ") + cudaGetErrorString(cudaGetLastError());
+        return -1;
+    }
+    groups += int64_t(hc.new_groups);
+    if (hc.deferred || hc.spilled || hc.error == DE_DEFER_FULL || hc.error == DE_SPILL_FULL) {
+        err = "more groups than the no-allocation table holds (" + std::to_string(cap / 2) + " at most)";
+        return -1;
+    }
+    if (hc.error) {
+        err = "no-allocation aggregate: device error " + std::to_string(hc.error);
+        return -1;
+    }
+    if (groups > cap / 2) {
+        err = "more groups than the no-allocation table holds (" + std::to_string(cap / 2) + " at most)";
+        return -1;
+    }
+    if (groups > out_capacity) {
+        err = "output capacity " + std::to_string(out_capacity) + " is below the group count " +
+              std::to_string(groups);
+        return -1;
+    }
+    AggFinalize(plan, out, t, cols, ncols, groups, block_counts, &counters->error, s);
+    int derr = 0;
+    cudaMemcpyAsync(&derr, &counters->error, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess || derr) {
+        err = "no-allocation aggregate finalize failed";
+        return -1;
+    }
+    return groups;
 }
 
 }  // namespace qdb

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
 
 #include "plan.h"
 
@@ -96,6 +97,12 @@ struct OutputPlan;
 size_t AggFinalizeScratch(const GTableDev& t);
 void AggFinalize(const AggPlan& p, const OutputPlan& out, const GTableDev& t, AggOutputCol* cols,
                  int ncols, int64_t groups, void* scratch, int* err, cudaStream_t s);
+
+// One whole aggregate in the file-scope scratch array of agg.cu (no device
+// allocation): returns the group count, or -1 with `err` set.
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
+int64_t AggRunNoAlloc(const AggPlan& plan, const OutputPlan& out, int64_t nrows, AggOutputCol* cols, int ncols,
+                      int64_t out_capacity, bool priv, cudaStream_t s, std::string& err);
 
 // ---- join ----
 struct JoinBuildArgs {
