@@ -361,6 +361,16 @@ int64_t qdb_gpu_jr_materialize(const qdb_gpu_program* program, void* pairs,
                                qdb_rowset* stream, int64_t start,
                                int64_t limit, qdb_rowset* out);
 
+/* Release of device state behind caller-owned state buffers.  The engine    */
+/* keeps these states in its task heap and drops them with the task          */
+/* (qdb/exec/row_join_exec.cpp:35-46 frees only row sets); a device library  */
+/* has no such heap, so a binding calls these where the processor is         */
+/* destroyed.  No reference counterpart.  Each pointer may be NULL; the      */
+/* buffers are zeroed and may be initialised again.  Frees are ordered on    */
+/* the library stream.                                                       */
+void qdb_gpu_agg_release(void* ht);
+void qdb_gpu_jr_release(void* arena, void* table, void* scratch, void* pairs);
+
 /* Probe of a fused join-aggregate program: probes `batch` against the built */
 /* arena/table and folds the joined rows into the aggregate state `ht`.      */
 /* Returns the matched pair count, < 0 on failure.                           */

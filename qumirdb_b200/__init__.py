@@ -330,6 +330,17 @@ class Aggregate:
             raise QdbError(f"aggregate finish failed: {last_error()}")
         return out
 
+    def release(self) -> None:
+        """Frees the device table of an aggregate that was not finished."""
+        if self.ht is not None:
+            lib().qdb_gpu_agg_release(self.ht)
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
 
 class RowJoin:
     """The engine's TRowJoinProcessor state: arena, table, scratch, pairs."""
@@ -379,6 +390,16 @@ class RowJoin:
         if n < 0:
             raise QdbError(f"join aggregate probe failed: {last_error()}")
         return n
+
+    def release(self) -> None:
+        """Frees the arena, table and pair buffer on the device."""
+        lib().qdb_gpu_jr_release(self.arena, self.table, self.scratch, self.pairs)
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
 
 
 def profile(on: bool) -> None:

@@ -116,6 +116,8 @@ SIGNATURES = {
     "qdb_gpu_hash": (BOOLC, [P, PRS, P]),
     "qdb_gpu_jr_dispatch": (BOOLC, [P, P, P, P, P, PRS, CI64]),
     "qdb_gpu_jr_materialize": (CI64, [P, P, PRS, CI64, CI64, PRS]),
+    "qdb_gpu_agg_release": (None, [P]),
+    "qdb_gpu_jr_release": (None, [P, P, P, P]),
     "qdb_gpu_join_aggregate_probe": (CI64, [P, P, P, P, PRS]),
     "qdb_gpu_sort_run": (CI64, [P, PRS, P, P, P, CI64, P, P, BOOLC, CI64, CI64, PRS]),
     "qdb_gpu_top_k_select": (CI64, [P, PRS, P, CI64, CI64]),

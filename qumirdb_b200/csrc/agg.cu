@@ -34,6 +34,7 @@
 
 #include "common.cuh"
 #include "eval.h"
+#include "jtable.cuh"
 #include "kernels.h"
 #include "lower.h"
 
@@ -81,6 +82,7 @@ struct AggLaunch {
     int32_t join;
     JoinKeyPlan jk;
     JTableDev jt;
+    FastPlan F;               // typed row shape (FAST kernels)
 };
 
 // ---------------------------------------------------------------------------
@@ -504,6 +506,140 @@ __device__ __noinline__ void FoldRow(const AggLaunch& L, RowAcc acc) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Typed row fold (FastPlan shape): columns loaded once as int64, 64-bit
+// predicates, products in 64 or 128 bits from 64-bit factors.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int64_t LoadI64(const AggPlan& P, const RowAcc& a, int slot) {
+    const ColDesc& cd = P.cols[slot];
+    const char* p = a.Ptr(slot);
+    const bool u = cd.kind == LK_UNSIGNED;
+    switch (cd.width) {
+        case 1: return u ? int64_t(*reinterpret_cast<const uint8_t*>(p)) : int64_t(*reinterpret_cast<const int8_t*>(p));
+        case 2: return u ? int64_t(*reinterpret_cast<const uint16_t*>(p)) : int64_t(*reinterpret_cast<const int16_t*>(p));
+        case 4: return u ? int64_t(*reinterpret_cast<const uint32_t*>(p)) : int64_t(*reinterpret_cast<const int32_t*>(p));
+        default: return *reinterpret_cast<const int64_t*>(p);
+    }
+}
+
+__device__ __forceinline__ int64_t Sel(const int64_t (&x)[kFastCols], int k) {
+    int64_t v = x[0];
+#pragma unroll
+    for (int j = 1; j < kFastCols; ++j) v = k == j ? x[j] : v;
+    return v;
+}
+
+// (hi:lo) * b mod 2^128 with b sign-extended.
+__device__ __forceinline__ void Mul128x64(uint64_t& lo, uint64_t& hi, int64_t b) {
+    const uint64_t bl = uint64_t(b);
+    const uint64_t nlo = lo * bl;
+    const uint64_t nhi = __umul64hi(lo, bl) + hi * bl - (b < 0 ? lo : 0);
+    lo = nlo;
+    hi = nhi;
+}
+
+template <bool PRIV>
+__device__ __noinline__ void FoldRowFast(const AggLaunch& L, RowAcc acc) {
+    const SmemTable sm = MakeSmem(L, false, PRIV);
+    const AggPlan& P = L.P;
+    const FastPlan& F = L.F;
+    int64_t x[kFastCols];
+#pragma unroll
+    for (int k = 0; k < kFastCols; ++k) x[k] = k < F.ncols ? LoadI64(P, acc, F.col_slot[k]) : 0;
+    if (F.natoms) {
+        uint32_t held = 0;
+        for (int j = 0; j < F.natoms; ++j) {
+            const FastAtom& t = F.atoms[j];
+            const int64_t v = Sel(x, t.col);
+            bool ok;
+            if (t.op == AT_BETWEEN) {
+                ok = v >= t.c0 && v <= t.c1;
+            } else if (t.op == AT_IN) {
+                ok = false;
+                for (int q = 0; q < t.list_len; ++q) ok = ok || P.list[t.list_off + q] == v;
+            } else {
+                ok = CmpHolds(t.op, v < t.c0 ? -1 : (v > t.c0 ? 1 : 0));
+            }
+            if (ok) held |= 1u << t.clause;
+        }
+        if (held != F.clause_mask) return;
+    }
+    uint64_t key = 0;
+    for (int j = 0; j < F.nkeys; ++j) {
+        uint64_t v = uint64_t(Sel(x, F.key_col[j]));
+        if (F.key_bits[j] < 64) v &= (1ull << F.key_bits[j]) - 1;
+        key |= v << F.key_shift[j];
+    }
+    int slot = -1;
+    int g = -1;
+    int64_t gslot = -1;
+    const bool special = P.key_full64 && key == kEmptyKey;
+    if (sm.S > 0 && !special) {
+        slot = sm.Find(key);
+        if (PRIV && slot >= 0) g = *reinterpret_cast<volatile int*>(&sm.gid[slot]);
+    }
+    if (slot < 0) {
+        if (special) {
+            gslot = L.T.capacity;
+            unsigned long long* flag = reinterpret_cast<unsigned long long*>(
+                L.T.slots + L.T.capacity * L.T.slot_words + L.T.key_off);
+            if (*reinterpret_cast<volatile unsigned long long*>(flag) == 0 && atomicExch(flag, 1ull) == 0) {
+                atomicAdd(sm.fresh, 1u);
+            }
+        } else {
+            int is_new = 0;
+            gslot = GlobalFind1(L.T, L.cap_mask, key, is_new);
+            if (is_new) atomicAdd(sm.fresh, 1u);
+        }
+        if (gslot < 0) {
+            Defer(L, acc.arow, acc.brow);
+            return;
+        }
+    }
+    const int bd = blockDim.x;
+    uint64_t* gbase = gslot >= 0 ? L.T.slots + gslot * L.T.slot_words + L.T.state_off : nullptr;
+    for (int s = 0; s < F.nstates; ++s) {
+        const FastState& st = F.states[s];
+        uint64_t lo = 1, hi = 0;
+        double fv = 0.0;
+        if (st.kind == ST_SUM_F64 || st.kind == ST_MIN_F64 || st.kind == ST_MAX_F64) {
+            // A double column travels as its raw bits.
+            fv = __longlong_as_double((long long)Sel(x, st.f[0].col));
+            lo = st.kind == ST_SUM_F64 ? 0 : F64Ordered(fv);
+        } else if (st.nf) {
+            const FastFactor& f0 = st.f[0];
+            const int64_t v0 = int64_t(uint64_t(f0.c) + uint64_t(f0.d) * uint64_t(Sel(x, f0.col)));
+            if (!st.wide) {
+                uint64_t v = uint64_t(v0);
+                for (int j = 1; j < st.nf; ++j) {
+                    const FastFactor& f = st.f[j];
+                    v *= uint64_t(f.c) + uint64_t(f.d) * uint64_t(Sel(x, f.col));
+                }
+                lo = v;
+                hi = int64_t(v) < 0 ? ~0ull : 0ull;   // a 64-bit value summed in 128 bits
+            } else {
+                lo = uint64_t(v0);
+                hi = v0 < 0 ? ~0ull : 0ull;
+                for (int j = 1; j < st.nf; ++j) {
+                    const FastFactor& f = st.f[j];
+                    Mul128x64(lo, hi, int64_t(uint64_t(f.c) + uint64_t(f.d) * uint64_t(Sel(x, f.col))));
+                }
+            }
+        }
+        const uint8_t kind = st.kind;
+        if (PRIV && g >= 0) {
+            uint64_t* w = sm.pacc + (int64_t(g) * P.state_words + st.word) * bd + threadIdx.x;
+            PrivFold(w, w + bd, kind, lo, hi, fv);
+        } else if (slot >= 0) {
+            uint64_t* w = sm.st + int64_t(st.word) * sm.S + slot;
+            ApplyState(w, w + sm.S, kind, lo, hi, fv);
+        } else {
+            uint64_t* w = gbase + st.word;
+            ApplyState(w, w + 1, kind, lo, hi, fv);
+        }
+    }
+}
+
 __device__ __forceinline__ uint64_t PackJoinKey(const JoinKeyPlan& jk, const RowAcc& a, bool& null) {
     null = false;
     if (jk.n == 1 && !jk.is_float[0]) {
@@ -526,27 +662,19 @@ __device__ __forceinline__ uint64_t PackJoinKey(const JoinKeyPlan& jk, const Row
     return k;
 }
 
-// Folds every joined row of one probe row whose first probed entry is `e`
-// (key, row) at slot `i`.
+// Folds every joined row of one probe row whose first bucket b (keys `k`)
+// is already loaded.
 template <bool WIDE, bool GEN, bool PRIV>
-__device__ __forceinline__ unsigned FoldMatches(const AggLaunch& L, RowAcc acc, uint64_t key, uint64_t i,
-                                                ulonglong2 e) {
-    unsigned matched = 0;
-    for (int64_t p = 0; p <= int64_t(L.jt.mask); ++p) {
-        if (e.x == kEmptyKey) break;
-        if (e.x == key) {
-            acc.brow = int64_t(e.y);
-            if (acc.inl_slot >= 0) acc.inl = L.jt.entries[4 * i + 2];
-            FoldRow<WIDE, GEN, PRIV>(L, acc);
-            ++matched;
-        }
-        i = (i + 1) & L.jt.mask;
-        e = *reinterpret_cast<const ulonglong2*>(&L.jt.entries[4 * i]);
-    }
-    return matched;
+__device__ __forceinline__ unsigned FoldMatches(const AggLaunch& L, RowAcc acc, uint64_t key, uint64_t b,
+                                                ulonglong2 k) {
+    return VisitMatches(L.jt, key, b, k, [&](uint64_t slot, uint64_t bk, int j) {
+        acc.brow = L.jt.rows[slot];
+        if (acc.inl_slot >= 0) acc.inl = L.jt.buckets[4 * bk + 2 + j];
+        FoldRow<WIDE, GEN, PRIV>(L, acc);
+    });
 }
 
-template <bool WIDE, bool JOIN, bool GEN, bool PRIV>
+template <bool WIDE, bool JOIN, bool GEN, bool PRIV, bool FAST = false>
 __global__ void __launch_bounds__(kAggThreads, 1) AggUpdateKernel(const __grid_constant__ AggLaunch L) {
     unsigned char* smem = DynSmem();
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.off_bars);
@@ -557,6 +685,7 @@ __global__ void __launch_bounds__(kAggThreads, 1) AggUpdateKernel(const __grid_c
     const int tid = threadIdx.x;
     const int bd = blockDim.x;
     const int nwarps = bd >> 5;
+    const int64_t nspecial = (JOIN && L.jt.nspecial) ? int64_t(*L.jt.nspecial) : 0;
 
     if (tid == 0) {
         misc[0] = 0;
@@ -648,7 +777,8 @@ __global__ void __launch_bounds__(kAggThreads, 1) AggUpdateKernel(const __grid_c
                     if (sel && !sel[r]) continue;
                     acc.r = r;
                     acc.arow = row0 + r;
-                    FoldRow<WIDE, GEN, PRIV>(L, acc);
+                    if (FAST) FoldRowFast<PRIV>(L, acc);
+                    else FoldRow<WIDE, GEN, PRIV>(L, acc);
                 }
             } else {
                 for (int rb = tid; rb < nrows; rb += bd * kProbeRows) {
@@ -668,9 +798,9 @@ __global__ void __launch_bounds__(kAggThreads, 1) AggUpdateKernel(const __grid_c
                             key[j] = PackJoinKey(L.jk, acc, null);
                         }
                         ok[j] = ok[j] && !null && !(L.jk.full64 && key[j] == kEmptyKey);
-                        slot[j] = Fmix64(key[j]) & L.jt.mask;
-                        e[j] = make_ulonglong2(kEmptyKey, 0);
-                        if (ok[j]) e[j] = *reinterpret_cast<const ulonglong2*>(&L.jt.entries[4 * slot[j]]);
+                        slot[j] = Fmix64(key[j]) & L.jt.bmask;
+                        e[j] = make_ulonglong2(kEmptyKey, kEmptyKey);
+                        if (ok[j]) e[j] = BucketKeys(L.jt, slot[j]);
                     }
 #pragma unroll 1
                     for (int j = 0; j < kProbeRows; ++j) {
@@ -680,11 +810,11 @@ __global__ void __launch_bounds__(kAggThreads, 1) AggUpdateKernel(const __grid_c
                         acc.arow = row0 + r;
                         if (ok[j]) matched += FoldMatches<WIDE, GEN, PRIV>(L, acc, key[j], slot[j], e[j]);
                         // Keys equal to the empty marker live in a side list.
-                        if (L.jk.full64 && L.jt.nspecial > 0 && (!sel || sel[r])) {
+                        if (L.jk.full64 && nspecial > 0 && (!sel || sel[r])) {
                             bool null = false;
                             const uint64_t k2 = PackJoinKey(L.jk, acc, null);
                             if (!null && k2 == kEmptyKey) {
-                                for (int64_t q = 0; q < L.jt.nspecial; ++q) {
+                                for (int64_t q = 0; q < nspecial; ++q) {
                                     acc.brow = L.jt.special_rows[2 * q];
                                     if (acc.inl_slot >= 0) acc.inl = uint64_t(L.jt.special_rows[2 * q + 1]);
                                     FoldRow<WIDE, GEN, PRIV>(L, acc);
@@ -1272,6 +1402,14 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
         kernel<<<grid, kAggThreads, smem_bytes, s>>>(L);
     };
     const int variant = (wide ? 8 : 0) | (a.join ? 4 : 0) | (gen ? 2 : 0) | (priv ? 1 : 0);
+    if (a.fast && variant <= 1) {
+        L.F = *a.fast;
+        if (priv) launch(AggUpdateKernel<false, false, false, true, true>);
+        else launch(AggUpdateKernel<false, false, false, false, true>);
+        ProfileEnd(s);
+        CountLaunch();
+        return;
+    }
     switch (variant) {
         case 0: launch(AggUpdateKernel<false, false, false, false>); break;
         case 1: launch(AggUpdateKernel<false, false, false, true>); break;

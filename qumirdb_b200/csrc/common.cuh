@@ -60,6 +60,24 @@ __device__ __forceinline__ void BulkG2S(void* dst, const void* src, uint32_t byt
         : "memory");
 }
 
+// L2 policy that evicts first: streamed input then does not displace the
+// tables a kernel keeps resident in L2.
+__device__ __forceinline__ uint64_t EvictFirstPolicy() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+// BulkG2S with an L2 cache policy (EvictFirstPolicy).
+__device__ __forceinline__ void BulkG2SHint(void* dst, const void* src, uint32_t bytes, uint64_t* bar,
+                                            uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::
+            "r"(SmemAddr(dst)),
+        "l"(src), "r"(bytes), "r"(SmemAddr(bar)), "l"(policy)
+        : "memory");
+}
+
 __device__ __forceinline__ bool MbarTryWait(uint64_t* bar, uint32_t phase) {
     uint32_t ok;
     asm volatile(

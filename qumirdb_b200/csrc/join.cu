@@ -1,19 +1,22 @@
 // join.cu — equi-join hash build and pair-emitting probe for sm_100a.
 //
 // The build side (the row arena, in append order) is indexed by an
-// open-addressing multi-map of 16-byte entries (packed key, arena row): every
-// arena row claims its own entry with one 64-bit CAS, so equal keys occupy
-// several entries along one probe sequence.  Capacity is a power of two of at
-// least twice the rows (load <= 1/2, as the row table sizes itself,
+// open-addressing multi-map of two-slot buckets, one 32-byte sector each
+// (keys, first payload words; layout in kernels.h JTableDev): every arena row
+// claims its own slot with one 64-bit CAS, so equal keys occupy several slots
+// along one bucket sequence.  Slots are a power of two of at least twice the
+// rows (load <= 1/2, as the row table sizes itself,
 // qdb/kernel/row_table.oz:140-166); a config-sized build of ~400K rows is a
-// 16 MB table that stays resident in the 126 MB L2 while the probe streams.
-// A probe row walks its sequence until an empty entry and emits one
-// (probe row, arena row) pair per equal key (jr_probe_candidates,
+// 16 MB bucket array that stays resident in the 126 MB L2 while the probe
+// streams, and almost every probe reads exactly one sector.  A probe row
+// walks its bucket sequence until an empty slot and emits one (probe row,
+// arena row) pair per equal key (jr_probe_candidates,
 // qdb/kernel/join/join_rows.oz:146-197); NULL keys match nothing.
 #include <algorithm>
 
 #include "common.cuh"
 #include "eval.h"
+#include "jtable.cuh"
 #include "kernels.h"
 
 namespace qdb {
@@ -60,10 +63,10 @@ __device__ __forceinline__ uint64_t PackKeyCols(const A& a, int64_t r, bool& nul
     return k;
 }
 
-__global__ void JoinInitKernel(uint64_t* entries, int64_t capacity) {
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < capacity; i += int64_t(gridDim.x) * blockDim.x) {
-        reinterpret_cast<ulonglong2*>(entries)[2 * i] = make_ulonglong2(kEmptyKey, 0);
-        reinterpret_cast<ulonglong2*>(entries)[2 * i + 1] = make_ulonglong2(0, 0);
+__global__ void JoinInitKernel(uint64_t* buckets, int64_t nbuckets) {
+    for (int64_t b = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; b < nbuckets; b += int64_t(gridDim.x) * blockDim.x) {
+        reinterpret_cast<ulonglong2*>(buckets)[2 * b] = make_ulonglong2(kEmptyKey, kEmptyKey);
+        reinterpret_cast<ulonglong2*>(buckets)[2 * b + 1] = make_ulonglong2(0, 0);
     }
 }
 
@@ -79,67 +82,80 @@ __global__ void __launch_bounds__(256) JoinBuildKernel(const __grid_constant__ J
             a.special_rows[2 * k + 1] = int64_t(pay);
             continue;
         }
-        uint64_t i = Fmix64(key) & a.mask;
-        for (uint64_t p = 0; p <= a.mask; ++p) {
-            auto* kp = reinterpret_cast<unsigned long long*>(&a.entries[4 * i]);
-            if (*reinterpret_cast<volatile unsigned long long*>(kp) == kEmptyKey &&
-                atomicCAS(kp, kEmptyKey, key) == kEmptyKey) {
-                a.entries[4 * i + 1] = uint64_t(a.row_base + r);
-                a.entries[4 * i + 2] = pay;
-                break;
+        uint64_t b = Fmix64(key) & a.bmask;
+        bool placed = false;
+        for (uint64_t p = 0; p <= a.bmask && !placed; ++p) {
+            for (int j = 0; j < 2; ++j) {
+                auto* kp = reinterpret_cast<unsigned long long*>(&a.buckets[4 * b + j]);
+                if (*reinterpret_cast<volatile unsigned long long*>(kp) == kEmptyKey &&
+                    atomicCAS(kp, kEmptyKey, key) == kEmptyKey) {
+                    a.buckets[4 * b + 2 + j] = pay;
+                    a.rows[2 * b + j] = a.row_base + r;
+                    placed = true;
+                    break;
+                }
             }
-            i = (i + 1) & a.mask;
+            b = (b + 1) & a.bmask;
         }
     }
 }
 
 __global__ void __launch_bounds__(256) JoinProbePairsKernel(const __grid_constant__ JoinProbeArgs a) {
     const int64_t warps = int64_t(gridDim.x) * (blockDim.x / 32);
-    for (int64_t b = (int64_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5)) * 32; b < a.nrows; b += warps * 32) {
-        const int64_t r = b + LaneId();
+    for (int64_t base = (int64_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5)) * 32; base < a.nrows;
+         base += warps * 32) {
+        const int64_t r = base + LaneId();
         bool act = r < a.nrows && (a.selection == nullptr || a.selection[r] != 0);
         bool null = false;
         uint64_t key = 0;
         if (act) key = PackKeyCols(a, r, null);
         act = act && !null;
         const bool special = act && a.jkey.full64 && key == kEmptyKey;
-        int64_t pos = -1;
-        uint64_t i = act ? (Fmix64(key) & a.jt.mask) : 0;
+        uint64_t b = act ? (Fmix64(key) & a.jt.bmask) : 0;
+        int j = 0;                      // next slot of bucket b to look at
+        ulonglong2 kk = make_ulonglong2(kEmptyKey, kEmptyKey);
+        if (act && !special) kk = BucketKeys(a.jt, b);
         int64_t sp = special ? 0 : -1;
-        int64_t probes = 0;
-        // Walk the probe sequence; emit a pair per equal key.
+        const int64_t nspecial = special ? int64_t(*a.jt.nspecial) : 0;
+        uint64_t buckets_seen = 0;
+        // Walk the bucket sequence; emit a pair per equal key.
         while (true) {
             int64_t brow = -1;
             if (act && !special) {
-                while (probes <= int64_t(a.jt.mask)) {
-                    const ulonglong2 e = *reinterpret_cast<const ulonglong2*>(&a.jt.entries[4 * i]);
-                    ++probes;
-                    if (e.x == kEmptyKey) {
+                while (true) {
+                    if (j == 2) {
+                        if (++buckets_seen > a.jt.bmask) {
+                            act = false;
+                            break;
+                        }
+                        b = (b + 1) & a.jt.bmask;
+                        j = 0;
+                        kk = BucketKeys(a.jt, b);
+                    }
+                    const uint64_t k = j == 0 ? kk.x : kk.y;
+                    const int jj = j++;
+                    if (k == kEmptyKey) {
                         act = false;
                         break;
                     }
-                    const uint64_t here = i;
-                    i = (i + 1) & a.jt.mask;
-                    if (e.x == key) {
-                        brow = int64_t(e.y);
-                        pos = int64_t(here);
+                    if (k == key) {
+                        brow = a.jt.rows[2 * b + jj];
                         break;
                     }
                 }
-                if (probes > int64_t(a.jt.mask)) act = false;
             } else if (special) {
-                if (sp < a.jt.nspecial) brow = a.jt.special_rows[2 * sp++];
+                if (sp < nspecial) brow = a.jt.special_rows[2 * sp++];
                 else act = false;
             }
             const bool emit = brow >= 0;
             const unsigned m = __ballot_sync(kFull, emit);
             if (m == 0 && !__any_sync(kFull, act)) break;
             if (m) {
-                unsigned long long base = 0;
-                if (LaneId() == __ffs(m) - 1) base = atomicAdd(a.npairs, (unsigned long long)__popc(m));
-                base = __shfl_sync(kFull, base, __ffs(m) - 1);
+                unsigned long long at = 0;
+                if (LaneId() == __ffs(m) - 1) at = atomicAdd(a.npairs, (unsigned long long)__popc(m));
+                at = __shfl_sync(kFull, at, __ffs(m) - 1);
                 if (emit) {
-                    const unsigned long long slot = base + __popc(m & ((1u << LaneId()) - 1));
+                    const unsigned long long slot = at + __popc(m & ((1u << LaneId()) - 1));
                     if (int64_t(slot) < a.pair_cap) {
                         a.pairs[2 * slot] = r;
                         a.pairs[2 * slot + 1] = brow;
@@ -148,7 +164,17 @@ __global__ void __launch_bounds__(256) JoinProbePairsKernel(const __grid_constan
             }
             if (!__any_sync(kFull, act)) break;
         }
-        (void)pos;
+    }
+}
+
+// Sets the Bloom bits of every occupied slot's key.
+__global__ void __launch_bounds__(256) JoinBloomKernel(const uint64_t* buckets, int64_t nbuckets, uint32_t* bloom,
+                                                       int32_t nwords) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < 2 * nbuckets; i += int64_t(gridDim.x) * blockDim.x) {
+        const uint64_t k = buckets[4 * (i >> 1) + (i & 1)];
+        if (k == kEmptyKey) continue;
+        const uint64_t h = Fmix64(k);
+        atomicOr(&bloom[BloomWord(h, nwords)], BloomBits(h));
     }
 }
 
@@ -158,9 +184,9 @@ int Blocks(int64_t n, int threads) {
 
 }  // namespace
 
-void JoinInitTable(uint64_t* entries, int64_t capacity, cudaStream_t s) {
-    ProfileBegin(s, "join_init_table", capacity);
-    JoinInitKernel<<<Blocks(capacity, 256), 256, 0, s>>>(entries, capacity);
+void JoinInitTable(uint64_t* buckets, int64_t nbuckets, cudaStream_t s) {
+    ProfileBegin(s, "join_init_table", nbuckets);
+    JoinInitKernel<<<Blocks(nbuckets, 256), 256, 0, s>>>(buckets, nbuckets);
     ProfileEnd(s);
     CountLaunch();
 }
@@ -169,6 +195,15 @@ void JoinBuild(const JoinBuildArgs& a, cudaStream_t s) {
     if (a.nrows == 0) return;
     ProfileBegin(s, "join_build", a.nrows);
     JoinBuildKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(a);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+void JoinBuildBloom(const JTableDev& jt, uint32_t* bloom, int32_t nwords, cudaStream_t s) {
+    const int64_t nbuckets = int64_t(jt.bmask) + 1;
+    cudaMemsetAsync(bloom, 0, size_t(nwords) * 4, s);
+    ProfileBegin(s, "join_bloom", 2 * nbuckets);
+    JoinBloomKernel<<<Blocks(2 * nbuckets, 256), 256, 0, s>>>(jt.buckets, nbuckets, bloom, nwords);
     ProfileEnd(s);
     CountLaunch();
 }

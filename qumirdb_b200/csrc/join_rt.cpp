@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstring>
 
+#include "fast.h"
 #include "runtime.h"
 
 namespace qdb {
@@ -37,20 +38,33 @@ struct ArenaState {
 struct TableState {
     uint32_t magic = kTableMagic;
     cudaStream_t s = nullptr;
-    uint64_t* entries = nullptr;
-    int64_t capacity = 0;
+    uint64_t* buckets = nullptr;   // two-slot buckets, 32 bytes each
+    int64_t* rows = nullptr;       // arena row per slot
+    int64_t slots = 0;             // power of two, >= 2 * rows
     int64_t* special = nullptr;
-    unsigned long long* nspecial_d = nullptr;
-    int64_t nspecial = 0;
+    unsigned long long* nspecial_d = nullptr;   // device count of special rows
+    uint32_t* bloom = nullptr;
+    int32_t bloom_words = 0;
     JTableDev dev() const {
         JTableDev j;
-        j.entries = entries;
-        j.mask = uint64_t(capacity - 1);
+        j.buckets = buckets;
+        j.bmask = uint64_t(slots / 2 - 1);
+        j.rows = rows;
         j.special_rows = special;
-        j.nspecial = nspecial;
+        j.nspecial = nspecial_d;
+        j.bloom = bloom;
+        j.bloom_words = bloom_words;
         return j;
     }
 };
+
+// Blocked Bloom filter size: about 8 bits per key, within a CTA's shared
+// memory next to the probe's staging buffers (kMaxBloomWords); tiny tables
+// get none.
+int32_t BloomWordsFor(int64_t rows) {
+    if (rows < 4096) return 0;
+    return int32_t(std::min<int64_t>(kMaxBloomWords, std::max<int64_t>(1024, rows / 4)) & ~int64_t(3));
+}
 
 constexpr uint32_t kPairMagic = 0x51445050;   // 'QDPP'
 
@@ -160,16 +174,16 @@ void DestroyArena(ArenaState* a) {
         DevFree(c.data, a->s);
         DevFree(c.valid, a->s);
     }
-    cudaStreamSynchronize(a->s);
     a->magic = 0;
     delete a;
 }
 
 void DestroyTable(TableState* t) {
-    DevFree(t->entries, t->s);
+    DevFree(t->bloom, t->s);
+    DevFree(t->buckets, t->s);
+    DevFree(t->rows, t->s);
     DevFree(t->special, t->s);
     DevFree(t->nspecial_d, t->s);
-    cudaStreamSynchronize(t->s);
     t->magic = 0;
     delete t;
 }
@@ -234,18 +248,22 @@ bool Build(const qdb_gpu_program* prog, ArenaState* a, void* table) {
     if (old) DestroyTable(old);
     auto* t = new TableState();
     t->s = a->s;
+    // Slots: a power of two >= 2x the rows; >= 4x while the buckets stay
+    // within 32 MB, so that few probes find their first bucket full.
     int64_t cap = 1024;
     while (cap < a->rows * 2) cap *= 2;
-    t->capacity = cap;
-    t->entries = static_cast<uint64_t*>(DevAlloc(size_t(cap) * 32, t->s));
+    if (cap * 2 * 16 <= (int64_t(32) << 20)) cap *= 2;
+    t->slots = cap;
+    t->buckets = static_cast<uint64_t*>(DevAlloc(size_t(cap / 2) * 32, t->s));
+    t->rows = static_cast<int64_t*>(DevAlloc(size_t(cap) * 8, t->s));
     t->special = static_cast<int64_t*>(DevAlloc(size_t(std::max<int64_t>(a->rows, 1)) * 16, t->s));
     t->nspecial_d = static_cast<unsigned long long*>(DevAlloc(8, t->s));
-    if (!t->entries || !t->special || !t->nspecial_d) {
+    if (!t->buckets || !t->rows || !t->special || !t->nspecial_d) {
         DestroyTable(t);
         return false;
     }
     cudaMemsetAsync(t->nspecial_d, 0, 8, t->s);
-    JoinInitTable(t->entries, cap, t->s);
+    JoinInitTable(t->buckets, cap / 2, t->s);
     JoinBuildArgs b;
     std::memset(&b, 0, sizeof(b));
     for (size_t j = 0; j < J.build_keys.size(); ++j) {
@@ -257,23 +275,30 @@ bool Build(const qdb_gpu_program* prog, ArenaState* a, void* table) {
     }
     b.jkey = J.build_jk;
     b.nrows = a->rows;
-    // The first 8-byte payload column rides in the entry: a probe reads one
-    // 32-byte sector for key, row and that value.
+    // The first 8-byte payload column rides in the bucket: a probe reads one
+    // 32-byte sector for the keys and those values.
     b.pay0 = (!a->payload.empty() && a->payload[0].width == 8) ? reinterpret_cast<const int64_t*>(a->payload[0].data)
                                                                 : nullptr;
-    b.entries = t->entries;
-    b.mask = uint64_t(cap - 1);
+    b.buckets = t->buckets;
+    b.bmask = uint64_t(cap / 2 - 1);
+    b.rows = t->rows;
     b.special_rows = t->special;
     b.nspecial = t->nspecial_d;
     b.row_base = 0;
     JoinBuild(b, t->s);
-    unsigned long long ns = 0;
-    cudaMemcpyAsync(&ns, t->nspecial_d, 8, cudaMemcpyDeviceToHost, t->s);
-    if (!CudaOk(cudaStreamSynchronize(t->s), "row join build")) {
+    t->bloom_words = BloomWordsFor(a->rows);
+    if (t->bloom_words > 0) {
+        t->bloom = static_cast<uint32_t*>(DevAlloc(size_t(t->bloom_words) * 4, t->s));
+        if (!t->bloom) {
+            DestroyTable(t);
+            return false;
+        }
+        JoinBuildBloom(t->dev(), t->bloom, t->bloom_words, t->s);
+    }
+    if (!CudaOk(cudaGetLastError(), "row join build")) {
         DestroyTable(t);
         return false;
     }
-    t->nspecial = int64_t(ns);
     *static_cast<TableState**>(table) = t;
     int64_t* w = static_cast<int64_t*>(table);
     w[1] = cap;        // Capacity
@@ -528,6 +553,28 @@ bool qdb_gpu_jr_dispatch(const qdb_gpu_program* prog, void* arena, void* table, 
     }
 }
 
+void qdb_gpu_jr_release(void* arena, void* table, void* scratch, void* pairs) {
+    (void)scratch;
+    if (pairs) {
+        auto* pb = static_cast<PairBuf*>(pairs);
+        PairState* ps = pb->state;
+        if (ps && ps->magic == kPairMagic) {
+            DevFree(ps->dev, ps->s);
+            ps->magic = 0;
+            delete ps;
+        }
+        std::memset(pairs, 0, QDB_PAIR_BUFFER_SIZE);
+    }
+    if (table) {
+        if (TableState* t = TableOf(table)) DestroyTable(t);
+        std::memset(table, 0, QDB_ROW_TABLE_SIZE);
+    }
+    if (arena) {
+        if (ArenaState* a = ArenaOf(arena)) DestroyArena(a);
+        std::memset(arena, 0, QDB_ROW_ARENA_SIZE);
+    }
+}
+
 int64_t qdb_gpu_jr_materialize(const qdb_gpu_program* prog, void* pairs_v, qdb_rowset* stream, int64_t start,
                                int64_t limit, qdb_rowset* out) {
     t_error.clear();
@@ -553,7 +600,7 @@ int64_t qdb_gpu_jr_materialize(const qdb_gpu_program* prog, void* pairs_v, qdb_r
                                            : J.build_columns[J.payload[J.out_column[k]]].type);
     }
     std::vector<AggOutputCol> cols;
-    if (!AllocOutputCols(types, n, true, cols)) {
+    if (!AllocOutputCols(types, n, true, cols, s)) {
         SetErr("jr_materialize: allocation failed");
         return -1;
     }
@@ -614,7 +661,14 @@ int64_t qdb_gpu_join_aggregate_probe(const qdb_gpu_program* prog, void* arena, v
     }
     const int64_t before = AggStateMatched(st);
     const JTableDev jt = t->dev();
-    if (!AggRun(st, plan, batch->RowCount, &J.agg_jk, &jt, inline_slot)) return -1;
+    JoinSumShape shape;
+    if (MatchJoinSum(plan, J.agg_jk, inline_slot, shape)) {
+        // Typed fast kernel for a keyless SUM / COUNT over 8-byte columns.
+        shape.selection = nullptr;
+        if (!AggRunJoinSum(st, shape, jt, batch->RowCount)) return -1;
+    } else if (!AggRun(st, plan, batch->RowCount, &J.agg_jk, &jt, inline_slot)) {
+        return -1;
+    }
     AggMirrorHeader(ht, st, prog->agg.plan);
     return AggStateMatched(st) - before;
 }

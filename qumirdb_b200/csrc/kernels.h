@@ -44,15 +44,34 @@ struct JoinKeyPlan {
     uint8_t is_float[4] = {};
 };
 
-// Built join table: 4 words (32 bytes, one sector) per slot: packed key,
-// arena row, first payload word, unused; EMPTY key = kEmptyKey.  Rows whose
-// key equals kEmptyKey are listed separately as (arena row, payload word).
+// Built join table: buckets of two slots, one 32-byte sector each: words
+// [4b, 4b+1] the packed keys of slots 2b, 2b+1 and words [4b+2, 4b+3] their
+// first payload words; rows[2b + j] is the arena row of slot 2b + j.  EMPTY
+// key = kEmptyKey.  A bucket fills slot 0 before slot 1, and a key only lands
+// in a later bucket when both slots of the earlier ones were taken, so a probe
+// stops at the first empty slot.  Rows whose key equals kEmptyKey are listed
+// separately as (arena row, payload word).
 struct JTableDev {
-    const uint64_t* entries = nullptr;
-    uint64_t mask = 0;
+    const uint64_t* buckets = nullptr;
+    uint64_t bmask = 0;                               // bucket count - 1
+    const int64_t* rows = nullptr;
     const int64_t* special_rows = nullptr;
-    int64_t nspecial = 0;
+    const unsigned long long* nspecial = nullptr;   // device count of special rows
+    // Blocked Bloom filter over the table's keys (one 32-bit word per key,
+    // two bits set), small enough for a CTA's shared memory; nullptr: none.
+    const uint32_t* bloom = nullptr;
+    int32_t bloom_words = 0;
 };
+constexpr int32_t kMaxBloomWords = 32768;   // 128 KB
+
+// Bloom filter word and bits of a mixed key hash h (shared by build and probe).
+__host__ __device__ __forceinline__ uint32_t BloomWord(uint64_t h, int32_t nwords) {
+    return uint32_t((uint64_t(uint32_t(h >> 32)) * uint32_t(nwords)) >> 32);
+}
+__host__ __device__ __forceinline__ uint32_t BloomBits(uint64_t h) {
+    return (1u << (h & 31)) | (1u << ((h >> 5) & 31));
+}
+void JoinBuildBloom(const JTableDev& jt, uint32_t* bloom, int32_t nwords, cudaStream_t s);
 
 struct AggUpdateArgs {
     const AggPlan* plan = nullptr;
@@ -67,6 +86,7 @@ struct AggUpdateArgs {
     int64_t spill_cap = 0;
     int32_t smem_slots = 0;            // 0 disables the shared-memory tier
     bool priv = false;                 // lane-private accumulators for the first groups
+    const FastPlan* fast = nullptr;    // typed row shape, when the plan has one
     int32_t inline_slot = -1;          // fused join: slot served by the entry's payload word
     bool join = false;
     JoinKeyPlan jkey;
@@ -114,14 +134,15 @@ struct JoinBuildArgs {
     uint8_t key_signed[4];
     JoinKeyPlan jkey;
     int64_t nrows;
-    const int64_t* pay0;    // first 8-byte payload column (stored in the entry) or nullptr
-    uint64_t* entries;      // capacity * 4 words
-    uint64_t mask;
+    const int64_t* pay0;    // first 8-byte payload column (stored in the bucket) or nullptr
+    uint64_t* buckets;      // (bmask + 1) * 4 words
+    uint64_t bmask;
+    int64_t* rows;          // (bmask + 1) * 2 arena rows
     int64_t* special_rows;
     unsigned long long* nspecial;
     int64_t row_base;       // arena row of build row 0
 };
-void JoinInitTable(uint64_t* entries, int64_t capacity, cudaStream_t s);
+void JoinInitTable(uint64_t* buckets, int64_t nbuckets, cudaStream_t s);
 void JoinBuild(const JoinBuildArgs& a, cudaStream_t s);
 
 struct JoinProbeArgs {

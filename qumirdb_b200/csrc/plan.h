@@ -250,6 +250,56 @@ struct AggPlan {
     int32_t probe_cols;
 };
 
+// Typed row shape (filled by the host when a plan qualifies): every column
+// the row reads is an integer of at most 8 bytes without NULLs; predicates
+// compare one column with 64-bit constants; states fold products of up to
+// three 64-bit affine factors.  Rows then load each column once as int64.
+constexpr int kFastCols = 8;
+constexpr int kFastAtoms = 4;
+constexpr int kFastStates = 8;
+
+struct FastAtom {
+    uint8_t op;         // AT_EQ..AT_GE, AT_BETWEEN, AT_IN
+    uint8_t col;        // index into the fast column list
+    uint8_t list_off;
+    uint8_t list_len;
+    uint8_t clause;
+    uint8_t pad[3];
+    int64_t c0, c1;
+};
+
+struct FastFactor {
+    uint8_t col;
+    uint8_t pad[7];
+    int64_t c;
+    int64_t d;
+};
+
+struct FastState {
+    uint8_t kind;       // ST_COUNT (no factors), ST_SUM_I64, ST_SUM_I128, ST_MIN_I64, ST_MAX_I64
+    uint8_t nf;         // 0..3
+    uint8_t wide;       // product kept in 128 bits (decimal)
+    uint8_t word;
+    uint8_t pad[4];
+    FastFactor f[3];
+};
+
+struct FastPlan {
+    int32_t ncols;
+    int32_t natoms;
+    uint32_t clause_mask;
+    int32_t nkeys;
+    int32_t nstates;
+    int32_t pad;
+    uint8_t col_slot[kFastCols];     // plan column slot of each fast column
+    uint8_t key_col[2];
+    uint8_t key_bits[2];
+    uint8_t key_shift[2];
+    uint8_t pad2[2];
+    FastAtom atoms[kFastAtoms];
+    FastState states[kFastStates];
+};
+
 // Order-preserving map of doubles onto u64 (min/max state images).
 QDB_HD inline uint64_t F64Ordered(double f) {
     uint64_t b;

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/qdb_gpu.h"
+#include "fast.h"
 #include "kernels.h"
 #include "lower.h"
 #include "runtime.h"
@@ -114,6 +115,36 @@ void* DevAlloc(size_t bytes, cudaStream_t s) {
 
 void DevFree(void* p, cudaStream_t s) {
     if (p) cudaFreeAsync(p, s);
+}
+
+// Pinned host mirrors of the per-state counters, carved from slabs pinned
+// once per process: pinning or unpinning a page synchronises the device and
+// costs milliseconds, far more than the query steps that use the mirrors.
+namespace {
+std::mutex g_pin_mu;
+std::vector<AggCounters*> g_pin_free;
+}  // namespace
+
+AggCounters* PinnedCountersGet() {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    if (g_pin_free.empty()) {
+        constexpr int kSlab = 256;
+        void* slab = nullptr;
+        if (cudaMallocHost(&slab, sizeof(AggCounters) * kSlab) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        for (int i = kSlab - 1; i >= 0; --i) g_pin_free.push_back(static_cast<AggCounters*>(slab) + i);
+    }
+    AggCounters* c = g_pin_free.back();
+    g_pin_free.pop_back();
+    return c;
+}
+
+void PinnedCountersPut(AggCounters* c) {
+    if (!c) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pin_free.push_back(c);
 }
 
 bool IsDevicePtr(const void* p) {
@@ -307,27 +338,40 @@ AggTableState* AggStateCreate(const AggPlan& p, int64_t capacity_hint, int64_t e
     st->expected = expected;
     int64_t cap = std::max<int64_t>(1024, NextPow2(std::max<int64_t>(capacity_hint, 1)));
     if (expected > 0) cap = std::max(cap, NextPow2(expected + expected / 2));
-    if (cudaMallocHost(&st->hc, sizeof(AggCounters)) != cudaSuccess) {
+    st->hc = PinnedCountersGet();
+    if (!st->hc) {
         delete st;
         SetErr("pinned allocation failed");
         return nullptr;
     }
     st->dc = static_cast<AggCounters*>(DevAlloc(sizeof(AggCounters), s));
     if (!st->dc || !AllocTable(p, cap, s, st->t)) {
-        cudaFreeHost(st->hc);
+        DevFree(st->dc, s);
+        PinnedCountersPut(st->hc);
         delete st;
         return nullptr;
     }
     ResetCounters(st);
-    // A keyless aggregate has its group before any row arrives.
+    // A keyless aggregate has its group before any row arrives: key 0 is
+    // all-zero bytes in its home slot.
     if (p.nkeyparts == 0) {
-        uint64_t zero = 0;
         const int64_t slot = int64_t(Fmix64(0) & uint64_t(cap - 1));
-        cudaMemcpyAsync(st->t.slots + slot * st->t.slot_words + st->t.key_off, &zero, 8, cudaMemcpyHostToDevice, s);
-        cudaStreamSynchronize(s);
+        cudaMemsetAsync(st->t.slots + slot * st->t.slot_words + st->t.key_off, 0, 8, s);
         st->groups = 1;
     }
     return st;
+}
+
+// Fused join + keyless aggregate through the join-sum fast kernel: folds into
+// the keyless group's slot (created with the table at key 0).
+bool AggRunJoinSum(AggTableState* st, const JoinSumShape& shape, const JTableDev& jt, int64_t nrows) {
+    const int64_t slot = int64_t(Fmix64(0) & uint64_t(st->t.capacity - 1));
+    uint64_t* states = st->t.slots + slot * st->t.slot_words + st->t.state_off;
+    ResetCounters(st);
+    JoinSumRun(shape, jt, nrows, states, st->dc, st->s);
+    if (!ReadCounters(st)) return false;
+    st->matched += int64_t(st->hc->matched);
+    return true;
 }
 
 int64_t AggStateGroups(const AggTableState* st) { return st ? st->groups : 0; }
@@ -342,8 +386,8 @@ void AggStateDestroy(AggTableState* st) {
     DevFree(st->deferred[0], st->s);
     DevFree(st->deferred[1], st->s);
     DevFree(st->spill, st->s);
-    cudaStreamSynchronize(st->s);
-    cudaFreeHost(st->hc);
+    // Every readback into the mirror was synchronised when it was read.
+    PinnedCountersPut(st->hc);
     st->magic = 0;
     delete st;
 }
@@ -356,6 +400,8 @@ bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyP
     // Few expected groups (or none): fold the first groups of each CTA into
     // lane-private accumulators.
     const bool priv = plan.nkeyparts == 0 || (st->expected > 0 && st->expected <= 64);
+    FastPlan fast;
+    const bool use_fast = jk == nullptr && MatchFast(plan, fast);
     for (int64_t begin = 0; begin < rows || (rows == 0 && begin == 0); begin += kChunkRows) {
         const int64_t n = std::min<int64_t>(kChunkRows, rows - begin);
         if (n <= 0) break;
@@ -371,6 +417,7 @@ bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyP
         a.spill_cap = st->spill_cap;
         a.smem_slots = st->smem_slots;
         a.priv = priv;
+        a.fast = use_fast ? &fast : nullptr;
         if (jk) {
             a.join = true;
             a.jkey = *jk;
@@ -421,13 +468,16 @@ struct OwnedRowset {
     std::vector<void*> host;
     std::vector<void*> dev;
     std::vector<qdb_column> cols;
+    cudaStream_t s = nullptr;   // device buffers are released in this stream's order
 };
 
+// Device outputs go back to the stream-ordered pool on the library stream:
+// a caller that read them on another stream synchronises that stream first.
 void DestroyOwned(qdb_rowset* rs) {
     if (!rs || !rs->Private) return;
     auto* o = static_cast<OwnedRowset*>(rs->Private);
     for (void* p : o->host) std::free(p);
-    for (void* p : o->dev) cudaFree(p);
+    for (void* p : o->dev) DevFree(p, o->s);
     delete o;
     rs->Private = nullptr;
     rs->Columns = nullptr;
@@ -437,11 +487,8 @@ void DestroyOwned(qdb_rowset* rs) {
 bool EmitRowset(std::vector<AggOutputCol>& cols, const std::vector<int>& types, int64_t rows, bool on_device,
                 cudaStream_t s, qdb_rowset* out) {
     auto* o = new OwnedRowset();
+    o->s = s;
     o->cols.resize(cols.size());
-    if (!CudaOk(cudaStreamSynchronize(s), "output")) {
-        delete o;
-        return false;
-    }
     for (size_t k = 0; k < cols.size(); ++k) {
         qdb_column& c = o->cols[k];
         std::memset(&c, 0, sizeof(c));
@@ -462,25 +509,36 @@ bool EmitRowset(std::vector<AggOutputCol>& cols, const std::vector<int>& types, 
             }
         } else {
             void* h = std::malloc(dbytes);
-            cudaMemcpy(h, cols[k].data, size_t(rows) * w, cudaMemcpyDeviceToHost);
+            cudaMemcpyAsync(h, cols[k].data, size_t(rows) * w, cudaMemcpyDeviceToHost, s);
             c.Data = static_cast<char*>(h);
             o->host.push_back(h);
-            cudaFree(cols[k].data);
             if (cols[k].valid) {
                 void* m = std::malloc(std::max<size_t>(4, mbytes));
-                cudaMemcpy(m, cols[k].valid, mbytes, cudaMemcpyDeviceToHost);
+                cudaMemcpyAsync(m, cols[k].valid, mbytes, cudaMemcpyDeviceToHost, s);
                 c.Mask = static_cast<const uint8_t*>(m);
                 o->host.push_back(m);
-                cudaFree(cols[k].valid);
             }
             if (cols[k].offsets) {
                 void* off = std::malloc(size_t(rows + 1) * 4);
-                cudaMemcpy(off, cols[k].offsets, size_t(rows + 1) * 4, cudaMemcpyDeviceToHost);
+                cudaMemcpyAsync(off, cols[k].offsets, size_t(rows + 1) * 4, cudaMemcpyDeviceToHost, s);
                 c.Offsets = off;
                 c.OffsetWidth = 4;
                 o->host.push_back(off);
-                cudaFree(cols[k].offsets);
             }
+        }
+    }
+    // The host copies have landed once the stream drains; only then do the
+    // device buffers go back to the pool.
+    if (!CudaOk(cudaStreamSynchronize(s), "output")) {
+        for (void* p : o->host) std::free(p);
+        delete o;
+        return false;
+    }
+    if (!on_device) {
+        for (auto& c : cols) {
+            DevFree(c.data, s);
+            DevFree(c.valid, s);
+            DevFree(c.offsets, s);
         }
     }
     std::memset(out, 0, sizeof(*out));
@@ -493,22 +551,34 @@ bool EmitRowset(std::vector<AggOutputCol>& cols, const std::vector<int>& types, 
     return true;
 }
 
-bool AllocOutputCols(const std::vector<int>& types, int64_t rows, bool with_valid, std::vector<AggOutputCol>& cols) {
+bool AllocOutputCols(const std::vector<int>& types, int64_t rows, bool with_valid, std::vector<AggOutputCol>& cols,
+                     cudaStream_t s) {
     cols.resize(types.size());
+    for (auto& c : cols) std::memset(&c, 0, sizeof(c));
+    auto fail = [&]() {
+        for (auto& c : cols) {
+            DevFree(c.data, s);
+            DevFree(c.valid, s);
+            DevFree(c.offsets, s);
+        }
+        return false;
+    };
     for (size_t k = 0; k < types.size(); ++k) {
         AggOutputCol& c = cols[k];
-        std::memset(&c, 0, sizeof(c));
         c.type = types[k];
         const size_t w = size_t(StorageWidth(types[k]));
-        if (cudaMalloc(&c.data, std::max<size_t>(16, size_t(rows) * w)) != cudaSuccess) return false;
+        c.data = static_cast<char*>(DevAlloc(std::max<size_t>(16, size_t(rows) * w), s));
+        if (!c.data) return fail();
         if (with_valid) {
             const size_t mb = std::max<size_t>(4, size_t((rows + 31) / 32) * 4);
-            if (cudaMalloc(&c.valid, mb) != cudaSuccess) return false;
-            cudaMemset(c.valid, 0, mb);
+            c.valid = static_cast<uint32_t*>(DevAlloc(mb, s));
+            if (!c.valid) return fail();
+            cudaMemsetAsync(c.valid, 0, mb, s);
         }
         if (types[k] == QDB_TYPE_CHAR1) {
-            if (cudaMalloc(&c.offsets, size_t(rows + 1) * 4) != cudaSuccess) return false;
-            cudaMemset(c.offsets, 0, 4);
+            c.offsets = static_cast<int32_t*>(DevAlloc(size_t(rows + 1) * 4, s));
+            if (!c.offsets) return fail();
+            cudaMemsetAsync(c.offsets, 0, 4, s);
         }
     }
     return true;
@@ -519,7 +589,7 @@ int64_t AggFinish(AggTableState* st, const AggLowering& lw, uint32_t flags, qdb_
     std::vector<int> types;
     for (int k = 0; k < lw.out.n; ++k) types.push_back(lw.out.out_type[k]);
     std::vector<AggOutputCol> cols;
-    if (!AllocOutputCols(types, groups, true, cols)) {
+    if (!AllocOutputCols(types, groups, true, cols, st->s)) {
         SetErr("output allocation failed");
         return -1;
     }
@@ -755,6 +825,12 @@ int64_t qdb_gpu_agg_dispatch(const qdb_gpu_program* prog, void* ht, qdb_rowset* 
         default:
             return 0;
     }
+}
+
+void qdb_gpu_agg_release(void* ht) {
+    if (!ht) return;
+    AggStateDestroy(StateOf(ht));
+    std::memset(ht, 0, QDB_HASH_TABLE_SIZE);
 }
 
 int64_t qdb_gpu_agg_finish_rowset(const qdb_gpu_program* prog, void* ht, qdb_rowset* out) {

@@ -18,6 +18,9 @@ bool CudaOk(cudaError_t e, const char* what);
 cudaStream_t CurStream();
 void* DevAlloc(size_t bytes, cudaStream_t s);
 void DevFree(void* p, cudaStream_t s);
+struct AggCounters;
+AggCounters* PinnedCountersGet();
+void PinnedCountersPut(AggCounters* c);
 bool IsDevicePtr(const void* p);
 int64_t NextPow2(int64_t v);
 
@@ -40,12 +43,15 @@ void AggStateDestroy(AggTableState* st);
 bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyPlan* jk, const JTableDev* jt,
             int inline_slot = -1);
 int64_t AggFinish(AggTableState* st, const AggLowering& lw, uint32_t flags, qdb_rowset* out);
+struct JoinSumShape;
+bool AggRunJoinSum(AggTableState* st, const JoinSumShape& shape, const JTableDev& jt, int64_t nrows);
 int64_t AggStateGroups(const AggTableState* st);
 int64_t AggStateMatched(const AggTableState* st);
 AggTableState* AggStateOf(void* ht);
 void AggMirrorHeader(void* ht, const AggTableState* st, const AggPlan& p);
 
-bool AllocOutputCols(const std::vector<int>& types, int64_t rows, bool with_valid, std::vector<AggOutputCol>& cols);
+bool AllocOutputCols(const std::vector<int>& types, int64_t rows, bool with_valid, std::vector<AggOutputCol>& cols,
+                     cudaStream_t s);
 bool EmitRowset(std::vector<AggOutputCol>& cols, const std::vector<int>& types, int64_t rows, bool on_device,
                 cudaStream_t s, qdb_rowset* out);
 

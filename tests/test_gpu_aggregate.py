@@ -51,6 +51,20 @@ def test_lineitem_device_resident_full_size():
     assert_same_groups(got, want, queries.LINEITEM_OUT_TYPES, nkeys=2)
 
 
+def test_lineitem_general_path_matches_typed_path():
+    # Validity masks (all valid) keep the plan off the typed row shape, so the
+    # general kernel computes the same query; both must equal the oracle.
+    cols = lineitem(80_000, seed=13)
+    spec = queries.lineitem_agg(int(cols[6].max()) - 60)
+    want = O.aggregate(spec, [q.HostRowSet(cols)])
+    typed = run_gpu(spec, [q.HostRowSet(cols)])
+    masked = run_gpu(spec, [q.HostRowSet(cols, masks=[np.ones(len(cols[0]), bool)] * len(cols))])
+    for out in (typed, masked):
+        got = gpu_rows(out, queries.LINEITEM_OUT_TYPES)
+        q.release(out)
+        assert_same_groups(got, want, queries.LINEITEM_OUT_TYPES, nkeys=2)
+
+
 def test_lineitem_several_batches_and_selection():
     cols = lineitem(50_000, seed=4)
     cutoff = int(cols[6].max()) - 300

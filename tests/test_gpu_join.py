@@ -106,3 +106,48 @@ def test_pair_probe_and_materialize():
     arena_payload = b[1][keep]
     want_rows = sorted((int(p[0][r]), int(p[1][r]), int(arena_payload[br])) for r, br in want)
     assert sorted(got) == want_rows
+
+
+def _shape_aggs(e, name):
+    """Aggregates over the joined row (fk, value, payload) for one shape."""
+    fk, val, pay = e.col(0, abi.I64), e.col(1, abi.I64), e.col(2, abi.I64)
+    mul = lambda a, b: e.op(abi.MUL, abi.I64, a, b)
+    add = lambda a, b: e.op(abi.ADD, abi.I64, a, b)
+    sub = lambda a, b: e.op(abi.SUB, abi.I64, a, b)
+    c = lambda v: e.const(v, abi.I64)
+    return {
+        "count": [(abi.COUNT_STAR, -1)],
+        "sum_pay": [(abi.SUM, pay)],
+        "sum_val": [(abi.SUM, val)],
+        "sum_val_pay": [(abi.SUM, mul(val, pay))],
+        "count_sum": [(abi.COUNT_STAR, -1), (abi.SUM, mul(pay, val))],
+        "sum_val_count": [(abi.SUM, val), (abi.COUNT_STAR, -1)],
+        "affine": [(abi.SUM, mul(add(pay, c(7)), sub(val, c(3)))), (abi.COUNT_STAR, -1)],
+        "sum_val_sq": [(abi.SUM, mul(val, val))],
+        "three_states": [(abi.SUM, val), (abi.SUM, pay), (abi.COUNT_STAR, -1)],
+        "fk_factor": [(abi.SUM, mul(fk, pay))],
+    }[name]
+
+
+@pytest.mark.parametrize("shape", ["count", "sum_pay", "sum_val", "sum_val_pay", "count_sum", "sum_val_count",
+                                   "affine", "sum_val_sq", "three_states", "fk_factor"])
+def test_join_aggregate_shapes(shape):
+    """Every compile-time state signature of the join-sum kernel, and the
+    runtime-interpreted fold, against the oracle on a probe that spans whole
+    staged tiles plus a ragged tail."""
+    b, p = join_data(300_000, 2_000_000 + 777, 375_000)
+    jspec, _ = queries.join_sum(20)
+    e = q.ExprBuilder()
+    aggs = _shape_aggs(e, shape)
+    aspec = queries.AggSpec([(abi.I64,), (abi.I64,), (abi.I64,)], e, None, [], aggs, expected_groups=1)
+    prog = q.compile_join_aggregate(jspec, aspec)
+    J = q.RowJoin(prog)
+    J.append(q.DeviceRowSet(b))
+    J.build()
+    agg = q.Aggregate(prog)
+    J.probe_aggregate(agg, q.DeviceRowSet(p))
+    out = agg.finish()
+    got = gpu_rows(out, [abi.I64] * len(aggs))
+    q.release(out)
+    want = O.join_aggregate(jspec, aspec, [q.HostRowSet(b)], [q.HostRowSet(p)])
+    assert got == want
