@@ -402,6 +402,69 @@ class RowJoin:
             pass
 
 
+def compile_sort(spec) -> Program:
+    err = C.create_string_buffer(512)
+    h = lib().qdb_gpu_compile_sort(C.byref(spec.struct), err, 512)
+    if not h:
+        raise QdbError(err.value.decode())
+    return Program(h, keep=(spec,))
+
+
+def rowset_array(rowsets) -> C.Array:
+    """A contiguous TRowSet array (a sort store) over row-set objects."""
+    arr = (abi.RowSet * max(1, len(rowsets)))()
+    for k, r in enumerate(rowsets):
+        arr[k] = r.rs
+    return arr
+
+
+class Sort:
+    """TSortProcessor's kernel calls (qdb/exec/sort_exec.cpp:393-490) over a
+    store of batches: qdb_sort_run and qdb_top_k_select.  Row ids are packed
+    (batch << 32) | row, in a host int64 array or a DeviceBuffer."""
+
+    def __init__(self, prog: Program, store):
+        _ensure_init()
+        self.prog = prog
+        self.store_objs = list(store)
+        self.store = rowset_array(self.store_objs)
+
+    @staticmethod
+    def _ids(row_ids):
+        if isinstance(row_ids, DeviceBuffer):
+            return row_ids.ptr, row_ids.nbytes // 8
+        return row_ids.ctypes.data, len(row_ids)
+
+    def sort(self, row_ids, descs=None, nulls_firsts=None, n=None) -> None:
+        ptr, m = self._ids(row_ids)
+        n = m if n is None else n
+        d = None if descs is None else (C.c_bool * len(descs))(*descs)
+        nf = None if nulls_firsts is None else (C.c_bool * len(nulls_firsts))(*nulls_firsts)
+        out = abi.RowSet()
+        r = lib().qdb_gpu_sort_run(self.prog.handle, self.store, ptr, None, None, n, d, nf, True, 0, 0,
+                                   C.byref(out))
+        if r < 0:
+            raise QdbError(f"sort failed: {last_error()}")
+
+    def materialize(self, row_ids, start: int, limit: int, n=None) -> tuple[int, abi.RowSet]:
+        ptr, m = self._ids(row_ids)
+        n = m if n is None else n
+        out = abi.RowSet()
+        r = lib().qdb_gpu_sort_run(self.prog.handle, self.store, ptr, None, None, n, None, None, False, start,
+                                   limit, C.byref(out))
+        if r < 0:
+            raise QdbError(f"sort materialize failed: {last_error()}")
+        return r, out
+
+    def top_k(self, row_ids, limit: int, n=None) -> int:
+        ptr, m = self._ids(row_ids)
+        n = m if n is None else n
+        k = lib().qdb_gpu_top_k_select(self.prog.handle, self.store, ptr, n, limit)
+        if k < 0:
+            raise QdbError(f"top-k failed: {last_error()}")
+        return k
+
+
 def profile(on: bool) -> None:
     lib().qdb_gpu_profile_enable(1 if on else 0)
 

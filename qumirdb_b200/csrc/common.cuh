@@ -20,6 +20,7 @@ enum DeviceError : int {
     DE_DEFER_FULL = 4,        // deferred-row buffer capacity exceeded
     DE_LOOKBACK_TIMEOUT = 5,  // a scan's decoupled look-back ran out of iterations
     DE_PROBE_LIMIT = 6,       // a table probe exceeded its bound
+    DE_BAD_ROW_ID = 7,        // a packed row id names a batch outside the store
 };
 
 // Upper bound of any spin in device code, in SM clock cycles (~1 s).

@@ -141,3 +141,39 @@ def zipf_agg(expected_groups: int = 0, flags: int = 0) -> AggSpec:
     x = e.col(2, abi.F64)
     aggs = [(abi.COUNT_STAR, -1), (abi.SUM, a), (abi.MIN, a), (abi.MAX, a), (abi.SUM, x)]
     return AggSpec(ZIPF_COLUMNS, e, None, [key], aggs, flags=flags, expected_groups=expected_groups)
+
+
+class SortSpec:
+    """qdb_sort_spec plus the arrays it points at.  keys: (column, desc,
+    nulls_first), most significant first."""
+
+    def __init__(self, columns, keys, out_columns=None, flags=0):
+        self.columns = coltypes(columns)
+        self.keys = (abi.SortKey * max(1, len(keys)))()
+        for k, key in enumerate(keys):
+            col, desc, nulls_first = (tuple(key) + (0, 0))[:3]
+            self.keys[k].column, self.keys[k].desc, self.keys[k].nulls_first = col, int(desc), int(nulls_first)
+        outs = list(range(len(columns))) if out_columns is None else list(out_columns)
+        self.out = i32s(outs)
+        s = abi.SortSpec()
+        s.n_columns, s.columns = len(columns), self.columns
+        s.n_keys, s.keys = len(keys), self.keys
+        s.n_out, s.out_columns = len(outs), self.out
+        s.flags = flags
+        self.struct = s
+        self.column_types = list(columns)
+        self.out_columns = outs
+
+
+SORT_COLUMNS = [(abi.I64,), (abi.I32,), (abi.I64,)]
+
+
+def sort_k1_desc_k2(flags: int = 0) -> SortSpec:
+    """ORDER BY k1 DESC, k2 ASC over (k1 i64, k2 i32, rowid i64); ties keep
+    input order."""
+    return SortSpec(SORT_COLUMNS, [(0, 1, 0), (1, 0, 0)], flags=flags)
+
+
+def top_k1(flags: int = 0) -> SortSpec:
+    """ORDER BY k1 (the LIMIT is the top-K call's)."""
+    return SortSpec(SORT_COLUMNS, [(0, 0, 0)], flags=flags)
