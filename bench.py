@@ -42,6 +42,7 @@ FK_DOMAIN = 2_500_000
 LINEITEM_ROWS = 6_001_215
 ZIPF_ROWS = 200_000_000
 ZIPF_DISTINCT = 20_000_000
+SORT_ROWS = 300_000_000
 METRIC = "rows/s & HBM GB/s vs peak per operator; mixed-stream queries/s and p50/p99"
 
 
@@ -254,6 +255,91 @@ def zipf_operator(q, peak):
             "l2": "inputs larger than L2", "gpu_launches": launches / 3}
 
 
+def sort_pass_plan_bytes(n: int) -> tuple[int, int]:
+    """Algorithmic bytes of the device sort of (k1 i64 DESC, k2 i32 ASC) over
+    n row ids, by the plan it runs: extraction (row id 8 + k1 8 + k2 4 read,
+    u32 k2 key 4 + u64 k1 key 8 written), a copy of the row ids (8 + 8), the
+    k2 stage's 3 non-constant digit passes (first 4 + 8 then 2 x 16), the k1
+    stage's 8 passes (first a gather 4 + 8 + 12, then 7 x 24), the final
+    row-id gather (4 + 8 + 8).  Returns (total per sort, per u64 pass)."""
+    per_row = 32 + 16 + (12 + 16 + 16) + (24 + 7 * 24) + 20
+    return n * per_row, n * 24
+
+
+def sort_operator(q, peak):
+    from qumirdb_b200 import abi, queries
+    n = SORT_ROWS
+    batch = 1 << 22
+    k1 = np.empty(n, np.int64)
+    k2 = np.empty(n, np.int32)
+    rowid = np.empty(n, np.int64)
+    q.lib().qdb_gen_sort(3, n, k1.ctypes.data, k2.ctypes.data, rowid.ctypes.data)
+    sizes = [min(batch, n - b) for b in range(0, n, batch)]
+    store, at = [], 0
+    for m in sizes:
+        store.append(q.DeviceRowSet([k1[at:at + m], k2[at:at + m], rowid[at:at + m]]))
+        at += m
+    ids = np.concatenate([(np.int64(b) << 32) | np.arange(m, dtype=np.int64) for b, m in enumerate(sizes)])
+    pristine = q.DeviceBuffer(ids.nbytes).upload(ids)
+    work = q.DeviceBuffer(ids.nbytes)
+    del ids
+    sorter = q.Sort(q.compile_sort(queries.sort_k1_desc_k2(flags=abi.OUT_DEVICE)), store)
+    topper = q.Sort(q.compile_sort(queries.top_k1(flags=abi.OUT_DEVICE)), store)
+    import torch
+    stream = torch.cuda.ExternalStream(q.lib().qdb_gpu_get_stream())
+
+    def run(fn, steps, warmup):
+        times = []
+        kern = []
+        for i in range(warmup + steps):
+            q.lib().qdb_gpu_memcpy(work.ptr, pristine.ptr, work.nbytes)   # in place: restore the input order
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            if i >= warmup:
+                q.profile(True)
+                q.profile_read()
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            if i >= warmup:
+                times.append(a.elapsed_time(b))
+                kern.append(q.profile_read())
+                q.profile(False)
+        return statistics.median(times), kern
+
+    ms, kern = run(lambda: sorter.sort(work), 3, 1)
+    passes = [ms_ for ks in kern for name, ms_, _ in ks if name == "sort_pass_u64"]
+    alg, per_pass = sort_pass_plan_bytes(n)
+    pass_ms = statistics.median(passes) if passes else None
+    tk_ms, _ = run(lambda: topper.top_k(work, 1000), 3, 1)
+    tk_alg = n * 32   # two passes over (row id 8, k1 8)
+    line = {"workload": "ORDER BY k1 DESC, k2 ASC (stable) over 300,000,000 row ids in 72 batches; "
+                        "top-N: ORDER BY k1 LIMIT 1000",
+            "rows_per_s": n / (ms / 1e3), "ms_per_sort": ms, "algorithmic_bytes": alg,
+            "bytes_per_row": alg // n, "sort_gbs": alg / (ms / 1e3) / 1e9,
+            "frac_of_measured_hbm": alg / (ms / 1e3) / 1e9 / peak,
+            "kernel": "sort_pass_u64", "kernel_ms": pass_ms,
+            "kernel_gbs": per_pass / (pass_ms / 1e3) / 1e9 if pass_ms else None,
+            "kernel_frac_of_measured_hbm": per_pass / (pass_ms / 1e3) / 1e9 / peak if pass_ms else None,
+            "topk_ms": tk_ms, "topk_rows_per_s": n / (tk_ms / 1e3), "topk_algorithmic_bytes": tk_alg,
+            "topk_gbs": tk_alg / (tk_ms / 1e3) / 1e9, "l2": "inputs larger than L2"}
+    del store, pristine, work
+    return line
+
+
+def cpu_baseline_sort(sample: int) -> dict:
+    from oracle import oracle as O
+    import qumirdb_b200 as q
+    k1 = np.empty(sample, np.int64)
+    k2 = np.empty(sample, np.int32)
+    q.lib().qdb_gen_sort(3, sample, k1.ctypes.data, k2.ctypes.data, None)
+    threads = os.cpu_count() or 1
+    sec = O.lib().oracle_bench_sort(k1.ctypes.data, k2.ctypes.data, sample, threads, None)
+    return {"value": sample / sec, "unit": "rows/s", "cores": threads, "kind": "port",
+            "sample": f"{sample:,} rows (of 300M): per-lane LSD + heap k-way merge of the CPU restatement",
+            "seconds": sec}
+
+
 def cpu_baseline_join(sample_probe: int, steps: int = 1) -> dict:
     from oracle import oracle as O
     import qumirdb_b200 as q
@@ -382,7 +468,11 @@ def main() -> None:
     }
     if rank == 0 and world == 1 and not args.no_operators:
         try:
-            line["operators"] = {"lineitem": lineitem_operator(q, peak), "zipf": zipf_operator(q, peak)}
+            line["operators"] = {"lineitem": lineitem_operator(q, peak), "zipf": zipf_operator(q, peak),
+                                 "sort": sort_operator(q, peak)}
+            if not args.no_cpu_baseline:
+                line["operators"]["sort"]["cpu_baseline"] = {
+                    k: v for k, v in cpu_baseline_sort(20_000_000).items() if k != "seconds"}
         except Exception as e:  # reported, never hidden
             line["operators_error"] = repr(e)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
