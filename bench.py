@@ -381,6 +381,64 @@ def reference_arm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def profile_case(name: str, rows: int) -> None:
+    """One workload run twice (a warm-up, then the launch a profiler
+    captures) at `rows` rows; prints "done <name>".  The workloads are the
+    bench's own generators at a size that a detailed capture finishes on."""
+    import qumirdb_b200 as q
+    from qumirdb_b200 import queries
+    q.init(0)
+    if name == "lineitem":
+        n = rows or LINEITEM_ROWS
+        cols = [np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64),
+                np.empty(n, np.uint8), np.empty(n, np.uint8), np.empty(n, np.int32)]
+        q.lib().qdb_gen_lineitem(0, n, *[c.ctypes.data for c in cols])
+        prog = q.compile_aggregate(queries.lineitem_agg(int(cols[6].max()) - 90))
+        drs = q.DeviceRowSet(cols)
+        for _ in range(2):
+            a = q.Aggregate(prog)
+            a.add(drs)
+            q.release(a.finish())
+    elif name == "join":
+        n = rows or PROBE_ROWS
+        b = [np.empty(BUILD_ROWS, np.int64), np.empty(BUILD_ROWS, np.int64), np.empty(BUILD_ROWS, np.int32)]
+        p = [np.empty(n, np.int64), np.empty(n, np.int64)]
+        q.lib().qdb_gen_join(1, BUILD_ROWS, n, FK_DOMAIN, *[x.ctypes.data for x in b + p])
+        j, a = queries.join_sum(20)
+        prog = q.compile_join_aggregate(j, a)
+        db, dp = q.DeviceRowSet(b), q.DeviceRowSet(p)
+        for _ in range(2):
+            J = q.RowJoin(prog)
+            J.append(db)
+            J.build()
+            agg = q.Aggregate(prog)
+            J.probe_aggregate(agg, dp)
+            q.release(agg.finish())
+    elif name == "zipf":
+        n = rows or ZIPF_ROWS
+        cols = [np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.float64)]
+        q.lib().qdb_gen_zipf(2, n, max(1, n // 10), 1.1, *[c.ctypes.data for c in cols])
+        prog = q.compile_aggregate(queries.zipf_agg(expected_groups=max(1, n // 10)))
+        drs = q.DeviceRowSet(cols)
+        for _ in range(2):
+            a = q.Aggregate(prog)
+            a.add(drs)
+            q.release(a.finish())
+    elif name == "sort":
+        n = rows or SORT_ROWS
+        k1 = np.empty(n, np.int64)
+        k2 = np.empty(n, np.int32)
+        rid = np.arange(n, dtype=np.int64)
+        q.lib().qdb_gen_sort(3, n, k1.ctypes.data, k2.ctypes.data, None)
+        s = q.Sort(q.compile_sort(queries.sort_k1_desc_k2()), [q.DeviceRowSet([k1, k2, rid])])
+        d = q.DeviceBuffer(rid.nbytes)
+        for _ in range(2):
+            d.upload(rid)
+            s.sort(d)
+    q.synchronize()
+    print("done", name, flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -389,7 +447,13 @@ def main() -> None:
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--no-operators", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", choices=["join", "sort", "lineitem", "zipf"],
+                    help="run one workload twice at --rows rows (for profiler captures) and exit")
+    ap.add_argument("--rows", type=int, default=0)
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args.profile_case, args.rows)
+        return
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         reference_arm(args)
