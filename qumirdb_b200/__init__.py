@@ -200,8 +200,8 @@ def synchronize() -> None:
 class DeviceRowSet:
     """A TRowSet whose columns live in HBM (the resident column cache)."""
 
-    def __init__(self, columns, masks=None, selection=None):
-        host = HostRowSet(columns, masks, selection)
+    def __init__(self, columns, masks=None, selection=None, rows=None):
+        host = HostRowSet(columns, masks, selection, rows)
         self.rows = host.rs.RowCount
         self.bufs = []
         self.cols = (abi.Column * max(1, len(host.arrays)))()

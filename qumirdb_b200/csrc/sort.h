@@ -37,7 +37,7 @@ struct SortStage {
     int32_t pad = 0;
 };
 
-constexpr int kMaxSortStages = 10;
+constexpr int kMaxSortStages = 16;
 constexpr int kSortDigits = 8;                     // 8-bit digits of a u64 key
 constexpr int kSortTile = 4096;                    // keys per onesweep tile
 
