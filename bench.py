@@ -150,6 +150,24 @@ class JoinWorkload:
         return res
 
 
+def combine_partials(dist, s: int, c: int, device: str = "cuda") -> tuple[int, int]:
+    """The join's partial SUM(payload*value) and COUNT(*) of every rank's probe
+    shard, summed over ranks (the one data-path collective: the partials are
+    two int64 words; SUM wraps like the engine's reducer)."""
+    import torch
+    t = torch.tensor([s, c], device=device, dtype=torch.int64)
+    dist.all_reduce(t)
+    return int(t[0]), int(t[1])
+
+
+def max_over_ranks(dist, ms: float, device: str = "cuda") -> float:
+    """The slowest rank's time: the whole job is done when the last rank is."""
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def timed(q, fn, steps: int, warmup: int, dist=None, profile: bool = False):
     """Device time of `steps` calls of fn on the library's stream (events)."""
     import torch
@@ -174,9 +192,7 @@ def timed(q, fn, steps: int, warmup: int, dist=None, profile: bool = False):
     kernels = q.profile_read() if profile else []
     q.profile(False)
     if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(dist, ms)
     return ms, results, launches, kernels
 
 
@@ -479,9 +495,7 @@ def main() -> None:
     def query():
         s, c = w.step(resident=True)
         if dist is not None:
-            t = torch.tensor([s, c], device="cuda", dtype=torch.int64)
-            dist.all_reduce(t)
-            return int(t[0]), int(t[1])
+            return combine_partials(dist, s, c)
         return s, c
 
     sampler = ClockSampler(local)
@@ -497,8 +511,7 @@ def main() -> None:
     def query_e2e():
         s, c = w.step(resident=False)
         if dist is not None:
-            t = torch.tensor([s, c], device="cuda", dtype=torch.int64)
-            dist.all_reduce(t)
+            return combine_partials(dist, s, c)
         return s, c
 
     ms_e2e, _, _, _ = timed(q, query_e2e, max(1, min(args.steps, 3)), 1, dist=dist)
