@@ -28,9 +28,11 @@
 // MAX fold non-NULL inputs, f64 sums are IEEE additions in device order.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 #include "eval.h"
@@ -933,6 +935,422 @@ __global__ void __launch_bounds__(kAggThreads, 1) AggUpdateKernel(const __grid_c
     }
 }
 
+// ---------------------------------------------------------------------------
+// Low-cardinality scan aggregate specialised by a compile-time query shape
+// (the typed row shape of FastPlan): column widths, filter atoms, key
+// columns and every state's factor columns are template constants, so each
+// value is one typed load at a fixed offset of the staged tile; constants
+// (filter bounds, affine factors, key packing) stay runtime-uniform.  Per
+// staged tile, phase A filters the rows, packs their keys and finds their
+// groups (a per-thread cache of the CTA's lane-private groups, else the
+// shared table), appending every row of the first kPrivGroups groups to that
+// group's list in shared memory; rows of other groups take the general
+// typed fold.  Phase B walks the lists one group at a time — the group is
+// the same for the whole warp, so the accumulators are registers addressed
+// at compile time — folding each row with the state list unrolled.  The
+// registers reach the shared table once, after the last tile.
+// ---------------------------------------------------------------------------
+enum SigKind : int { SK_COUNT = 0, SK_SUM64 = 1, SK_SUM128_OF64 = 2, SK_SUM128 = 3 };
+
+template <int... V>
+struct IntList {
+    static constexpr int n = int(sizeof...(V));
+    __host__ __device__ static constexpr int at(int s) {
+        int i = 0, r = 0;
+        ((r = (i++ == s ? V : r)), ...);
+        return r;
+    }
+};
+
+// Column code: width in bytes * 2 + 1 when unsigned.  Atom code: AtomOp * 8 +
+// column.  State code: kind << 11 | factors << 9 | col0 << 6 | col1 << 3 | col2.
+constexpr int ColCode(int width, bool uns) { return width * 2 + (uns ? 1 : 0); }
+constexpr int AtomCode(int op, int col) { return op * 8 + col; }
+constexpr int StateCode(int kind, int nf, int c0 = 0, int c1 = 0, int c2 = 0) {
+    return (kind << 11) | (nf << 9) | (c0 << 6) | (c1 << 3) | c2;
+}
+
+template <class COLS, class ATOMS, class KEYS, class STATES>
+struct Shape {
+    using Cols = COLS;
+    using Atoms = ATOMS;
+    using Keys = KEYS;
+    using States = STATES;
+    static constexpr int n = States::n;
+    __host__ __device__ static constexpr int kind(int s) { return States::at(s) >> 11; }
+    __host__ __device__ static constexpr int nf(int s) { return (States::at(s) >> 9) & 3; }
+    __host__ __device__ static constexpr int fcol(int s, int j) { return (States::at(s) >> (6 - 3 * j)) & 7; }
+    __host__ __device__ static constexpr int width(int s) { return kind(s) >= SK_SUM128_OF64 ? 2 : 1; }
+    __host__ __device__ static constexpr int off(int s) {
+        int o = 0;
+        for (int i = 0; i < s; ++i) o += width(i);
+        return o;
+    }
+    static constexpr int words = off(n);
+    __host__ __device__ static constexpr int cw(int k) { return Cols::at(k) >> 1; }
+    __host__ __device__ static constexpr bool cu(int k) { return (Cols::at(k) & 1) != 0; }
+};
+
+__device__ __forceinline__ void Add128(uint64_t& lo, uint64_t& hi, uint64_t l, uint64_t h) {
+    const uint64_t n = lo + l;
+    hi += h + (n < lo ? 1ull : 0ull);
+    lo = n;
+}
+
+// Fast column K of tile row r (cb: the tile's column bases).
+template <class SH, int K>
+__device__ __forceinline__ int64_t ColVal(const char* const (&cb)[kFastCols], int r) {
+    constexpr int w = SH::cw(K);
+    constexpr bool u = SH::cu(K);
+    const char* p = cb[K] + int64_t(r) * w;
+    if constexpr (w == 1) return u ? int64_t(*reinterpret_cast<const uint8_t*>(p)) : int64_t(*reinterpret_cast<const int8_t*>(p));
+    else if constexpr (w == 2) return u ? int64_t(*reinterpret_cast<const uint16_t*>(p)) : int64_t(*reinterpret_cast<const int16_t*>(p));
+    else if constexpr (w == 4) return u ? int64_t(*reinterpret_cast<const uint32_t*>(p)) : int64_t(*reinterpret_cast<const int32_t*>(p));
+    else return *reinterpret_cast<const int64_t*>(p);
+}
+
+template <class SH, int S, int J>
+__device__ __forceinline__ int64_t ShapeFactor(const FastPlan& F, const char* const (&cb)[kFastCols], int r) {
+    const FastFactor& f = F.states[S].f[J];
+    const int64_t x = ColVal<SH, SH::fcol(S, J)>(cb, r);
+    return int64_t(uint64_t(f.c) + uint64_t(f.d) * uint64_t(x));
+}
+
+// Folds one row into its group's lane-private accumulators: p points at
+// word 0 of the group for this lane; word w lives at p[w * stride].
+template <class SH, int S = 0>
+__device__ __forceinline__ void ShapeFoldP(uint64_t* p, int stride, const FastPlan& F,
+                                           const char* const (&cb)[kFastCols], int r) {
+    if constexpr (S < SH::n) {
+        constexpr int K = SH::kind(S);
+        constexpr int NF = SH::nf(S);
+        constexpr int O = SH::off(S);
+        uint64_t lo, hi = 0;
+        if constexpr (K == SK_COUNT) {
+            lo = 1;
+        } else if constexpr (K == SK_SUM128) {
+            lo = uint64_t(ShapeFactor<SH, S, 0>(F, cb, r));
+            hi = int64_t(lo) < 0 ? ~0ull : 0ull;
+            if constexpr (NF > 1) Mul128x64(lo, hi, ShapeFactor<SH, S, 1>(F, cb, r));
+            if constexpr (NF > 2) Mul128x64(lo, hi, ShapeFactor<SH, S, 2>(F, cb, r));
+        } else {
+            lo = uint64_t(ShapeFactor<SH, S, 0>(F, cb, r));
+            if constexpr (NF > 1) lo *= uint64_t(ShapeFactor<SH, S, 1>(F, cb, r));
+            if constexpr (NF > 2) lo *= uint64_t(ShapeFactor<SH, S, 2>(F, cb, r));
+            if constexpr (K == SK_SUM128_OF64) hi = int64_t(lo) < 0 ? ~0ull : 0ull;
+        }
+        if constexpr (SH::width(S) == 2) {
+            uint64_t a = p[O * stride];
+            uint64_t b = p[(O + 1) * stride];
+            Add128(a, b, lo, hi);
+            p[O * stride] = a;
+            p[(O + 1) * stride] = b;
+        } else {
+            p[O * stride] += lo;
+        }
+        ShapeFoldP<SH, S + 1>(p, stride, F, cb, r);
+    }
+}
+
+// Clauses held by the row's filter atoms (AND of OR clauses).
+template <class SH, int J = 0>
+__device__ __forceinline__ uint32_t ShapeHeld(const AggPlan& P, const FastPlan& F, const char* const (&cb)[kFastCols],
+                                              int r) {
+    if constexpr (J < SH::Atoms::n) {
+        constexpr int op = SH::Atoms::at(J) >> 3;
+        constexpr int col = SH::Atoms::at(J) & 7;
+        const FastAtom& t = F.atoms[J];
+        const int64_t v = ColVal<SH, col>(cb, r);
+        bool ok;
+        if constexpr (op == AT_BETWEEN) {
+            ok = v >= t.c0 && v <= t.c1;
+        } else if constexpr (op == AT_IN) {
+            ok = false;
+            for (int q = 0; q < t.list_len; ++q) ok = ok || P.list[t.list_off + q] == v;
+        } else if constexpr (op == AT_EQ) {
+            ok = v == t.c0;
+        } else if constexpr (op == AT_NE) {
+            ok = v != t.c0;
+        } else if constexpr (op == AT_LT) {
+            ok = v < t.c0;
+        } else if constexpr (op == AT_LE) {
+            ok = v <= t.c0;
+        } else if constexpr (op == AT_GT) {
+            ok = v > t.c0;
+        } else {
+            ok = v >= t.c0;
+        }
+        return (ok ? (1u << t.clause) : 0u) | ShapeHeld<SH, J + 1>(P, F, cb, r);
+    } else {
+        return 0u;
+    }
+}
+
+template <class SH, int J = 0>
+__device__ __forceinline__ uint64_t ShapeKey(const FastPlan& F, const char* const (&cb)[kFastCols], int r) {
+    if constexpr (J < SH::Keys::n) {
+        uint64_t v = uint64_t(ColVal<SH, SH::Keys::at(J)>(cb, r));
+        if (F.key_bits[J] < 64) v &= (1ull << F.key_bits[J]) - 1;
+        return (v << F.key_shift[J]) | ShapeKey<SH, J + 1>(F, cb, r);
+    } else {
+        return 0ull;
+    }
+}
+
+// Sum of a 64- or 128-bit accumulator over the warp.
+__device__ __forceinline__ void WarpSum128(uint64_t& lo, uint64_t& hi) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        const uint64_t ol = __shfl_xor_sync(kFull, lo, d);
+        const uint64_t oh = __shfl_xor_sync(kFull, hi, d);
+        Add128(lo, hi, ol, oh);
+    }
+}
+
+constexpr int kSigThreads = 384;   // the accumulator words of kPrivGroups groups stay in registers
+
+template <class SIG>
+__global__ void __launch_bounds__(kSigThreads, 1) AggSigKernel(const __grid_constant__ AggLaunch L) {
+    unsigned char* smem = DynSmem();
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.off_bars);
+    unsigned* misc = reinterpret_cast<unsigned*>(smem + L.off_misc);
+    const SmemTable sm = MakeSmem(L, false, true);
+    const AggPlan& P = L.P;
+    const FastPlan& F = L.F;
+    const int tid = threadIdx.x;
+    const int bd = blockDim.x;
+    const int lane = tid & 31;
+    const int T = L.tile_rows;
+
+    if (tid == 0) {
+        misc[0] = 0;
+        misc[1] = 0;
+        misc[2] = 0;
+        misc[4] = 0;
+        for (int s = 0; s < L.stages; ++s) MbarInit(&full[s], 1);
+        FenceBarrierInit();
+    }
+    for (int i = tid; i < sm.S; i += bd) {
+        sm.keys[i] = kEmptyKey;
+        sm.gid[i] = -1;
+        for (int s = 0; s < P.nstates; ++s) {
+            const StateDesc sd = P.states[s];
+            sm.st[int64_t(sd.word) * sm.S + i] = StateIdentity(sd.kind);
+            if (sd.kind == ST_SUM_I128) sm.st[int64_t(sd.word + 1) * sm.S + i] = 0;
+        }
+    }
+    __syncthreads();
+    if (P.nkeyparts == 0 && tid == 0 && sm.S > 0) {
+        // A keyless aggregate has one group: key 0, lane-private group 0.
+        const int i = int(uint32_t(Fmix64(0)) & uint32_t(sm.S - 1));
+        sm.keys[i] = 0;
+        sm.gid[i] = 0;
+        sm.gid_slot[0] = i;
+        misc[0] = 1;
+        misc[2] = 1;
+    }
+    __syncthreads();
+
+    const int64_t ntiles = (L.nrows + T - 1) / T;
+    auto tile_full = [&](int64_t t) { return L.any_staged && (t + 1) * int64_t(T) <= L.nrows; };
+    auto issue = [&](int64_t t, int s) {
+        unsigned char* st = smem + int64_t(s) * L.stage_bytes;
+        FenceProxyAsync();
+        MbarArriveExpectTx(&full[s], uint32_t(L.stage_bytes));
+        for (int c = 0; c < P.ncols; ++c) {
+            const ColDesc& cd = P.cols[c];
+            if (!cd.stage) continue;
+            BulkG2S(st + cd.smem_off, cd.data + t * T * cd.width, uint32_t(T * cd.width), &full[s]);
+        }
+        if (L.sel_off >= 0) BulkG2S(st + L.sel_off, P.selection + t * T, uint32_t(T), &full[s]);
+    };
+    if (tid == 0) {
+        for (int k = 0; k < L.stages; ++k) {
+            const int64_t t = blockIdx.x + int64_t(k) * gridDim.x;
+            if (t < ntiles && tile_full(t)) issue(t, k);
+        }
+    }
+
+    // Lane-private accumulators: word w of group q of this thread at
+    // pacc[(q * words + w) * bd + tid] (consecutive lanes, consecutive banks).
+    uint64_t* pacc = reinterpret_cast<uint64_t*>(smem + L.off_pacc);
+    for (int i = tid; i < kPrivGroups * SIG::words * bd; i += bd) pacc[i] = 0;
+    // This thread's view of the lane-private groups it has met.
+    uint64_t ckey[kPrivGroups];
+    int cgid[kPrivGroups];
+#pragma unroll
+    for (int j = 0; j < kPrivGroups; ++j) {
+        ckey[j] = kEmptyKey;
+        cgid[j] = -1;
+    }
+    int ncache = 0;
+    if (P.nkeyparts == 0) {
+        ckey[0] = 0;
+        cgid[0] = 0;
+        ncache = 1;
+    }
+
+    bool aborted = false;
+    for (int64_t k = 0;; ++k) {
+        const int64_t t = blockIdx.x + k * gridDim.x;
+        if (t >= ntiles) break;
+        const int s = int(k % L.stages);
+        const uint32_t phase = uint32_t((k / L.stages) & 1);
+        const bool full_tile = tile_full(t);
+        const int64_t row0 = t * T;
+        const unsigned char* stage = full_tile ? smem + int64_t(s) * L.stage_bytes : nullptr;
+        if (full_tile && !MbarWaitBounded(&full[s], phase)) {
+            SetError(&L.counters->error, DE_WAIT_TIMEOUT);
+            *reinterpret_cast<volatile unsigned*>(&misc[4]) = 1;
+        }
+        if (*reinterpret_cast<volatile unsigned*>(&misc[4])) {
+            aborted = true;
+            break;
+        }
+        const int nrows = int(min(int64_t(T), L.nrows - row0));
+        const uint8_t* sel = P.selection == nullptr ? nullptr
+                             : (stage && L.sel_off >= 0) ? stage + L.sel_off : P.selection + row0;
+        // The tile's base of every fast column: the stage, or global memory.
+        const char* cb[kFastCols];
+#pragma unroll
+        for (int c = 0; c < kFastCols; ++c) {
+            cb[c] = nullptr;
+            if (c < SIG::Cols::n) {
+                const ColDesc& cd = P.cols[F.col_slot[c]];
+                cb[c] = (stage && cd.stage) ? reinterpret_cast<const char*>(stage) + cd.smem_off
+                                            : cd.data + row0 * SIG::cw(c);
+            }
+        }
+        for (int r = tid; r < nrows; r += bd) {
+            if (sel && !sel[r]) continue;
+            if (SIG::Atoms::n && ShapeHeld<SIG>(P, F, cb, r) != F.clause_mask) continue;
+            const uint64_t key = ShapeKey<SIG>(F, cb, r);
+            int g = -1;
+#pragma unroll
+            for (int j = 0; j < kPrivGroups; ++j) g = ckey[j] == key ? cgid[j] : g;
+            if (g < 0) {
+                // First row of this group for this thread: the shared table.
+                if (!(P.key_full64 && key == kEmptyKey)) {
+                    const int slot = sm.Find(key);
+                    if (slot >= 0) {
+                        const int gg = *reinterpret_cast<volatile int*>(&sm.gid[slot]);
+                        if (gg >= 0 && gg < kPrivGroups && ncache < kPrivGroups) {
+                            g = gg;
+#pragma unroll
+                            for (int j = 0; j < kPrivGroups; ++j) {
+                                if (j == ncache) {
+                                    ckey[j] = key;
+                                    cgid[j] = gg;
+                                }
+                            }
+                            ++ncache;
+                        }
+                    }
+                }
+                if (g < 0) {
+                    RowAcc acc{&P, stage, r, row0 + r, 0, -1, 0};
+                    FoldRowFast<false>(L, acc);
+                    continue;
+                }
+            }
+            ShapeFoldP<SIG>(pacc + int64_t(g) * SIG::words * bd + tid, bd, F, cb, r);
+        }
+        // Every warp is done with the stage: refill it.
+        __syncthreads();
+        if (tid == 0) {
+            const int64_t nt = t + int64_t(L.stages) * gridDim.x;
+            if (nt < ntiles && tile_full(nt)) issue(nt, s);
+        }
+    }
+    __syncthreads();
+    if (aborted || *reinterpret_cast<volatile unsigned*>(&misc[4])) {
+        // Let copies already issued land before the CTA's memory goes away.
+        if (tid == 0) {
+            const long long start = clock64();
+            while (clock64() - start < 2000000) {
+            }
+        }
+        __syncthreads();
+        return;
+    }
+
+    // Lane-private accumulators -> shared table: one warp per (group,
+    // state) sums the lanes, then one shared-memory update.
+    const int ng = int(min(*reinterpret_cast<volatile unsigned*>(sm.ngid), unsigned(kPrivGroups)));
+    const int nwarps = bd >> 5;
+    for (int item = tid >> 5; item < ng * SIG::n; item += nwarps) {
+        const int q = item / SIG::n;
+        const int st2 = item - q * SIG::n;
+        const int o = SIG::off(st2);
+        const bool wide2 = SIG::width(st2) == 2;
+        uint64_t lo = 0, hi = 0;
+        for (int t2 = lane; t2 < bd; t2 += 32) {
+            const uint64_t* w = pacc + int64_t(q * SIG::words + o) * bd + t2;
+            Add128(lo, hi, w[0], wide2 ? w[bd] : 0ull);
+        }
+        WarpSum128(lo, hi);
+        if (lane == 0 && (lo | hi)) {
+            const int slot = *reinterpret_cast<volatile int*>(&sm.gid_slot[q]);
+            const StateDesc sd = P.states[st2];
+            uint64_t* w = sm.st + int64_t(sd.word) * sm.S + slot;
+            ApplyState(w, w + sm.S, sd.kind, lo, hi, 0.0);
+        }
+    }
+    __syncthreads();
+
+    // Shared table -> global table.
+    for (int i = tid; i < sm.S; i += bd) {
+        const uint64_t key = sm.keys[i];
+        if (key == kEmptyKey) continue;
+        int is_new = 0;
+        const int64_t g = GlobalFind1(L.T, L.cap_mask, key, is_new);
+        if (is_new) atomicAdd(sm.fresh, 1u);
+        if (g < 0) {
+            const unsigned long long e = atomicAdd(&L.counters->spilled, 1ull);
+            if (int64_t(e) >= L.spill_cap) {
+                SetError(&L.counters->error, DE_SPILL_FULL);
+                continue;
+            }
+            uint64_t* rec = L.spill + int64_t(e) * (1 + P.state_words);
+            rec[0] = key;
+            for (int w = 0; w < P.state_words; ++w) rec[1 + w] = sm.st[int64_t(w) * sm.S + i];
+            continue;
+        }
+        uint64_t* gbase = L.T.slots + g * L.T.slot_words + L.T.state_off;
+        for (int st2 = 0; st2 < P.nstates; ++st2) {
+            const StateDesc sd = P.states[st2];
+            const uint64_t lo = sm.st[int64_t(sd.word) * sm.S + i];
+            const uint64_t hi = sd.kind == ST_SUM_I128 ? sm.st[int64_t(sd.word + 1) * sm.S + i] : 0;
+            if (IsIdentity(sd.kind, lo, hi)) continue;
+            ApplyState(gbase + sd.word, gbase + sd.word + 1, sd.kind, lo, hi, 0.0);
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
+}
+
+// The instantiated query shapes.  QDB_C(w, u): a fast column of w bytes
+// (u: unsigned); QDB_A(op, col): a filter atom; QDB_S(kind, nf, cols...): a
+// state.  A plan whose shape is not listed runs the general typed kernel.
+#define QDB_C(w, u) ColCode(w, u)
+#define QDB_A(op, c) AtomCode(op, c)
+#define QDB_S(...) StateCode(__VA_ARGS__)
+#define QDB_SHAPE_LIST(X)                                                                                    \
+    /* lineitem (TPC-H Q1 shape): GROUP BY two one-byte codes WHERE date <= c: SUM(qty), SUM(price),       \
+       SUM(price*(c-disc)), SUM(price*(c-disc)*(c+tax)), COUNT(*), SUM(disc) */                            \
+    X(Shape<IntList<QDB_C(1, 1), QDB_C(1, 1), QDB_C(4, 0), QDB_C(8, 0), QDB_C(8, 0), QDB_C(8, 0), QDB_C(8, 0)>, \
+            IntList<QDB_A(AT_LE, 2)>, IntList<0, 1>,                                                         \
+            IntList<QDB_S(SK_SUM64, 1, 3), QDB_S(SK_SUM128_OF64, 1, 4), QDB_S(SK_SUM128, 2, 4, 5),            \
+                    QDB_S(SK_SUM128, 3, 4, 5, 6), QDB_S(SK_COUNT, 0), QDB_S(SK_SUM64, 1, 5)>>)                  \
+    /* COUNT(*) GROUP BY an 8-byte key */                                                                    \
+    X(Shape<IntList<QDB_C(8, 0)>, IntList<>, IntList<0>, IntList<QDB_S(SK_COUNT, 0)>>)                        \
+    /* SUM(x), COUNT(*) GROUP BY an 8-byte key */                                                            \
+    X(Shape<IntList<QDB_C(8, 0), QDB_C(8, 0)>, IntList<>, IntList<0>,                                         \
+            IntList<QDB_S(SK_SUM64, 1, 1), QDB_S(SK_COUNT, 0)>>)                                               \
+    /* keyless SUM(x * y) WHERE x BETWEEN a AND b over 8-byte columns (a TPC-H Q6 shape) */                  \
+    X(Shape<IntList<QDB_C(8, 0), QDB_C(8, 0)>, IntList<QDB_A(AT_BETWEEN, 0)>, IntList<>,                      \
+            IntList<QDB_S(SK_SUM64, 2, 0, 1), QDB_S(SK_COUNT, 0)>>)
+
 // Index mode: rows named by (row, build row) pairs, global table only.
 template <bool WIDE>
 __global__ void __launch_bounds__(256) AggIndexKernel(const __grid_constant__ AggLaunch L) {
@@ -1283,6 +1701,73 @@ static void FillTableArgs(AggLaunch& L, const GTableDev& t) {
     L.cap_mask = uint64_t(t.capacity - 1);
 }
 
+namespace {
+
+// Shape key of a typed plan: column codes, -1, atom codes, -1, key columns,
+// -1, state codes; empty when a state has no compile-time kind.
+std::vector<int> ShapeKeyOf(const AggPlan& P, const FastPlan& F) {
+    std::vector<int> key;
+    for (int c = 0; c < F.ncols; ++c) {
+        const ColDesc& cd = P.cols[F.col_slot[c]];
+        key.push_back(ColCode(cd.width, cd.kind == LK_UNSIGNED));
+    }
+    key.push_back(-1);
+    for (int j = 0; j < F.natoms; ++j) key.push_back(AtomCode(F.atoms[j].op, F.atoms[j].col));
+    key.push_back(-1);
+    for (int j = 0; j < F.nkeys; ++j) key.push_back(F.key_col[j]);
+    key.push_back(-1);
+    for (int s = 0; s < F.nstates; ++s) {
+        const FastState& st = F.states[s];
+        int kind;
+        switch (st.kind) {
+            case ST_COUNT: kind = SK_COUNT; break;
+            case ST_SUM_I64: kind = SK_SUM64; break;
+            case ST_SUM_I128: kind = st.wide ? SK_SUM128 : SK_SUM128_OF64; break;
+            default: return {};
+        }
+        if ((kind == SK_COUNT) != (st.nf == 0)) return {};
+        key.push_back(StateCode(kind, st.nf, st.nf > 0 ? st.f[0].col : 0, st.nf > 1 ? st.f[1].col : 0,
+                                st.nf > 2 ? st.f[2].col : 0));
+    }
+    return key;
+}
+
+template <class LIST>
+void AppendList(std::vector<int>& key) {
+    for (int i = 0; i < LIST::n; ++i) key.push_back(LIST::at(i));
+}
+
+template <class SH>
+bool ShapeMatches(const std::vector<int>& key) {
+    std::vector<int> want;
+    AppendList<typename SH::Cols>(want);
+    want.push_back(-1);
+    AppendList<typename SH::Atoms>(want);
+    want.push_back(-1);
+    AppendList<typename SH::Keys>(want);
+    want.push_back(-1);
+    AppendList<typename SH::States>(want);
+    return key == want;
+}
+
+using SigKernelFn = void (*)(AggLaunch);
+
+SigKernelFn FindSigKernel(const AggPlan& P, const FastPlan& F) {
+    const std::vector<int> key = ShapeKeyOf(P, F);
+    if (key.empty()) return nullptr;
+#define QDB_SHAPE_FIND(...) if (ShapeMatches<__VA_ARGS__>(key)) return AggSigKernel<__VA_ARGS__>;
+    QDB_SHAPE_LIST(QDB_SHAPE_FIND)
+#undef QDB_SHAPE_FIND
+    if (std::getenv("QDB_SHAPE_DEBUG")) {
+        std::fprintf(stderr, "qdb: no compiled shape for key");
+        for (int v : key) std::fprintf(stderr, " %d", v);
+        std::fprintf(stderr, "\n");
+    }
+    return nullptr;
+}
+
+}  // namespace
+
 void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
     EnsureDeviceInfo();
     static thread_local AggLaunch* Lp = nullptr;
@@ -1394,14 +1879,43 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
 
     const int64_t ntiles = (a.nrows + T - 1) / T;
     const int grid = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, g_sms)));
-    const char* name = a.join ? "join_agg_probe" : "agg_update";
     const bool gen = L.P.generic_root >= 0;
+    const int variant = (wide ? 8 : 0) | (a.join ? 4 : 0) | (gen ? 2 : 0) | (priv ? 1 : 0);
+    if (a.fast && variant == 1 && any) {
+        // A typed plan with an instantiated state signature: the listed-row
+        // kernel (no lane-private arrays; the group lists take their place).
+        if (SigKernelFn fn = FindSigKernel(L.P, *a.fast)) {
+            L.F = *a.fast;
+            int Ts = 4096;
+            size_t bytes = 0;
+            const size_t pacc_sig = size_t(kPrivGroups) * sw * kSigThreads * 8;
+            for (;; Ts >>= 1) {
+                layout(Ts, Ts > 1024 ? 2 : 3, 64);
+                bytes = size_t(L.off_pacc) + pacc_sig;
+                if (bytes <= budget || Ts <= 256) break;
+            }
+            if (bytes <= budget) {
+                L.smem_slots = 64;
+                L.smem_limit = 32;
+                L.priv = 1;
+                const int64_t nt = (a.nrows + Ts - 1) / Ts;
+                const int g2 = int(std::max<int64_t>(1, std::min<int64_t>(nt, g_sms)));
+                SetSmem(fn, bytes);
+                ProfileBegin(s, "agg_update_sig", a.nrows);
+                fn<<<g2, kSigThreads, bytes, s>>>(L);
+                ProfileEnd(s);
+                CountLaunch();
+                return;
+            }
+            layout(T, stages, S);
+        }
+    }
+    const char* name = a.join ? "join_agg_probe" : "agg_update";
     ProfileBegin(s, name, a.nrows);
     auto launch = [&](auto kernel) {
         SetSmem(kernel, smem_bytes);
         kernel<<<grid, kAggThreads, smem_bytes, s>>>(L);
     };
-    const int variant = (wide ? 8 : 0) | (a.join ? 4 : 0) | (gen ? 2 : 0) | (priv ? 1 : 0);
     if (a.fast && variant <= 1) {
         L.F = *a.fast;
         if (priv) launch(AggUpdateKernel<false, false, false, true, true>);

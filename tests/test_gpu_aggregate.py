@@ -167,3 +167,73 @@ def test_device_output_stays_resident():
     assert out.RowCount == 4
     assert q.lib().qdb_gpu_launch_count(0) > 0
     q.release(out)
+
+
+def _shape_case(shape, groups, n, rng):
+    """(columns, spec, output types) of a plan whose shape is compiled in the
+    listed-row kernel's catalogue."""
+    k = rng.integers(0, groups, n).astype(np.int64) * 1009 + 5
+    a = rng.integers(-10**12, 10**12, n).astype(np.int64)
+    e = q.ExprBuilder()
+    if shape == "count":
+        kc = e.col(0, abi.I64)
+        spec = queries.AggSpec([(abi.I64,)], e, None, [kc], [(abi.COUNT_STAR, -1)], expected_groups=64)
+        return [k], spec, [abi.I64, abi.I64]
+    if shape == "sum_count":
+        kc, ac = e.col(0, abi.I64), e.col(1, abi.I64)
+        spec = queries.AggSpec([(abi.I64,), (abi.I64,)], e, None, [kc], [(abi.SUM, ac), (abi.COUNT_STAR, -1)],
+                               expected_groups=64)
+        return [k, a], spec, [abi.I64, abi.I64, abi.I64]
+    if shape == "q6":
+        x = rng.integers(0, 1000, n).astype(np.int64)
+        xc, ac = e.col(0, abi.I64), e.col(1, abi.I64)
+        filt = e.op(abi.BETWEEN, abi.BOOL, xc, e.const(100, abi.I64), e.const(700, abi.I64))
+        spec = queries.AggSpec([(abi.I64,), (abi.I64,)], e, filt, [], [(abi.SUM, e.op(abi.MUL, abi.I64, xc, ac))],
+                               expected_groups=1)
+        return [x, a], spec, [abi.I64]
+    # lineitem shape with `groups` flag codes (two one-byte keys).
+    cols = lineitem(n, seed=9)
+    cols[4] = (rng.integers(0, groups, n) + 65).astype(np.uint8)
+    spec = queries.lineitem_agg(int(cols[6].max()) - 90)
+    return cols, spec, queries.LINEITEM_OUT_TYPES
+
+
+@pytest.mark.parametrize("groups", [1, 3, 40])
+@pytest.mark.parametrize("shape", ["count", "sum_count", "q6", "lineitem"])
+def test_shape_kernels(shape, groups):
+    """Each compiled query shape of the listed-row kernel, with all groups in
+    registers (1 and 3 groups) and with 40 groups (the first four in
+    registers, the rest through the shared table); rows in three batches, the
+    last ending in a partial tile."""
+    rng = np.random.default_rng(7 + groups)
+    n = 150_001
+    cols, spec, types = _shape_case(shape, groups, n, rng)
+    bounds = [(0, 70_000), (70_000, 140_000), (140_000, n)]
+    q.profile(True)
+    q.profile_read()
+    out = run_gpu(spec, [q.DeviceRowSet([c[lo:hi] for c in cols]) for lo, hi in bounds])
+    names = {kk[0] for kk in q.profile_read()}
+    q.profile(False)
+    got = gpu_rows(out, types)
+    q.release(out)
+    assert "agg_update_sig" in names, names
+    want = O.aggregate(spec, [q.HostRowSet([c[lo:hi] for c in cols]) for lo, hi in bounds])
+    nkeys = 0 if shape == "q6" else (2 if shape == "lineitem" else 1)
+    assert_same_groups(got, want, types, nkeys=nkeys)
+
+
+def test_lineitem_runs_the_signature_kernel():
+    """The lineitem query's typed plan has an instantiated state signature:
+    its update is the listed-row kernel, with the same groups as the oracle."""
+    cols = lineitem(300_000, seed=5)
+    spec = queries.lineitem_agg(int(cols[6].max()) - 90)
+    q.profile(True)
+    q.profile_read()
+    out = run_gpu(spec, [q.DeviceRowSet(cols)])
+    names = {k[0] for k in q.profile_read()}
+    q.profile(False)
+    got = gpu_rows(out, queries.LINEITEM_OUT_TYPES)
+    q.release(out)
+    assert "agg_update_sig" in names, names
+    want = O.aggregate(spec, [q.HostRowSet(cols)])
+    assert_same_groups(got, want, queries.LINEITEM_OUT_TYPES, nkeys=2)
