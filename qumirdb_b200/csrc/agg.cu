@@ -965,9 +965,14 @@ struct IntList {
 // Column code: width in bytes * 2 + 1 when unsigned.  Atom code: AtomOp * 8 +
 // column.  State code: kind << 11 | factors << 9 | col0 << 6 | col1 << 3 | col2.
 constexpr int ColCode(int width, bool uns) { return width * 2 + (uns ? 1 : 0); }
+// Key code: fast column + 8 * bits + 1024 * shift (the key packing of the plan).
+constexpr int KeyCode(int col, int bits, int shift) { return col + 8 * bits + 1024 * shift; }
 constexpr int AtomCode(int op, int col) { return op * 8 + col; }
-constexpr int StateCode(int kind, int nf, int c0 = 0, int c1 = 0, int c2 = 0) {
-    return (kind << 11) | (nf << 9) | (c0 << 6) | (c1 << 3) | c2;
+// Factor forms (bits 13-18 of a state code, two per factor): 0 x, 1 c + x,
+// 2 c - x, 3 c + d * x.
+enum FactorForm : int { FF_X = 0, FF_ADD = 1, FF_SUB = 2, FF_AFFINE = 3 };
+constexpr int StateCode(int kind, int nf, int c0 = 0, int c1 = 0, int c2 = 0, int f0 = 0, int f1 = 0, int f2 = 0) {
+    return (f2 << 17) | (f1 << 15) | (f0 << 13) | (kind << 11) | (nf << 9) | (c0 << 6) | (c1 << 3) | c2;
 }
 
 template <class COLS, class ATOMS, class KEYS, class STATES>
@@ -977,7 +982,8 @@ struct Shape {
     using Keys = KEYS;
     using States = STATES;
     static constexpr int n = States::n;
-    __host__ __device__ static constexpr int kind(int s) { return States::at(s) >> 11; }
+    __host__ __device__ static constexpr int kind(int s) { return (States::at(s) >> 11) & 3; }
+    __host__ __device__ static constexpr int form(int s, int j) { return (States::at(s) >> (13 + 2 * j)) & 3; }
     __host__ __device__ static constexpr int nf(int s) { return (States::at(s) >> 9) & 3; }
     __host__ __device__ static constexpr int fcol(int s, int j) { return (States::at(s) >> (6 - 3 * j)) & 7; }
     __host__ __device__ static constexpr int width(int s) { return kind(s) >= SK_SUM128_OF64 ? 2 : 1; }
@@ -1011,9 +1017,52 @@ __device__ __forceinline__ int64_t ColVal(const char* const (&cb)[kFastCols], in
 
 template <class SH, int S, int J>
 __device__ __forceinline__ int64_t ShapeFactor(const FastPlan& F, const char* const (&cb)[kFastCols], int r) {
+    constexpr int FM = SH::form(S, J);
     const FastFactor& f = F.states[S].f[J];
     const int64_t x = ColVal<SH, SH::fcol(S, J)>(cb, r);
-    return int64_t(uint64_t(f.c) + uint64_t(f.d) * uint64_t(x));
+    if constexpr (FM == FF_X) return x;
+    else if constexpr (FM == FF_ADD) return int64_t(uint64_t(f.c) + uint64_t(x));
+    else if constexpr (FM == FF_SUB) return int64_t(uint64_t(f.c) - uint64_t(x));
+    else return int64_t(uint64_t(f.c) + uint64_t(f.d) * uint64_t(x));
+}
+
+__device__ __forceinline__ bool Fits32(int64_t v) { return v == int64_t(int32_t(v)); }
+
+// Product of a state's factors: wrapping 64-bit (a, b, c), or exact 128-bit
+// when WIDE.  Factors that fit in 32 bits multiply as 32 x 32 -> 64; others
+// take the full 64 / 128-bit path (same result).
+template <class SH, int S, bool WIDE>
+__device__ __forceinline__ void ShapeProduct(const FastPlan& F, const char* const (&cb)[kFastCols], int r,
+                                             uint64_t& lo, uint64_t& hi) {
+    constexpr int NF = SH::nf(S);
+    const int64_t a = ShapeFactor<SH, S, 0>(F, cb, r);
+    if constexpr (NF == 1) {
+        lo = uint64_t(a);
+        hi = a < 0 ? ~0ull : 0ull;
+        return;
+    } else {
+        const int64_t b = ShapeFactor<SH, S, 1>(F, cb, r);
+        int64_t c = 1;
+        if constexpr (NF > 2) c = ShapeFactor<SH, S, 2>(F, cb, r);
+        if (Fits32(a) && Fits32(b) && Fits32(c)) {
+            const int64_t ab = int64_t(int32_t(a)) * int32_t(b);
+            if (NF == 2 || Fits32(ab)) {
+                const int64_t p = NF == 2 ? ab : int64_t(int32_t(ab)) * int32_t(c);
+                lo = uint64_t(p);
+                hi = p < 0 ? ~0ull : 0ull;
+                return;
+            }
+        }
+        if constexpr (WIDE) {
+            lo = uint64_t(a);
+            hi = a < 0 ? ~0ull : 0ull;
+            Mul128x64(lo, hi, b);
+            if constexpr (NF > 2) Mul128x64(lo, hi, c);
+        } else {
+            lo = uint64_t(a) * uint64_t(b) * uint64_t(c);
+            hi = int64_t(lo) < 0 ? ~0ull : 0ull;
+        }
+    }
 }
 
 // Folds one row into its group's lane-private accumulators: p points at
@@ -1025,20 +1074,9 @@ __device__ __forceinline__ void ShapeFoldP(uint64_t* p, int stride, const FastPl
         constexpr int K = SH::kind(S);
         constexpr int NF = SH::nf(S);
         constexpr int O = SH::off(S);
-        uint64_t lo, hi = 0;
-        if constexpr (K == SK_COUNT) {
-            lo = 1;
-        } else if constexpr (K == SK_SUM128) {
-            lo = uint64_t(ShapeFactor<SH, S, 0>(F, cb, r));
-            hi = int64_t(lo) < 0 ? ~0ull : 0ull;
-            if constexpr (NF > 1) Mul128x64(lo, hi, ShapeFactor<SH, S, 1>(F, cb, r));
-            if constexpr (NF > 2) Mul128x64(lo, hi, ShapeFactor<SH, S, 2>(F, cb, r));
-        } else {
-            lo = uint64_t(ShapeFactor<SH, S, 0>(F, cb, r));
-            if constexpr (NF > 1) lo *= uint64_t(ShapeFactor<SH, S, 1>(F, cb, r));
-            if constexpr (NF > 2) lo *= uint64_t(ShapeFactor<SH, S, 2>(F, cb, r));
-            if constexpr (K == SK_SUM128_OF64) hi = int64_t(lo) < 0 ? ~0ull : 0ull;
-        }
+        uint64_t lo = 1, hi = 0;
+        if constexpr (K != SK_COUNT) ShapeProduct<SH, S, K == SK_SUM128>(F, cb, r, lo, hi);
+        (void)NF;
         if constexpr (SH::width(S) == 2) {
             uint64_t a = p[O * stride];
             uint64_t b = p[(O + 1) * stride];
@@ -1087,11 +1125,16 @@ __device__ __forceinline__ uint32_t ShapeHeld(const AggPlan& P, const FastPlan& 
 }
 
 template <class SH, int J = 0>
-__device__ __forceinline__ uint64_t ShapeKey(const FastPlan& F, const char* const (&cb)[kFastCols], int r) {
+__device__ __forceinline__ uint64_t ShapeKey(const char* const (&cb)[kFastCols], int r) {
     if constexpr (J < SH::Keys::n) {
-        uint64_t v = uint64_t(ColVal<SH, SH::Keys::at(J)>(cb, r));
-        if (F.key_bits[J] < 64) v &= (1ull << F.key_bits[J]) - 1;
-        return (v << F.key_shift[J]) | ShapeKey<SH, J + 1>(F, cb, r);
+        constexpr int code = SH::Keys::at(J);
+        constexpr int col = code & 7;
+        constexpr int bits = (code >> 3) & 127;
+        constexpr int shift = code >> 10;
+        uint64_t v = uint64_t(ColVal<SH, col>(cb, r));
+        // A zero-extended column narrower than its key field needs no mask.
+        if constexpr (bits < 64 && !(SH::cu(col) && SH::cw(col) * 8 <= bits)) v &= (1ull << bits) - 1;
+        return (v << shift) | ShapeKey<SH, J + 1>(cb, r);
     } else {
         return 0ull;
     }
@@ -1107,7 +1150,7 @@ __device__ __forceinline__ void WarpSum128(uint64_t& lo, uint64_t& hi) {
     }
 }
 
-constexpr int kSigThreads = 384;   // the accumulator words of kPrivGroups groups stay in registers
+constexpr int kSigThreads = 512;
 
 template <class SIG>
 __global__ void __launch_bounds__(kSigThreads, 1) AggSigKernel(const __grid_constant__ AggLaunch L) {
@@ -1190,6 +1233,17 @@ __global__ void __launch_bounds__(kSigThreads, 1) AggSigKernel(const __grid_cons
         ncache = 1;
     }
 
+    // Stage offset of every fast column (-1: not staged), fixed for the launch.
+    int coff[kFastCols];
+#pragma unroll
+    for (int c = 0; c < kFastCols; ++c) {
+        coff[c] = -1;
+        if (c < SIG::Cols::n) {
+            const ColDesc& cd = P.cols[F.col_slot[c]];
+            if (cd.stage) coff[c] = cd.smem_off;
+        }
+    }
+
     bool aborted = false;
     for (int64_t k = 0;; ++k) {
         const int64_t t = blockIdx.x + k * gridDim.x;
@@ -1216,15 +1270,15 @@ __global__ void __launch_bounds__(kSigThreads, 1) AggSigKernel(const __grid_cons
         for (int c = 0; c < kFastCols; ++c) {
             cb[c] = nullptr;
             if (c < SIG::Cols::n) {
-                const ColDesc& cd = P.cols[F.col_slot[c]];
-                cb[c] = (stage && cd.stage) ? reinterpret_cast<const char*>(stage) + cd.smem_off
-                                            : cd.data + row0 * SIG::cw(c);
+                cb[c] = coff[c] >= 0 && stage ? reinterpret_cast<const char*>(stage) + coff[c]
+                                              : P.cols[F.col_slot[c]].data + row0 * SIG::cw(c);
             }
         }
+#pragma unroll 2
         for (int r = tid; r < nrows; r += bd) {
             if (sel && !sel[r]) continue;
             if (SIG::Atoms::n && ShapeHeld<SIG>(P, F, cb, r) != F.clause_mask) continue;
-            const uint64_t key = ShapeKey<SIG>(F, cb, r);
+            const uint64_t key = ShapeKey<SIG>(cb, r);
             int g = -1;
 #pragma unroll
             for (int j = 0; j < kPrivGroups; ++j) g = ckey[j] == key ? cgid[j] : g;
@@ -1339,13 +1393,15 @@ __global__ void __launch_bounds__(kSigThreads, 1) AggSigKernel(const __grid_cons
     /* lineitem (TPC-H Q1 shape): GROUP BY two one-byte codes WHERE date <= c: SUM(qty), SUM(price),       \
        SUM(price*(c-disc)), SUM(price*(c-disc)*(c+tax)), COUNT(*), SUM(disc) */                            \
     X(Shape<IntList<QDB_C(1, 1), QDB_C(1, 1), QDB_C(4, 0), QDB_C(8, 0), QDB_C(8, 0), QDB_C(8, 0), QDB_C(8, 0)>, \
-            IntList<QDB_A(AT_LE, 2)>, IntList<0, 1>,                                                         \
-            IntList<QDB_S(SK_SUM64, 1, 3), QDB_S(SK_SUM128_OF64, 1, 4), QDB_S(SK_SUM128, 2, 4, 5),            \
-                    QDB_S(SK_SUM128, 3, 4, 5, 6), QDB_S(SK_COUNT, 0), QDB_S(SK_SUM64, 1, 5)>>)                  \
+            IntList<QDB_A(AT_LE, 2)>, IntList<KeyCode(0, 8, 0), KeyCode(1, 8, 8)>,                                                         \
+            IntList<QDB_S(SK_SUM64, 1, 3), QDB_S(SK_SUM128_OF64, 1, 4),                                       \
+                    QDB_S(SK_SUM128, 2, 4, 5, 0, FF_X, FF_SUB),                                                \
+                    QDB_S(SK_SUM128, 3, 4, 5, 6, FF_X, FF_SUB, FF_ADD), QDB_S(SK_COUNT, 0),                    \
+                    QDB_S(SK_SUM64, 1, 5)>>)                                                                   \
     /* COUNT(*) GROUP BY an 8-byte key */                                                                    \
-    X(Shape<IntList<QDB_C(8, 0)>, IntList<>, IntList<0>, IntList<QDB_S(SK_COUNT, 0)>>)                        \
+    X(Shape<IntList<QDB_C(8, 0)>, IntList<>, IntList<KeyCode(0, 64, 0)>, IntList<QDB_S(SK_COUNT, 0)>>)                        \
     /* SUM(x), COUNT(*) GROUP BY an 8-byte key */                                                            \
-    X(Shape<IntList<QDB_C(8, 0), QDB_C(8, 0)>, IntList<>, IntList<0>,                                         \
+    X(Shape<IntList<QDB_C(8, 0), QDB_C(8, 0)>, IntList<>, IntList<KeyCode(0, 64, 0)>,                                         \
             IntList<QDB_S(SK_SUM64, 1, 1), QDB_S(SK_COUNT, 0)>>)                                               \
     /* keyless SUM(x * y) WHERE x BETWEEN a AND b over 8-byte columns (a TPC-H Q6 shape) */                  \
     X(Shape<IntList<QDB_C(8, 0), QDB_C(8, 0)>, IntList<QDB_A(AT_BETWEEN, 0)>, IntList<>,                      \
@@ -1714,7 +1770,7 @@ std::vector<int> ShapeKeyOf(const AggPlan& P, const FastPlan& F) {
     key.push_back(-1);
     for (int j = 0; j < F.natoms; ++j) key.push_back(AtomCode(F.atoms[j].op, F.atoms[j].col));
     key.push_back(-1);
-    for (int j = 0; j < F.nkeys; ++j) key.push_back(F.key_col[j]);
+    for (int j = 0; j < F.nkeys; ++j) key.push_back(KeyCode(F.key_col[j], F.key_bits[j], F.key_shift[j]));
     key.push_back(-1);
     for (int s = 0; s < F.nstates; ++s) {
         const FastState& st = F.states[s];
@@ -1726,8 +1782,15 @@ std::vector<int> ShapeKeyOf(const AggPlan& P, const FastPlan& F) {
             default: return {};
         }
         if ((kind == SK_COUNT) != (st.nf == 0)) return {};
+        auto form = [&](int j) {
+            if (j >= st.nf) return 0;
+            const FastFactor& f = st.f[j];
+            if (f.d == 1) return f.c == 0 ? int(FF_X) : int(FF_ADD);
+            if (f.d == -1) return int(FF_SUB);
+            return int(FF_AFFINE);
+        };
         key.push_back(StateCode(kind, st.nf, st.nf > 0 ? st.f[0].col : 0, st.nf > 1 ? st.f[1].col : 0,
-                                st.nf > 2 ? st.f[2].col : 0));
+                                st.nf > 2 ? st.f[2].col : 0, form(0), form(1), form(2)));
     }
     return key;
 }
@@ -1890,7 +1953,7 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
             size_t bytes = 0;
             const size_t pacc_sig = size_t(kPrivGroups) * sw * kSigThreads * 8;
             for (;; Ts >>= 1) {
-                layout(Ts, Ts > 1024 ? 2 : 3, 64);
+                layout(Ts, 2, 64);
                 bytes = size_t(L.off_pacc) + pacc_sig;
                 if (bytes <= budget || Ts <= 256) break;
             }
