@@ -950,7 +950,10 @@ __global__ void __launch_bounds__(kAggThreads, 1) AggUpdateKernel(const __grid_c
 // at compile time — folding each row with the state list unrolled.  The
 // registers reach the shared table once, after the last tile.
 // ---------------------------------------------------------------------------
-enum SigKind : int { SK_COUNT = 0, SK_SUM64 = 1, SK_SUM128_OF64 = 2, SK_SUM128 = 3 };
+enum SigKind : int {
+    SK_COUNT = 0, SK_SUM64 = 1, SK_SUM128_OF64 = 2, SK_SUM128 = 3,
+    SK_MIN64 = 4, SK_MAX64 = 5, SK_SUMF64 = 6, SK_MINMAXF64 = 7   // (high-cardinality kernel only)
+};
 
 template <int... V>
 struct IntList {
@@ -968,11 +971,11 @@ constexpr int ColCode(int width, bool uns) { return width * 2 + (uns ? 1 : 0); }
 // Key code: fast column + 8 * bits + 1024 * shift (the key packing of the plan).
 constexpr int KeyCode(int col, int bits, int shift) { return col + 8 * bits + 1024 * shift; }
 constexpr int AtomCode(int op, int col) { return op * 8 + col; }
-// Factor forms (bits 13-18 of a state code, two per factor): 0 x, 1 c + x,
+// Factor forms (bits 14-19 of a state code, two per factor): 0 x, 1 c + x,
 // 2 c - x, 3 c + d * x.
 enum FactorForm : int { FF_X = 0, FF_ADD = 1, FF_SUB = 2, FF_AFFINE = 3 };
 constexpr int StateCode(int kind, int nf, int c0 = 0, int c1 = 0, int c2 = 0, int f0 = 0, int f1 = 0, int f2 = 0) {
-    return (f2 << 17) | (f1 << 15) | (f0 << 13) | (kind << 11) | (nf << 9) | (c0 << 6) | (c1 << 3) | c2;
+    return (f2 << 18) | (f1 << 16) | (f0 << 14) | (kind << 11) | (nf << 9) | (c0 << 6) | (c1 << 3) | c2;
 }
 
 template <class COLS, class ATOMS, class KEYS, class STATES>
@@ -982,11 +985,13 @@ struct Shape {
     using Keys = KEYS;
     using States = STATES;
     static constexpr int n = States::n;
-    __host__ __device__ static constexpr int kind(int s) { return (States::at(s) >> 11) & 3; }
-    __host__ __device__ static constexpr int form(int s, int j) { return (States::at(s) >> (13 + 2 * j)) & 3; }
+    __host__ __device__ static constexpr int kind(int s) { return (States::at(s) >> 11) & 7; }
+    __host__ __device__ static constexpr int form(int s, int j) { return (States::at(s) >> (14 + 2 * j)) & 3; }
     __host__ __device__ static constexpr int nf(int s) { return (States::at(s) >> 9) & 3; }
     __host__ __device__ static constexpr int fcol(int s, int j) { return (States::at(s) >> (6 - 3 * j)) & 7; }
-    __host__ __device__ static constexpr int width(int s) { return kind(s) >= SK_SUM128_OF64 ? 2 : 1; }
+    __host__ __device__ static constexpr int width(int s) {
+        return (kind(s) == SK_SUM128_OF64 || kind(s) == SK_SUM128) ? 2 : 1;
+    }
     __host__ __device__ static constexpr int off(int s) {
         int o = 0;
         for (int i = 0; i < s; ++i) o += width(i);
@@ -1383,6 +1388,211 @@ __global__ void __launch_bounds__(kSigThreads, 1) AggSigKernel(const __grid_cons
     if (tid == 0 && sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
 }
 
+// ---------------------------------------------------------------------------
+// High-cardinality scan aggregate specialised by query shape: typed loads
+// from the staged tile, the CTA's shared table for the keys it holds (the
+// hot keys of a skewed stream settle there), the global HBM table for the
+// rest, and each state's update a typed atomic chosen at compile time.
+// ---------------------------------------------------------------------------
+template <class SH, int S = 0>
+__device__ __forceinline__ void ShapeApply(uint64_t* w, int64_t stride, const FastPlan& F,
+                                           const char* const (&cb)[kFastCols], int r) {
+    if constexpr (S < SH::n) {
+        constexpr int K = SH::kind(S);
+        constexpr int O = SH::off(S);
+        auto* u = reinterpret_cast<unsigned long long*>(w + O * stride);
+        if constexpr (K == SK_COUNT) {
+            atomicAdd(u, 1ull);
+        } else if constexpr (K == SK_SUMF64) {
+            const int64_t bits = ColVal<SH, SH::fcol(S, 0)>(cb, r);
+            atomicAdd(reinterpret_cast<double*>(u), __longlong_as_double((long long)bits));
+        } else if constexpr (K == SK_MIN64 || K == SK_MAX64) {
+            const int64_t v = ShapeFactor<SH, S, 0>(F, cb, r);
+            if constexpr (K == SK_MIN64) atomicMin(reinterpret_cast<long long*>(u), (long long)v);
+            else atomicMax(reinterpret_cast<long long*>(u), (long long)v);
+        } else {
+            uint64_t lo, hi;
+            ShapeProduct<SH, S, K == SK_SUM128>(F, cb, r, lo, hi);
+            if constexpr (K == SK_SUM64) {
+                atomicAdd(u, (unsigned long long)lo);
+            } else {
+                const unsigned long long old = atomicAdd(u, (unsigned long long)lo);
+                const unsigned long long carry = (old + lo < old) ? 1ull : 0ull;
+                if (hi + carry) atomicAdd(reinterpret_cast<unsigned long long*>(w + (O + 1) * stride), hi + carry);
+            }
+        }
+        ShapeApply<SH, S + 1>(w, stride, F, cb, r);
+    }
+}
+
+template <class SH>
+__global__ void __launch_bounds__(kAggThreads, 1) AggHighKernel(const __grid_constant__ AggLaunch L) {
+    unsigned char* smem = DynSmem();
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.off_bars);
+    unsigned* misc = reinterpret_cast<unsigned*>(smem + L.off_misc);
+    const SmemTable sm = MakeSmem(L, false, false);
+    const AggPlan& P = L.P;
+    const FastPlan& F = L.F;
+    const int tid = threadIdx.x;
+    const int bd = blockDim.x;
+    const int T = L.tile_rows;
+
+    if (tid == 0) {
+        misc[0] = 0;
+        misc[1] = 0;
+        misc[2] = 0;
+        misc[4] = 0;
+        for (int s = 0; s < L.stages; ++s) MbarInit(&full[s], 1);
+        FenceBarrierInit();
+    }
+    for (int i = tid; i < sm.S; i += bd) {
+        sm.keys[i] = kEmptyKey;
+        sm.gid[i] = -1;
+        for (int s = 0; s < P.nstates; ++s) {
+            const StateDesc sd = P.states[s];
+            sm.st[int64_t(sd.word) * sm.S + i] = StateIdentity(sd.kind);
+            if (sd.kind == ST_SUM_I128) sm.st[int64_t(sd.word + 1) * sm.S + i] = 0;
+        }
+    }
+    __syncthreads();
+
+    const int64_t ntiles = (L.nrows + T - 1) / T;
+    auto tile_full = [&](int64_t t) { return L.any_staged && (t + 1) * int64_t(T) <= L.nrows; };
+    auto issue = [&](int64_t t, int s) {
+        unsigned char* st = smem + int64_t(s) * L.stage_bytes;
+        FenceProxyAsync();
+        MbarArriveExpectTx(&full[s], uint32_t(L.stage_bytes));
+        for (int c = 0; c < P.ncols; ++c) {
+            const ColDesc& cd = P.cols[c];
+            if (!cd.stage) continue;
+            BulkG2S(st + cd.smem_off, cd.data + t * T * cd.width, uint32_t(T * cd.width), &full[s]);
+        }
+        if (L.sel_off >= 0) BulkG2S(st + L.sel_off, P.selection + t * T, uint32_t(T), &full[s]);
+    };
+    if (tid == 0) {
+        for (int k = 0; k < L.stages; ++k) {
+            const int64_t t = blockIdx.x + int64_t(k) * gridDim.x;
+            if (t < ntiles && tile_full(t)) issue(t, k);
+        }
+    }
+    int coff[kFastCols];
+#pragma unroll
+    for (int c = 0; c < kFastCols; ++c) {
+        coff[c] = -1;
+        if (c < SH::Cols::n) {
+            const ColDesc& cd = P.cols[F.col_slot[c]];
+            if (cd.stage) coff[c] = cd.smem_off;
+        }
+    }
+
+    bool aborted = false;
+    for (int64_t k = 0;; ++k) {
+        const int64_t t = blockIdx.x + k * gridDim.x;
+        if (t >= ntiles) break;
+        const int s = int(k % L.stages);
+        const uint32_t phase = uint32_t((k / L.stages) & 1);
+        const bool full_tile = tile_full(t);
+        const int64_t row0 = t * T;
+        const unsigned char* stage = full_tile ? smem + int64_t(s) * L.stage_bytes : nullptr;
+        if (full_tile && !MbarWaitBounded(&full[s], phase)) {
+            SetError(&L.counters->error, DE_WAIT_TIMEOUT);
+            *reinterpret_cast<volatile unsigned*>(&misc[4]) = 1;
+        }
+        if (*reinterpret_cast<volatile unsigned*>(&misc[4])) {
+            aborted = true;
+            break;
+        }
+        const int nrows = int(min(int64_t(T), L.nrows - row0));
+        const uint8_t* sel = P.selection == nullptr ? nullptr
+                             : (stage && L.sel_off >= 0) ? stage + L.sel_off : P.selection + row0;
+        const char* cb[kFastCols];
+#pragma unroll
+        for (int c = 0; c < kFastCols; ++c) {
+            cb[c] = nullptr;
+            if (c < SH::Cols::n) {
+                cb[c] = coff[c] >= 0 && stage ? reinterpret_cast<const char*>(stage) + coff[c]
+                                              : P.cols[F.col_slot[c]].data + row0 * SH::cw(c);
+            }
+        }
+        for (int r = tid; r < nrows; r += bd) {
+            if (sel && !sel[r]) continue;
+            if (SH::Atoms::n && ShapeHeld<SH>(P, F, cb, r) != F.clause_mask) continue;
+            const uint64_t key = ShapeKey<SH>(cb, r);
+            const bool special = P.key_full64 && key == kEmptyKey;
+            const int slot = special ? -1 : sm.Find(key);
+            if (slot >= 0) {
+                ShapeApply<SH>(sm.st + slot, sm.S, F, cb, r);
+                continue;
+            }
+            int64_t gslot;
+            if (special) {
+                gslot = L.T.capacity;
+                unsigned long long* flag = reinterpret_cast<unsigned long long*>(
+                    L.T.slots + L.T.capacity * L.T.slot_words + L.T.key_off);
+                if (*reinterpret_cast<volatile unsigned long long*>(flag) == 0 && atomicExch(flag, 1ull) == 0) {
+                    atomicAdd(sm.fresh, 1u);
+                }
+            } else {
+                int is_new = 0;
+                gslot = GlobalFind1(L.T, L.cap_mask, key, is_new);
+                if (is_new) atomicAdd(sm.fresh, 1u);
+            }
+            if (gslot < 0) {
+                Defer(L, row0 + r, 0);
+                continue;
+            }
+            ShapeApply<SH>(L.T.slots + gslot * L.T.slot_words + L.T.state_off, 1, F, cb, r);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const int64_t nt = t + int64_t(L.stages) * gridDim.x;
+            if (nt < ntiles && tile_full(nt)) issue(nt, s);
+        }
+    }
+    __syncthreads();
+    if (aborted || *reinterpret_cast<volatile unsigned*>(&misc[4])) {
+        if (tid == 0) {
+            const long long start = clock64();
+            while (clock64() - start < 2000000) {
+            }
+        }
+        __syncthreads();
+        return;
+    }
+
+    // Shared table -> global table.
+    for (int i = tid; i < sm.S; i += bd) {
+        const uint64_t key = sm.keys[i];
+        if (key == kEmptyKey) continue;
+        int is_new = 0;
+        const int64_t g = GlobalFind1(L.T, L.cap_mask, key, is_new);
+        if (is_new) atomicAdd(sm.fresh, 1u);
+        if (g < 0) {
+            const unsigned long long e = atomicAdd(&L.counters->spilled, 1ull);
+            if (int64_t(e) >= L.spill_cap) {
+                SetError(&L.counters->error, DE_SPILL_FULL);
+                continue;
+            }
+            uint64_t* rec = L.spill + int64_t(e) * (1 + P.state_words);
+            rec[0] = key;
+            for (int w = 0; w < P.state_words; ++w) rec[1 + w] = sm.st[int64_t(w) * sm.S + i];
+            continue;
+        }
+        uint64_t* gbase = L.T.slots + g * L.T.slot_words + L.T.state_off;
+        for (int st2 = 0; st2 < P.nstates; ++st2) {
+            const StateDesc sd = P.states[st2];
+            const uint64_t lo = sm.st[int64_t(sd.word) * sm.S + i];
+            const uint64_t hi = sd.kind == ST_SUM_I128 ? sm.st[int64_t(sd.word + 1) * sm.S + i] : 0;
+            if (IsIdentity(sd.kind, lo, hi)) continue;
+            double f;
+            __builtin_memcpy(&f, &lo, 8);
+            ApplyState(gbase + sd.word, gbase + sd.word + 1, sd.kind, lo, hi, f);
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
+}
+
 // The instantiated query shapes.  QDB_C(w, u): a fast column of w bytes
 // (u: unsigned); QDB_A(op, col): a filter atom; QDB_S(kind, nf, cols...): a
 // state.  A plan whose shape is not listed runs the general typed kernel.
@@ -1406,6 +1616,18 @@ __global__ void __launch_bounds__(kSigThreads, 1) AggSigKernel(const __grid_cons
     /* keyless SUM(x * y) WHERE x BETWEEN a AND b over 8-byte columns (a TPC-H Q6 shape) */                  \
     X(Shape<IntList<QDB_C(8, 0), QDB_C(8, 0)>, IntList<QDB_A(AT_BETWEEN, 0)>, IntList<>,                      \
             IntList<QDB_S(SK_SUM64, 2, 0, 1), QDB_S(SK_COUNT, 0)>>)
+
+// Shapes of the high-cardinality kernel (global table, typed atomics).
+#define QDB_HIGH_SHAPE_LIST(X)                                                                               \
+    /* GROUP BY an 8-byte key: COUNT(*), SUM(a), MIN(a), MAX(a), SUM(double x) */                          \
+    X(Shape<IntList<QDB_C(8, 0), QDB_C(8, 0), QDB_C(8, 0)>, IntList<>, IntList<KeyCode(0, 64, 0)>,            \
+            IntList<QDB_S(SK_COUNT, 0), QDB_S(SK_SUM64, 1, 1), QDB_S(SK_MIN64, 1, 1), QDB_S(SK_MAX64, 1, 1),    \
+                    QDB_S(SK_SUMF64, 1, 2)>>)                                                                 \
+    /* COUNT(*) GROUP BY an 8-byte key */                                                                    \
+    X(Shape<IntList<QDB_C(8, 0)>, IntList<>, IntList<KeyCode(0, 64, 0)>, IntList<QDB_S(SK_COUNT, 0)>>)        \
+    /* SUM(x), COUNT(*) GROUP BY an 8-byte key */                                                            \
+    X(Shape<IntList<QDB_C(8, 0), QDB_C(8, 0)>, IntList<>, IntList<KeyCode(0, 64, 0)>,                         \
+            IntList<QDB_S(SK_SUM64, 1, 1), QDB_S(SK_COUNT, 0)>>)
 
 // Index mode: rows named by (row, build row) pairs, global table only.
 template <bool WIDE>
@@ -1779,11 +2001,14 @@ std::vector<int> ShapeKeyOf(const AggPlan& P, const FastPlan& F) {
             case ST_COUNT: kind = SK_COUNT; break;
             case ST_SUM_I64: kind = SK_SUM64; break;
             case ST_SUM_I128: kind = st.wide ? SK_SUM128 : SK_SUM128_OF64; break;
+            case ST_MIN_I64: kind = SK_MIN64; break;
+            case ST_MAX_I64: kind = SK_MAX64; break;
+            case ST_SUM_F64: kind = SK_SUMF64; break;
             default: return {};
         }
         if ((kind == SK_COUNT) != (st.nf == 0)) return {};
         auto form = [&](int j) {
-            if (j >= st.nf) return 0;
+            if (j >= st.nf || kind == SK_SUMF64) return 0;
             const FastFactor& f = st.f[j];
             if (f.d == 1) return f.c == 0 ? int(FF_X) : int(FF_ADD);
             if (f.d == -1) return int(FF_SUB);
@@ -1798,6 +2023,17 @@ std::vector<int> ShapeKeyOf(const AggPlan& P, const FastPlan& F) {
 template <class LIST>
 void AppendList(std::vector<int>& key) {
     for (int i = 0; i < LIST::n; ++i) key.push_back(LIST::at(i));
+}
+
+// The shape's compile-time state words must be the plan's (the kernels
+// address the table's state words by them).
+template <class SH>
+bool ShapeWordsMatch(const FastPlan& F) {
+    if (SH::n != F.nstates) return false;
+    for (int s = 0; s < SH::n; ++s) {
+        if (SH::off(s) != F.states[s].word) return false;
+    }
+    return true;
 }
 
 template <class SH>
@@ -1815,10 +2051,26 @@ bool ShapeMatches(const std::vector<int>& key) {
 
 using SigKernelFn = void (*)(AggLaunch);
 
+SigKernelFn FindHighKernel(const AggPlan& P, const FastPlan& F) {
+    const std::vector<int> key = ShapeKeyOf(P, F);
+    if (key.empty()) return nullptr;
+#define QDB_SHAPE_FIND(...) \
+    if (ShapeMatches<__VA_ARGS__>(key) && ShapeWordsMatch<__VA_ARGS__>(F)) return AggHighKernel<__VA_ARGS__>;
+    QDB_HIGH_SHAPE_LIST(QDB_SHAPE_FIND)
+#undef QDB_SHAPE_FIND
+    if (std::getenv("QDB_SHAPE_DEBUG")) {
+        std::fprintf(stderr, "qdb: no compiled high-cardinality shape for key");
+        for (int v : key) std::fprintf(stderr, " %d", v);
+        std::fprintf(stderr, "\n");
+    }
+    return nullptr;
+}
+
 SigKernelFn FindSigKernel(const AggPlan& P, const FastPlan& F) {
     const std::vector<int> key = ShapeKeyOf(P, F);
     if (key.empty()) return nullptr;
-#define QDB_SHAPE_FIND(...) if (ShapeMatches<__VA_ARGS__>(key)) return AggSigKernel<__VA_ARGS__>;
+#define QDB_SHAPE_FIND(...) \
+    if (ShapeMatches<__VA_ARGS__>(key) && ShapeWordsMatch<__VA_ARGS__>(F)) return AggSigKernel<__VA_ARGS__>;
     QDB_SHAPE_LIST(QDB_SHAPE_FIND)
 #undef QDB_SHAPE_FIND
     if (std::getenv("QDB_SHAPE_DEBUG")) {
@@ -1971,6 +2223,17 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
                 return;
             }
             layout(T, stages, S);
+        }
+    }
+    if (a.fast && variant == 0 && any) {
+        if (SigKernelFn fn = FindHighKernel(L.P, *a.fast)) {
+            L.F = *a.fast;
+            SetSmem(fn, smem_bytes);
+            ProfileBegin(s, "agg_update_high", a.nrows);
+            fn<<<grid, kAggThreads, smem_bytes, s>>>(L);
+            ProfileEnd(s);
+            CountLaunch();
+            return;
         }
     }
     const char* name = a.join ? "join_agg_probe" : "agg_update";

@@ -237,3 +237,37 @@ def test_lineitem_runs_the_signature_kernel():
     assert "agg_update_sig" in names, names
     want = O.aggregate(spec, [q.HostRowSet(cols)])
     assert_same_groups(got, want, queries.LINEITEM_OUT_TYPES, nkeys=2)
+
+
+@pytest.mark.parametrize("shape", ["zipf", "count", "sum_count"])
+def test_high_cardinality_shape_kernels(shape):
+    """The high-cardinality shape kernel (shared tier for hot keys, global
+    table for the rest, typed atomics) on a skewed key stream whose groups
+    overflow the initial table (growth and replay of deferred rows)."""
+    n = 400_000
+    cols = zipf_data(n, 60_000, 4)
+    e = q.ExprBuilder()
+    key, a, x = e.col(0, abi.I64), e.col(1, abi.I64), e.col(2, abi.F64)
+    if shape == "zipf":
+        spec = queries.zipf_agg(expected_groups=2000)
+        types = queries.ZIPF_OUT_TYPES
+    elif shape == "count":
+        spec = queries.AggSpec(queries.ZIPF_COLUMNS[:1], e, None, [key], [(abi.COUNT_STAR, -1)], expected_groups=2000)
+        cols = cols[:1]
+        types = [abi.I64, abi.I64]
+    else:
+        spec = queries.AggSpec(queries.ZIPF_COLUMNS[:2], e, None, [key], [(abi.SUM, a), (abi.COUNT_STAR, -1)],
+                               expected_groups=2000)
+        cols = cols[:2]
+        types = [abi.I64, abi.I64, abi.I64]
+    bounds = [(0, 150_000), (150_000, 300_000), (300_000, n)]
+    q.profile(True)
+    q.profile_read()
+    out = run_gpu(spec, [q.DeviceRowSet([c[lo:hi] for c in cols]) for lo, hi in bounds], initial_capacity=1024)
+    names = {kk[0] for kk in q.profile_read()}
+    q.profile(False)
+    got = gpu_rows(out, types)
+    q.release(out)
+    assert "agg_update_high" in names, names
+    want = O.aggregate(spec, [q.HostRowSet([c[lo:hi] for c in cols]) for lo, hi in bounds])
+    assert_same_groups(got, want, types, nkeys=1)
