@@ -1394,34 +1394,77 @@ __global__ void __launch_bounds__(kSigThreads, 1) AggSigKernel(const __grid_cons
 // hot keys of a skewed stream settle there), the global HBM table for the
 // rest, and each state's update a typed atomic chosen at compile time.
 // ---------------------------------------------------------------------------
+// One row's contribution to every state (COUNT 1, sums, min/max values,
+// double bits), combined over the rows of one key within a warp.
+template <class SH>
+struct ShapeVals {
+    uint64_t lo[SH::n];
+    uint64_t hi[SH::n];
+};
+
 template <class SH, int S = 0>
-__device__ __forceinline__ void ShapeApply(uint64_t* w, int64_t stride, const FastPlan& F,
-                                           const char* const (&cb)[kFastCols], int r) {
+__device__ __forceinline__ void ShapeRowVals(ShapeVals<SH>& v, const FastPlan& F, const char* const (&cb)[kFastCols],
+                                             int r) {
+    if constexpr (S < SH::n) {
+        constexpr int K = SH::kind(S);
+        v.hi[S] = 0;
+        if constexpr (K == SK_COUNT) {
+            v.lo[S] = 1;
+        } else if constexpr (K == SK_SUMF64) {
+            v.lo[S] = uint64_t(ColVal<SH, SH::fcol(S, 0)>(cb, r));
+        } else if constexpr (K == SK_MIN64 || K == SK_MAX64) {
+            v.lo[S] = uint64_t(ShapeFactor<SH, S, 0>(F, cb, r));
+        } else {
+            ShapeProduct<SH, S, K == SK_SUM128>(F, cb, r, v.lo[S], v.hi[S]);
+        }
+        ShapeRowVals<SH, S + 1>(v, F, cb, r);
+    }
+}
+
+// a <- a (+) b state by state.
+template <class SH, int S = 0>
+__device__ __forceinline__ void ShapeCombine(ShapeVals<SH>& a, const ShapeVals<SH>& b) {
+    if constexpr (S < SH::n) {
+        constexpr int K = SH::kind(S);
+        if constexpr (K == SK_SUMF64) {
+            a.lo[S] = uint64_t(__double_as_longlong(__longlong_as_double((long long)a.lo[S]) +
+                                                    __longlong_as_double((long long)b.lo[S])));
+        } else if constexpr (K == SK_MIN64) {
+            if (int64_t(b.lo[S]) < int64_t(a.lo[S])) a.lo[S] = b.lo[S];
+        } else if constexpr (K == SK_MAX64) {
+            if (int64_t(b.lo[S]) > int64_t(a.lo[S])) a.lo[S] = b.lo[S];
+        } else if constexpr (SH::width(S) == 2) {
+            Add128(a.lo[S], a.hi[S], b.lo[S], b.hi[S]);
+        } else {
+            a.lo[S] += b.lo[S];
+        }
+        ShapeCombine<SH, S + 1>(a, b);
+    }
+}
+
+// Folds combined values into state words w[O * stride] with atomics.
+template <class SH, int S = 0>
+__device__ __forceinline__ void ShapeAtomics(uint64_t* w, int64_t stride, const ShapeVals<SH>& v) {
     if constexpr (S < SH::n) {
         constexpr int K = SH::kind(S);
         constexpr int O = SH::off(S);
         auto* u = reinterpret_cast<unsigned long long*>(w + O * stride);
-        if constexpr (K == SK_COUNT) {
-            atomicAdd(u, 1ull);
-        } else if constexpr (K == SK_SUMF64) {
-            const int64_t bits = ColVal<SH, SH::fcol(S, 0)>(cb, r);
-            atomicAdd(reinterpret_cast<double*>(u), __longlong_as_double((long long)bits));
-        } else if constexpr (K == SK_MIN64 || K == SK_MAX64) {
-            const int64_t v = ShapeFactor<SH, S, 0>(F, cb, r);
-            if constexpr (K == SK_MIN64) atomicMin(reinterpret_cast<long long*>(u), (long long)v);
-            else atomicMax(reinterpret_cast<long long*>(u), (long long)v);
-        } else {
-            uint64_t lo, hi;
-            ShapeProduct<SH, S, K == SK_SUM128>(F, cb, r, lo, hi);
-            if constexpr (K == SK_SUM64) {
-                atomicAdd(u, (unsigned long long)lo);
-            } else {
-                const unsigned long long old = atomicAdd(u, (unsigned long long)lo);
-                const unsigned long long carry = (old + lo < old) ? 1ull : 0ull;
-                if (hi + carry) atomicAdd(reinterpret_cast<unsigned long long*>(w + (O + 1) * stride), hi + carry);
+        if constexpr (K == SK_SUMF64) {
+            atomicAdd(reinterpret_cast<double*>(u), __longlong_as_double((long long)v.lo[S]));
+        } else if constexpr (K == SK_MIN64) {
+            atomicMin(reinterpret_cast<long long*>(u), (long long)v.lo[S]);
+        } else if constexpr (K == SK_MAX64) {
+            atomicMax(reinterpret_cast<long long*>(u), (long long)v.lo[S]);
+        } else if constexpr (SH::width(S) == 2) {
+            const unsigned long long old = atomicAdd(u, (unsigned long long)v.lo[S]);
+            const unsigned long long carry = (old + v.lo[S] < old) ? 1ull : 0ull;
+            if (v.hi[S] + carry) {
+                atomicAdd(reinterpret_cast<unsigned long long*>(w + (O + 1) * stride), v.hi[S] + carry);
             }
+        } else {
+            atomicAdd(u, (unsigned long long)v.lo[S]);
         }
-        ShapeApply<SH, S + 1>(w, stride, F, cb, r);
+        ShapeAtomics<SH, S + 1>(w, stride, v);
     }
 }
 
@@ -1514,14 +1557,33 @@ __global__ void __launch_bounds__(kAggThreads, 1) AggHighKernel(const __grid_con
                                               : P.cols[F.col_slot[c]].data + row0 * SH::cw(c);
             }
         }
-        for (int r = tid; r < nrows; r += bd) {
-            if (sel && !sel[r]) continue;
-            if (SH::Atoms::n && ShapeHeld<SH>(P, F, cb, r) != F.clause_mask) continue;
+        for (int rb = 0; rb < nrows; rb += bd) {
+            const int r = rb + tid;
+            bool ok = r < nrows && (!sel || sel[r]);
+            if (ok && SH::Atoms::n) ok = ShapeHeld<SH>(P, F, cb, r) == F.clause_mask;
+            const unsigned act = __ballot_sync(kFull, ok);
+            if (!ok) continue;
             const uint64_t key = ShapeKey<SH>(cb, r);
+            // Rows of one key in this warp fold into their lowest lane first.
+            ShapeVals<SH> v;
+            ShapeRowVals<SH>(v, F, cb, r);
+            const unsigned peers = __match_any_sync(act, key);
+            const int lane = tid & 31;
+            const int leader = __ffs(peers) - 1;
+            if (peers != (1u << lane)) {
+                ShapeVals<SH>* xs = reinterpret_cast<ShapeVals<SH>*>(smem + L.off_pacc) + (tid & ~31);
+                xs[lane] = v;
+                __syncwarp(peers);
+                if (lane == leader) {
+                    for (unsigned m = peers & (peers - 1); m; m &= m - 1) ShapeCombine<SH>(v, xs[__ffs(m) - 1]);
+                }
+                __syncwarp(peers);
+                if (lane != leader) continue;
+            }
             const bool special = P.key_full64 && key == kEmptyKey;
             const int slot = special ? -1 : sm.Find(key);
             if (slot >= 0) {
-                ShapeApply<SH>(sm.st + slot, sm.S, F, cb, r);
+                ShapeAtomics<SH>(sm.st + slot, sm.S, v);
                 continue;
             }
             int64_t gslot;
@@ -1538,10 +1600,11 @@ __global__ void __launch_bounds__(kAggThreads, 1) AggHighKernel(const __grid_con
                 if (is_new) atomicAdd(sm.fresh, 1u);
             }
             if (gslot < 0) {
-                Defer(L, row0 + r, 0);
+                // Replayed row by row after the table grows: every row of the group.
+                for (unsigned m = peers; m; m &= m - 1) Defer(L, row0 + rb + (tid & ~31) + (__ffs(m) - 1), 0);
                 continue;
             }
-            ShapeApply<SH>(L.T.slots + gslot * L.T.slot_words + L.T.state_off, 1, F, cb, r);
+            ShapeAtomics<SH>(L.T.slots + gslot * L.T.slot_words + L.T.state_off, 1, v);
         }
         __syncthreads();
         if (tid == 0) {
@@ -2227,13 +2290,26 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
     }
     if (a.fast && variant == 0 && any) {
         if (SigKernelFn fn = FindHighKernel(L.P, *a.fast)) {
-            L.F = *a.fast;
-            SetSmem(fn, smem_bytes);
-            ProfileBegin(s, "agg_update_high", a.nrows);
-            fn<<<grid, kAggThreads, smem_bytes, s>>>(L);
-            ProfileEnd(s);
-            CountLaunch();
-            return;
+            // Room after the shared table for each thread's combine scratch.
+            const size_t scratch = size_t(kAggThreads) * 16 * a.fast->nstates;
+            int S2 = S;
+            size_t bytes = layout(T, stages, S2) + scratch;
+            while (bytes > budget && S2 > 256) {
+                S2 >>= 1;
+                bytes = layout(T, stages, S2) + scratch;
+            }
+            if (bytes <= budget) {
+                L.smem_slots = S2;
+                L.smem_limit = S2 / 2;
+                L.F = *a.fast;
+                SetSmem(fn, bytes);
+                ProfileBegin(s, "agg_update_high", a.nrows);
+                fn<<<grid, kAggThreads, bytes, s>>>(L);
+                ProfileEnd(s);
+                CountLaunch();
+                return;
+            }
+            layout(T, stages, S);
         }
     }
     const char* name = a.join ? "join_agg_probe" : "agg_update";
