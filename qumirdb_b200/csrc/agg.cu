@@ -1468,192 +1468,289 @@ __device__ __forceinline__ void ShapeAtomics(uint64_t* w, int64_t stride, const 
     }
 }
 
+// Shared-memory adds of the high-cardinality kernel.  A 64-bit add goes as
+// two native 32-bit adds: the low half's carry (read from the value the
+// atomic returned) joins the high half, so the pair sums exactly mod 2^64.
+__device__ __forceinline__ void SmemAdd64(uint64_t* p, uint64_t v) {
+    unsigned* q = reinterpret_cast<unsigned*>(p);
+    const unsigned lo = unsigned(v);
+    const unsigned hi = unsigned(v >> 32);
+    const unsigned old = atomicAdd(q, lo);
+    const unsigned up = hi + (old + lo < old ? 1u : 0u);
+    if (up) atomicAdd(q + 1, up);
+}
+
+// Folds combined values into the shared tier's state words w[O * stride].
+// MIN/MAX read the word first: once a hot group's extreme has settled, most
+// rows change nothing and need no atomic.
+template <class SH, int S = 0>
+__device__ __forceinline__ void ShapeSmemAtomics(uint64_t* w, int stride, const ShapeVals<SH>& v) {
+    if constexpr (S < SH::n) {
+        constexpr int K = SH::kind(S);
+        constexpr int O = SH::off(S);
+        uint64_t* p = w + O * stride;
+        if constexpr (K == SK_SUMF64) {
+            atomicAdd(reinterpret_cast<double*>(p), __longlong_as_double((long long)v.lo[S]));
+        } else if constexpr (K == SK_MIN64) {
+            if (int64_t(v.lo[S]) < *reinterpret_cast<volatile int64_t*>(p)) {
+                atomicMin(reinterpret_cast<long long*>(p), (long long)v.lo[S]);
+            }
+        } else if constexpr (K == SK_MAX64) {
+            if (int64_t(v.lo[S]) > *reinterpret_cast<volatile int64_t*>(p)) {
+                atomicMax(reinterpret_cast<long long*>(p), (long long)v.lo[S]);
+            }
+        } else if constexpr (SH::width(S) == 2) {
+            auto* u = reinterpret_cast<unsigned long long*>(p);
+            const unsigned long long old = atomicAdd(u, (unsigned long long)v.lo[S]);
+            const unsigned long long carry = (old + v.lo[S] < old) ? 1ull : 0ull;
+            if (v.hi[S] + carry) atomicAdd(reinterpret_cast<unsigned long long*>(w + (O + 1) * stride), v.hi[S] + carry);
+        } else {
+            SmemAdd64(p, v.lo[S]);
+        }
+        ShapeSmemAtomics<SH, S + 1>(w, stride, v);
+    }
+}
+
+constexpr int kHighThreads = 1024;
+constexpr int kHighSmemProbe = 16;   // shared-tier probes before a row goes to the global table
+
+// Shared tier of the high-cardinality kernel: S one-word keys, the state
+// words of slot i at st[w * S + i].  Its index comes from the high bits of
+// the key's hash, the global table's from the low bits.
+struct HighSmem {
+    uint64_t* keys;
+    uint64_t* st;
+    unsigned* count;    // keys inserted
+    unsigned* fresh;    // global groups this CTA created
+    int S;
+    int limit;
+
+    __device__ __forceinline__ int Find(uint64_t h, uint64_t key) const {
+        uint32_t i = uint32_t(h >> 40) & uint32_t(S - 1);
+#pragma unroll 1
+        for (int p = 0; p < kHighSmemProbe; ++p) {
+            const uint64_t cur = *reinterpret_cast<volatile uint64_t*>(&keys[i]);
+            if (cur == key) return int(i);
+            if (cur == kEmptyKey) {
+                if (*reinterpret_cast<volatile unsigned*>(count) >= unsigned(limit)) return -1;
+                const uint64_t old = atomicCAS(reinterpret_cast<unsigned long long*>(&keys[i]), kEmptyKey, key);
+                if (old == kEmptyKey) {
+                    atomicAdd(count, 1u);
+                    return int(i);
+                }
+                if (old == key) return int(i);
+            }
+            i = (i + 1) & uint32_t(S - 1);
+        }
+        return -1;
+    }
+};
+
+__device__ __forceinline__ int64_t GlobalFindH(const GTableDev& T, uint64_t mask, uint64_t h, uint64_t key,
+                                               int& is_new) {
+    uint64_t i = h & mask;
+#pragma unroll 1
+    for (int p = 0; p < kMaxProbe; ++p) {
+        unsigned long long* kp =
+            reinterpret_cast<unsigned long long*>(T.slots + int64_t(i) * T.slot_words + T.key_off);
+        const uint64_t cur = *reinterpret_cast<volatile unsigned long long*>(kp);
+        if (cur == key) return int64_t(i);
+        if (cur == kEmptyKey) {
+            const uint64_t old = atomicCAS(kp, kEmptyKey, key);
+            if (old == kEmptyKey) {
+                is_new = 1;
+                return int64_t(i);
+            }
+            if (old == key) return int64_t(i);
+        }
+        i = (i + 1) & mask;
+    }
+    return -1;
+}
+
+// Shared tier layout inside dynamic shared memory: misc words, keys, state
+// words, then each warp's combine scratch.
+struct HighLayout {
+    int off_keys;
+    int off_st;
+    int off_scratch;
+    int bytes;
+};
+
+__host__ __device__ inline HighLayout HighLayoutOf(int S, int state_words, int nstates, int threads) {
+    HighLayout h;
+    h.off_keys = 128;
+    h.off_st = h.off_keys + S * 8;
+    h.off_scratch = h.off_st + S * state_words * 8;
+    h.bytes = h.off_scratch + threads * 16 * nstates;
+    return h;
+}
+
+// One range of rows through the tiers: each warp takes 32 consecutive rows
+// at a time (coalesced loads straight from HBM, no staging and no block
+// barrier), folds the rows of one key into their lowest lane, then the
+// leader updates the shared tier or, when its key is not there, the global
+// table.  `defer_base` numbers the range's rows for the replay list.
 template <class SH>
-__global__ void __launch_bounds__(kAggThreads, 1) AggHighKernel(const __grid_constant__ AggLaunch L) {
-    unsigned char* smem = DynSmem();
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.off_bars);
-    unsigned* misc = reinterpret_cast<unsigned*>(smem + L.off_misc);
-    const SmemTable sm = MakeSmem(L, false, false);
+__device__ __forceinline__ void HighRows(const AggLaunch& L, const HighSmem& sm, ShapeVals<SH>* xs,
+                                         const char* const (&cb)[kFastCols], const uint8_t* sel, int nrows,
+                                         int64_t defer_base, int wid, int nw) {
     const AggPlan& P = L.P;
     const FastPlan& F = L.F;
-    const int tid = threadIdx.x;
-    const int bd = blockDim.x;
-    const int T = L.tile_rows;
-
-    if (tid == 0) {
-        misc[0] = 0;
-        misc[1] = 0;
-        misc[2] = 0;
-        misc[4] = 0;
-        for (int s = 0; s < L.stages; ++s) MbarInit(&full[s], 1);
-        FenceBarrierInit();
+    const int lane = threadIdx.x & 31;
+#pragma unroll 1
+    for (int base = wid * 32; base < nrows; base += nw * 32) {
+        const int r = base + lane;
+        bool ok = r < nrows && (!sel || sel[r]);
+        if (ok && SH::Atoms::n) ok = ShapeHeld<SH>(P, F, cb, r) == F.clause_mask;
+        const unsigned act = __ballot_sync(kFull, ok);
+        if (!ok) continue;
+        const uint64_t key = ShapeKey<SH>(cb, r);
+        ShapeVals<SH> v;
+        ShapeRowVals<SH>(v, F, cb, r);
+        const unsigned peers = __match_any_sync(act, key);
+        if (peers != (1u << lane)) {
+            const int leader = __ffs(peers) - 1;
+            xs[lane] = v;
+            __syncwarp(peers);
+            if (lane == leader) {
+                for (unsigned m = peers & (peers - 1); m; m &= m - 1) ShapeCombine<SH>(v, xs[__ffs(m) - 1]);
+            }
+            __syncwarp(peers);
+            if (lane != leader) continue;
+        }
+        const uint64_t h = Fmix64(key);
+        const bool special = P.key_full64 && key == kEmptyKey;
+        if (!special) {
+            const int slot = sm.Find(h, key);
+            if (slot >= 0) {
+                ShapeSmemAtomics<SH>(sm.st + slot, sm.S, v);
+                continue;
+            }
+        }
+        int64_t gslot;
+        if (special) {
+            gslot = L.T.capacity;
+            unsigned long long* flag =
+                reinterpret_cast<unsigned long long*>(L.T.slots + L.T.capacity * L.T.slot_words + L.T.key_off);
+            if (*reinterpret_cast<volatile unsigned long long*>(flag) == 0 && atomicExch(flag, 1ull) == 0) {
+                atomicAdd(sm.fresh, 1u);
+            }
+        } else {
+            int is_new = 0;
+            gslot = GlobalFindH(L.T, L.cap_mask, h, key, is_new);
+            if (is_new) atomicAdd(sm.fresh, 1u);
+        }
+        if (gslot < 0) {
+            // Replayed row by row after the table grows: every row of the group.
+            for (unsigned m = peers; m; m &= m - 1) Defer(L, defer_base + base + (__ffs(m) - 1), 0);
+            continue;
+        }
+        ShapeAtomics<SH>(L.T.slots + gslot * L.T.slot_words + L.T.state_off, 1, v);
     }
-    for (int i = tid; i < sm.S; i += bd) {
+}
+
+// Shared tier -> global table (spilling what the global table cannot take),
+// then clears the tier for the next range.  Called by the whole CTA.
+__device__ __forceinline__ void HighFlush(const AggLaunch& L, const HighSmem& sm, bool reset) {
+    const AggPlan& P = L.P;
+    for (int i = threadIdx.x; i < sm.S; i += blockDim.x) {
+        const uint64_t key = sm.keys[i];
+        if (key == kEmptyKey) continue;
+        int is_new = 0;
+        const int64_t g = GlobalFindH(L.T, L.cap_mask, Fmix64(key), key, is_new);
+        if (is_new) atomicAdd(sm.fresh, 1u);
+        if (g < 0) {
+            const unsigned long long e = atomicAdd(&L.counters->spilled, 1ull);
+            if (int64_t(e) >= L.spill_cap) {
+                SetError(&L.counters->error, DE_SPILL_FULL);
+            } else {
+                uint64_t* rec = L.spill + int64_t(e) * (1 + P.state_words);
+                rec[0] = key;
+                for (int w = 0; w < P.state_words; ++w) rec[1 + w] = sm.st[int64_t(w) * sm.S + i];
+            }
+        } else {
+            uint64_t* gbase = L.T.slots + g * L.T.slot_words + L.T.state_off;
+            for (int st2 = 0; st2 < P.nstates; ++st2) {
+                const StateDesc sd = P.states[st2];
+                const uint64_t lo = sm.st[int64_t(sd.word) * sm.S + i];
+                const uint64_t hi = sd.kind == ST_SUM_I128 ? sm.st[int64_t(sd.word + 1) * sm.S + i] : 0;
+                if (IsIdentity(sd.kind, lo, hi)) continue;
+                double f;
+                __builtin_memcpy(&f, &lo, 8);
+                ApplyState(gbase + sd.word, gbase + sd.word + 1, sd.kind, lo, hi, f);
+            }
+        }
+        if (reset) {
+            sm.keys[i] = kEmptyKey;
+            for (int s = 0; s < P.nstates; ++s) {
+                const StateDesc sd = P.states[s];
+                sm.st[int64_t(sd.word) * sm.S + i] = StateIdentity(sd.kind);
+                if (sd.kind == ST_SUM_I128) sm.st[int64_t(sd.word + 1) * sm.S + i] = 0;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ HighSmem HighSmemOf(const AggLaunch& L, const HighLayout& hl) {
+    unsigned char* smem = DynSmem();
+    HighSmem sm;
+    sm.count = reinterpret_cast<unsigned*>(smem);
+    sm.fresh = sm.count + 1;
+    sm.keys = reinterpret_cast<uint64_t*>(smem + hl.off_keys);
+    sm.st = reinterpret_cast<uint64_t*>(smem + hl.off_st);
+    sm.S = L.smem_slots;
+    sm.limit = L.smem_limit;
+    return sm;
+}
+
+__device__ __forceinline__ void HighInit(const AggLaunch& L, const HighSmem& sm) {
+    const AggPlan& P = L.P;
+    if (threadIdx.x == 0) {
+        sm.count[0] = 0;
+        sm.fresh[0] = 0;
+    }
+    for (int i = threadIdx.x; i < sm.S; i += blockDim.x) {
         sm.keys[i] = kEmptyKey;
-        sm.gid[i] = -1;
         for (int s = 0; s < P.nstates; ++s) {
             const StateDesc sd = P.states[s];
             sm.st[int64_t(sd.word) * sm.S + i] = StateIdentity(sd.kind);
             if (sd.kind == ST_SUM_I128) sm.st[int64_t(sd.word + 1) * sm.S + i] = 0;
         }
     }
-    __syncthreads();
+}
 
-    const int64_t ntiles = (L.nrows + T - 1) / T;
-    auto tile_full = [&](int64_t t) { return L.any_staged && (t + 1) * int64_t(T) <= L.nrows; };
-    auto issue = [&](int64_t t, int s) {
-        unsigned char* st = smem + int64_t(s) * L.stage_bytes;
-        FenceProxyAsync();
-        MbarArriveExpectTx(&full[s], uint32_t(L.stage_bytes));
-        for (int c = 0; c < P.ncols; ++c) {
-            const ColDesc& cd = P.cols[c];
-            if (!cd.stage) continue;
-            BulkG2S(st + cd.smem_off, cd.data + t * T * cd.width, uint32_t(T * cd.width), &full[s]);
-        }
-        if (L.sel_off >= 0) BulkG2S(st + L.sel_off, P.selection + t * T, uint32_t(T), &full[s]);
-    };
-    if (tid == 0) {
-        for (int k = 0; k < L.stages; ++k) {
-            const int64_t t = blockIdx.x + int64_t(k) * gridDim.x;
-            if (t < ntiles && tile_full(t)) issue(t, k);
-        }
-    }
-    int coff[kFastCols];
+template <class SH>
+__device__ __forceinline__ void HighColumns(const AggLaunch& L, int64_t row0, const char* (&cb)[kFastCols]) {
 #pragma unroll
     for (int c = 0; c < kFastCols; ++c) {
-        coff[c] = -1;
-        if (c < SH::Cols::n) {
-            const ColDesc& cd = P.cols[F.col_slot[c]];
-            if (cd.stage) coff[c] = cd.smem_off;
-        }
+        cb[c] = nullptr;
+        if (c < SH::Cols::n) cb[c] = L.P.cols[L.F.col_slot[c]].data + row0 * SH::cw(c);
     }
+}
 
-    bool aborted = false;
-    for (int64_t k = 0;; ++k) {
-        const int64_t t = blockIdx.x + k * gridDim.x;
-        if (t >= ntiles) break;
-        const int s = int(k % L.stages);
-        const uint32_t phase = uint32_t((k / L.stages) & 1);
-        const bool full_tile = tile_full(t);
-        const int64_t row0 = t * T;
-        const unsigned char* stage = full_tile ? smem + int64_t(s) * L.stage_bytes : nullptr;
-        if (full_tile && !MbarWaitBounded(&full[s], phase)) {
-            SetError(&L.counters->error, DE_WAIT_TIMEOUT);
-            *reinterpret_cast<volatile unsigned*>(&misc[4]) = 1;
-        }
-        if (*reinterpret_cast<volatile unsigned*>(&misc[4])) {
-            aborted = true;
-            break;
-        }
-        const int nrows = int(min(int64_t(T), L.nrows - row0));
-        const uint8_t* sel = P.selection == nullptr ? nullptr
-                             : (stage && L.sel_off >= 0) ? stage + L.sel_off : P.selection + row0;
-        const char* cb[kFastCols];
-#pragma unroll
-        for (int c = 0; c < kFastCols; ++c) {
-            cb[c] = nullptr;
-            if (c < SH::Cols::n) {
-                cb[c] = coff[c] >= 0 && stage ? reinterpret_cast<const char*>(stage) + coff[c]
-                                              : P.cols[F.col_slot[c]].data + row0 * SH::cw(c);
-            }
-        }
-        for (int rb = 0; rb < nrows; rb += bd) {
-            const int r = rb + tid;
-            bool ok = r < nrows && (!sel || sel[r]);
-            if (ok && SH::Atoms::n) ok = ShapeHeld<SH>(P, F, cb, r) == F.clause_mask;
-            const unsigned act = __ballot_sync(kFull, ok);
-            if (!ok) continue;
-            const uint64_t key = ShapeKey<SH>(cb, r);
-            // Rows of one key in this warp fold into their lowest lane first.
-            ShapeVals<SH> v;
-            ShapeRowVals<SH>(v, F, cb, r);
-            const unsigned peers = __match_any_sync(act, key);
-            const int lane = tid & 31;
-            const int leader = __ffs(peers) - 1;
-            if (peers != (1u << lane)) {
-                ShapeVals<SH>* xs = reinterpret_cast<ShapeVals<SH>*>(smem + L.off_pacc) + (tid & ~31);
-                xs[lane] = v;
-                __syncwarp(peers);
-                if (lane == leader) {
-                    for (unsigned m = peers & (peers - 1); m; m &= m - 1) ShapeCombine<SH>(v, xs[__ffs(m) - 1]);
-                }
-                __syncwarp(peers);
-                if (lane != leader) continue;
-            }
-            const bool special = P.key_full64 && key == kEmptyKey;
-            const int slot = special ? -1 : sm.Find(key);
-            if (slot >= 0) {
-                ShapeAtomics<SH>(sm.st + slot, sm.S, v);
-                continue;
-            }
-            int64_t gslot;
-            if (special) {
-                gslot = L.T.capacity;
-                unsigned long long* flag = reinterpret_cast<unsigned long long*>(
-                    L.T.slots + L.T.capacity * L.T.slot_words + L.T.key_off);
-                if (*reinterpret_cast<volatile unsigned long long*>(flag) == 0 && atomicExch(flag, 1ull) == 0) {
-                    atomicAdd(sm.fresh, 1u);
-                }
-            } else {
-                int is_new = 0;
-                gslot = GlobalFind1(L.T, L.cap_mask, key, is_new);
-                if (is_new) atomicAdd(sm.fresh, 1u);
-            }
-            if (gslot < 0) {
-                // Replayed row by row after the table grows: every row of the group.
-                for (unsigned m = peers; m; m &= m - 1) Defer(L, row0 + rb + (tid & ~31) + (__ffs(m) - 1), 0);
-                continue;
-            }
-            ShapeAtomics<SH>(L.T.slots + gslot * L.T.slot_words + L.T.state_off, 1, v);
-        }
-        __syncthreads();
-        if (tid == 0) {
-            const int64_t nt = t + int64_t(L.stages) * gridDim.x;
-            if (nt < ntiles && tile_full(nt)) issue(nt, s);
-        }
-    }
+// High-cardinality scan aggregate specialised by query shape.  The launch's
+// rows are cut into one contiguous range per CTA; the shared tier holds the
+// first keys a CTA meets (the hot keys of a skewed stream settle there) and
+// goes to the global table once, at the end.
+template <class SH>
+__global__ void __launch_bounds__(kHighThreads, 1) AggHighKernel(const __grid_constant__ AggLaunch L) {
+    const HighLayout hl = HighLayoutOf(L.smem_slots, L.P.state_words, SH::n, blockDim.x);
+    const HighSmem sm = HighSmemOf(L, hl);
+    ShapeVals<SH>* xs = reinterpret_cast<ShapeVals<SH>*>(DynSmem() + hl.off_scratch) + (threadIdx.x & ~31);
+    HighInit(L, sm);
     __syncthreads();
-    if (aborted || *reinterpret_cast<volatile unsigned*>(&misc[4])) {
-        if (tid == 0) {
-            const long long start = clock64();
-            while (clock64() - start < 2000000) {
-            }
-        }
-        __syncthreads();
-        return;
-    }
-
-    // Shared table -> global table.
-    for (int i = tid; i < sm.S; i += bd) {
-        const uint64_t key = sm.keys[i];
-        if (key == kEmptyKey) continue;
-        int is_new = 0;
-        const int64_t g = GlobalFind1(L.T, L.cap_mask, key, is_new);
-        if (is_new) atomicAdd(sm.fresh, 1u);
-        if (g < 0) {
-            const unsigned long long e = atomicAdd(&L.counters->spilled, 1ull);
-            if (int64_t(e) >= L.spill_cap) {
-                SetError(&L.counters->error, DE_SPILL_FULL);
-                continue;
-            }
-            uint64_t* rec = L.spill + int64_t(e) * (1 + P.state_words);
-            rec[0] = key;
-            for (int w = 0; w < P.state_words; ++w) rec[1 + w] = sm.st[int64_t(w) * sm.S + i];
-            continue;
-        }
-        uint64_t* gbase = L.T.slots + g * L.T.slot_words + L.T.state_off;
-        for (int st2 = 0; st2 < P.nstates; ++st2) {
-            const StateDesc sd = P.states[st2];
-            const uint64_t lo = sm.st[int64_t(sd.word) * sm.S + i];
-            const uint64_t hi = sd.kind == ST_SUM_I128 ? sm.st[int64_t(sd.word + 1) * sm.S + i] : 0;
-            if (IsIdentity(sd.kind, lo, hi)) continue;
-            double f;
-            __builtin_memcpy(&f, &lo, 8);
-            ApplyState(gbase + sd.word, gbase + sd.word + 1, sd.kind, lo, hi, f);
-        }
-    }
+    const int64_t per = (L.nrows + gridDim.x - 1) / gridDim.x;
+    const int64_t row0 = int64_t(blockIdx.x) * per;
+    const int n = int(max(int64_t(0), min(per, L.nrows - row0)));
+    const char* cb[kFastCols];
+    HighColumns<SH>(L, row0, cb);
+    const uint8_t* sel = L.P.selection ? L.P.selection + row0 : nullptr;
+    HighRows<SH>(L, sm, xs, cb, sel, n, row0, threadIdx.x >> 5, blockDim.x >> 5);
     __syncthreads();
-    if (tid == 0 && sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
+    HighFlush(L, sm, false);
+    __syncthreads();
+    if (threadIdx.x == 0 && sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
 }
 
 // The instantiated query shapes.  QDB_C(w, u): a fast column of w bytes
@@ -2290,26 +2387,23 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
     }
     if (a.fast && variant == 0 && any) {
         if (SigKernelFn fn = FindHighKernel(L.P, *a.fast)) {
-            // Room after the shared table for each thread's combine scratch.
-            const size_t scratch = size_t(kAggThreads) * 16 * a.fast->nstates;
-            int S2 = S;
-            size_t bytes = layout(T, stages, S2) + scratch;
-            while (bytes > budget && S2 > 256) {
-                S2 >>= 1;
-                bytes = layout(T, stages, S2) + scratch;
-            }
-            if (bytes <= budget) {
+            // The largest shared tier (up to the state's slot budget) that
+            // fits beside each thread's combine scratch.
+            int S2 = std::max(256, a.smem_slots);
+            while (S2 > 256 && size_t(HighLayoutOf(S2, sw, a.fast->nstates, kHighThreads).bytes) > budget) S2 >>= 1;
+            const HighLayout hl = HighLayoutOf(S2, sw, a.fast->nstates, kHighThreads);
+            if (size_t(hl.bytes) <= budget) {
                 L.smem_slots = S2;
                 L.smem_limit = S2 / 2;
                 L.F = *a.fast;
-                SetSmem(fn, bytes);
+                const int hgrid = int(std::max<int64_t>(1, std::min<int64_t>((a.nrows + 4095) / 4096, g_sms)));
+                SetSmem(fn, size_t(hl.bytes));
                 ProfileBegin(s, "agg_update_high", a.nrows);
-                fn<<<grid, kAggThreads, bytes, s>>>(L);
+                fn<<<hgrid, kHighThreads, size_t(hl.bytes), s>>>(L);
                 ProfileEnd(s);
                 CountLaunch();
                 return;
             }
-            layout(T, stages, S);
         }
     }
     const char* name = a.join ? "join_agg_probe" : "agg_update";
