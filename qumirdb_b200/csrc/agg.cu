@@ -1010,7 +1010,7 @@ __device__ __forceinline__ void Add128(uint64_t& lo, uint64_t& hi, uint64_t l, u
 
 // Fast column K of tile row r (cb: the tile's column bases).
 template <class SH, int K>
-__device__ __forceinline__ int64_t ColVal(const char* const (&cb)[kFastCols], int r) {
+__device__ __forceinline__ int64_t ColVal(const char* const* cb, int r) {
     constexpr int w = SH::cw(K);
     constexpr bool u = SH::cu(K);
     const char* p = cb[K] + int64_t(r) * w;
@@ -1020,11 +1020,27 @@ __device__ __forceinline__ int64_t ColVal(const char* const (&cb)[kFastCols], in
     else return *reinterpret_cast<const int64_t*>(p);
 }
 
-template <class SH, int S, int J>
-__device__ __forceinline__ int64_t ShapeFactor(const FastPlan& F, const char* const (&cb)[kFastCols], int r) {
+// Row accessors of the shape helpers: a row of a staged tile (or of the
+// launch's global columns) read in place, or a row already in registers.
+struct TileRow {
+    const char* const* cb;
+    int r;
+    template <class SH, int K>
+    __device__ __forceinline__ int64_t col() const { return ColVal<SH, K>(cb, r); }
+};
+
+template <int N>
+struct RegRow {
+    int64_t v[N > 0 ? N : 1];
+    template <class SH, int K>
+    __device__ __forceinline__ int64_t col() const { return v[K]; }
+};
+
+template <class SH, int S, int J, class A>
+__device__ __forceinline__ int64_t ShapeFactor(const FastPlan& F, const A& row) {
     constexpr int FM = SH::form(S, J);
     const FastFactor& f = F.states[S].f[J];
-    const int64_t x = ColVal<SH, SH::fcol(S, J)>(cb, r);
+    const int64_t x = row.template col<SH, SH::fcol(S, J)>();
     if constexpr (FM == FF_X) return x;
     else if constexpr (FM == FF_ADD) return int64_t(uint64_t(f.c) + uint64_t(x));
     else if constexpr (FM == FF_SUB) return int64_t(uint64_t(f.c) - uint64_t(x));
@@ -1036,19 +1052,18 @@ __device__ __forceinline__ bool Fits32(int64_t v) { return v == int64_t(int32_t(
 // Product of a state's factors: wrapping 64-bit (a, b, c), or exact 128-bit
 // when WIDE.  Factors that fit in 32 bits multiply as 32 x 32 -> 64; others
 // take the full 64 / 128-bit path (same result).
-template <class SH, int S, bool WIDE>
-__device__ __forceinline__ void ShapeProduct(const FastPlan& F, const char* const (&cb)[kFastCols], int r,
-                                             uint64_t& lo, uint64_t& hi) {
+template <class SH, int S, bool WIDE, class A>
+__device__ __forceinline__ void ShapeProduct(const FastPlan& F, const A& row, uint64_t& lo, uint64_t& hi) {
     constexpr int NF = SH::nf(S);
-    const int64_t a = ShapeFactor<SH, S, 0>(F, cb, r);
+    const int64_t a = ShapeFactor<SH, S, 0>(F, row);
     if constexpr (NF == 1) {
         lo = uint64_t(a);
         hi = a < 0 ? ~0ull : 0ull;
         return;
     } else {
-        const int64_t b = ShapeFactor<SH, S, 1>(F, cb, r);
+        const int64_t b = ShapeFactor<SH, S, 1>(F, row);
         int64_t c = 1;
-        if constexpr (NF > 2) c = ShapeFactor<SH, S, 2>(F, cb, r);
+        if constexpr (NF > 2) c = ShapeFactor<SH, S, 2>(F, row);
         if (Fits32(a) && Fits32(b) && Fits32(c)) {
             const int64_t ab = int64_t(int32_t(a)) * int32_t(b);
             if (NF == 2 || Fits32(ab)) {
@@ -1072,15 +1087,14 @@ __device__ __forceinline__ void ShapeProduct(const FastPlan& F, const char* cons
 
 // Folds one row into its group's lane-private accumulators: p points at
 // word 0 of the group for this lane; word w lives at p[w * stride].
-template <class SH, int S = 0>
-__device__ __forceinline__ void ShapeFoldP(uint64_t* p, int stride, const FastPlan& F,
-                                           const char* const (&cb)[kFastCols], int r) {
+template <class SH, int S = 0, class A>
+__device__ __forceinline__ void ShapeFoldP(uint64_t* p, int stride, const FastPlan& F, const A& row) {
     if constexpr (S < SH::n) {
         constexpr int K = SH::kind(S);
         constexpr int NF = SH::nf(S);
         constexpr int O = SH::off(S);
         uint64_t lo = 1, hi = 0;
-        if constexpr (K != SK_COUNT) ShapeProduct<SH, S, K == SK_SUM128>(F, cb, r, lo, hi);
+        if constexpr (K != SK_COUNT) ShapeProduct<SH, S, K == SK_SUM128>(F, row, lo, hi);
         (void)NF;
         if constexpr (SH::width(S) == 2) {
             uint64_t a = p[O * stride];
@@ -1091,19 +1105,18 @@ __device__ __forceinline__ void ShapeFoldP(uint64_t* p, int stride, const FastPl
         } else {
             p[O * stride] += lo;
         }
-        ShapeFoldP<SH, S + 1>(p, stride, F, cb, r);
+        ShapeFoldP<SH, S + 1>(p, stride, F, row);
     }
 }
 
 // Clauses held by the row's filter atoms (AND of OR clauses).
-template <class SH, int J = 0>
-__device__ __forceinline__ uint32_t ShapeHeld(const AggPlan& P, const FastPlan& F, const char* const (&cb)[kFastCols],
-                                              int r) {
+template <class SH, int J = 0, class A>
+__device__ __forceinline__ uint32_t ShapeHeld(const AggPlan& P, const FastPlan& F, const A& row) {
     if constexpr (J < SH::Atoms::n) {
         constexpr int op = SH::Atoms::at(J) >> 3;
         constexpr int col = SH::Atoms::at(J) & 7;
         const FastAtom& t = F.atoms[J];
-        const int64_t v = ColVal<SH, col>(cb, r);
+        const int64_t v = row.template col<SH, col>();
         bool ok;
         if constexpr (op == AT_BETWEEN) {
             ok = v >= t.c0 && v <= t.c1;
@@ -1123,23 +1136,23 @@ __device__ __forceinline__ uint32_t ShapeHeld(const AggPlan& P, const FastPlan& 
         } else {
             ok = v >= t.c0;
         }
-        return (ok ? (1u << t.clause) : 0u) | ShapeHeld<SH, J + 1>(P, F, cb, r);
+        return (ok ? (1u << t.clause) : 0u) | ShapeHeld<SH, J + 1>(P, F, row);
     } else {
         return 0u;
     }
 }
 
-template <class SH, int J = 0>
-__device__ __forceinline__ uint64_t ShapeKey(const char* const (&cb)[kFastCols], int r) {
+template <class SH, int J = 0, class A>
+__device__ __forceinline__ uint64_t ShapeKey(const A& row) {
     if constexpr (J < SH::Keys::n) {
         constexpr int code = SH::Keys::at(J);
         constexpr int col = code & 7;
         constexpr int bits = (code >> 3) & 127;
         constexpr int shift = code >> 10;
-        uint64_t v = uint64_t(ColVal<SH, col>(cb, r));
+        uint64_t v = uint64_t(row.template col<SH, col>());
         // A zero-extended column narrower than its key field needs no mask.
         if constexpr (bits < 64 && !(SH::cu(col) && SH::cw(col) * 8 <= bits)) v &= (1ull << bits) - 1;
-        return (v << shift) | ShapeKey<SH, J + 1>(cb, r);
+        return (v << shift) | ShapeKey<SH, J + 1>(row);
     } else {
         return 0ull;
     }
@@ -1282,8 +1295,8 @@ __global__ void __launch_bounds__(kSigThreads, 1) AggSigKernel(const __grid_cons
 #pragma unroll 2
         for (int r = tid; r < nrows; r += bd) {
             if (sel && !sel[r]) continue;
-            if (SIG::Atoms::n && ShapeHeld<SIG>(P, F, cb, r) != F.clause_mask) continue;
-            const uint64_t key = ShapeKey<SIG>(cb, r);
+            if (SIG::Atoms::n && ShapeHeld<SIG>(P, F, TileRow{cb, r}) != F.clause_mask) continue;
+            const uint64_t key = ShapeKey<SIG>(TileRow{cb, r});
             int g = -1;
 #pragma unroll
             for (int j = 0; j < kPrivGroups; ++j) g = ckey[j] == key ? cgid[j] : g;
@@ -1312,7 +1325,7 @@ __global__ void __launch_bounds__(kSigThreads, 1) AggSigKernel(const __grid_cons
                     continue;
                 }
             }
-            ShapeFoldP<SIG>(pacc + int64_t(g) * SIG::words * bd + tid, bd, F, cb, r);
+            ShapeFoldP<SIG>(pacc + int64_t(g) * SIG::words * bd + tid, bd, F, TileRow{cb, r});
         }
         // Every warp is done with the stage: refill it.
         __syncthreads();
@@ -1395,54 +1408,32 @@ __global__ void __launch_bounds__(kSigThreads, 1) AggSigKernel(const __grid_cons
 // rest, and each state's update a typed atomic chosen at compile time.
 // ---------------------------------------------------------------------------
 // One row's contribution to every state (COUNT 1, sums, min/max values,
-// double bits), combined over the rows of one key within a warp.
+// double bits).
 template <class SH>
 struct ShapeVals {
     uint64_t lo[SH::n];
     uint64_t hi[SH::n];
 };
 
-template <class SH, int S = 0>
-__device__ __forceinline__ void ShapeRowVals(ShapeVals<SH>& v, const FastPlan& F, const char* const (&cb)[kFastCols],
-                                             int r) {
+template <class SH, int S = 0, class A>
+__device__ __forceinline__ void ShapeRowVals(ShapeVals<SH>& v, const FastPlan& F, const A& row) {
     if constexpr (S < SH::n) {
         constexpr int K = SH::kind(S);
         v.hi[S] = 0;
         if constexpr (K == SK_COUNT) {
             v.lo[S] = 1;
         } else if constexpr (K == SK_SUMF64) {
-            v.lo[S] = uint64_t(ColVal<SH, SH::fcol(S, 0)>(cb, r));
+            v.lo[S] = uint64_t(row.template col<SH, SH::fcol(S, 0)>());
         } else if constexpr (K == SK_MIN64 || K == SK_MAX64) {
-            v.lo[S] = uint64_t(ShapeFactor<SH, S, 0>(F, cb, r));
+            v.lo[S] = uint64_t(ShapeFactor<SH, S, 0>(F, row));
         } else {
-            ShapeProduct<SH, S, K == SK_SUM128>(F, cb, r, v.lo[S], v.hi[S]);
+            ShapeProduct<SH, S, K == SK_SUM128>(F, row, v.lo[S], v.hi[S]);
         }
-        ShapeRowVals<SH, S + 1>(v, F, cb, r);
+        ShapeRowVals<SH, S + 1>(v, F, row);
     }
 }
 
-// a <- a (+) b state by state.
-template <class SH, int S = 0>
-__device__ __forceinline__ void ShapeCombine(ShapeVals<SH>& a, const ShapeVals<SH>& b) {
-    if constexpr (S < SH::n) {
-        constexpr int K = SH::kind(S);
-        if constexpr (K == SK_SUMF64) {
-            a.lo[S] = uint64_t(__double_as_longlong(__longlong_as_double((long long)a.lo[S]) +
-                                                    __longlong_as_double((long long)b.lo[S])));
-        } else if constexpr (K == SK_MIN64) {
-            if (int64_t(b.lo[S]) < int64_t(a.lo[S])) a.lo[S] = b.lo[S];
-        } else if constexpr (K == SK_MAX64) {
-            if (int64_t(b.lo[S]) > int64_t(a.lo[S])) a.lo[S] = b.lo[S];
-        } else if constexpr (SH::width(S) == 2) {
-            Add128(a.lo[S], a.hi[S], b.lo[S], b.hi[S]);
-        } else {
-            a.lo[S] += b.lo[S];
-        }
-        ShapeCombine<SH, S + 1>(a, b);
-    }
-}
-
-// Folds combined values into state words w[O * stride] with atomics.
+// Folds one row's values into state words w[O * stride] with atomics.
 template <class SH, int S = 0>
 __device__ __forceinline__ void ShapeAtomics(uint64_t* w, int64_t stride, const ShapeVals<SH>& v) {
     if constexpr (S < SH::n) {
@@ -1480,7 +1471,7 @@ __device__ __forceinline__ void SmemAdd64(uint64_t* p, uint64_t v) {
     if (up) atomicAdd(q + 1, up);
 }
 
-// Folds combined values into the shared tier's state words w[O * stride].
+// Folds one row's values into the shared tier's state words w[O * stride].
 // MIN/MAX read the word first: once a hot group's extreme has settled, most
 // rows change nothing and need no atomic.
 template <class SH, int S = 0>
@@ -1568,85 +1559,89 @@ __device__ __forceinline__ int64_t GlobalFindH(const GTableDev& T, uint64_t mask
     return -1;
 }
 
-// Shared tier layout inside dynamic shared memory: misc words, keys, state
-// words, then each warp's combine scratch.
+// Shared tier layout inside dynamic shared memory: misc words, keys, then
+// the state words.
 struct HighLayout {
     int off_keys;
     int off_st;
-    int off_scratch;
     int bytes;
 };
 
-__host__ __device__ inline HighLayout HighLayoutOf(int S, int state_words, int nstates, int threads) {
+__host__ __device__ inline HighLayout HighLayoutOf(int S, int state_words) {
     HighLayout h;
     h.off_keys = 128;
     h.off_st = h.off_keys + S * 8;
-    h.off_scratch = h.off_st + S * state_words * 8;
-    h.bytes = h.off_scratch + threads * 16 * nstates;
+    h.bytes = h.off_st + S * state_words * 8;
     return h;
 }
 
-// One range of rows through the tiers: each warp takes 32 consecutive rows
-// at a time (coalesced loads straight from HBM, no staging and no block
-// barrier), folds the rows of one key into their lowest lane, then the
-// leader updates the shared tier or, when its key is not there, the global
-// table.  `defer_base` numbers the range's rows for the replay list.
+// Loads the shape's columns of row r into registers (zeros past the end).
+template <class SH, int K = 0>
+__device__ __forceinline__ void LoadRow(RegRow<SH::Cols::n>& row, const char* const* cb, int r, bool in) {
+    if constexpr (K < SH::Cols::n) {
+        row.v[K] = in ? ColVal<SH, K>(cb, r) : 0;
+        LoadRow<SH, K + 1>(row, cb, r, in);
+    }
+}
+
+// One range of rows through the tiers.  Each warp takes 32 consecutive rows
+// at a time, coalesced straight from HBM with the next 32 already loading
+// while these are folded; each lane then goes its own way (the shared tier
+// when its key is there, else the global table) and the warp reconverges
+// before the next rows.
+// `defer_base` numbers the range's rows for the replay list.
 template <class SH>
-__device__ __forceinline__ void HighRows(const AggLaunch& L, const HighSmem& sm, ShapeVals<SH>* xs,
-                                         const char* const (&cb)[kFastCols], const uint8_t* sel, int nrows,
-                                         int64_t defer_base, int wid, int nw) {
+__device__ __forceinline__ void HighRows(const AggLaunch& L, const HighSmem& sm, const char* const* cb,
+                                         const uint8_t* sel, int nrows, int64_t defer_base, int wid, int nw) {
     const AggPlan& P = L.P;
     const FastPlan& F = L.F;
-    const int lane = threadIdx.x & 31;
+    const int lane = int(threadIdx.x & 31);
+    const int step = nw * 32;
+    int r = wid * 32 + lane;
+    RegRow<SH::Cols::n> cur;
+    LoadRow<SH>(cur, cb, r, r < nrows);
+    bool cur_sel = r < nrows && (!sel || sel[r]);
 #pragma unroll 1
-    for (int base = wid * 32; base < nrows; base += nw * 32) {
-        const int r = base + lane;
-        bool ok = r < nrows && (!sel || sel[r]);
-        if (ok && SH::Atoms::n) ok = ShapeHeld<SH>(P, F, cb, r) == F.clause_mask;
-        const unsigned act = __ballot_sync(kFull, ok);
-        if (!ok) continue;
-        const uint64_t key = ShapeKey<SH>(cb, r);
-        ShapeVals<SH> v;
-        ShapeRowVals<SH>(v, F, cb, r);
-        const unsigned peers = __match_any_sync(act, key);
-        if (peers != (1u << lane)) {
-            const int leader = __ffs(peers) - 1;
-            xs[lane] = v;
-            __syncwarp(peers);
-            if (lane == leader) {
-                for (unsigned m = peers & (peers - 1); m; m &= m - 1) ShapeCombine<SH>(v, xs[__ffs(m) - 1]);
-            }
-            __syncwarp(peers);
-            if (lane != leader) continue;
-        }
-        const uint64_t h = Fmix64(key);
-        const bool special = P.key_full64 && key == kEmptyKey;
-        if (!special) {
-            const int slot = sm.Find(h, key);
+    for (; r - lane < nrows; r += step) {
+        const int rn = r + step;
+        RegRow<SH::Cols::n> nxt;
+        LoadRow<SH>(nxt, cb, rn, rn < nrows);
+        const bool nxt_sel = rn < nrows && (!sel || sel[rn]);
+        bool ok = cur_sel;
+        if (ok && SH::Atoms::n) ok = ShapeHeld<SH>(P, F, cur) == F.clause_mask;
+        if (ok) {
+            const uint64_t key = ShapeKey<SH>(cur);
+            ShapeVals<SH> v;
+            ShapeRowVals<SH>(v, F, cur);
+            const uint64_t h = Fmix64(key);
+            const bool special = P.key_full64 && key == kEmptyKey;
+            const int slot = special ? -1 : sm.Find(h, key);
             if (slot >= 0) {
                 ShapeSmemAtomics<SH>(sm.st + slot, sm.S, v);
-                continue;
+            } else {
+                int64_t gslot;
+                if (special) {
+                    gslot = L.T.capacity;
+                    unsigned long long* flag = reinterpret_cast<unsigned long long*>(
+                        L.T.slots + L.T.capacity * L.T.slot_words + L.T.key_off);
+                    if (*reinterpret_cast<volatile unsigned long long*>(flag) == 0 && atomicExch(flag, 1ull) == 0) {
+                        atomicAdd(sm.fresh, 1u);
+                    }
+                } else {
+                    int is_new = 0;
+                    gslot = GlobalFindH(L.T, L.cap_mask, h, key, is_new);
+                    if (is_new) atomicAdd(sm.fresh, 1u);
+                }
+                if (gslot < 0) {
+                    Defer(L, defer_base + r, 0);    // replayed after the table grows
+                } else {
+                    ShapeAtomics<SH>(L.T.slots + gslot * L.T.slot_words + L.T.state_off, 1, v);
+                }
             }
         }
-        int64_t gslot;
-        if (special) {
-            gslot = L.T.capacity;
-            unsigned long long* flag =
-                reinterpret_cast<unsigned long long*>(L.T.slots + L.T.capacity * L.T.slot_words + L.T.key_off);
-            if (*reinterpret_cast<volatile unsigned long long*>(flag) == 0 && atomicExch(flag, 1ull) == 0) {
-                atomicAdd(sm.fresh, 1u);
-            }
-        } else {
-            int is_new = 0;
-            gslot = GlobalFindH(L.T, L.cap_mask, h, key, is_new);
-            if (is_new) atomicAdd(sm.fresh, 1u);
-        }
-        if (gslot < 0) {
-            // Replayed row by row after the table grows: every row of the group.
-            for (unsigned m = peers; m; m &= m - 1) Defer(L, defer_base + base + (__ffs(m) - 1), 0);
-            continue;
-        }
-        ShapeAtomics<SH>(L.T.slots + gslot * L.T.slot_words + L.T.state_off, 1, v);
+        cur = nxt;
+        cur_sel = nxt_sel;
+        __syncwarp();   // the lanes' paths meet again before the next 32 rows
     }
 }
 
@@ -1735,9 +1730,8 @@ __device__ __forceinline__ void HighColumns(const AggLaunch& L, int64_t row0, co
 // goes to the global table once, at the end.
 template <class SH>
 __global__ void __launch_bounds__(kHighThreads, 1) AggHighKernel(const __grid_constant__ AggLaunch L) {
-    const HighLayout hl = HighLayoutOf(L.smem_slots, L.P.state_words, SH::n, blockDim.x);
+    const HighLayout hl = HighLayoutOf(L.smem_slots, L.P.state_words);
     const HighSmem sm = HighSmemOf(L, hl);
-    ShapeVals<SH>* xs = reinterpret_cast<ShapeVals<SH>*>(DynSmem() + hl.off_scratch) + (threadIdx.x & ~31);
     HighInit(L, sm);
     __syncthreads();
     const int64_t per = (L.nrows + gridDim.x - 1) / gridDim.x;
@@ -1746,7 +1740,7 @@ __global__ void __launch_bounds__(kHighThreads, 1) AggHighKernel(const __grid_co
     const char* cb[kFastCols];
     HighColumns<SH>(L, row0, cb);
     const uint8_t* sel = L.P.selection ? L.P.selection + row0 : nullptr;
-    HighRows<SH>(L, sm, xs, cb, sel, n, row0, threadIdx.x >> 5, blockDim.x >> 5);
+    HighRows<SH>(L, sm, cb, sel, n, row0, threadIdx.x >> 5, blockDim.x >> 5);
     __syncthreads();
     HighFlush(L, sm, false);
     __syncthreads();
@@ -2387,11 +2381,10 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
     }
     if (a.fast && variant == 0 && any) {
         if (SigKernelFn fn = FindHighKernel(L.P, *a.fast)) {
-            // The largest shared tier (up to the state's slot budget) that
-            // fits beside each thread's combine scratch.
+            // The largest shared tier (up to the state's slot budget) that fits.
             int S2 = std::max(256, a.smem_slots);
-            while (S2 > 256 && size_t(HighLayoutOf(S2, sw, a.fast->nstates, kHighThreads).bytes) > budget) S2 >>= 1;
-            const HighLayout hl = HighLayoutOf(S2, sw, a.fast->nstates, kHighThreads);
+            while (S2 > 256 && size_t(HighLayoutOf(S2, sw).bytes) > budget) S2 >>= 1;
+            const HighLayout hl = HighLayoutOf(S2, sw);
             if (size_t(hl.bytes) <= budget) {
                 L.smem_slots = S2;
                 L.smem_limit = S2 / 2;
