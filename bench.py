@@ -41,6 +41,7 @@ PROBE_ROWS = 120_000_000
 FK_DOMAIN = 2_500_000
 LINEITEM_ROWS = 6_001_215
 ZIPF_ROWS = 200_000_000
+ZIPF_PARTS = 4096
 ZIPF_DISTINCT = 20_000_000
 SORT_ROWS = 300_000_000
 METRIC = "rows/s & HBM GB/s vs peak per operator; mixed-stream queries/s and p50/p99"
@@ -273,6 +274,50 @@ def zipf_operator(q, peak):
             "l2": "inputs larger than L2", "gpu_launches": launches / 3}
 
 
+def zipf_partition_sizes(parts: int = ZIPF_PARTS) -> np.ndarray:
+    """Log-uniform partition sizes in [1e3, 1e6] rows (seeded)."""
+    rng = np.random.default_rng(5)
+    return np.exp(rng.uniform(np.log(1e3), np.log(1e6), parts)).astype(np.int64)
+
+
+def zipf_batched_operator(q, peak):
+    """The high-cardinality GROUP BY run as 4096 independent partitions of
+    log-uniform size, each its own aggregate, all in one persistent launch
+    per step (plus the batched finalize).  The partitions are consecutive
+    slices of one Zipf(1.1 over 20M) stream, resident in HBM."""
+    from qumirdb_b200 import abi, queries
+    sizes = zipf_partition_sizes()
+    n = int(sizes.sum())
+    cols = [np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.float64)]
+    q.lib().qdb_gen_zipf(6, n, ZIPF_DISTINCT, 1.1, *[c.ctypes.data for c in cols])
+    prog = q.compile_aggregate(queries.zipf_agg(flags=abi.OUT_DEVICE))
+    drs = q.DeviceRowSet(cols)
+    del cols
+    bounds = np.concatenate([[0], np.cumsum(sizes)])
+    parts = [q.SliceRowSet(drs, int(lo), int(hi)) for lo, hi in zip(bounds[:-1], bounds[1:])]
+    groups = []
+
+    def step():
+        b = q.AggregateBatch(prog, len(parts))
+        b.add(parts)
+        groups.append(sum(b.groups))
+        for o in b.finish():
+            q.release(o)
+
+    ms, _, launches, _ = timed(q, step, 3, 3)
+    _, _, _, kernels = timed(q, step, 2, 0, profile=True)
+    kms, _ = kernel_avg(kernels, "agg_batch_update", 2)
+    fms, _ = kernel_avg(kernels, "agg_finalize_batch", 2)
+    alg = n * 24
+    return {"workload": f"GROUP BY key (Zipf 1.1 over 20M) as {len(sizes)} independent partitions of "
+                        f"log-uniform 1K-1M rows ({n} rows), COUNT/SUM/MIN/MAX/SUM(f64), one persistent launch",
+            "rows_per_s": n / (ms / 1e3), "ms_per_query": ms, "groups": groups[-1], "kernel": "agg_batch_update",
+            "kernel_ms": kms, "finalize_ms": fms, "algorithmic_bytes": alg,
+            "kernel_gbs": alg / (kms / 1e3) / 1e9 if kms else None,
+            "frac_of_measured_hbm": (alg / (kms / 1e3) / 1e9) / peak if kms else None,
+            "l2": "inputs larger than L2", "gpu_launches": launches / 3, "autotune": q.autotune_info()}
+
+
 def sort_pass_plan_bytes(n: int) -> tuple[int, int]:
     """Algorithmic bytes of the device sort of (k1 i64 DESC, k2 i32 ASC) over
     n row ids, by the plan it runs: extraction (row id 8 + k1 8 + k2 4 read,
@@ -442,6 +487,23 @@ def profile_case(name: str, rows: int) -> None:
             a = q.Aggregate(prog)
             a.add(drs)
             q.release(a.finish())
+    elif name == "zipf_batched":
+        from qumirdb_b200 import abi
+        sizes = zipf_partition_sizes()
+        if rows:
+            sizes = np.maximum(1, sizes * rows // int(sizes.sum()))
+        n = int(sizes.sum())
+        cols = [np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.float64)]
+        q.lib().qdb_gen_zipf(6, n, ZIPF_DISTINCT, 1.1, *[c.ctypes.data for c in cols])
+        prog = q.compile_aggregate(queries.zipf_agg(flags=abi.OUT_DEVICE))
+        drs = q.DeviceRowSet(cols)
+        bounds = np.concatenate([[0], np.cumsum(sizes)])
+        parts = [q.SliceRowSet(drs, int(lo), int(hi)) for lo, hi in zip(bounds[:-1], bounds[1:])]
+        for _ in range(2):
+            b = q.AggregateBatch(prog, len(parts))
+            b.add(parts)
+            for o in b.finish():
+                q.release(o)
     elif name == "sort":
         n = rows or SORT_ROWS
         k1 = np.empty(n, np.int64)
@@ -465,7 +527,7 @@ def main() -> None:
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--no-operators", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-case", choices=["join", "sort", "lineitem", "zipf"],
+    ap.add_argument("--profile-case", choices=["join", "sort", "lineitem", "zipf", "zipf_batched"],
                     help="run one workload twice at --rows rows (for profiler captures) and exit")
     ap.add_argument("--rows", type=int, default=0)
     args = ap.parse_args()
@@ -548,7 +610,7 @@ def main() -> None:
     if rank == 0 and world == 1 and not args.no_operators:
         try:
             line["operators"] = {"lineitem": lineitem_operator(q, peak), "zipf": zipf_operator(q, peak),
-                                 "sort": sort_operator(q, peak)}
+                                 "zipf_batched": zipf_batched_operator(q, peak), "sort": sort_operator(q, peak)}
             if not args.no_cpu_baseline:
                 line["operators"]["sort"]["cpu_baseline"] = {
                     k: v for k, v in cpu_baseline_sort(20_000_000).items() if k != "seconds"}

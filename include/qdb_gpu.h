@@ -396,6 +396,37 @@ int64_t qdb_gpu_top_k_select(const qdb_gpu_program* program, qdb_rowset* store,
                              int64_t* row_ids, int64_t size, int64_t limit);
 
 /* ------------------------------------------------------------------------ */
+/* Batched aggregation: many aggregate states of one program per launch.    */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces a loop of agg_dispatch(ht, batch, 0, Update) over independent    */
+/* aggregate tasks of one program (the partitions of a partitioned GROUP BY, */
+/* qdb/exec/aggregate_exec.cpp:104-117 per task; or small aggregations of    */
+/* many queries of one template): states[i] is updated with batches[i] as    */
+/* one call of qdb_gpu_agg_dispatch would, all in one persistent launch.  A  */
+/* zeroed state buffer is initialised first (as Init with no hint), its table */
+/* taken from a device arena shared by the batch.  Block shape and work item */
+/* size come from an autotuner (set QDB_AUTOTUNE=0 to keep the defaults); the */
+/* launch sequence is replayed as a CUDA graph while the batch keeps its     */
+/* structure.  States whose program shape has no batched kernel are updated  */
+/* one by one.  Returns n, or < 0 on failure.                                */
+int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* program, void* const* states,
+                                   qdb_rowset* const* batches, int64_t n);
+
+/* agg_finish_rowset (qdb/kernel/compiler.h:232-242) for n states in one      */
+/* batched finalize: outs[i] receives state i's groups and the states are     */
+/* destroyed and zeroed.  The outputs are slices of shared buffers, freed     */
+/* when the last of them is destroyed.  Returns the total group count.       */
+int64_t qdb_gpu_agg_finish_batch(const qdb_gpu_program* program, void* const* states, int64_t n,
+                                 qdb_rowset* outs);
+
+/* The autotuner's state as JSON (searches, timed trials, reuses, graph      */
+/* replays, chosen configurations); returns the JSON length.  No reference   */
+/* counterpart.                                                              */
+int64_t qdb_gpu_autotune_info(char* buf, int64_t cap);
+void qdb_gpu_autotune_reset(void);
+
+/* ------------------------------------------------------------------------ */
 /* Aggregation without device allocation.                                   */
 /* ------------------------------------------------------------------------ */
 

@@ -203,6 +203,7 @@ class DeviceRowSet:
     def __init__(self, columns, masks=None, selection=None, rows=None):
         host = HostRowSet(columns, masks, selection, rows)
         self.rows = host.rs.RowCount
+        self.widths = [a.dtype.itemsize for a in host.arrays]
         self.bufs = []
         self.cols = (abi.Column * max(1, len(host.arrays)))()
         for k, a in enumerate(host.arrays):
@@ -229,14 +230,56 @@ class DeviceRowSet:
         return C.byref(self.rs)
 
 
-def read_rowset(rs: abi.RowSet, types) -> tuple[list[np.ndarray], list[np.ndarray]]:
-    """Host output row set -> (values, validity) numpy columns by qdb type."""
+class SliceRowSet:
+    """Rows [lo, hi) of a DeviceRowSet as a row set of its own, without a
+    copy: the column pointers move by lo values, validity by lo bits."""
+
+    def __init__(self, base: "DeviceRowSet", lo: int, hi: int):
+        self.base = base
+        src = base.rs
+        n = src.ColumnCount
+        self.cols = (abi.Column * max(1, n))()
+        for k in range(n):
+            c = src.Columns[k]
+            d = self.cols[k]
+            d.Data = (c.Data or 0) + lo * base.widths[k]
+            if c.Mask:
+                d.Mask = c.Mask
+                d.MaskBitOffset = c.MaskBitOffset + lo
+        self.rs = abi.RowSet()
+        self.rs.Columns = self.cols
+        self.rs.ColumnCount = n
+        self.rs.RowCount = hi - lo
+        if src.Selection:
+            self.rs.Selection = src.Selection + lo
+        self.rs.RefCount = 1
+
+    @property
+    def ptr(self):
+        return C.byref(self.rs)
+
+
+def _fetch(ptr, nbytes: int, on_device: bool) -> np.ndarray:
+    if nbytes <= 0:
+        return np.zeros(0, np.uint8)
+    if on_device:
+        out = np.empty(nbytes, np.uint8)
+        if lib().qdb_gpu_memcpy(out.ctypes.data, ptr, nbytes) != 0:
+            raise QdbError(last_error())
+        synchronize()
+        return out
+    return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint8)), shape=(nbytes,)).copy()
+
+
+def read_rowset(rs: abi.RowSet, types, on_device: bool = False) -> tuple[list[np.ndarray], list[np.ndarray]]:
+    """Output row set -> (values, validity) numpy columns by qdb type; with
+    on_device the row set's buffers are in device memory (QDB_OUT_DEVICE)."""
     n = rs.RowCount
     values, valid = [], []
     for k, t in enumerate(types):
         col = rs.Columns[k]
         w = abi.WIDTH[t]
-        raw = np.ctypeslib.as_array(C.cast(col.Data, C.POINTER(C.c_uint8)), shape=(max(1, n * w),))[: n * w].copy()
+        raw = _fetch(col.Data, n * w, on_device)
         if t == abi.DECIMAL128:
             words = raw.view(np.uint64).reshape(n, 2)
             vals = np.array([int(lo) | (int(hi) << 64) for lo, hi in words], dtype=object)
@@ -248,8 +291,8 @@ def read_rowset(rs: abi.RowSet, types) -> tuple[list[np.ndarray], list[np.ndarra
                   abi.BOOL: np.uint8}[t]
             vals = raw.view(dt)
         values.append(vals)
-        if col.Mask:
-            bits = np.ctypeslib.as_array(C.cast(col.Mask, C.POINTER(C.c_uint8)), shape=(max(1, (n + 7) // 8),))
+        if col.Mask and n:
+            bits = _fetch(col.Mask, (n + 7) // 8, on_device)
             valid.append(np.unpackbits(bits, bitorder="little")[:n].astype(bool))
         else:
             valid.append(np.ones(n, dtype=bool))
@@ -340,6 +383,61 @@ class Aggregate:
             self.release()
         except Exception:
             pass
+
+
+class AggregateBatch:
+    """Many independent aggregates of one program (the partitions of a
+    partitioned GROUP BY, or small aggregations of many queries of one
+    template), each updated like an Aggregate but all in one persistent
+    launch (qdb_gpu_agg_dispatch_batch) and finished by one batched finalize
+    (qdb_gpu_agg_finish_batch)."""
+
+    def __init__(self, prog: Program, n: int):
+        _ensure_init()
+        self.prog = prog
+        self.n = n
+        self.hts = [(C.c_uint8 * abi.HASH_TABLE_SIZE)() for _ in range(n)]
+        self._ptrs = (C.c_void_p * n)(*[C.cast(h, C.c_void_p) for h in self.hts])
+
+    @property
+    def groups(self) -> list[int]:
+        return [C.cast(h, C.POINTER(C.c_int64))[9] for h in self.hts]
+
+    def add(self, rowsets) -> None:
+        """Updates aggregate i with rowsets[i]."""
+        if len(rowsets) != self.n:
+            raise ValueError(f"{self.n} aggregates, {len(rowsets)} row sets")
+        ptrs = (abi.PRS * self.n)(*[C.pointer(r.rs) for r in rowsets])
+        if lib().qdb_gpu_agg_dispatch_batch(self.prog.handle, self._ptrs, ptrs, self.n) < 0:
+            raise QdbError(f"batched aggregate update failed: {last_error()}")
+
+    def finish(self) -> list:
+        outs = (abi.RowSet * self.n)()
+        if lib().qdb_gpu_agg_finish_batch(self.prog.handle, self._ptrs, self.n, outs) < 0:
+            raise QdbError(f"batched aggregate finish failed: {last_error()}")
+        return [outs[i] for i in range(self.n)]
+
+    def release(self) -> None:
+        for h in self.hts:
+            lib().qdb_gpu_agg_release(h)
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+def autotune_info() -> dict:
+    import json
+    n = lib().qdb_gpu_autotune_info(None, 0)
+    buf = C.create_string_buffer(int(n) + 1)
+    lib().qdb_gpu_autotune_info(buf, n + 1)
+    return json.loads(buf.value.decode())
+
+
+def autotune_reset() -> None:
+    lib().qdb_gpu_autotune_reset()
 
 
 class RowJoin:

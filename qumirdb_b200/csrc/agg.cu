@@ -1559,6 +1559,48 @@ __device__ __forceinline__ int64_t GlobalFindH(const GTableDev& T, uint64_t mask
     return -1;
 }
 
+// Where a range's rows land: the aggregate's global table, its replay list
+// and its spill buffer.  `tag` names the aggregate in a batched launch (-1:
+// the launch's only aggregate): it is the second word of a replay pair and
+// the last word of a spill record.
+struct HighDst {
+    GTableDev T;
+    uint64_t cap_mask;
+    int64_t* deferred;
+    int64_t deferred_cap;
+    unsigned long long* ndeferred;
+    uint64_t* spill;
+    int64_t spill_cap;
+    unsigned long long* nspill;
+    int* error;
+    int32_t tag;
+};
+
+__device__ __forceinline__ HighDst HighDstOf(const AggLaunch& L) {
+    HighDst d;
+    d.T = L.T;
+    d.cap_mask = L.cap_mask;
+    d.deferred = L.deferred;
+    d.deferred_cap = L.deferred_cap;
+    d.ndeferred = &L.counters->deferred;
+    d.spill = L.spill;
+    d.spill_cap = L.spill_cap;
+    d.nspill = &L.counters->spilled;
+    d.error = &L.counters->error;
+    d.tag = -1;
+    return d;
+}
+
+__device__ __forceinline__ void DeferTo(const HighDst& D, int64_t row) {
+    const unsigned long long k = atomicAdd(D.ndeferred, 1ull);
+    if (int64_t(k) < D.deferred_cap) {
+        D.deferred[2 * k] = row;
+        D.deferred[2 * k + 1] = D.tag < 0 ? 0 : D.tag;
+    } else {
+        SetError(D.error, DE_DEFER_FULL);
+    }
+}
+
 // Shared tier layout inside dynamic shared memory: misc words, keys, then
 // the state words.
 struct HighLayout {
@@ -1591,10 +1633,9 @@ __device__ __forceinline__ void LoadRow(RegRow<SH::Cols::n>& row, const char* co
 // before the next rows.
 // `defer_base` numbers the range's rows for the replay list.
 template <class SH>
-__device__ __forceinline__ void HighRows(const AggLaunch& L, const HighSmem& sm, const char* const* cb,
-                                         const uint8_t* sel, int nrows, int64_t defer_base, int wid, int nw) {
-    const AggPlan& P = L.P;
-    const FastPlan& F = L.F;
+__device__ __forceinline__ void HighRows(const AggPlan& P, const FastPlan& F, const HighDst& D, const HighSmem& sm,
+                                         const char* const* cb, const uint8_t* sel, int nrows, int64_t defer_base,
+                                         int wid, int nw) {
     const int lane = int(threadIdx.x & 31);
     const int step = nw * 32;
     int r = wid * 32 + lane;
@@ -1621,21 +1662,21 @@ __device__ __forceinline__ void HighRows(const AggLaunch& L, const HighSmem& sm,
             } else {
                 int64_t gslot;
                 if (special) {
-                    gslot = L.T.capacity;
+                    gslot = D.T.capacity;
                     unsigned long long* flag = reinterpret_cast<unsigned long long*>(
-                        L.T.slots + L.T.capacity * L.T.slot_words + L.T.key_off);
+                        D.T.slots + D.T.capacity * D.T.slot_words + D.T.key_off);
                     if (*reinterpret_cast<volatile unsigned long long*>(flag) == 0 && atomicExch(flag, 1ull) == 0) {
                         atomicAdd(sm.fresh, 1u);
                     }
                 } else {
                     int is_new = 0;
-                    gslot = GlobalFindH(L.T, L.cap_mask, h, key, is_new);
+                    gslot = GlobalFindH(D.T, D.cap_mask, h, key, is_new);
                     if (is_new) atomicAdd(sm.fresh, 1u);
                 }
                 if (gslot < 0) {
-                    Defer(L, defer_base + r, 0);    // replayed after the table grows
+                    DeferTo(D, defer_base + r);    // replayed after the table grows
                 } else {
-                    ShapeAtomics<SH>(L.T.slots + gslot * L.T.slot_words + L.T.state_off, 1, v);
+                    ShapeAtomics<SH>(D.T.slots + gslot * D.T.slot_words + D.T.state_off, 1, v);
                 }
             }
         }
@@ -1647,25 +1688,26 @@ __device__ __forceinline__ void HighRows(const AggLaunch& L, const HighSmem& sm,
 
 // Shared tier -> global table (spilling what the global table cannot take),
 // then clears the tier for the next range.  Called by the whole CTA.
-__device__ __forceinline__ void HighFlush(const AggLaunch& L, const HighSmem& sm, bool reset) {
-    const AggPlan& P = L.P;
+__device__ __forceinline__ void HighFlush(const AggPlan& P, const HighDst& D, const HighSmem& sm, bool reset) {
+    const int rec_words = 1 + P.state_words + (D.tag >= 0 ? 1 : 0);
     for (int i = threadIdx.x; i < sm.S; i += blockDim.x) {
         const uint64_t key = sm.keys[i];
         if (key == kEmptyKey) continue;
         int is_new = 0;
-        const int64_t g = GlobalFindH(L.T, L.cap_mask, Fmix64(key), key, is_new);
+        const int64_t g = GlobalFindH(D.T, D.cap_mask, Fmix64(key), key, is_new);
         if (is_new) atomicAdd(sm.fresh, 1u);
         if (g < 0) {
-            const unsigned long long e = atomicAdd(&L.counters->spilled, 1ull);
-            if (int64_t(e) >= L.spill_cap) {
-                SetError(&L.counters->error, DE_SPILL_FULL);
+            const unsigned long long e = atomicAdd(D.nspill, 1ull);
+            if (int64_t(e) >= D.spill_cap) {
+                SetError(D.error, DE_SPILL_FULL);
             } else {
-                uint64_t* rec = L.spill + int64_t(e) * (1 + P.state_words);
+                uint64_t* rec = D.spill + int64_t(e) * rec_words;
                 rec[0] = key;
                 for (int w = 0; w < P.state_words; ++w) rec[1 + w] = sm.st[int64_t(w) * sm.S + i];
+                if (D.tag >= 0) rec[1 + P.state_words] = uint64_t(D.tag);
             }
         } else {
-            uint64_t* gbase = L.T.slots + g * L.T.slot_words + L.T.state_off;
+            uint64_t* gbase = D.T.slots + g * D.T.slot_words + D.T.state_off;
             for (int st2 = 0; st2 < P.nstates; ++st2) {
                 const StateDesc sd = P.states[st2];
                 const uint64_t lo = sm.st[int64_t(sd.word) * sm.S + i];
@@ -1740,11 +1782,140 @@ __global__ void __launch_bounds__(kHighThreads, 1) AggHighKernel(const __grid_co
     const char* cb[kFastCols];
     HighColumns<SH>(L, row0, cb);
     const uint8_t* sel = L.P.selection ? L.P.selection + row0 : nullptr;
-    HighRows<SH>(L, sm, cb, sel, n, row0, threadIdx.x >> 5, blockDim.x >> 5);
+    const HighDst D = HighDstOf(L);
+    HighRows<SH>(L.P, L.F, D, sm, cb, sel, n, row0, threadIdx.x >> 5, blockDim.x >> 5);
     __syncthreads();
-    HighFlush(L, sm, false);
+    HighFlush(L.P, D, sm, false);
     __syncthreads();
     if (threadIdx.x == 0 && sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
+}
+
+// ---------------------------------------------------------------------------
+// Batched high-cardinality aggregate: many independent aggregates of one
+// program (partitions of a table, or small queries of one template) in one
+// persistent launch.  Each CTA takes work items (aggregate, row range) from
+// a device queue until it runs dry, folds the range through its shared tier
+// into that aggregate's own global table, flushes the tier and takes the
+// next item.  Items come biggest aggregate first, so the short ones fill the
+// tail of the launch.
+// ---------------------------------------------------------------------------
+template <class SH>
+__global__ void __launch_bounds__(kHighThreads, 1) AggHighBatchKernel(const __grid_constant__ AggLaunch L,
+                                                                      const __grid_constant__ HighBatch B) {
+    const HighLayout hl = HighLayoutOf(L.smem_slots, L.P.state_words);
+    const HighSmem sm = HighSmemOf(L, hl);
+    __shared__ long long item_at;
+    HighInit(L, sm);
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) item_at = (long long)atomicAdd(&B.counters->next_item, 1ull);
+        __syncthreads();
+        const int64_t it = item_at;
+        if (it >= B.nitems) break;
+        const HighItem item = B.items[it];
+        const HighTask& tk = B.tasks[item.task];
+        HighDst D;
+        D.T = tk.T;
+        D.cap_mask = uint64_t(tk.T.capacity - 1);
+        D.deferred = B.deferred;
+        D.deferred_cap = B.deferred_cap;
+        D.ndeferred = &B.counters->ndeferred;
+        D.spill = B.spill;
+        D.spill_cap = B.spill_cap;
+        D.nspill = &B.counters->nspill;
+        D.error = &B.counters->error;
+        D.tag = item.task;
+        const char* cb[kFastCols];
+#pragma unroll
+        for (int c = 0; c < kFastCols; ++c) {
+            cb[c] = nullptr;
+            if (c < SH::Cols::n) cb[c] = tk.cols[c] + item.row0 * SH::cw(c);
+        }
+        const uint8_t* sel = tk.sel ? tk.sel + item.row0 : nullptr;
+        HighRows<SH>(L.P, L.F, D, sm, cb, sel, item.nrows, item.row0, threadIdx.x >> 5, blockDim.x >> 5);
+        __syncthreads();
+        HighFlush(L.P, D, sm, true);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (sm.fresh[0]) atomicAdd(&B.new_groups[item.task], (unsigned long long)sm.fresh[0]);
+            sm.fresh[0] = 0;
+            sm.count[0] = 0;
+        }
+    }
+}
+
+// Replay of a batched launch's deferred rows, one thread per (row, task)
+// pair, into tables grown since: the same typed fold, global table only.
+template <class SH>
+__global__ void __launch_bounds__(256) AggBatchReplayKernel(const __grid_constant__ AggLaunch L,
+                                                            const __grid_constant__ HighBatch B,
+                                                            const int64_t* pairs, int64_t n) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t row = pairs[2 * i];
+    const int task = int(pairs[2 * i + 1]);
+    const HighTask& tk = B.tasks[task];
+    const char* cb[kFastCols];
+#pragma unroll
+    for (int c = 0; c < kFastCols; ++c) cb[c] = c < SH::Cols::n ? tk.cols[c] : nullptr;
+    const TileRow row_acc{cb, int(row)};
+    if (SH::Atoms::n && ShapeHeld<SH>(L.P, L.F, row_acc) != L.F.clause_mask) return;
+    const uint64_t key = ShapeKey<SH>(row_acc);
+    ShapeVals<SH> v;
+    ShapeRowVals<SH>(v, L.F, row_acc);
+    int64_t gslot;
+    int is_new = 0;
+    if (L.P.key_full64 && key == kEmptyKey) {
+        gslot = tk.T.capacity;
+        unsigned long long* flag =
+            reinterpret_cast<unsigned long long*>(tk.T.slots + tk.T.capacity * tk.T.slot_words + tk.T.key_off);
+        if (*reinterpret_cast<volatile unsigned long long*>(flag) == 0 && atomicExch(flag, 1ull) == 0) is_new = 1;
+    } else {
+        gslot = GlobalFindH(tk.T, uint64_t(tk.T.capacity - 1), Fmix64(key), key, is_new);
+    }
+    if (is_new) atomicAdd(&B.new_groups[task], 1ull);
+    if (gslot < 0) {
+        HighDst D;
+        D.deferred = B.deferred;
+        D.deferred_cap = B.deferred_cap;
+        D.ndeferred = &B.counters->ndeferred;
+        D.error = &B.counters->error;
+        D.tag = task;
+        DeferTo(D, row);
+        return;
+    }
+    ShapeAtomics<SH>(tk.T.slots + gslot * tk.T.slot_words + tk.T.state_off, 1, v);
+}
+
+// Spill records [key, states..., task] of a batched launch into the grown
+// tables.
+__global__ void __launch_bounds__(256) AggBatchSpillKernel(const __grid_constant__ AggLaunch L,
+                                                           const __grid_constant__ HighBatch B,
+                                                           const uint64_t* recs, int64_t n) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const AggPlan& P = L.P;
+    const uint64_t* rec = recs + i * (2 + P.state_words);
+    const int task = int(rec[1 + P.state_words]);
+    const HighTask& tk = B.tasks[task];
+    const uint64_t key = rec[0];
+    int is_new = 0;
+    const int64_t g = GlobalFindH(tk.T, uint64_t(tk.T.capacity - 1), Fmix64(key), key, is_new);
+    if (is_new) atomicAdd(&B.new_groups[task], 1ull);
+    if (g < 0) {
+        SetError(&B.counters->error, DE_SPILL_FULL);
+        return;
+    }
+    uint64_t* gbase = tk.T.slots + g * tk.T.slot_words + tk.T.state_off;
+    for (int st2 = 0; st2 < P.nstates; ++st2) {
+        const StateDesc sd = P.states[st2];
+        const uint64_t lo = rec[1 + sd.word];
+        const uint64_t hi = sd.kind == ST_SUM_I128 ? rec[2 + sd.word] : 0;
+        if (IsIdentity(sd.kind, lo, hi)) continue;
+        double f;
+        __builtin_memcpy(&f, &lo, 8);
+        ApplyState(gbase + sd.word, gbase + sd.word + 1, sd.kind, lo, hi, f);
+    }
 }
 
 // The instantiated query shapes.  QDB_C(w, u): a fast column of w bytes
@@ -1880,7 +2051,7 @@ __global__ void AggMergeSpillKernel(const __grid_constant__ AggLaunch L, const u
 // Finalize: compact the occupied slots, in slot order, into output columns.
 // ---------------------------------------------------------------------------
 constexpr int kFinThreads = 256;
-constexpr int kFinChunk = 4096;   // slots per block
+constexpr int64_t kFinChunk = kFinChunkSlots;   // slots per block
 
 struct FinLaunch {
     AggPlan P;
@@ -1891,7 +2062,30 @@ struct FinLaunch {
     int64_t groups;
     unsigned long long* block_counts;
     int* err;
+    // Batched finalize: block b covers chunk blocks[b].chunk of table
+    // tables[blocks[b].task] (nullptr: one table, T).
+    const GTableDev* tables;
+    const FinBlock* blocks;
 };
+
+// The table and slot range of a finalize block.
+__device__ __forceinline__ GTableDev FinBlockTable(const FinLaunch& L, int64_t& begin, int64_t& end, int64_t& delta,
+                                                   int64_t& slice0) {
+    GTableDev T = L.T;
+    int64_t chunk = blockIdx.x;
+    delta = 0;
+    slice0 = -1;
+    if (L.blocks) {
+        const FinBlock fb = L.blocks[blockIdx.x];
+        T = L.tables[fb.task];
+        chunk = fb.chunk;
+        delta = fb.delta;
+        slice0 = fb.slice0;
+    }
+    begin = chunk * kFinChunk;
+    end = Min64(begin + kFinChunk, T.capacity + 1);
+    return T;
+}
 
 __device__ __forceinline__ bool SlotOccupied(const GTableDev& T, int64_t i) {
     const uint64_t* s = T.slots + i * T.slot_words;
@@ -1904,10 +2098,10 @@ __global__ void __launch_bounds__(kFinThreads) FinCountKernel(const __grid_const
     __shared__ unsigned cnt;
     if (threadIdx.x == 0) cnt = 0;
     __syncthreads();
-    const int64_t begin = int64_t(blockIdx.x) * kFinChunk;
-    const int64_t end = Min64(begin + kFinChunk, L.T.capacity + 1);
+    int64_t begin, end, delta, slice0;
+    const GTableDev T = FinBlockTable(L, begin, end, delta, slice0);
     unsigned local = 0;
-    for (int64_t i = begin + threadIdx.x; i < end; i += blockDim.x) local += SlotOccupied(L.T, i) ? 1 : 0;
+    for (int64_t i = begin + threadIdx.x; i < end; i += blockDim.x) local += SlotOccupied(T, i) ? 1 : 0;
     atomicAdd(&cnt, local);
     __syncthreads();
     if (threadIdx.x == 0) L.block_counts[blockIdx.x] = cnt;
@@ -1958,7 +2152,11 @@ struct OutRowAcc {
     __device__ bool Null(int c) const { return (nulls >> c) & 1; }
 };
 
-__device__ __forceinline__ void StoreValue(const AggOutputCol& col, int64_t row, const GVal& v, bool null) {
+// slice0 >= 0: the output is cut into per-aggregate slices and `row`'s
+// slice starts at row slice0; string offsets count from the slice start and
+// each row writes its own start offset too.
+__device__ __forceinline__ void StoreValue(const AggOutputCol& col, int64_t row, const GVal& v, bool null,
+                                           int64_t slice0 = -1) {
     if (col.valid && !null) atomicOr(&col.valid[row >> 5], 1u << (row & 31));
     char* p = col.data;
     switch (col.type) {
@@ -1978,8 +2176,13 @@ __device__ __forceinline__ void StoreValue(const AggOutputCol& col, int64_t row,
         default:
             reinterpret_cast<uint8_t*>(p)[row] = null ? 0 : uint8_t(v.i);
             if (col.offsets) {
-                col.offsets[row + 1] = int32_t(row + 1);
-                if (row == 0) col.offsets[0] = 0;
+                if (slice0 >= 0) {
+                    col.offsets[row] = int32_t(row - slice0);
+                    col.offsets[row + 1] = int32_t(row + 1 - slice0);
+                } else {
+                    col.offsets[row + 1] = int32_t(row + 1);
+                    if (row == 0) col.offsets[0] = 0;
+                }
             }
             break;
     }
@@ -1992,12 +2195,12 @@ __global__ void __launch_bounds__(kFinThreads) FinWriteKernel(const __grid_const
     const OutputPlan& O = L.O;
     if (threadIdx.x == 0) running = 0;
     __syncthreads();
-    const int64_t begin = int64_t(blockIdx.x) * kFinChunk;
-    const int64_t end = Min64(begin + kFinChunk, L.T.capacity + 1);
-    const unsigned long long block_off = L.block_counts[blockIdx.x];
+    int64_t begin, end, delta, slice0;
+    const GTableDev T = FinBlockTable(L, begin, end, delta, slice0);
+    const unsigned long long block_off = L.block_counts[blockIdx.x] + uint64_t(delta);
     for (int64_t b = begin; b < end; b += blockDim.x) {
         const int64_t i = b + threadIdx.x;
-        const bool occ = i < end && SlotOccupied(L.T, i);
+        const bool occ = i < end && SlotOccupied(T, i);
         const unsigned m = __ballot_sync(kFull, occ);
         if (LaneId() == 0) warp_off[threadIdx.x >> 5] = __popc(m);
         __syncthreads();
@@ -2013,12 +2216,12 @@ __global__ void __launch_bounds__(kFinThreads) FinWriteKernel(const __grid_const
         if (occ) {
             const int64_t row = int64_t(block_off) + before;
             if (row < L.groups) {
-                const uint64_t* s = L.T.slots + i * L.T.slot_words;
+                const uint64_t* s = T.slots + i * T.slot_words;
                 uint64_t kw[kMaxKeyWords];
-                if (!L.T.wide && i == L.T.capacity) {
+                if (!T.wide && i == T.capacity) {
                     kw[0] = kEmptyKey;
                 } else {
-                    for (int w = 0; w < P.key_words; ++w) kw[w] = s[L.T.key_off + w];
+                    for (int w = 0; w < P.key_words; ++w) kw[w] = s[T.key_off + w];
                 }
                 GVal rowv[kMaxCols + kMaxAggs];
                 uint64_t nulls = 0;
@@ -2038,7 +2241,7 @@ __global__ void __launch_bounds__(kFinThreads) FinWriteKernel(const __grid_const
                         rowv[c].i = UnpackKeyInt(k, kw);
                     }
                 }
-                const uint64_t* st = s + L.T.state_off;
+                const uint64_t* st = s + T.state_off;
                 for (int j = 0; j < P.naggs; ++j, ++c) {
                     const AggOut& ao = P.aggs[j];
                     const StateDesc sd = P.states[ao.state];
@@ -2062,7 +2265,7 @@ __global__ void __launch_bounds__(kFinThreads) FinWriteKernel(const __grid_const
                     }
                 }
                 if (O.identity) {
-                    for (int k = 0; k < L.ncols; ++k) StoreValue(L.cols[k], row, rowv[k], (nulls >> k) & 1);
+                    for (int k = 0; k < L.ncols; ++k) StoreValue(L.cols[k], row, rowv[k], (nulls >> k) & 1, slice0);
                 } else {
                     GVal gv[kMaxGNodes];
                     uint64_t gn = 0;
@@ -2070,7 +2273,7 @@ __global__ void __launch_bounds__(kFinThreads) FinWriteKernel(const __grid_const
                     if (!EvalGeneric(O.prog, O.root_max, O.list, oa, gv, gn)) SetError(L.err, DE_DIV_ZERO);
                     for (int k = 0; k < L.ncols; ++k) {
                         const int rt = O.roots[k];
-                        StoreValue(L.cols[k], row, gv[rt], (gn >> rt) & 1);
+                        StoreValue(L.cols[k], row, gv[rt], (gn >> rt) & 1, slice0);
                     }
                 }
             }
@@ -2493,6 +2696,148 @@ void AggFinalize(const AggPlan& p, const OutputPlan& out, const GTableDev& t, Ag
     FinCountKernel<<<int(blocks), kFinThreads, 0, s>>>(L);
     FinScanKernel<<<1, 1024, 0, s>>>(L.block_counts, blocks);
     FinWriteKernel<<<int(blocks), kFinThreads, 0, s>>>(L);
+    ProfileEnd(s);
+    CountLaunch(3);
+}
+
+// ---------------------------------------------------------------------------
+// Batched aggregate launchers.
+// ---------------------------------------------------------------------------
+__global__ void AggBatchMarkKernel(const HighTask* tasks, int ntasks, int keyless) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ntasks) return;
+    const GTableDev& T = tasks[i].T;
+    if (!T.wide) T.slots[T.capacity * T.slot_words + T.key_off] = 0;   // flag slot: unused
+    if (keyless) T.slots[int64_t(Fmix64(0) & uint64_t(T.capacity - 1)) * T.slot_words + T.key_off] = 0;
+}
+
+void AggBatchInitTables(const AggPlan& p, const GTableDev& all, const HighTask* tasks, int ntasks,
+                        cudaStream_t s) {
+    AggInitTable(p, all, s);
+    if (ntasks <= 0) return;
+    AggBatchMarkKernel<<<(ntasks + 255) / 256, 256, 0, s>>>(tasks, ntasks, p.nkeyparts == 0 ? 1 : 0);
+    CountLaunch();
+}
+
+namespace {
+
+struct BatchFns {
+    void (*update)(AggLaunch, HighBatch) = nullptr;
+    void (*replay)(AggLaunch, HighBatch, const int64_t*, int64_t) = nullptr;
+};
+
+BatchFns FindBatchKernels(const AggPlan& P, const FastPlan& F) {
+    BatchFns b;
+    const std::vector<int> key = ShapeKeyOf(P, F);
+    if (key.empty()) return b;
+#define QDB_SHAPE_FIND(...)                                                           \
+    if (!b.update && ShapeMatches<__VA_ARGS__>(key) && ShapeWordsMatch<__VA_ARGS__>(F)) { \
+        b.update = AggHighBatchKernel<__VA_ARGS__>;                                   \
+        b.replay = AggBatchReplayKernel<__VA_ARGS__>;                                 \
+    }
+    QDB_HIGH_SHAPE_LIST(QDB_SHAPE_FIND)
+    QDB_SHAPE_LIST(QDB_SHAPE_FIND)
+#undef QDB_SHAPE_FIND
+    return b;
+}
+
+AggLaunch& BatchLaunchOf(const AggPlan& p, const FastPlan& f, int smem_slots) {
+    static thread_local AggLaunch* Lp = nullptr;
+    if (!Lp) Lp = new AggLaunch();
+    AggLaunch& L = *Lp;
+    std::memset(&L, 0, sizeof(L));
+    L.P = p;
+    L.F = f;
+    L.smem_slots = smem_slots;
+    L.smem_limit = smem_slots / 2;
+    L.inline_slot = -1;
+    return L;
+}
+
+}  // namespace
+
+std::string AggBatchShapeKey(const AggPlan& p, const FastPlan& f) {
+    std::string k;
+    for (int v : ShapeKeyOf(p, f)) k += std::to_string(v) + ",";
+    return k;
+}
+
+bool AggBatchSupported(const AggPlan& p, const FastPlan& f) {
+    return p.key_words <= 1 && FindBatchKernels(p, f).update != nullptr;
+}
+
+int AggBatchOccupancy(const AggPlan& p, const FastPlan& f, int threads, int smem_slots) {
+    EnsureDeviceInfo();
+    const BatchFns fns = FindBatchKernels(p, f);
+    if (!fns.update) return 0;
+    const size_t bytes = size_t(HighLayoutOf(smem_slots, p.state_words).bytes) + 64;
+    if (bytes > g_smem_optin) return 0;
+    SetSmem(fns.update, bytes);
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fns.update, threads, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+void AggBatchUpdate(const AggPlan& p, const FastPlan& f, const HighBatch& b, int threads, int smem_slots, int grid,
+                    cudaStream_t s) {
+    EnsureDeviceInfo();
+    const BatchFns fns = FindBatchKernels(p, f);
+    AggLaunch& L = BatchLaunchOf(p, f, smem_slots);
+    const size_t bytes = size_t(HighLayoutOf(smem_slots, p.state_words).bytes);
+    SetSmem(fns.update, bytes + 64);
+    ProfileBegin(s, "agg_batch_update", b.nitems);
+    fns.update<<<grid, threads, bytes, s>>>(L, b);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+void AggBatchReplay(const AggPlan& p, const FastPlan& f, const HighBatch& b, const int64_t* pairs, int64_t n,
+                    cudaStream_t s) {
+    if (n <= 0) return;
+    const BatchFns fns = FindBatchKernels(p, f);
+    AggLaunch& L = BatchLaunchOf(p, f, 0);
+    ProfileBegin(s, "agg_batch_replay", n);
+    fns.replay<<<int((n + 255) / 256), 256, 0, s>>>(L, b, pairs, n);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+void AggBatchSpill(const AggPlan& p, const HighBatch& b, const uint64_t* recs, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    FastPlan f{};
+    AggLaunch& L = BatchLaunchOf(p, f, 0);
+    ProfileBegin(s, "agg_batch_spill", n);
+    AggBatchSpillKernel<<<int((n + 255) / 256), 256, 0, s>>>(L, b, recs, n);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+size_t AggFinalizeBatchScratch(int64_t nblocks) { return size_t(std::max<int64_t>(nblocks, 1)) * 8; }
+
+void AggFinalizeBatch(const AggPlan& p, const OutputPlan& out, const GTableDev* tables, const FinBlock* blocks,
+                      int64_t nblocks, AggOutputCol* cols, int ncols, int64_t out_rows, void* scratch, int* err,
+                      cudaStream_t s) {
+    if (nblocks <= 0) return;
+    static thread_local FinLaunch* Lp = nullptr;
+    if (!Lp) Lp = new FinLaunch();
+    FinLaunch& L = *Lp;
+    std::memset(&L, 0, sizeof(L));
+    L.P = p;
+    L.O = out;
+    for (int k = 0; k < ncols; ++k) L.cols[k] = cols[k];
+    L.ncols = ncols;
+    L.groups = out_rows;
+    L.block_counts = static_cast<unsigned long long*>(scratch);
+    L.err = err;
+    L.tables = tables;
+    L.blocks = blocks;
+    ProfileBegin(s, "agg_finalize_batch", nblocks);
+    FinCountKernel<<<int(nblocks), kFinThreads, 0, s>>>(L);
+    FinScanKernel<<<1, 1024, 0, s>>>(L.block_counts, nblocks);
+    FinWriteKernel<<<int(nblocks), kFinThreads, 0, s>>>(L);
     ProfileEnd(s);
     CountLaunch(3);
 }

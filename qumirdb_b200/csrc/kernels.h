@@ -204,7 +204,72 @@ size_t CompactScratch(int64_t n);
 void CompactFlags(const uint8_t* flags, int64_t n, int64_t* out_idx, unsigned long long* d_count, void* scratch,
                   cudaStream_t s);
 
+// ---- batched aggregate: many aggregates of one program per launch ----
+// One aggregate of a batched launch: its columns (the program's typed shape
+// columns, at the aggregate's row 0), selection, rows and global table.
+struct HighTask {
+    const char* cols[kFastCols];
+    const uint8_t* sel;
+    int64_t nrows;
+    GTableDev T;
+};
+// A work item: rows [row0, row0 + nrows) of one aggregate.
+struct HighItem {
+    int32_t task;
+    int32_t nrows;
+    int64_t row0;
+};
+struct BatchCounters {
+    unsigned long long next_item;   // work queue head
+    unsigned long long ndeferred;
+    unsigned long long nspill;
+    int error;
+    int pad;
+};
+struct HighBatch {
+    const HighTask* tasks;
+    const HighItem* items;
+    int64_t nitems;
+    unsigned long long* new_groups;   // per aggregate
+    BatchCounters* counters;
+    int64_t* deferred;                // (row, aggregate) pairs
+    int64_t deferred_cap;
+    uint64_t* spill;                  // [key, states..., aggregate] records
+    int64_t spill_cap;
+};
+// The program's batched kernel exists when its typed shape was compiled in.
+bool AggBatchSupported(const AggPlan& p, const FastPlan& f);
+// A name of the program's typed shape (the autotuner's key).
+std::string AggBatchShapeKey(const AggPlan& p, const FastPlan& f);
+// Resident CTAs per SM of the batched kernel at this block shape.
+int AggBatchOccupancy(const AggPlan& p, const FastPlan& f, int threads, int smem_slots);
+void AggBatchUpdate(const AggPlan& p, const FastPlan& f, const HighBatch& b, int threads, int smem_slots, int grid,
+                    cudaStream_t s);
+void AggBatchReplay(const AggPlan& p, const FastPlan& f, const HighBatch& b, const int64_t* pairs, int64_t n,
+                    cudaStream_t s);
+void AggBatchSpill(const AggPlan& p, const HighBatch& b, const uint64_t* recs, int64_t n, cudaStream_t s);
+// Initialises `total` slots laid out like the tables of `tasks` (contiguous
+// tables of one slot layout), then marks each table's one-word-key flag slot
+// (and, keyless, its group at key 0).
+void AggBatchInitTables(const AggPlan& p, const GTableDev& all, const HighTask* tasks, int ntasks,
+                        cudaStream_t s);
+// Batched finalize: block b covers slots [chunk * kFinChunkSlots, ...) of
+// table `task`; its groups land at output row (scan of the block counts) +
+// delta, in the task's output slice that starts at row slice0.
+struct FinBlock {
+    int32_t task;
+    int32_t chunk;
+    int64_t delta;
+    int64_t slice0;
+};
+constexpr int64_t kFinChunkSlots = 4096;
+size_t AggFinalizeBatchScratch(int64_t nblocks);
+void AggFinalizeBatch(const AggPlan& p, const OutputPlan& out, const GTableDev* tables, const FinBlock* blocks,
+                      int64_t nblocks, AggOutputCol* cols, int ncols, int64_t out_rows, void* scratch, int* err,
+                      cudaStream_t s);
+
 // Kernel timing hooks (runtime.cpp).
+bool ProfileOn();
 void ProfileBegin(cudaStream_t s, const char* name, int64_t units);
 void ProfileEnd(cudaStream_t s);
 void CountLaunch(int n = 1);

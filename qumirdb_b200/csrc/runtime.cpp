@@ -80,6 +80,8 @@ cudaStream_t CurStream() {
     return g_lib_stream;
 }
 
+bool ProfileOn() { return g_prof_on.load(std::memory_order_relaxed); }
+
 void ProfileBegin(cudaStream_t s, const char* name, int64_t units) {
     if (!g_prof_on.load(std::memory_order_relaxed)) return;
     ProfRec r;
@@ -232,26 +234,11 @@ int64_t NextPow2(int64_t v) {
 // ---------------------------------------------------------------------------
 // Aggregate table state.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kAggMagic = 0x51444741;   // 'QDGA'
-constexpr int64_t kChunkRows = int64_t(64) << 20;
-
-struct AggTableState {
-    uint32_t magic = kAggMagic;
-    cudaStream_t s = nullptr;
-    GTableDev t;
-    AggCounters* dc = nullptr;      // device counters
-    AggCounters* hc = nullptr;      // pinned host mirror
-    int64_t groups = 0;
-    int64_t expected = 0;
-    int64_t* deferred[2] = {nullptr, nullptr};
-    int64_t deferred_cap = 0;
-    uint64_t* spill = nullptr;
-    int64_t spill_cap = 0;
-    int smem_slots = 2048;
-    int64_t matched = 0;
-};
-
-namespace {
+void AggArenaRelease(AggArena* a) {
+    if (!a || --a->refs > 0) return;
+    DevFree(a->p, a->s);
+    delete a;
+}
 
 // Slots are 16-byte aligned; a 48-byte slot still spans two 32-byte sectors.
 int SlotWords(const AggPlan& p, bool wide) {
@@ -272,6 +259,7 @@ bool AllocTable(const AggPlan& p, int64_t capacity, cudaStream_t s, GTableDev& t
 }
 
 AggTableState* StateOf(void* ht) {
+    if (!ht) return nullptr;
     AggTableState* st = *static_cast<AggTableState**>(ht);
     if (!st || st->magic != kAggMagic) return nullptr;
     return st;
@@ -305,7 +293,8 @@ bool Grow(AggTableState* st, const AggPlan& p, int64_t min_groups) {
     GTableDev nt;
     if (!AllocTable(p, cap, st->s, nt)) return false;
     AggRehash(p, st->t, nt, st->dc, st->s);
-    DevFree(st->t.slots, st->s);
+    if (!st->table_in_arena) DevFree(st->t.slots, st->s);
+    st->table_in_arena = false;
     st->t = nt;
     return true;
 }
@@ -329,8 +318,6 @@ bool EnsureBuffers(AggTableState* st, const AggPlan& p, int64_t rows) {
     }
     return true;
 }
-
-}  // namespace
 
 AggTableState* AggStateCreate(const AggPlan& p, int64_t capacity_hint, int64_t expected, cudaStream_t s) {
     auto* st = new AggTableState();
@@ -381,8 +368,9 @@ void AggMirrorHeader(void* ht, const AggTableState* st, const AggPlan& p) { Mirr
 
 void AggStateDestroy(AggTableState* st) {
     if (!st) return;
-    DevFree(st->t.slots, st->s);
-    DevFree(st->dc, st->s);
+    if (!st->table_in_arena) DevFree(st->t.slots, st->s);
+    if (!st->dc_in_arena) DevFree(st->dc, st->s);
+    AggArenaRelease(st->arena);
     DevFree(st->deferred[0], st->s);
     DevFree(st->deferred[1], st->s);
     DevFree(st->spill, st->s);
@@ -429,34 +417,40 @@ bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyP
         if (!ReadCounters(st)) return false;
         st->groups += int64_t(st->hc->new_groups);
         st->matched += int64_t(st->hc->matched);
-        int64_t ndef = int64_t(st->hc->deferred);
-        int64_t nspill = int64_t(st->hc->spilled);
-        int cur = 0;
-        for (int round = 0; (ndef > 0 || nspill > 0); ++round) {
-            if (round > 16) {
-                SetErr("aggregate replay did not converge");
-                return false;
-            }
-            if (!Grow(st, plan, st->groups + ndef + nspill)) return false;
-            ResetCounters(st);
-            AggMergeSpill(plan, st->spill, nspill, st->t, st->dc, st->s);
-            // Replay deferred rows into the grown table; new deferrals go to the other buffer.
-            AggUpdateArgs r = a;
-            r.table = st->t;
-            r.index = st->deferred[cur];
-            r.nindex = ndef;
-            r.deferred = st->deferred[cur ^ 1];
-            r.join = jk != nullptr;
-            AggUpdate(r, st->s);
-            cur ^= 1;
-            if (!ReadCounters(st)) return false;
-            st->groups += int64_t(st->hc->new_groups);
-            ndef = int64_t(st->hc->deferred);
-            nspill = int64_t(st->hc->spilled);
+        if (!AggReplay(st, plan, a, int64_t(st->hc->deferred), int64_t(st->hc->spilled))) return false;
+    }
+    return true;
+}
+
+bool AggReplay(AggTableState* st, const AggPlan& plan, const AggUpdateArgs& a, int64_t ndef, int64_t nspill) {
+    int cur = 0;
+    for (int round = 0; (ndef > 0 || nspill > 0); ++round) {
+        if (round > 16) {
+            SetErr("aggregate replay did not converge");
+            return false;
         }
-        if (st->groups * 2 > st->t.capacity) {
-            if (!Grow(st, plan, st->groups)) return false;
-        }
+        if (!Grow(st, plan, st->groups + ndef + nspill)) return false;
+        ResetCounters(st);
+        AggMergeSpill(plan, st->spill, nspill, st->t, st->dc, st->s);
+        // Replay deferred rows into the grown table; new deferrals go to the other buffer.
+        AggUpdateArgs r = a;
+        r.table = st->t;
+        r.counters = st->dc;
+        r.index = st->deferred[cur];
+        r.nindex = ndef;
+        r.deferred = st->deferred[cur ^ 1];
+        r.deferred_cap = st->deferred_cap;
+        r.spill = st->spill;
+        r.spill_cap = st->spill_cap;
+        AggUpdate(r, st->s);
+        cur ^= 1;
+        if (!ReadCounters(st)) return false;
+        st->groups += int64_t(st->hc->new_groups);
+        ndef = int64_t(st->hc->deferred);
+        nspill = int64_t(st->hc->spilled);
+    }
+    if (st->groups * 2 > st->t.capacity) {
+        if (!Grow(st, plan, st->groups)) return false;
     }
     return true;
 }

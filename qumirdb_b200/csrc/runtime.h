@@ -37,7 +37,50 @@ bool ResolveColumns(AggPlan& P, const ColumnMap& cm, const qdb_column_type* type
                     Staging& st);
 AggPlan OffsetPlan(const AggPlan& P, int64_t begin);
 
-struct AggTableState;
+// Device memory shared by the tables of a batch of aggregate states; freed
+// with the last state that uses it.
+struct AggArena {
+    void* p = nullptr;
+    int64_t refs = 0;
+    cudaStream_t s = nullptr;
+};
+void AggArenaRelease(AggArena* a);
+
+constexpr uint32_t kAggMagic = 0x51444741;   // 'QDGA'
+constexpr int64_t kChunkRows = int64_t(64) << 20;
+
+// Device state behind an aggregate's caller-owned HashTable buffer.
+struct AggTableState {
+    uint32_t magic = kAggMagic;
+    cudaStream_t s = nullptr;
+    GTableDev t;
+    AggCounters* dc = nullptr;      // device counters
+    AggCounters* hc = nullptr;      // pinned host mirror
+    int64_t groups = 0;
+    int64_t expected = 0;
+    int64_t* deferred[2] = {nullptr, nullptr};
+    int64_t deferred_cap = 0;
+    uint64_t* spill = nullptr;
+    int64_t spill_cap = 0;
+    int smem_slots = 2048;
+    int64_t matched = 0;
+    AggArena* arena = nullptr;      // batch-created: table and counters may live here
+    bool table_in_arena = false;
+    bool dc_in_arena = false;
+};
+
+AggTableState* StateOf(void* ht);
+int SlotWords(const AggPlan& p, bool wide);
+bool AllocTable(const AggPlan& p, int64_t capacity, cudaStream_t s, GTableDev& t);
+bool Grow(AggTableState* st, const AggPlan& p, int64_t min_groups);
+bool EnsureBuffers(AggTableState* st, const AggPlan& p, int64_t rows);
+bool ReadCounters(AggTableState* st);
+void ResetCounters(AggTableState* st);
+void MirrorHeader(void* ht, const AggTableState* st, const AggPlan& p);
+// Grows the table and replays `ndef` deferred rows (st->deferred[0], as
+// (row, build row) pairs) and `nspill` spilled entries (st->spill) of an
+// update described by `a`, until none is left.
+bool AggReplay(AggTableState* st, const AggPlan& plan, const AggUpdateArgs& a, int64_t ndef, int64_t nspill);
 AggTableState* AggStateCreate(const AggPlan& p, int64_t capacity_hint, int64_t expected, cudaStream_t s);
 void AggStateDestroy(AggTableState* st);
 bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyPlan* jk, const JTableDev* jt,
