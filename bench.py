@@ -301,8 +301,7 @@ def zipf_batched_operator(q, peak):
         b = q.AggregateBatch(prog, len(parts))
         b.add(parts)
         groups.append(sum(b.groups))
-        for o in b.finish():
-            q.release(o)
+        b.finish().release()
 
     ms, _, launches, _ = timed(q, step, 3, 3)
     _, _, _, kernels = timed(q, step, 2, 0, profile=True)
@@ -502,8 +501,7 @@ def profile_case(name: str, rows: int) -> None:
         for _ in range(2):
             b = q.AggregateBatch(prog, len(parts))
             b.add(parts)
-            for o in b.finish():
-                q.release(o)
+            b.finish().release()
     elif name == "sort":
         n = rows or SORT_ROWS
         k1 = np.empty(n, np.int64)

@@ -420,6 +420,11 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* program, void* const* 
 int64_t qdb_gpu_agg_finish_batch(const qdb_gpu_program* program, void* const* states, int64_t n,
                                  qdb_rowset* outs);
 
+/* Calls Destroy on each of n row sets (the outputs of a batched finish):    */
+/* one call instead of n for a binding that pays per foreign call.  No       */
+/* reference counterpart.                                                    */
+void qdb_gpu_release_rowsets(qdb_rowset* rowsets, int64_t n);
+
 /* The autotuner's state as JSON (searches, timed trials, reuses, graph      */
 /* replays, chosen configurations); returns the JSON length.  No reference   */
 /* counterpart.                                                              */

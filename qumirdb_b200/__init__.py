@@ -396,12 +396,15 @@ class AggregateBatch:
         _ensure_init()
         self.prog = prog
         self.n = n
-        self.hts = [(C.c_uint8 * abi.HASH_TABLE_SIZE)() for _ in range(n)]
-        self._ptrs = (C.c_void_p * n)(*[C.cast(h, C.c_void_p) for h in self.hts])
+        # The n HashTable buffers side by side in one array.
+        self._buf = (C.c_uint8 * (abi.HASH_TABLE_SIZE * max(n, 1)))()
+        base = C.addressof(self._buf)
+        self._ptrs = (C.c_void_p * max(n, 1))(*range(base, base + abi.HASH_TABLE_SIZE * n, abi.HASH_TABLE_SIZE))
 
     @property
     def groups(self) -> list[int]:
-        return [C.cast(h, C.POINTER(C.c_int64))[9] for h in self.hts]
+        words = np.frombuffer(self._buf, dtype=np.int64).reshape(max(self.n, 1), abi.HASH_TABLE_SIZE // 8)
+        return words[: self.n, 9].tolist()
 
     def add(self, rowsets) -> None:
         """Updates aggregate i with rowsets[i]."""
@@ -411,21 +414,47 @@ class AggregateBatch:
         if lib().qdb_gpu_agg_dispatch_batch(self.prog.handle, self._ptrs, ptrs, self.n) < 0:
             raise QdbError(f"batched aggregate update failed: {last_error()}")
 
-    def finish(self) -> list:
-        outs = (abi.RowSet * self.n)()
+    def finish(self) -> "RowSets":
+        outs = (abi.RowSet * max(self.n, 1))()
         if lib().qdb_gpu_agg_finish_batch(self.prog.handle, self._ptrs, self.n, outs) < 0:
             raise QdbError(f"batched aggregate finish failed: {last_error()}")
-        return [outs[i] for i in range(self.n)]
+        self._finished = True   # the states are destroyed and zeroed
+        return RowSets(outs, self.n)
 
     def release(self) -> None:
-        for h in self.hts:
-            lib().qdb_gpu_agg_release(h)
+        if getattr(self, "_finished", False):
+            return
+        for i in range(self.n):
+            lib().qdb_gpu_agg_release(self._ptrs[i])
 
     def __del__(self):
         try:
             self.release()
         except Exception:
             pass
+
+
+class RowSets:
+    """Output row sets of a batched finish: indexable like a list, released
+    together by release() (one foreign call)."""
+
+    def __init__(self, arr, n: int):
+        self.arr = arr
+        self.n = n
+
+    def __len__(self) -> int:
+        return self.n
+
+    def __getitem__(self, i: int) -> abi.RowSet:
+        if not -self.n <= i < self.n:
+            raise IndexError(i)
+        return self.arr[i % self.n]
+
+    def __iter__(self):
+        return (self.arr[i] for i in range(self.n))
+
+    def release(self) -> None:
+        lib().qdb_gpu_release_rowsets(self.arr, self.n)
 
 
 def autotune_info() -> dict:

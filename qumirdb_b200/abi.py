@@ -121,6 +121,7 @@ SIGNATURES = {
     "qdb_gpu_agg_finish_batch": (CI64, [P, C.POINTER(P), CI64, PRS]),
     "qdb_gpu_autotune_info": (CI64, [C.c_char_p, CI64]),
     "qdb_gpu_autotune_reset": (None, []),
+    "qdb_gpu_release_rowsets": (None, [PRS, CI64]),
     "qdb_gpu_jr_release": (None, [P, P, P, P]),
     "qdb_gpu_join_aggregate_probe": (CI64, [P, P, P, P, PRS]),
     "qdb_gpu_sort_run": (CI64, [P, PRS, P, P, P, CI64, P, P, BOOLC, CI64, CI64, PRS]),

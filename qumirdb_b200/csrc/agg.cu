@@ -1972,22 +1972,44 @@ __global__ void __launch_bounds__(256) AggIndexKernel(const __grid_constant__ Ag
 // ---------------------------------------------------------------------------
 // Table maintenance kernels.
 // ---------------------------------------------------------------------------
+// An empty slot's words are built once per block in shared memory.  With a
+// 16-byte aligned table the table is one array of 16-byte vectors, slot_words
+// / 2 per slot; blocks hold a multiple of that many threads and the grid
+// strides by a multiple too, so each thread always writes the same vector of
+// the slot, and consecutive threads consecutive vectors.  The host then
+// clears the flag slot's key word (slot_words <= kInitMaxSlotWords: at most
+// 1 + kMaxKeyWords + kMaxStates).
+constexpr int kInitMaxSlotWords = 64;
+static_assert(1 + kMaxKeyWords + kMaxStates <= kInitMaxSlotWords + 1, "slot template too small");
+
 __global__ void AggInitKernel(uint64_t* slots, int64_t capacity, int32_t slot_words, int32_t key_off,
-                              int32_t state_off, int32_t wide, const __grid_constant__ StatesParam sp) {
-    const int64_t total = (capacity + 1) * slot_words;
-    for (int64_t w = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; w < total; w += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t slot = w / slot_words;
-        const int32_t off = int32_t(w - slot * slot_words);
+                              int32_t state_off, int32_t wide, int32_t vec16, const __grid_constant__ StatesParam sp) {
+    __shared__ __align__(16) uint64_t tmpl[kInitMaxSlotWords];
+    for (int off = threadIdx.x; off < slot_words; off += blockDim.x) {
         uint64_t v = 0;
         if (!wide && off == key_off) {
-            v = slot == capacity ? 0 : kEmptyKey;
+            v = kEmptyKey;
         } else if (off >= state_off) {
             const int32_t sw = off - state_off;
             for (int s = 0; s < sp.n; ++s) {
                 if (sp.s[s].word == sw) v = StateIdentity(sp.s[s].kind);
             }
         }
-        slots[w] = v;
+        tmpl[off] = v;
+    }
+    __syncthreads();
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    const int64_t first = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (vec16) {
+        const int vec = slot_words / 2;
+        const uint4 v = reinterpret_cast<const uint4*>(tmpl)[threadIdx.x % vec];
+        uint4* dst = reinterpret_cast<uint4*>(slots);
+        const int64_t total = (capacity + 1) * vec;
+        for (int64_t i = first; i < total; i += stride) dst[i] = v;
+    } else {
+        const uint64_t v = tmpl[threadIdx.x % slot_words];
+        const int64_t total = (capacity + 1) * slot_words;
+        for (int64_t i = first; i < total; i += stride) slots[i] = v;
     }
 }
 
@@ -2066,6 +2088,12 @@ struct FinLaunch {
     // tables[blocks[b].task] (nullptr: one table, T).
     const GTableDev* tables;
     const FinBlock* blocks;
+    // Copy plan: every output column is one (or, for DECIMAL128, two) slot
+    // words stored as they are (copy_n = ncols), else 0.
+    int32_t copy_n;
+    int8_t copy_word[kMaxCols + kMaxAggs];
+    int8_t copy_two[kMaxCols + kMaxAggs];
+    int8_t copy_key[kMaxCols + kMaxAggs];
 };
 
 // The table and slot range of a finalize block.
@@ -2213,7 +2241,23 @@ __global__ void __launch_bounds__(kFinThreads) FinWriteKernel(const __grid_const
             for (int w = 0; w < kFinThreads / 32; ++w) tot += warp_off[w];
             running += tot;
         }
-        if (occ) {
+        if (occ && L.copy_n) {
+            const int64_t row = int64_t(block_off) + before;
+            if (row < L.groups) {
+                const uint64_t* s = T.slots + i * T.slot_words;
+                const bool flag_slot = !T.wide && i == T.capacity;
+                for (int k = 0; k < L.copy_n; ++k) {
+                    uint64_t* dst = reinterpret_cast<uint64_t*>(L.cols[k].data);
+                    const int w = L.copy_word[k];
+                    if (L.copy_two[k]) {
+                        dst[2 * row] = s[w];
+                        dst[2 * row + 1] = s[w + 1];
+                    } else {
+                        dst[row] = (L.copy_key[k] && flag_slot) ? kEmptyKey : s[w];
+                    }
+                }
+            }
+        } else if (occ) {
             const int64_t row = int64_t(block_off) + before;
             if (row < L.groups) {
                 const uint64_t* s = T.slots + i * T.slot_words;
@@ -2323,10 +2367,16 @@ void AggInitTable(const AggPlan& p, const GTableDev& t, cudaStream_t s) {
     StatesParam sp;
     std::memcpy(sp.s, p.states, sizeof(sp.s));
     sp.n = p.nstates;
-    const int64_t total = (t.capacity + 1) * t.slot_words;
-    const int blocks = int(std::min<int64_t>((total + 255) / 256, int64_t(DeviceSMs()) * 16));
+    // Threads per block: a multiple of the vectors (or words) per slot.
+    const bool vec16 = (reinterpret_cast<uintptr_t>(t.slots) & 15) == 0 && (t.slot_words & 1) == 0;
+    const int per_slot = vec16 ? t.slot_words / 2 : t.slot_words;
+    const int threads = per_slot * std::max(1, 512 / per_slot);
+    const int64_t total = (t.capacity + 1) * per_slot;
+    const int blocks = int(std::min<int64_t>((total + threads - 1) / threads, int64_t(DeviceSMs()) * 8));
     ProfileBegin(s, "agg_init_table", t.capacity);
-    AggInitKernel<<<blocks, 256, 0, s>>>(t.slots, t.capacity, t.slot_words, t.key_off, t.state_off, t.wide, sp);
+    AggInitKernel<<<blocks, threads, 0, s>>>(t.slots, t.capacity, t.slot_words, t.key_off, t.state_off, t.wide,
+                                             vec16 ? 1 : 0, sp);
+    if (!t.wide) cudaMemsetAsync(t.slots + t.capacity * t.slot_words + t.key_off, 0, 8, s);   // flag slot: unused
     ProfileEnd(s);
     CountLaunch();
 }
@@ -2672,6 +2722,67 @@ void ExclusiveScanU64(unsigned long long* counts, int64_t n, cudaStream_t s) {
     CountLaunch();
 }
 
+// Output columns of an identity output that no group can leave NULL (keys
+// and aggregates over non-nullable inputs) get an all-valid bitmap up front
+// instead of one atomic per row.
+static void PresetValidity(const AggPlan& p, const OutputPlan& out, FinLaunch& L, int64_t rows, cudaStream_t s) {
+    if (!out.identity) return;
+    for (int k = 0; k < L.ncols; ++k) {
+        AggOutputCol& c = L.cols[k];
+        if (!c.valid) continue;
+        bool never_null;
+        if (k < p.nkeyparts) never_null = p.keys[k].null_shift == 0xFF;
+        else if (k - p.nkeyparts < p.naggs) never_null = p.aggs[k - p.nkeyparts].valid_state == 0xFF;
+        else never_null = false;
+        if (!never_null) continue;
+        cudaMemsetAsync(c.valid, 0xFF, size_t((rows + 31) / 32) * 4, s);
+        c.valid = nullptr;
+    }
+}
+
+// Copy plan of an identity output whose columns are all never NULL and are
+// each one slot word as stored: 64-bit keys unpacked from one word, and
+// COUNT / SUM / MIN / MAX of integers, SUM of doubles (bits as summed) and
+// 128-bit decimal sums.  `t` gives the slot layout.
+static void PlanCopy(const AggPlan& p, const OutputPlan& out, const GTableDev& t, FinLaunch& L) {
+    L.copy_n = 0;
+    if (!out.identity || t.wide || p.key_words != 1) return;
+    for (int k = 0; k < L.ncols; ++k) {
+        const AggOutputCol& c = L.cols[k];
+        if (c.valid || c.offsets) return;
+        const bool i64 = c.type == QDB_TYPE_I64 || c.type == QDB_TYPE_U64 || c.type == QDB_TYPE_DECIMAL64;
+        L.copy_two[k] = 0;
+        L.copy_key[k] = 0;
+        if (k < p.nkeyparts) {
+            const KeyPart& kp = p.keys[k];
+            if (kp.bits != 64 || kp.shift != 0 || kp.null_shift != 0xFF) return;
+            if (!(kp.is_float ? c.type == QDB_TYPE_F64 : i64)) return;
+            L.copy_word[k] = int8_t(t.key_off + kp.word);
+            L.copy_key[k] = 1;
+        } else if (k - p.nkeyparts < p.naggs) {
+            const AggOut& ao = p.aggs[k - p.nkeyparts];
+            const StateDesc& sd = p.states[ao.state];
+            if (ao.valid_state != 0xFF) return;
+            const int w = t.state_off + sd.word;
+            if (sd.kind == ST_COUNT || sd.kind == ST_SUM_I64 || sd.kind == ST_MIN_I64 || sd.kind == ST_MAX_I64) {
+                if (!i64) return;
+            } else if (sd.kind == ST_SUM_F64) {
+                if (c.type != QDB_TYPE_F64) return;
+            } else if (sd.kind == ST_SUM_I128) {
+                if (c.type != QDB_TYPE_DECIMAL128) return;
+                L.copy_two[k] = 1;
+            } else {
+                return;
+            }
+            if (w > 127) return;
+            L.copy_word[k] = int8_t(w);
+        } else {
+            return;
+        }
+    }
+    L.copy_n = L.ncols;
+}
+
 size_t AggFinalizeScratch(const GTableDev& t) {
     const int64_t blocks = (t.capacity + 1 + kFinChunk - 1) / kFinChunk;
     return size_t(blocks) * sizeof(unsigned long long);
@@ -2691,6 +2802,8 @@ void AggFinalize(const AggPlan& p, const OutputPlan& out, const GTableDev& t, Ag
     L.groups = groups;
     L.block_counts = static_cast<unsigned long long*>(scratch);
     L.err = err;
+    PresetValidity(p, out, L, groups, s);
+    PlanCopy(p, out, t, L);
     const int64_t blocks = (t.capacity + 1 + kFinChunk - 1) / kFinChunk;
     ProfileBegin(s, "agg_finalize", t.capacity);
     FinCountKernel<<<int(blocks), kFinThreads, 0, s>>>(L);
@@ -2817,9 +2930,9 @@ void AggBatchSpill(const AggPlan& p, const HighBatch& b, const uint64_t* recs, i
 
 size_t AggFinalizeBatchScratch(int64_t nblocks) { return size_t(std::max<int64_t>(nblocks, 1)) * 8; }
 
-void AggFinalizeBatch(const AggPlan& p, const OutputPlan& out, const GTableDev* tables, const FinBlock* blocks,
-                      int64_t nblocks, AggOutputCol* cols, int ncols, int64_t out_rows, void* scratch, int* err,
-                      cudaStream_t s) {
+void AggFinalizeBatch(const AggPlan& p, const OutputPlan& out, const GTableDev& layout, const GTableDev* tables,
+                      const FinBlock* blocks, int64_t nblocks, AggOutputCol* cols, int ncols, int64_t out_rows,
+                      void* scratch, int* err, cudaStream_t s) {
     if (nblocks <= 0) return;
     static thread_local FinLaunch* Lp = nullptr;
     if (!Lp) Lp = new FinLaunch();
@@ -2834,6 +2947,8 @@ void AggFinalizeBatch(const AggPlan& p, const OutputPlan& out, const GTableDev* 
     L.err = err;
     L.tables = tables;
     L.blocks = blocks;
+    PresetValidity(p, out, L, out_rows, s);
+    PlanCopy(p, out, layout, L);
     ProfileBegin(s, "agg_finalize_batch", nblocks);
     FinCountKernel<<<int(nblocks), kFinThreads, 0, s>>>(L);
     FinScanKernel<<<1, 1024, 0, s>>>(L.block_counts, nblocks);

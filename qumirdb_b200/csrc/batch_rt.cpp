@@ -384,13 +384,17 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
         }
         if (!ResolveColumns(plans[size_t(i)], lw.cols, prog->columns.data(), batches[i], stg)) return -1;
         rows[size_t(i)] = batches[i]->RowCount;
+        // The batched kernel is looked up once; later row sets of the same
+        // typed shape only compare their plans with the first.
         FastPlan fi{};
-        if (MatchFast(plans[size_t(i)], fi) && AggBatchSupported(plans[size_t(i)], fi)) {
-            if (!have_fast) {
+        if (MatchFast(plans[size_t(i)], fi)) {
+            if (have_fast) {
+                typed[size_t(i)] = std::memcmp(&fi, &fast, sizeof(FastPlan)) == 0 ? 1 : 0;
+            } else if (AggBatchSupported(plans[size_t(i)], fi)) {
                 fast = fi;
                 have_fast = true;
+                typed[size_t(i)] = 1;
             }
-            typed[size_t(i)] = std::memcmp(&fi, &fast, sizeof(FastPlan)) == 0 ? 1 : 0;
         }
     }
     // States outside the batched kernel (no compiled shape, nullable columns)
@@ -428,7 +432,7 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
         }
         fresh.push_back(int(k));
         const int64_t est = BatchEstimateGroups(shape, rows[size_t(i)], prog->expected_groups);
-        caps[size_t(k)] = std::max<int64_t>(1024, NextPow2(2 * est));
+        caps[size_t(k)] = std::max<int64_t>(1024, NextPow2(est + est / 4));
     }
     std::vector<HighTask> tasks(static_cast<size_t>(m));
     AggArena* arena = nullptr;
@@ -671,7 +675,9 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
         for (int64_t k = 0; k < m; ++k) {
             const int i = members[size_t(k)];
             AggTableState* st = StateOf(hts[i]);
-            if (st->groups * 2 > st->t.capacity && !Grow(st, lw.plan, st->groups)) return -1;
+            // Batch tables run fuller than one-state tables (sized from the
+            // learned ratio): grown past 85% load.
+            if (st->groups * 20 > st->t.capacity * 17 && !Grow(st, lw.plan, st->groups)) return -1;
             MirrorHeader(hts[i], st, lw.plan);
             if (rows[size_t(i)] >= 1024) {
                 const double r = double(st->groups) / double(rows[size_t(i)]);
@@ -750,8 +756,8 @@ int64_t qdb_gpu_agg_finish_batch(const qdb_gpu_program* prog, void* const* hts, 
     cudaMemcpyAsync(d_blocks, blocks.data(), blocks.size() * sizeof(FinBlock), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d_tables, tables.data(), tables.size() * sizeof(GTableDev), cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(d_err, 0, sizeof(int), s);
-    AggFinalizeBatch(lw.plan, lw.out, d_tables, d_blocks, nblocks, cols.data(), int(cols.size()), out_rows, dev,
-                     d_err, s);
+    AggFinalizeBatch(lw.plan, lw.out, tables[0], d_tables, d_blocks, nblocks, cols.data(), int(cols.size()),
+                     out_rows, dev, d_err, s);
     int herr = 0;
     cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (!CudaOk(cudaStreamSynchronize(s), "batched finalize")) return -1;
@@ -822,6 +828,12 @@ int64_t qdb_gpu_agg_finish_batch(const qdb_gpu_program* prog, void* const* hts, 
         std::memset(hts[i], 0, QDB_HASH_TABLE_SIZE);
     }
     return total;
+}
+
+void qdb_gpu_release_rowsets(qdb_rowset* rs, int64_t n) {
+    for (int64_t i = 0; rs && i < n; ++i) {
+        if (rs[i].Destroy) rs[i].Destroy(&rs[i]);
+    }
 }
 
 int64_t qdb_gpu_autotune_info(char* buf, int64_t cap) {

@@ -264,9 +264,10 @@ struct FinBlock {
 };
 constexpr int64_t kFinChunkSlots = 4096;
 size_t AggFinalizeBatchScratch(int64_t nblocks);
-void AggFinalizeBatch(const AggPlan& p, const OutputPlan& out, const GTableDev* tables, const FinBlock* blocks,
-                      int64_t nblocks, AggOutputCol* cols, int ncols, int64_t out_rows, void* scratch, int* err,
-                      cudaStream_t s);
+// `layout`: any of the tables (all share one slot layout).
+void AggFinalizeBatch(const AggPlan& p, const OutputPlan& out, const GTableDev& layout, const GTableDev* tables,
+                      const FinBlock* blocks, int64_t nblocks, AggOutputCol* cols, int ncols, int64_t out_rows,
+                      void* scratch, int* err, cudaStream_t s);
 
 // Kernel timing hooks (runtime.cpp).
 bool ProfileOn();

@@ -160,9 +160,45 @@ bool IsDevicePtr(const void* p) {
 }
 
 // Device copy of `bytes` at `p` (host or device); adds owned buffers to st.
+namespace {
+
+// cuMemGetAddressRange through the runtime's driver entry point (no link
+// against the driver library).
+using AddrRangeFn = int (*)(unsigned long long*, size_t*, unsigned long long);
+
+AddrRangeFn AddrRange() {
+    static AddrRangeFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return AddrRangeFn(nullptr);
+        }
+        return reinterpret_cast<AddrRangeFn>(f);
+    }();
+    return fn;
+}
+
+}  // namespace
+
 const void* Staging::Device(const void* p, size_t bytes) {
     if (!p) return nullptr;
-    if (IsDevicePtr(p)) return p;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    for (const auto& r : dev_ranges) {
+        if (a >= r.first && a + bytes <= r.second) return p;
+    }
+    if (IsDevicePtr(p)) {
+        unsigned long long base = 0;
+        size_t size = 0;
+        if (AddrRangeFn fn = AddrRange()) {
+            if (fn(&base, &size, static_cast<unsigned long long>(a)) == 0 && size) {
+                if (dev_ranges.size() >= 16) dev_ranges.erase(dev_ranges.begin());
+                dev_ranges.emplace_back(uintptr_t(base), uintptr_t(base) + size);
+            }
+        }
+        return p;
+    }
     void* d = DevAlloc(bytes, s);
     if (!d) return nullptr;
     cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, s);

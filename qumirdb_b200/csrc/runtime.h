@@ -31,6 +31,9 @@ struct Staging {
     const void* Device(const void* p, size_t bytes);
     cudaStream_t s;
     std::vector<void*> owned;
+    // Device allocations met during this call: a pointer inside one needs no
+    // driver query (many row sets of a batch slice the same columns).
+    std::vector<std::pair<uintptr_t, uintptr_t>> dev_ranges;
 };
 
 bool ResolveColumns(AggPlan& P, const ColumnMap& cm, const qdb_column_type* types, const qdb_rowset* rs,
