@@ -360,6 +360,12 @@ class Aggregate:
     def groups(self) -> int:
         return C.cast(self.ht, C.POINTER(C.c_int64))[9]
 
+    def expect_groups(self, n: int) -> None:
+        """The planner's group estimate (agg_dispatch ExpectRowGroups): the
+        table is sized for it up front."""
+        if lib().qdb_gpu_agg_dispatch(self.prog.handle, self.ht, None, n, abi.AGG_EXPECT_ROW_GROUPS) == 0:
+            raise QdbError(f"aggregate ExpectRowGroups failed: {last_error()}")
+
     def add(self, rowset) -> int:
         r = lib().qdb_gpu_agg_dispatch(self.prog.handle, self.ht, rowset.ptr, 0, abi.AGG_UPDATE)
         if r < 0:

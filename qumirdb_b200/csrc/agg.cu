@@ -2848,8 +2848,10 @@ BatchFns FindBatchKernels(const AggPlan& P, const FastPlan& F) {
         b.update = AggHighBatchKernel<__VA_ARGS__>;                                   \
         b.replay = AggBatchReplayKernel<__VA_ARGS__>;                                 \
     }
+    // High-cardinality shapes only: the few groups of a low-cardinality
+    // program would pile every row's atomics onto a handful of shared slots;
+    // its states take the one-state path (lane-private accumulators).
     QDB_HIGH_SHAPE_LIST(QDB_SHAPE_FIND)
-    QDB_SHAPE_LIST(QDB_SHAPE_FIND)
 #undef QDB_SHAPE_FIND
     return b;
 }

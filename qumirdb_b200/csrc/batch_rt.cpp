@@ -46,6 +46,8 @@ struct BatchConfig {
     int64_t chunk_rows = int64_t(1) << 17;
 };
 
+constexpr int64_t kTuneMinRows = int64_t(16) << 20;   // rows in a batch worth a search
+
 int SizeClass(int64_t rows) {
     int c = 0;
     while (c < 40 && (int64_t(1) << (c + 1)) <= rows) ++c;
@@ -87,9 +89,12 @@ struct BatchContext {
     unsigned long long* h_new = nullptr;
     BatchCounters* h_counters = nullptr;
     cudaStream_t s = nullptr;
-    // Graph of the launch sequence and the key it was captured for.
+    // Graph of the launch sequence and the key it was captured for; a key is
+    // captured the second time in a row it comes (a one-off batch runs
+    // eagerly).
     cudaGraphExec_t exec = nullptr;
     std::string graph_key;
+    std::string last_key;
     int64_t graph_launches = 0;
     int64_t graph_replays = 0;
 
@@ -340,7 +345,7 @@ struct BatchOutputs {
     std::vector<void*> host;
     cudaStream_t s = nullptr;
     ~BatchOutputs() {
-        for (void* p : host) std::free(p);
+        for (void* p : host) HostOutFree(p);
         for (void* p : dev) DevFree(p, s);
     }
 };
@@ -504,12 +509,29 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
     for (int64_t r : rows) total_rows += r;
     const int rows_class = SizeClass(total_rows / std::max<int64_t>(m, 1));
     const int states_class = SizeClass(m);
+    // Batches too small to pay for a search run the defaults.
+    const bool worth_tuning = total_rows >= kTuneMinRows;
+    // A stored choice for this shape and size class; else the choice of the
+    // nearest size class of the shape (a search costs tens of launches, so
+    // a shape is searched once and its later batches, of whatever mix, reuse
+    // the nearest choice); a shape never searched is searched now.
     BatchConfig cfg;
     bool found = false;
     {
         Tuner& tn = Tune();
         std::lock_guard<std::mutex> lk(tn.mu);
         auto it = tn.best.find({shape, rows_class, states_class});
+        if (it == tn.best.end()) {
+            int best_d = 1 << 30;
+            for (auto j = tn.best.begin(); j != tn.best.end(); ++j) {
+                if (std::get<0>(j->first) != shape) continue;
+                const int d = std::abs(std::get<1>(j->first) - rows_class) * 4 + std::abs(std::get<2>(j->first) - states_class);
+                if (d < best_d) {
+                    best_d = d;
+                    it = j;
+                }
+            }
+        }
         if (it != tn.best.end()) {
             cfg = it->second;
             found = true;
@@ -517,7 +539,7 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
         }
     }
     BatchContext& cx = Ctx();
-    if (!found && TuningEnabled()) {
+    if (!found && TuningEnabled() && worth_tuning) {
         // Fresh tables must be initialised before the search reuses the
         // context's device buffers; it runs on scratch tables of its own.
         cfg = Search(P0, fast, tasks, caps, s);
@@ -570,7 +592,9 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
     };
     const std::string gkey = ConfigKey(shape, m, nitems, cfg, cx);
     bool ran = false;
-    if (!ProfileOn() && s != nullptr) {
+    const bool repeat = gkey == cx.last_key;
+    cx.last_key = gkey;
+    if (!ProfileOn() && s != nullptr && (repeat || (cx.exec && cx.graph_key == gkey))) {
         if (cx.exec && cx.graph_key != gkey) {
             cudaGraphExecDestroy(cx.exec);
             cx.exec = nullptr;
@@ -781,17 +805,17 @@ int64_t qdb_gpu_agg_finish_batch(const qdb_gpu_program* prog, void* const* hts, 
         for (size_t k = 0; k < cols.size(); ++k) {
             const size_t w = size_t(StorageWidth(types[k]));
             const size_t db = size_t(std::max<int64_t>(out_rows, 1)) * w;
-            base[k] = static_cast<char*>(std::malloc(db));
+            base[k] = static_cast<char*>(HostOutAlloc(db));
             host->host.push_back(base[k]);
             cudaMemcpyAsync(base[k], cols[k].data, db, cudaMemcpyDeviceToHost, s);
             if (cols[k].valid) {
                 const size_t mb = size_t((out_rows + 31) / 32) * 4 + 4;
-                vbase[k] = static_cast<uint32_t*>(std::malloc(mb));
+                vbase[k] = static_cast<uint32_t*>(HostOutAlloc(mb));
                 host->host.push_back(vbase[k]);
                 cudaMemcpyAsync(vbase[k], cols[k].valid, mb - 4, cudaMemcpyDeviceToHost, s);
             }
             if (cols[k].offsets) {
-                obase[k] = static_cast<int32_t*>(std::malloc(size_t(out_rows + 1) * 4));
+                obase[k] = static_cast<int32_t*>(HostOutAlloc(size_t(out_rows + 1) * 4));
                 host->host.push_back(obase[k]);
                 cudaMemcpyAsync(obase[k], cols[k].offsets, size_t(out_rows + 1) * 4, cudaMemcpyDeviceToHost, s);
             }

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -75,6 +76,12 @@ cudaStream_t CurStream() {
         if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
             uint64_t threshold = UINT64_MAX;
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+            // Memory freed on one stream is not handed to another stream's
+            // allocation with a wait on the first stream's work behind it:
+            // concurrent queries on their own streams must not serialise
+            // through the pool (it grows instead).
+            int no = 0;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
         }
     }
     return g_lib_stream;
@@ -141,6 +148,53 @@ AggCounters* PinnedCountersGet() {
     AggCounters* c = g_pin_free.back();
     g_pin_free.pop_back();
     return c;
+}
+
+namespace {
+
+std::mutex g_host_mu;
+std::vector<std::vector<void*>> g_host_free(64);     // by power-of-two size class
+std::vector<std::pair<void*, int>> g_host_class;     // live buffer -> class (sorted by address)
+
+int HostClass(size_t bytes) {
+    int c = 16;   // 64 KiB and up
+    while (c < 63 && (size_t(1) << c) < bytes) ++c;
+    return c;
+}
+
+}  // namespace
+
+void* HostOutAlloc(size_t bytes) {
+    const int c = HostClass(std::max<size_t>(bytes, 1));
+    std::lock_guard<std::mutex> lk(g_host_mu);
+    void* p = nullptr;
+    if (!g_host_free[size_t(c)].empty()) {
+        p = g_host_free[size_t(c)].back();
+        g_host_free[size_t(c)].pop_back();
+    } else if (cudaMallocHost(&p, size_t(1) << c) != cudaSuccess) {
+        cudaGetLastError();
+        p = std::malloc(size_t(1) << c);   // pageable when pinned memory runs out
+        if (!p) return nullptr;
+        g_host_class.insert(std::upper_bound(g_host_class.begin(), g_host_class.end(), std::make_pair(p, -1)),
+                            std::make_pair(p, -c));
+        return p;
+    }
+    auto it = std::lower_bound(g_host_class.begin(), g_host_class.end(), std::make_pair(p, INT32_MIN));
+    if (it == g_host_class.end() || it->first != p) g_host_class.insert(it, std::make_pair(p, c));
+    return p;
+}
+
+void HostOutFree(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_host_mu);
+    auto it = std::lower_bound(g_host_class.begin(), g_host_class.end(), std::make_pair(p, INT32_MIN));
+    if (it == g_host_class.end() || it->first != p) return;
+    if (it->second < 0) {   // pageable fallback
+        std::free(p);
+        g_host_class.erase(it);
+        return;
+    }
+    g_host_free[size_t(it->second)].push_back(p);
 }
 
 void PinnedCountersPut(AggCounters* c) {
@@ -426,9 +480,30 @@ bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyP
     const bool priv = plan.nkeyparts == 0 || (st->expected > 0 && st->expected <= 64);
     FastPlan fast;
     const bool use_fast = jk == nullptr && MatchFast(plan, fast);
-    for (int64_t begin = 0; begin < rows || (rows == 0 && begin == 0); begin += kChunkRows) {
-        const int64_t n = std::min<int64_t>(kChunkRows, rows - begin);
-        if (n <= 0) break;
+    // The table is grown before a chunk that could overfill it (a full
+    // table turns every new group's rows into replays): the chunk's new
+    // groups are projected from the groups per row this call has seen so
+    // far, or, with no planner hint, from a first chunk of kProbeRows rows
+    // that the table is grown to hold whole.
+    constexpr int64_t kProbeRows = int64_t(1) << 20;
+    int64_t seen_rows = 0, seen_groups = 0;
+    for (int64_t begin = 0, n = 0; begin < rows; begin += n) {
+        n = std::min<int64_t>(kChunkRows, rows - begin);
+        if (plan.nkeyparts > 0 && jk == nullptr) {
+            int64_t add;
+            if (seen_rows > 0) {
+                const double r = double(seen_groups) / double(seen_rows);
+                add = std::min<int64_t>(n, int64_t(std::ceil(r * 1.25 * double(n))) + 1024);
+            } else if (st->expected > 0) {
+                add = std::min<int64_t>(n, std::max<int64_t>(0, st->expected - st->groups));
+            } else {
+                n = std::min<int64_t>(n, kProbeRows);
+                add = n;
+            }
+            if (double(st->groups + add) > 0.85 * double(st->t.capacity) && !Grow(st, plan, st->groups + add))
+                return false;
+        }
+        const int64_t groups_before = st->groups;
         const AggPlan chunk = OffsetPlan(plan, begin);
         AggUpdateArgs a;
         a.plan = &chunk;
@@ -454,6 +529,8 @@ bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyP
         st->groups += int64_t(st->hc->new_groups);
         st->matched += int64_t(st->hc->matched);
         if (!AggReplay(st, plan, a, int64_t(st->hc->deferred), int64_t(st->hc->spilled))) return false;
+        seen_rows += n;
+        seen_groups += st->groups - groups_before;
     }
     return true;
 }
@@ -506,7 +583,7 @@ struct OwnedRowset {
 void DestroyOwned(qdb_rowset* rs) {
     if (!rs || !rs->Private) return;
     auto* o = static_cast<OwnedRowset*>(rs->Private);
-    for (void* p : o->host) std::free(p);
+    for (void* p : o->host) HostOutFree(p);
     for (void* p : o->dev) DevFree(p, o->s);
     delete o;
     rs->Private = nullptr;
@@ -538,18 +615,18 @@ bool EmitRowset(std::vector<AggOutputCol>& cols, const std::vector<int>& types, 
                 o->dev.push_back(cols[k].offsets);
             }
         } else {
-            void* h = std::malloc(dbytes);
+            void* h = HostOutAlloc(dbytes);
             cudaMemcpyAsync(h, cols[k].data, size_t(rows) * w, cudaMemcpyDeviceToHost, s);
             c.Data = static_cast<char*>(h);
             o->host.push_back(h);
             if (cols[k].valid) {
-                void* m = std::malloc(std::max<size_t>(4, mbytes));
+                void* m = HostOutAlloc(std::max<size_t>(4, mbytes));
                 cudaMemcpyAsync(m, cols[k].valid, mbytes, cudaMemcpyDeviceToHost, s);
                 c.Mask = static_cast<const uint8_t*>(m);
                 o->host.push_back(m);
             }
             if (cols[k].offsets) {
-                void* off = std::malloc(size_t(rows + 1) * 4);
+                void* off = HostOutAlloc(size_t(rows + 1) * 4);
                 cudaMemcpyAsync(off, cols[k].offsets, size_t(rows + 1) * 4, cudaMemcpyDeviceToHost, s);
                 c.Offsets = off;
                 c.OffsetWidth = 4;
@@ -560,7 +637,7 @@ bool EmitRowset(std::vector<AggOutputCol>& cols, const std::vector<int>& types, 
     // The host copies have landed once the stream drains; only then do the
     // device buffers go back to the pool.
     if (!CudaOk(cudaStreamSynchronize(s), "output")) {
-        for (void* p : o->host) std::free(p);
+        for (void* p : o->host) HostOutFree(p);
         delete o;
         return false;
     }

@@ -20,6 +20,10 @@ void* DevAlloc(size_t bytes, cudaStream_t s);
 void DevFree(void* p, cudaStream_t s);
 struct AggCounters;
 AggCounters* PinnedCountersGet();
+// Host output buffers: pinned (page-locked) memory from a size-class pool,
+// so output copies run at full link speed; returned to the pool on free.
+void* HostOutAlloc(size_t bytes);
+void HostOutFree(void* p);
 void PinnedCountersPut(AggCounters* c);
 bool IsDevicePtr(const void* p);
 int64_t NextPow2(int64_t v);

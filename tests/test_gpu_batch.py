@@ -83,7 +83,9 @@ def test_batch_matches_each_aggregate_alone(flags):
 
 def test_batch_autotune_and_graph_replay():
     q.autotune_reset()
-    sizes = [50_000, 3000, 20_000, 700, 120_000, 9000, 40_000, 1500] * 4
+    # 23M rows: big enough for the autotuner to search (small batches run
+    # the defaults).
+    sizes = [2_000_000, 100_000, 800_000, 30_000, 1_500_000, 300_000, 1_000_000, 50_000] * 4
     parts = partitions(2, sizes, 30_000)
     prog = q.compile_aggregate(queries.zipf_agg(flags=abi.OUT_DEVICE))
     types = queries.ZIPF_OUT_TYPES
