@@ -1686,9 +1686,33 @@ __device__ __forceinline__ void HighRows(const AggPlan& P, const FastPlan& F, co
     }
 }
 
-// Shared tier -> global table (spilling what the global table cannot take),
-// then clears the tier for the next range.  Called by the whole CTA.
-__device__ __forceinline__ void HighFlush(const AggPlan& P, const HighDst& D, const HighSmem& sm, bool reset) {
+// Typed flush of the shared tier: every occupied slot's states (each
+// updated by every row of its key, so none is at its identity) go to the
+// global table as the shape's own atomics; with `reset` the tier is cleared
+// to the shape's identities for the next range.
+template <class SH, int S = 0>
+__device__ __forceinline__ void ShapeReadSlot(ShapeVals<SH>& v, const HighSmem& sm, int i) {
+    if constexpr (S < SH::n) {
+        constexpr int O = SH::off(S);
+        v.lo[S] = sm.st[int64_t(O) * sm.S + i];
+        v.hi[S] = SH::width(S) == 2 ? sm.st[int64_t(O + 1) * sm.S + i] : 0;
+        ShapeReadSlot<SH, S + 1>(v, sm, i);
+    }
+}
+
+template <class SH, int S = 0>
+__device__ __forceinline__ void ShapeClearSlot(const HighSmem& sm, int i) {
+    if constexpr (S < SH::n) {
+        constexpr int K = SH::kind(S);
+        constexpr int O = SH::off(S);
+        sm.st[int64_t(O) * sm.S + i] = K == SK_MIN64 ? uint64_t(INT64_MAX) : K == SK_MAX64 ? uint64_t(INT64_MIN) : 0;
+        if constexpr (SH::width(S) == 2) sm.st[int64_t(O + 1) * sm.S + i] = 0;
+        ShapeClearSlot<SH, S + 1>(sm, i);
+    }
+}
+
+template <class SH>
+__device__ __forceinline__ void ShapeFlush(const AggPlan& P, const HighDst& D, const HighSmem& sm, bool reset) {
     const int rec_words = 1 + P.state_words + (D.tag >= 0 ? 1 : 0);
     for (int i = threadIdx.x; i < sm.S; i += blockDim.x) {
         const uint64_t key = sm.keys[i];
@@ -1707,24 +1731,13 @@ __device__ __forceinline__ void HighFlush(const AggPlan& P, const HighDst& D, co
                 if (D.tag >= 0) rec[1 + P.state_words] = uint64_t(D.tag);
             }
         } else {
-            uint64_t* gbase = D.T.slots + g * D.T.slot_words + D.T.state_off;
-            for (int st2 = 0; st2 < P.nstates; ++st2) {
-                const StateDesc sd = P.states[st2];
-                const uint64_t lo = sm.st[int64_t(sd.word) * sm.S + i];
-                const uint64_t hi = sd.kind == ST_SUM_I128 ? sm.st[int64_t(sd.word + 1) * sm.S + i] : 0;
-                if (IsIdentity(sd.kind, lo, hi)) continue;
-                double f;
-                __builtin_memcpy(&f, &lo, 8);
-                ApplyState(gbase + sd.word, gbase + sd.word + 1, sd.kind, lo, hi, f);
-            }
+            ShapeVals<SH> v;
+            ShapeReadSlot<SH>(v, sm, i);
+            ShapeAtomics<SH>(D.T.slots + g * D.T.slot_words + D.T.state_off, 1, v);
         }
         if (reset) {
             sm.keys[i] = kEmptyKey;
-            for (int s = 0; s < P.nstates; ++s) {
-                const StateDesc sd = P.states[s];
-                sm.st[int64_t(sd.word) * sm.S + i] = StateIdentity(sd.kind);
-                if (sd.kind == ST_SUM_I128) sm.st[int64_t(sd.word + 1) * sm.S + i] = 0;
-            }
+            ShapeClearSlot<SH>(sm, i);
         }
     }
 }
@@ -1785,7 +1798,7 @@ __global__ void __launch_bounds__(kHighThreads, 1) AggHighKernel(const __grid_co
     const HighDst D = HighDstOf(L);
     HighRows<SH>(L.P, L.F, D, sm, cb, sel, n, row0, threadIdx.x >> 5, blockDim.x >> 5);
     __syncthreads();
-    HighFlush(L.P, D, sm, false);
+    ShapeFlush<SH>(L.P, D, sm, false);
     __syncthreads();
     if (threadIdx.x == 0 && sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
 }
@@ -1834,7 +1847,7 @@ __global__ void __launch_bounds__(kHighThreads, 1) AggHighBatchKernel(const __gr
         const uint8_t* sel = tk.sel ? tk.sel + item.row0 : nullptr;
         HighRows<SH>(L.P, L.F, D, sm, cb, sel, item.nrows, item.row0, threadIdx.x >> 5, blockDim.x >> 5);
         __syncthreads();
-        HighFlush(L.P, D, sm, true);
+        ShapeFlush<SH>(L.P, D, sm, true);
         __syncthreads();
         if (threadIdx.x == 0) {
             if (sm.fresh[0]) atomicAdd(&B.new_groups[item.task], (unsigned long long)sm.fresh[0]);
@@ -2082,7 +2095,7 @@ struct FinLaunch {
     AggOutputCol cols[kMaxCols + kMaxAggs];
     int32_t ncols;
     int64_t groups;
-    unsigned long long* block_counts;
+    unsigned long long* row_counters;   // per aggregate: output rows claimed so far
     int* err;
     // Batched finalize: block b covers chunk blocks[b].chunk of table
     // tables[blocks[b].task] (nullptr: one table, T).
@@ -2098,14 +2111,16 @@ struct FinLaunch {
 
 // The table and slot range of a finalize block.
 __device__ __forceinline__ GTableDev FinBlockTable(const FinLaunch& L, int64_t& begin, int64_t& end, int64_t& delta,
-                                                   int64_t& slice0) {
+                                                   int64_t& slice0, int& task) {
     GTableDev T = L.T;
     int64_t chunk = blockIdx.x;
     delta = 0;
     slice0 = -1;
+    task = 0;
     if (L.blocks) {
         const FinBlock fb = L.blocks[blockIdx.x];
         T = L.tables[fb.task];
+        task = fb.task;
         chunk = fb.chunk;
         delta = fb.delta;
         slice0 = fb.slice0;
@@ -2120,19 +2135,6 @@ __device__ __forceinline__ bool SlotOccupied(const GTableDev& T, int64_t i) {
     if (T.wide) return i < T.capacity && s[0] == 2;
     if (i == T.capacity) return s[T.key_off] != 0;
     return s[T.key_off] != kEmptyKey;
-}
-
-__global__ void __launch_bounds__(kFinThreads) FinCountKernel(const __grid_constant__ FinLaunch L) {
-    __shared__ unsigned cnt;
-    if (threadIdx.x == 0) cnt = 0;
-    __syncthreads();
-    int64_t begin, end, delta, slice0;
-    const GTableDev T = FinBlockTable(L, begin, end, delta, slice0);
-    unsigned local = 0;
-    for (int64_t i = begin + threadIdx.x; i < end; i += blockDim.x) local += SlotOccupied(T, i) ? 1 : 0;
-    atomicAdd(&cnt, local);
-    __syncthreads();
-    if (threadIdx.x == 0) L.block_counts[blockIdx.x] = cnt;
 }
 
 __global__ void __launch_bounds__(1024) FinScanKernel(unsigned long long* counts, int64_t n) {
@@ -2216,33 +2218,65 @@ __device__ __forceinline__ void StoreValue(const AggOutputCol& col, int64_t row,
     }
 }
 
-__global__ void __launch_bounds__(kFinThreads) FinWriteKernel(const __grid_constant__ FinLaunch L) {
-    __shared__ unsigned warp_off[kFinThreads / 32];
-    __shared__ unsigned running;
-    const AggPlan& P = L.P;
-    const OutputPlan& O = L.O;
-    if (threadIdx.x == 0) running = 0;
-    __syncthreads();
+// The copy-plan finalize: the same one-pass row claiming as FinWriteKernel,
+// each output column one (or two) slot words as stored.  Kept apart from the
+// general kernel so that its few registers leave room for many warps, the
+// only way a pass bound by dependent loads and row claims fills HBM.
+__global__ void __launch_bounds__(kFinThreads) FinCopyKernel(const __grid_constant__ FinLaunch L) {
     int64_t begin, end, delta, slice0;
-    const GTableDev T = FinBlockTable(L, begin, end, delta, slice0);
-    const unsigned long long block_off = L.block_counts[blockIdx.x] + uint64_t(delta);
-    for (int64_t b = begin; b < end; b += blockDim.x) {
-        const int64_t i = b + threadIdx.x;
+    int task = 0;
+    const GTableDev T = FinBlockTable(L, begin, end, delta, slice0, task);
+    const int64_t row_base = slice0 < 0 ? 0 : slice0;
+    const int lane = LaneId();
+    for (int64_t b = begin + (threadIdx.x & ~31); b < end; b += blockDim.x) {
+        const int64_t i = b + lane;
         const bool occ = i < end && SlotOccupied(T, i);
         const unsigned m = __ballot_sync(kFull, occ);
-        if (LaneId() == 0) warp_off[threadIdx.x >> 5] = __popc(m);
-        __syncthreads();
-        unsigned before = running;
-        for (int w = 0; w < int(threadIdx.x >> 5); ++w) before += warp_off[w];
-        before += __popc(m & ((1u << LaneId()) - 1));
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) {
-            unsigned tot = 0;
-            for (int w = 0; w < kFinThreads / 32; ++w) tot += warp_off[w];
-            running += tot;
+        if (!m) continue;
+        unsigned long long first = 0;
+        if (lane == 0) first = atomicAdd(&L.row_counters[task], (unsigned long long)__popc(m));
+        first = __shfl_sync(kFull, first, 0);
+        if (!occ) continue;
+        const int64_t row = row_base + int64_t(first) + __popc(m & ((1u << lane) - 1));
+        if (row >= L.groups) continue;
+        const uint64_t* s = T.slots + i * T.slot_words;
+        const bool flag_slot = !T.wide && i == T.capacity;
+        for (int k = 0; k < L.copy_n; ++k) {
+            uint64_t* dst = reinterpret_cast<uint64_t*>(L.cols[k].data);
+            const int w = L.copy_word[k];
+            if (L.copy_two[k]) {
+                dst[2 * row] = s[w];
+                dst[2 * row + 1] = s[w + 1];
+            } else {
+                dst[row] = (L.copy_key[k] && flag_slot) ? kEmptyKey : s[w];
+            }
         }
+    }
+}
+
+// One pass over the table: each warp takes 32 consecutive slots at a time
+// and claims output rows for its occupied ones with one atomic on the
+// aggregate's row counter (groups come out in no particular order: an
+// aggregate's output is a set of groups).
+__global__ void __launch_bounds__(kFinThreads) FinWriteKernel(const __grid_constant__ FinLaunch L) {
+    const AggPlan& P = L.P;
+    const OutputPlan& O = L.O;
+    int64_t begin, end, delta, slice0;
+    int task = 0;
+    const GTableDev T = FinBlockTable(L, begin, end, delta, slice0, task);
+    const int64_t row_base = slice0 < 0 ? 0 : slice0;
+    const int lane = LaneId();
+    for (int64_t b = begin + (threadIdx.x & ~31); b < end; b += blockDim.x) {
+        const int64_t i = b + lane;
+        const bool occ = i < end && SlotOccupied(T, i);
+        const unsigned m = __ballot_sync(kFull, occ);
+        if (!m) continue;
+        unsigned long long first = 0;
+        if (lane == 0) first = atomicAdd(&L.row_counters[task], (unsigned long long)__popc(m));
+        first = __shfl_sync(kFull, first, 0);
+        const int64_t before = int64_t(first) + __popc(m & ((1u << lane) - 1));
         if (occ && L.copy_n) {
-            const int64_t row = int64_t(block_off) + before;
+            const int64_t row = row_base + before;
             if (row < L.groups) {
                 const uint64_t* s = T.slots + i * T.slot_words;
                 const bool flag_slot = !T.wide && i == T.capacity;
@@ -2258,7 +2292,7 @@ __global__ void __launch_bounds__(kFinThreads) FinWriteKernel(const __grid_const
                 }
             }
         } else if (occ) {
-            const int64_t row = int64_t(block_off) + before;
+            const int64_t row = row_base + before;
             if (row < L.groups) {
                 const uint64_t* s = T.slots + i * T.slot_words;
                 uint64_t kw[kMaxKeyWords];
@@ -2322,7 +2356,6 @@ __global__ void __launch_bounds__(kFinThreads) FinWriteKernel(const __grid_const
                 }
             }
         }
-        __syncthreads();
     }
 }
 
@@ -2783,10 +2816,7 @@ static void PlanCopy(const AggPlan& p, const OutputPlan& out, const GTableDev& t
     L.copy_n = L.ncols;
 }
 
-size_t AggFinalizeScratch(const GTableDev& t) {
-    const int64_t blocks = (t.capacity + 1 + kFinChunk - 1) / kFinChunk;
-    return size_t(blocks) * sizeof(unsigned long long);
-}
+size_t AggFinalizeScratch(const GTableDev&) { return sizeof(unsigned long long); }
 
 void AggFinalize(const AggPlan& p, const OutputPlan& out, const GTableDev& t, AggOutputCol* cols, int ncols,
                  int64_t groups, void* scratch, int* err, cudaStream_t s) {
@@ -2800,17 +2830,17 @@ void AggFinalize(const AggPlan& p, const OutputPlan& out, const GTableDev& t, Ag
     for (int k = 0; k < ncols; ++k) L.cols[k] = cols[k];
     L.ncols = ncols;
     L.groups = groups;
-    L.block_counts = static_cast<unsigned long long*>(scratch);
+    L.row_counters = static_cast<unsigned long long*>(scratch);
     L.err = err;
     PresetValidity(p, out, L, groups, s);
     PlanCopy(p, out, t, L);
     const int64_t blocks = (t.capacity + 1 + kFinChunk - 1) / kFinChunk;
+    cudaMemsetAsync(L.row_counters, 0, sizeof(unsigned long long), s);
     ProfileBegin(s, "agg_finalize", t.capacity);
-    FinCountKernel<<<int(blocks), kFinThreads, 0, s>>>(L);
-    FinScanKernel<<<1, 1024, 0, s>>>(L.block_counts, blocks);
-    FinWriteKernel<<<int(blocks), kFinThreads, 0, s>>>(L);
+    if (L.copy_n) FinCopyKernel<<<int(blocks), kFinThreads, 0, s>>>(L);
+    else FinWriteKernel<<<int(blocks), kFinThreads, 0, s>>>(L);
     ProfileEnd(s);
-    CountLaunch(3);
+    CountLaunch(1);
 }
 
 // ---------------------------------------------------------------------------
@@ -2945,18 +2975,18 @@ void AggFinalizeBatch(const AggPlan& p, const OutputPlan& out, const GTableDev& 
     for (int k = 0; k < ncols; ++k) L.cols[k] = cols[k];
     L.ncols = ncols;
     L.groups = out_rows;
-    L.block_counts = static_cast<unsigned long long*>(scratch);
+    L.row_counters = static_cast<unsigned long long*>(scratch);
     L.err = err;
     L.tables = tables;
     L.blocks = blocks;
     PresetValidity(p, out, L, out_rows, s);
     PlanCopy(p, out, layout, L);
+    cudaMemsetAsync(L.row_counters, 0, AggFinalizeBatchScratch(nblocks), s);
     ProfileBegin(s, "agg_finalize_batch", nblocks);
-    FinCountKernel<<<int(nblocks), kFinThreads, 0, s>>>(L);
-    FinScanKernel<<<1, 1024, 0, s>>>(L.block_counts, nblocks);
-    FinWriteKernel<<<int(nblocks), kFinThreads, 0, s>>>(L);
+    if (L.copy_n) FinCopyKernel<<<int(nblocks), kFinThreads, 0, s>>>(L);
+    else FinWriteKernel<<<int(nblocks), kFinThreads, 0, s>>>(L);
     ProfileEnd(s);
-    CountLaunch(3);
+    CountLaunch(1);
 }
 
 // ---------------------------------------------------------------------------

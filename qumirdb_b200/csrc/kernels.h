@@ -254,8 +254,8 @@ void AggBatchSpill(const AggPlan& p, const HighBatch& b, const uint64_t* recs, i
 void AggBatchInitTables(const AggPlan& p, const GTableDev& all, const HighTask* tasks, int ntasks,
                         cudaStream_t s);
 // Batched finalize: block b covers slots [chunk * kFinChunkSlots, ...) of
-// table `task`; its groups land at output row (scan of the block counts) +
-// delta, in the task's output slice that starts at row slice0.
+// table `task`; its groups land in the task's output slice that starts at
+// row slice0 (delta: unused, kept for the descriptor's layout).
 struct FinBlock {
     int32_t task;
     int32_t chunk;
@@ -263,6 +263,7 @@ struct FinBlock {
     int64_t slice0;
 };
 constexpr int64_t kFinChunkSlots = 4096;
+// Per-aggregate row counters: at least one word per aggregate.
 size_t AggFinalizeBatchScratch(int64_t nblocks);
 // `layout`: any of the tables (all share one slot layout).
 void AggFinalizeBatch(const AggPlan& p, const OutputPlan& out, const GTableDev& layout, const GTableDev* tables,
