@@ -297,7 +297,7 @@ def zipf_batched_operator(q, peak):
     drs = q.DeviceRowSet(cols)
     del cols
     bounds = np.concatenate([[0], np.cumsum(sizes)])
-    parts = [q.SliceRowSet(drs, int(lo), int(hi)) for lo, hi in zip(bounds[:-1], bounds[1:])]
+    parts = q.RowSetPointers([q.SliceRowSet(drs, int(lo), int(hi)) for lo, hi in zip(bounds[:-1], bounds[1:])])
     groups = []
 
     def step():
@@ -558,7 +558,7 @@ def profile_case(name: str, rows: int) -> None:
         prog = q.compile_aggregate(queries.zipf_agg(flags=abi.OUT_DEVICE))
         drs = q.DeviceRowSet(cols)
         bounds = np.concatenate([[0], np.cumsum(sizes)])
-        parts = [q.SliceRowSet(drs, int(lo), int(hi)) for lo, hi in zip(bounds[:-1], bounds[1:])]
+        parts = q.RowSetPointers([q.SliceRowSet(drs, int(lo), int(hi)) for lo, hi in zip(bounds[:-1], bounds[1:])])
         for _ in range(2):
             b = q.AggregateBatch(prog, len(parts))
             b.add(parts)

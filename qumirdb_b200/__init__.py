@@ -413,10 +413,11 @@ class AggregateBatch:
         return words[: self.n, 9].tolist()
 
     def add(self, rowsets) -> None:
-        """Updates aggregate i with rowsets[i]."""
+        """Updates aggregate i with rowsets[i] (row-set objects, or a
+        RowSetPointers built once for a batch that repeats)."""
         if len(rowsets) != self.n:
             raise ValueError(f"{self.n} aggregates, {len(rowsets)} row sets")
-        ptrs = (abi.PRS * self.n)(*[C.pointer(r.rs) for r in rowsets])
+        ptrs = rowsets.arr if isinstance(rowsets, RowSetPointers) else RowSetPointers(rowsets).arr
         if lib().qdb_gpu_agg_dispatch_batch(self.prog.handle, self._ptrs, ptrs, self.n) < 0:
             raise QdbError(f"batched aggregate update failed: {last_error()}")
 
@@ -438,6 +439,17 @@ class AggregateBatch:
             self.release()
         except Exception:
             pass
+
+
+class RowSetPointers:
+    """A C array of TRowSet pointers over row-set objects (kept alive)."""
+
+    def __init__(self, rowsets):
+        self.objs = list(rowsets)
+        self.arr = (abi.PRS * max(1, len(self.objs)))(*[C.pointer(r.rs) for r in self.objs])
+
+    def __len__(self) -> int:
+        return len(self.objs)
 
 
 class RowSets:

@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -315,21 +316,51 @@ std::string ConfigKey(const std::string& shape, int64_t ntasks, int64_t nitems, 
 
 }  // namespace
 
+using RatioTable = std::array<double, 64>;
+
+// The groups-per-row ratios seen for a shape, by size class (0: none yet).
+RatioTable RatiosOf(const std::string& shape) {
+    RatioTable r{};
+    Tuner& t = Tune();
+    std::lock_guard<std::mutex> lk(t.mu);
+    for (auto it = t.ratio.lower_bound({shape, 0}); it != t.ratio.end() && it->first.first == shape; ++it) {
+        if (it->first.second >= 0 && it->first.second < int(r.size())) r[size_t(it->first.second)] = it->second;
+    }
+    return r;
+}
+
 // Estimated groups of a state of `rows` rows: the largest groups-per-row
 // ratio seen for its size class (half the rows before any was seen), with
 // a quarter of headroom, never above the rows or the program's hint.
-int64_t BatchEstimateGroups(const std::string& shape, int64_t rows, int64_t expected) {
-    double r = 0.5;
-    {
-        Tuner& t = Tune();
-        std::lock_guard<std::mutex> lk(t.mu);
-        auto it = t.ratio.find({shape, SizeClass(rows)});
-        if (it != t.ratio.end()) r = std::min(1.0, it->second * 1.25);
-    }
+int64_t EstimateGroups(const RatioTable& ratios, int64_t rows, int64_t expected) {
+    const double seen = ratios[size_t(SizeClass(rows))];
+    const double r = seen > 0 ? std::min(1.0, seen * 1.25) : 0.5;
     int64_t est = int64_t(std::ceil(r * double(rows))) + 64;
     est = std::min(est, std::max<int64_t>(rows, 1));
     if (expected > 0) est = std::min(est, expected);
     return est;
+}
+
+// The typed shape's columns of one row set (the batched kernel's task),
+// resolved against the program's first resolved plan: false when a column
+// has a validity bitmap (outside the typed shapes) or no data.
+bool ResolveShapeColumns(const AggPlan& P0, const FastPlan& F, const ColumnMap& cm, const qdb_column_type* types,
+                         const qdb_rowset* rs, Staging& st, HighTask& t) {
+    std::memset(&t, 0, sizeof(t));
+    const int64_t n = rs->RowCount;
+    for (int c = 0; c < F.ncols && c < kFastCols; ++c) {
+        const int slot = F.col_slot[c];
+        const int input = cm.input_of[slot];
+        if (input >= rs->ColumnCount || types[input].type == QDB_TYPE_BOOL) return false;
+        const qdb_column& col = rs->Columns[input];
+        if (col.Mask) return false;
+        t.cols[c] = static_cast<const char*>(st.Device(col.Data, size_t(n) * P0.cols[slot].width));
+        if (n > 0 && !t.cols[c]) return false;
+    }
+    t.sel = rs->Selection ? static_cast<const uint8_t*>(st.Device(rs->Selection, size_t(n))) : nullptr;
+    if (n > 0 && rs->Selection && !t.sel) return false;
+    t.nrows = n;
+    return true;
 }
 
 }  // namespace qdb
@@ -377,29 +408,35 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
     const AggLowering& lw = prog->agg;
     cudaStream_t s = CurStream();
     Staging stg(s);
-    std::vector<AggPlan> plans(static_cast<size_t>(n), lw.plan);
     std::vector<int64_t> rows(static_cast<size_t>(n));
     std::vector<char> typed(static_cast<size_t>(n), 0);
+    std::vector<HighTask> resolved(static_cast<size_t>(n));
+    // The first row set resolves the whole plan and finds the batched
+    // kernel; the others only resolve the typed shape's columns (a plan copy
+    // per row set would cost more host time than the launch saves).
     FastPlan fast{};
     bool have_fast = false;
+    AggPlan P0 = lw.plan;
     for (int64_t i = 0; i < n; ++i) {
         if (!hts[i] || !batches[i]) {
             SetErr("agg_dispatch_batch: state or batch %lld is NULL", (long long)i);
             return -1;
         }
-        if (!ResolveColumns(plans[size_t(i)], lw.cols, prog->columns.data(), batches[i], stg)) return -1;
         rows[size_t(i)] = batches[i]->RowCount;
-        // The batched kernel is looked up once; later row sets of the same
-        // typed shape only compare their plans with the first.
+        if (have_fast) {
+            typed[size_t(i)] = ResolveShapeColumns(P0, fast, lw.cols, prog->columns.data(), batches[i], stg,
+                                                   resolved[size_t(i)]) ? 1 : 0;
+            continue;
+        }
+        AggPlan pi = lw.plan;
+        if (!ResolveColumns(pi, lw.cols, prog->columns.data(), batches[i], stg)) return -1;
         FastPlan fi{};
-        if (MatchFast(plans[size_t(i)], fi)) {
-            if (have_fast) {
-                typed[size_t(i)] = std::memcmp(&fi, &fast, sizeof(FastPlan)) == 0 ? 1 : 0;
-            } else if (AggBatchSupported(plans[size_t(i)], fi)) {
-                fast = fi;
-                have_fast = true;
-                typed[size_t(i)] = 1;
-            }
+        if (MatchFast(pi, fi) && AggBatchSupported(pi, fi)) {
+            fast = fi;
+            have_fast = true;
+            P0 = pi;
+            typed[size_t(i)] = ResolveShapeColumns(P0, fast, lw.cols, prog->columns.data(), batches[i], stg,
+                                                   resolved[size_t(i)]) ? 1 : 0;
         }
     }
     // States outside the batched kernel (no compiled shape, nullable columns)
@@ -416,11 +453,12 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
             *static_cast<AggTableState**>(hts[i]) = st;
             if (!st) return -1;
         }
-        if (!AggRun(st, plans[size_t(i)], rows[size_t(i)], nullptr, nullptr)) return -1;
+        AggPlan pi = lw.plan;
+        if (!ResolveColumns(pi, lw.cols, prog->columns.data(), batches[i], stg)) return -1;
+        if (!AggRun(st, pi, rows[size_t(i)], nullptr, nullptr)) return -1;
         MirrorHeader(hts[i], st, lw.plan);
     }
     if (members.empty()) return n;
-    const AggPlan& P0 = plans[size_t(members[0])];
     const std::string shape = AggBatchShapeKey(P0, fast);
     const int sw = SlotWords(lw.plan, false);
     const int64_t m = int64_t(members.size());
@@ -428,6 +466,7 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
     // Fresh states: tables (and device counters) carved from one arena.
     std::vector<int> fresh;
     std::vector<int64_t> caps(static_cast<size_t>(m));
+    const RatioTable ratios = RatiosOf(shape);
     for (int64_t k = 0; k < m; ++k) {
         const int i = members[size_t(k)];
         AggTableState* st = StateOf(hts[i]);
@@ -436,7 +475,7 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
             continue;
         }
         fresh.push_back(int(k));
-        const int64_t est = BatchEstimateGroups(shape, rows[size_t(i)], prog->expected_groups);
+        const int64_t est = EstimateGroups(ratios, rows[size_t(i)], prog->expected_groups);
         caps[size_t(k)] = std::max<int64_t>(1024, NextPow2(est + est / 4));
     }
     std::vector<HighTask> tasks(static_cast<size_t>(m));
@@ -495,13 +534,8 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
     }
     for (int64_t k = 0; k < m; ++k) {
         const int i = members[size_t(k)];
-        const AggPlan& pi = plans[size_t(i)];
-        HighTask& t = tasks[size_t(k)];
-        std::memset(&t, 0, sizeof(t));
-        for (int c = 0; c < fast.ncols && c < kFastCols; ++c) t.cols[c] = pi.cols[fast.col_slot[c]].data;
-        t.sel = pi.selection;
-        t.nrows = rows[size_t(i)];
-        t.T = StateOf(hts[i])->t;
+        tasks[size_t(k)] = resolved[size_t(i)];
+        tasks[size_t(k)].T = StateOf(hts[i])->t;
     }
 
     // Block shape and item size.
@@ -660,9 +694,11 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
             if (dpairs[size_t(k)].empty() && srecs[size_t(k)].empty()) continue;
             const int i = members[size_t(k)];
             AggTableState* st = StateOf(hts[i]);
+            AggPlan pi = lw.plan;
+            if (!ResolveColumns(pi, lw.cols, prog->columns.data(), batches[i], stg)) return -1;
             const int64_t nd = int64_t(dpairs[size_t(k)].size() / 2);
             const int64_t ns = int64_t(srecs[size_t(k)].size()) / (1 + lw.plan.state_words);
-            if (!EnsureBuffers(st, plans[size_t(i)], std::max(rows[size_t(i)], nd))) return -1;
+            if (!EnsureBuffers(st, pi, std::max(rows[size_t(i)], nd))) return -1;
             if (st->spill_cap < ns) {
                 DevFree(st->spill, s);
                 st->spill = static_cast<uint64_t*>(DevAlloc(size_t(ns) * (1 + lw.plan.state_words) * 8, s));
@@ -677,9 +713,9 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
                 cudaMemcpyAsync(st->spill, srecs[size_t(k)].data(), srecs[size_t(k)].size() * 8, cudaMemcpyHostToDevice, s);
             cudaStreamSynchronize(s);
             FastPlan fi{};
-            const bool fi_ok = MatchFast(plans[size_t(i)], fi);
+            const bool fi_ok = MatchFast(pi, fi);
             AggUpdateArgs a;
-            a.plan = &plans[size_t(i)];
+            a.plan = &pi;
             a.nrows = rows[size_t(i)];
             a.table = st->t;
             a.counters = st->dc;
@@ -689,13 +725,13 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
             a.spill_cap = st->spill_cap;
             a.smem_slots = st->smem_slots;
             a.fast = fi_ok ? &fi : nullptr;
-            if (!AggReplay(st, plans[size_t(i)], a, nd, ns)) return -1;
+            if (!AggReplay(st, pi, a, nd, ns)) return -1;
         }
     }
     // Tables over half full grow now, as after a one-state update; the ratio
     // of groups to rows is remembered per size class for later batches.
     {
-        Tuner& tn = Tune();
+        RatioTable seen{};
         for (int64_t k = 0; k < m; ++k) {
             const int i = members[size_t(k)];
             AggTableState* st = StateOf(hts[i]);
@@ -704,11 +740,16 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
             if (st->groups * 20 > st->t.capacity * 17 && !Grow(st, lw.plan, st->groups)) return -1;
             MirrorHeader(hts[i], st, lw.plan);
             if (rows[size_t(i)] >= 1024) {
-                const double r = double(st->groups) / double(rows[size_t(i)]);
-                std::lock_guard<std::mutex> lk(tn.mu);
-                double& v = tn.ratio[{shape, SizeClass(rows[size_t(i)])}];
-                v = std::max(v, r);
+                double& v = seen[size_t(SizeClass(rows[size_t(i)]))];
+                v = std::max(v, double(st->groups) / double(rows[size_t(i)]));
             }
+        }
+        Tuner& tn = Tune();
+        std::lock_guard<std::mutex> lk(tn.mu);
+        for (size_t c = 0; c < seen.size(); ++c) {
+            if (seen[c] <= 0) continue;
+            double& v = tn.ratio[{shape, int(c)}];
+            v = std::max(v, seen[c]);
         }
     }
     return n;
