@@ -936,19 +936,14 @@ __global__ void __launch_bounds__(kAggThreads, 1) AggUpdateKernel(const __grid_c
 }
 
 // ---------------------------------------------------------------------------
-// Low-cardinality scan aggregate specialised by a compile-time query shape
-// (the typed row shape of FastPlan): column widths, filter atoms, key
-// columns and every state's factor columns are template constants, so each
-// value is one typed load at a fixed offset of the staged tile; constants
-// (filter bounds, affine factors, key packing) stay runtime-uniform.  Per
-// staged tile, phase A filters the rows, packs their keys and finds their
-// groups (a per-thread cache of the CTA's lane-private groups, else the
-// shared table), appending every row of the first kPrivGroups groups to that
-// group's list in shared memory; rows of other groups take the general
-// typed fold.  Phase B walks the lists one group at a time — the group is
-// the same for the whole warp, so the accumulators are registers addressed
-// at compile time — folding each row with the state list unrolled.  The
-// registers reach the shared table once, after the last tile.
+// Scan aggregates specialised by a compile-time query shape (the typed row
+// shape of FastPlan): column widths, filter atoms, key columns and every
+// state's factor columns are template constants, so each value is one typed
+// load at a fixed offset; constants (filter bounds, affine factors, key
+// packing) stay runtime-uniform.  The shape machinery below serves the
+// low-cardinality kernel (AggSigDirectKernel: lane-private accumulators of
+// the first groups a CTA meets) and the high-cardinality kernels
+// (AggHighKernel, AggHighBatchKernel: a shared tier and the global table).
 // ---------------------------------------------------------------------------
 enum SigKind : int {
     SK_COUNT = 0, SK_SUM64 = 1, SK_SUM128_OF64 = 2, SK_SUM128 = 3,
@@ -1170,236 +1165,6 @@ __device__ __forceinline__ void WarpSum128(uint64_t& lo, uint64_t& hi) {
 
 constexpr int kSigThreads = 512;
 
-template <class SIG>
-__global__ void __launch_bounds__(kSigThreads, 1) AggSigKernel(const __grid_constant__ AggLaunch L) {
-    unsigned char* smem = DynSmem();
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.off_bars);
-    unsigned* misc = reinterpret_cast<unsigned*>(smem + L.off_misc);
-    const SmemTable sm = MakeSmem(L, false, true);
-    const AggPlan& P = L.P;
-    const FastPlan& F = L.F;
-    const int tid = threadIdx.x;
-    const int bd = blockDim.x;
-    const int lane = tid & 31;
-    const int T = L.tile_rows;
-
-    if (tid == 0) {
-        misc[0] = 0;
-        misc[1] = 0;
-        misc[2] = 0;
-        misc[4] = 0;
-        for (int s = 0; s < L.stages; ++s) MbarInit(&full[s], 1);
-        FenceBarrierInit();
-    }
-    for (int i = tid; i < sm.S; i += bd) {
-        sm.keys[i] = kEmptyKey;
-        sm.gid[i] = -1;
-        for (int s = 0; s < P.nstates; ++s) {
-            const StateDesc sd = P.states[s];
-            sm.st[int64_t(sd.word) * sm.S + i] = StateIdentity(sd.kind);
-            if (sd.kind == ST_SUM_I128) sm.st[int64_t(sd.word + 1) * sm.S + i] = 0;
-        }
-    }
-    __syncthreads();
-    if (P.nkeyparts == 0 && tid == 0 && sm.S > 0) {
-        // A keyless aggregate has one group: key 0, lane-private group 0.
-        const int i = int(uint32_t(Fmix64(0)) & uint32_t(sm.S - 1));
-        sm.keys[i] = 0;
-        sm.gid[i] = 0;
-        sm.gid_slot[0] = i;
-        misc[0] = 1;
-        misc[2] = 1;
-    }
-    __syncthreads();
-
-    const int64_t ntiles = (L.nrows + T - 1) / T;
-    auto tile_full = [&](int64_t t) { return L.any_staged && (t + 1) * int64_t(T) <= L.nrows; };
-    auto issue = [&](int64_t t, int s) {
-        unsigned char* st = smem + int64_t(s) * L.stage_bytes;
-        FenceProxyAsync();
-        MbarArriveExpectTx(&full[s], uint32_t(L.stage_bytes));
-        for (int c = 0; c < P.ncols; ++c) {
-            const ColDesc& cd = P.cols[c];
-            if (!cd.stage) continue;
-            BulkG2S(st + cd.smem_off, cd.data + t * T * cd.width, uint32_t(T * cd.width), &full[s]);
-        }
-        if (L.sel_off >= 0) BulkG2S(st + L.sel_off, P.selection + t * T, uint32_t(T), &full[s]);
-    };
-    if (tid == 0) {
-        for (int k = 0; k < L.stages; ++k) {
-            const int64_t t = blockIdx.x + int64_t(k) * gridDim.x;
-            if (t < ntiles && tile_full(t)) issue(t, k);
-        }
-    }
-
-    // Lane-private accumulators: word w of group q of this thread at
-    // pacc[(q * words + w) * bd + tid] (consecutive lanes, consecutive banks).
-    uint64_t* pacc = reinterpret_cast<uint64_t*>(smem + L.off_pacc);
-    for (int i = tid; i < kPrivGroups * SIG::words * bd; i += bd) pacc[i] = 0;
-    // This thread's view of the lane-private groups it has met.
-    uint64_t ckey[kPrivGroups];
-    int cgid[kPrivGroups];
-#pragma unroll
-    for (int j = 0; j < kPrivGroups; ++j) {
-        ckey[j] = kEmptyKey;
-        cgid[j] = -1;
-    }
-    int ncache = 0;
-    if (P.nkeyparts == 0) {
-        ckey[0] = 0;
-        cgid[0] = 0;
-        ncache = 1;
-    }
-
-    // Stage offset of every fast column (-1: not staged), fixed for the launch.
-    int coff[kFastCols];
-#pragma unroll
-    for (int c = 0; c < kFastCols; ++c) {
-        coff[c] = -1;
-        if (c < SIG::Cols::n) {
-            const ColDesc& cd = P.cols[F.col_slot[c]];
-            if (cd.stage) coff[c] = cd.smem_off;
-        }
-    }
-
-    bool aborted = false;
-    for (int64_t k = 0;; ++k) {
-        const int64_t t = blockIdx.x + k * gridDim.x;
-        if (t >= ntiles) break;
-        const int s = int(k % L.stages);
-        const uint32_t phase = uint32_t((k / L.stages) & 1);
-        const bool full_tile = tile_full(t);
-        const int64_t row0 = t * T;
-        const unsigned char* stage = full_tile ? smem + int64_t(s) * L.stage_bytes : nullptr;
-        if (full_tile && !MbarWaitBounded(&full[s], phase)) {
-            SetError(&L.counters->error, DE_WAIT_TIMEOUT);
-            *reinterpret_cast<volatile unsigned*>(&misc[4]) = 1;
-        }
-        if (*reinterpret_cast<volatile unsigned*>(&misc[4])) {
-            aborted = true;
-            break;
-        }
-        const int nrows = int(min(int64_t(T), L.nrows - row0));
-        const uint8_t* sel = P.selection == nullptr ? nullptr
-                             : (stage && L.sel_off >= 0) ? stage + L.sel_off : P.selection + row0;
-        // The tile's base of every fast column: the stage, or global memory.
-        const char* cb[kFastCols];
-#pragma unroll
-        for (int c = 0; c < kFastCols; ++c) {
-            cb[c] = nullptr;
-            if (c < SIG::Cols::n) {
-                cb[c] = coff[c] >= 0 && stage ? reinterpret_cast<const char*>(stage) + coff[c]
-                                              : P.cols[F.col_slot[c]].data + row0 * SIG::cw(c);
-            }
-        }
-#pragma unroll 2
-        for (int r = tid; r < nrows; r += bd) {
-            if (sel && !sel[r]) continue;
-            if (SIG::Atoms::n && ShapeHeld<SIG>(P, F, TileRow{cb, r}) != F.clause_mask) continue;
-            const uint64_t key = ShapeKey<SIG>(TileRow{cb, r});
-            int g = -1;
-#pragma unroll
-            for (int j = 0; j < kPrivGroups; ++j) g = ckey[j] == key ? cgid[j] : g;
-            if (g < 0) {
-                // First row of this group for this thread: the shared table.
-                if (!(P.key_full64 && key == kEmptyKey)) {
-                    const int slot = sm.Find(key);
-                    if (slot >= 0) {
-                        const int gg = *reinterpret_cast<volatile int*>(&sm.gid[slot]);
-                        if (gg >= 0 && gg < kPrivGroups && ncache < kPrivGroups) {
-                            g = gg;
-#pragma unroll
-                            for (int j = 0; j < kPrivGroups; ++j) {
-                                if (j == ncache) {
-                                    ckey[j] = key;
-                                    cgid[j] = gg;
-                                }
-                            }
-                            ++ncache;
-                        }
-                    }
-                }
-                if (g < 0) {
-                    RowAcc acc{&P, stage, r, row0 + r, 0, -1, 0};
-                    FoldRowFast<false>(L, acc);
-                    continue;
-                }
-            }
-            ShapeFoldP<SIG>(pacc + int64_t(g) * SIG::words * bd + tid, bd, F, TileRow{cb, r});
-        }
-        // Every warp is done with the stage: refill it.
-        __syncthreads();
-        if (tid == 0) {
-            const int64_t nt = t + int64_t(L.stages) * gridDim.x;
-            if (nt < ntiles && tile_full(nt)) issue(nt, s);
-        }
-    }
-    __syncthreads();
-    if (aborted || *reinterpret_cast<volatile unsigned*>(&misc[4])) {
-        // Let copies already issued land before the CTA's memory goes away.
-        if (tid == 0) {
-            const long long start = clock64();
-            while (clock64() - start < 2000000) {
-            }
-        }
-        __syncthreads();
-        return;
-    }
-
-    // Lane-private accumulators -> shared table: one warp per (group,
-    // state) sums the lanes, then one shared-memory update.
-    const int ng = int(min(*reinterpret_cast<volatile unsigned*>(sm.ngid), unsigned(kPrivGroups)));
-    const int nwarps = bd >> 5;
-    for (int item = tid >> 5; item < ng * SIG::n; item += nwarps) {
-        const int q = item / SIG::n;
-        const int st2 = item - q * SIG::n;
-        const int o = SIG::off(st2);
-        const bool wide2 = SIG::width(st2) == 2;
-        uint64_t lo = 0, hi = 0;
-        for (int t2 = lane; t2 < bd; t2 += 32) {
-            const uint64_t* w = pacc + int64_t(q * SIG::words + o) * bd + t2;
-            Add128(lo, hi, w[0], wide2 ? w[bd] : 0ull);
-        }
-        WarpSum128(lo, hi);
-        if (lane == 0 && (lo | hi)) {
-            const int slot = *reinterpret_cast<volatile int*>(&sm.gid_slot[q]);
-            const StateDesc sd = P.states[st2];
-            uint64_t* w = sm.st + int64_t(sd.word) * sm.S + slot;
-            ApplyState(w, w + sm.S, sd.kind, lo, hi, 0.0);
-        }
-    }
-    __syncthreads();
-
-    // Shared table -> global table.
-    for (int i = tid; i < sm.S; i += bd) {
-        const uint64_t key = sm.keys[i];
-        if (key == kEmptyKey) continue;
-        int is_new = 0;
-        const int64_t g = GlobalFind1(L.T, L.cap_mask, key, is_new);
-        if (is_new) atomicAdd(sm.fresh, 1u);
-        if (g < 0) {
-            const unsigned long long e = atomicAdd(&L.counters->spilled, 1ull);
-            if (int64_t(e) >= L.spill_cap) {
-                SetError(&L.counters->error, DE_SPILL_FULL);
-                continue;
-            }
-            uint64_t* rec = L.spill + int64_t(e) * (1 + P.state_words);
-            rec[0] = key;
-            for (int w = 0; w < P.state_words; ++w) rec[1 + w] = sm.st[int64_t(w) * sm.S + i];
-            continue;
-        }
-        uint64_t* gbase = L.T.slots + g * L.T.slot_words + L.T.state_off;
-        for (int st2 = 0; st2 < P.nstates; ++st2) {
-            const StateDesc sd = P.states[st2];
-            const uint64_t lo = sm.st[int64_t(sd.word) * sm.S + i];
-            const uint64_t hi = sd.kind == ST_SUM_I128 ? sm.st[int64_t(sd.word + 1) * sm.S + i] : 0;
-            if (IsIdentity(sd.kind, lo, hi)) continue;
-            ApplyState(gbase + sd.word, gbase + sd.word + 1, sd.kind, lo, hi, 0.0);
-        }
-    }
-    __syncthreads();
-    if (tid == 0 && sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
-}
 
 // ---------------------------------------------------------------------------
 // High-cardinality scan aggregate specialised by query shape: typed loads
@@ -1929,6 +1694,181 @@ __global__ void __launch_bounds__(256) AggBatchSpillKernel(const __grid_constant
         __builtin_memcpy(&f, &lo, 8);
         ApplyState(gbase + sd.word, gbase + sd.word + 1, sd.kind, lo, hi, f);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Low-cardinality scan aggregate read straight from HBM: the signature
+// kernel's folds (lane-private accumulators of the first kPrivGroups groups,
+// the shared table, the general typed fold past them) over one contiguous
+// row range per CTA, each warp taking 32 consecutive rows at a time with the
+// next 32 already loading into registers; no staging, no block barrier
+// until the merge.
+// ---------------------------------------------------------------------------
+template <class SIG>
+__global__ void __launch_bounds__(kSigThreads, 1) AggSigDirectKernel(const __grid_constant__ AggLaunch L) {
+    unsigned char* smem = DynSmem();
+    unsigned* misc = reinterpret_cast<unsigned*>(smem + L.off_misc);
+    const SmemTable sm = MakeSmem(L, false, true);
+    const AggPlan& P = L.P;
+    const FastPlan& F = L.F;
+    const int tid = threadIdx.x;
+    const int bd = blockDim.x;
+    const int lane = tid & 31;
+
+    if (tid == 0) {
+        misc[0] = 0;
+        misc[1] = 0;
+        misc[2] = 0;
+        misc[4] = 0;
+    }
+    for (int i = tid; i < sm.S; i += bd) {
+        sm.keys[i] = kEmptyKey;
+        sm.gid[i] = -1;
+        for (int s = 0; s < P.nstates; ++s) {
+            const StateDesc sd = P.states[s];
+            sm.st[int64_t(sd.word) * sm.S + i] = StateIdentity(sd.kind);
+            if (sd.kind == ST_SUM_I128) sm.st[int64_t(sd.word + 1) * sm.S + i] = 0;
+        }
+    }
+    uint64_t* pacc = reinterpret_cast<uint64_t*>(smem + L.off_pacc);
+    for (int i = tid; i < kPrivGroups * SIG::words * bd; i += bd) pacc[i] = 0;
+    __syncthreads();
+    if (P.nkeyparts == 0 && tid == 0 && sm.S > 0) {
+        const int i = int(uint32_t(Fmix64(0)) & uint32_t(sm.S - 1));
+        sm.keys[i] = 0;
+        sm.gid[i] = 0;
+        sm.gid_slot[0] = i;
+        misc[0] = 1;
+        misc[2] = 1;
+    }
+    __syncthreads();
+
+    uint64_t ckey[kPrivGroups];
+    int cgid[kPrivGroups];
+#pragma unroll
+    for (int j = 0; j < kPrivGroups; ++j) {
+        ckey[j] = kEmptyKey;
+        cgid[j] = -1;
+    }
+    int ncache = 0;
+    if (P.nkeyparts == 0) {
+        ckey[0] = 0;
+        cgid[0] = 0;
+        ncache = 1;
+    }
+
+    const int64_t per = (L.nrows + gridDim.x - 1) / gridDim.x;
+    const int64_t row0 = int64_t(blockIdx.x) * per;
+    const int n = int(max(int64_t(0), min(per, L.nrows - row0)));
+    const char* cb[kFastCols];
+#pragma unroll
+    for (int c = 0; c < kFastCols; ++c) {
+        cb[c] = nullptr;
+        if (c < SIG::Cols::n) cb[c] = P.cols[F.col_slot[c]].data + row0 * SIG::cw(c);
+    }
+    const uint8_t* sel = P.selection ? P.selection + row0 : nullptr;
+    const int step = (bd >> 5) * 32;
+    int r = (tid >> 5) * 32 + lane;
+    RegRow<SIG::Cols::n> cur;
+    LoadRow<SIG>(cur, cb, r, r < n);
+    bool cur_sel = r < n && (!sel || sel[r]);
+#pragma unroll 1
+    for (; r - lane < n; r += step) {
+        const int rn = r + step;
+        RegRow<SIG::Cols::n> nxt;
+        LoadRow<SIG>(nxt, cb, rn, rn < n);
+        const bool nxt_sel = rn < n && (!sel || sel[rn]);
+        bool ok = cur_sel;
+        if (ok && SIG::Atoms::n) ok = ShapeHeld<SIG>(P, F, cur) == F.clause_mask;
+        if (ok) {
+            const uint64_t key = ShapeKey<SIG>(cur);
+            int g = -1;
+#pragma unroll
+            for (int j = 0; j < kPrivGroups; ++j) g = ckey[j] == key ? cgid[j] : g;
+            if (g < 0 && !(P.key_full64 && key == kEmptyKey)) {
+                // First row of this group for this thread: the shared table.
+                const int slot = sm.Find(key);
+                if (slot >= 0) {
+                    const int gg = *reinterpret_cast<volatile int*>(&sm.gid[slot]);
+                    if (gg >= 0 && gg < kPrivGroups && ncache < kPrivGroups) {
+                        g = gg;
+#pragma unroll
+                        for (int j = 0; j < kPrivGroups; ++j) {
+                            if (j == ncache) {
+                                ckey[j] = key;
+                                cgid[j] = gg;
+                            }
+                        }
+                        ++ncache;
+                    }
+                }
+            }
+            if (g >= 0) {
+                ShapeFoldP<SIG>(pacc + int64_t(g) * SIG::words * bd + tid, bd, F, cur);
+            } else {
+                RowAcc acc{&P, nullptr, r, row0 + r, 0, -1, 0};
+                FoldRowFast<false>(L, acc);
+            }
+        }
+        cur = nxt;
+        cur_sel = nxt_sel;
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // Lane-private accumulators -> shared table: one warp per (group,
+    // state) sums the lanes, then one shared-memory update.
+    const int ng = int(min(*reinterpret_cast<volatile unsigned*>(sm.ngid), unsigned(kPrivGroups)));
+    const int nwarps = bd >> 5;
+    for (int item = tid >> 5; item < ng * SIG::n; item += nwarps) {
+        const int q = item / SIG::n;
+        const int st2 = item - q * SIG::n;
+        const int o = SIG::off(st2);
+        const bool wide2 = SIG::width(st2) == 2;
+        uint64_t lo = 0, hi = 0;
+        for (int t2 = lane; t2 < bd; t2 += 32) {
+            const uint64_t* w = pacc + int64_t(q * SIG::words + o) * bd + t2;
+            Add128(lo, hi, w[0], wide2 ? w[bd] : 0ull);
+        }
+        WarpSum128(lo, hi);
+        if (lane == 0 && (lo | hi)) {
+            const int slot = *reinterpret_cast<volatile int*>(&sm.gid_slot[q]);
+            const StateDesc sd = P.states[st2];
+            uint64_t* w = sm.st + int64_t(sd.word) * sm.S + slot;
+            ApplyState(w, w + sm.S, sd.kind, lo, hi, 0.0);
+        }
+    }
+    __syncthreads();
+
+    // Shared table -> global table.
+    for (int i = tid; i < sm.S; i += bd) {
+        const uint64_t key = sm.keys[i];
+        if (key == kEmptyKey) continue;
+        int is_new = 0;
+        const int64_t g = GlobalFind1(L.T, L.cap_mask, key, is_new);
+        if (is_new) atomicAdd(sm.fresh, 1u);
+        if (g < 0) {
+            const unsigned long long e = atomicAdd(&L.counters->spilled, 1ull);
+            if (int64_t(e) >= L.spill_cap) {
+                SetError(&L.counters->error, DE_SPILL_FULL);
+                continue;
+            }
+            uint64_t* rec = L.spill + int64_t(e) * (1 + P.state_words);
+            rec[0] = key;
+            for (int w = 0; w < P.state_words; ++w) rec[1 + w] = sm.st[int64_t(w) * sm.S + i];
+            continue;
+        }
+        uint64_t* gbase = L.T.slots + g * L.T.slot_words + L.T.state_off;
+        for (int st2 = 0; st2 < P.nstates; ++st2) {
+            const StateDesc sd = P.states[st2];
+            const uint64_t lo = sm.st[int64_t(sd.word) * sm.S + i];
+            const uint64_t hi = sd.kind == ST_SUM_I128 ? sm.st[int64_t(sd.word + 1) * sm.S + i] : 0;
+            if (IsIdentity(sd.kind, lo, hi)) continue;
+            ApplyState(gbase + sd.word, gbase + sd.word + 1, sd.kind, lo, hi, 0.0);
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
 }
 
 // The instantiated query shapes.  QDB_C(w, u): a fast column of w bytes
@@ -2510,7 +2450,7 @@ SigKernelFn FindSigKernel(const AggPlan& P, const FastPlan& F) {
     const std::vector<int> key = ShapeKeyOf(P, F);
     if (key.empty()) return nullptr;
 #define QDB_SHAPE_FIND(...) \
-    if (ShapeMatches<__VA_ARGS__>(key) && ShapeWordsMatch<__VA_ARGS__>(F)) return AggSigKernel<__VA_ARGS__>;
+    if (ShapeMatches<__VA_ARGS__>(key) && ShapeWordsMatch<__VA_ARGS__>(F)) return AggSigDirectKernel<__VA_ARGS__>;
     QDB_SHAPE_LIST(QDB_SHAPE_FIND)
 #undef QDB_SHAPE_FIND
     if (std::getenv("QDB_SHAPE_DEBUG")) {
@@ -2641,14 +2581,11 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
         // kernel (no lane-private arrays; the group lists take their place).
         if (SigKernelFn fn = FindSigKernel(L.P, *a.fast)) {
             L.F = *a.fast;
-            int Ts = 4096;
-            size_t bytes = 0;
+            // The kernel stages nothing: a token stage keeps the layout's offsets.
+            layout(16, 1, 64);
             const size_t pacc_sig = size_t(kPrivGroups) * sw * kSigThreads * 8;
-            for (;; Ts >>= 1) {
-                layout(Ts, 2, 64);
-                bytes = size_t(L.off_pacc) + pacc_sig;
-                if (bytes <= budget || Ts <= 256) break;
-            }
+            const size_t bytes = size_t(L.off_pacc) + pacc_sig;
+            const int Ts = 2048;                   // rows per CTA at least, for the grid size
             if (bytes <= budget) {
                 L.smem_slots = 64;
                 L.smem_limit = 32;
