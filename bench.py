@@ -463,6 +463,33 @@ def cpu_baseline_sort(sample: int) -> dict:
             "seconds": sec}
 
 
+def cpu_baseline_agg(kind: str, sample: int) -> dict:
+    """The CPU restatement's threaded aggregate plan (per-lane partial
+    tables, then the hash-partitioned final) on all host threads, over the
+    lineitem table or a sample of the Zipf stream."""
+    from oracle import oracle as O
+    import qumirdb_b200 as q
+    from qumirdb_b200 import queries
+    if kind == "lineitem":
+        cols = [np.empty(sample, np.int64), np.empty(sample, np.int64), np.empty(sample, np.int64),
+                np.empty(sample, np.int64), np.empty(sample, np.uint8), np.empty(sample, np.uint8),
+                np.empty(sample, np.int32)]
+        q.lib().qdb_gen_lineitem(0, sample, *[c.ctypes.data for c in cols])
+        spec = queries.lineitem_agg(int(cols[6].max()) - 90)
+        what = f"{sample:,} rows (the whole table)"
+    else:
+        cols = [np.empty(sample, np.int64), np.empty(sample, np.int64), np.empty(sample, np.float64)]
+        q.lib().qdb_gen_zipf(2, sample, ZIPF_DISTINCT, 1.1, *[c.ctypes.data for c in cols])
+        spec = queries.zipf_agg(expected_groups=ZIPF_DISTINCT)
+        what = f"{sample:,} rows (of 200M) of the same Zipf stream"
+    threads = os.cpu_count() or 1
+    rs = q.HostRowSet(cols)
+    sec = O.lib().oracle_bench_aggregate(C.byref(spec.struct), rs.ptr, threads, None)
+    return {"value": sample / sec, "unit": "rows/s", "cores": threads, "kind": "port",
+            "sample": what + ": per-lane partial tables + hash-partitioned final of the CPU restatement",
+            "seconds": sec}
+
+
 def cpu_baseline_join(sample_probe: int, steps: int = 1) -> dict:
     from oracle import oracle as O
     import qumirdb_b200 as q
@@ -685,6 +712,10 @@ def main() -> None:
             if not args.no_cpu_baseline:
                 line["operators"]["sort"]["cpu_baseline"] = {
                     k: v for k, v in cpu_baseline_sort(20_000_000).items() if k != "seconds"}
+                line["operators"]["lineitem"]["cpu_baseline"] = {
+                    k: v for k, v in cpu_baseline_agg("lineitem", LINEITEM_ROWS).items() if k != "seconds"}
+                line["operators"]["zipf"]["cpu_baseline"] = {
+                    k: v for k, v in cpu_baseline_agg("zipf", 20_000_000).items() if k != "seconds"}
         except Exception as e:  # reported, never hidden
             line["operators_error"] = repr(e)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
