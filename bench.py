@@ -45,6 +45,7 @@ ZIPF_PARTS = 4096
 SERVE_TABLES = 16
 SERVE_BUDGET = 150 * 10**9
 SERVE_WORKERS = 3
+SERVE_COALESCE_ROWS = 0     # rows up to which waiting Zipf aggregations coalesce (0: off)
 ZIPF_DISTINCT = 20_000_000
 SORT_ROWS = 300_000_000
 METRIC = "rows/s & HBM GB/s vs peak per operator; mixed-stream queries/s and p50/p99"
@@ -347,7 +348,7 @@ def serving_operator(q):
                        f"{int(sizes.sum())} rows, {resident / 1e9:.1f} GB), templates lineitem/join/zipf/sort, "
                        "Poisson arrivals", "plain_service_ms": service * 1e3, "budget_bytes": budget,
            "resident_bytes": resident, "sweeps": {}}
-    srv = serving.BatchingServer(progs, budget, resident, workers=SERVE_WORKERS, small_rows=2 << 20,
+    srv = serving.BatchingServer(progs, budget, resident, workers=SERVE_WORKERS, small_rows=SERVE_COALESCE_ROWS,
                                  max_sort_rows=max_sort, keep_results=False)
     # Warm-up: the autotuner's search for the coalesced aggregation shape,
     # then the workers.

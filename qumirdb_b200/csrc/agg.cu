@@ -2319,7 +2319,7 @@ void EnsureDeviceInfo() {
 
 template <class K>
 void SetSmem(K kernel, size_t bytes) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    EnsureSmemLimit(reinterpret_cast<const void*>(kernel), bytes);
 }
 
 int64_t Align(int64_t v, int64_t a) { return (v + a - 1) / a * a; }

@@ -408,7 +408,7 @@ void JoinSumRun(const JoinSumShape& shape, const JTableDev& jt, int64_t nrows, u
     const int64_t tiles = std::max<int64_t>(1, (nrows + kJsTile - 1) / kJsTile);
     const int blocks = int(std::min<int64_t>(tiles, DeviceSMs()));
     const JsKernelFn fn = PickKernel(L);
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    EnsureSmemLimit(reinterpret_cast<const void*>(fn), smem);
     ProfileBegin(s, "join_agg_probe", nrows);
     fn<<<blocks, kJsThreads, smem, s>>>(L);
     ProfileEnd(s);

@@ -270,6 +270,12 @@ void AggFinalizeBatch(const AggPlan& p, const OutputPlan& out, const GTableDev& 
                       const FinBlock* blocks, int64_t nblocks, AggOutputCol* cols, int ncols, int64_t out_rows,
                       void* scratch, int* err, cudaStream_t s);
 
+// Raises a kernel's dynamic shared memory limit to `bytes` when it is
+// below (runtime.cpp): the attribute only grows, and an unchanged kernel is
+// not touched again (a change can wait on the kernel's launches in flight
+// on every stream).
+void EnsureSmemLimit(const void* fn, size_t bytes);
+
 // Kernel timing hooks (runtime.cpp).
 bool ProfileOn();
 void ProfileBegin(cudaStream_t s, const char* name, int64_t units);

@@ -89,6 +89,27 @@ cudaStream_t CurStream() {
 
 bool ProfileOn() { return g_prof_on.load(std::memory_order_relaxed); }
 
+void EnsureSmemLimit(const void* fn, size_t bytes) {
+    static std::mutex mu;
+    static std::vector<std::pair<const void*, size_t>> limits;
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto& l : limits) {
+        if (l.first != fn) continue;
+        if (l.second >= bytes) return;
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)) == cudaSuccess) {
+            l.second = bytes;
+        } else {
+            cudaGetLastError();
+        }
+        return;
+    }
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)) == cudaSuccess) {
+        limits.emplace_back(fn, bytes);
+    } else {
+        cudaGetLastError();
+    }
+}
+
 void ProfileBegin(cudaStream_t s, const char* name, int64_t units) {
     if (!g_prof_on.load(std::memory_order_relaxed)) return;
     ProfRec r;
@@ -155,6 +176,9 @@ namespace {
 std::mutex g_host_mu;
 std::vector<std::vector<void*>> g_host_free(64);     // by power-of-two size class
 std::vector<std::pair<void*, int>> g_host_class;     // live buffer -> class (sorted by address)
+char* g_host_arena = nullptr;                        // page-locked once, carved by size class
+size_t g_host_arena_size = 0;
+size_t g_host_arena_used = 0;
 
 int HostClass(size_t bytes) {
     int c = 16;   // 64 KiB and up
@@ -162,25 +186,48 @@ int HostClass(size_t bytes) {
     return c;
 }
 
+// Bytes of page-locked memory reserved for host outputs at the first output
+// (QDB_PINNED_OUTPUT_MB, default 4 GiB): page-locking later, while queries
+// run, would hold the driver and stall every stream.
+size_t HostArenaBytes() {
+    const char* e = std::getenv("QDB_PINNED_OUTPUT_MB");
+    const long long mb = e ? std::atoll(e) : 4096;
+    return size_t(std::max<long long>(mb, 0)) << 20;
+}
+
 }  // namespace
 
 void* HostOutAlloc(size_t bytes) {
     const int c = HostClass(std::max<size_t>(bytes, 1));
+    const size_t size = size_t(1) << c;
     std::lock_guard<std::mutex> lk(g_host_mu);
-    void* p = nullptr;
     if (!g_host_free[size_t(c)].empty()) {
-        p = g_host_free[size_t(c)].back();
+        void* p = g_host_free[size_t(c)].back();
         g_host_free[size_t(c)].pop_back();
-    } else if (cudaMallocHost(&p, size_t(1) << c) != cudaSuccess) {
-        cudaGetLastError();
-        p = std::malloc(size_t(1) << c);   // pageable when pinned memory runs out
-        if (!p) return nullptr;
-        g_host_class.insert(std::upper_bound(g_host_class.begin(), g_host_class.end(), std::make_pair(p, -1)),
-                            std::make_pair(p, -c));
         return p;
     }
+    if (!g_host_arena && g_host_arena_size == 0) {
+        g_host_arena_size = HostArenaBytes();
+        void* a = nullptr;
+        if (g_host_arena_size && cudaMallocHost(&a, g_host_arena_size) == cudaSuccess) {
+            g_host_arena = static_cast<char*>(a);
+        } else {
+            cudaGetLastError();
+            g_host_arena_size = 1;   // not again
+        }
+    }
+    void* p = nullptr;
+    int tag = c;
+    if (g_host_arena && g_host_arena_used + size <= g_host_arena_size) {
+        p = g_host_arena + g_host_arena_used;
+        g_host_arena_used += size;
+    } else {
+        p = std::malloc(size);   // pageable once the page-locked arena is used up
+        if (!p) return nullptr;
+        tag = -c;
+    }
     auto it = std::lower_bound(g_host_class.begin(), g_host_class.end(), std::make_pair(p, INT32_MIN));
-    if (it == g_host_class.end() || it->first != p) g_host_class.insert(it, std::make_pair(p, c));
+    g_host_class.insert(it, std::make_pair(p, tag));
     return p;
 }
 
@@ -189,7 +236,7 @@ void HostOutFree(void* p) {
     std::lock_guard<std::mutex> lk(g_host_mu);
     auto it = std::lower_bound(g_host_class.begin(), g_host_class.end(), std::make_pair(p, INT32_MIN));
     if (it == g_host_class.end() || it->first != p) return;
-    if (it->second < 0) {   // pageable fallback
+    if (it->second < 0) {   // pageable
         std::free(p);
         g_host_class.erase(it);
         return;

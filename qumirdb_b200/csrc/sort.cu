@@ -509,7 +509,7 @@ void SortExtract(const int64_t* ids, int64_t n, const StoreTable& st, const Sort
     L.hist = hist;
     L.err = err;
     const size_t smem = size_t(nstages) * kSortDigits * 256 * 4;
-    cudaFuncSetAttribute(SortExtractKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    EnsureSmemLimit(reinterpret_cast<const void*>(SortExtractKernel), smem);
     ProfileBegin(s, "sort_extract", n);
     SortExtractKernel<<<Blocks(n, kExtractThreads, 4), kExtractThreads, smem, s>>>(L);
     ProfileEnd(s);
@@ -538,7 +538,7 @@ void SortPass(bool wide, const void* keys_in, const uint32_t* idx_in, bool gathe
         L.tile_counter = tile_counter;
         L.err = err;
         const size_t smem = size_t(kSortTile) * (sizeof(K) + 4);
-        cudaFuncSetAttribute(SortPassKernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        EnsureSmemLimit(reinterpret_cast<const void*>(SortPassKernel<K>), smem);
         ProfileBegin(s, wide ? "sort_pass_u64" : "sort_pass_u32", n);
         SortPassKernel<K><<<int(tiles), kPassThreads, smem, s>>>(L);
         ProfileEnd(s);
