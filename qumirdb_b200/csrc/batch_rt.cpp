@@ -75,6 +75,15 @@ bool TuningEnabled() {
     return !(e && e[0] == '0');
 }
 
+// QDB_BATCH_GRAPHS=0 runs every batched launch sequence eagerly.
+bool GraphsEnabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("QDB_BATCH_GRAPHS");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 // Device buffers and pinned staging of one host thread's batched launches;
 // they only grow, so a captured graph stays valid while its key holds.
 struct BatchContext {
@@ -90,12 +99,14 @@ struct BatchContext {
     unsigned long long* h_new = nullptr;
     BatchCounters* h_counters = nullptr;
     cudaStream_t s = nullptr;
-    // Graph of the launch sequence and the key it was captured for; a key is
-    // captured the second time in a row it comes (a one-off batch runs
-    // eagerly).
+    // Graph of the launch sequence and the key it was captured for.  A key is
+    // captured the third time in a row it comes: batches of changing makeup
+    // (a serving mix) run eagerly, since capturing and instantiating a graph
+    // holds up the launches of other threads.
     cudaGraphExec_t exec = nullptr;
     std::string graph_key;
     std::string last_key;
+    int repeats = 0;
     int64_t graph_launches = 0;
     int64_t graph_replays = 0;
 
@@ -110,17 +121,14 @@ struct BatchContext {
         cap = p ? n : 0;
         return p != nullptr;
     }
+    // Pinned staging comes from the library's page-locked output pool:
+    // page-locking fresh memory while other streams run stalls them all.
     template <class T>
     static bool GrowPinned(T*& p, int64_t cap_before, int64_t n) {
         if (p && n <= cap_before) return true;
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        if (cudaMallocHost(reinterpret_cast<void**>(&p), size_t(std::max<int64_t>(n, 1)) * sizeof(T)) != cudaSuccess) {
-            cudaGetLastError();
-            p = nullptr;
-            return false;
-        }
-        return true;
+        HostOutFree(p);
+        p = static_cast<T*>(HostOutAlloc(size_t(std::max<int64_t>(n, 1)) * sizeof(T)));
+        return p != nullptr;
     }
 
     bool Reserve(int64_t ntasks, int64_t nitems, int64_t deferred, int64_t spill_words, cudaStream_t st) {
@@ -626,9 +634,10 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
     };
     const std::string gkey = ConfigKey(shape, m, nitems, cfg, cx);
     bool ran = false;
-    const bool repeat = gkey == cx.last_key;
+    cx.repeats = gkey == cx.last_key ? cx.repeats + 1 : 1;
     cx.last_key = gkey;
-    if (!ProfileOn() && s != nullptr && (repeat || (cx.exec && cx.graph_key == gkey))) {
+    const bool repeat = cx.repeats >= 3;
+    if (GraphsEnabled() && !ProfileOn() && s != nullptr && (repeat || (cx.exec && cx.graph_key == gkey))) {
         if (cx.exec && cx.graph_key != gkey) {
             cudaGraphExecDestroy(cx.exec);
             cx.exec = nullptr;

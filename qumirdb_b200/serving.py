@@ -441,6 +441,9 @@ class BatchingServer:
         for r in range(rounds):
             burst = [Query(i, t, 0.0) for i, t in enumerate(sorted(tables, key=lambda t: -t.rows) * self.workers)]
             self.run(burst)
+            small = [t for t in tables if self._coalescable(Query(0, t, 0.0))]
+            if small:   # coalesced batches on every worker
+                self.run([Query(i, t, 0.0) for i, t in enumerate(small * self.max_batch * self.workers)])
 
     def run(self, stream: list[Query]) -> dict:
         """Serves one stream of queries (arrivals at their `arrival` times)

@@ -90,7 +90,7 @@ def test_batch_autotune_and_graph_replay():
     prog = q.compile_aggregate(queries.zipf_agg(flags=abi.OUT_DEVICE))
     types = queries.ZIPF_OUT_TYPES
     results = []
-    for rep in range(3):
+    for rep in range(4):
         batch = q.AggregateBatch(prog, len(parts))
         batch.add([q.DeviceRowSet(cols) for cols in parts])
         outs = batch.finish()
@@ -99,10 +99,10 @@ def test_batch_autotune_and_graph_replay():
             q.release(o)
     info = q.autotune_info()
     assert info["searches"] == 1 and info["trials"] >= 2, info
-    assert info["reused"] >= 2, info
-    assert info["graph_replays"] >= 2, info
+    assert info["reused"] >= 3, info
+    assert info["graph_replays"] >= 2, info      # captured on the third identical batch
     assert len(info["configs"]) == 1 and info["configs"][0]["threads"] in (512, 1024), info
-    for rep in (1, 2):
+    for rep in (1, 2, 3):
         for a, b in zip(results[0], results[rep]):
             assert_tables_equal(a, b, types)
 
