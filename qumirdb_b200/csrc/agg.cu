@@ -1391,12 +1391,81 @@ __device__ __forceinline__ void LoadRow(RegRow<SH::Cols::n>& row, const char* co
     }
 }
 
-// One range of rows through the tiers.  Each warp takes 32 consecutive rows
-// at a time, coalesced straight from HBM with the next 32 already loading
-// while these are folded; each lane then goes its own way (the shared tier
-// when its key is there, else the global table) and the warp reconverges
-// before the next rows.
-// `defer_base` numbers the range's rows for the replay list.
+// The probe of `key` from its home slot, whose key word `cur` is already
+// loaded (so that two rows' first probes can be in flight together).
+__device__ __forceinline__ int64_t GlobalFindFrom(const GTableDev& T, uint64_t mask, uint64_t h, uint64_t key,
+                                                  uint64_t cur, int& is_new) {
+    uint64_t i = h & mask;
+#pragma unroll 1
+    for (int p = 0; p < kMaxProbe; ++p) {
+        unsigned long long* kp =
+            reinterpret_cast<unsigned long long*>(T.slots + int64_t(i) * T.slot_words + T.key_off);
+        if (p > 0) cur = *reinterpret_cast<volatile unsigned long long*>(kp);
+        if (cur == key) return int64_t(i);
+        if (cur == kEmptyKey) {
+            const uint64_t old = atomicCAS(kp, kEmptyKey, key);
+            if (old == kEmptyKey) {
+                is_new = 1;
+                return int64_t(i);
+            }
+            if (old == key) return int64_t(i);
+        }
+        i = (i + 1) & mask;
+    }
+    return -1;
+}
+
+// One row's fold up to the global table: filter, key, values, the shared
+// tier.  Returns true when the row still needs the global table.
+template <class SH>
+__device__ __forceinline__ bool HighRowTier(const AggPlan& P, const FastPlan& F, const HighDst& D,
+                                            const HighSmem& sm, const RegRow<SH::Cols::n>& row, bool ok,
+                                            int64_t defer_row, uint64_t& key, uint64_t& h, ShapeVals<SH>& v) {
+    if (ok && SH::Atoms::n) ok = ShapeHeld<SH>(P, F, row) == F.clause_mask;
+    if (!ok) return false;
+    key = ShapeKey<SH>(row);
+    ShapeRowVals<SH>(v, F, row);
+    h = Fmix64(key);
+    if (P.key_full64 && key == kEmptyKey) {
+        // The one key equal to the empty marker: the table's flag slot.
+        unsigned long long* flag =
+            reinterpret_cast<unsigned long long*>(D.T.slots + D.T.capacity * D.T.slot_words + D.T.key_off);
+        if (*reinterpret_cast<volatile unsigned long long*>(flag) == 0 && atomicExch(flag, 1ull) == 0) {
+            atomicAdd(sm.fresh, 1u);
+        }
+        ShapeAtomics<SH>(D.T.slots + D.T.capacity * D.T.slot_words + D.T.state_off, 1, v);
+        return false;
+    }
+    const int slot = sm.Find(h, key);
+    if (slot >= 0) {
+        ShapeSmemAtomics<SH>(sm.st + slot, sm.S, v);
+        return false;
+    }
+    (void)defer_row;
+    return true;
+}
+
+template <class SH>
+__device__ __forceinline__ void HighRowGlobal(const HighDst& D, const HighSmem& sm, uint64_t key, uint64_t h,
+                                              uint64_t first, const ShapeVals<SH>& v, int64_t defer_row) {
+    int is_new = 0;
+    const int64_t gslot = GlobalFindFrom(D.T, D.cap_mask, h, key, first, is_new);
+    if (is_new) atomicAdd(sm.fresh, 1u);
+    if (gslot < 0) {
+        DeferTo(D, defer_row);    // replayed after the table grows
+    } else {
+        ShapeAtomics<SH>(D.T.slots + gslot * D.T.slot_words + D.T.state_off, 1, v);
+    }
+}
+
+// One range of rows through the tiers.  Each warp takes two groups of 32
+// consecutive rows at a time (each lane one row of each), coalesced straight
+// from HBM with the next two groups already loading into registers while
+// these are folded.  A lane resolves both rows against the shared tier, then
+// issues the first global-table probe of each row that missed before it
+// waits on either, so two dependent probe chains overlap; the warp
+// reconverges before the next rows.  `defer_base` numbers the range's rows
+// for the replay list.
 template <class SH>
 __device__ __forceinline__ void HighRows(const AggPlan& P, const FastPlan& F, const HighDst& D, const HighSmem& sm,
                                          const char* const* cb, const uint8_t* sel, int nrows, int64_t defer_base,
@@ -1404,50 +1473,37 @@ __device__ __forceinline__ void HighRows(const AggPlan& P, const FastPlan& F, co
     const int lane = int(threadIdx.x & 31);
     const int step = nw * 32;
     int r = wid * 32 + lane;
-    RegRow<SH::Cols::n> cur;
-    LoadRow<SH>(cur, cb, r, r < nrows);
-    bool cur_sel = r < nrows && (!sel || sel[r]);
+    RegRow<SH::Cols::n> ca, cbr;
+    LoadRow<SH>(ca, cb, r, r < nrows);
+    LoadRow<SH>(cbr, cb, r + step, r + step < nrows);
+    bool sa = r < nrows && (!sel || sel[r]);
+    bool sb = r + step < nrows && (!sel || sel[r + step]);
 #pragma unroll 1
-    for (; r - lane < nrows; r += step) {
-        const int rn = r + step;
-        RegRow<SH::Cols::n> nxt;
-        LoadRow<SH>(nxt, cb, rn, rn < nrows);
-        const bool nxt_sel = rn < nrows && (!sel || sel[rn]);
-        bool ok = cur_sel;
-        if (ok && SH::Atoms::n) ok = ShapeHeld<SH>(P, F, cur) == F.clause_mask;
-        if (ok) {
-            const uint64_t key = ShapeKey<SH>(cur);
-            ShapeVals<SH> v;
-            ShapeRowVals<SH>(v, F, cur);
-            const uint64_t h = Fmix64(key);
-            const bool special = P.key_full64 && key == kEmptyKey;
-            const int slot = special ? -1 : sm.Find(h, key);
-            if (slot >= 0) {
-                ShapeSmemAtomics<SH>(sm.st + slot, sm.S, v);
-            } else {
-                int64_t gslot;
-                if (special) {
-                    gslot = D.T.capacity;
-                    unsigned long long* flag = reinterpret_cast<unsigned long long*>(
-                        D.T.slots + D.T.capacity * D.T.slot_words + D.T.key_off);
-                    if (*reinterpret_cast<volatile unsigned long long*>(flag) == 0 && atomicExch(flag, 1ull) == 0) {
-                        atomicAdd(sm.fresh, 1u);
-                    }
-                } else {
-                    int is_new = 0;
-                    gslot = GlobalFindH(D.T, D.cap_mask, h, key, is_new);
-                    if (is_new) atomicAdd(sm.fresh, 1u);
-                }
-                if (gslot < 0) {
-                    DeferTo(D, defer_base + r);    // replayed after the table grows
-                } else {
-                    ShapeAtomics<SH>(D.T.slots + gslot * D.T.slot_words + D.T.state_off, 1, v);
-                }
-            }
-        }
-        cur = nxt;
-        cur_sel = nxt_sel;
-        __syncwarp();   // the lanes' paths meet again before the next 32 rows
+    for (; r - lane < nrows; r += 2 * step) {
+        const int ra = r + 2 * step, rb = r + 3 * step;
+        RegRow<SH::Cols::n> na, nb;
+        LoadRow<SH>(na, cb, ra, ra < nrows);
+        LoadRow<SH>(nb, cb, rb, rb < nrows);
+        const bool nsa = ra < nrows && (!sel || sel[ra]);
+        const bool nsb = rb < nrows && (!sel || sel[rb]);
+        uint64_t ka = 0, ha = 0, kb = 0, hb = 0;
+        ShapeVals<SH> va, vb;
+        const bool ga = HighRowTier<SH>(P, F, D, sm, ca, sa, defer_base + r, ka, ha, va);
+        const bool gb = HighRowTier<SH>(P, F, D, sm, cbr, sb, defer_base + r + step, kb, hb, vb);
+        // Both rows' first probes before either is examined.
+        const uint64_t fa = ga ? *reinterpret_cast<volatile unsigned long long*>(
+                                     D.T.slots + int64_t(ha & D.cap_mask) * D.T.slot_words + D.T.key_off)
+                               : 0;
+        const uint64_t fb = gb ? *reinterpret_cast<volatile unsigned long long*>(
+                                     D.T.slots + int64_t(hb & D.cap_mask) * D.T.slot_words + D.T.key_off)
+                               : 0;
+        if (ga) HighRowGlobal<SH>(D, sm, ka, ha, fa, va, defer_base + r);
+        if (gb) HighRowGlobal<SH>(D, sm, kb, hb, fb, vb, defer_base + r + step);
+        ca = na;
+        cbr = nb;
+        sa = nsa;
+        sb = nsb;
+        __syncwarp();   // the lanes' paths meet again before the next rows
     }
 }
 
