@@ -316,6 +316,25 @@ class PlainServer:
         return latency_stats(stream, wall)
 
 
+class _DeviceExecutor:
+    """The serving loop's queries on the device: a CUDA stream per worker."""
+
+    def __init__(self, server: "BatchingServer"):
+        self.server = server
+
+    def bind(self) -> None:
+        _bind_stream()
+
+    def scratch(self) -> "Scratch":
+        return Scratch(self.server.max_sort_rows)
+
+    def one(self, table: Table, scratch: "Scratch"):
+        return run_query(self.server.progs, table, scratch, self.server.keep)
+
+    def batch(self, tables: list[Table]):
+        return run_agg_batch(self.server.progs, tables, self.server.keep)
+
+
 class BatchingServer:
     """Admission by HBM budget, continuous batching over worker streams and
     coalescing of small aggregations into one batched launch.  The workers
@@ -324,9 +343,13 @@ class BatchingServer:
 
     def __init__(self, progs: Programs, budget_bytes: int, resident_bytes: int, workers: int = 4,
                  small_rows: int = 8 << 20, max_batch: int = 16, max_sort_rows: int = 0,
-                 keep_results: bool = True):
+                 keep_results: bool = True, executor=None):
         self.progs = progs
         self.keep = keep_results
+        # What runs the queries: the device by default; tests of the loop's
+        # own logic give an executor with bind(), scratch(), one(table,
+        # scratch) and batch(tables).
+        self.executor = executor or _DeviceExecutor(self)
         self.max_sort_rows = max_sort_rows
         self.budget = budget_bytes
         self.resident = resident_bytes
@@ -396,9 +419,10 @@ class BatchingServer:
             self._cv.wait(timeout=0.05)
 
     def _worker(self) -> None:
+        ex = self.executor
         try:
-            _bind_stream()
-            scratch = Scratch(self.max_sort_rows)
+            ex.bind()
+            scratch = ex.scratch()
         except Exception as e:
             with self._cv:
                 self._error = e
@@ -411,9 +435,9 @@ class BatchingServer:
                 return
             try:
                 if len(group) > 1:
-                    results = run_agg_batch(self.progs, [y.table for y in group], self.keep)
+                    results = ex.batch([y.table for y in group])
                 else:
-                    results = [run_query(self.progs, group[0].table, scratch, self.keep)]
+                    results = [ex.one(group[0].table, scratch)]
             except Exception as e:
                 with self._cv:
                     self._error = e
