@@ -460,6 +460,9 @@ AggTableState* AggStateCreate(const AggPlan& p, int64_t capacity_hint, int64_t e
     auto* st = new AggTableState();
     st->s = s;
     st->expected = expected;
+    // A high-cardinality hint gets the larger shared tier (4096 slots: the
+    // more of a skewed stream's hot keys stay out of the global table).
+    if (expected > (int64_t(1) << 16)) st->smem_slots = 4096;
     int64_t cap = std::max<int64_t>(1024, NextPow2(std::max<int64_t>(capacity_hint, 1)));
     if (expected > 0) cap = std::max(cap, NextPow2(expected + expected / 2));
     st->hc = PinnedCountersGet();
