@@ -1082,8 +1082,9 @@ __device__ __forceinline__ void ShapeProduct(const FastPlan& F, const A& row, ui
 
 // Folds one row into its group's lane-private accumulators: p points at
 // word 0 of the group for this lane; word w lives at p[w * stride].
-template <class SH, int S = 0, class A>
-__device__ __forceinline__ void ShapeFoldP(uint64_t* p, int stride, const FastPlan& F, const A& row) {
+template <class SH, int STRIDE, int S = 0, class A>
+__device__ __forceinline__ void ShapeFoldP(uint64_t* p, const FastPlan& F, const A& row) {
+    constexpr int stride = STRIDE;   // compile time: every word is an immediate offset
     if constexpr (S < SH::n) {
         constexpr int K = SH::kind(S);
         constexpr int NF = SH::nf(S);
@@ -1100,7 +1101,7 @@ __device__ __forceinline__ void ShapeFoldP(uint64_t* p, int stride, const FastPl
         } else {
             p[O * stride] += lo;
         }
-        ShapeFoldP<SH, S + 1>(p, stride, F, row);
+        ShapeFoldP<SH, STRIDE, S + 1>(p, F, row);
     }
 }
 
@@ -1860,7 +1861,7 @@ __global__ void __launch_bounds__(kSigThreads, 1) AggSigDirectKernel(const __gri
                 }
             }
             if (g >= 0) {
-                ShapeFoldP<SIG>(pacc + int64_t(g) * SIG::words * bd + tid, bd, F, cur);
+                ShapeFoldP<SIG, kSigThreads>(pacc + g * SIG::words * kSigThreads + tid, F, cur);
             } else {
                 RowAcc acc{&P, nullptr, r, row0 + r, 0, -1, 0};
                 FoldRowFast<false>(L, acc);
