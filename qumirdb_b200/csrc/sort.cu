@@ -20,9 +20,10 @@
 // * a stage's first pass gathers its keys through the positions left by the
 //   previous stage; the last pass's positions gather the row ids.
 //
-// Top-K selects a threshold on the first key's order-preserving "primary"
-// key by 12-bit radix select (histogram passes), collects the rows at or
-// below it and orders only those exactly.
+// Top-K picks a threshold on the first key's order-preserving "primary" key
+// from an evenly spread sample (or, when the sample misses, by 12-bit radix
+// select over histogram passes), collects the rows at or below it in one
+// pass and orders only those exactly.
 #include <algorithm>
 
 #include "../../include/qdb_gpu.h"
@@ -342,14 +343,44 @@ __global__ void SortGatherIdsKernel(const int64_t* ids, const uint32_t* idx, int
     }
 }
 
-__global__ void SortMaxBatchKernel(const int64_t* ids, int64_t n, unsigned long long* out) {
+// Row ids per warp tile of the id scans: lane l holds positions
+// tile * kIdTile + u * 32 + l, u < kIdTile / 32.
+constexpr int kIdTile = kSortIdTile;
+
+// Largest batch index among the row ids.  With TILES, also marks every full
+// warp tile whose ids are consecutive rows of one batch: tiles[t] = its first
+// id, else -1.
+template <bool TILES>
+__global__ void __launch_bounds__(256) SortMaxBatchKernel(const int64_t* ids, int64_t n, unsigned long long* out,
+                                                          int64_t* tiles) {
+    constexpr int U = kIdTile / 32;
+    const int lane = LaneId();
+    const int64_t ntiles = (n + kIdTile - 1) / kIdTile;
+    const int64_t warps = int64_t(gridDim.x) * (blockDim.x / 32);
     unsigned long long m = 0;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        m = max(m, (unsigned long long)(uint64_t(ids[i]) >> 32));
+    for (int64_t t = int64_t(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32; t < ntiles; t += warps) {
+        const int64_t base = t * kIdTile;
+        int64_t v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t i = base + u * 32 + lane;
+            v[u] = i < n ? ids[i] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) m = max(m, (unsigned long long)(uint64_t(v[u]) >> 32));
+        if constexpr (TILES) {
+            const uint64_t first = uint64_t(__shfl_sync(kFull, v[0], 0));
+            bool dense = base + kIdTile <= n && int64_t(first) >= 0 &&
+                         uint64_t(uint32_t(first)) + (kIdTile - 1) <= 0xffffffffull;
+#pragma unroll
+            for (int u = 0; u < U; ++u) dense = dense && uint64_t(v[u]) == first + uint64_t(u * 32 + lane);
+            dense = __all_sync(kFull, dense);
+            if (lane == 0) tiles[t] = dense ? int64_t(first) : -1;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(kFull, m, o));
-    if (LaneId() == 0 && m) atomicMax(out, m);
+    if (lane == 0 && m) atomicMax(out, m);
 }
 
 struct MaterializeLaunch {
@@ -416,75 +447,372 @@ __global__ void __launch_bounds__(256) SortMaterializeKernel(const __grid_consta
 // ---------------------------------------------------------------------------
 constexpr int kTopKBins = 4096;
 
+// PrimaryKey of a loaded cell as straight-line arithmetic on constants the
+// host derives from the stage: k = raw ^ flip (integers; floats map their
+// bits), DESC xors all key bits, the key is left-aligned by lsh and, when
+// nullable, shifted down one bit under its NULL rank.
+struct KeyCodec {
+    uint64_t flip;
+    uint64_t dmask;
+    uint64_t rank_valid;   // bit 63 set when a valid cell's NULL rank is 1 (nullable keys)
+    uint64_t rank_null;
+    int32_t lsh;
+    int32_t nsh;
+};
+
 struct TopKLaunch {
     const int64_t* ids;
     int64_t n;
     StoreTable st;
     SortStage stage;
+    KeyCodec kc;
     int32_t shift;
     int32_t dbits;
-    uint64_t prefix;
-    int32_t prefix_bits;
-    int32_t pad;
+    uint64_t hmask;        // histogram: rows with (p & hmask) == hval
+    uint64_t hval;
+    uint64_t limit;        // collect: rows with p <= limit, or <= *limit_dev when set
+    const uint64_t* limit_dev;
     unsigned long long* counts;
     int64_t* out;
     int64_t out_cap;
+    const int64_t* tiles;  // dense-run marks of the ids (SortMaxBatch)
     int* err;
 };
 
-__device__ __forceinline__ bool UnderPrefix(uint64_t p, uint64_t prefix, int prefix_bits, bool le) {
-    if (prefix_bits == 0) return true;
-    const uint64_t top = p >> (64 - prefix_bits);
-    return le ? top <= prefix : top == prefix;
+__device__ __forceinline__ uint64_t F32Radix(uint64_t raw) {
+    uint32_t b = uint32_t(raw);
+    const uint32_t mag = b & 0x7fffffffu;
+    b = mag == 0 ? 0u : b;
+    const uint32_t k = (b >> 31) ? ~b : (b ^ 0x80000000u);
+    return mag > 0x7f800000u ? 0xffffffffu : k;
 }
 
+__device__ __forceinline__ uint64_t F64Radix(uint64_t b) {
+    const uint64_t mag = b & 0x7fffffffffffffffull;
+    b = mag == 0 ? 0ull : b;
+    const uint64_t k = (b >> 63) ? ~b : (b ^ (1ull << 63));
+    return mag > 0x7ff0000000000000ull ? ~0ull : k;
+}
+
+// PrimaryKey from a cell's validity and raw bits (zero extended); FLT: a
+// float cell of W bytes.
+template <int W, bool FLT>
+__device__ __forceinline__ uint64_t PrimaryOf(const KeyCodec& kc, bool valid, uint64_t raw) {
+    uint64_t k;
+    if constexpr (FLT) k = W == 4 ? F32Radix(raw) : F64Radix(raw);
+    else k = raw ^ kc.flip;
+    k = valid ? (k ^ kc.dmask) : 0;
+    return ((k << kc.lsh) >> kc.nsh) | (valid ? kc.rank_valid : kc.rank_null);
+}
+
+// Loads the cell of `row` from column data `d` (W bytes, 0 = one bit at
+// data_bit + row).
+template <int W>
+__device__ __forceinline__ uint64_t LoadCell(const char* d, int64_t data_bit, int64_t row) {
+    if constexpr (W == 0) return BitAt(reinterpret_cast<const uint8_t*>(d), data_bit + row);
+    if constexpr (W == 1) return reinterpret_cast<const uint8_t*>(d)[row];
+    if constexpr (W == 2) return reinterpret_cast<const uint16_t*>(d)[row];
+    if constexpr (W == 4) return reinterpret_cast<const uint32_t*>(d)[row];
+    if constexpr (W == 8) return reinterpret_cast<const uint64_t*>(d)[row];
+    return 0;
+}
+
+// PrimaryKey of U rows at once: every row's batch pointers, then every row's
+// validity bit, then every row's cell are loaded before any is used, so a
+// thread keeps U row fetches in flight instead of one dependent chain.  A
+// row id outside the store sets `bad` and reads nothing (key 0, NULL), as
+// CellRadix does; a NULL cell's data is not read.
+template <int W, bool FLT, int U>
+__device__ __forceinline__ void PrimaryKeys(const StoreTable& st, const SortStage& sg, const KeyCodec& kc,
+                                            const int64_t (&id)[U], const bool (&live)[U], uint64_t (&p)[U],
+                                            bool& bad) {
+    bool ok[U];
+    int64_t row[U], c[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const uint32_t batch = uint32_t(uint64_t(id[u]) >> 32);
+        ok[u] = live[u] && batch < uint32_t(st.nbatches);
+        bad = bad || (live[u] && !ok[u]);
+        row[u] = int64_t(uint32_t(uint64_t(id[u])));
+        c[u] = ok[u] ? int64_t(batch) * st.ncols + sg.tcol : 0;
+    }
+    const char* d[U];
+    const uint8_t* m[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        d[u] = ok[u] ? st.data[c[u]] : nullptr;
+        m[u] = ok[u] ? st.mask[c[u]] : nullptr;
+    }
+    bool valid[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) valid[u] = ok[u] && (m[u] == nullptr || BitAt(m[u], st.mask_bit[c[u]] + row[u]));
+    uint64_t raw[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) raw[u] = valid[u] ? LoadCell<W>(d[u], W == 0 ? st.data_bit[c[u]] : 0, row[u]) : 0;
+#pragma unroll
+    for (int u = 0; u < U; ++u) p[u] = PrimaryOf<W, FLT>(kc, valid[u], raw[u]);
+}
+
+// PrimaryKeys of the U rows a lane holds in a dense tile: rows
+// row0 + u * 32 + lane of the batch of `first`, whose pointers are looked up
+// once.  The caller has checked the batch.
+template <int W, bool FLT, int U>
+__device__ __forceinline__ void DenseKeys(const StoreTable& st, const SortStage& sg, const KeyCodec& kc,
+                                          int64_t first, int lane, uint64_t (&p)[U]) {
+    const int64_t c = int64_t(uint64_t(first) >> 32) * st.ncols + sg.tcol;
+    const int64_t row0 = int64_t(uint32_t(uint64_t(first))) + lane;
+    const char* d = st.data[c];
+    const uint8_t* m = st.mask[c];
+    const int64_t db = W == 0 ? st.data_bit[c] : 0;
+    uint64_t raw[U];
+    if (m == nullptr) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) raw[u] = LoadCell<W>(d, db, row0 + u * 32);
+#pragma unroll
+        for (int u = 0; u < U; ++u) p[u] = PrimaryOf<W, FLT>(kc, true, raw[u]);
+    } else {
+        const int64_t mb = st.mask_bit[c] + row0;
+        bool valid[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) valid[u] = BitAt(m, mb + u * 32);
+#pragma unroll
+        for (int u = 0; u < U; ++u) raw[u] = valid[u] ? LoadCell<W>(d, db, row0 + u * 32) : 0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) p[u] = PrimaryOf<W, FLT>(kc, valid[u], raw[u]);
+    }
+}
+
+// Rows per thread per step of the top-K passes.
+constexpr int kTopKUnroll = 4;
+
+// Row ids of one step: thread t takes rows base + u * blockDim.x + t.
+template <int U>
+__device__ __forceinline__ void TopKIds(const TopKLaunch& a, int64_t base, int64_t (&id)[U], bool (&live)[U]) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int64_t i = base + int64_t(u) * blockDim.x + threadIdx.x;
+        live[u] = i < a.n;
+        id[u] = live[u] ? a.ids[i] : 0;
+    }
+}
+
+template <int W, bool FLT>
 __global__ void __launch_bounds__(256) TopKHistogramKernel(const __grid_constant__ TopKLaunch a) {
+    constexpr int U = kTopKUnroll;
     __shared__ unsigned int sh[kTopKBins];
     for (int i = threadIdx.x; i < kTopKBins; i += blockDim.x) sh[i] = 0;
     __syncthreads();
     const int lane = LaneId();
     const uint64_t dmask = (1ull << a.dbits) - 1;
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < a.n; base += stride) {
-        const int64_t i = base + threadIdx.x;
-        bool in = false;
-        unsigned dig = 0;
-        if (i < a.n) {
-            const uint64_t p = PrimaryKey(a.st, a.stage, a.ids[i], a.err);
-            in = UnderPrefix(p, a.prefix, a.prefix_bits, false);
-            dig = unsigned((p >> a.shift) & dmask);
-        }
-        const unsigned act = __ballot_sync(kFull, in);
-        if (in) {
-            const unsigned peers = __match_any_sync(act, dig);
-            if (lane == __ffs(peers) - 1) atomicAdd(&sh[dig], unsigned(__popc(peers)));
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x * U;
+    bool bad = false;
+    for (int64_t base = int64_t(blockIdx.x) * blockDim.x * U; base < a.n; base += stride) {
+        int64_t id[U];
+        bool live[U];
+        uint64_t p[U];
+        TopKIds<U>(a, base, id, live);
+        PrimaryKeys<W, FLT, U>(a.st, a.stage, a.kc, id, live, p, bad);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const bool in = live[u] && (p[u] & a.hmask) == a.hval;
+            const unsigned dig = unsigned((p[u] >> a.shift) & dmask);
+            const unsigned act = __ballot_sync(kFull, in);
+            if (in) {
+                const unsigned peers = __match_any_sync(act, dig);
+                if (lane == __ffs(peers) - 1) atomicAdd(&sh[dig], unsigned(__popc(peers)));
+            }
         }
     }
+    if (bad) SetError(a.err, DE_BAD_ROW_ID);
     __syncthreads();
     for (int i = threadIdx.x; i < kTopKBins; i += blockDim.x) {
         if (sh[i]) atomicAdd(&a.counts[i], (unsigned long long)sh[i]);
     }
 }
 
-__global__ void __launch_bounds__(256) TopKCollectKernel(const __grid_constant__ TopKLaunch a) {
+// Appends the row ids of the lanes with `in` to a.out (first a.out_cap
+// slots) and counts them in *a.counts.
+__device__ __forceinline__ void TopKAppend(const TopKLaunch& a, bool in, int64_t id, int lane) {
+    const unsigned m = __ballot_sync(kFull, in);
+    if (m == 0) return;
+    unsigned long long at = 0;
+    if (lane == __ffs(m) - 1) at = atomicAdd(a.counts, (unsigned long long)__popc(m));
+    at = __shfl_sync(kFull, at, __ffs(m) - 1);
+    const unsigned long long slot = at + __popc(m & ((1u << lane) - 1u));
+    if (in && int64_t(slot) < a.out_cap) a.out[slot] = id;
+}
+
+// Collects the rows at or below the threshold, one warp tile of the ids at a
+// time.  A tile of consecutive rows of one batch (a.tiles) reads no ids and
+// looks its column up once, so each lane's U cells are independent loads;
+// the next tile's mark is loaded while this one's cells are in flight, and
+// a tile with no row at or below the threshold (nearly all of them) costs
+// one vote.  Any other tile takes the general fetch, H rows per lane at a
+// time.
+template <int W, bool FLT>
+__global__ void __launch_bounds__(256, 4) TopKCollectKernel(const __grid_constant__ TopKLaunch a) {
+    constexpr int U = kIdTile / 32;
+    constexpr int H = 2;
     const int lane = LaneId();
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < a.n; base += stride) {
-        const int64_t i = base + threadIdx.x;
-        bool in = false;
-        int64_t id = 0;
-        if (i < a.n) {
-            id = a.ids[i];
-            in = UnderPrefix(PrimaryKey(a.st, a.stage, id, a.err), a.prefix, a.prefix_bits, true);
+    const int64_t ntiles = (a.n + kIdTile - 1) / kIdTile;
+    const int64_t warps = int64_t(gridDim.x) * (blockDim.x / 32);
+    const uint64_t limit = a.limit_dev ? *a.limit_dev : a.limit;
+    bool bad = false;
+    int64_t t = int64_t(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32;
+    int64_t next = t < ntiles ? a.tiles[t] : -1;
+    for (; t < ntiles; t += warps) {
+        const int64_t first = next;
+        next = t + warps < ntiles ? a.tiles[t + warps] : -1;
+        if (first >= 0 && uint32_t(uint64_t(first) >> 32) < uint32_t(a.st.nbatches)) {
+            uint64_t p[U];
+            DenseKeys<W, FLT, U>(a.st, a.stage, a.kc, first, lane, p);
+            bool any = false;
+#pragma unroll
+            for (int u = 0; u < U; ++u) any = any || p[u] <= limit;
+            if (__any_sync(kFull, any)) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) TopKAppend(a, p[u] <= limit, first + u * 32 + lane, lane);
+            }
+        } else {
+#pragma unroll
+            for (int h = 0; h < U; h += H) {
+                int64_t id[H];
+                bool live[H];
+                uint64_t p[H];
+#pragma unroll
+                for (int u = 0; u < H; ++u) {
+                    const int64_t i = t * kIdTile + (h + u) * 32 + lane;
+                    live[u] = i < a.n;
+                    id[u] = live[u] ? a.ids[i] : 0;
+                }
+                PrimaryKeys<W, FLT, H>(a.st, a.stage, a.kc, id, live, p, bad);
+#pragma unroll
+                for (int u = 0; u < H; ++u) TopKAppend(a, live[u] && p[u] <= limit, id[u], lane);
+            }
         }
-        const unsigned m = __ballot_sync(kFull, in);
-        if (m == 0) continue;
-        unsigned long long at = 0;
-        if (lane == __ffs(m) - 1) at = atomicAdd(a.counts, (unsigned long long)__popc(m));
-        at = __shfl_sync(kFull, at, __ffs(m) - 1);
-        const unsigned long long slot = at + __popc(m & ((1u << lane) - 1u));
-        if (in && int64_t(slot) < a.out_cap) a.out[slot] = id;
     }
+    if (bad) SetError(a.err, DE_BAD_ROW_ID);
+}
+
+__global__ void TopKSampleKernel(const __grid_constant__ TopKLaunch a, uint64_t* keys, int64_t ns) {
+    const int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    keys[j] = PrimaryKey(a.st, a.stage, a.ids[j * a.n / ns], a.err);
+}
+
+// The r-th smallest (1-based) of keys[0, ns) into *out, by one block of
+// 1024 threads: eight rounds of an 8-bit radix select, most significant
+// digit first, each a shared histogram of the keys still under the prefix
+// and a one-warp scan for the digit holding the r-th key.
+__global__ void __launch_bounds__(1024) TopKSelectKernel(const uint64_t* keys, int64_t ns, int64_t r,
+                                                          uint64_t* out) {
+    __shared__ unsigned int hist[256];
+    __shared__ uint64_t s_prefix;
+    __shared__ unsigned long long s_need;
+    if (threadIdx.x == 0) {
+        s_prefix = 0;
+        s_need = (unsigned long long)r;
+    }
+    uint64_t mask = 0;
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        const uint64_t prefix = s_prefix;
+        for (int64_t i = threadIdx.x; i < ns; i += blockDim.x) {
+            const uint64_t k = keys[i];
+            if ((k & mask) == prefix) atomicAdd(&hist[(k >> shift) & 255], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            unsigned long long c[8], own = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                c[j] = hist[lane * 8 + j];
+                own += c[j];
+            }
+            unsigned long long incl = own;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long v = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const unsigned long long need = s_need;
+            const unsigned long long before = incl - own;
+            const unsigned hit = __ballot_sync(kFull, incl >= need);
+            if (hit && lane == __ffs(hit) - 1) {
+                unsigned long long run = before;
+                int j = 0;
+                for (; j < 7; ++j) {
+                    if (run + c[j] >= need) break;
+                    run += c[j];
+                }
+                s_need = need - run;
+                s_prefix = prefix | (uint64_t(lane * 8 + j) << shift);
+            }
+        }
+        mask |= 0xffull << shift;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s_prefix;
+}
+
+using TopKKernel = void (*)(const TopKLaunch);
+
+// Kernel instances for the first key's type: cell width, and float or not.
+TopKKernel TopKHistogramFor(int type) {
+    switch (type) {
+        case QDB_TYPE_F32: return TopKHistogramKernel<4, true>;
+        case QDB_TYPE_F64: return TopKHistogramKernel<8, true>;
+        default: break;
+    }
+    switch (SortKeyWidth(type)) {
+        case 0: return TopKHistogramKernel<0, false>;
+        case 1: return TopKHistogramKernel<1, false>;
+        case 2: return TopKHistogramKernel<2, false>;
+        case 4: return TopKHistogramKernel<4, false>;
+        case 8: return TopKHistogramKernel<8, false>;
+        default: return nullptr;
+    }
+}
+
+TopKKernel TopKCollectFor(int type) {
+    switch (type) {
+        case QDB_TYPE_F32: return TopKCollectKernel<4, true>;
+        case QDB_TYPE_F64: return TopKCollectKernel<8, true>;
+        default: break;
+    }
+    switch (SortKeyWidth(type)) {
+        case 0: return TopKCollectKernel<0, false>;
+        case 1: return TopKCollectKernel<1, false>;
+        case 2: return TopKCollectKernel<2, false>;
+        case 4: return TopKCollectKernel<4, false>;
+        case 8: return TopKCollectKernel<8, false>;
+        default: return nullptr;
+    }
+}
+
+// The codec of a stage's primary key (PrimaryKey's arithmetic).
+KeyCodec CodecOf(const SortStage& sg) {
+    KeyCodec kc{};
+    const int bits = SortKeyBits(sg.type);
+    switch (sg.type) {
+        case QDB_TYPE_I8: kc.flip = 0x80u; break;
+        case QDB_TYPE_I16: kc.flip = 0x8000u; break;
+        case QDB_TYPE_I32:
+        case QDB_TYPE_DATE32: kc.flip = 0x80000000u; break;
+        case QDB_TYPE_I64:
+        case QDB_TYPE_DECIMAL64: kc.flip = 1ull << 63; break;
+        default: kc.flip = 0; break;
+    }
+    kc.dmask = sg.desc ? (bits >= 64 ? ~0ull : ((1ull << bits) - 1)) : 0;
+    kc.lsh = 64 - bits;
+    kc.nsh = sg.nullable ? 1 : 0;
+    if (sg.nullable) {
+        kc.rank_valid = sg.nulls_first ? (1ull << 63) : 0;
+        kc.rank_null = sg.nulls_first ? 0 : (1ull << 63);
+    }
+    return kc;
 }
 
 int Blocks(int64_t n, int threads, int per_sm) {
@@ -556,10 +884,16 @@ void SortGatherIds(const int64_t* ids, const uint32_t* idx, int64_t n, int64_t* 
     CountLaunch();
 }
 
-void SortMaxBatch(const int64_t* ids, int64_t n, unsigned long long* out, cudaStream_t s) {
+void SortMaxBatch(const int64_t* ids, int64_t n, unsigned long long* out, int64_t* tiles, cudaStream_t s) {
     cudaMemsetAsync(out, 0, sizeof(unsigned long long), s);
     if (n == 0) return;
-    SortMaxBatchKernel<<<Blocks(n, 256, 8), 256, 0, s>>>(ids, n, out);
+    ProfileBegin(s, "sort_max_batch", n);
+    const int64_t threads = (n + kIdTile - 1) / kIdTile * 32;
+    if (tiles)
+        SortMaxBatchKernel<true><<<Blocks(threads, 256, 8), 256, 0, s>>>(ids, n, out, tiles);
+    else
+        SortMaxBatchKernel<false><<<Blocks(threads, 256, 8), 256, 0, s>>>(ids, n, out, nullptr);
+    ProfileEnd(s);
     CountLaunch();
 }
 
@@ -583,6 +917,25 @@ void SortMaterialize(const StoreTable& st, int tcol, int type, const int64_t* id
     CountLaunch();
 }
 
+void TopKThreshold(const int64_t* ids, int64_t n, const StoreTable& st, const SortStage& stage, uint64_t* keys,
+                   int64_t n_samples, int64_t r, uint64_t* out, int* err, cudaStream_t s) {
+    if (n == 0 || n_samples == 0) return;
+    TopKLaunch L{};
+    L.ids = ids;
+    L.n = n;
+    L.st = st;
+    L.stage = stage;
+    L.err = err;
+    ProfileBegin(s, "topk_sample", n_samples);
+    TopKSampleKernel<<<int((n_samples + 255) / 256), 256, 0, s>>>(L, keys, n_samples);
+    ProfileEnd(s);
+    CountLaunch();
+    ProfileBegin(s, "topk_select", n_samples);
+    TopKSelectKernel<<<1, 1024, 0, s>>>(keys, n_samples, r, out);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
 void TopKHistogram(const int64_t* ids, int64_t n, const StoreTable& st, const SortStage& stage, int shift,
                    int dbits, uint64_t prefix, int prefix_bits, unsigned long long* counts, int* err, cudaStream_t s) {
     cudaMemsetAsync(counts, 0, sizeof(unsigned long long) * kTopKBins, s);
@@ -592,21 +945,22 @@ void TopKHistogram(const int64_t* ids, int64_t n, const StoreTable& st, const So
     L.n = n;
     L.st = st;
     L.stage = stage;
+    L.kc = CodecOf(stage);
     L.shift = shift;
     L.dbits = dbits;
-    L.prefix = prefix;
-    L.prefix_bits = prefix_bits;
+    L.hmask = prefix_bits == 0 ? 0 : (~0ull << (64 - prefix_bits));
+    L.hval = prefix_bits == 0 ? 0 : (prefix << (64 - prefix_bits));
     L.counts = counts;
     L.err = err;
     ProfileBegin(s, "topk_histogram", n);
-    TopKHistogramKernel<<<Blocks(n, 256, 8), 256, 0, s>>>(L);
+    TopKHistogramFor(stage.type)<<<Blocks((n + kTopKUnroll - 1) / kTopKUnroll, 256, 4), 256, 0, s>>>(L);
     ProfileEnd(s);
     CountLaunch();
 }
 
 void TopKCollect(const int64_t* ids, int64_t n, const StoreTable& st, const SortStage& stage, uint64_t prefix,
-                 int prefix_bits, int64_t* out, int64_t out_cap, unsigned long long* count, int* err,
-                 cudaStream_t s) {
+                 int prefix_bits, const uint64_t* limit_dev, int64_t* out, int64_t out_cap,
+                 unsigned long long* count, const int64_t* tiles, int* err, cudaStream_t s) {
     cudaMemsetAsync(count, 0, sizeof(unsigned long long), s);
     if (n == 0) return;
     TopKLaunch L{};
@@ -614,14 +968,18 @@ void TopKCollect(const int64_t* ids, int64_t n, const StoreTable& st, const Sort
     L.n = n;
     L.st = st;
     L.stage = stage;
-    L.prefix = prefix;
-    L.prefix_bits = prefix_bits;
+    L.kc = CodecOf(stage);
+    // p >> (64 - prefix_bits) <= prefix  <=>  p <= prefix followed by ones.
+    L.limit = prefix_bits == 0 ? ~0ull
+                               : (prefix_bits == 64 ? prefix : ((prefix << (64 - prefix_bits)) | (~0ull >> prefix_bits)));
+    L.limit_dev = limit_dev;
     L.counts = count;
     L.out = out;
     L.out_cap = out_cap;
+    L.tiles = tiles;
     L.err = err;
     ProfileBegin(s, "topk_collect", n);
-    TopKCollectKernel<<<Blocks(n, 256, 8), 256, 0, s>>>(L);
+    TopKCollectFor(stage.type)<<<Blocks((n + kIdTile - 1) / kIdTile * 32, 256, 4), 256, 0, s>>>(L);
     ProfileEnd(s);
     CountLaunch();
 }

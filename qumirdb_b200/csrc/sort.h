@@ -70,8 +70,14 @@ void SortPass(bool wide, const void* keys_in, const uint32_t* idx_in, bool gathe
 // out[i] = ids[idx[i]].
 void SortGatherIds(const int64_t* ids, const uint32_t* idx, int64_t n, int64_t* out, cudaStream_t s);
 
-// Largest batch index among n row ids (written to *out, device).
-void SortMaxBatch(const int64_t* ids, int64_t n, unsigned long long* out, cudaStream_t s);
+// Row ids per tile of `SortMaxBatch`'s dense-run marks.
+constexpr int kSortIdTile = 256;
+
+// Largest batch index among n row ids (written to *out, device).  With
+// `tiles` (ceil(n / kSortIdTile) words), also marks each full tile of
+// kSortIdTile ids that are consecutive rows of one batch: tiles[t] = the
+// tile's first id, -1 for every other tile.
+void SortMaxBatch(const int64_t* ids, int64_t n, unsigned long long* out, int64_t* tiles, cudaStream_t s);
 
 // Materializes column slot `tcol` of the rows `ids[0, n)` into `out` (width
 // bytes per row; BOOL as one byte 0/1) and sets validity bits in `valid`
@@ -79,15 +85,36 @@ void SortMaxBatch(const int64_t* ids, int64_t n, unsigned long long* out, cudaSt
 void SortMaterialize(const StoreTable& st, int tcol, int type, const int64_t* ids, int64_t n, char* out,
                      uint32_t* valid, int* err, cudaStream_t s);
 
+// Bytes one cell of a sort key type occupies in its batch column (0: one bit,
+// BOOL; -1: not a sort key type).
+__host__ __device__ inline int SortKeyWidth(int type) {
+    switch (type) {
+        case 1: return 0;                              // BOOL
+        case 2: case 6: case 15: return 1;             // I8, U8, CHAR1
+        case 3: case 7: return 2;                      // I16, U16
+        case 4: case 8: case 10: case 12: return 4;    // I32, U32, F32, DATE32
+        case 5: case 9: case 11: case 13: return 8;    // I64, U64, F64, DECIMAL64
+        default: return -1;
+    }
+}
+
+// Primary keys of `n_samples` rows spread evenly over `ids` (the row id at
+// position j * n / n_samples) written to `keys`, and the r-th smallest of
+// them (1-based) to *out (device).
+void TopKThreshold(const int64_t* ids, int64_t n, const StoreTable& st, const SortStage& stage, uint64_t* keys,
+                   int64_t n_samples, int64_t r, uint64_t* out, int* err, cudaStream_t s);
+
 // Top-K radix select on the primary key of `stage`: counts (4096 bins) of
 // digit (p >> shift) & (2^dbits - 1) among rows whose top prefix_bits of p
 // equal `prefix` (all rows when prefix_bits == 0).
 void TopKHistogram(const int64_t* ids, int64_t n, const StoreTable& st, const SortStage& stage, int shift,
                    int dbits, uint64_t prefix, int prefix_bits, unsigned long long* counts, int* err, cudaStream_t s);
 // Appends every row id whose primary key p satisfies p >> (64 - prefix_bits)
-// <= prefix to `out` (at most out_cap rows written; the full count in *count).
+// <= prefix (p <= *limit_dev when limit_dev is set) to `out` (at most out_cap
+// rows written; the full count in *count).  `tiles`: SortMaxBatch's
+// dense-run marks of the same ids.
 void TopKCollect(const int64_t* ids, int64_t n, const StoreTable& st, const SortStage& stage, uint64_t prefix,
-                 int prefix_bits, int64_t* out, int64_t out_cap, unsigned long long* count, int* err,
-                 cudaStream_t s);
+                 int prefix_bits, const uint64_t* limit_dev, int64_t* out, int64_t out_cap,
+                 unsigned long long* count, const int64_t* tiles, int* err, cudaStream_t s);
 
 }  // namespace qdb

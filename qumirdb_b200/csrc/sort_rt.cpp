@@ -8,6 +8,7 @@
 // one.  Columns may live in host or device memory; host columns are staged
 // for the call.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -18,6 +19,9 @@
 namespace qdb {
 
 namespace {
+
+// Rows the top-K threshold is estimated from.
+constexpr int64_t kTopKSamples = 32768;
 
 // Device pointer tables of `cols` (store column indexes) over nbatches batches.
 struct StoreView {
@@ -101,10 +105,10 @@ struct Scratch {
 };
 
 // Number of batches the row ids touch (largest batch index + 1).
-bool BatchCount(const int64_t* ids, int64_t n, Scratch& sc, int64_t& nbatches) {
+bool BatchCount(const int64_t* ids, int64_t n, Scratch& sc, int64_t& nbatches, int64_t* tiles = nullptr) {
     auto* d = static_cast<unsigned long long*>(sc.Get(8));
     if (!d) return false;
-    SortMaxBatch(ids, n, d, sc.s);
+    SortMaxBatch(ids, n, d, tiles, sc.s);
     unsigned long long m = 0;
     cudaMemcpyAsync(&m, d, 8, cudaMemcpyDeviceToHost, sc.s);
     if (!CudaOk(cudaStreamSynchronize(sc.s), "sort: batch count")) return false;
@@ -420,8 +424,11 @@ int64_t qdb_gpu_top_k_select(const qdb_gpu_program* program, qdb_rowset* store, 
         if (!ids) return -1;
         cudaMemcpyAsync(ids, row_ids, size_t(size) * 8, cudaMemcpyHostToDevice, s);
     }
+    // Runs of consecutive rows (a scan's row ids) are fetched without their ids.
+    auto* tiles = static_cast<int64_t*>(sc.Get(size_t((size + kSortIdTile - 1) / kSortIdTile) * 8));
+    if (!tiles) return -1;
     int64_t nbatches = 0;
-    if (!BatchCount(ids, size, sc, nbatches)) return -1;
+    if (!BatchCount(ids, size, sc, nbatches, tiles)) return -1;
     StoreView v;
     // Exact order: row id first (the tie break, compiler.h:135-148), then the keys.
     const std::vector<SortStage> stages = MakeStages(prog->sort, nullptr, nullptr, true, v);
@@ -432,41 +439,79 @@ int64_t qdb_gpu_top_k_select(const qdb_gpu_program* program, qdb_rowset* store, 
     if (!derr || !counts) return -1;
     cudaMemsetAsync(derr, 0, sizeof(int), s);
 
+    if (SortKeyWidth(primary.type) < 0) {
+        SetErr("top-k: the first key's type is not a sort key type");
+        return -1;
+    }
+    const int64_t cap = std::max<int64_t>(4 * k, int64_t(1) << 20);
+    int64_t* cand = nullptr;
+    int64_t take = -1;
+
+    // Sampled threshold: the r-th smallest primary key of ns rows spread
+    // evenly over the input has about r * size / ns rows at or below it
+    // (spread sqrt(r) * size / ns).  r is chosen so that count is at least K
+    // with a margin of six spreads and is expected to fit the candidate
+    // buffer.  The sample, the selection of its r-th key and the pass that
+    // collects every row at or below it run back to back on the device; the
+    // host reads only the count.  The result is exact whatever the sample
+    // says: a count below K or above the buffer falls through to the radix
+    // select.
+    if (size > cap) {
+        const int64_t ns = std::min<int64_t>(kTopKSamples, size);
+        const double per = double(size) / double(ns);
+        const double mk = double(k) / per;
+        const int64_t r = int64_t(std::ceil(mk + 6.0 * std::sqrt(mk) + 8.0));
+        if (r <= ns && (double(r) + 6.0 * std::sqrt(double(r))) * per <= double(cap)) {
+            auto* skeys = static_cast<uint64_t*>(sc.Get(size_t(ns) * 8));
+            auto* tau = static_cast<uint64_t*>(sc.Get(8));
+            cand = static_cast<int64_t*>(sc.Get(size_t(cap) * 8));
+            auto* ccount = static_cast<unsigned long long*>(sc.Get(8));
+            if (!skeys || !tau || !cand || !ccount) return -1;
+            TopKThreshold(ids, size, v.t, primary, skeys, ns, r, tau, derr, s);
+            TopKCollect(ids, size, v.t, primary, 0, 64, tau, cand, cap, ccount, tiles, derr, s);
+            unsigned long long got = 0;
+            cudaMemcpyAsync(&got, ccount, 8, cudaMemcpyDeviceToHost, s);
+            if (!ReadError(derr, s, "top-k: collect")) return -1;
+            if (int64_t(got) >= k && int64_t(got) <= cap) take = int64_t(got);
+        }
+    }
+
     // Radix select on the primary key: narrow the bucket holding the K-th
     // row until the rows at or below it are few enough to order exactly.
-    const int64_t cap = std::max<int64_t>(4 * k, int64_t(1) << 20);
-    uint64_t prefix = 0;
-    int pbits = 0;
-    int64_t below = 0;
-    int64_t take = size;
-    std::vector<unsigned long long> h(4096);
-    while (pbits < 64) {
-        const int dbits = std::min(12, 64 - pbits);
-        TopKHistogram(ids, size, v.t, primary, 64 - pbits - dbits, dbits, prefix, pbits, counts, derr, s);
-        cudaMemcpyAsync(h.data(), counts, 4096 * 8, cudaMemcpyDeviceToHost, s);
-        if (!ReadError(derr, s, "top-k: histogram")) return -1;
-        int64_t run = below;
-        int b = 0;
-        for (; b < (1 << dbits) - 1; ++b) {
-            if (run + int64_t(h[b]) >= k) break;
-            run += int64_t(h[b]);
+    if (take < 0) {
+        uint64_t prefix = 0;
+        int pbits = 0;
+        int64_t below = 0;
+        take = size;
+        std::vector<unsigned long long> h(4096);
+        while (pbits < 64) {
+            const int dbits = std::min(12, 64 - pbits);
+            TopKHistogram(ids, size, v.t, primary, 64 - pbits - dbits, dbits, prefix, pbits, counts, derr, s);
+            cudaMemcpyAsync(h.data(), counts, 4096 * 8, cudaMemcpyDeviceToHost, s);
+            if (!ReadError(derr, s, "top-k: histogram")) return -1;
+            int64_t run = below;
+            int b = 0;
+            for (; b < (1 << dbits) - 1; ++b) {
+                if (run + int64_t(h[b]) >= k) break;
+                run += int64_t(h[b]);
+            }
+            below = run;
+            prefix = (prefix << dbits) | uint64_t(b);
+            pbits += dbits;
+            take = below + int64_t(h[b]);
+            if (take <= cap) break;
         }
-        below = run;
-        prefix = (prefix << dbits) | uint64_t(b);
-        pbits += dbits;
-        take = below + int64_t(h[b]);
-        if (take <= cap) break;
-    }
-    int64_t* cand = static_cast<int64_t*>(sc.Get(size_t(take) * 8));
-    auto* ccount = static_cast<unsigned long long*>(sc.Get(8));
-    if (!cand || !ccount) return -1;
-    TopKCollect(ids, size, v.t, primary, prefix, pbits, cand, take, ccount, derr, s);
-    unsigned long long got = 0;
-    cudaMemcpyAsync(&got, ccount, 8, cudaMemcpyDeviceToHost, s);
-    if (!ReadError(derr, s, "top-k: collect")) return -1;
-    if (int64_t(got) != take) {
-        SetErr("top-k: collected %llu rows, expected %lld", got, (long long)take);
-        return -1;
+        if (!cand || take > cap) cand = static_cast<int64_t*>(sc.Get(size_t(take) * 8));
+        auto* ccount = static_cast<unsigned long long*>(sc.Get(8));
+        if (!cand || !ccount) return -1;
+        TopKCollect(ids, size, v.t, primary, prefix, pbits, nullptr, cand, take, ccount, tiles, derr, s);
+        unsigned long long got = 0;
+        cudaMemcpyAsync(&got, ccount, 8, cudaMemcpyDeviceToHost, s);
+        if (!ReadError(derr, s, "top-k: collect")) return -1;
+        if (int64_t(got) != take) {
+            SetErr("top-k: collected %llu rows, expected %lld", got, (long long)take);
+            return -1;
+        }
     }
     if (!SortIds(cand, take, stages, v.t, sc)) return -1;
     cudaMemcpyAsync(row_ids, cand, size_t(k) * 8, dev_ids ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);

@@ -225,3 +225,49 @@ def test_sort_50m_rows_order_property():
     assert (d2[same1] >= 0).all()
     same2 = same1 & (d2 == 0)
     assert (np.diff(pos)[same2] > 0).all()
+
+
+@pytest.mark.parametrize("case,k,desc", [("random", 1000, 0), ("random", 5000, 1), ("random", 300_000, 0),
+                                         ("by_position", 1000, 0), ("by_position", 777, 1),
+                                         ("three_values", 1000, 0), ("two_values", 1000, 0)])
+def test_top_k_sampled_threshold(case, k, desc):
+    """Inputs above the candidate buffer (3M rows): the threshold comes from
+    an evenly spread sample; keys ordered by position, and ties so heavy that
+    the rows at or below the sampled threshold overflow the buffer (the radix
+    select takes over), give the same rows as the oracle."""
+    n = 3_000_000
+    rng = np.random.default_rng(41)
+    if case == "random":
+        k1 = rng.integers(-2**63, 2**63 - 1, n, dtype=np.int64)
+    elif case == "by_position":
+        k1 = np.arange(n, dtype=np.int64) * 3 - 10**6
+    else:
+        k1 = rng.integers(0, 3 if case == "three_values" else 2, n, dtype=np.int64)
+    cols = [k1, rng.integers(0, 100_000, n, dtype=np.int32), np.arange(n, dtype=np.int64)]
+    sizes = [1 << 20, 1 << 20, n - 2 * (1 << 20)]
+    spec = queries.SortSpec(queries.SORT_COLUMNS, [(0, desc, 0), (1, 0, 0)])
+    prog = q.compile_sort(spec)
+    ids = packed_ids(sizes)
+    want = O.top_k(spec, split(cols, sizes), ids, k)
+    dids = q.DeviceBuffer(ids.nbytes).upload(ids)
+    kk = q.Sort(prog, split(cols, sizes, device=True)).top_k(dids, k)
+    assert kk == k
+    assert np.array_equal(dids.download(np.int64, kk), want)
+
+
+def test_top_k_sampled_key_types():
+    """The sampled path over every cell width (1, 2, 4 and 8 bytes), nullable
+    keys with NULLs first and last, both directions."""
+    n = 2_500_000
+    cols, types, masks, _ = typed_columns(n, 43)
+    sizes = [n // 2, n - n // 2]
+    ids = packed_ids(sizes)
+    host, dev = split(cols, sizes, masks), split(cols, sizes, masks, device=True)
+    for key, desc, first, k in ((4, 0, 1, 1000), (4, 1, 0, 20_000), (0, 0, 0, 1000), (1, 1, 0, 3000),
+                                (3, 0, 1, 1000), (5, 1, 0, 1000), (9, 0, 0, 100), (6, 1, 0, 1000)):
+        spec = queries.SortSpec(types, [(key, desc, first), (8, 1, 0)])
+        prog = q.compile_sort(spec)
+        want = O.top_k(spec, host, ids, k)
+        got = ids.copy()
+        kk = q.Sort(prog, dev).top_k(got, k)
+        assert np.array_equal(got[:kk], want), (key, desc, first, k)
