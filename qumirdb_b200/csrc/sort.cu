@@ -37,6 +37,23 @@ namespace {
 
 __device__ __forceinline__ bool BitAt(const uint8_t* m, int64_t bit) { return (m[bit >> 3] >> (bit & 7)) & 1; }
 
+// Order-preserving images of float bits (NaN above every number, -0 == +0).
+__device__ __forceinline__ uint64_t F32Radix(uint64_t raw) {
+    uint32_t b = uint32_t(raw);
+    const uint32_t mag = b & 0x7fffffffu;
+    b = mag == 0 ? 0u : b;
+    const uint32_t k = (b >> 31) ? ~b : (b ^ 0x80000000u);
+    return mag > 0x7f800000u ? 0xffffffffu : k;
+}
+
+__device__ __forceinline__ uint64_t F64Radix(uint64_t b) {
+    const uint64_t mag = b & 0x7fffffffffffffffull;
+    b = mag == 0 ? 0ull : b;
+    const uint64_t k = (b >> 63) ? ~b : (b ^ (1ull << 63));
+    return mag > 0x7ff0000000000000ull ? ~0ull : k;
+}
+
+
 // Order-preserving unsigned key of a cell (qumir_radix_key,
 // qdb/kernel/sort/radix.oz:4-64): signed integers flip the sign bit; floats
 // order as PostgreSQL does (NaN above every number, -0 == +0).  Returns false
@@ -96,19 +113,6 @@ __device__ __forceinline__ bool CellRadix(const StoreTable& st, int tcol, int ty
 
 __device__ __forceinline__ uint64_t KeyMask(int bits) { return bits >= 64 ? ~0ull : ((1ull << bits) - 1); }
 
-// The key one stage sorts on.
-__device__ __forceinline__ uint64_t StageKey(const StoreTable& st, const SortStage& sg, int64_t id, int* err) {
-    if (sg.src == SS_ROW_ID) return uint64_t(id);
-    uint64_t k;
-    const bool valid = CellRadix(st, sg.tcol, sg.type, id, k, err);
-    const uint64_t rank = sg.nulls_first ? (valid ? 1 : 0) : (valid ? 0 : 1);
-    if (sg.src == SS_NULL_RANK) return rank;
-    const int bits = SortKeyBits(sg.type);
-    if (valid && sg.desc) k = ~k & KeyMask(bits);
-    if (sg.nullable && bits <= 32) k |= rank << 32;
-    return k;
-}
-
 // First-key primary order for top-K: the stage key left-aligned to 64 bits
 // with the NULL rank on top.  Non-decreasing along the true order, so the
 // rows at or below the K-th smallest primary key contain the true top K.
@@ -126,6 +130,32 @@ __device__ __forceinline__ uint64_t PrimaryKey(const StoreTable& st, const SortS
 // ---------------------------------------------------------------------------
 // Extraction + upfront histograms.
 // ---------------------------------------------------------------------------
+// Loads the cell of `row` from column data `d` (W bytes, 0 = one bit at
+// data_bit + row).
+template <int W>
+__device__ __forceinline__ uint64_t LoadCell(const char* d, int64_t data_bit, int64_t row) {
+    if constexpr (W == 0) return BitAt(reinterpret_cast<const uint8_t*>(d), data_bit + row);
+    if constexpr (W == 1) return reinterpret_cast<const uint8_t*>(d)[row];
+    if constexpr (W == 2) return reinterpret_cast<const uint16_t*>(d)[row];
+    if constexpr (W == 4) return reinterpret_cast<const uint32_t*>(d)[row];
+    if constexpr (W == 8) return reinterpret_cast<const uint64_t*>(d)[row];
+    return 0;
+}
+
+// StageKey arithmetic on host-derived constants: a key stage is
+// valid ? (image ^ dmask) | rank_valid : rank_null, where the image is the
+// cell's bits ^ flip (or a float image), dmask inverts the key bits for DESC
+// and the rank words carry the NULL rank above keys of <= 32 bits; a NULL-rank
+// stage is rank_valid / rank_null alone; a row-id stage is the id.
+struct StageCodec {
+    uint64_t flip;
+    uint64_t dmask;
+    uint64_t rank_valid;
+    uint64_t rank_null;
+    int32_t width;   // cell bytes, 0 = one bit
+    int32_t flt;     // 0: integer image, 4: F32, 8: F64
+};
+
 struct ExtractLaunch {
     const int64_t* ids;
     int64_t n;
@@ -133,44 +163,132 @@ struct ExtractLaunch {
     int32_t nstages;
     int32_t pad;
     SortStage stages[kMaxSortStages];
+    StageCodec codec[kMaxSortStages];
     void* keys[kMaxSortStages];
     unsigned long long* hist;
     int* err;
 };
 
 constexpr int kExtractThreads = 256;
+constexpr int kExtractUnroll = 4;
+
+template <int W, int U>
+__device__ __forceinline__ void LoadCells(const char* const (&d)[U], const int64_t (&db)[U], const int64_t (&row)[U],
+                                          const bool (&valid)[U], uint64_t (&raw)[U]) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) raw[u] = valid[u] ? LoadCell<W>(d[u], db[u], row[u]) : 0;
+}
+
+// The stage keys of U rows: every row's batch pointers, validity bits and
+// cells are loaded before any is used.  A row id outside the store sets
+// `bad` and reads nothing (key of a NULL), as CellRadix does.
+template <int U>
+__device__ __forceinline__ void StageKeys(const StoreTable& st, const SortStage& sg, const StageCodec& sc,
+                                          const int64_t (&id)[U], const bool (&live)[U], uint64_t (&k)[U],
+                                          bool& bad) {
+    if (sg.src == SS_ROW_ID) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) k[u] = uint64_t(id[u]);
+        return;
+    }
+    bool valid[U];
+    int64_t row[U], c[U], db[U];
+    const char* d[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const uint32_t batch = uint32_t(uint64_t(id[u]) >> 32);
+        const bool ok = live[u] && batch < uint32_t(st.nbatches);
+        bad = bad || (live[u] && !ok);
+        row[u] = int64_t(uint32_t(uint64_t(id[u])));
+        c[u] = ok ? int64_t(batch) * st.ncols + sg.tcol : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const uint8_t* m = c[u] >= 0 ? st.mask[c[u]] : nullptr;
+        valid[u] = c[u] >= 0 && (m == nullptr || BitAt(m, st.mask_bit[c[u]] + row[u]));
+        d[u] = c[u] >= 0 ? st.data[c[u]] : nullptr;
+        db[u] = (sc.width == 0 && c[u] >= 0) ? st.data_bit[c[u]] : 0;
+    }
+    uint64_t raw[U];
+    if (sg.src == SS_NULL_RANK) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) k[u] = valid[u] ? sc.rank_valid : sc.rank_null;
+        return;
+    }
+    switch (sc.width) {
+        case 0: LoadCells<0, U>(d, db, row, valid, raw); break;
+        case 1: LoadCells<1, U>(d, db, row, valid, raw); break;
+        case 2: LoadCells<2, U>(d, db, row, valid, raw); break;
+        case 4: LoadCells<4, U>(d, db, row, valid, raw); break;
+        default: LoadCells<8, U>(d, db, row, valid, raw); break;
+    }
+    if (sc.flt == 4) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) raw[u] = F32Radix(raw[u]);
+    } else if (sc.flt == 8) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) raw[u] = F64Radix(raw[u]);
+    } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) raw[u] ^= sc.flip;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) k[u] = valid[u] ? ((raw[u] ^ sc.dmask) | sc.rank_valid) : sc.rank_null;
+}
+
+// One row's digit into a shared histogram: a warp whose live lanes share the
+// digit (constant high digits) adds once, otherwise each lane adds its own.
+__device__ __forceinline__ void HistAdd(unsigned int* bins, unsigned dig, bool live, unsigned act, int lane) {
+    const int lead = __ffs(act) - 1;
+    const unsigned d0 = __shfl_sync(kFull, dig, lead);
+    if (__all_sync(kFull, !live || dig == d0)) {
+        if (lane == lead) atomicAdd(&bins[d0], unsigned(__popc(act)));
+    } else if (live) {
+        atomicAdd(&bins[dig], 1u);
+    }
+}
 
 __global__ void __launch_bounds__(kExtractThreads) SortExtractKernel(const __grid_constant__ ExtractLaunch a) {
+    constexpr int U = kExtractUnroll;
     extern __shared__ unsigned int sh[];   // nstages * kSortDigits * 256
     const int nh = a.nstages * kSortDigits * 256;
     for (int i = threadIdx.x; i < nh; i += blockDim.x) sh[i] = 0;
     __syncthreads();
     const int lane = LaneId();
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < a.n; base += stride) {
-        const int64_t i = base + threadIdx.x;
-        const bool ok = i < a.n;
-        const unsigned act = __ballot_sync(kFull, ok);
-        const int64_t id = ok ? a.ids[i] : 0;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x * U;
+    bool bad = false;
+    for (int64_t base = int64_t(blockIdx.x) * blockDim.x * U; base < a.n; base += stride) {
+        int64_t id[U];
+        bool live[U];
+        unsigned act[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t i = base + int64_t(u) * blockDim.x + threadIdx.x;
+            live[u] = i < a.n;
+            id[u] = live[u] ? a.ids[i] : 0;
+            act[u] = __ballot_sync(kFull, live[u]);
+        }
         for (int s = 0; s < a.nstages; ++s) {
             const SortStage& sg = a.stages[s];
-            const uint64_t k = ok ? StageKey(a.st, sg, id, a.err) : 0;
-            if (ok) {
-                if (sg.wide) static_cast<uint64_t*>(a.keys[s])[i] = k;
-                else static_cast<uint32_t*>(a.keys[s])[i] = uint32_t(k);
+            uint64_t k[U];
+            StageKeys<U>(a.st, sg, a.codec[s], id, live, k, bad);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (!live[u]) continue;
+                const int64_t i = base + int64_t(u) * blockDim.x + threadIdx.x;
+                if (sg.wide) static_cast<uint64_t*>(a.keys[s])[i] = k[u];
+                else static_cast<uint32_t*>(a.keys[s])[i] = uint32_t(k[u]);
             }
             const int nd = sg.wide ? 8 : 4;
-            if (ok) {
-                for (int d = 0; d < nd; ++d) {
-                    const unsigned dig = unsigned(k >> (8 * d)) & 255u;
-                    const unsigned peers = __match_any_sync(act, dig);
-                    if (lane == __ffs(peers) - 1) {
-                        atomicAdd(&sh[(s * kSortDigits + d) * 256 + dig], unsigned(__popc(peers)));
-                    }
-                }
+            unsigned int* hs = sh + s * kSortDigits * 256;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (act[u] == 0) continue;
+                for (int dg = 0; dg < nd; ++dg) HistAdd(hs + dg * 256, unsigned(k[u] >> (8 * dg)) & 255u, live[u], act[u], lane);
             }
         }
     }
+    if (bad) SetError(a.err, DE_BAD_ROW_ID);
     __syncthreads();
     for (int i = threadIdx.x; i < nh; i += blockDim.x) {
         if (sh[i]) atomicAdd(&a.hist[i], (unsigned long long)sh[i]);
@@ -244,15 +362,21 @@ __global__ void __launch_bounds__(kPassThreads, 2) SortPassKernel(const __grid_c
         key[j] = ok ? (a.gather ? a.keys_in[idx[j]] : a.keys_in[p]) : K(0);
     }
     // Stable rank of every key among the equal digits of its warp's segment.
+    // The lanes sharing a digit come from one ballot per digit bit.
 #pragma unroll
     for (int j = 0; j < kPassItems; ++j) {
         const int lp = w * (32 * kPassItems) + j * 32 + lane;
         const bool ok = lp < tile_n;
+        const unsigned d = unsigned(uint64_t(key[j]) >> a.shift) & 255u;
         const unsigned act = __ballot_sync(kFull, ok);
+        unsigned peers = act;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const unsigned set = __ballot_sync(kFull, (d >> b) & 1u);
+            peers &= ((d >> b) & 1u) ? set : ~set;
+        }
         rank[j] = 0;
         if (ok) {
-            const unsigned d = unsigned(uint64_t(key[j]) >> a.shift) & 255u;
-            const unsigned peers = __match_any_sync(act, d);
             const int leader = __ffs(peers) - 1;
             uint32_t old = 0;
             if (lane == leader) {
@@ -337,9 +461,45 @@ __global__ void __launch_bounds__(kPassThreads, 2) SortPassKernel(const __grid_c
     }
 }
 
-__global__ void SortGatherIdsKernel(const int64_t* ids, const uint32_t* idx, int64_t n, int64_t* out) {
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        out[i] = ids[idx[i]];
+// out[i] = ids[idx[i]], four rows per thread per step with every position
+// and then every id load in flight together.  With `tiles` (dense-run marks
+// of ids), an id in a dense tile is its tile's first id plus its offset; ids
+// is read only for the other tiles (and may be null when there are none).
+__global__ void __launch_bounds__(256) SortGatherIdsKernel(const int64_t* ids, const uint32_t* idx, int64_t n,
+                                                           const int64_t* tiles, int64_t* out) {
+    constexpr int U = 4;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x * U;
+    for (int64_t base = int64_t(blockIdx.x) * blockDim.x * U; base < n; base += stride) {
+        uint32_t pos[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t i = base + int64_t(u) * blockDim.x + threadIdx.x;
+            pos[u] = i < n ? idx[i] : 0;
+        }
+        int64_t v[U];
+        if (tiles) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int64_t i = base + int64_t(u) * blockDim.x + threadIdx.x;
+                v[u] = i < n ? tiles[pos[u] / kSortIdTile] : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int64_t i = base + int64_t(u) * blockDim.x + threadIdx.x;
+                if (i < n) v[u] = v[u] >= 0 ? v[u] + int64_t(pos[u] % kSortIdTile) : ids[pos[u]];
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int64_t i = base + int64_t(u) * blockDim.x + threadIdx.x;
+                v[u] = i < n ? ids[pos[u]] : 0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t i = base + int64_t(u) * blockDim.x + threadIdx.x;
+            if (i < n) out[i] = v[u];
+        }
     }
 }
 
@@ -357,7 +517,7 @@ __global__ void __launch_bounds__(256) SortMaxBatchKernel(const int64_t* ids, in
     const int lane = LaneId();
     const int64_t ntiles = (n + kIdTile - 1) / kIdTile;
     const int64_t warps = int64_t(gridDim.x) * (blockDim.x / 32);
-    unsigned long long m = 0;
+    unsigned long long m = 0, sparse = 0;
     for (int64_t t = int64_t(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32; t < ntiles; t += warps) {
         const int64_t base = t * kIdTile;
         int64_t v[U];
@@ -376,11 +536,13 @@ __global__ void __launch_bounds__(256) SortMaxBatchKernel(const int64_t* ids, in
             for (int u = 0; u < U; ++u) dense = dense && uint64_t(v[u]) == first + uint64_t(u * 32 + lane);
             dense = __all_sync(kFull, dense);
             if (lane == 0) tiles[t] = dense ? int64_t(first) : -1;
+            sparse += dense ? 0 : 1;
         }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(kFull, m, o));
     if (lane == 0 && m) atomicMax(out, m);
+    if (TILES && lane == 0 && sparse) atomicAdd(out + 1, sparse);
 }
 
 struct MaterializeLaunch {
@@ -479,21 +641,6 @@ struct TopKLaunch {
     int* err;
 };
 
-__device__ __forceinline__ uint64_t F32Radix(uint64_t raw) {
-    uint32_t b = uint32_t(raw);
-    const uint32_t mag = b & 0x7fffffffu;
-    b = mag == 0 ? 0u : b;
-    const uint32_t k = (b >> 31) ? ~b : (b ^ 0x80000000u);
-    return mag > 0x7f800000u ? 0xffffffffu : k;
-}
-
-__device__ __forceinline__ uint64_t F64Radix(uint64_t b) {
-    const uint64_t mag = b & 0x7fffffffffffffffull;
-    b = mag == 0 ? 0ull : b;
-    const uint64_t k = (b >> 63) ? ~b : (b ^ (1ull << 63));
-    return mag > 0x7ff0000000000000ull ? ~0ull : k;
-}
-
 // PrimaryKey from a cell's validity and raw bits (zero extended); FLT: a
 // float cell of W bytes.
 template <int W, bool FLT>
@@ -503,18 +650,6 @@ __device__ __forceinline__ uint64_t PrimaryOf(const KeyCodec& kc, bool valid, ui
     else k = raw ^ kc.flip;
     k = valid ? (k ^ kc.dmask) : 0;
     return ((k << kc.lsh) >> kc.nsh) | (valid ? kc.rank_valid : kc.rank_null);
-}
-
-// Loads the cell of `row` from column data `d` (W bytes, 0 = one bit at
-// data_bit + row).
-template <int W>
-__device__ __forceinline__ uint64_t LoadCell(const char* d, int64_t data_bit, int64_t row) {
-    if constexpr (W == 0) return BitAt(reinterpret_cast<const uint8_t*>(d), data_bit + row);
-    if constexpr (W == 1) return reinterpret_cast<const uint8_t*>(d)[row];
-    if constexpr (W == 2) return reinterpret_cast<const uint16_t*>(d)[row];
-    if constexpr (W == 4) return reinterpret_cast<const uint32_t*>(d)[row];
-    if constexpr (W == 8) return reinterpret_cast<const uint64_t*>(d)[row];
-    return 0;
 }
 
 // PrimaryKey of U rows at once: every row's batch pointers, then every row's
@@ -815,6 +950,33 @@ KeyCodec CodecOf(const SortStage& sg) {
     return kc;
 }
 
+// The codec of a stage (StageKey's arithmetic).
+StageCodec StageCodecOf(const SortStage& sg) {
+    StageCodec c{};
+    const int bits = SortKeyBits(sg.type);
+    c.width = SortKeyWidth(sg.type) < 0 ? 8 : SortKeyWidth(sg.type);
+    c.flt = sg.type == QDB_TYPE_F32 ? 4 : (sg.type == QDB_TYPE_F64 ? 8 : 0);
+    switch (sg.type) {
+        case QDB_TYPE_I8: c.flip = 0x80u; break;
+        case QDB_TYPE_I16: c.flip = 0x8000u; break;
+        case QDB_TYPE_I32:
+        case QDB_TYPE_DATE32: c.flip = 0x80000000u; break;
+        case QDB_TYPE_I64:
+        case QDB_TYPE_DECIMAL64: c.flip = 1ull << 63; break;
+        default: c.flip = 0; break;
+    }
+    c.dmask = sg.desc ? (bits >= 64 ? ~0ull : ((1ull << bits) - 1)) : 0;
+    const uint64_t rv = sg.nulls_first ? 1 : 0, rn = sg.nulls_first ? 0 : 1;
+    if (sg.src == SS_NULL_RANK) {
+        c.rank_valid = rv;
+        c.rank_null = rn;
+    } else if (sg.nullable && bits <= 32) {
+        c.rank_valid = rv << 32;
+        c.rank_null = rn << 32;
+    }
+    return c;
+}
+
 int Blocks(int64_t n, int threads, int per_sm) {
     return int(std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, int64_t(DeviceSMs()) * per_sm)));
 }
@@ -832,6 +994,7 @@ void SortExtract(const int64_t* ids, int64_t n, const StoreTable& st, const Sort
     L.nstages = nstages;
     for (int i = 0; i < nstages; ++i) {
         L.stages[i] = stages[i];
+        L.codec[i] = StageCodecOf(stages[i]);
         L.keys[i] = keys[i];
     }
     L.hist = hist;
@@ -839,7 +1002,8 @@ void SortExtract(const int64_t* ids, int64_t n, const StoreTable& st, const Sort
     const size_t smem = size_t(nstages) * kSortDigits * 256 * 4;
     EnsureSmemLimit(reinterpret_cast<const void*>(SortExtractKernel), smem);
     ProfileBegin(s, "sort_extract", n);
-    SortExtractKernel<<<Blocks(n, kExtractThreads, 4), kExtractThreads, smem, s>>>(L);
+    SortExtractKernel<<<Blocks((n + kExtractUnroll - 1) / kExtractUnroll, kExtractThreads, 4), kExtractThreads, smem,
+                        s>>>(L);
     ProfileEnd(s);
     CountLaunch();
 }
@@ -876,16 +1040,17 @@ void SortPass(bool wide, const void* keys_in, const uint32_t* idx_in, bool gathe
     else launch(uint32_t{});
 }
 
-void SortGatherIds(const int64_t* ids, const uint32_t* idx, int64_t n, int64_t* out, cudaStream_t s) {
+void SortGatherIds(const int64_t* ids, const uint32_t* idx, int64_t n, const int64_t* tiles, int64_t* out,
+                   cudaStream_t s) {
     if (n == 0) return;
     ProfileBegin(s, "sort_gather_ids", n);
-    SortGatherIdsKernel<<<Blocks(n, 256, 8), 256, 0, s>>>(ids, idx, n, out);
+    SortGatherIdsKernel<<<Blocks((n + 3) / 4, 256, 8), 256, 0, s>>>(ids, idx, n, tiles, out);
     ProfileEnd(s);
     CountLaunch();
 }
 
 void SortMaxBatch(const int64_t* ids, int64_t n, unsigned long long* out, int64_t* tiles, cudaStream_t s) {
-    cudaMemsetAsync(out, 0, sizeof(unsigned long long), s);
+    cudaMemsetAsync(out, 0, sizeof(unsigned long long) * (tiles ? 2 : 1), s);
     if (n == 0) return;
     ProfileBegin(s, "sort_max_batch", n);
     const int64_t threads = (n + kIdTile - 1) / kIdTile * 32;

@@ -67,16 +67,20 @@ void SortPass(bool wide, const void* keys_in, const uint32_t* idx_in, bool gathe
               int64_t n, int shift, const unsigned long long* bucket_base, unsigned long long* status, uint32_t epoch,
               unsigned int* tile_counter, int* err, cudaStream_t s);
 
-// out[i] = ids[idx[i]].
-void SortGatherIds(const int64_t* ids, const uint32_t* idx, int64_t n, int64_t* out, cudaStream_t s);
+// out[i] = ids[idx[i]].  With `tiles` (SortMaxBatch's dense-run marks of
+// ids), ids in dense tiles are computed from the marks; ids may then be null
+// when every tile is dense.
+void SortGatherIds(const int64_t* ids, const uint32_t* idx, int64_t n, const int64_t* tiles, int64_t* out,
+                   cudaStream_t s);
 
 // Row ids per tile of `SortMaxBatch`'s dense-run marks.
 constexpr int kSortIdTile = 256;
 
-// Largest batch index among n row ids (written to *out, device).  With
+// Largest batch index among n row ids (written to out[0], device).  With
 // `tiles` (ceil(n / kSortIdTile) words), also marks each full tile of
 // kSortIdTile ids that are consecutive rows of one batch: tiles[t] = the
-// tile's first id, -1 for every other tile.
+// tile's first id, -1 for every other tile, and counts the other tiles in
+// out[1].
 void SortMaxBatch(const int64_t* ids, int64_t n, unsigned long long* out, int64_t* tiles, cudaStream_t s);
 
 // Materializes column slot `tcol` of the rows `ids[0, n)` into `out` (width

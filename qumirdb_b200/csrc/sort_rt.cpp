@@ -104,16 +104,25 @@ struct Scratch {
     std::vector<void*> owned;
 };
 
-// Number of batches the row ids touch (largest batch index + 1).
-bool BatchCount(const int64_t* ids, int64_t n, Scratch& sc, int64_t& nbatches, int64_t* tiles = nullptr) {
-    auto* d = static_cast<unsigned long long*>(sc.Get(8));
+// Number of batches the row ids touch (largest batch index + 1).  With
+// `tiles`, also their dense-run marks and the number of tiles that are not
+// dense (*sparse).
+bool BatchCount(const int64_t* ids, int64_t n, Scratch& sc, int64_t& nbatches, int64_t* tiles = nullptr,
+                int64_t* sparse = nullptr) {
+    auto* d = static_cast<unsigned long long*>(sc.Get(16));
     if (!d) return false;
     SortMaxBatch(ids, n, d, tiles, sc.s);
-    unsigned long long m = 0;
-    cudaMemcpyAsync(&m, d, 8, cudaMemcpyDeviceToHost, sc.s);
+    unsigned long long m[2] = {0, 0};
+    cudaMemcpyAsync(m, d, tiles ? 16 : 8, cudaMemcpyDeviceToHost, sc.s);
     if (!CudaOk(cudaStreamSynchronize(sc.s), "sort: batch count")) return false;
-    nbatches = n > 0 ? int64_t(m) + 1 : 0;
+    nbatches = n > 0 ? int64_t(m[0]) + 1 : 0;
+    if (sparse) *sparse = int64_t(m[1]);
     return true;
+}
+
+// Dense-run marks of n row ids (one word per kSortIdTile ids).
+int64_t* TileMarks(int64_t n, Scratch& sc) {
+    return static_cast<int64_t*>(sc.Get(size_t((n + kSortIdTile - 1) / kSortIdTile) * 8));
 }
 
 bool ReadError(int* derr, cudaStream_t s, const char* what) {
@@ -167,8 +176,10 @@ std::vector<SortStage> MakeStages(const SortProgram& P, const bool* descs, const
     return st;
 }
 
-// Sorts n device row ids in place by the stages (stable).
-bool SortIds(int64_t* ids, int64_t n, const std::vector<SortStage>& stages, const StoreTable& table, Scratch& sc) {
+// Sorts n device row ids in place by the stages (stable).  `id_tiles`: the
+// ids' dense-run marks (or nullptr), `sparse`: how many tiles are not dense.
+bool SortIds(int64_t* ids, int64_t n, const std::vector<SortStage>& stages, const StoreTable& table, Scratch& sc,
+             const int64_t* id_tiles = nullptr, int64_t sparse = 1) {
     cudaStream_t s = sc.s;
     const int ns = int(stages.size());
     if (n <= 1 || ns == 0) return true;
@@ -226,11 +237,14 @@ bool SortIds(int64_t* ids, int64_t n, const std::vector<SortStage>& stages, cons
     auto* counter = static_cast<unsigned int*>(sc.Get(sizeof(unsigned int)));
     void* kbuf[2] = {sc.Get(size_t(n) * (any_wide ? 8 : 4)), sc.Get(size_t(n) * (any_wide ? 8 : 4))};
     uint32_t* ibuf[2] = {static_cast<uint32_t*>(sc.Get(size_t(n) * 4)), static_cast<uint32_t*>(sc.Get(size_t(n) * 4))};
-    int64_t* orig = static_cast<int64_t*>(sc.Get(size_t(n) * 8));
-    if (!dbases || !status || !counter || !kbuf[0] || !kbuf[1] || !ibuf[0] || !ibuf[1] || !orig) return false;
+    // The ids are rewritten in place at the end: keep the originals unless
+    // every one of them follows from its tile's mark.
+    const bool keep = !(id_tiles && sparse == 0);
+    int64_t* orig = keep ? static_cast<int64_t*>(sc.Get(size_t(n) * 8)) : nullptr;
+    if (!dbases || !status || !counter || !kbuf[0] || !kbuf[1] || !ibuf[0] || !ibuf[1] || (keep && !orig)) return false;
     cudaMemcpyAsync(dbases, bases.data(), bases.size() * 8, cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(status, 0, size_t(tiles) * 256 * 8, s);
-    cudaMemcpyAsync(orig, ids, size_t(n) * 8, cudaMemcpyDeviceToDevice, s);
+    if (keep) cudaMemcpyAsync(orig, ids, size_t(n) * 8, cudaMemcpyDeviceToDevice, s);
 
     const uint32_t* idx = nullptr;   // identity
     int cur = 0;
@@ -248,7 +262,7 @@ bool SortIds(int64_t* ids, int64_t n, const std::vector<SortStage>& stages, cons
         cur ^= 1;
         prev_stage = st;
     }
-    SortGatherIds(orig, idx, n, ids, s);
+    SortGatherIds(orig, idx, n, id_tiles, ids, s);
     return ReadError(derr, s, "sort: radix passes");
 }
 
@@ -370,12 +384,14 @@ int64_t qdb_gpu_sort_run(const qdb_gpu_program* program, qdb_rowset* store, int6
             if (!ids) return -1;
             cudaMemcpyAsync(ids, row_ids, size_t(n) * 8, cudaMemcpyHostToDevice, s);
         }
-        int64_t nbatches = 0;
-        if (!BatchCount(ids, n, sc, nbatches)) return -1;
+        int64_t* tiles = TileMarks(n, sc);
+        if (!tiles) return -1;
+        int64_t nbatches = 0, sparse = 0;
+        if (!BatchCount(ids, n, sc, nbatches, tiles, &sparse)) return -1;
         StoreView v;
         const std::vector<SortStage> stages = MakeStages(prog->sort, descs, nulls_firsts, false, v);
         if (!BuildStoreView(prog->sort, store, nbatches, stg, v)) return -1;
-        if (!SortIds(ids, n, stages, v.t, sc)) return -1;
+        if (!SortIds(ids, n, stages, v.t, sc, tiles, sparse)) return -1;
         if (!dev_ids) {
             cudaMemcpyAsync(row_ids, ids, size_t(n) * 8, cudaMemcpyDeviceToHost, s);
             if (!CudaOk(cudaStreamSynchronize(s), "sort: row ids")) return -1;
@@ -425,7 +441,7 @@ int64_t qdb_gpu_top_k_select(const qdb_gpu_program* program, qdb_rowset* store, 
         cudaMemcpyAsync(ids, row_ids, size_t(size) * 8, cudaMemcpyHostToDevice, s);
     }
     // Runs of consecutive rows (a scan's row ids) are fetched without their ids.
-    auto* tiles = static_cast<int64_t*>(sc.Get(size_t((size + kSortIdTile - 1) / kSortIdTile) * 8));
+    int64_t* tiles = TileMarks(size, sc);
     if (!tiles) return -1;
     int64_t nbatches = 0;
     if (!BatchCount(ids, size, sc, nbatches, tiles)) return -1;
