@@ -381,12 +381,14 @@ def serving_operator(q):
 
 def sort_pass_plan_bytes(n: int) -> tuple[int, int]:
     """Algorithmic bytes of the device sort of (k1 i64 DESC, k2 i32 ASC) over
-    n row ids, by the plan it runs: extraction (row id 8 + k1 8 + k2 4 read,
-    u32 k2 key 4 + u64 k1 key 8 written), a copy of the row ids (8 + 8), the
-    k2 stage's 3 non-constant digit passes (first 4 + 8 then 2 x 16), the k1
-    stage's 8 passes (first a gather 4 + 8 + 12, then 7 x 24), the final
-    row-id gather (4 + 8 + 8).  Returns (total per sort, per u64 pass)."""
-    per_row = 32 + 16 + (12 + 16 + 16) + (24 + 7 * 24) + 20
+    n row ids, by the plan it runs: the id scan (row id 8: batch count and
+    dense-run marks), extraction (row id 8 + k1 8 + k2 4 read, u32 k2 key 4 +
+    u64 k1 key 8 written), the k2 stage's 3 non-constant digit passes (first
+    4 + 8 then 2 x 16), the k1 stage's 8 passes (first a gather 4 + 8 + 12,
+    then 7 x 24), the final row-id write from the positions and the marks
+    (4 + 8; the ids are consecutive rows, so no copy of them is kept and the
+    marks stay in L2).  Returns (total per sort, per u64 pass)."""
+    per_row = 8 + 32 + (12 + 16 + 16) + (24 + 7 * 24) + 12
     return n * per_row, n * 24
 
 
@@ -456,8 +458,9 @@ def sort_operator(q, peak):
             "kernel_frac_of_measured_hbm": per_pass / (pass_ms / 1e3) / 1e9 / peak if pass_ms else None,
             "topk_ms": tk_ms, "topk_rows_per_s": n / (tk_ms / 1e3), "topk_algorithmic_bytes": tk_alg,
             "topk_gbs": tk_alg / (tk_ms / 1e3) / 1e9, "topk_kernels_ms": tk_parts,
-            "topk_collect_gbs": tk_alg / (collect_ms / 1e3) / 1e9 if collect_ms else None,
-            "topk_collect_frac_of_measured_hbm": tk_alg / (collect_ms / 1e3) / 1e9 / peak if collect_ms else None,
+            # The collect pass reads k1 alone here (every id tile is a dense run: no id reads).
+            "topk_collect_gbs": n * 8 / (collect_ms / 1e3) / 1e9 if collect_ms else None,
+            "topk_collect_frac_of_measured_hbm": n * 8 / (collect_ms / 1e3) / 1e9 / peak if collect_ms else None,
             "l2": "inputs larger than L2"}
     del store, pristine, work
     return line
