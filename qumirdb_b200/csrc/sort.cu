@@ -330,25 +330,24 @@ __device__ __forceinline__ unsigned long long LoadVolatile(const unsigned long l
     return *reinterpret_cast<const volatile unsigned long long*>(p);
 }
 
-template <typename K>
-__global__ void __launch_bounds__(kPassThreads, 2) SortPassKernel(const __grid_constant__ PassLaunch<K> a) {
-    extern __shared__ __align__(16) unsigned char dyn[];
-    K* skeys = reinterpret_cast<K*>(dyn);
-    uint32_t* sidx = reinterpret_cast<uint32_t*>(dyn + size_t(kSortTile) * sizeof(K));
-    __shared__ uint32_t whist[kPassWarps][256];
-    __shared__ uint32_t local_off[256];
-    __shared__ unsigned long long gbase[256];
-    __shared__ uint32_t wsum[8];
-    __shared__ uint32_t tile_s;
+// Shared state of one onesweep tile.
+struct PassShared {
+    uint32_t whist[kPassWarps][256];
+    uint32_t local_off[256];
+    unsigned long long gbase[256];
+    uint32_t wsum[8];
+    uint32_t tile;
+};
+
+// One tile of the pass.  FULL: the tile holds kSortTile keys, so no key
+// needs a bounds check.
+template <typename K, bool FULL>
+__device__ __forceinline__ void PassTile(const PassLaunch<K>& a, PassShared& sh, K* skeys, uint32_t* sidx,
+                                         int64_t tile, int tile_n) {
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int w = tid >> 5;
-    if (tid == 0) tile_s = atomicAdd(a.tile_counter, 1u);
-    for (int i = tid; i < kPassWarps * 256; i += kPassThreads) (&whist[0][0])[i] = 0;
-    __syncthreads();
-    const int64_t tile = tile_s;
     const int64_t t0 = tile * kSortTile;
-    const int tile_n = int(min((long long)kSortTile, (long long)(a.n - t0)));
 
     K key[kPassItems];
     uint32_t idx[kPassItems];
@@ -357,31 +356,33 @@ __global__ void __launch_bounds__(kPassThreads, 2) SortPassKernel(const __grid_c
     for (int j = 0; j < kPassItems; ++j) {
         const int lp = w * (32 * kPassItems) + j * 32 + lane;
         const int64_t p = t0 + lp;
-        const bool ok = lp < tile_n;
+        const bool ok = FULL || lp < tile_n;
         idx[j] = ok ? (a.idx_in ? a.idx_in[p] : uint32_t(p)) : 0u;
         key[j] = ok ? (a.gather ? a.keys_in[idx[j]] : a.keys_in[p]) : K(0);
     }
     // Stable rank of every key among the equal digits of its warp's segment.
-    // The lanes sharing a digit come from one ballot per digit bit.
+    // The lanes sharing a digit come from one ballot per digit bit: lane i
+    // keeps the ballot where its bit is set and the complement where not.
 #pragma unroll
     for (int j = 0; j < kPassItems; ++j) {
         const int lp = w * (32 * kPassItems) + j * 32 + lane;
-        const bool ok = lp < tile_n;
+        const bool ok = FULL || lp < tile_n;
         const unsigned d = unsigned(uint64_t(key[j]) >> a.shift) & 255u;
-        const unsigned act = __ballot_sync(kFull, ok);
+        const unsigned act = FULL ? kFull : __ballot_sync(kFull, ok);
         unsigned peers = act;
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
-            const unsigned set = __ballot_sync(kFull, (d >> b) & 1u);
-            peers &= ((d >> b) & 1u) ? set : ~set;
+        for (int bt = 0; bt < 8; ++bt) {
+            const unsigned bit = (d >> bt) & 1u;
+            const unsigned set = __ballot_sync(kFull, bit);
+            peers &= set ^ (bit - 1u);
         }
         rank[j] = 0;
         if (ok) {
             const int leader = __ffs(peers) - 1;
             uint32_t old = 0;
             if (lane == leader) {
-                old = whist[w][d];
-                whist[w][d] = old + uint32_t(__popc(peers));
+                old = sh.whist[w][d];
+                sh.whist[w][d] = old + uint32_t(__popc(peers));
             }
             old = __shfl_sync(act, old, leader);
             rank[j] = old + uint32_t(__popc(peers & ((1u << lane) - 1u)));
@@ -392,9 +393,10 @@ __global__ void __launch_bounds__(kPassThreads, 2) SortPassKernel(const __grid_c
     if (tid < 256) {
         // Warp prefixes in place, then publish this tile's count at once.
         uint32_t cnt = 0;
+#pragma unroll
         for (int ww = 0; ww < kPassWarps; ++ww) {
-            const uint32_t c = whist[ww][tid];
-            whist[ww][tid] = cnt;
+            const uint32_t c = sh.whist[ww][tid];
+            sh.whist[ww][tid] = cnt;
             cnt += c;
         }
         const unsigned long long ep = (unsigned long long)(a.epoch & kEpochMask) << 40;
@@ -407,42 +409,42 @@ __global__ void __launch_bounds__(kPassThreads, 2) SortPassKernel(const __grid_c
             const uint32_t t = __shfl_up_sync(kFull, v, o);
             if (lane >= o) v += t;
         }
-        if (lane == 31) wsum[w] = v;
+        if (lane == 31) sh.wsum[w] = v;
         asm volatile("bar.sync 1, 256;" ::: "memory");
         uint32_t off = v - cnt;
-        for (int ww = 0; ww < w; ++ww) off += wsum[ww];
-        local_off[tid] = off;
+        for (int ww = 0; ww < w; ++ww) off += sh.wsum[ww];
+        sh.local_off[tid] = off;
         // Decoupled look-back: sum earlier tiles' counts until an inclusive one.
         unsigned long long excl = 0;
         if (tile > 0) {
             int64_t t = tile - 1;
             const long long start = clock64();
             while (t >= 0) {
-                const unsigned long long s = LoadVolatile(a.status + t * 256 + tid);
-                const unsigned flag = unsigned(s >> 62);
-                if (flag == 0 || uint32_t((s >> 40) & kEpochMask) != (a.epoch & kEpochMask)) {
+                const unsigned long long st = LoadVolatile(a.status + t * 256 + tid);
+                const unsigned flag = unsigned(st >> 62);
+                if (flag == 0 || uint32_t((st >> 40) & kEpochMask) != (a.epoch & kEpochMask)) {
                     if (clock64() - start > kSpinCycles) {
                         SetError(a.err, DE_LOOKBACK_TIMEOUT);
                         break;
                     }
                     continue;
                 }
-                excl += s & kValueMask;
+                excl += st & kValueMask;
                 if (flag == 2) break;
                 --t;
             }
             StoreVolatile(mine, kFlagInc | ep | (excl + cnt));
         }
-        gbase[tid] = a.base[tid] + excl;
+        sh.gbase[tid] = a.base[tid] + excl;
     }
     __syncthreads();
     // Reorder the tile by digit in shared memory, then write coalesced runs.
 #pragma unroll
     for (int j = 0; j < kPassItems; ++j) {
         const int lp = w * (32 * kPassItems) + j * 32 + lane;
-        if (lp < tile_n) {
+        if (FULL || lp < tile_n) {
             const unsigned d = unsigned(uint64_t(key[j]) >> a.shift) & 255u;
-            const uint32_t pos = local_off[d] + whist[w][d] + rank[j];
+            const uint32_t pos = sh.local_off[d] + sh.whist[w][d] + rank[j];
             if (pos < uint32_t(kSortTile)) {
                 skeys[pos] = key[j];
                 sidx[pos] = idx[j];
@@ -450,15 +452,35 @@ __global__ void __launch_bounds__(kPassThreads, 2) SortPassKernel(const __grid_c
         }
     }
     __syncthreads();
-    for (int p = tid; p < tile_n; p += kPassThreads) {
-        const K k = skeys[p];
-        const unsigned d = unsigned(uint64_t(k) >> a.shift) & 255u;
-        const unsigned long long g = gbase[d] + uint64_t(p - int(local_off[d]));
-        if (g < (unsigned long long)a.n) {   // only a timed-out look-back can break this
-            a.keys_out[g] = k;
-            a.idx_out[g] = sidx[p];
+#pragma unroll
+    for (int j = 0; j < kPassItems; ++j) {
+        const int p = tid + j * kPassThreads;
+        if (FULL || p < tile_n) {
+            const K k = skeys[p];
+            const unsigned d = unsigned(uint64_t(k) >> a.shift) & 255u;
+            const unsigned long long g = sh.gbase[d] + uint64_t(p - int(sh.local_off[d]));
+            if (g < (unsigned long long)a.n) {   // only a timed-out look-back can break this
+                a.keys_out[g] = k;
+                a.idx_out[g] = sidx[p];
+            }
         }
     }
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kPassThreads, 2) SortPassKernel(const __grid_constant__ PassLaunch<K> a) {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    K* skeys = reinterpret_cast<K*>(dyn);
+    uint32_t* sidx = reinterpret_cast<uint32_t*>(dyn + size_t(kSortTile) * sizeof(K));
+    __shared__ PassShared sh;
+    const int tid = threadIdx.x;
+    if (tid == 0) sh.tile = atomicAdd(a.tile_counter, 1u);
+    for (int i = tid; i < kPassWarps * 256; i += kPassThreads) (&sh.whist[0][0])[i] = 0;
+    __syncthreads();
+    const int64_t tile = sh.tile;
+    const int tile_n = int(min((long long)kSortTile, (long long)(a.n - tile * kSortTile)));
+    if (tile_n == kSortTile) PassTile<K, true>(a, sh, skeys, sidx, tile, tile_n);
+    else PassTile<K, false>(a, sh, skeys, sidx, tile, tile_n);
 }
 
 // out[i] = ids[idx[i]], four rows per thread per step with every position
