@@ -617,6 +617,17 @@ def profile_case(name: str, rows: int) -> None:
         for _ in range(2):
             d.upload(rid)
             s.sort(d)
+    elif name == "topk":
+        n = rows or SORT_ROWS
+        k1 = np.empty(n, np.int64)
+        k2 = np.empty(n, np.int32)
+        rid = np.arange(n, dtype=np.int64)
+        q.lib().qdb_gen_sort(3, n, k1.ctypes.data, k2.ctypes.data, None)
+        s = q.Sort(q.compile_sort(queries.top_k1()), [q.DeviceRowSet([k1, k2, rid])])
+        d = q.DeviceBuffer(rid.nbytes)
+        for _ in range(2):
+            d.upload(rid)
+            s.top_k(d, 1000)
     q.synchronize()
     print("done", name, flush=True)
 
@@ -629,7 +640,7 @@ def main() -> None:
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--no-operators", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-case", choices=["join", "sort", "lineitem", "zipf", "zipf_batched"],
+    ap.add_argument("--profile-case", choices=["join", "sort", "topk", "lineitem", "zipf", "zipf_batched"],
                     help="run one workload twice at --rows rows (for profiler captures) and exit")
     ap.add_argument("--rows", type=int, default=0)
     ap.add_argument("--only", choices=["lineitem", "zipf", "zipf_batched", "sort", "serving"],

@@ -330,6 +330,9 @@ __device__ __forceinline__ unsigned long long LoadVolatile(const unsigned long l
     return *reinterpret_cast<const volatile unsigned long long*>(p);
 }
 
+// Earlier tiles' states one look-back round trip reads.
+constexpr int kLookWindow = 4;
+
 // Shared state of one onesweep tile.
 struct PassShared {
     uint32_t whist[kPassWarps][256];
@@ -414,24 +417,33 @@ __device__ __forceinline__ void PassTile(const PassLaunch<K>& a, PassShared& sh,
         uint32_t off = v - cnt;
         for (int ww = 0; ww < w; ++ww) off += sh.wsum[ww];
         sh.local_off[tid] = off;
-        // Decoupled look-back: sum earlier tiles' counts until an inclusive one.
+        // Decoupled look-back: sum earlier tiles' counts until an inclusive
+        // one, reading a window of kLookWindow earlier tiles per round trip
+        // (tile 0 publishes an inclusive count, so no walk passes it).
         unsigned long long excl = 0;
         if (tile > 0) {
             int64_t t = tile - 1;
             const long long start = clock64();
-            while (t >= 0) {
-                const unsigned long long st = LoadVolatile(a.status + t * 256 + tid);
-                const unsigned flag = unsigned(st >> 62);
-                if (flag == 0 || uint32_t((st >> 40) & kEpochMask) != (a.epoch & kEpochMask)) {
-                    if (clock64() - start > kSpinCycles) {
-                        SetError(a.err, DE_LOOKBACK_TIMEOUT);
-                        break;
-                    }
-                    continue;
+            bool done = false;
+            while (!done) {
+                unsigned long long st[kLookWindow];
+#pragma unroll
+                for (int q = 0; q < kLookWindow; ++q) st[q] = t - q >= 0 ? LoadVolatile(a.status + (t - q) * 256 + tid) : 0;
+                int used = 0;
+#pragma unroll
+                for (int q = 0; q < kLookWindow; ++q) {
+                    if (done || used < q) break;
+                    const unsigned flag = unsigned(st[q] >> 62);
+                    if (flag == 0 || uint32_t((st[q] >> 40) & kEpochMask) != (a.epoch & kEpochMask)) break;
+                    excl += st[q] & kValueMask;
+                    used = q + 1;
+                    done = flag == 2;
                 }
-                excl += st & kValueMask;
-                if (flag == 2) break;
-                --t;
+                t -= used;
+                if (!done && used == 0 && clock64() - start > kSpinCycles) {
+                    SetError(a.err, DE_LOOKBACK_TIMEOUT);
+                    break;
+                }
             }
             StoreVolatile(mine, kFlagInc | ep | (excl + cnt));
         }
