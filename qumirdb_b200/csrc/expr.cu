@@ -56,6 +56,21 @@ struct ExprLaunch {
     ExprArgs A;
 };
 
+// Filters without a generic expression (selection, NULL rejects, atoms): no
+// evaluation stack, so it keeps a full SM of warps where FilterKernel's
+// generic evaluator (154 registers, a 1.7 KB stack) holds eight.
+__global__ void __launch_bounds__(256) FilterAtomsKernel(const __grid_constant__ ExprLaunch L) {
+    const AggPlan& P = L.P;
+    for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < L.A.nrows;
+         r += int64_t(gridDim.x) * blockDim.x) {
+        bool pass = P.selection == nullptr || P.selection[r] != 0;
+        GlobalAcc acc{&P, r};
+        for (int j = 0; j < L.A.n_null_reject && pass; ++j) pass = !acc.Null(L.A.null_reject[j]);
+        if (pass && P.filter_kind == 1) pass = AtomsPass(P, acc);
+        L.A.out_sel[r] = pass ? 1 : 0;
+    }
+}
+
 __global__ void __launch_bounds__(256) FilterKernel(const __grid_constant__ ExprLaunch L) {
     const AggPlan& P = L.P;
     for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < L.A.nrows;
@@ -249,7 +264,8 @@ void FilterRows(const ExprArgs& a, cudaStream_t s) {
     L.P = *a.plan;
     L.A = a;
     ProfileBegin(s, "filter", a.nrows);
-    FilterKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(L);
+    if (L.P.filter_kind == 2) FilterKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(L);
+    else FilterAtomsKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(L);
     ProfileEnd(s);
     CountLaunch();
 }
