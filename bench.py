@@ -468,10 +468,9 @@ def sort_operator(q, peak):
 
 def cpu_baseline_sort(sample: int) -> dict:
     from oracle import oracle as O
-    import qumirdb_b200 as q
     k1 = np.empty(sample, np.int64)
     k2 = np.empty(sample, np.int32)
-    q.lib().qdb_gen_sort(3, sample, k1.ctypes.data, k2.ctypes.data, None)
+    O.lib().qdb_gen_sort(3, sample, k1.ctypes.data, k2.ctypes.data, None)
     threads = os.cpu_count() or 1
     sec = O.lib().oracle_bench_sort(k1.ctypes.data, k2.ctypes.data, sample, threads, None)
     return {"value": sample / sec, "unit": "rows/s", "cores": threads, "kind": "port",
@@ -484,22 +483,21 @@ def cpu_baseline_agg(kind: str, sample: int) -> dict:
     tables, then the hash-partitioned final) on all host threads, over the
     lineitem table or a sample of the Zipf stream."""
     from oracle import oracle as O
-    import qumirdb_b200 as q
-    from qumirdb_b200 import queries
+    from qumirdb_b200 import HostRowSet, queries
     if kind == "lineitem":
         cols = [np.empty(sample, np.int64), np.empty(sample, np.int64), np.empty(sample, np.int64),
                 np.empty(sample, np.int64), np.empty(sample, np.uint8), np.empty(sample, np.uint8),
                 np.empty(sample, np.int32)]
-        q.lib().qdb_gen_lineitem(0, sample, *[c.ctypes.data for c in cols])
+        O.lib().qdb_gen_lineitem(0, sample, *[c.ctypes.data for c in cols])
         spec = queries.lineitem_agg(int(cols[6].max()) - 90)
         what = f"{sample:,} rows (the whole table)"
     else:
         cols = [np.empty(sample, np.int64), np.empty(sample, np.int64), np.empty(sample, np.float64)]
-        q.lib().qdb_gen_zipf(2, sample, ZIPF_DISTINCT, 1.1, *[c.ctypes.data for c in cols])
+        O.lib().qdb_gen_zipf(2, sample, ZIPF_DISTINCT, 1.1, *[c.ctypes.data for c in cols])
         spec = queries.zipf_agg(expected_groups=ZIPF_DISTINCT)
         what = f"{sample:,} rows (of 200M) of the same Zipf stream"
     threads = os.cpu_count() or 1
-    rs = q.HostRowSet(cols)
+    rs = HostRowSet(cols)
     sec = O.lib().oracle_bench_aggregate(C.byref(spec.struct), rs.ptr, threads, None)
     return {"value": sample / sec, "unit": "rows/s", "cores": threads, "kind": "port",
             "sample": what + ": per-lane partial tables + hash-partitioned final of the CPU restatement",
@@ -507,13 +505,15 @@ def cpu_baseline_agg(kind: str, sample: int) -> dict:
 
 
 def cpu_baseline_join(sample_probe: int, steps: int = 1) -> dict:
+    """The CPU restatement's threaded join plan over the bench's own seeded
+    inputs (the same generators, linked into the oracle library, so this
+    leg loads no device code)."""
     from oracle import oracle as O
-    import qumirdb_b200 as q
     b = [np.empty(BUILD_ROWS, np.int64), np.empty(BUILD_ROWS, np.int64), np.empty(BUILD_ROWS, np.int32)]
     p = [np.empty(sample_probe, np.int64), np.empty(sample_probe, np.int64)]
-    q.lib().qdb_gen_join(1, BUILD_ROWS, 0, FK_DOMAIN, *[x.ctypes.data for x in b], None, None)
+    O.lib().qdb_gen_join(1, BUILD_ROWS, 0, FK_DOMAIN, *[x.ctypes.data for x in b], None, None)
     tmp = [np.empty(1, np.int64), np.empty(1, np.int64), np.empty(1, np.int32)]
-    q.lib().qdb_gen_join(1000, 1, sample_probe, FK_DOMAIN, *[t.ctypes.data for t in tmp], *[x.ctypes.data for x in p])
+    O.lib().qdb_gen_join(1000, 1, sample_probe, FK_DOMAIN, *[t.ctypes.data for t in tmp], *[x.ctypes.data for x in p])
     threads = os.cpu_count() or 1
     times = []
     s = C.c_int64()
@@ -524,26 +524,46 @@ def cpu_baseline_join(sample_probe: int, steps: int = 1) -> dict:
                                           C.byref(c))
         times.append(t)
     sec = min(times)
+    what = "the whole 120,000,000-row probe" if sample_probe == PROBE_ROWS else \
+        f"a probe sample of {sample_probe:,} rows (of 120M)"
     return {"value": (BUILD_ROWS + sample_probe) / sec, "unit": "rows/s", "cores": threads, "kind": "port",
-            "sample": f"build 2,000,000 rows + probe sample of {sample_probe:,} rows (of 120M), threaded "
-                      f"partitioned row-table plan of the CPU restatement", "seconds": sec}
+            "sample": f"build 2,000,000 rows + {what}, threaded partitioned row-table plan of the CPU "
+                      f"restatement (fastest of {steps} runs)", "seconds": sec, "times": times,
+            "result": [s.value, c.value]}
+
+
+JOIN_CONFIG = {"workload": "equi-join: build 2,000,000 rows (unique keys, attr<20 filter fused), probe "
+                           "120,000,000 rows per GPU (fk uniform over 1..2.5M), SUM(payload*value), COUNT(*)",
+               "build_rows": BUILD_ROWS, "probe_rows_per_gpu": PROBE_ROWS,
+               "l2": "inputs larger than L2 (1.92 GB probe stream per step)"}
 
 
 def reference_arm(args) -> None:
+    """The reference's CPU path for the headline workload: the oracle's
+    threaded partitioned row-join plan (the reference engine cannot be built
+    here), on all host threads, over the whole 2M x 120M workload with the
+    same seeded inputs; one step is one whole query.  Only the oracle
+    library is loaded."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    sample = 24_000_000
     steps = max(1, args.steps)
-    cb = cpu_baseline_join(sample, steps=args.warmup + steps)
-    line = {"metric": METRIC, "value": cb["value"], "unit": "rows/s", "n_gpus": args.gpus, "steps": steps,
-            "warmup": args.warmup, "ms_per_step": cb["seconds"] * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
+    cb = cpu_baseline_join(PROBE_ROWS, steps=args.warmup + steps)
+    timed_s = cb["times"][args.warmup:]
+    sec = statistics.median(timed_s)
+    rows = BUILD_ROWS + PROBE_ROWS
+    value = rows / sec
+    line = {"metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded generators with the workload's shapes and distributions)",
             "impl": "reference",
-            "config": {"workload": "equi-join build 2M (attr<20) / probe sample, SUM(payload*value), COUNT(*)",
-                       "build_rows": BUILD_ROWS, "probe_rows": sample},
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": cb["value"], "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": dict(JOIN_CONFIG, parallelism=f"shard{world}", result=cb["result"]),
+            "cpu_baseline": {"value": value, "unit": "rows/s", "cores": cb["cores"], "kind": "port",
+                             "sample": cb["sample"].replace(f"(fastest of {args.warmup + steps} runs)",
+                                                            f"(median of {steps} timed runs)")},
+            "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -632,6 +652,50 @@ def profile_case(name: str, rows: int) -> None:
     print("done", name, flush=True)
 
 
+def compact_operators(ops: dict) -> dict:
+    """The per-operator figures that go on the one JSON line: rows/s, time,
+    the dominant kernel's time and fraction of the measured HBM peak, its
+    ncu traffic over the algorithmic bytes, and the CPU baseline; the
+    serving stream's best sustained points (the sweeps stay in --detail)."""
+    traffic = load_traffic()
+
+    def r(x, nd=4):
+        return None if x is None else float(f"{x:.{nd}g}")
+
+    out = {}
+    for name in ("lineitem", "zipf", "zipf_batched", "sort"):
+        o = ops.get(name)
+        if not o:
+            continue
+        c = {"rows_per_s": r(o.get("rows_per_s")), "ms": r(o.get("ms_per_query", o.get("ms_per_sort"))),
+             "kernel": o.get("kernel"), "kernel_ms": r(o.get("kernel_ms")),
+             "frac_of_measured_hbm": r(o.get("kernel_frac_of_measured_hbm", o.get("frac_of_measured_hbm")), 3)}
+        ratio = traffic.get(f"{o.get('kernel')}_traffic_over_algorithmic")
+        if ratio is not None:
+            c["traffic_over_algorithmic"] = ratio
+        if name == "sort":
+            c.update({"sort_frac_of_measured_hbm": r(o.get("frac_of_measured_hbm"), 3),
+                      "bytes_per_row": o.get("bytes_per_row"), "topk_ms": r(o.get("topk_ms")),
+                      "topk_rows_per_s": r(o.get("topk_rows_per_s"))})
+        if name in ("zipf", "zipf_batched"):
+            c["groups"] = o.get("groups")
+        if "finalize_ms" in o:
+            c["finalize_ms"] = r(o.get("finalize_ms"))
+        cb = o.get("cpu_baseline")
+        if cb:
+            c["cpu_baseline"] = {"rows_per_s": r(cb["value"]), "cores": cb["cores"], "kind": cb["kind"]}
+        out[name] = c
+    sv = ops.get("serving")
+    if sv:
+        pick = lambda d: {k: r(d[k]) for k in ("queries_per_s", "p50_ms", "p99_ms")}  # noqa: E731
+        out["serving"] = {"plain": pick(sv["plain"]), "serving": pick(sv["serving"]),
+                          "serving_over_plain_qps": r(sv["serving_over_plain_qps"], 3)}
+        for k in ("cpu", "coalesced_queries", "batched_launches"):
+            if k in sv:
+                out["serving"][k] = sv[k] if not isinstance(sv[k], dict) else pick(sv[k])
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -643,6 +707,7 @@ def main() -> None:
     ap.add_argument("--profile-case", choices=["join", "sort", "topk", "lineitem", "zipf", "zipf_batched"],
                     help="run one workload twice at --rows rows (for profiler captures) and exit")
     ap.add_argument("--rows", type=int, default=0)
+    ap.add_argument("--detail", help="write every operator's full figures (serving sweeps included) to this file")
     ap.add_argument("--only", choices=["lineitem", "zipf", "zipf_batched", "sort", "serving"],
                     help="run one operator's measurement and print its JSON")
     args = ap.parse_args()
@@ -717,11 +782,7 @@ def main() -> None:
         "vs_baseline": None,
         "dtype": "int64",
         "data": "synthetic (seeded generators with the workload's shapes and distributions)",
-        "config": {"workload": "equi-join: build 2,000,000 rows (unique keys, attr<20 filter fused), probe "
-                               "120,000,000 rows per GPU (fk uniform over 1..2.5M), SUM(payload*value), COUNT(*)",
-                   "build_rows": BUILD_ROWS, "probe_rows_per_gpu": PROBE_ROWS, "parallelism": f"shard{world}",
-                   "l2": "inputs larger than L2 (1.92 GB probe stream per step)",
-                   "result": list(results[-1])},
+        "config": dict(JOIN_CONFIG, parallelism=f"shard{world}", result=list(results[-1])),
         "roofline": {"bound": "hbm", "kernel": "join_agg_probe", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
                      "traffic": traffic * PROBE_ROWS if traffic else None,
@@ -732,21 +793,26 @@ def main() -> None:
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_operators:
+        ops = {}
         try:
-            line["operators"] = {"lineitem": lineitem_operator(q, peak), "zipf": zipf_operator(q, peak),
-                                 "zipf_batched": zipf_batched_operator(q, peak), "sort": sort_operator(q, peak),
-                                 "serving": serving_operator(q)}
+            ops = {"lineitem": lineitem_operator(q, peak), "zipf": zipf_operator(q, peak),
+                   "zipf_batched": zipf_batched_operator(q, peak), "sort": sort_operator(q, peak),
+                   "serving": serving_operator(q)}
             if not args.no_cpu_baseline:
-                line["operators"]["sort"]["cpu_baseline"] = {
+                ops["sort"]["cpu_baseline"] = {
                     k: v for k, v in cpu_baseline_sort(20_000_000).items() if k != "seconds"}
-                line["operators"]["lineitem"]["cpu_baseline"] = {
+                ops["lineitem"]["cpu_baseline"] = {
                     k: v for k, v in cpu_baseline_agg("lineitem", LINEITEM_ROWS).items() if k != "seconds"}
-                line["operators"]["zipf"]["cpu_baseline"] = {
+                ops["zipf"]["cpu_baseline"] = {
                     k: v for k, v in cpu_baseline_agg("zipf", 20_000_000).items() if k != "seconds"}
         except Exception as e:  # reported, never hidden
             line["operators_error"] = repr(e)
+        if args.detail:
+            Path(args.detail).parent.mkdir(parents=True, exist_ok=True)
+            Path(args.detail).write_text(json.dumps(ops, indent=1))
+        line["operators"] = compact_operators(ops)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline_join(24_000_000)
+        cb = cpu_baseline_join(PROBE_ROWS)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if dist is not None:
         dist.barrier()

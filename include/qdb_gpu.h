@@ -395,6 +395,28 @@ int64_t qdb_gpu_sort_run(const qdb_gpu_program* program, qdb_rowset* store,
 int64_t qdb_gpu_top_k_select(const qdb_gpu_program* program, qdb_rowset* store,
                              int64_t* row_ids, int64_t size, int64_t limit);
 
+/* qdb_top_sort_update (TTopSortDispatch, qdb/kernel/compiler.h:570-583;    */
+/* the update built by BuildTopSortUpdateAst, compiler.cpp:881-975), the     */
+/* step of TTopSortProcessor::Add (qdb/exec/sort_exec.cpp:627-760) for a     */
+/* LIMIT the heap rule turns away (K > 1024 or K > rows / 4).  `state` holds  */
+/* the rows kept so far, in order (zeroed before the first call: no rows);    */
+/* `batch` the new rows, named by row_ids[0, n) = (0 << 32) | row in         */
+/* ascending order.  With sort_input the batch's rows are ordered here        */
+/* (stable: equal keys keep row-id order); without it row_ids already lists  */
+/* them in order (qdb_gpu_top_k_select's output).  They are merged with the  */
+/* state, a state row first on equal keys, and the first `limit` rows are    */
+/* materialized into `out` (every column: the program's out_columns must be  */
+/* all columns in order, so `out` can be the next call's state).  Writes     */
+/* pick_src[i] (0 = state, 1 = batch), pick_idx[i] (row in it) and           */
+/* row_ids[i] = pick_src << 32 | pick_idx for the kept rows (host or device   */
+/* arrays), and returns their count (0 when limit <= 0), < 0 on failure.     */
+/* `work`/`counts` may be NULL: the device path keeps its own scratch.        */
+/* Two NULL keys compare equal here (the earlier row first).                  */
+int64_t qdb_gpu_top_sort_update(const qdb_gpu_program* program, qdb_rowset* state, qdb_rowset* batch,
+                                int64_t* row_ids, int64_t* work, uint32_t* counts, int64_t n,
+                                bool sort_input, uint8_t* pick_src, uint32_t* pick_idx, int64_t limit,
+                                qdb_rowset* out);
+
 /* ------------------------------------------------------------------------ */
 /* Batched aggregation: many aggregate states of one program per launch.    */
 /* ------------------------------------------------------------------------ */
@@ -437,28 +459,35 @@ void qdb_gpu_autotune_reset(void);
 
 /* No counterpart in the reference: an addition for embedders that cannot     */
 /* allocate device memory while a query runs — an engine that hands the GPU   */
-/* a fixed memory budget up front, a caller recording work into a CUDA graph, */
-/* or a process whose device allocator belongs to another runtime.           */
+/* a fixed memory budget up front and must not exceed it mid-query, or a      */
+/* process whose device allocator belongs to another runtime (a host that     */
+/* owns all of the device's memory through its own pool).                     */
 /*                                                                           */
 /* Runs one whole aggregate of an aggregate program (table set-up, the fused  */
 /* filter -> project -> aggregate over `batch`, finalize) and writes the      */
 /* groups into the caller's output columns.  Every column, mask and the       */
 /* selection of `batch` must already be in device memory (nothing is copied), */
-/* and out_columns[k].Data must be a device buffer of out_capacity values of  */
-/* output column k (Mask, when set, a device bitmap of out_capacity bits;     */
-/* Offsets, when set on a one-byte string column, out_capacity + 1 int32).   */
+/* and out_columns[k] describes caller-owned device buffers for output        */
+/* column k: Data holds out_capacity values (aligned to the value width);    */
+/* Mask, when set, is (out_capacity + 31) / 32 uint32 words, 4-byte aligned   */
+/* (all of them are cleared, then bit i set for a valid row i); Offsets,      */
+/* when set on a one-byte string column, out_capacity + 1 int32.             */
 /* Returns the group count, or -1 (see qdb_gpu_last_error) when an input is   */
-/* not in device memory, the groups exceed out_capacity, or the state does    */
-/* not fit the scratch.                                                       */
+/* not in device memory, a buffer is misaligned, the groups exceed            */
+/* out_capacity or the scratch table.  The call returns after the device     */
+/* work has finished (it reads the group count back).                        */
 /*                                                                           */
 /* Table, counters and finalize scratch live in one file-scope device array   */
 /* of QDB_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds      */
-/* until the process exits; it fits one-word group keys and at most 2^19     */
-/* groups (fewer for wide aggregate states).  The first call on a device      */
-/* looks up that array's device address, so make it before any stream        */
-/* capture.  Calls share the array: each clears what it uses, and calls whose */
-/* work overlaps on the GPU race and must be serialised by the caller.  It    */
-/* runs on the stream set by qdb_gpu_set_stream.                              */
+/* until the process exits.  It serves one-word group keys; the table holds  */
+/* at most 2^18 groups with one state word, and fewer for wider states        */
+/* (2^17 for 2 to 5 state words, e.g. COUNT, SUM, MIN, MAX and an f64 SUM);   */
+/* the error message states the limit of the program at hand.  The first      */
+/* call on a device looks up that array's device address, so make the first  */
+/* call before any stream capture.  Calls share the array and each clears    */
+/* what it uses: calls whose work overlaps on the GPU (other streams, other   */
+/* host threads) race on it and must be serialised by the caller.  It runs on */
+/* the stream set by qdb_gpu_set_stream.                                      */
 #define QDB_NOALLOC_SCRATCH_BYTES (16u << 20)
 int64_t qdb_gpu_agg_run_noalloc(const qdb_gpu_program* program, const qdb_rowset* batch,
                                 qdb_column* out_columns, int64_t out_capacity);

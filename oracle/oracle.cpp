@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <queue>
 #include <stdexcept>
 #include <string>
@@ -399,13 +400,18 @@ uint64_t LeafHash(const Val& v, int t) {
     }
 }
 
-// Struct key: boost-style ordered combine of the field hashes; a NULL field
-// contributes 0 (gen.cpp:345-375).
-uint64_t StructHash(const Val* vals, const int* types, int n) {
+// Struct key: boost-style ordered combine over the fields of the key struct
+// (gen.cpp:345-375).  A nullable key column j is two fields of that struct,
+// `valid_j` (BOOL) before `key_j` (BuildAggregateKeyDescriptor,
+// qdb/kernel/aggregate_key.cpp:211-260): the validity flag is hashed like a
+// BOOL leaf (flag * 2685821657736338717), and a NULL key field contributes 0.
+// Without `nullable` every field is taken as NOT NULL (internal placement).
+uint64_t StructHash(const Val* vals, const int* types, int n, const bool* nullable = nullptr) {
     uint64_t h = 0;
+    auto combine = [&h](uint64_t fh) { h ^= fh + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2); };
     for (int j = 0; j < n; ++j) {
-        const uint64_t fh = vals[j].null ? 0 : LeafHash(vals[j], types[j]);
-        h ^= fh + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2);
+        if (nullable && nullable[j]) combine(vals[j].null ? 0 : 2685821657736338717ULL);
+        combine(vals[j].null ? 0 : LeafHash(vals[j], types[j]));
     }
     return h;
 }
@@ -1076,6 +1082,25 @@ void SortOneKey(const qdb_sort_spec& s, const qdb_rowset* store, std::vector<int
     else { ids = valid_ids; ids.insert(ids.end(), null_ids.begin(), null_ids.end()); }
 }
 
+// Key order only (AppendSortLessBody, qdb/kernel/compiler.cpp:700-753): true
+// when row a's keys come strictly before row b's.
+bool KeysLess(const qdb_sort_spec& s, const qdb_rowset* store, int64_t a, int64_t b) {
+    for (int k = 0; k < s.n_keys; ++k) {
+        const int col = s.keys[k].column;
+        const int t = s.columns[col].type;
+        const Val x = StoreCell(s, store, a, col), y = StoreCell(s, store, b, col);
+        const bool desc = s.keys[k].desc, nf = s.keys[k].nulls_first;
+        if (x.null || y.null) {
+            if (x.null && y.null) continue;
+            return x.null ? nf : !nf;
+        }
+        const uint64_t kx = RadixKey(x, t), ky = RadixKey(y, t);
+        if (kx == ky) continue;
+        return desc ? kx > ky : kx < ky;
+    }
+    return false;
+}
+
 // SortRowsLess (qdb/exec/sort_exec.cpp:126-293) with the packed row id as the
 // final tie break (qdb/kernel/compiler.h:135-148).
 bool RowLess(const qdb_sort_spec& s, const qdb_rowset* store, const bool* descs,
@@ -1211,13 +1236,17 @@ int oracle_hash(int32_t n_columns, const qdb_column_type* columns, int32_t n_key
     try {
         std::vector<Val> key(n_keys);
         std::vector<int> types(n_keys);
-        for (int j = 0; j < n_keys; ++j) types[j] = columns[key_columns[j]].type;
+        std::unique_ptr<bool[]> nullable(new bool[size_t(n_keys)]);
+        for (int j = 0; j < n_keys; ++j) {
+            types[j] = columns[key_columns[j]].type;
+            nullable[j] = columns[key_columns[j]].nullable != 0;
+        }
         for (int64_t r = 0; r < batch->RowCount; ++r) {
             if (batch->Selection && !batch->Selection[r]) continue;
             for (int j = 0; j < n_keys; ++j) {
                 key[j] = ReadCell(batch->Columns[key_columns[j]], columns[key_columns[j]], r);
             }
-            hashes[r] = StructHash(key.data(), types.data(), n_keys);
+            hashes[r] = StructHash(key.data(), types.data(), n_keys, nullable.get());
         }
         return 0;
     } catch (const std::exception& ex) {
@@ -1341,6 +1370,50 @@ int64_t oracle_top_k(const qdb_sort_spec* spec, const qdb_rowset* store, int64_t
     }
     std::memcpy(row_ids, h.data(), sizeof(int64_t) * kept);
     return kept;
+}
+
+int64_t oracle_top_sort_update(const qdb_sort_spec* spec, const qdb_rowset* state, const qdb_rowset* batch,
+                               int64_t* row_ids, int64_t n, bool sort_input, uint8_t* pick_src,
+                               uint32_t* pick_idx, int64_t limit, char* err, size_t err_len) {
+    try {
+        // qdb_top_sort_update (BuildTopSortUpdateAst, compiler.cpp:881-975):
+        // sort the batch's row ids when asked (keys last to first, stable),
+        // then top_sort_merge_picks (qdb/kernel/sort/top_sort.oz:15-57).
+        if (sort_input && n > 0) {
+            std::vector<int64_t> ids(row_ids, row_ids + n);
+            for (int k = spec->n_keys - 1; k >= 0; --k) {
+                SortOneKey(*spec, batch, ids, spec->keys[k].column, spec->keys[k].desc, spec->keys[k].nulls_first);
+            }
+            std::memcpy(row_ids, ids.data(), sizeof(int64_t) * size_t(n));
+        }
+        const qdb_rowset both[2] = {*state, *batch};
+        const int64_t state_n = state->RowCount;
+        int64_t left = 0, right = 0, out = 0;
+        while (out < limit && (left < state_n || right < n)) {
+            bool take_temp;
+            if (right == n) take_temp = false;
+            else if (left == state_n) take_temp = true;
+            else {
+                // qdb_top_sort_temp_before_state: the batch row strictly first.
+                const int64_t temp_row = int64_t(uint32_t(row_ids[right]));
+                take_temp = KeysLess(*spec, both, (int64_t(1) << 32) | temp_row, left);
+            }
+            if (take_temp) {
+                pick_src[out] = 1;
+                pick_idx[out] = uint32_t(row_ids[right]);
+                ++right;
+            } else {
+                pick_src[out] = 0;
+                pick_idx[out] = uint32_t(left);
+                ++left;
+            }
+            ++out;
+        }
+        return out;
+    } catch (const std::exception& e) {
+        SetErr(err, err_len, e.what());
+        return -1;
+    }
 }
 
 double oracle_bench_aggregate(const qdb_aggregate_spec* spec, const qdb_rowset* batch, int32_t threads,

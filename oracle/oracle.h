@@ -89,6 +89,16 @@ int64_t oracle_top_k(const qdb_sort_spec* spec, const qdb_rowset* store,
                      int64_t* row_ids, int64_t size, int64_t limit,
                      const bool* descs, const bool* nulls_firsts);
 
+/* One TTopSortProcessor::Add step (qdb/exec/sort_exec.cpp:627-760) through  */
+/* qdb_top_sort_update (qdb/kernel/compiler.cpp:881-975): sorts the batch's  */
+/* row ids in place when sort_input, then merges them with the `state` rows  */
+/* (already in order), a state row first on equal keys; writes the picks     */
+/* (0 = state row pick_idx, 1 = batch row pick_idx) and returns their count. */
+int64_t oracle_top_sort_update(const qdb_sort_spec* spec, const qdb_rowset* state,
+                               const qdb_rowset* batch, int64_t* row_ids, int64_t n,
+                               bool sort_input, uint8_t* pick_src, uint32_t* pick_idx,
+                               int64_t limit, char* err, size_t err_len);
+
 /* Threaded baselines (timed on the host; the reference's plan shapes).      */
 /* Each returns elapsed seconds of the operator only, or < 0 on error.       */
 double oracle_bench_aggregate(const qdb_aggregate_spec* spec,

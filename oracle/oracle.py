@@ -26,7 +26,8 @@ class OracleTable(C.Structure):
 
 
 def build() -> Path:
-    srcs = [HERE / "oracle.cpp", HERE / "oracle.h", HERE.parent / "include" / "qdb_gpu.h"]
+    srcs = [HERE / "oracle.cpp", HERE / "oracle.h", HERE / "Makefile", HERE.parent / "include" / "qdb_gpu.h",
+            HERE.parent / "qumirdb_b200" / "csrc" / "datagen.cpp"]
     if not LIB.exists() or LIB.stat().st_mtime < max(s.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
@@ -61,6 +62,11 @@ def lib() -> C.CDLL:
             "oracle_bench_join_sum": (C.c_double, [P, P, P, C.c_int64, C.c_int32, P, P, C.c_int64, C.c_int32,
                                                    C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
             "oracle_bench_sort": (C.c_double, [P, P, C.c_int64, C.c_int32, P]),
+            # The seeded workload generators (same code as the device library's).
+            "qdb_gen_lineitem": (None, [C.c_uint64, C.c_int64, P, P, P, P, P, P, P]),
+            "qdb_gen_join": (None, [C.c_uint64, C.c_int64, C.c_int64, C.c_int64, P, P, P, P, P]),
+            "qdb_gen_zipf": (None, [C.c_uint64, C.c_int64, C.c_int64, C.c_double, P, P, P]),
+            "qdb_gen_sort": (None, [C.c_uint64, C.c_int64, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -177,3 +183,47 @@ def top_k(spec, store_rowsets, row_ids: np.ndarray, limit: int, descs=None, null
     k = lib().oracle_top_k(C.byref(spec.struct), store, ids.ctypes.data, len(ids), limit,
                            None if d is None else d.ctypes.data, None if nf is None else nf.ctypes.data)
     return ids[:k]
+
+
+def _table_arrays(t: OracleTable) -> tuple[list[np.ndarray], list[np.ndarray]]:
+    """Columns of an oracle table as numpy arrays: int64 for integers (object
+    for 128-bit decimals), float64 for doubles, and a validity array each."""
+    n, m = t.rows, t.cols
+    if n == 0:
+        return [np.zeros(0, np.int64) for _ in range(m)], [np.zeros(0, bool) for _ in range(m)]
+    cells = np.ctypeslib.as_array(t.cells, shape=(n * m * 2,)).reshape(n, m, 2).copy()
+    valid = np.ctypeslib.as_array(t.valid, shape=(n * m,)).reshape(n, m).astype(bool)
+    values = []
+    for c in range(m):
+        ty = t.types[c]
+        lo = cells[:, c, 0]
+        if ty in (abi.F64, abi.F32):
+            values.append(lo.view(np.float64))
+        elif ty == abi.DECIMAL128:
+            hi = cells[:, c, 1]
+            values.append(np.array([(int(h) << 64) | (int(x) & ((1 << 64) - 1)) for x, h in zip(lo, hi)], dtype=object))
+        else:
+            values.append(lo)
+    return values, [valid[:, c].copy() for c in range(m)]
+
+
+def aggregate_arrays(spec, rowsets, lanes: int = 1) -> tuple[list[np.ndarray], list[np.ndarray]]:
+    """oracle_aggregate with the result as numpy columns (for large tables)."""
+    t = OracleTable()
+    err = C.create_string_buffer(512)
+    arr = _rowsets(rowsets)
+    if lib().oracle_aggregate(C.byref(spec.struct), arr, len(rowsets), lanes, C.byref(t), err, 512) != 0:
+        raise RuntimeError(err.value.decode())
+    try:
+        return _table_arrays(t)
+    finally:
+        lib().oracle_table_free(C.byref(t))
+
+
+def sorted_row_indices(k1: np.ndarray, k2: np.ndarray, threads: int) -> np.ndarray:
+    """Row indices in the stable order ORDER BY k1 DESC, k2 ASC (ties in
+    input order) by the threaded LSD + k-way merge plan."""
+    n = len(k1)
+    out = np.empty(n, np.int64)
+    lib().oracle_bench_sort(k1.ctypes.data, k2.ctypes.data, n, threads, out.ctypes.data)
+    return out

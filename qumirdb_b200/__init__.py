@@ -610,6 +610,55 @@ class Sort:
         return k
 
 
+class TopSort:
+    """TTopSortProcessor (qdb/exec/sort_exec.cpp:627-760) over the device:
+    Add(batch) keeps the first `limit` rows of the order seen so far
+    (qdb_gpu_top_sort_update), choosing top-K selection of the batch first
+    when the engine's heap rule takes it (K <= 1024 and K <= rows / 4,
+    sort_exec.cpp:56-65); state() is the kept rows, in order."""
+
+    def __init__(self, prog: Program, limit: int):
+        _ensure_init()
+        self.prog = prog
+        self.limit = limit
+        self.state = abi.RowSet()
+        self.calls = []
+
+    def add(self, batch, selection=None) -> int:
+        n = batch.rs.RowCount
+        rows = np.arange(n, dtype=np.int64) if selection is None else np.flatnonzero(selection).astype(np.int64)
+        if len(rows) == 0 or self.limit <= 0:
+            return int(self.state.RowCount)
+        ids = np.ascontiguousarray(rows)            # (0 << 32) | row
+        sort_input = True
+        m = len(ids)
+        if self.limit <= 1024 and self.limit <= m // 4:
+            one = rowset_array([batch])
+            k = lib().qdb_gpu_top_k_select(self.prog.handle, one, ids.ctypes.data, m, self.limit)
+            if k <= 0:
+                raise QdbError(f"top-k failed: {last_error()}")
+            m, sort_input = k, False
+        cap = min(self.limit, int(self.state.RowCount) + m)
+        ids = np.concatenate([ids, np.zeros(max(0, cap - len(ids)), np.int64)])
+        src = np.zeros(max(cap, 1), np.uint8)
+        idx = np.zeros(max(cap, 1), np.uint32)
+        nxt = abi.RowSet()
+        r = lib().qdb_gpu_top_sort_update(self.prog.handle, C.byref(self.state), batch.ptr, ids.ctypes.data, None,
+                                          None, m, sort_input, src.ctypes.data, idx.ctypes.data, self.limit,
+                                          C.byref(nxt))
+        if r < 0:
+            raise QdbError(f"top-sort update failed: {last_error()}")
+        self.calls.append((src[:r].copy(), idx[:r].copy()))
+        if r > 0:
+            release(self.state)
+            self.state = nxt
+        return int(self.state.RowCount)
+
+    def release(self) -> None:
+        release(self.state)
+        self.state = abi.RowSet()
+
+
 def profile(on: bool) -> None:
     lib().qdb_gpu_profile_enable(1 if on else 0)
 

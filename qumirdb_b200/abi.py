@@ -126,6 +126,7 @@ SIGNATURES = {
     "qdb_gpu_join_aggregate_probe": (CI64, [P, P, P, P, PRS]),
     "qdb_gpu_sort_run": (CI64, [P, PRS, P, P, P, CI64, P, P, BOOLC, CI64, CI64, PRS]),
     "qdb_gpu_top_k_select": (CI64, [P, PRS, P, CI64, CI64]),
+    "qdb_gpu_top_sort_update": (CI64, [P, PRS, PRS, P, P, P, CI64, BOOLC, P, P, CI64, PRS]),
     "qdb_gpu_agg_run_noalloc": (CI64, [P, PRS, C.POINTER(Column), CI64]),
     "qdb_gpu_init": (C.c_int, [C.c_int]),
     "qdb_gpu_last_error": (C.c_char_p, []),

@@ -2987,9 +2987,9 @@ void AggFinalizeBatch(const AggPlan& p, const OutputPlan& out, const GTableDev& 
 // Aggregation without device allocation.
 //
 // Some embedders cannot allocate device memory while a query runs: an engine
-// that hands the GPU a fixed memory budget up front, a caller recording work
-// into a CUDA graph, or a process whose allocator belongs to another runtime.
-// For them one whole aggregate (table init, fused update, finalize) runs in
+// that hands the GPU a fixed memory budget up front and must stay inside it,
+// or a process whose device allocator belongs to another runtime.  For them
+// one whole aggregate (table init, fused update, finalize) runs in
 // this file-scope scratch array instead of cudaMalloc'd buffers.  Every GPU
 // that loads the library holds it until the process exits.  All calls share
 // it and it keeps the last call's contents, so each call clears the counters

@@ -313,12 +313,26 @@ BatchConfig Search(const AggPlan& p, const FastPlan& f, const std::vector<HighTa
     return best;
 }
 
-std::string ConfigKey(const std::string& shape, int64_t ntasks, int64_t nitems, const BatchConfig& c,
-                      const BatchContext& cx) {
-    char buf[256];
-    std::snprintf(buf, sizeof(buf), "|%lld|%lld|%d|%d|%lld|%p|%p|%p|%p|%p", (long long)ntasks, (long long)nitems,
-                  c.threads, c.smem_slots, (long long)c.chunk_rows, (void*)cx.d_tasks, (void*)cx.d_items,
-                  (void*)cx.d_new, (void*)cx.d_deferred, (void*)cx.d_spill);
+// FNV-1a over a plan's bytes.
+uint64_t PlanBytesHash(const void* p, size_t n, uint64_t h = 1469598103934665603ull) {
+    const auto* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    return h;
+}
+
+// Identity of a recorded launch sequence.  A captured graph holds the
+// launch's AggLaunch by value: the resolved plan (column pointers of the
+// first row set, filter literals, affine constants, IN-lists) and the typed
+// shape's constants.  Two programs of one shape that differ only in a
+// literal must not share a graph, so the key covers every byte of both
+// plans besides the batch structure and the context's buffers.
+std::string ConfigKey(const std::string& shape, const AggPlan& plan, const FastPlan& fast, int64_t ntasks,
+                      int64_t nitems, const BatchConfig& c, const BatchContext& cx) {
+    const uint64_t h = PlanBytesHash(&fast, sizeof(fast), PlanBytesHash(&plan, sizeof(plan)));
+    char buf[320];
+    std::snprintf(buf, sizeof(buf), "|%016llx|%lld|%lld|%d|%d|%lld|%p|%p|%p|%p|%p", (unsigned long long)h,
+                  (long long)ntasks, (long long)nitems, c.threads, c.smem_slots, (long long)c.chunk_rows,
+                  (void*)cx.d_tasks, (void*)cx.d_items, (void*)cx.d_new, (void*)cx.d_deferred, (void*)cx.d_spill);
     return shape + buf;
 }
 
@@ -632,7 +646,7 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
         cudaMemcpyAsync(cx.h_new, cx.d_new, size_t(m) * 8, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(cx.h_counters, cx.d_counters, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st);
     };
-    const std::string gkey = ConfigKey(shape, m, nitems, cfg, cx);
+    const std::string gkey = ConfigKey(shape, P0, fast, m, nitems, cfg, cx);
     bool ran = false;
     cx.repeats = gkey == cx.last_key ? cx.repeats + 1 : 1;
     cx.last_key = gkey;

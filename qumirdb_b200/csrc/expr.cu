@@ -156,8 +156,11 @@ __global__ void __launch_bounds__(256) HashKernel(const __grid_constant__ ExprLa
         for (int j = 0; j < L.A.nhash; ++j) {
             const int c = L.A.hash_slot[j];
             const int t = L.A.hash_type[j];
+            const bool null = acc.Null(c);
+            // A nullable key is two struct fields: its BOOL validity, then the value.
+            if (L.A.hash_nullable[j]) h = Combine(h, null ? 0 : LeafHashOf(QDB_TYPE_BOOL, 1, 0.0));
             uint64_t fh = 0;
-            if (!acc.Null(c)) {
+            if (!null) {
                 const bool fl = t == QDB_TYPE_F32 || t == QDB_TYPE_F64;
                 fh = LeafHashOf(t, fl ? i128(0) : acc.Int(c), fl ? acc.F64(c) : 0.0);
             }

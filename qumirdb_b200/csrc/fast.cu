@@ -192,6 +192,8 @@ __global__ void __launch_bounds__(kJsThreads, 1) JoinSumKernel(const __grid_cons
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const int32_t nb = L.bloom_words;
+    // Tiles the producer issued bulk copies for (read only on the abort path).
+    __shared__ long long issued_tiles;
 
     if (tid == 0) {
         for (int s = 0; s < kJsStages; ++s) {
@@ -199,6 +201,7 @@ __global__ void __launch_bounds__(kJsThreads, 1) JoinSumKernel(const __grid_cons
             MbarInit(&empty[s], kJsConsumerWarps);
         }
         *abort = 0;
+        issued_tiles = 0;
         FenceBarrierInit();
     }
     // The build side's Bloom filter goes to shared memory: most probe rows
@@ -220,7 +223,8 @@ __global__ void __launch_bounds__(kJsThreads, 1) JoinSumKernel(const __grid_cons
         if ((tid & 31) == 0) {
             const uint64_t pol = EvictFirstPolicy();
             const uint32_t half = uint32_t(kJsTile * 8);
-            for (int64_t k = 0;; ++k) {
+            int64_t k = 0;
+            for (;; ++k) {
                 const int64_t t = blockIdx.x + k * gridDim.x;
                 if (t >= L.staged_tiles) break;
                 const int s = int(k % kJsStages);
@@ -234,6 +238,7 @@ __global__ void __launch_bounds__(kJsThreads, 1) JoinSumKernel(const __grid_cons
                 BulkG2SHint(st, L.S.probe_key + t * kJsTile, half, &full[s], pol);
                 if (L.vcol) BulkG2SHint(st + half, L.vcol + t * kJsTile, half, &full[s], pol);
             }
+            issued_tiles = k;
         }
     } else {
         // Consumers: staged tiles, then the rows past the last full tile.
@@ -292,10 +297,20 @@ __global__ void __launch_bounds__(kJsThreads, 1) JoinSumKernel(const __grid_cons
     }
     __syncthreads();
     if (*abort) {
-        // Let copies already issued land before the CTA's memory goes away.
+        // Copies already issued must land before the CTA's shared memory goes
+        // away.  Only the last kJsStages issued tiles can still be in flight
+        // (the producer reuses a stage only after its consumers released it,
+        // which they do after its copy landed): wait for each of their `full`
+        // phases, each wait bounded.
         if (tid == 0) {
-            const long long start = clock64();
-            while (clock64() - start < 2000000) {
+            const long long n = issued_tiles;
+            for (long long k = n > kJsStages ? n - kJsStages : 0; k < n; ++k) {
+                const int s = int(k % kJsStages);
+                const uint32_t phase = uint32_t((k / kJsStages) & 1);
+                const long long start = clock64();
+                while (!MbarTryWait(&full[s], phase)) {
+                    if (clock64() - start > kSpinCycles) break;
+                }
             }
         }
         __syncthreads();

@@ -11,7 +11,9 @@
 // streams, and almost every probe reads exactly one sector.  A probe row
 // walks its bucket sequence until an empty slot and emits one (probe row,
 // arena row) pair per equal key (jr_probe_candidates,
-// qdb/kernel/join/join_rows.oz:146-197); NULL keys match nothing.
+// qdb/kernel/join/join_rows.oz:146-197); NULL keys match nothing.  Pairs
+// come out in the engine's order: probe rows ascending, a row's build rows
+// in append order (a count pass, a scan, then a write pass).
 #include <algorithm>
 
 #include "common.cuh"
@@ -100,69 +102,103 @@ __global__ void __launch_bounds__(256) JoinBuildKernel(const __grid_constant__ J
     }
 }
 
-__global__ void __launch_bounds__(256) JoinProbePairsKernel(const __grid_constant__ JoinProbeArgs a) {
-    const int64_t warps = int64_t(gridDim.x) * (blockDim.x / 32);
-    for (int64_t base = (int64_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5)) * 32; base < a.nrows;
-         base += warps * 32) {
-        const int64_t r = base + LaneId();
-        bool act = r < a.nrows && (a.selection == nullptr || a.selection[r] != 0);
-        bool null = false;
-        uint64_t key = 0;
-        if (act) key = PackKeyCols(a, r, null);
-        act = act && !null;
-        const bool special = act && a.jkey.full64 && key == kEmptyKey;
-        uint64_t b = act ? (Fmix64(key) & a.jt.bmask) : 0;
-        int j = 0;                      // next slot of bucket b to look at
-        ulonglong2 kk = make_ulonglong2(kEmptyKey, kEmptyKey);
-        if (act && !special) kk = BucketKeys(a.jt, b);
-        int64_t sp = special ? 0 : -1;
-        const int64_t nspecial = special ? int64_t(*a.jt.nspecial) : 0;
-        uint64_t buckets_seen = 0;
-        // Walk the bucket sequence; emit a pair per equal key.
-        while (true) {
-            int64_t brow = -1;
-            if (act && !special) {
-                while (true) {
-                    if (j == 2) {
-                        if (++buckets_seen > a.jt.bmask) {
-                            act = false;
-                            break;
-                        }
-                        b = (b + 1) & a.jt.bmask;
-                        j = 0;
-                        kk = BucketKeys(a.jt, b);
-                    }
-                    const uint64_t k = j == 0 ? kk.x : kk.y;
-                    const int jj = j++;
-                    if (k == kEmptyKey) {
-                        act = false;
-                        break;
-                    }
-                    if (k == key) {
-                        brow = a.jt.rows[2 * b + jj];
-                        break;
-                    }
-                }
-            } else if (special) {
-                if (sp < nspecial) brow = a.jt.special_rows[2 * sp++];
-                else act = false;
+// Calls emit(arena row) for every build row whose key equals probe row r's
+// (none for an unselected row or a NULL key) and returns their number.
+template <class F>
+__device__ __forceinline__ unsigned ProbeRowMatches(const JoinProbeArgs& a, int64_t r, F&& emit) {
+    if (a.selection != nullptr && a.selection[r] == 0) return 0;
+    bool null = false;
+    const uint64_t key = PackKeyCols(a, r, null);
+    if (null) return 0;
+    if (a.jkey.full64 && key == kEmptyKey) {
+        const int64_t nspecial = int64_t(*a.jt.nspecial);
+        for (int64_t sp = 0; sp < nspecial; ++sp) emit(a.jt.special_rows[2 * sp]);
+        return unsigned(nspecial);
+    }
+    const uint64_t b = Fmix64(key) & a.jt.bmask;
+    return VisitMatches(a.jt, key, b, BucketKeys(a.jt, b),
+                        [&](uint64_t slot, uint64_t, int) { emit(a.jt.rows[slot]); });
+}
+
+// Rows of one chunk of the pair probe (one block per chunk).
+constexpr int kPairChunk = 2048;
+constexpr int kPairThreads = 256;
+
+// Pass 1: every row's match count, and the chunk's total.
+__global__ void __launch_bounds__(kPairThreads) JoinPairCountKernel(const __grid_constant__ JoinProbeArgs a,
+                                                                    uint32_t* counts,
+                                                                    unsigned long long* chunk_tot) {
+    __shared__ unsigned long long warp_sum[kPairThreads / 32];
+    const int64_t begin = int64_t(blockIdx.x) * kPairChunk;
+    const int64_t end = min(a.nrows, begin + kPairChunk);
+    unsigned long long local = 0;
+    for (int64_t r = begin + threadIdx.x; r < end; r += kPairThreads) {
+        const unsigned c = ProbeRowMatches(a, r, [](int64_t) {});
+        counts[r] = c;
+        local += c;
+    }
+    local = WarpSumU64(local);
+    if (LaneId() == 0) warp_sum[threadIdx.x >> 5] = local;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kPairThreads / 32; ++w) t += warp_sum[w];
+        chunk_tot[blockIdx.x] = t;
+    }
+}
+
+// Pass 2: row r's pairs go to [off(r), off(r) + counts[r]), off = the
+// chunk's offset plus the counts of the chunk's earlier rows, so pairs list
+// probe rows in order; a row's own pairs are then put in arena (build
+// append) order, the order of the engine's chains (jr_build_rows links the
+// table last -> first, qdb/kernel/join/join_rows.oz:70-113).
+__global__ void __launch_bounds__(kPairThreads) JoinPairWriteKernel(const __grid_constant__ JoinProbeArgs a,
+                                                                    const uint32_t* counts,
+                                                                    const unsigned long long* chunk_off) {
+    __shared__ unsigned long long warp_sum[kPairThreads / 32];
+    const int64_t begin = int64_t(blockIdx.x) * kPairChunk;
+    const int64_t end = min(a.nrows, begin + kPairChunk);
+    unsigned long long base = chunk_off[blockIdx.x];
+    for (int64_t t0 = begin; t0 < end; t0 += kPairThreads) {
+        const int64_t r = t0 + threadIdx.x;
+        const unsigned long long c = r < end ? counts[r] : 0;
+        // Block-wide exclusive scan of the tile's counts.
+        unsigned long long incl = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kFull, incl, d);
+            if (LaneId() >= d) incl += y;
+        }
+        if (LaneId() == 31) warp_sum[threadIdx.x >> 5] = incl;
+        __syncthreads();
+        unsigned long long before = 0, tile = 0;
+        for (int w = 0; w < kPairThreads / 32; ++w) {
+            const unsigned long long v = warp_sum[w];
+            if (w < int(threadIdx.x >> 5)) before += v;
+            tile += v;
+        }
+        __syncthreads();
+        const unsigned long long off = base + before + incl - c;
+        base += tile;
+        if (c == 0 || int64_t(off + c) > a.pair_cap) continue;
+        int64_t* out = a.pairs + 2 * off;
+        unsigned k = 0;
+        ProbeRowMatches(a, r, [&](int64_t brow) {
+            if (k < c) {
+                out[2 * k] = r;
+                out[2 * k + 1] = brow;
             }
-            const bool emit = brow >= 0;
-            const unsigned m = __ballot_sync(kFull, emit);
-            if (m == 0 && !__any_sync(kFull, act)) break;
-            if (m) {
-                unsigned long long at = 0;
-                if (LaneId() == __ffs(m) - 1) at = atomicAdd(a.npairs, (unsigned long long)__popc(m));
-                at = __shfl_sync(kFull, at, __ffs(m) - 1);
-                if (emit) {
-                    const unsigned long long slot = at + __popc(m & ((1u << LaneId()) - 1));
-                    if (int64_t(slot) < a.pair_cap) {
-                        a.pairs[2 * slot] = r;
-                        a.pairs[2 * slot + 1] = brow;
-                    }
-                }
+            ++k;
+        });
+        // Arena order within the row (insertion sort; chains are short).
+        for (unsigned x = 1; x < c; ++x) {
+            const int64_t v = out[2 * x + 1];
+            unsigned y = x;
+            while (y > 0 && out[2 * (y - 1) + 1] > v) {
+                out[2 * y + 1] = out[2 * (y - 1) + 1];
+                --y;
             }
-            if (!__any_sync(kFull, act)) break;
+            out[2 * y + 1] = v;
         }
     }
 }
@@ -208,10 +244,21 @@ void JoinBuildBloom(const JTableDev& jt, uint32_t* bloom, int32_t nwords, cudaSt
     CountLaunch();
 }
 
-void JoinProbePairs(const JoinProbeArgs& a, cudaStream_t s) {
+int64_t JoinPairChunks(int64_t nrows) { return (nrows + kPairChunk - 1) / kPairChunk; }
+
+void JoinProbeCount(const JoinProbeArgs& a, uint32_t* counts, unsigned long long* chunk_tot, cudaStream_t s) {
+    if (a.nrows == 0) return;
+    ProfileBegin(s, "join_probe_count", a.nrows);
+    JoinPairCountKernel<<<unsigned(JoinPairChunks(a.nrows)), kPairThreads, 0, s>>>(a, counts, chunk_tot);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+void JoinProbeWrite(const JoinProbeArgs& a, const uint32_t* counts, const unsigned long long* chunk_off,
+                    cudaStream_t s) {
     if (a.nrows == 0) return;
     ProfileBegin(s, "join_probe_pairs", a.nrows);
-    JoinProbePairsKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(a);
+    JoinPairWriteKernel<<<unsigned(JoinPairChunks(a.nrows)), kPairThreads, 0, s>>>(a, counts, chunk_off);
     ProfileEnd(s);
     CountLaunch();
 }

@@ -347,30 +347,45 @@ bool Probe(const qdb_gpu_program* prog, ArenaState* a, TableState* t, PairBuf* p
     }
     PairState* ps = pairs->state;
     ps->arena = a;
-    unsigned long long* dn = static_cast<unsigned long long*>(DevAlloc(8, s));
-    int64_t want = std::max<int64_t>(n, 1024);
-    for (int attempt = 0; attempt < 2; ++attempt) {
-        if (ps->cap < want) {
-            DevFree(ps->dev, s);
-            ps->cap = want;
-            ps->dev = static_cast<int64_t*>(DevAlloc(size_t(ps->cap) * 16, s));
-            if (!ps->dev) return false;
-        }
-        cudaMemsetAsync(dn, 0, 8, s);
-        p.pairs = ps->dev;
-        p.pair_cap = ps->cap;
-        p.npairs = dn;
-        JoinProbePairs(p, s);
-        unsigned long long cnt = 0;
-        cudaMemcpyAsync(&cnt, dn, 8, cudaMemcpyDeviceToHost, s);
-        if (!CudaOk(cudaStreamSynchronize(s), "row join probe")) return false;
-        pairs->count = int64_t(cnt);
-        pairs->capacity = ps->cap;
-        if (pairs->count <= ps->cap) break;
-        want = pairs->count;   // too small: size it to the count and probe again
+    // Count pass, scan of the chunk totals (the last entry becomes the
+    // total), then the write pass into a buffer of exactly that size.
+    const int64_t nch = JoinPairChunks(n);
+    auto* counts = static_cast<uint32_t*>(DevAlloc(size_t(std::max<int64_t>(n, 1)) * 4, s));
+    auto* off = static_cast<unsigned long long*>(DevAlloc(size_t(nch + 1) * 8, s));
+    if (!counts || !off) {
+        DevFree(counts, s);
+        DevFree(off, s);
+        return false;
     }
-    DevFree(dn, s);
-    return true;
+    cudaMemsetAsync(off, 0, size_t(nch + 1) * 8, s);
+    JoinProbeCount(p, counts, off, s);
+    ExclusiveScanU64(off, nch + 1, s);
+    unsigned long long total = 0;
+    cudaMemcpyAsync(&total, off + nch, 8, cudaMemcpyDeviceToHost, s);
+    if (!CudaOk(cudaStreamSynchronize(s), "row join probe count")) {
+        DevFree(counts, s);
+        DevFree(off, s);
+        return false;
+    }
+    if (ps->cap < int64_t(total) || !ps->dev) {
+        DevFree(ps->dev, s);
+        ps->cap = std::max<int64_t>(int64_t(total), 1024);
+        ps->dev = static_cast<int64_t*>(DevAlloc(size_t(ps->cap) * 16, s));
+        if (!ps->dev) {
+            ps->cap = 0;
+            DevFree(counts, s);
+            DevFree(off, s);
+            return false;
+        }
+    }
+    p.pairs = ps->dev;
+    p.pair_cap = ps->cap;
+    JoinProbeWrite(p, counts, off, s);
+    DevFree(counts, s);
+    DevFree(off, s);
+    pairs->count = int64_t(total);
+    pairs->capacity = ps->cap;
+    return CudaOk(cudaStreamSynchronize(s), "row join probe");
 }
 
 }  // namespace

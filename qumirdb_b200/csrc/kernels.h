@@ -157,10 +157,16 @@ struct JoinProbeArgs {
     int64_t nrows;
     int64_t* pairs;          // (probe row, build row)
     int64_t pair_cap;
-    unsigned long long* npairs;
     int* err;
 };
-void JoinProbePairs(const JoinProbeArgs& a, cudaStream_t s);
+// The pair probe in two passes: per-row match counts plus per-chunk totals
+// (JoinPairChunks(nrows) of them), then, after an exclusive scan of the
+// totals, the pairs themselves at their offsets (probe rows ascending, a
+// row's build rows in append order).  Pairs past pair_cap are not written.
+int64_t JoinPairChunks(int64_t nrows);
+void JoinProbeCount(const JoinProbeArgs& a, uint32_t* counts, unsigned long long* chunk_tot, cudaStream_t s);
+void JoinProbeWrite(const JoinProbeArgs& a, const uint32_t* counts, const unsigned long long* chunk_off,
+                    cudaStream_t s);
 
 // Gathers rows: out[i] = src[idx[i]] for `width`-byte values (idx < 0 -> 0).
 void GatherColumn(const char* src, int width, const int64_t* idx, int idx_stride, int64_t n, char* out,
@@ -192,6 +198,7 @@ struct ExprArgs {
     int32_t nhash = 0;
     uint8_t hash_slot[kMaxKeyParts] = {};
     int32_t hash_type[kMaxKeyParts] = {};
+    uint8_t hash_nullable[kMaxKeyParts] = {};   // the key struct has a validity field
     uint64_t* hashes = nullptr;
     int* err = nullptr;
 };

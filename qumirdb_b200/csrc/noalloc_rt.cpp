@@ -2,6 +2,7 @@
 // (qdb_gpu_agg_run_noalloc).  Inputs and outputs must already be in device
 // memory; table, counters and finalize scratch live in a fixed file-scope
 // device array (agg.cu).
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -55,21 +56,37 @@ extern "C" int64_t qdb_gpu_agg_run_noalloc(const qdb_gpu_program* prog, const qd
 
     cudaStream_t s = CurStream();
     std::vector<AggOutputCol> cols(size_t(lw.out.n));
+    // Every output buffer is checked before anything is written.
     for (int k = 0; k < lw.out.n; ++k) {
-        qdb_column& oc = out_columns[k];
+        const qdb_column& oc = out_columns[k];
         if (!oc.Data || !IsDevicePtr(oc.Data)) {
             SetErr("agg_run_noalloc: output column %d needs a device buffer", k);
             return -1;
         }
+        const int type = lw.out.out_type[k];
+        const uintptr_t align = type == QDB_TYPE_DECIMAL128 ? 16 : uintptr_t(std::max(1, StorageWidth(type)));
+        if (reinterpret_cast<uintptr_t>(oc.Data) % std::min<uintptr_t>(align, 8)) {
+            SetErr("agg_run_noalloc: output column %d is not aligned to its value width", k);
+            return -1;
+        }
+        if (oc.Mask && (!IsDevicePtr(oc.Mask) || reinterpret_cast<uintptr_t>(oc.Mask) % 4)) {
+            SetErr("agg_run_noalloc: output mask %d must be 4-byte aligned device memory of "
+                   "(out_capacity + 31) / 32 uint32 words", k);
+            return -1;
+        }
+        if (oc.Offsets && type == QDB_TYPE_CHAR1 &&
+            (!IsDevicePtr(oc.Offsets) || reinterpret_cast<uintptr_t>(oc.Offsets) % 4)) {
+            SetErr("agg_run_noalloc: output offsets %d must be 4-byte aligned device memory", k);
+            return -1;
+        }
+    }
+    for (int k = 0; k < lw.out.n; ++k) {
+        qdb_column& oc = out_columns[k];
         AggOutputCol& c = cols[size_t(k)];
         std::memset(&c, 0, sizeof(c));
         c.type = lw.out.out_type[k];
         c.data = oc.Data;
         if (oc.Mask) {
-            if (!IsDevicePtr(oc.Mask)) {
-                SetErr("agg_run_noalloc: output mask %d is not in device memory", k);
-                return -1;
-            }
             c.valid = reinterpret_cast<uint32_t*>(const_cast<uint8_t*>(oc.Mask));
             cudaMemsetAsync(c.valid, 0, size_t((out_capacity + 31) / 32) * 4, s);
         }

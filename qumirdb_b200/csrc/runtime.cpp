@@ -905,8 +905,6 @@ qdb_gpu_program* qdb_gpu_compile_hash(int32_t n_columns, const qdb_column_type* 
         for (int j = 0; j < n_keys; ++j) {
             if (key_columns[j] < 0 || key_columns[j] >= n_columns) throw LowerError("key column out of range");
             const qdb_column_type& ct = columns[key_columns[j]];
-            if (ct.nullable) throw LowerError("nullable shuffle keys are not served");
-            if (ct.type == QDB_TYPE_BOOL) throw LowerError("boolean shuffle keys are not served");
             std::memset(&nodes[j], 0, sizeof(qdb_expr));
             nodes[j].op = QDB_EXPR_COLUMN;
             nodes[j].type = ct.type;
@@ -1108,6 +1106,7 @@ bool qdb_gpu_hash(const qdb_gpu_program* prog, qdb_rowset* batch, uint64_t* hash
     for (int j = 0; j < a.nhash; ++j) {
         a.hash_slot[j] = uint8_t(prog->expr.value_idx[j]);
         a.hash_type[j] = prog->expr.out_types[j];
+        a.hash_nullable[j] = plan.cols[a.hash_slot[j]].nullable;
     }
     const bool dev_out = IsDevicePtr(hashes);
     uint64_t* out = dev_out ? hashes : static_cast<uint64_t*>(DevAlloc(size_t(batch->RowCount) * 8, s));

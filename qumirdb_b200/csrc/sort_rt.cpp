@@ -1,6 +1,8 @@
 // sort_rt.cpp — sort entries of the C ABI: qdb_sort_run (sort + slice
-// materialize, BuildSortRunWrapperAst, qdb/kernel/compiler.cpp:1165-1218) and
-// qdb_top_k_select (THeapTopKDispatch, qdb/kernel/compiler.h:585-596).
+// materialize, BuildSortRunWrapperAst, qdb/kernel/compiler.cpp:1165-1218),
+// qdb_top_k_select (THeapTopKDispatch, qdb/kernel/compiler.h:585-596) and
+// qdb_top_sort_update (TTopSortDispatch, compiler.h:570-583; the update of
+// BuildTopSortUpdateAst, compiler.cpp:881-975).
 //
 // The store is the engine's array of retained batches (TSortProcessor::Add,
 // qdb/exec/sort_exec.cpp:427-440) addressed by packed row ids; the number of
@@ -293,6 +295,106 @@ int64_t Materialize(const qdb_gpu_program* prog, qdb_rowset* store, const int64_
     return rows;
 }
 
+// The first k row ids of the order (the keys, then the packed row id as the
+// tie break, compiler.h:135-148) among the `size` device row ids `ids`,
+// left in ids[0, k); returns k, or -1.
+int64_t TopKDevice(const qdb_gpu_program* prog, qdb_rowset* store, int64_t* ids, int64_t size, int64_t k,
+                   Scratch& sc, Staging& stg) {
+    cudaStream_t s = sc.s;
+    // Runs of consecutive rows (a scan's row ids) are fetched without their ids.
+    int64_t* tiles = TileMarks(size, sc);
+    if (!tiles) return -1;
+    int64_t nbatches = 0;
+    if (!BatchCount(ids, size, sc, nbatches, tiles)) return -1;
+    StoreView v;
+    // Exact order: row id first (the tie break, compiler.h:135-148), then the keys.
+    const std::vector<SortStage> stages = MakeStages(prog->sort, nullptr, nullptr, true, v);
+    if (!BuildStoreView(prog->sort, store, nbatches, stg, v)) return -1;
+    const SortStage primary = stages.back().src == SS_NULL_RANK ? stages[stages.size() - 2] : stages.back();
+    int* derr = static_cast<int*>(sc.Get(sizeof(int)));
+    auto* counts = static_cast<unsigned long long*>(sc.Get(4096 * 8));
+    if (!derr || !counts) return -1;
+    cudaMemsetAsync(derr, 0, sizeof(int), s);
+
+    if (SortKeyWidth(primary.type) < 0) {
+        SetErr("top-k: the first key's type is not a sort key type");
+        return -1;
+    }
+    const int64_t cap = std::max<int64_t>(4 * k, int64_t(1) << 20);
+    int64_t* cand = nullptr;
+    int64_t take = -1;
+
+    // Sampled threshold: the r-th smallest primary key of ns rows spread
+    // evenly over the input has about r * size / ns rows at or below it
+    // (spread sqrt(r) * size / ns).  r is chosen so that count is at least K
+    // with a margin of six spreads and is expected to fit the candidate
+    // buffer.  The sample, the selection of its r-th key and the pass that
+    // collects every row at or below it run back to back on the device; the
+    // host reads only the count.  The result is exact whatever the sample
+    // says: a count below K or above the buffer falls through to the radix
+    // select.
+    if (size > cap) {
+        const int64_t ns = std::min<int64_t>(kTopKSamples, size);
+        const double per = double(size) / double(ns);
+        const double mk = double(k) / per;
+        const int64_t r = int64_t(std::ceil(mk + 6.0 * std::sqrt(mk) + 8.0));
+        if (r <= ns && (double(r) + 6.0 * std::sqrt(double(r))) * per <= double(cap)) {
+            auto* skeys = static_cast<uint64_t*>(sc.Get(size_t(ns) * 8));
+            auto* tau = static_cast<uint64_t*>(sc.Get(8));
+            cand = static_cast<int64_t*>(sc.Get(size_t(cap) * 8));
+            auto* ccount = static_cast<unsigned long long*>(sc.Get(8));
+            if (!skeys || !tau || !cand || !ccount) return -1;
+            TopKThreshold(ids, size, v.t, primary, skeys, ns, r, tau, derr, s);
+            TopKCollect(ids, size, v.t, primary, 0, 64, tau, cand, cap, ccount, tiles, derr, s);
+            unsigned long long got = 0;
+            cudaMemcpyAsync(&got, ccount, 8, cudaMemcpyDeviceToHost, s);
+            if (!ReadError(derr, s, "top-k: collect")) return -1;
+            if (int64_t(got) >= k && int64_t(got) <= cap) take = int64_t(got);
+        }
+    }
+
+    // Radix select on the primary key: narrow the bucket holding the K-th
+    // row until the rows at or below it are few enough to order exactly.
+    if (take < 0) {
+        uint64_t prefix = 0;
+        int pbits = 0;
+        int64_t below = 0;
+        take = size;
+        std::vector<unsigned long long> h(4096);
+        while (pbits < 64) {
+            const int dbits = std::min(12, 64 - pbits);
+            TopKHistogram(ids, size, v.t, primary, 64 - pbits - dbits, dbits, prefix, pbits, counts, derr, s);
+            cudaMemcpyAsync(h.data(), counts, 4096 * 8, cudaMemcpyDeviceToHost, s);
+            if (!ReadError(derr, s, "top-k: histogram")) return -1;
+            int64_t run = below;
+            int b = 0;
+            for (; b < (1 << dbits) - 1; ++b) {
+                if (run + int64_t(h[b]) >= k) break;
+                run += int64_t(h[b]);
+            }
+            below = run;
+            prefix = (prefix << dbits) | uint64_t(b);
+            pbits += dbits;
+            take = below + int64_t(h[b]);
+            if (take <= cap) break;
+        }
+        if (!cand || take > cap) cand = static_cast<int64_t*>(sc.Get(size_t(take) * 8));
+        auto* ccount = static_cast<unsigned long long*>(sc.Get(8));
+        if (!cand || !ccount) return -1;
+        TopKCollect(ids, size, v.t, primary, prefix, pbits, nullptr, cand, take, ccount, tiles, derr, s);
+        unsigned long long got = 0;
+        cudaMemcpyAsync(&got, ccount, 8, cudaMemcpyDeviceToHost, s);
+        if (!ReadError(derr, s, "top-k: collect")) return -1;
+        if (int64_t(got) != take) {
+            SetErr("top-k: collected %llu rows, expected %lld", got, (long long)take);
+            return -1;
+        }
+    }
+    if (!SortIds(cand, take, stages, v.t, sc)) return -1;
+    if (cand != ids) cudaMemcpyAsync(ids, cand, size_t(k) * 8, cudaMemcpyDeviceToDevice, s);
+    return k;
+}
+
 const qdb_gpu_program* SortProgramOf(const qdb_gpu_program* p) {
     if (!p || p->kind != PK_SORT) {
         SetErr("not a sort program");
@@ -440,99 +542,144 @@ int64_t qdb_gpu_top_k_select(const qdb_gpu_program* program, qdb_rowset* store, 
         if (!ids) return -1;
         cudaMemcpyAsync(ids, row_ids, size_t(size) * 8, cudaMemcpyHostToDevice, s);
     }
-    // Runs of consecutive rows (a scan's row ids) are fetched without their ids.
-    int64_t* tiles = TileMarks(size, sc);
-    if (!tiles) return -1;
-    int64_t nbatches = 0;
-    if (!BatchCount(ids, size, sc, nbatches, tiles)) return -1;
-    StoreView v;
-    // Exact order: row id first (the tie break, compiler.h:135-148), then the keys.
-    const std::vector<SortStage> stages = MakeStages(prog->sort, nullptr, nullptr, true, v);
-    if (!BuildStoreView(prog->sort, store, nbatches, stg, v)) return -1;
-    const SortStage primary = stages.back().src == SS_NULL_RANK ? stages[stages.size() - 2] : stages.back();
-    int* derr = static_cast<int*>(sc.Get(sizeof(int)));
-    auto* counts = static_cast<unsigned long long*>(sc.Get(4096 * 8));
-    if (!derr || !counts) return -1;
-    cudaMemsetAsync(derr, 0, sizeof(int), s);
-
-    if (SortKeyWidth(primary.type) < 0) {
-        SetErr("top-k: the first key's type is not a sort key type");
-        return -1;
-    }
-    const int64_t cap = std::max<int64_t>(4 * k, int64_t(1) << 20);
-    int64_t* cand = nullptr;
-    int64_t take = -1;
-
-    // Sampled threshold: the r-th smallest primary key of ns rows spread
-    // evenly over the input has about r * size / ns rows at or below it
-    // (spread sqrt(r) * size / ns).  r is chosen so that count is at least K
-    // with a margin of six spreads and is expected to fit the candidate
-    // buffer.  The sample, the selection of its r-th key and the pass that
-    // collects every row at or below it run back to back on the device; the
-    // host reads only the count.  The result is exact whatever the sample
-    // says: a count below K or above the buffer falls through to the radix
-    // select.
-    if (size > cap) {
-        const int64_t ns = std::min<int64_t>(kTopKSamples, size);
-        const double per = double(size) / double(ns);
-        const double mk = double(k) / per;
-        const int64_t r = int64_t(std::ceil(mk + 6.0 * std::sqrt(mk) + 8.0));
-        if (r <= ns && (double(r) + 6.0 * std::sqrt(double(r))) * per <= double(cap)) {
-            auto* skeys = static_cast<uint64_t*>(sc.Get(size_t(ns) * 8));
-            auto* tau = static_cast<uint64_t*>(sc.Get(8));
-            cand = static_cast<int64_t*>(sc.Get(size_t(cap) * 8));
-            auto* ccount = static_cast<unsigned long long*>(sc.Get(8));
-            if (!skeys || !tau || !cand || !ccount) return -1;
-            TopKThreshold(ids, size, v.t, primary, skeys, ns, r, tau, derr, s);
-            TopKCollect(ids, size, v.t, primary, 0, 64, tau, cand, cap, ccount, tiles, derr, s);
-            unsigned long long got = 0;
-            cudaMemcpyAsync(&got, ccount, 8, cudaMemcpyDeviceToHost, s);
-            if (!ReadError(derr, s, "top-k: collect")) return -1;
-            if (int64_t(got) >= k && int64_t(got) <= cap) take = int64_t(got);
-        }
-    }
-
-    // Radix select on the primary key: narrow the bucket holding the K-th
-    // row until the rows at or below it are few enough to order exactly.
-    if (take < 0) {
-        uint64_t prefix = 0;
-        int pbits = 0;
-        int64_t below = 0;
-        take = size;
-        std::vector<unsigned long long> h(4096);
-        while (pbits < 64) {
-            const int dbits = std::min(12, 64 - pbits);
-            TopKHistogram(ids, size, v.t, primary, 64 - pbits - dbits, dbits, prefix, pbits, counts, derr, s);
-            cudaMemcpyAsync(h.data(), counts, 4096 * 8, cudaMemcpyDeviceToHost, s);
-            if (!ReadError(derr, s, "top-k: histogram")) return -1;
-            int64_t run = below;
-            int b = 0;
-            for (; b < (1 << dbits) - 1; ++b) {
-                if (run + int64_t(h[b]) >= k) break;
-                run += int64_t(h[b]);
-            }
-            below = run;
-            prefix = (prefix << dbits) | uint64_t(b);
-            pbits += dbits;
-            take = below + int64_t(h[b]);
-            if (take <= cap) break;
-        }
-        if (!cand || take > cap) cand = static_cast<int64_t*>(sc.Get(size_t(take) * 8));
-        auto* ccount = static_cast<unsigned long long*>(sc.Get(8));
-        if (!cand || !ccount) return -1;
-        TopKCollect(ids, size, v.t, primary, prefix, pbits, nullptr, cand, take, ccount, tiles, derr, s);
-        unsigned long long got = 0;
-        cudaMemcpyAsync(&got, ccount, 8, cudaMemcpyDeviceToHost, s);
-        if (!ReadError(derr, s, "top-k: collect")) return -1;
-        if (int64_t(got) != take) {
-            SetErr("top-k: collected %llu rows, expected %lld", got, (long long)take);
-            return -1;
-        }
-    }
-    if (!SortIds(cand, take, stages, v.t, sc)) return -1;
-    cudaMemcpyAsync(row_ids, cand, size_t(k) * 8, dev_ids ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);
+    if (TopKDevice(prog, store, ids, size, k, sc, stg) < 0) return -1;
+    if (!dev_ids) cudaMemcpyAsync(row_ids, ids, size_t(k) * 8, cudaMemcpyDeviceToHost, s);
     if (!CudaOk(cudaStreamSynchronize(s), "top-k")) return -1;
     return k;
+}
+
+// Writes n int64 values to `dst`, host or device memory.
+static bool PutI64(int64_t* dst, const int64_t* src, int64_t n, cudaStream_t s) {
+    if (n <= 0) return true;
+    if (IsDevicePtr(dst)) return CudaOk(cudaMemcpyAsync(dst, src, size_t(n) * 8, cudaMemcpyHostToDevice, s), "copy");
+    std::memcpy(dst, src, size_t(n) * 8);
+    return true;
+}
+
+int64_t qdb_gpu_top_sort_update(const qdb_gpu_program* program, qdb_rowset* state, qdb_rowset* batch,
+                                int64_t* row_ids, int64_t* work, uint32_t* counts, int64_t n, bool sort_input,
+                                uint8_t* pick_src, uint32_t* pick_idx, int64_t limit, qdb_rowset* out) {
+    (void)work;
+    (void)counts;
+    t_error.clear();
+    const qdb_gpu_program* prog = SortProgramOf(program);
+    if (!prog) return -1;
+    const SortProgram& P = prog->sort;
+    if (!state || !batch || !out || (n > 0 && !row_ids) || n < 0) {
+        SetErr("top-sort: state, batch, output and row ids are needed");
+        return -1;
+    }
+    // The state is this call's output of the previous call: it must have the
+    // batch's schema, so the program materializes every column in order.
+    bool identity = P.out_columns.size() == P.columns.size();
+    for (size_t c = 0; identity && c < P.out_columns.size(); ++c) identity = P.out_columns[c] == int(c);
+    if (!identity) {
+        SetErr("top-sort: the program must materialize every input column in order (the state keeps the schema)");
+        return -1;
+    }
+    if (n > int64_t(UINT32_MAX)) {
+        SetErr("top-sort: more than 2^32 rows");
+        return -1;
+    }
+    const int64_t state_n = std::max<int64_t>(0, state->RowCount);
+    if (limit <= 0) {
+        std::memset(out, 0, sizeof(*out));
+        return 0;
+    }
+    cudaStream_t s = CurStream();
+    Scratch sc(s);
+    Staging stg(s);
+
+    // 1. The batch's first k rows of the order (sort_input: sort them here,
+    // stable in row-id order; else they arrive ordered, e.g. by top-K).
+    const int64_t k = std::min(n, limit);
+    std::vector<int64_t> temp(size_t(std::max<int64_t>(k, 0)));
+    if (k > 0) {
+        int64_t* ids = row_ids;
+        if (!IsDevicePtr(row_ids)) {
+            ids = static_cast<int64_t*>(sc.Get(size_t(n) * 8));
+            if (!ids) return -1;
+            cudaMemcpyAsync(ids, row_ids, size_t(n) * 8, cudaMemcpyHostToDevice, s);
+        }
+        if (sort_input && n > 1) {
+            int64_t nbatches = 0;
+            if (!BatchCount(ids, n, sc, nbatches)) return -1;
+            if (nbatches > 1) {
+                SetErr("top-sort: the batch's row ids must name batch 0");
+                return -1;
+            }
+            qdb_rowset one[1] = {*batch};
+            if (k < n) {
+                if (TopKDevice(prog, one, ids, n, k, sc, stg) < 0) return -1;
+            } else {
+                StoreView v;
+                const std::vector<SortStage> stages = MakeStages(P, nullptr, nullptr, false, v);
+                if (!BuildStoreView(P, one, 1, stg, v)) return -1;
+                if (!SortIds(ids, n, stages, v.t, sc)) return -1;
+            }
+        }
+        cudaMemcpyAsync(temp.data(), ids, size_t(k) * 8, cudaMemcpyDeviceToHost, s);
+        if (!CudaOk(cudaStreamSynchronize(s), "top-sort: batch order")) return -1;
+    }
+
+    // 2. Merge with the state (top_sort_merge_picks, qdb/kernel/sort/top_sort.oz:15-57):
+    // a stable sort of the state rows followed by the batch rows keeps the
+    // state row first on equal keys, as the merge does.  Row ids name the
+    // store [state, batch].
+    const int64_t m = state_n + k;
+    const int64_t out_count = std::min(limit, m);
+    std::vector<int64_t> comb(size_t(std::max<int64_t>(m, 1)));
+    for (int64_t i = 0; i < state_n; ++i) comb[size_t(i)] = i;
+    for (int64_t j = 0; j < k; ++j) comb[size_t(state_n + j)] = (int64_t(1) << 32) | int64_t(uint32_t(temp[size_t(j)]));
+    qdb_rowset two[2] = {*state, *batch};
+    int64_t* dcomb = static_cast<int64_t*>(sc.Get(size_t(std::max<int64_t>(m, 1)) * 8));
+    if (!dcomb) return -1;
+    if (state_n > 0 && k > 0) {
+        cudaMemcpyAsync(dcomb, comb.data(), size_t(m) * 8, cudaMemcpyHostToDevice, s);
+        StoreView v;
+        const std::vector<SortStage> stages = MakeStages(P, nullptr, nullptr, false, v);
+        if (!BuildStoreView(P, two, 2, stg, v)) return -1;
+        if (!SortIds(dcomb, m, stages, v.t, sc)) return -1;
+        cudaMemcpyAsync(comb.data(), dcomb, size_t(out_count) * 8, cudaMemcpyDeviceToHost, s);
+        if (!CudaOk(cudaStreamSynchronize(s), "top-sort: merge")) return -1;
+    }
+
+    // 3. The picks, and row_ids[i] = (pick_src << 32) | pick_idx as the
+    // reference leaves them.
+    for (int64_t i = 0; i < out_count; ++i) {
+        const int64_t id = comb[size_t(i)];
+        if (pick_src && !IsDevicePtr(pick_src)) pick_src[i] = uint8_t(id >> 32);
+        if (pick_idx && !IsDevicePtr(pick_idx)) pick_idx[i] = uint32_t(id);
+    }
+    if (pick_src && IsDevicePtr(pick_src)) {
+        std::vector<uint8_t> ps(static_cast<size_t>(out_count));
+        for (int64_t i = 0; i < out_count; ++i) ps[size_t(i)] = uint8_t(comb[size_t(i)] >> 32);
+        cudaMemcpyAsync(pick_src, ps.data(), ps.size(), cudaMemcpyHostToDevice, s);
+        if (!CudaOk(cudaStreamSynchronize(s), "top-sort: picks")) return -1;
+    }
+    if (pick_idx && IsDevicePtr(pick_idx)) {
+        std::vector<uint32_t> pi(static_cast<size_t>(out_count));
+        for (int64_t i = 0; i < out_count; ++i) pi[size_t(i)] = uint32_t(comb[size_t(i)]);
+        cudaMemcpyAsync(pick_idx, pi.data(), pi.size() * 4, cudaMemcpyHostToDevice, s);
+        if (!CudaOk(cudaStreamSynchronize(s), "top-sort: picks")) return -1;
+    }
+    if (out_count > 0 && row_ids && !PutI64(row_ids, comb.data(), out_count, s)) return -1;
+    if (out_count <= 0) {
+        std::memset(out, 0, sizeof(*out));
+        return 0;
+    }
+
+    // 4. Materialize the kept rows from [state, batch] (just the batch when
+    // the state is empty).
+    qdb_rowset* store = two;
+    if (state_n == 0) {
+        for (int64_t i = 0; i < out_count; ++i) comb[size_t(i)] &= 0xffffffffll;
+        store = two + 1;
+    }
+    cudaMemcpyAsync(dcomb, comb.data(), size_t(out_count) * 8, cudaMemcpyHostToDevice, s);
+    const int64_t r = Materialize(prog, store, dcomb, out_count, sc, stg, out);
+    if (r >= 0 && !CudaOk(cudaStreamSynchronize(s), "top-sort")) return -1;
+    return r;
 }
 
 }  // extern "C"

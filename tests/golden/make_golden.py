@@ -8,7 +8,8 @@ goldens it has for aggregation, sort and join.  test_golden.py restates each
 listed query as this library's operator descriptors and compares the oracle
 (CPU) and the device path (GPU) with the expected rows.
 
-usage: python tests/golden/make_golden.py [REFERENCE_REGTEST_DIR]
+usage: python tests/golden/make_golden.py REFERENCE_REGTEST_DIR
+(the test/regtest directory of a checkout of the reference)
 """
 from __future__ import annotations
 
@@ -37,7 +38,9 @@ CASES = {
 
 
 def main() -> None:
-    root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/test/regtest")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py REFERENCE_REGTEST_DIR")
+    root = Path(sys.argv[1])
     out = {"source": "test/regtest of the reference (cases/<suite>/tables, goldens/<suite>/<case>.result.json)",
            "tables": {}, "cases": {}}
     for suite, cases in CASES.items():

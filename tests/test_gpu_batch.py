@@ -145,3 +145,35 @@ def test_batch_states_without_a_batched_kernel():
         want = O.aggregate(spec, [q.HostRowSet(p, m)])
         assert_same_groups(gpu_rows(o, types), want, types, nkeys=1)
         q.release(o)
+
+
+@pytest.mark.parametrize("form", ["filter_literal", "affine_constant"])
+def test_same_shape_programs_with_other_literals_do_not_share_a_graph(form):
+    """Two programs of one shape that differ only in a literal (a filter
+    constant, or the constant of SUM(a + c)) alternate after the launch
+    sequence of the first was captured as a graph (three identical batches
+    in a row): each batch must give its own program's groups."""
+    sizes = [20_000, 3_000, 45_000, 9_000]
+    parts = partitions(9, sizes, 5_000)
+
+    def spec(c):
+        e = q.ExprBuilder()
+        key, a = e.col(0, abi.I64), e.col(1, abi.I64)
+        if form == "filter_literal":
+            pred = e.op(abi.LT, abi.BOOL, a, e.const(c, abi.I64))
+            return queries.AggSpec(queries.ZIPF_COLUMNS, e, pred, [key], [(abi.SUM, a), (abi.COUNT_STAR, -1)])
+        val = e.op(abi.ADD, abi.I64, a, e.const(c, abi.I64))
+        return queries.AggSpec(queries.ZIPF_COLUMNS, e, None, [key], [(abi.SUM, val), (abi.COUNT_STAR, -1)])
+
+    specs = {c: spec(c) for c in (5, 90_000)}
+    progs = {c: q.compile_aggregate(s) for c, s in specs.items()}
+    rowsets = [q.DeviceRowSet(p) for p in parts]
+    types = [abi.I64, abi.I64, abi.I64]
+    want = {c: [O.aggregate(specs[c], [q.HostRowSet(p)]) for p in parts] for c in specs}
+    for c in [5, 5, 5, 5, 90_000, 5, 90_000, 90_000, 90_000, 5]:
+        batch = q.AggregateBatch(progs[c], len(parts))
+        batch.add(rowsets)
+        outs = batch.finish()
+        for i in range(len(parts)):
+            assert_same_groups(gpu_rows(outs[i], types), want[c][i], types, nkeys=1)
+        outs.release()

@@ -82,8 +82,18 @@ def test_duplicate_build_keys_and_null_keys():
     assert got == want
 
 
-def test_pair_probe_and_materialize():
+@pytest.mark.parametrize("dups", [False, True])
+def test_pair_probe_and_materialize(dups):
+    """Pairs in the engine's emission order, compared without sorting: probe
+    rows ascending, a probe row's build rows in append order (the chain order
+    of jr_build_rows / jr_probe_candidates, join_rows.oz:70-197), then
+    materialized in 1000-row slices."""
     b, p = join_data(5000, 20_000, 6000)
+    if dups:
+        rng = np.random.default_rng(4)
+        b[0] = rng.integers(1, 800, len(b[0])).astype(np.int64)   # ~6 build rows per key
+        b[1] = np.arange(1, len(b[0]) + 1, dtype=np.int64)         # payload names the build row
+        p[0][::13] = -1                                              # keys that match nothing
     jspec, _ = queries.join_sum(20)
     prog = q.compile_row_join(jspec)
     J = q.RowJoin(prog)
@@ -93,7 +103,6 @@ def test_pair_probe_and_materialize():
     n = J.probe(prs)
     want = O.row_join(jspec, [brs], prs)
     assert n == len(want)
-    # Materialize in 1000-row slices: (fk, value, payload) per pair.
     got = []
     start = 0
     while start < n:
@@ -104,8 +113,8 @@ def test_pair_probe_and_materialize():
         start += k
     keep = b[2] < 20
     arena_payload = b[1][keep]
-    want_rows = sorted((int(p[0][r]), int(p[1][r]), int(arena_payload[br])) for r, br in want)
-    assert sorted(got) == want_rows
+    want_rows = [(int(p[0][r]), int(p[1][r]), int(arena_payload[br])) for r, br in want]
+    assert got == want_rows
 
 
 def _shape_aggs(e, name):
