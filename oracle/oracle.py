@@ -57,6 +57,9 @@ def lib() -> C.CDLL:
                                       C.c_char_p, C.c_size_t]),
             "oracle_top_k": (C.c_int64, [C.POINTER(abi.SortSpec), C.POINTER(abi.RowSet), P, C.c_int64, C.c_int64,
                                          P, P]),
+            "oracle_top_sort_update": (C.c_int64, [C.POINTER(abi.SortSpec), C.POINTER(abi.RowSet),
+                                                   C.POINTER(abi.RowSet), P, C.c_int64, C.c_bool, P, P, C.c_int64,
+                                                   C.c_char_p, C.c_size_t]),
             "oracle_bench_aggregate": (C.c_double, [C.POINTER(abi.AggregateSpec), C.POINTER(abi.RowSet), C.c_int32,
                                                     C.POINTER(C.c_int64)]),
             "oracle_bench_join_sum": (C.c_double, [P, P, P, C.c_int64, C.c_int32, P, P, C.c_int64, C.c_int32,

@@ -997,10 +997,10 @@ struct Shape {
     __host__ __device__ static constexpr bool cu(int k) { return (Cols::at(k) & 1) != 0; }
 };
 
+// 128-bit add through the carry flag (add.cc / addc): no compare and select
+// for the carry.
 __device__ __forceinline__ void Add128(uint64_t& lo, uint64_t& hi, uint64_t l, uint64_t h) {
-    const uint64_t n = lo + l;
-    hi += h + (n < lo ? 1ull : 0ull);
-    lo = n;
+    asm("add.cc.u64 %0, %0, %2;\n\taddc.u64 %1, %1, %3;" : "+l"(lo), "+l"(hi) : "l"(l), "l"(h));
 }
 
 // Fast column K of tile row r (cb: the tile's column bases).
@@ -1928,6 +1928,264 @@ __global__ void __launch_bounds__(kSigThreads, 1) AggSigDirectKernel(const __gri
     if (tid == 0 && sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
 }
 
+// ---------------------------------------------------------------------------
+// Low-cardinality scan aggregate, four rows per thread: each lane of a warp
+// takes four consecutive rows of a 128-row warp tile, loading every column
+// of the four with one or two vector loads (8-byte columns 2 x 16 B, 4-byte
+// 16 B, 2-byte 8 B, 1-byte 4 B; all coalesced across the warp), so loads and
+// their address arithmetic are a quarter of the one-row walk's and four rows'
+// loads are in flight per lane.  Rows fold into the same lane-private
+// accumulators (the first kPrivGroups groups) as AggSigDirectKernel; two CTAs
+// of 256 threads share an SM.  Columns must start on a boundary of four
+// values (16 B at most), checked by the host.
+// ---------------------------------------------------------------------------
+constexpr int kQuadThreads = 256;
+constexpr int kQuadRows = 4;
+
+// Column K of the four rows starting at row r4 (nvalid of them inside the
+// range; zeros past it).
+template <class SH, int K>
+__device__ __forceinline__ void LoadQuadCol(int64_t (&out)[kQuadRows], const char* base, int64_t r4, int nvalid) {
+    constexpr int w = SH::cw(K);
+    constexpr bool u = SH::cu(K);
+    const char* p = base + r4 * w;
+    if (nvalid == kQuadRows) {
+        if constexpr (w == 8) {
+            const longlong2 a = __ldcs(reinterpret_cast<const longlong2*>(p));
+            const longlong2 b = __ldcs(reinterpret_cast<const longlong2*>(p) + 1);
+            out[0] = a.x;
+            out[1] = a.y;
+            out[2] = b.x;
+            out[3] = b.y;
+        } else if constexpr (w == 4) {
+            const int4 a = __ldcs(reinterpret_cast<const int4*>(p));
+            const int32_t v[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) out[j] = u ? int64_t(uint32_t(v[j])) : int64_t(v[j]);
+        } else if constexpr (w == 2) {
+            const uint2 a = __ldcs(reinterpret_cast<const uint2*>(p));
+            const uint32_t v[4] = {a.x & 0xffffu, a.x >> 16, a.y & 0xffffu, a.y >> 16};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) out[j] = u ? int64_t(v[j]) : int64_t(int16_t(uint16_t(v[j])));
+        } else {
+            const uint32_t a = __ldcs(reinterpret_cast<const unsigned int*>(p));
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t b = (a >> (8 * j)) & 0xffu;
+                out[j] = u ? int64_t(b) : int64_t(int8_t(uint8_t(b)));
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < kQuadRows; ++j) {
+            const char* pj = p + j * w;
+            int64_t v = 0;
+            if (j < nvalid) {
+                if constexpr (w == 8) v = *reinterpret_cast<const int64_t*>(pj);
+                else if constexpr (w == 4) v = u ? int64_t(*reinterpret_cast<const uint32_t*>(pj))
+                                                 : int64_t(*reinterpret_cast<const int32_t*>(pj));
+                else if constexpr (w == 2) v = u ? int64_t(*reinterpret_cast<const uint16_t*>(pj))
+                                                 : int64_t(*reinterpret_cast<const int16_t*>(pj));
+                else v = u ? int64_t(*reinterpret_cast<const uint8_t*>(pj)) : int64_t(*reinterpret_cast<const int8_t*>(pj));
+            }
+            out[j] = v;
+        }
+    }
+}
+
+template <class SH, int K = 0>
+__device__ __forceinline__ void LoadQuad(int64_t (&q)[SH::Cols::n > 0 ? SH::Cols::n : 1][kQuadRows],
+                                         const char* const* cb, int64_t r4, int nvalid) {
+    if constexpr (K < SH::Cols::n) {
+        LoadQuadCol<SH, K>(q[K], cb[K], r4, nvalid);
+        LoadQuad<SH, K + 1>(q, cb, r4, nvalid);
+    }
+}
+
+template <class SH, int K = 0>
+__device__ __forceinline__ void QuadRow(RegRow<SH::Cols::n>& row,
+                                        const int64_t (&q)[SH::Cols::n > 0 ? SH::Cols::n : 1][kQuadRows], int j) {
+    if constexpr (K < SH::Cols::n) {
+        row.v[K] = q[K][j];
+        QuadRow<SH, K + 1>(row, q, j);
+    }
+}
+
+template <class SIG>
+__global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid_constant__ AggLaunch L) {
+    unsigned char* smem = DynSmem();
+    unsigned* misc = reinterpret_cast<unsigned*>(smem + L.off_misc);
+    const SmemTable sm = MakeSmem(L, false, true);
+    const AggPlan& P = L.P;
+    const FastPlan& F = L.F;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    constexpr int bd = kQuadThreads;
+
+    if (tid == 0) {
+        misc[0] = 0;
+        misc[1] = 0;
+        misc[2] = 0;
+        misc[4] = 0;
+    }
+    for (int i = tid; i < sm.S; i += bd) {
+        sm.keys[i] = kEmptyKey;
+        sm.gid[i] = -1;
+        for (int s = 0; s < P.nstates; ++s) {
+            const StateDesc sd = P.states[s];
+            sm.st[int64_t(sd.word) * sm.S + i] = StateIdentity(sd.kind);
+            if (sd.kind == ST_SUM_I128) sm.st[int64_t(sd.word + 1) * sm.S + i] = 0;
+        }
+    }
+    uint64_t* pacc = reinterpret_cast<uint64_t*>(smem + L.off_pacc);
+    for (int i = tid; i < kPrivGroups * SIG::words * bd; i += bd) pacc[i] = 0;
+    __syncthreads();
+    if (P.nkeyparts == 0 && tid == 0 && sm.S > 0) {
+        const int i = int(uint32_t(Fmix64(0)) & uint32_t(sm.S - 1));
+        sm.keys[i] = 0;
+        sm.gid[i] = 0;
+        sm.gid_slot[0] = i;
+        misc[0] = 1;
+        misc[2] = 1;
+    }
+    __syncthreads();
+
+    uint64_t ckey[kPrivGroups];
+    int cgid[kPrivGroups];
+#pragma unroll
+    for (int j = 0; j < kPrivGroups; ++j) {
+        ckey[j] = kEmptyKey;
+        cgid[j] = -1;
+    }
+    int ncache = 0;
+    if (P.nkeyparts == 0) {
+        ckey[0] = 0;
+        cgid[0] = 0;
+        ncache = 1;
+    }
+
+    // Contiguous range per CTA, a multiple of the 128-row warp tile.
+    constexpr int kWarpRows = 32 * kQuadRows;
+    int64_t per = (L.nrows + gridDim.x - 1) / gridDim.x;
+    per = (per + kWarpRows - 1) / kWarpRows * kWarpRows;
+    const int64_t row0 = int64_t(blockIdx.x) * per;
+    const int64_t n = max(int64_t(0), min(per, L.nrows - row0));
+    const char* cb[kFastCols];
+#pragma unroll
+    for (int c = 0; c < kFastCols; ++c) {
+        cb[c] = nullptr;
+        if (c < SIG::Cols::n) cb[c] = P.cols[F.col_slot[c]].data + row0 * SIG::cw(c);
+    }
+    const uint8_t* sel = P.selection ? P.selection + row0 : nullptr;
+    constexpr int NC = SIG::Cols::n > 0 ? SIG::Cols::n : 1;
+#pragma unroll 1
+    for (int64_t r4 = int64_t(tid >> 5) * kWarpRows + lane * kQuadRows; r4 < n; r4 += (bd >> 5) * kWarpRows) {
+        const int nvalid = int(min(int64_t(kQuadRows), n - r4));
+        int64_t q[NC][kQuadRows];
+        LoadQuad<SIG>(q, cb, r4, nvalid);
+        uint32_t selq = nvalid == kQuadRows ? 0x01010101u : 0u;
+        if (nvalid < kQuadRows) {
+            for (int j = 0; j < nvalid; ++j) selq |= 1u << (8 * j);
+        }
+        if (sel) {
+            if (nvalid == kQuadRows) {
+                selq = __ldcs(reinterpret_cast<const unsigned int*>(sel + r4));
+            } else {
+                uint32_t m = 0;
+                for (int j = 0; j < nvalid; ++j) m |= uint32_t(sel[r4 + j]) << (8 * j);
+                selq = m;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kQuadRows; ++j) {
+            if (((selq >> (8 * j)) & 0xffu) == 0) continue;
+            RegRow<SIG::Cols::n> cur;
+            QuadRow<SIG>(cur, q, j);
+            if (SIG::Atoms::n && ShapeHeld<SIG>(P, F, cur) != F.clause_mask) continue;
+            const uint64_t key = ShapeKey<SIG>(cur);
+            int g = -1;
+#pragma unroll
+            for (int k = 0; k < kPrivGroups; ++k) g = ckey[k] == key ? cgid[k] : g;
+            if (g < 0 && !(P.key_full64 && key == kEmptyKey)) {
+                const int slot = sm.Find(key);
+                if (slot >= 0) {
+                    const int gg = *reinterpret_cast<volatile int*>(&sm.gid[slot]);
+                    if (gg >= 0 && gg < kPrivGroups && ncache < kPrivGroups) {
+                        g = gg;
+#pragma unroll
+                        for (int k = 0; k < kPrivGroups; ++k) {
+                            if (k == ncache) {
+                                ckey[k] = key;
+                                cgid[k] = gg;
+                            }
+                        }
+                        ++ncache;
+                    }
+                }
+            }
+            if (g >= 0) {
+                ShapeFoldP<SIG, kQuadThreads>(pacc + g * SIG::words * kQuadThreads + tid, F, cur);
+            } else {
+                RowAcc acc{&P, nullptr, 0, row0 + r4 + j, 0, -1, 0};
+                FoldRowFast<false>(L, acc);
+            }
+        }
+    }
+    __syncthreads();
+
+    // Lane-private accumulators -> shared table -> global table, as in
+    // AggSigDirectKernel.
+    const int ng = int(min(*reinterpret_cast<volatile unsigned*>(sm.ngid), unsigned(kPrivGroups)));
+    constexpr int nwarps = bd >> 5;
+    for (int item = tid >> 5; item < ng * SIG::n; item += nwarps) {
+        const int qg = item / SIG::n;
+        const int st2 = item - qg * SIG::n;
+        const int o = SIG::off(st2);
+        const bool wide2 = SIG::width(st2) == 2;
+        uint64_t lo = 0, hi = 0;
+        for (int t2 = lane; t2 < bd; t2 += 32) {
+            const uint64_t* w = pacc + int64_t(qg * SIG::words + o) * bd + t2;
+            Add128(lo, hi, w[0], wide2 ? w[bd] : 0ull);
+        }
+        WarpSum128(lo, hi);
+        if (lane == 0 && (lo | hi)) {
+            const int slot = *reinterpret_cast<volatile int*>(&sm.gid_slot[qg]);
+            const StateDesc sd = P.states[st2];
+            uint64_t* w = sm.st + int64_t(sd.word) * sm.S + slot;
+            ApplyState(w, w + sm.S, sd.kind, lo, hi, 0.0);
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < sm.S; i += bd) {
+        const uint64_t key = sm.keys[i];
+        if (key == kEmptyKey) continue;
+        int is_new = 0;
+        const int64_t g = GlobalFind1(L.T, L.cap_mask, key, is_new);
+        if (is_new) atomicAdd(sm.fresh, 1u);
+        if (g < 0) {
+            const unsigned long long e = atomicAdd(&L.counters->spilled, 1ull);
+            if (int64_t(e) >= L.spill_cap) {
+                SetError(&L.counters->error, DE_SPILL_FULL);
+                continue;
+            }
+            uint64_t* rec = L.spill + int64_t(e) * (1 + P.state_words);
+            rec[0] = key;
+            for (int w = 0; w < P.state_words; ++w) rec[1 + w] = sm.st[int64_t(w) * sm.S + i];
+            continue;
+        }
+        uint64_t* gbase = L.T.slots + g * L.T.slot_words + L.T.state_off;
+        for (int st2 = 0; st2 < P.nstates; ++st2) {
+            const StateDesc sd = P.states[st2];
+            const uint64_t lo = sm.st[int64_t(sd.word) * sm.S + i];
+            const uint64_t hi = sd.kind == ST_SUM_I128 ? sm.st[int64_t(sd.word + 1) * sm.S + i] : 0;
+            if (IsIdentity(sd.kind, lo, hi)) continue;
+            ApplyState(gbase + sd.word, gbase + sd.word + 1, sd.kind, lo, hi, 0.0);
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
+}
+
 // The instantiated query shapes.  QDB_C(w, u): a fast column of w bytes
 // (u: unsigned); QDB_A(op, col): a filter atom; QDB_S(kind, nf, cols...): a
 // state.  A plan whose shape is not listed runs the general typed kernel.
@@ -2503,11 +2761,12 @@ SigKernelFn FindHighKernel(const AggPlan& P, const FastPlan& F) {
     return nullptr;
 }
 
-SigKernelFn FindSigKernel(const AggPlan& P, const FastPlan& F) {
+SigKernelFn FindSigKernel(const AggPlan& P, const FastPlan& F, bool quad) {
     const std::vector<int> key = ShapeKeyOf(P, F);
     if (key.empty()) return nullptr;
-#define QDB_SHAPE_FIND(...) \
-    if (ShapeMatches<__VA_ARGS__>(key) && ShapeWordsMatch<__VA_ARGS__>(F)) return AggSigDirectKernel<__VA_ARGS__>;
+#define QDB_SHAPE_FIND(...)                                                            \
+    if (ShapeMatches<__VA_ARGS__>(key) && ShapeWordsMatch<__VA_ARGS__>(F))             \
+        return quad ? AggSigQuadKernel<__VA_ARGS__> : AggSigDirectKernel<__VA_ARGS__>;
     QDB_SHAPE_LIST(QDB_SHAPE_FIND)
 #undef QDB_SHAPE_FIND
     if (std::getenv("QDB_SHAPE_DEBUG")) {
@@ -2636,7 +2895,43 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
     if (a.fast && variant == 1 && any) {
         // A typed plan with an instantiated state signature: the listed-row
         // kernel (no lane-private arrays; the group lists take their place).
-        if (SigKernelFn fn = FindSigKernel(L.P, *a.fast)) {
+        // Four rows per thread when every typed column (and the selection)
+        // starts on a boundary of four values.
+        bool quad = true;
+        for (int c = 0; c < a.fast->ncols && quad; ++c) {
+            const ColDesc& cd = L.P.cols[a.fast->col_slot[c]];
+            quad = (reinterpret_cast<uintptr_t>(cd.data) % uintptr_t(std::min(16, 4 * int(cd.width)))) == 0;
+        }
+        if (L.P.selection && (reinterpret_cast<uintptr_t>(L.P.selection) & 3)) quad = false;
+        if (quad) {
+            if (SigKernelFn fn = FindSigKernel(L.P, *a.fast, true)) {
+                L.F = *a.fast;
+                layout(16, 1, 64);
+                const size_t bytes = size_t(L.off_pacc) + size_t(kPrivGroups) * sw * kQuadThreads * 8;
+                if (bytes <= budget) {
+                    L.smem_slots = 64;
+                    L.smem_limit = 32;
+                    L.priv = 1;
+                    SetSmem(fn, bytes);
+                    int per_sm = 1;
+                    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kQuadThreads, bytes) != cudaSuccess) {
+                        cudaGetLastError();
+                        per_sm = 1;
+                    }
+                    // At least 16K rows per CTA: the merge at the end costs a few
+                    // microseconds per CTA.
+                    const int64_t nt = (a.nrows + (int64_t(1) << 14) - 1) >> 14;
+                    const int g2 = int(std::max<int64_t>(1, std::min<int64_t>(nt, int64_t(g_sms) * std::max(1, per_sm))));
+                    ProfileBegin(s, "agg_update_sig", a.nrows);
+                    fn<<<g2, kQuadThreads, bytes, s>>>(L);
+                    ProfileEnd(s);
+                    CountLaunch();
+                    return;
+                }
+                layout(T, stages, S);
+            }
+        }
+        if (SigKernelFn fn = FindSigKernel(L.P, *a.fast, false)) {
             L.F = *a.fast;
             // The kernel stages nothing: a token stage keeps the layout's offsets.
             layout(16, 1, 64);

@@ -271,3 +271,25 @@ def test_high_cardinality_shape_kernels(shape):
     assert "agg_update_high" in names, names
     want = O.aggregate(spec, [q.HostRowSet([c[lo:hi] for c in cols]) for lo, hi in bounds])
     assert_same_groups(got, want, types, nkeys=1)
+
+
+@pytest.mark.parametrize("offset", [0, 1, 4, 129])
+def test_low_cardinality_kernels_at_any_column_alignment(offset):
+    """Columns that start on a four-value boundary take the four-rows-per-
+    thread kernel; a slice starting at another row takes the one-row walk.
+    Both, over ranges whose CTA tails are ragged, equal the oracle."""
+    n = 300_007
+    cols = lineitem(n + offset, seed=17)
+    spec = queries.lineitem_agg(int(cols[6].max()) - 90)
+    base = q.DeviceRowSet(cols)
+    part = q.SliceRowSet(base, offset, n + offset)
+    q.profile(True)
+    q.profile_read()
+    out = run_gpu(spec, [part])
+    names = {kk[0] for kk in q.profile_read()}
+    q.profile(False)
+    got = gpu_rows(out, queries.LINEITEM_OUT_TYPES)
+    q.release(out)
+    assert "agg_update_sig" in names, names
+    want = O.aggregate(spec, [q.HostRowSet([c[offset:offset + n] for c in cols])])
+    assert_same_groups(got, want, queries.LINEITEM_OUT_TYPES, nkeys=2)
