@@ -470,7 +470,8 @@ void qdb_gpu_autotune_reset(void);
 /* and out_columns[k] describes caller-owned device buffers for output        */
 /* column k: Data holds out_capacity values (aligned to the value width);    */
 /* Mask, when set, is (out_capacity + 31) / 32 uint32 words, 4-byte aligned   */
-/* (all of them are cleared, then bit i set for a valid row i); Offsets,      */
+/* (all are cleared, then bit i set for a valid row i; bits past the group    */
+/* count inside the last word written are unspecified); Offsets,             */
 /* when set on a one-byte string column, out_capacity + 1 int32.             */
 /* Returns the group count, or -1 (see qdb_gpu_last_error) when an input is   */
 /* not in device memory, a buffer is misaligned, the groups exceed            */

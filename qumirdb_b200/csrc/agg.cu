@@ -2892,9 +2892,9 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
     const int grid = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, g_sms)));
     const bool gen = L.P.generic_root >= 0;
     const int variant = (wide ? 8 : 0) | (a.join ? 4 : 0) | (gen ? 2 : 0) | (priv ? 1 : 0);
-    if (a.fast && variant == 1 && any) {
+    if (a.fast && variant == 1) {
         // A typed plan with an instantiated state signature: the listed-row
-        // kernel (no lane-private arrays; the group lists take their place).
+        // kernels read their columns straight from HBM (nothing is staged).
         // Four rows per thread when every typed column (and the selection)
         // starts on a boundary of four values.
         bool quad = true;

@@ -35,6 +35,7 @@
 #include <tuple>
 #include <vector>
 
+#include "common.cuh"
 #include "fast.h"
 #include "runtime.h"
 
@@ -63,6 +64,7 @@ struct Tuner {
     int64_t tuned = 0;      // searches run
     int64_t trials = 0;     // candidate launches timed
     int64_t reused = 0;     // batches served from a stored choice
+    int64_t resized = 0;    // launches run again with tables for one group per row
 };
 
 Tuner& Tune() {
@@ -321,14 +323,26 @@ uint64_t PlanBytesHash(const void* p, size_t n, uint64_t h = 1469598103934665603
 }
 
 // Identity of a recorded launch sequence.  A captured graph holds the
-// launch's AggLaunch by value: the resolved plan (column pointers of the
-// first row set, filter literals, affine constants, IN-lists) and the typed
-// shape's constants.  Two programs of one shape that differ only in a
-// literal must not share a graph, so the key covers every byte of both
-// plans besides the batch structure and the context's buffers.
+// launch's AggLaunch by value: the resolved plan (filter literals, affine
+// constants, IN-lists) and the typed shape's constants.  Two programs of one
+// shape that differ only in a literal must not share a graph, so the key
+// covers both plans' bytes besides the batch structure and the context's
+// buffers.
 std::string ConfigKey(const std::string& shape, const AggPlan& plan, const FastPlan& fast, int64_t ntasks,
                       int64_t nitems, const BatchConfig& c, const BatchContext& cx) {
-    const uint64_t h = PlanBytesHash(&fast, sizeof(fast), PlanBytesHash(&plan, sizeof(plan)));
+    // The batched kernel reads every row set's columns from its task (uploaded
+    // on each replay); the plan's own column and selection pointers (those
+    // of the first row set) are not part of the identity.
+    AggPlan bare = plan;
+    for (int c = 0; c < kMaxCols; ++c) {
+        bare.cols[c].data = nullptr;
+        bare.cols[c].mask = nullptr;
+        bare.cols[c].mask_off = 0;
+        bare.cols[c].bit_off = 0;
+    }
+    bare.selection = nullptr;
+    bare.has_selection = 0;
+    const uint64_t h = PlanBytesHash(&fast, sizeof(fast), PlanBytesHash(&bare, sizeof(bare)));
     char buf[320];
     std::snprintf(buf, sizeof(buf), "|%016llx|%lld|%lld|%d|%d|%lld|%p|%p|%p|%p|%p", (unsigned long long)h,
                   (long long)ntasks, (long long)nitems, c.threads, c.smem_slots, (long long)c.chunk_rows,
@@ -417,11 +431,28 @@ void DestroySlice(qdb_rowset* rs) {
 
 }  // namespace
 
+namespace {
+int64_t DispatchBatch(const qdb_gpu_program* prog, void* const* hts, qdb_rowset* const* batches, int64_t n,
+                      bool every_row_a_group);
+}
+
 extern "C" {
 
 int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts, qdb_rowset* const* batches,
                                    int64_t n) {
     t_error.clear();
+    return DispatchBatch(prog, hts, batches, n, false);
+}
+
+}  // extern "C"
+
+namespace {
+
+// The batched update.  Fresh tables are sized from the groups-per-row ratio
+// seen so far for the program's shape; with every_row_a_group they are sized
+// for one group per row instead (no insert can then run out of room).
+int64_t DispatchBatch(const qdb_gpu_program* prog, void* const* hts, qdb_rowset* const* batches, int64_t n,
+                      bool every_row_a_group) {
     if (!prog || prog->kind != PK_AGG || (n > 0 && (!hts || !batches))) {
         SetErr("agg_dispatch_batch: not an aggregate program, or no states");
         return -1;
@@ -497,7 +528,8 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
             continue;
         }
         fresh.push_back(int(k));
-        const int64_t est = EstimateGroups(ratios, rows[size_t(i)], prog->expected_groups);
+        const int64_t est = every_row_a_group ? std::max<int64_t>(rows[size_t(i)], 1)
+                                              : EstimateGroups(ratios, rows[size_t(i)], prog->expected_groups);
         caps[size_t(k)] = std::max<int64_t>(1024, NextPow2(est + est / 4));
     }
     std::vector<HighTask> tasks(static_cast<size_t>(m));
@@ -686,6 +718,28 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
     if (!CudaOk(cudaStreamSynchronize(s), "batched aggregate update")) return -1;
     const BatchCounters bc = *cx.h_counters;
     if (bc.error) {
+        // More rows were turned away than the replay buffers hold: the tables
+        // were sized from a ratio that these row sets do not follow.  When
+        // every state of the launch was created by this call, its tables are
+        // dropped and the launch runs again with tables sized for one group
+        // per row.
+        const bool overflow = bc.error == qdb::DE_SPILL_FULL || bc.error == qdb::DE_DEFER_FULL;
+        if (overflow && !every_row_a_group && fresh.size() == size_t(m)) {
+            std::vector<void*> mh;
+            std::vector<qdb_rowset*> mb;
+            for (int64_t k = 0; k < m; ++k) {
+                const int i = members[size_t(k)];
+                AggStateDestroy(StateOf(hts[i]));
+                std::memset(hts[i], 0, QDB_HASH_TABLE_SIZE);
+                mh.push_back(hts[i]);
+                mb.push_back(batches[i]);
+            }
+            {
+                std::lock_guard<std::mutex> lk(Tune().mu);
+                Tune().resized++;
+            }
+            return DispatchBatch(prog, mh.data(), mb.data(), m, true) < 0 ? -1 : n;
+        }
         SetErr("batched aggregate kernel reported device error %d", bc.error);
         return -1;
     }
@@ -777,6 +831,10 @@ int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* prog, void* const* hts
     }
     return n;
 }
+
+}  // namespace
+
+extern "C" {
 
 int64_t qdb_gpu_agg_finish_batch(const qdb_gpu_program* prog, void* const* hts, int64_t n, qdb_rowset* outs) {
     t_error.clear();
@@ -929,6 +987,7 @@ int64_t qdb_gpu_autotune_info(char* buf, int64_t cap) {
     std::lock_guard<std::mutex> lk(t.mu);
     std::string js = "{\"searches\": " + std::to_string(t.tuned) + ", \"trials\": " + std::to_string(t.trials) +
                      ", \"reused\": " + std::to_string(t.reused) +
+                     ", \"resized\": " + std::to_string(t.resized) +
                      ", \"graph_replays\": " + std::to_string(Ctx().graph_replays) + ", \"configs\": [";
     bool first = true;
     for (auto& kv : t.best) {
@@ -954,7 +1013,7 @@ void qdb_gpu_autotune_reset(void) {
     std::lock_guard<std::mutex> lk(t.mu);
     t.best.clear();
     t.ratio.clear();
-    t.tuned = t.trials = t.reused = 0;
+    t.tuned = t.trials = t.reused = t.resized = 0;
 }
 
 }  // extern "C"

@@ -276,8 +276,9 @@ def test_high_cardinality_shape_kernels(shape):
 @pytest.mark.parametrize("offset", [0, 1, 4, 129])
 def test_low_cardinality_kernels_at_any_column_alignment(offset):
     """Columns that start on a four-value boundary take the four-rows-per-
-    thread kernel; a slice starting at another row takes the one-row walk.
-    Both, over ranges whose CTA tails are ragged, equal the oracle."""
+    thread kernel; a slice starting at another row takes the one-row walk
+    (both named agg_update_sig).  Both, over ranges whose CTA tails are
+    ragged, equal the oracle."""
     n = 300_007
     cols = lineitem(n + offset, seed=17)
     spec = queries.lineitem_agg(int(cols[6].max()) - 90)

@@ -65,8 +65,9 @@ def run_noalloc(prog, drs, types, capacity, with_offsets=False):
     for k, t in enumerate(types):
         raw = bufs[2 * k].download(np.uint8, n * abi.WIDTH[t])
         bits = np.unpackbits(bufs[2 * k + 1].download(np.uint8, words * 4), bitorder="little").astype(bool)
-        # Bits past the group count stay clear (the mask is cleared first).
-        assert not bits[n:].any()
+        # Words past the last one holding a group stay clear (the mask is
+        # cleared first; bits after the count inside that word are unspecified).
+        assert not bits[(n + 31) // 32 * 32:].any()
         host.append((raw, bits[:n]))
     rows = []
     for r in range(n):
