@@ -783,6 +783,21 @@ def main() -> None:
     achieved = alg_bytes / (kms / 1e3) / 1e9 if kms else None
     traffic = load_traffic().get("join_agg_probe_bytes_per_probe_row")
 
+    # The same query with the fused probe kept on the hashed bucket table
+    # (QDB_JOIN_DIRECT=0): the build keys here are unique over a dense range,
+    # so the measured step above probes the direct-address index instead.
+    hashed = None
+    if rank == 0 and world == 1:
+        os.environ["QDB_JOIN_DIRECT"] = "0"
+        try:
+            hms, hres, _, hk = timed(q, lambda: w.step(resident=True), 5, 3, profile=True)
+            hkms, _ = kernel_avg(hk, "join_agg_probe", 5)
+            hashed = {"ms_per_step": hms, "kernel_ms": hkms,
+                      "frac_of_measured_hbm": alg_bytes / (hkms / 1e3) / 1e9 / peak if hkms else None,
+                      "same_result": list(hres[-1]) == list(results[-1])}
+        finally:
+            del os.environ["QDB_JOIN_DIRECT"]
+
     # End to end through the C ABI from pinned host buffers.
     def query_e2e():
         s, c = w.step(resident=False)
@@ -815,6 +830,8 @@ def main() -> None:
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if hashed:
+        line["join_hashed_probe"] = {k: (round(v, 4) if isinstance(v, float) else v) for k, v in hashed.items()}
     if rank == 0 and world == 1 and not args.no_operators:
         ops = {}
         try:

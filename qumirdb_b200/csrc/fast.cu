@@ -15,6 +15,7 @@
 // accumulators; a block reduction and one atomic per state word per CTA end
 // the launch.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "common.cuh"
@@ -181,7 +182,32 @@ __device__ __forceinline__ bool JsWait(uint64_t* bar, uint32_t phase, const vola
     return true;
 }
 
+// Probes kJsRows rows of one thread against the direct-address index: the
+// key's offset in the dense range, the presence bit in shared memory, then
+// every surviving row's 16-byte entry {key, payload} in one batch (a folded
+// bitmap lets a neighbour's key through; the key compare settles it).
 template <int NS, int C0, int C1>
+__device__ __forceinline__ void JsProbeDense(const JsLaunch& L, JsAcc& a, const uint32_t* bits,
+                                             const int64_t (&row)[kJsRows], const uint64_t (&key)[kJsRows],
+                                             const int64_t (&sv)[kJsRows], const bool (&valid)[kJsRows]) {
+    const JTableDev& jt = L.jt;
+    ulonglong2 e[kJsRows];
+    bool ok[kJsRows];
+#pragma unroll
+    for (int j = 0; j < kJsRows; ++j) {
+        const uint64_t d = key[j] - uint64_t(jt.dense_min);
+        ok[j] = valid[j] && d < jt.dense_range;
+        const uint64_t bit = ok[j] ? (d >> jt.dense_shift) : 0;
+        ok[j] = ok[j] && ((bits[bit >> 5] >> (bit & 31)) & 1u);
+        e[j] = ok[j] ? __ldg(jt.dense + d) : make_ulonglong2(kEmptyKey, 0);
+    }
+#pragma unroll
+    for (int j = 0; j < kJsRows; ++j) {
+        if (ok[j] && e[j].x == key[j]) JsFoldSlot<NS, C0, C1>(L, a, row[j], sv[j], e[j].y, 0);
+    }
+}
+
+template <int NS, int C0, int C1, bool DENSE>
 __global__ void __launch_bounds__(kJsThreads, 1) JoinSumKernel(const __grid_constant__ JsLaunch L) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
@@ -204,10 +230,12 @@ __global__ void __launch_bounds__(kJsThreads, 1) JoinSumKernel(const __grid_cons
         issued_tiles = 0;
         FenceBarrierInit();
     }
-    // The build side's Bloom filter goes to shared memory: most probe rows
-    // miss and are rejected there without touching the table in L2.
+    // The build side's Bloom filter (or the direct index's presence bitmap)
+    // goes to shared memory: most probe rows miss and are rejected there
+    // without touching the table in L2.
+    const uint32_t* filter_src = DENSE ? L.jt.dense_bits : L.jt.bloom;
     for (int w = tid * 4; w < nb; w += blockDim.x * 4) {
-        *reinterpret_cast<uint4*>(&bloom[w]) = __ldg(reinterpret_cast<const uint4*>(&L.jt.bloom[w]));
+        *reinterpret_cast<uint4*>(&bloom[w]) = __ldg(reinterpret_cast<const uint4*>(&filter_src[w]));
     }
     __syncthreads();
 
@@ -270,7 +298,8 @@ __global__ void __launch_bounds__(kJsThreads, 1) JoinSumKernel(const __grid_cons
             if ((tid & 31) == 0) {
                 asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(SmemAddr(&empty[s])) : "memory");
             }
-            JsProbe<NS, C0, C1>(L, acc, bloom, nb, nspecial, row, key, sv, valid);
+            if constexpr (DENSE) JsProbeDense<NS, C0, C1>(L, acc, bloom, row, key, sv, valid);
+            else JsProbe<NS, C0, C1>(L, acc, bloom, nb, nspecial, row, key, sv, valid);
         }
         if (!failed) {
             const int64_t step = int64_t(gridDim.x) * kJsConsumers;
@@ -287,7 +316,8 @@ __global__ void __launch_bounds__(kJsThreads, 1) JoinSumKernel(const __grid_cons
                     key[j] = valid[j] ? uint64_t(__ldcs(&L.S.probe_key[row[j]])) : 0;
                     sv[j] = (valid[j] && L.vcol) ? __ldcs(&L.vcol[row[j]]) : 0;
                 }
-                JsProbe<NS, C0, C1>(L, acc, bloom, nb, nspecial, row, key, sv, valid);
+                if constexpr (DENSE) JsProbeDense<NS, C0, C1>(L, acc, bloom, row, key, sv, valid);
+                else JsProbe<NS, C0, C1>(L, acc, bloom, nb, nspecial, row, key, sv, valid);
             }
         }
     }
@@ -344,6 +374,13 @@ __global__ void __launch_bounds__(kJsThreads, 1) JoinSumKernel(const __grid_cons
 
 bool Aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
+// QDB_JOIN_DIRECT=0 keeps the fused probe on the hashed bucket table even
+// when the build has a direct-address index (to compare the two paths).
+bool DenseDisabled() {
+    const char* e = std::getenv("QDB_JOIN_DIRECT");
+    return e && e[0] == '0';
+}
+
 // State code of `st` (see JsTerm), canonicalising f(sv) * g(pay) to
 // g(pay) * f(sv) (wrapping products commute); -1: only the runtime fold.
 int StateCode(JsState& st) {
@@ -364,34 +401,36 @@ int StateCode(JsState& st) {
 using JsKernelFn = void (*)(JsLaunch);
 
 // The instantiated signatures: one state of any code, or a SUM of codes 1-3
-// beside a COUNT(*) in either order; anything else runs the runtime fold.
-JsKernelFn PickKernel(JsLaunch& L) {
+// beside a COUNT(*) in either order; anything else runs the runtime fold
+// (never with the direct index, which carries no arena row).
+template <bool DENSE>
+JsKernelFn PickKernelOf(JsLaunch& L) {
     int code[kJsMaxStates];
     for (int st = 0; st < L.S.nstates; ++st) {
         code[st] = StateCode(L.S.states[st]);
-        if (code[st] < 0 || L.S.need_row) return JoinSumKernel<0, 0, 0>;
+        if (code[st] < 0 || L.S.need_row) return JoinSumKernel<0, 0, 0, DENSE>;
     }
     if (L.S.nstates == 1) {
         switch (code[0]) {
-            case 0: return JoinSumKernel<1, 0, 0>;
-            case 1: return JoinSumKernel<1, 1, 0>;
-            case 2: return JoinSumKernel<1, 2, 0>;
-            case 3: return JoinSumKernel<1, 3, 0>;
+            case 0: return JoinSumKernel<1, 0, 0, DENSE>;
+            case 1: return JoinSumKernel<1, 1, 0, DENSE>;
+            case 2: return JoinSumKernel<1, 2, 0, DENSE>;
+            case 3: return JoinSumKernel<1, 3, 0, DENSE>;
             default: break;
         }
     } else if (L.S.nstates == 2) {
         const int k = code[0] * 8 + code[1];
         switch (k) {
-            case 1 * 8 + 0: return JoinSumKernel<2, 1, 0>;
-            case 2 * 8 + 0: return JoinSumKernel<2, 2, 0>;
-            case 3 * 8 + 0: return JoinSumKernel<2, 3, 0>;
-            case 0 * 8 + 1: return JoinSumKernel<2, 0, 1>;
-            case 0 * 8 + 2: return JoinSumKernel<2, 0, 2>;
-            case 0 * 8 + 3: return JoinSumKernel<2, 0, 3>;
+            case 1 * 8 + 0: return JoinSumKernel<2, 1, 0, DENSE>;
+            case 2 * 8 + 0: return JoinSumKernel<2, 2, 0, DENSE>;
+            case 3 * 8 + 0: return JoinSumKernel<2, 3, 0, DENSE>;
+            case 0 * 8 + 1: return JoinSumKernel<2, 0, 1, DENSE>;
+            case 0 * 8 + 2: return JoinSumKernel<2, 0, 2, DENSE>;
+            case 0 * 8 + 3: return JoinSumKernel<2, 0, 3, DENSE>;
             default: break;
         }
     }
-    return JoinSumKernel<0, 0, 0>;
+    return JoinSumKernel<0, 0, 0, DENSE>;
 }
 
 }  // namespace
@@ -421,11 +460,19 @@ void JoinSumRun(const JoinSumShape& shape, const JTableDev& jt, int64_t nrows, u
     L.staged_tiles = aligned ? nrows / kJsTile : 0;
     const size_t base = size_t(kJsBarBytes) + size_t(kJsStages) * L.stage_bytes;
     const size_t room = MaxSmemOptin() > base + 1024 ? (MaxSmemOptin() - base - 1024) / 4 : 0;
-    L.bloom_words = (jt.bloom && size_t(jt.bloom_words) <= room) ? jt.bloom_words : 0;
+    // The direct index when the table has one and the shape needs no arena
+    // row; its presence bitmap takes the Bloom filter's place.
+    const bool dense = jt.dense && !L.S.need_row && size_t(jt.dense_words) <= room && !DenseDisabled();
+    if (dense) {
+        L.bloom_words = (jt.dense_words + 3) & ~3;
+    } else {
+        L.jt.dense = nullptr;
+        L.bloom_words = (jt.bloom && size_t(jt.bloom_words) <= room) ? jt.bloom_words : 0;
+    }
     const size_t smem = base + size_t(L.bloom_words) * 4;
     const int64_t tiles = std::max<int64_t>(1, (nrows + kJsTile - 1) / kJsTile);
     const int blocks = int(std::min<int64_t>(tiles, DeviceSMs()));
-    const JsKernelFn fn = PickKernel(L);
+    const JsKernelFn fn = dense ? PickKernelOf<true>(L) : PickKernelOf<false>(L);
     EnsureSmemLimit(reinterpret_cast<const void*>(fn), smem);
     ProfileBegin(s, "join_agg_probe", nrows);
     fn<<<blocks, kJsThreads, smem, s>>>(L);

@@ -15,6 +15,7 @@
 // come out in the engine's order: probe rows ascending, a row's build rows
 // in append order (a count pass, a scan, then a write pass).
 #include <algorithm>
+#include <climits>
 
 #include "common.cuh"
 #include "eval.h"
@@ -203,6 +204,58 @@ __global__ void __launch_bounds__(kPairThreads) JoinPairWriteKernel(const __grid
     }
 }
 
+__global__ void __launch_bounds__(256) JoinKeyRangeKernel(const __grid_constant__ JoinBuildArgs a, long long* out) {
+    long long lo = LLONG_MAX, hi = LLONG_MIN;
+    for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < a.nrows; r += int64_t(gridDim.x) * blockDim.x) {
+        bool null = false;
+        const long long k = (long long)PackKeyCols(a, r, null);
+        if (null) continue;
+        lo = min(lo, k);
+        hi = max(hi, k);
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        lo = min(lo, __shfl_xor_sync(kFull, lo, d));
+        hi = max(hi, __shfl_xor_sync(kFull, hi, d));
+    }
+    if (LaneId() == 0) {
+        atomicMin(&out[0], lo);
+        atomicMax(&out[1], hi);
+    }
+}
+
+__global__ void __launch_bounds__(256) JoinDenseInitKernel(ulonglong2* dense, uint64_t range, uint32_t* bits,
+                                                           int32_t words) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < int64_t(range); i += stride) {
+        dense[i] = make_ulonglong2(kEmptyKey, 0);
+    }
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < words; i += stride) bits[i] = 0;
+}
+
+__global__ void __launch_bounds__(256) JoinDenseBuildKernel(const __grid_constant__ JoinBuildArgs a, ulonglong2* dense,
+                                                            int64_t kmin, uint64_t range, uint32_t* bits, int32_t shift,
+                                                            unsigned long long* dup) {
+    for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < a.nrows; r += int64_t(gridDim.x) * blockDim.x) {
+        bool null = false;
+        const uint64_t key = PackKeyCols(a, r, null);
+        if (null) continue;
+        const uint64_t d = key - uint64_t(kmin);
+        if (d >= range) {   // outside the measured range: cannot happen; counted as a duplicate (no index)
+            atomicAdd(dup, 1ull);
+            continue;
+        }
+        auto* kp = reinterpret_cast<unsigned long long*>(&dense[d].x);
+        if (atomicCAS(kp, kEmptyKey, key) != kEmptyKey) {
+            atomicAdd(dup, 1ull);
+            continue;
+        }
+        dense[d].y = a.pay0 ? uint64_t(a.pay0[r]) : 0ull;
+        const uint64_t bit = d >> shift;
+        atomicOr(&bits[bit >> 5], 1u << (bit & 31));
+    }
+}
+
 // Sets the Bloom bits of every occupied slot's key.
 __global__ void __launch_bounds__(256) JoinBloomKernel(const uint64_t* buckets, int64_t nbuckets, uint32_t* bloom,
                                                        int32_t nwords) {
@@ -233,6 +286,23 @@ void JoinBuild(const JoinBuildArgs& a, cudaStream_t s) {
     JoinBuildKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(a);
     ProfileEnd(s);
     CountLaunch();
+}
+
+void JoinKeyRange(const JoinBuildArgs& a, long long* out, cudaStream_t s) {
+    if (a.nrows == 0) return;
+    ProfileBegin(s, "join_key_range", a.nrows);
+    JoinKeyRangeKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(a, out);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+void JoinDenseBuild(const JoinBuildArgs& a, ulonglong2* dense, int64_t kmin, uint64_t range, uint32_t* bits,
+                    int32_t words, int32_t shift, unsigned long long* dup, cudaStream_t s) {
+    ProfileBegin(s, "join_dense_build", int64_t(range));
+    JoinDenseInitKernel<<<Blocks(int64_t(range), 256), 256, 0, s>>>(dense, range, bits, words);
+    if (a.nrows > 0) JoinDenseBuildKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(a, dense, kmin, range, bits, shift, dup);
+    ProfileEnd(s);
+    CountLaunch(a.nrows > 0 ? 2 : 1);
 }
 
 void JoinBuildBloom(const JTableDev& jt, uint32_t* bloom, int32_t nwords, cudaStream_t s) {

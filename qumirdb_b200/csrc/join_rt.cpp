@@ -6,6 +6,7 @@
 // table.Capacity (8) / Rows (32) / Keys (40), pairs.Count (0).  Word 0 of the
 // arena and table buffers holds this library's device state.
 #include <algorithm>
+#include <climits>
 #include <cstring>
 
 #include "fast.h"
@@ -45,6 +46,12 @@ struct TableState {
     unsigned long long* nspecial_d = nullptr;   // device count of special rows
     uint32_t* bloom = nullptr;
     int32_t bloom_words = 0;
+    ulonglong2* dense = nullptr;   // direct-address index (see JTableDev)
+    int64_t dense_min = 0;
+    uint64_t dense_range = 0;
+    uint32_t* dense_bits = nullptr;
+    int32_t dense_words = 0;
+    int32_t dense_shift = 0;
     JTableDev dev() const {
         JTableDev j;
         j.buckets = buckets;
@@ -54,6 +61,12 @@ struct TableState {
         j.nspecial = nspecial_d;
         j.bloom = bloom;
         j.bloom_words = bloom_words;
+        j.dense = dense;
+        j.dense_min = dense_min;
+        j.dense_range = dense_range;
+        j.dense_bits = dense_bits;
+        j.dense_words = dense_words;
+        j.dense_shift = dense_shift;
         return j;
     }
 };
@@ -179,6 +192,8 @@ void DestroyArena(ArenaState* a) {
 }
 
 void DestroyTable(TableState* t) {
+    DevFree(t->dense, t->s);
+    DevFree(t->dense_bits, t->s);
     DevFree(t->bloom, t->s);
     DevFree(t->buckets, t->s);
     DevFree(t->rows, t->s);
@@ -242,6 +257,70 @@ bool Append(const qdb_gpu_program* prog, ArenaState* a, qdb_rowset* batch) {
     return ok;
 }
 
+// Entries of the direct-address index at most: 2^24 (256 MB) and eight per
+// build row (plus 64K), so a sparse key set keeps the hashed table alone.
+constexpr uint64_t kDenseMaxRange = uint64_t(1) << 24;
+
+// The direct-address index beside the bucket table, for one integer key
+// (signed, or unsigned of at most 32 bits) whose build values are unique
+// and dense: a probe of it is a subtraction, a bit test in shared memory and
+// at most one 16-byte read, with no hashing.  Any duplicate key, a range too
+// wide, or the empty marker inside the range leaves the table without it.
+// Returns false only on a device failure.
+bool BuildDense(const JoinProgram& J, const ArenaState* a, const JoinBuildArgs& b, TableState* t) {
+    if (J.build_jk.n != 1 || J.build_jk.is_float[0] || a->rows < 4096) return true;
+    const int ty = J.build_columns[J.build_keys[0]].type;
+    if (ty == QDB_TYPE_U64) return true;
+    auto* buf = static_cast<long long*>(DevAlloc(24, t->s));
+    if (!buf) return false;
+    const long long init[3] = {LLONG_MAX, LLONG_MIN, 0};
+    cudaMemcpyAsync(buf, init, 24, cudaMemcpyHostToDevice, t->s);
+    JoinKeyRange(b, buf, t->s);
+    long long mm[3] = {0, 0, 0};
+    cudaMemcpyAsync(mm, buf, 24, cudaMemcpyDeviceToHost, t->s);
+    if (!CudaOk(cudaStreamSynchronize(t->s), "row join key range")) {
+        DevFree(buf, t->s);
+        return false;
+    }
+    const long long kmin = mm[0], kmax = mm[1];
+    const uint64_t range = kmin <= kmax ? uint64_t(kmax) - uint64_t(kmin) + 1 : 0;
+    const uint64_t limit = std::min<uint64_t>(kDenseMaxRange, uint64_t(a->rows) * 8 + (uint64_t(1) << 16));
+    const bool marker_inside = kmin <= -1 && kmax >= -1;   // kEmptyKey as int64
+    if (range == 0 || range > limit || marker_inside) {
+        DevFree(buf, t->s);
+        return true;
+    }
+    int32_t shift = 0;
+    while ((((range - 1) >> shift) + 1) > uint64_t(kMaxBloomWords) * 32 - 96) ++shift;
+    // Bitmap words, a multiple of four (the probe copies it in 16-byte loads).
+    const int32_t words = int32_t(((((range - 1) >> shift) + 32) / 32 + 3) & ~uint64_t(3));
+    t->dense = static_cast<ulonglong2*>(DevAlloc(size_t(range) * 16, t->s));
+    t->dense_bits = static_cast<uint32_t*>(DevAlloc(size_t(words) * 4, t->s));
+    if (!t->dense || !t->dense_bits) {
+        DevFree(buf, t->s);
+        return false;
+    }
+    auto* dup = reinterpret_cast<unsigned long long*>(buf + 2);
+    JoinDenseBuild(b, t->dense, kmin, range, t->dense_bits, words, shift, dup, t->s);
+    unsigned long long ndup = 0;
+    cudaMemcpyAsync(&ndup, dup, 8, cudaMemcpyDeviceToHost, t->s);
+    const bool ok = CudaOk(cudaStreamSynchronize(t->s), "row join direct index");
+    DevFree(buf, t->s);
+    if (!ok) return false;
+    if (ndup) {
+        DevFree(t->dense, t->s);
+        DevFree(t->dense_bits, t->s);
+        t->dense = nullptr;
+        t->dense_bits = nullptr;
+        return true;
+    }
+    t->dense_min = kmin;
+    t->dense_range = range;
+    t->dense_words = words;
+    t->dense_shift = shift;
+    return true;
+}
+
 bool Build(const qdb_gpu_program* prog, ArenaState* a, void* table) {
     const JoinProgram& J = prog->join;
     TableState* old = TableOf(table);
@@ -294,6 +373,10 @@ bool Build(const qdb_gpu_program* prog, ArenaState* a, void* table) {
             return false;
         }
         JoinBuildBloom(t->dev(), t->bloom, t->bloom_words, t->s);
+    }
+    if (!BuildDense(J, a, b, t)) {
+        DestroyTable(t);
+        return false;
     }
     if (!CudaOk(cudaGetLastError(), "row join build")) {
         DestroyTable(t);

@@ -61,6 +61,17 @@ struct JTableDev {
     // two bits set), small enough for a CTA's shared memory; nullptr: none.
     const uint32_t* bloom = nullptr;
     int32_t bloom_words = 0;
+    // Direct-address index, built when the table has one integer key whose
+    // build values are unique and span a dense range (nullptr: none).  Entry
+    // key - dense_min holds {key, first 8-byte payload word} ({kEmptyKey, 0}
+    // when absent); a presence bitmap over the range, each bit covering
+    // 2^dense_shift keys, fits a CTA's shared memory.
+    const ulonglong2* dense = nullptr;
+    int64_t dense_min = 0;
+    uint64_t dense_range = 0;
+    const uint32_t* dense_bits = nullptr;
+    int32_t dense_words = 0;
+    int32_t dense_shift = 0;
 };
 constexpr int32_t kMaxBloomWords = 32768;   // 128 KB
 
@@ -144,6 +155,14 @@ struct JoinBuildArgs {
 };
 void JoinInitTable(uint64_t* buckets, int64_t nbuckets, cudaStream_t s);
 void JoinBuild(const JoinBuildArgs& a, cudaStream_t s);
+// Smallest and largest key of the build rows (a single integer key): out[0]
+// and out[1] as int64, preset to INT64_MAX / INT64_MIN by the caller.
+void JoinKeyRange(const JoinBuildArgs& a, long long* out, cudaStream_t s);
+// Fills the direct-address index of the build rows over [kmin, kmin + range):
+// entries (preset here), the presence bitmap (words of 32 bits, each bit for
+// 2^shift keys) and *dup, the count of keys met twice.
+void JoinDenseBuild(const JoinBuildArgs& a, ulonglong2* dense, int64_t kmin, uint64_t range, uint32_t* bits,
+                    int32_t words, int32_t shift, unsigned long long* dup, cudaStream_t s);
 
 struct JoinProbeArgs {
     const char* key_data[4];

@@ -160,3 +160,40 @@ def test_join_aggregate_shapes(shape):
     q.release(out)
     want = O.join_aggregate(jspec, aspec, [q.HostRowSet(b)], [q.HostRowSet(p)])
     assert got == want
+
+
+@pytest.mark.parametrize("keys", ["dense", "dense_negative", "spans_marker", "sparse", "duplicates"])
+def test_join_sum_build_key_layouts(keys):
+    """The fused join-sum over build keys that do and do not get the
+    direct-address index (unique keys over a dense range; a range holding the
+    empty marker -1, sparse 64-bit keys and duplicate keys keep the hashed
+    table), each equal to the oracle; probe keys also fall outside the range."""
+    rng = np.random.default_rng(40)
+    nb, npr = 50_000, 1_500_017
+    if keys == "dense":
+        bk = rng.permutation(nb).astype(np.int64) + 1000
+    elif keys == "dense_negative":
+        bk = -(rng.permutation(nb).astype(np.int64) + 2)           # -2 .. -nb-1
+    elif keys == "spans_marker":
+        bk = rng.permutation(nb).astype(np.int64) - nb // 2         # includes -1
+    elif keys == "sparse":
+        bk = rng.integers(-2**62, 2**62, nb, dtype=np.int64)
+    else:
+        bk = rng.integers(1000, 1000 + nb // 3, nb).astype(np.int64)
+    b = [bk, rng.integers(1, 10**6, nb).astype(np.int64), rng.integers(0, 100, nb).astype(np.int32)]
+    lo, hi = int(bk.min()), int(bk.max())
+    span = hi - lo + 1
+    pk = np.where(rng.random(npr) < 0.7, rng.choice(bk, npr), rng.integers(lo - span, hi + span, npr)).astype(np.int64)
+    p = [pk, rng.integers(1, 10**4, npr).astype(np.int64)]
+    jspec, aspec = queries.join_sum(60)
+    prog = q.compile_join_aggregate(jspec, aspec)
+    J = q.RowJoin(prog)
+    J.append(q.DeviceRowSet(b))
+    J.build()
+    agg = q.Aggregate(prog)
+    J.probe_aggregate(agg, q.DeviceRowSet(p))
+    out = agg.finish()
+    got = gpu_rows(out, [abi.I64, abi.I64])
+    q.release(out)
+    want = O.join_aggregate(jspec, aspec, [q.HostRowSet(b)], [q.HostRowSet(p)])
+    assert got == want
