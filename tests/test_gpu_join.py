@@ -183,7 +183,8 @@ def test_join_sum_build_key_layouts(keys):
     b = [bk, rng.integers(1, 10**6, nb).astype(np.int64), rng.integers(0, 100, nb).astype(np.int32)]
     lo, hi = int(bk.min()), int(bk.max())
     span = hi - lo + 1
-    pk = np.where(rng.random(npr) < 0.7, rng.choice(bk, npr), rng.integers(lo - span, hi + span, npr)).astype(np.int64)
+    other = max(lo - span, -2**63), min(hi + span, 2**63 - 1)
+    pk = np.where(rng.random(npr) < 0.7, rng.choice(bk, npr), rng.integers(other[0], other[1], npr)).astype(np.int64)
     p = [pk, rng.integers(1, 10**4, npr).astype(np.int64)]
     jspec, aspec = queries.join_sum(60)
     prog = q.compile_join_aggregate(jspec, aspec)
