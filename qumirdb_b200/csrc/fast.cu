@@ -17,11 +17,13 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "common.cuh"
 #include "fast.h"
 #include "jtable.cuh"
 #include "kernels.h"
+#include "runtime.h"
 
 namespace qdb {
 
@@ -435,8 +437,10 @@ JsKernelFn PickKernelOf(JsLaunch& L) {
 
 }  // namespace
 
-void JoinSumRun(const JoinSumShape& shape, const JTableDev& jt, int64_t nrows, uint64_t* group_states,
-                AggCounters* counters, cudaStream_t s) {
+namespace {
+
+void JoinSumLaunch(const JoinSumShape& shape, const JTableDev& jt, int64_t nrows, uint64_t* group_states,
+                   AggCounters* counters, cudaStream_t s) {
     if (nrows == 0) return;
     static thread_local JsLaunch L;
     std::memset(&L, 0, sizeof(L));
@@ -478,6 +482,95 @@ void JoinSumRun(const JoinSumShape& shape, const JTableDev& jt, int64_t nrows, u
     fn<<<blocks, kJsThreads, smem, s>>>(L);
     ProfileEnd(s);
     CountLaunch();
+}
+
+// The probe-side column every probe factor reads (the one staged beside the
+// keys), or nullptr when none does; false when factors read two different
+// probe columns or a build column through the arena row.
+bool SingleProbeColumn(const JoinSumShape& shape, const int64_t*& vcol) {
+    vcol = nullptr;
+    if (shape.need_row) return false;
+    for (int st = 0; st < shape.nstates; ++st) {
+        for (int f = 0; f < shape.states[st].nf; ++f) {
+            const JsFactor& jf = shape.states[st].f[f];
+            if (jf.side == 2) return false;
+            if (jf.side != 0 && jf.side != 3) continue;
+            if (vcol && jf.data != vcol) return false;
+            vcol = jf.data;
+        }
+    }
+    return true;
+}
+
+// A probe of a table larger than L2: the probe rows (key, and the one value
+// column the factors read) are radix-partitioned by the high bits of their
+// home bucket into 16-row-aligned runs, then each partition is probed by its
+// own launch, whose bucket reads stay inside one L2-sized slice.
+bool JoinSumPartitioned(const JoinSumShape& shape, const JTableDev& jt, int64_t nrows, uint64_t* group_states,
+                        AggCounters* counters, int parts, int part_shift, const int64_t* vcol, cudaStream_t s) {
+    const int64_t cap = nrows + int64_t(parts) * 16;
+    auto* counts = static_cast<unsigned long long*>(DevAlloc(size_t(parts) * 16, s));
+    auto* pkeys = static_cast<int64_t*>(DevAlloc(size_t(cap) * 8, s));
+    auto* pvals = vcol ? static_cast<int64_t*>(DevAlloc(size_t(cap) * 8, s)) : nullptr;
+    auto cleanup = [&] {
+        DevFree(counts, s);
+        DevFree(pkeys, s);
+        DevFree(pvals, s);
+    };
+    if (!counts || !pkeys || (vcol && !pvals)) {
+        cleanup();
+        return false;
+    }
+    unsigned long long* cursor = counts + parts;
+    cudaMemsetAsync(counts, 0, size_t(parts) * 8, s);
+    JoinPartCountProbe(shape.probe_key, nrows, jt.bmask, part_shift, parts, counts, s);
+    std::vector<unsigned long long> cnt(static_cast<size_t>(parts)), off(static_cast<size_t>(parts));
+    cudaMemcpyAsync(cnt.data(), counts, size_t(parts) * 8, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+        cleanup();
+        return false;
+    }
+    unsigned long long run = 0;
+    for (int p = 0; p < parts; ++p) {
+        off[size_t(p)] = run;
+        run += (cnt[size_t(p)] + 15) / 16 * 16;   // each run starts on a 128-byte boundary
+    }
+    cudaMemcpyAsync(cursor, off.data(), size_t(parts) * 8, cudaMemcpyHostToDevice, s);
+    JoinPartScatterProbe(shape.probe_key, vcol, nrows, jt.bmask, part_shift, parts, cursor, pkeys, pvals, s);
+    JTableDev pt = jt;
+    pt.bloom = nullptr;      // a filter of a table this size rejects little
+    pt.bloom_words = 0;
+    pt.dense = nullptr;
+    for (int p = 0; p < parts; ++p) {
+        if (!cnt[size_t(p)]) continue;
+        JoinSumShape sp = shape;
+        sp.probe_key = pkeys + off[size_t(p)];
+        for (int st = 0; st < sp.nstates; ++st) {
+            for (int f = 0; f < sp.states[st].nf; ++f) {
+                JsFactor& jf = sp.states[st].f[f];
+                if ((jf.side == 0 || jf.side == 3) && jf.data == vcol) jf.data = pvals + off[size_t(p)];
+            }
+        }
+        JoinSumLaunch(sp, pt, int64_t(cnt[size_t(p)]), group_states, counters, s);
+    }
+    cleanup();
+    return true;
+}
+
+}  // namespace
+
+void JoinSumRun(const JoinSumShape& shape, const JTableDev& jt, int64_t nrows, uint64_t* group_states,
+                AggCounters* counters, cudaStream_t s) {
+    if (nrows == 0) return;
+    const bool direct = jt.dense && !shape.need_row && !DenseDisabled();
+    int part_shift = 0;
+    const int parts = direct ? 1 : JoinPartsFor(int64_t(jt.bmask) + 1, part_shift);
+    const int64_t* vcol = nullptr;
+    if (parts > 1 && SingleProbeColumn(shape, vcol) &&
+        JoinSumPartitioned(shape, jt, nrows, group_states, counters, parts, part_shift, vcol, s)) {
+        return;
+    }
+    JoinSumLaunch(shape, jt, nrows, group_states, counters, s);
 }
 
 }  // namespace qdb

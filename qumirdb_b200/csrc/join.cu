@@ -256,6 +256,123 @@ __global__ void __launch_bounds__(256) JoinDenseBuildKernel(const __grid_constan
     }
 }
 
+// Partition of a packed key: the high bits of its home bucket.
+__device__ __forceinline__ int PartOf(uint64_t key, uint64_t bmask, int part_shift) {
+    return int((Fmix64(key) & bmask) >> part_shift);
+}
+
+// Per-CTA histogram in shared memory, then one global add per partition.
+template <class KeyAt>
+__device__ __forceinline__ void PartCount(KeyAt key_at, int64_t n, uint64_t bmask, int part_shift, int nparts,
+                                          unsigned long long* counts) {
+    __shared__ unsigned hist[kMaxJoinParts];
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n; r += int64_t(gridDim.x) * blockDim.x) {
+        bool skip = false;
+        const uint64_t k = key_at(r, skip);
+        if (!skip) atomicAdd(&hist[PartOf(k, bmask, part_shift)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+        if (hist[i]) atomicAdd(&counts[i], (unsigned long long)hist[i]);
+    }
+}
+
+// Rows of a block-sized tile reserve their places per partition with one
+// global add per (tile, partition), then write.
+template <class KeyAt, class Write>
+__device__ __forceinline__ void PartScatter(KeyAt key_at, Write write, int64_t n, uint64_t bmask, int part_shift,
+                                            int nparts, unsigned long long* cursor) {
+    __shared__ unsigned hist[kMaxJoinParts];
+    __shared__ unsigned long long base[kMaxJoinParts];
+    for (int64_t t0 = int64_t(blockIdx.x) * blockDim.x; t0 < n; t0 += int64_t(gridDim.x) * blockDim.x) {
+        for (int i = threadIdx.x; i < nparts; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        const int64_t r = t0 + threadIdx.x;
+        bool skip = r >= n;
+        uint64_t k = 0;
+        if (!skip) k = key_at(r, skip);
+        const int p = skip ? 0 : PartOf(k, bmask, part_shift);
+        const unsigned rank = skip ? 0u : atomicAdd(&hist[p], 1u);
+        __syncthreads();
+        for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+            base[i] = hist[i] ? atomicAdd(&cursor[i], (unsigned long long)hist[i]) : 0ull;
+        }
+        __syncthreads();
+        if (!skip) write(r, k, int64_t(base[p] + rank));
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) JoinPartCountBuildKernel(const __grid_constant__ JoinBuildArgs a, int part_shift,
+                                                                int nparts, unsigned long long* counts) {
+    PartCount([&](int64_t r, bool& skip) { return PackKeyCols(a, r, skip); }, a.nrows, a.bmask, part_shift, nparts,
+              counts);
+}
+
+__global__ void __launch_bounds__(256) JoinPartScatterBuildKernel(const __grid_constant__ JoinBuildArgs a,
+                                                                  int part_shift, int nparts,
+                                                                  unsigned long long* cursor, uint64_t* keys,
+                                                                  int64_t* pays, int64_t* rows) {
+    PartScatter([&](int64_t r, bool& skip) { return PackKeyCols(a, r, skip); },
+                [&](int64_t r, uint64_t k, int64_t at) {
+                    keys[at] = k;
+                    pays[at] = a.pay0 ? a.pay0[r] : 0;
+                    rows[at] = a.row_base + r;
+                },
+                a.nrows, a.bmask, part_shift, nparts, cursor);
+}
+
+// JoinBuildKernel's insert over partitioned rows.
+__global__ void __launch_bounds__(256) JoinBuildRowsKernel(const __grid_constant__ JoinBuildArgs a,
+                                                           const uint64_t* keys, const int64_t* pays,
+                                                           const int64_t* rows, int64_t n) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const uint64_t key = keys[i];
+        const uint64_t pay = uint64_t(pays[i]);
+        if (a.jkey.full64 && key == kEmptyKey) {
+            const unsigned long long k = atomicAdd(a.nspecial, 1ull);
+            a.special_rows[2 * k] = rows[i];
+            a.special_rows[2 * k + 1] = int64_t(pay);
+            continue;
+        }
+        uint64_t b = Fmix64(key) & a.bmask;
+        bool placed = false;
+        for (uint64_t p = 0; p <= a.bmask && !placed; ++p) {
+            for (int j = 0; j < 2; ++j) {
+                auto* kp = reinterpret_cast<unsigned long long*>(&a.buckets[4 * b + j]);
+                if (*reinterpret_cast<volatile unsigned long long*>(kp) == kEmptyKey &&
+                    atomicCAS(kp, kEmptyKey, key) == kEmptyKey) {
+                    a.buckets[4 * b + 2 + j] = pay;
+                    a.rows[2 * b + j] = rows[i];
+                    placed = true;
+                    break;
+                }
+            }
+            b = (b + 1) & a.bmask;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) JoinPartCountProbeKernel(const int64_t* key, int64_t n, uint64_t bmask,
+                                                                int part_shift, int nparts,
+                                                                unsigned long long* counts) {
+    PartCount([&](int64_t r, bool&) { return uint64_t(__ldcs(&key[r])); }, n, bmask, part_shift, nparts, counts);
+}
+
+__global__ void __launch_bounds__(256) JoinPartScatterProbeKernel(const int64_t* key, const int64_t* val, int64_t n,
+                                                                  uint64_t bmask, int part_shift, int nparts,
+                                                                  unsigned long long* cursor, int64_t* out_key,
+                                                                  int64_t* out_val) {
+    PartScatter([&](int64_t r, bool&) { return uint64_t(__ldcs(&key[r])); },
+                [&](int64_t r, uint64_t k, int64_t at) {
+                    out_key[at] = int64_t(k);
+                    if (val) out_val[at] = __ldcs(&val[r]);
+                },
+                n, bmask, part_shift, nparts, cursor);
+}
+
 // Sets the Bloom bits of every occupied slot's key.
 __global__ void __launch_bounds__(256) JoinBloomKernel(const uint64_t* buckets, int64_t nbuckets, uint32_t* bloom,
                                                        int32_t nwords) {
@@ -284,6 +401,52 @@ void JoinBuild(const JoinBuildArgs& a, cudaStream_t s) {
     if (a.nrows == 0) return;
     ProfileBegin(s, "join_build", a.nrows);
     JoinBuildKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(a);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+void JoinPartCountBuild(const JoinBuildArgs& a, int part_shift, int nparts, unsigned long long* counts,
+                        cudaStream_t s) {
+    if (a.nrows == 0) return;
+    ProfileBegin(s, "join_part_count", a.nrows);
+    JoinPartCountBuildKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(a, part_shift, nparts, counts);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+void JoinPartScatterBuild(const JoinBuildArgs& a, int part_shift, int nparts, unsigned long long* cursor,
+                          uint64_t* keys, int64_t* pays, int64_t* rows, cudaStream_t s) {
+    if (a.nrows == 0) return;
+    ProfileBegin(s, "join_part_scatter", a.nrows);
+    JoinPartScatterBuildKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(a, part_shift, nparts, cursor, keys, pays, rows);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+void JoinBuildRows(const JoinBuildArgs& a, const uint64_t* keys, const int64_t* pays, const int64_t* rows, int64_t n,
+                   cudaStream_t s) {
+    if (n == 0) return;
+    ProfileBegin(s, "join_build", n);
+    JoinBuildRowsKernel<<<Blocks(n, 256), 256, 0, s>>>(a, keys, pays, rows, n);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+void JoinPartCountProbe(const int64_t* key, int64_t n, uint64_t bmask, int part_shift, int nparts,
+                        unsigned long long* counts, cudaStream_t s) {
+    if (n == 0) return;
+    ProfileBegin(s, "join_part_count", n);
+    JoinPartCountProbeKernel<<<Blocks(n, 256), 256, 0, s>>>(key, n, bmask, part_shift, nparts, counts);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+void JoinPartScatterProbe(const int64_t* key, const int64_t* val, int64_t n, uint64_t bmask, int part_shift,
+                          int nparts, unsigned long long* cursor, int64_t* out_key, int64_t* out_val, cudaStream_t s) {
+    if (n == 0) return;
+    ProfileBegin(s, "join_part_scatter", n);
+    JoinPartScatterProbeKernel<<<Blocks(n, 256), 256, 0, s>>>(key, val, n, bmask, part_shift, nparts, cursor, out_key,
+                                                               out_val);
     ProfileEnd(s);
     CountLaunch();
 }

@@ -257,9 +257,54 @@ bool Append(const qdb_gpu_program* prog, ArenaState* a, qdb_rowset* batch) {
     return ok;
 }
 
-// Entries of the direct-address index at most: 2^24 (256 MB) and eight per
-// build row (plus 64K), so a sparse key set keeps the hashed table alone.
-constexpr uint64_t kDenseMaxRange = uint64_t(1) << 24;
+// A table larger than L2: the arena rows are radix-partitioned by the high
+// bits of their home bucket, then inserted partition by partition, so the
+// inserts of one pass stay inside one L2-sized slice of the buckets.
+bool BuildPartitioned(const ArenaState* a, const JoinBuildArgs& b, int parts, int part_shift, cudaStream_t s) {
+    const int64_t n = a->rows;
+    auto* counts = static_cast<unsigned long long*>(DevAlloc(size_t(parts) * 8 * 2, s));
+    auto* keys = static_cast<uint64_t*>(DevAlloc(size_t(std::max<int64_t>(n, 1)) * 8, s));
+    auto* pays = static_cast<int64_t*>(DevAlloc(size_t(std::max<int64_t>(n, 1)) * 8, s));
+    auto* rows = static_cast<int64_t*>(DevAlloc(size_t(std::max<int64_t>(n, 1)) * 8, s));
+    auto cleanup = [&] {
+        DevFree(counts, s);
+        DevFree(keys, s);
+        DevFree(pays, s);
+        DevFree(rows, s);
+    };
+    if (!counts || !keys || !pays || !rows) {
+        cleanup();
+        return false;
+    }
+    unsigned long long* cursor = counts + parts;
+    cudaMemsetAsync(counts, 0, size_t(parts) * 8, s);
+    JoinPartCountBuild(b, part_shift, parts, counts, s);
+    std::vector<unsigned long long> cnt(static_cast<size_t>(parts)), off(static_cast<size_t>(parts));
+    cudaMemcpyAsync(cnt.data(), counts, size_t(parts) * 8, cudaMemcpyDeviceToHost, s);
+    if (!CudaOk(cudaStreamSynchronize(s), "row join partition count")) {
+        cleanup();
+        return false;
+    }
+    unsigned long long run = 0;
+    for (int p = 0; p < parts; ++p) {
+        off[size_t(p)] = run;
+        run += cnt[size_t(p)];
+    }
+    cudaMemcpyAsync(cursor, off.data(), size_t(parts) * 8, cudaMemcpyHostToDevice, s);
+    JoinPartScatterBuild(b, part_shift, parts, cursor, keys, pays, rows, s);
+    for (int p = 0; p < parts; ++p) {
+        const size_t o = size_t(off[size_t(p)]);
+        JoinBuildRows(b, keys + o, pays + o, rows + o, int64_t(cnt[size_t(p)]), s);
+    }
+    const bool ok = CudaOk(cudaStreamSynchronize(s), "row join partitioned build");
+    cleanup();
+    return ok;
+}
+
+// Entries of the direct-address index at most: 48 MB of entries (so the
+// index stays in L2) and eight per build row (plus 64K), so a sparse key set
+// keeps the hashed table alone.
+constexpr uint64_t kDenseMaxRange = uint64_t(kJoinPartitionBytes) / 16;
 
 // The direct-address index beside the bucket table, for one integer key
 // (signed, or unsigned of at most 32 bits) whose build values are unique
@@ -364,7 +409,14 @@ bool Build(const qdb_gpu_program* prog, ArenaState* a, void* table) {
     b.special_rows = t->special;
     b.nspecial = t->nspecial_d;
     b.row_base = 0;
-    JoinBuild(b, t->s);
+    int part_shift = 0;
+    const int parts = JoinPartsFor(cap / 2, part_shift);
+    if (parts == 1) {
+        JoinBuild(b, t->s);
+    } else if (!BuildPartitioned(a, b, parts, part_shift, t->s)) {
+        DestroyTable(t);
+        return false;
+    }
     t->bloom_words = BloomWordsFor(a->rows);
     if (t->bloom_words > 0) {
         t->bloom = static_cast<uint32_t*>(DevAlloc(size_t(t->bloom_words) * 4, t->s));

@@ -155,6 +155,44 @@ struct JoinBuildArgs {
 };
 void JoinInitTable(uint64_t* buckets, int64_t nbuckets, cudaStream_t s);
 void JoinBuild(const JoinBuildArgs& a, cudaStream_t s);
+// Radix partitioning of join rows for tables larger than L2: partition =
+// home bucket (Fmix64(key) & bmask) >> part_shift, so partition p's rows
+// touch only bucket slice p (and the slot after a full bucket).
+// Build rows (packed keys, the first 8-byte payload word, the arena row):
+// counts[p] += rows of partition p; then each row goes to cursor[p]++.
+void JoinPartCountBuild(const JoinBuildArgs& a, int part_shift, int nparts, unsigned long long* counts,
+                        cudaStream_t s);
+void JoinPartScatterBuild(const JoinBuildArgs& a, int part_shift, int nparts, unsigned long long* cursor,
+                          uint64_t* keys, int64_t* pays, int64_t* rows, cudaStream_t s);
+// Inserts n partitioned build rows (as JoinBuild, from the arrays).
+void JoinBuildRows(const JoinBuildArgs& a, const uint64_t* keys, const int64_t* pays, const int64_t* rows, int64_t n,
+                   cudaStream_t s);
+// Probe rows of an 8-byte key column (and one 8-byte value column, or none).
+void JoinPartCountProbe(const int64_t* key, int64_t n, uint64_t bmask, int part_shift, int nparts,
+                        unsigned long long* counts, cudaStream_t s);
+void JoinPartScatterProbe(const int64_t* key, const int64_t* val, int64_t n, uint64_t bmask, int part_shift,
+                          int nparts, unsigned long long* cursor, int64_t* out_key, int64_t* out_val, cudaStream_t s);
+constexpr int kMaxJoinParts = 256;
+// Bucket tables above this size are built and probed by partition: a slice
+// of at most kJoinSliceBytes is what one partition's rows touch, so it stays
+// in the 126 MB L2 beside the streamed rows.
+constexpr int64_t kJoinPartitionBytes = int64_t(48) << 20;
+constexpr int64_t kJoinSliceBytes = int64_t(24) << 20;
+// Partitions for a table of nbuckets 32-byte buckets (1: none) and the
+// shift from a bucket index to its partition.
+inline int JoinPartsFor(int64_t nbuckets, int& part_shift) {
+    part_shift = 0;
+    if (nbuckets * 32 <= kJoinPartitionBytes) return 1;
+    int parts = 1;
+    while (nbuckets * 32 / parts > kJoinSliceBytes && parts < kMaxJoinParts) parts *= 2;
+    int lb = 0;
+    while ((int64_t(1) << lb) < nbuckets) ++lb;
+    int lp = 0;
+    while ((1 << lp) < parts) ++lp;
+    part_shift = lb - lp;
+    return parts;
+}
+
 // Smallest and largest key of the build rows (a single integer key): out[0]
 // and out[1] as int64, preset to INT64_MAX / INT64_MIN by the caller.
 void JoinKeyRange(const JoinBuildArgs& a, long long* out, cudaStream_t s);

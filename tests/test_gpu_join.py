@@ -198,3 +198,30 @@ def test_join_sum_build_key_layouts(keys):
     q.release(out)
     want = O.join_aggregate(jspec, aspec, [q.HostRowSet(b)], [q.HostRowSet(p)])
     assert got == want
+
+
+@pytest.mark.parametrize("attr_lt", [20, 100])
+def test_join_sum_partitioned_build_and_probe_40m(attr_lt):
+    """A 40M-row build whose bucket table is larger than L2 (256 MB with
+    attr < 20, 1.3 GB with every row kept): the build is radix-partitioned by
+    bucket and inserted slice by slice, the probe rows are partitioned the
+    same way and probed one L2-sized slice per launch; the result equals the
+    oracle's."""
+    b, p = join_data(40_000_000, 20_000_000, 50_000_000, seed=41)
+    jspec, aspec = queries.join_sum(attr_lt)
+    prog = q.compile_join_aggregate(jspec, aspec)
+    J = q.RowJoin(prog)
+    J.append(q.DeviceRowSet(b))
+    J.build()
+    agg = q.Aggregate(prog)
+    q.profile(True)
+    q.profile_read()
+    J.probe_aggregate(agg, q.DeviceRowSet(p))
+    names = [k[0] for k in q.profile_read()]
+    q.profile(False)
+    out = agg.finish()
+    got = gpu_rows(out, [abi.I64, abi.I64])
+    q.release(out)
+    assert "join_part_scatter" in names and names.count("join_agg_probe") > 1, names
+    want = O.join_aggregate(jspec, aspec, [q.HostRowSet(b)], [q.HostRowSet(p)])
+    assert got == want
