@@ -198,11 +198,31 @@ typedef struct qdb_aggregate_spec {
 #define QDB_HASH_TABLE_SIZE 304
 
 /* ------------------------------------------------------------------------ */
-/* Row join (inner equi-join, build side fixed).                            */
+/* Row join (equi-join, build side fixed).                                  */
 /* ------------------------------------------------------------------------ */
 
+/* EJoinType (qdb/plan/ops/join_type.h:5-18), in its order.  Served, as by   */
+/* TKernelCompiler::CompileRowJoin (qdb/kernel/compiler.cpp:3127-3148):      */
+/*   INNER;                                                                  */
+/*   LEFT with the right side built and RIGHT with the left side built: the  */
+/*     preserved side streams through Probe, and a probe row that matches    */
+/*     nothing (a NULL key included) is paired with a NULL build row;        */
+/*   LEFT_SEMI / LEFT_ANTI with the left side built: Probe marks the build   */
+/*     rows it matches and emits nothing; once the probe side has ended,     */
+/*     EMIT_BY_MARK pairs the marked (SEMI) or unmarked (ANTI) build rows,   */
+/*     in build order, and materialize writes build columns only.  An ANTI   */
+/*     join keeps its NULL-key build rows in a second arena (APPEND_NULL_KEYS */
+/*     with that arena), whose EMIT_BY_MARK pairs every row.                  */
+/* The others are rejected at compile time.                                  */
 typedef enum qdb_join_type {
-    QDB_JOIN_INNER = 0
+    QDB_JOIN_INNER = 0,
+    QDB_JOIN_LEFT = 1,
+    QDB_JOIN_RIGHT = 2,
+    QDB_JOIN_FULL = 3,
+    QDB_JOIN_LEFT_SEMI = 4,
+    QDB_JOIN_RIGHT_SEMI = 5,
+    QDB_JOIN_LEFT_ANTI = 6,
+    QDB_JOIN_RIGHT_ANTI = 7
 } qdb_join_type;
 
 typedef struct qdb_row_join_spec {
@@ -235,6 +255,8 @@ typedef struct qdb_row_join_spec {
 #define QDB_JR_OP_APPEND 1
 #define QDB_JR_OP_BUILD 2
 #define QDB_JR_OP_PROBE 3
+#define QDB_JR_OP_APPEND_NULL_KEYS 5   /* LEFT_ANTI: NULL-key rows, into the second arena */
+#define QDB_JR_OP_EMIT_BY_MARK 6       /* LEFT_SEMI / LEFT_ANTI: appends (NULL, build row) pairs */
 
 /* Caller-owned zeroed state sizes (qdb/kernel/compiler.h:599-621).  The    */
 /* pair buffer's int64 at offset 0 is its pair count, read by               */
@@ -350,7 +372,10 @@ bool qdb_gpu_hash(const qdb_gpu_program* program, qdb_rowset* batch,
                   uint64_t* hashes);
 
 /* jr_dispatch(arena, table, scratch, pairs, batch, op)                      */
-/* (qdb/kernel/compiler.h:390-395); returns false on failure.                */
+/* (qdb/kernel/compiler.h:390-395); returns false on failure, and for an op  */
+/* the program's join type does not use.  Probe replaces the pair buffer's   */
+/* pairs; EMIT_BY_MARK appends to them (TRowJoinProcessor::Finish calls it   */
+/* for the arena, then for the NULL-key arena, qdb/exec/row_join_exec.cpp).   */
 bool qdb_gpu_jr_dispatch(const qdb_gpu_program* program, void* arena,
                          void* table, void* scratch, void* pairs,
                          qdb_rowset* batch, int64_t op);
@@ -452,6 +477,106 @@ void qdb_gpu_release_rowsets(qdb_rowset* rowsets, int64_t n);
 /* counterpart.                                                              */
 int64_t qdb_gpu_autotune_info(char* buf, int64_t cap);
 void qdb_gpu_autotune_reset(void);
+
+/* ------------------------------------------------------------------------ */
+/* Runtime join filter (qdb/kernel/join/runtime_filter.oz, driven by         */
+/* qdb/exec/runtime_filter.cpp): a join's build side publishes its key       */
+/* hashes as an exact set (at most MaxKeys distinct) or a blocked Bloom      */
+/* filter, and the probe side's scan drops rows whose hash it rejects.       */
+/* The four entries take the kernel's state structs (mirrored below, field   */
+/* for field) with every array they point at in DEVICE memory; hashes,       */
+/* selections and outputs passed to them are device arrays too.  Results     */
+/* are the reference's, bit for bit: the build's mode, key count, key order  */
+/* and Bloom words; the published kind, exact key count, table size, Bloom   */
+/* words and set bits; the probe's output bytes (1 kept, 0 rejected).        */
+/* ------------------------------------------------------------------------ */
+
+/* RuntimeFilterBuild (runtime_filter.oz:29-41; TRuntimeFilterBuildState).   */
+/* Mode 0 collecting, 1 deduplicating, 2 overflowing, 3 Bloom; Want 1 asks   */
+/* for SortOrder / SortKeys / the set, 2 for Bloom storage (BloomWords >= 0). */
+/* Keys has room for KeyCount + the batch's rows; SetSlots for SetCapacity   */
+/* words (the device keeps its own set layout there; SetCtrl is unused);     */
+/* SortOrder holds 2 * KeyCount + 256 words and SortKeys KeyCount.           */
+typedef struct qdb_rf_build_state {
+    int64_t MaxKeys;
+    int64_t Mode;
+    int64_t Want;
+    uint64_t* Keys;
+    int64_t KeyCount;
+    uint8_t* SetCtrl;
+    uint64_t* SetSlots;
+    int64_t SetCapacity;
+    uint32_t* SortOrder;
+    uint64_t* SortKeys;
+    uint64_t* Bloom;
+    int64_t BloomWords;
+} qdb_rf_build_state;
+
+/* RuntimeFilterPartial (runtime_filter.oz:44-48).                           */
+typedef struct qdb_rf_partial {
+    const uint64_t* Keys;
+    int64_t KeyCount;
+    const uint64_t* Bloom;
+    int64_t BloomWords;
+} qdb_rf_partial;
+
+/* RuntimeFilterPublish (runtime_filter.oz:56-69; TPublishState).  Kind: 0   */
+/* cannot answer, 1 exact, 2 Bloom.  Table is zeroed and sized for           */
+/* min(keys, MaxKeys) keys; Bloom is zeroed, or holds one fragment when      */
+/* BloomSeeded.                                                              */
+typedef struct qdb_rf_publish_state {
+    int64_t MaxKeys;
+    uint64_t* Keys;
+    uint8_t* SetCtrl;
+    uint64_t* SetSlots;
+    int64_t SetCapacity;
+    uint64_t* Table;
+    uint64_t* Bloom;
+    int64_t BloomWords;
+    int64_t BloomSeeded;
+    int64_t Kind;
+    int64_t ExactKeys;
+    int64_t TableSize;
+    int64_t BloomSetBits;
+} qdb_rf_publish_state;
+
+/* RuntimeFilterData (runtime_filter.oz:72-75): Words is the exact table     */
+/* (Kind 1) or the Bloom words (Kind 2).                                     */
+typedef struct qdb_rf_data {
+    int64_t Kind;
+    const uint64_t* Words;
+    int64_t WordCount;
+} qdb_rf_data;
+
+/* rf_build (runtime_filter.oz:419-499): adds the selected hashes to a        */
+/* producer's contribution; returns the rows consumed (all of them unless    */
+/* state->Want asks for storage), < 0 on failure.                            */
+int64_t qdb_gpu_rf_build(qdb_rf_build_state* state, const uint64_t* hashes, const uint8_t* selection,
+                         int64_t count);
+/* rf_publish (runtime_filter.oz:502-556): merges the producers'             */
+/* contributions into the published filter.  Returns 0, < 0 on failure.     */
+int64_t qdb_gpu_rf_publish(qdb_rf_publish_state* state, const qdb_rf_partial* partials,
+                           int64_t partial_count);
+/* rf_probe (runtime_filter.oz:561-577): output[i] = 1 when selected row i's  */
+/* hash may be in the filter, else 0; returns the kept count (< 0 on         */
+/* failure).  `vectorized` and the two scratch arrays serve the CPU's vector */
+/* probe and are ignored.                                                    */
+int64_t qdb_gpu_rf_probe(const qdb_rf_data* data, const uint64_t* hashes, const uint8_t* selection,
+                         uint8_t* output, int64_t count, int64_t vectorized, uint64_t* selected_hashes,
+                         uint8_t* selected_output);
+/* rf_merge (runtime_filter.oz:580-584): ORs Bloom fragment `source` into    */
+/* `target` (count words).  Returns 0, < 0 on failure.                       */
+int64_t qdb_gpu_rf_merge(uint64_t* target, const uint64_t* source, int64_t count);
+
+/* The probe-side scan fused with the filter: for a hash program (the join   */
+/* key's rh_hash, qdb_gpu_compile_hash), output[i] = 1 when batch row i is    */
+/* selected and its key hash may be in the filter, without writing the       */
+/* hashes.  Equals qdb_gpu_hash followed by qdb_gpu_rf_probe.  No reference  */
+/* counterpart (the engine hashes, then probes).  `output` and the filter's  */
+/* words are device memory; the batch may be host or device.  Returns the    */
+/* kept count, < 0 on failure.                                               */
+int64_t qdb_gpu_rf_probe_rowset(const qdb_gpu_program* hash_program, const qdb_rf_data* data,
+                                qdb_rowset* batch, uint8_t* output);
 
 /* ------------------------------------------------------------------------ */
 /* Aggregation without device allocation.                                   */

@@ -7,6 +7,8 @@
 #include "oracle.h"
 
 #include <algorithm>
+#include <unordered_set>
+#include <random>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -926,9 +928,14 @@ void BuildTable(const BuildArena& a, int nk, const int* types, RowTable& t, std:
 // row_table.oz:260-277, jr_probe_candidates join_rows.oz:146-197): a seek
 // pass over every selected valid row, then key passes; a salt collision moves
 // the row on to the next pass.  Emits (probe row, build arena row).
+// With emit_unmatched (an outer join streaming its preserved side), a NULL
+// key is paired with build row -1 at once in the collect pass
+// (join_gen.cpp:2206-2230), and a row whose seek reaches an empty entry
+// after its key passes (jr_probe_candidates' emit_unmatched).
 template <class Emit>
 void ProbeBatch(const JoinSide& side, const BuildArena& a, const RowTable& t,
-                const std::vector<int64_t>& next, const qdb_rowset& p, Emit&& emit) {
+                const std::vector<int64_t>& next, const qdb_rowset& p, Emit&& emit,
+                bool emit_unmatched = false) {
     const int nk = side.n_keys;
     std::vector<int64_t> rows;
     std::vector<Val> keys;
@@ -936,7 +943,10 @@ void ProbeBatch(const JoinSide& side, const BuildArena& a, const RowTable& t,
     std::vector<Val> key(nk);
     for (int64_t r = 0; r < p.RowCount; ++r) {
         if (p.Selection && !p.Selection[r]) continue;
-        if (!ReadKey(side, p, r, key.data())) continue;
+        if (!ReadKey(side, p, r, key.data())) {
+            if (emit_unmatched) emit(r, int64_t(-1));
+            continue;
+        }
         rows.push_back(r);
         keys.insert(keys.end(), key.begin(), key.end());
     }
@@ -955,7 +965,10 @@ void ProbeBatch(const JoinSide& side, const BuildArena& a, const RowTable& t,
         for (int64_t q = 0; q < k; ++q) {
             const int64_t j = first ? q : work[q];
             const uint64_t e = found[j];
-            if (e == 0) continue;
+            if (e == 0) {
+                if (emit_unmatched) emit(rows[j], int64_t(-1));
+                continue;
+            }
             const int64_t head = int64_t(e & 0xFFFFFFFFFFFFULL) - 1;
             if (ArenaKeyEqual(a, nk, head, &keys[j * nk], side.key_types.data())) {
                 for (int64_t cur = head; cur >= 0; cur = next[cur]) emit(rows[j], cur);
@@ -1280,6 +1293,75 @@ int64_t oracle_row_join(const qdb_row_join_spec* spec, const qdb_rowset* build, 
     }
 }
 
+int64_t oracle_row_join_typed(const qdb_row_join_spec* spec, const qdb_rowset* build, int32_t n_build,
+                              const qdb_rowset* probe, int32_t n_probe, int64_t* pairs, int64_t pair_cap,
+                              char* err, size_t err_len) {
+    try {
+        // CompileRowJoin's served shapes (qdb/kernel/compiler.cpp:3134-3148).
+        const int jt = spec->join_type;
+        const bool preserved = spec->build_is_left ? jt == QDB_JOIN_RIGHT : jt == QDB_JOIN_LEFT;
+        const bool marks = spec->build_is_left && (jt == QDB_JOIN_LEFT_SEMI || jt == QDB_JOIN_LEFT_ANTI);
+        if (jt != QDB_JOIN_INNER && !preserved && !marks) throw Error("join type not served by the row join");
+        const JoinSide bs = MakeSide(*spec, true), ps = MakeSide(*spec, false);
+        BuildArena a;
+        AppendBuild(bs, build, n_build, a);
+        RowTable t;
+        std::vector<int64_t> next;
+        BuildTable(a, bs.n_keys, bs.key_types.data(), t, next);
+        std::vector<int64_t> first_row(size_t(n_build) + 1, 0);
+        for (int32_t b = 0; b < n_build; ++b) first_row[b + 1] = first_row[b] + build[b].RowCount;
+        auto source_row = [&](int64_t arena_row) { return first_row[a.batch[arena_row]] + a.row[arena_row]; };
+        int64_t count = 0;
+        auto push = [&](int64_t left, int64_t right) {
+            if (pairs && count < pair_cap) {
+                pairs[2 * count] = left;
+                pairs[2 * count + 1] = right;
+            }
+            ++count;
+        };
+        std::vector<uint8_t> marked(a.row.size(), 0);
+        for (int32_t pb = 0; pb < n_probe; ++pb) {
+            ProbeBatch(ps, a, t, next, probe[pb], [&](int64_t prow, int64_t brow) {
+                if (marks) {
+                    if (brow >= 0) marked[size_t(brow)] = 1;   // jr_mark_chain: every row of the chain
+                    return;
+                }
+                push((int64_t(pb) << 32) | prow, brow < 0 ? -1 : source_row(brow));
+            }, preserved);
+        }
+        if (marks) {
+            // jr_emit_by_mark (join_rows.oz:199-224) in build order, then the
+            // NULL-key arena of an ANTI join (jr_append_null_keys), all of it.
+            const bool semi = jt == QDB_JOIN_LEFT_SEMI;
+            for (size_t r = 0; r < a.row.size(); ++r) {
+                if ((marked[r] != 0) == semi) push(-1, source_row(int64_t(r)));
+            }
+            if (!semi) {
+                const qdb_row_join_spec& js = *spec;
+                const Expr fexpr{js.build_nodes, js.n_build_nodes};
+                std::vector<Val> tmp, key(size_t(bs.n_keys));
+                for (int32_t bi = 0; bi < n_build; ++bi) {
+                    const qdb_rowset& b = build[bi];
+                    for (int64_t r = 0; r < b.RowCount; ++r) {
+                        if (b.Selection && !b.Selection[r]) continue;
+                        if (js.build_filter >= 0) {
+                            EvalAll(fexpr, js.build_filter,
+                                    [&](int32_t c) { return ReadCell(b.Columns[c], js.build_columns[c], r); }, tmp);
+                            if (tmp[js.build_filter].null || tmp[js.build_filter].i == 0) continue;
+                        }
+                        if (ReadKey(bs, b, r, key.data())) continue;
+                        push(-1, first_row[bi] + r);
+                    }
+                }
+            }
+        }
+        return count;
+    } catch (const std::exception& e) {
+        SetErr(err, err_len, e.what());
+        return -1;
+    }
+}
+
 int oracle_join_aggregate(const qdb_row_join_spec* join, const qdb_aggregate_spec* agg,
                           const qdb_rowset* build, int32_t n_build, const qdb_rowset* probe,
                           int32_t n_probe, int32_t lanes, oracle_table* out, char* err, size_t err_len) {
@@ -1571,6 +1653,194 @@ double oracle_bench_sort(const int64_t* k1, const int32_t* k2, int64_t rows, int
     }
     const auto t1 = std::chrono::steady_clock::now();
     return std::chrono::duration<double>(t1 - t0).count();
+}
+
+
+// ---------------------------------------------------------------------------
+// Runtime join filter (qdb/kernel/join/runtime_filter.oz), on host memory.
+// ---------------------------------------------------------------------------
+static uint64_t RfMixHost(uint64_t v) {   // rf_mix (:78-84)
+    v ^= v >> 30;
+    v *= 0xbf58476d1ce4e5b9ULL;
+    v ^= v >> 27;
+    v *= 0x94d049bb133111ebULL;
+    return v ^ (v >> 31);
+}
+
+static bool RfSelected(const uint8_t* sel, int64_t r) { return sel == nullptr || sel[r] != 0; }
+
+// rf_bloom_base / rf_bloom_bits / rf_bloom_bit (:88-106) and rf_bloom_add (:126-147).
+static void RfBloomAdd(uint64_t* words, int64_t nwords, const uint64_t* hashes, const uint8_t* sel, int64_t n) {
+    const uint64_t block_mask = uint64_t(nwords / 8 - 1);
+    for (int64_t r = 0; r < n; ++r) {
+        if (!RfSelected(sel, r)) continue;
+        const uint64_t h = hashes[r];
+        const uint64_t base = (RfMixHost(h) & block_mask) * 8;
+        const uint64_t bits = RfMixHost(h ^ 0x9e3779b97f4a7c15ULL);
+        for (int w = 0; w < 8; ++w) words[base + w] |= 1ULL << ((bits >> (8 * w)) & 63);
+    }
+}
+
+static bool RfBloomContains(const uint64_t* words, int64_t nwords, uint64_t h) {   // :114-124
+    const uint64_t block_mask = uint64_t(nwords / 8 - 1);
+    const uint64_t base = (RfMixHost(h) & block_mask) * 8;
+    const uint64_t bits = RfMixHost(h ^ 0x9e3779b97f4a7c15ULL);
+    for (int w = 0; w < 8; ++w) {
+        if ((words[base + w] & (1ULL << ((bits >> (8 * w)) & 63))) == 0) return false;
+    }
+    return true;
+}
+
+// rf_exact_stored / rf_exact_slot (:257-279).
+static uint64_t RfStored(uint64_t h) { return h == 0 ? 1 : h; }
+static int64_t RfExactSlot(const uint64_t* table, uint64_t mask, uint64_t h) {
+    const uint64_t stored = RfStored(h);
+    uint64_t slot = h & mask;
+    while (table[slot] != 0 && table[slot] != stored) slot = (slot + 1) & mask;
+    return int64_t(slot);
+}
+
+// The dedup set (:336-396): ctrl 0x80 marks an empty slot; a probe walks
+// from mix(h) & (capacity - 1).  Only membership is observable.
+static bool RfSetInsert(uint8_t* ctrl, uint64_t* slots, int64_t capacity, uint64_t h) {
+    const uint64_t mask = uint64_t(capacity - 1);
+    uint64_t slot = RfMixHost(h) & mask;
+    for (int64_t p = 0; p < capacity; ++p) {
+        if (ctrl[slot] == 0x80) {
+            ctrl[slot] = uint8_t(RfMixHost(h) & 127);
+            slots[slot] = h;
+            return true;
+        }
+        if (slots[slot] == h) return false;
+        slot = (slot + 1) & mask;
+    }
+    return false;
+}
+
+static void RfSetFill(uint8_t* ctrl, uint64_t* slots, int64_t capacity, const uint64_t* keys, int64_t n) {
+    std::fill(ctrl, ctrl + capacity, uint8_t(0x80));
+    for (int64_t i = 0; i < n; ++i) RfSetInsert(ctrl, slots, capacity, keys[i]);
+}
+
+int64_t oracle_rf_build(qdb_rf_build_state* st, const uint64_t* hashes, const uint8_t* sel, int64_t count) {
+    // rf_build (:419-499).
+    const int64_t max_keys = st->MaxKeys;
+    uint64_t* keys = st->Keys;
+    int64_t row = 0;
+    st->Want = 0;
+    if (st->Mode == 0) {
+        const int64_t limit = max_keys * 2;
+        int64_t used = st->KeyCount;
+        while (row < count && used < limit) {
+            if (RfSelected(sel, row)) keys[used++] = hashes[row];
+            ++row;
+        }
+        st->KeyCount = used;
+        if (used < limit) return row;
+        if (st->SetCapacity == 0) {
+            st->Want = 1;
+            return row;
+        }
+        // rf_keys_sort_unique (:307-333).
+        std::sort(keys, keys + used);
+        used = int64_t(std::unique(keys, keys + used) - keys);
+        st->KeyCount = used;
+        if (used > max_keys) {
+            st->Mode = 2;
+        } else {
+            RfSetFill(st->SetCtrl, st->SetSlots, st->SetCapacity, keys, used);
+            st->Mode = 1;
+        }
+    }
+    if (st->Mode == 1) {
+        int64_t used = st->KeyCount;
+        while (row < count && used <= max_keys) {
+            if (RfSelected(sel, row) && RfSetInsert(st->SetCtrl, st->SetSlots, st->SetCapacity, hashes[row])) {
+                keys[used++] = hashes[row];
+            }
+            ++row;
+        }
+        st->KeyCount = used;
+        if (used <= max_keys) return row;
+        st->Mode = 2;
+    }
+    if (st->Mode == 2) {
+        if (st->BloomWords < 0) {
+            st->Want = 2;
+            return row;
+        }
+        if (st->BloomWords > 0) RfBloomAdd(st->Bloom, st->BloomWords, keys, nullptr, st->KeyCount);
+        st->KeyCount = 0;
+        st->Mode = 3;
+    }
+    if (st->BloomWords > 0) RfBloomAdd(st->Bloom, st->BloomWords, hashes, sel, count);
+    return count;
+}
+
+int64_t oracle_rf_publish(qdb_rf_publish_state* st, const qdb_rf_partial* partials, int64_t n) {
+    // rf_publish (:502-556).
+    st->Kind = 0;
+    if (st->BloomSeeded == 0) {
+        std::vector<uint64_t> distinct;
+        std::unordered_set<uint64_t> seen;
+        for (int64_t i = 0; i < n && int64_t(distinct.size()) <= st->MaxKeys; ++i) {
+            for (int64_t k = 0; k < partials[i].KeyCount && int64_t(distinct.size()) <= st->MaxKeys; ++k) {
+                const uint64_t h = partials[i].Keys[k];
+                if (seen.insert(h).second) distinct.push_back(h);
+            }
+        }
+        if (int64_t(distinct.size()) <= st->MaxKeys) {
+            int64_t size = 8;
+            while (size < int64_t(distinct.size()) * 2) size *= 2;
+            for (uint64_t h : distinct) st->Table[RfExactSlot(st->Table, uint64_t(size - 1), h)] = RfStored(h);
+            st->TableSize = size;
+            st->ExactKeys = int64_t(distinct.size());
+            st->Kind = 1;
+            return 0;
+        }
+        if (st->BloomWords == 0) return 0;
+    }
+    for (int64_t p = 0; p < n; ++p) {
+        for (int64_t w = 0; w < partials[p].BloomWords; ++w) st->Bloom[w] |= partials[p].Bloom[w];
+        RfBloomAdd(st->Bloom, st->BloomWords, partials[p].Keys, nullptr, partials[p].KeyCount);
+    }
+    st->Kind = 2;
+    int64_t bits = 0;
+    for (int64_t w = 0; w < st->BloomWords; ++w) bits += __builtin_popcountll(st->Bloom[w]);
+    st->BloomSetBits = bits;
+    return 0;
+}
+
+int64_t oracle_rf_probe(const qdb_rf_data* data, const uint64_t* hashes, const uint8_t* sel, uint8_t* out,
+                        int64_t count) {
+    // rf_probe (:561-577), scalar paths (:149-170, :292-305).
+    int64_t kept = 0;
+    for (int64_t r = 0; r < count; ++r) {
+        bool keep = false;
+        if (RfSelected(sel, r)) {
+            const uint64_t h = hashes[r];
+            if (data->Kind == 1) {
+                const uint64_t mask = uint64_t(data->WordCount - 1);
+                keep = data->Words[RfExactSlot(data->Words, mask, h)] == RfStored(h);
+            } else {
+                keep = RfBloomContains(data->Words, data->WordCount, h);
+            }
+        }
+        out[r] = keep ? 1 : 0;
+        kept += keep;
+    }
+    return kept;
+}
+
+void oracle_rf_merge(uint64_t* target, const uint64_t* source, int64_t count) {   // rf_merge (:580-584)
+    for (int64_t i = 0; i < count; ++i) target[i] |= source[i];
+}
+
+// std::mt19937_64 output (the generator the reference's runtime-filter
+// tests draw their hashes from, test/test_runtime_filter.cpp:31-39).
+void oracle_mt19937_64(uint64_t seed, int64_t n, uint64_t* out) {
+    std::mt19937_64 rng(seed);
+    for (int64_t i = 0; i < n; ++i) out[i] = rng();
 }
 
 }  // extern "C"

@@ -70,6 +70,14 @@ int64_t oracle_row_join(const qdb_row_join_spec* spec,
                         int64_t pair_cap, char* err, size_t err_len);
 
 /* Join then aggregate over (probe columns ++ build payload columns).        */
+/* Row join of any served join type over probe batches: pairs of
+   (probe batch << 32 | probe row, or -1 for an emitted build row;
+   build row as an index over the concatenated build batches, or -1 for a
+   padded probe row), in the order the engine emits them. */
+int64_t oracle_row_join_typed(const qdb_row_join_spec* spec, const qdb_rowset* build, int32_t n_build,
+                              const qdb_rowset* probe, int32_t n_probe, int64_t* pairs, int64_t pair_cap,
+                              char* err, size_t err_len);
+
 int oracle_join_aggregate(const qdb_row_join_spec* join,
                           const qdb_aggregate_spec* agg,
                           const qdb_rowset* build, int32_t n_build,
@@ -112,6 +120,15 @@ double oracle_bench_join_sum(const int64_t* b_key, const int64_t* b_payload,
                              int64_t* count_out);
 double oracle_bench_sort(const int64_t* k1, const int32_t* k2, int64_t rows,
                          int32_t threads, int64_t* rowids_out);
+
+/* Runtime join filter (qdb/kernel/join/runtime_filter.oz) on host memory:
+   the same state structs as the device entries (qdb_gpu.h). */
+int64_t oracle_rf_build(qdb_rf_build_state* st, const uint64_t* hashes, const uint8_t* sel, int64_t count);
+int64_t oracle_rf_publish(qdb_rf_publish_state* st, const qdb_rf_partial* partials, int64_t n);
+int64_t oracle_rf_probe(const qdb_rf_data* data, const uint64_t* hashes, const uint8_t* sel, uint8_t* out,
+                        int64_t count);
+void oracle_rf_merge(uint64_t* target, const uint64_t* source, int64_t count);
+void oracle_mt19937_64(uint64_t seed, int64_t n, uint64_t* out);
 
 #ifdef __cplusplus
 }

@@ -50,6 +50,14 @@ def lib() -> C.CDLL:
             "oracle_hash": (C.c_int, [C.c_int32, P, C.c_int32, P, C.POINTER(abi.RowSet), P, C.c_char_p, C.c_size_t]),
             "oracle_row_join": (C.c_int64, [C.POINTER(abi.RowJoinSpec), C.POINTER(abi.RowSet), C.c_int32,
                                             C.POINTER(abi.RowSet), P, C.c_int64, C.c_char_p, C.c_size_t]),
+            "oracle_row_join_typed": (C.c_int64, [C.POINTER(abi.RowJoinSpec), C.POINTER(abi.RowSet), C.c_int32,
+                                                  C.POINTER(abi.RowSet), C.c_int32, P, C.c_int64, C.c_char_p,
+                                                  C.c_size_t]),
+            "oracle_rf_build": (C.c_int64, [C.POINTER(abi.RfBuildState), P, P, C.c_int64]),
+            "oracle_rf_publish": (C.c_int64, [C.POINTER(abi.RfPublishState), C.POINTER(abi.RfPartial), C.c_int64]),
+            "oracle_rf_probe": (C.c_int64, [C.POINTER(abi.RfData), P, P, P, C.c_int64]),
+            "oracle_rf_merge": (None, [P, P, C.c_int64]),
+            "oracle_mt19937_64": (None, [C.c_uint64, C.c_int64, P]),
             "oracle_join_aggregate": (C.c_int, [C.POINTER(abi.RowJoinSpec), C.POINTER(abi.AggregateSpec),
                                                 C.POINTER(abi.RowSet), C.c_int32, C.POINTER(abi.RowSet), C.c_int32,
                                                 C.c_int32, C.POINTER(OracleTable), C.c_char_p, C.c_size_t]),
@@ -139,6 +147,21 @@ def row_join(jspec, build_rowsets, probe_rowset) -> np.ndarray:
     pairs = np.zeros(max(1, 2 * n), dtype=np.int64)
     lib().oracle_row_join(C.byref(jspec.struct), b, len(build_rowsets), probe_rowset.ptr, pairs.ctypes.data, n, err,
                           512)
+    return pairs[: 2 * n].reshape(n, 2)
+
+
+def row_join_typed(jspec, build_rowsets, probe_rowsets) -> np.ndarray:
+    """Pairs of any served join type, in the engine's order: (probe batch << 32
+    | probe row, or -1; build row over the concatenated build batches, or -1)."""
+    err = C.create_string_buffer(512)
+    b = _rowsets(build_rowsets)
+    p = _rowsets(probe_rowsets)
+    args = (C.byref(jspec.struct), b, len(build_rowsets), p, len(probe_rowsets))
+    n = lib().oracle_row_join_typed(*args, None, 0, err, 512)
+    if n < 0:
+        raise RuntimeError(err.value.decode())
+    pairs = np.zeros(max(1, 2 * n), dtype=np.int64)
+    lib().oracle_row_join_typed(*args, pairs.ctypes.data, n, err, 512)
     return pairs[: 2 * n].reshape(n, 2)
 
 

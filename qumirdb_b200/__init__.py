@@ -488,25 +488,42 @@ def autotune_reset() -> None:
 
 
 class RowJoin:
-    """The engine's TRowJoinProcessor state: arena, table, scratch, pairs."""
+    """The engine's TRowJoinProcessor state: arena, table, scratch, pairs,
+    and for a LEFT_ANTI join the second arena of NULL-key build rows
+    (qdb/exec/row_join_exec.cpp:80-220)."""
 
-    def __init__(self, prog: Program):
+    def __init__(self, prog: Program, keeps_null_keys: bool = False):
         _ensure_init()
         self.prog = prog
         self.arena = (C.c_uint8 * abi.ROW_ARENA_SIZE)()
         self.table = (C.c_uint8 * abi.ROW_TABLE_SIZE)()
         self.scratch = (C.c_uint8 * abi.ROW_SCRATCH_SIZE)()
         self.pairs = (C.c_uint8 * abi.PAIR_BUFFER_SIZE)()
+        self.null_arena = (C.c_uint8 * abi.ROW_ARENA_SIZE)() if keeps_null_keys else None
         self._op(None, abi.JR_INIT)
+        if self.null_arena is not None:
+            self._op(None, abi.JR_INIT, self.null_arena)
 
-    def _op(self, batch, op) -> None:
-        ok = lib().qdb_gpu_jr_dispatch(self.prog.handle, self.arena, self.table, self.scratch, self.pairs,
-                                       None if batch is None else batch.ptr, op)
+    def _op(self, batch, op, arena=None) -> None:
+        ok = lib().qdb_gpu_jr_dispatch(self.prog.handle, self.arena if arena is None else arena, self.table,
+                                       self.scratch, self.pairs, None if batch is None else batch.ptr, op)
         if not ok:
             raise QdbError(f"jr_dispatch({op}) failed: {last_error()}")
 
     def append(self, batch) -> None:
         self._op(batch, abi.JR_APPEND)
+        if self.null_arena is not None:
+            self._op(batch, abi.JR_APPEND_NULL_KEYS, self.null_arena)
+
+    def emit_by_mark(self) -> int:
+        """A SEMI/ANTI join's output pairs once the probe side has ended
+        (TRowJoinProcessor::Finish): the arena's rows by mark, then the
+        NULL-key arena's rows.  Returns the pair count."""
+        C.cast(self.pairs, C.POINTER(C.c_int64))[0] = 0
+        self._op(None, abi.JR_EMIT_BY_MARK)
+        if self.null_arena is not None:
+            self._op(None, abi.JR_EMIT_BY_MARK, self.null_arena)
+        return self.pair_count
 
     def build(self) -> None:
         self._op(None, abi.JR_BUILD)
@@ -525,7 +542,8 @@ class RowJoin:
 
     def materialize(self, stream, start: int, limit: int) -> tuple[int, abi.RowSet]:
         out = abi.RowSet()
-        n = lib().qdb_gpu_jr_materialize(self.prog.handle, self.pairs, stream.ptr, start, limit, C.byref(out))
+        n = lib().qdb_gpu_jr_materialize(self.prog.handle, self.pairs, None if stream is None else stream.ptr,
+                                         start, limit, C.byref(out))
         if n < 0:
             raise QdbError(f"jr_materialize failed: {last_error()}")
         return n, out
@@ -537,8 +555,10 @@ class RowJoin:
         return n
 
     def release(self) -> None:
-        """Frees the arena, table and pair buffer on the device."""
+        """Frees the arena(s), table and pair buffer on the device."""
         lib().qdb_gpu_jr_release(self.arena, self.table, self.scratch, self.pairs)
+        if self.null_arena is not None:
+            lib().qdb_gpu_jr_release(self.null_arena, None, None, None)
 
     def __del__(self):
         try:

@@ -19,6 +19,10 @@ COUNT_STAR, COUNT, SUM, MIN, MAX = range(1, 6)
 AGG_INIT, AGG_UPDATE, AGG_INIT_ROWS, AGG_SWITCH_TO_ROWS_AT, AGG_EXPECT_ROW_GROUPS = 0, 1, 3, 4, 5
 # jr_dispatch ops
 JR_INIT, JR_APPEND, JR_BUILD, JR_PROBE = 0, 1, 2, 3
+JR_APPEND_NULL_KEYS, JR_EMIT_BY_MARK = 5, 6
+# qdb_join_type (EJoinType order)
+JOIN_INNER, JOIN_LEFT, JOIN_RIGHT, JOIN_FULL = 0, 1, 2, 3
+JOIN_LEFT_SEMI, JOIN_RIGHT_SEMI, JOIN_LEFT_ANTI, JOIN_RIGHT_ANTI = 4, 5, 6, 7
 OUT_DEVICE = 1
 
 HASH_TABLE_SIZE = 304
@@ -91,6 +95,32 @@ class SortSpec(C.Structure):
                 ("n_out", C.c_int32), ("out_columns", C.POINTER(C.c_int32)), ("flags", C.c_uint32)]
 
 
+class RfBuildState(C.Structure):
+    """qdb_rf_build_state (RuntimeFilterBuild)."""
+    _fields_ = [("MaxKeys", C.c_int64), ("Mode", C.c_int64), ("Want", C.c_int64), ("Keys", C.c_void_p),
+                ("KeyCount", C.c_int64), ("SetCtrl", C.c_void_p), ("SetSlots", C.c_void_p),
+                ("SetCapacity", C.c_int64), ("SortOrder", C.c_void_p), ("SortKeys", C.c_void_p),
+                ("Bloom", C.c_void_p), ("BloomWords", C.c_int64)]
+
+
+class RfPartial(C.Structure):
+    """qdb_rf_partial (RuntimeFilterPartial)."""
+    _fields_ = [("Keys", C.c_void_p), ("KeyCount", C.c_int64), ("Bloom", C.c_void_p), ("BloomWords", C.c_int64)]
+
+
+class RfPublishState(C.Structure):
+    """qdb_rf_publish_state (RuntimeFilterPublish)."""
+    _fields_ = [("MaxKeys", C.c_int64), ("Keys", C.c_void_p), ("SetCtrl", C.c_void_p), ("SetSlots", C.c_void_p),
+                ("SetCapacity", C.c_int64), ("Table", C.c_void_p), ("Bloom", C.c_void_p),
+                ("BloomWords", C.c_int64), ("BloomSeeded", C.c_int64), ("Kind", C.c_int64),
+                ("ExactKeys", C.c_int64), ("TableSize", C.c_int64), ("BloomSetBits", C.c_int64)]
+
+
+class RfData(C.Structure):
+    """qdb_rf_data (RuntimeFilterData)."""
+    _fields_ = [("Kind", C.c_int64), ("Words", C.c_void_p), ("WordCount", C.c_int64)]
+
+
 class KernelTime(C.Structure):
     _fields_ = [("name", C.c_char * 48), ("ms", C.c_double), ("units", C.c_int64)]
 
@@ -128,6 +158,11 @@ SIGNATURES = {
     "qdb_gpu_top_k_select": (CI64, [P, PRS, P, CI64, CI64]),
     "qdb_gpu_top_sort_update": (CI64, [P, PRS, PRS, P, P, P, CI64, BOOLC, P, P, CI64, PRS]),
     "qdb_gpu_agg_run_noalloc": (CI64, [P, PRS, C.POINTER(Column), CI64]),
+    "qdb_gpu_rf_build": (CI64, [C.POINTER(RfBuildState), P, P, CI64]),
+    "qdb_gpu_rf_publish": (CI64, [C.POINTER(RfPublishState), C.POINTER(RfPartial), CI64]),
+    "qdb_gpu_rf_probe": (CI64, [C.POINTER(RfData), P, P, P, CI64, CI64, P, P]),
+    "qdb_gpu_rf_merge": (CI64, [P, P, CI64]),
+    "qdb_gpu_rf_probe_rowset": (CI64, [P, C.POINTER(RfData), PRS, P]),
     "qdb_gpu_init": (C.c_int, [C.c_int]),
     "qdb_gpu_last_error": (C.c_char_p, []),
     "qdb_gpu_set_stream": (None, [P]),

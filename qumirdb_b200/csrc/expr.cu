@@ -8,6 +8,7 @@
 #include "eval.h"
 #include "hash.h"
 #include "kernels.h"
+#include "rfilter.cuh"
 
 namespace qdb {
 
@@ -56,6 +57,20 @@ struct ExprLaunch {
     ExprArgs A;
 };
 
+// The NULL tests of the key slots: normally every key must be valid; with
+// null_keys_only at least one must be NULL.
+__device__ __forceinline__ bool KeyNullsPass(const ExprArgs& A, const GlobalAcc& acc) {
+    if (A.null_keys_only) {
+        bool any = false;
+        for (int j = 0; j < A.n_null_reject; ++j) any |= acc.Null(A.null_reject[j]);
+        return any;
+    }
+    for (int j = 0; j < A.n_null_reject; ++j) {
+        if (acc.Null(A.null_reject[j])) return false;
+    }
+    return true;
+}
+
 // Filters without a generic expression (selection, NULL rejects, atoms): no
 // evaluation stack, so it keeps a full SM of warps where FilterKernel's
 // generic evaluator (154 registers, a 1.7 KB stack) holds eight.
@@ -65,7 +80,7 @@ __global__ void __launch_bounds__(256) FilterAtomsKernel(const __grid_constant__
          r += int64_t(gridDim.x) * blockDim.x) {
         bool pass = P.selection == nullptr || P.selection[r] != 0;
         GlobalAcc acc{&P, r};
-        for (int j = 0; j < L.A.n_null_reject && pass; ++j) pass = !acc.Null(L.A.null_reject[j]);
+        if (pass) pass = KeyNullsPass(L.A, acc);
         if (pass && P.filter_kind == 1) pass = AtomsPass(P, acc);
         L.A.out_sel[r] = pass ? 1 : 0;
     }
@@ -77,7 +92,7 @@ __global__ void __launch_bounds__(256) FilterKernel(const __grid_constant__ Expr
          r += int64_t(gridDim.x) * blockDim.x) {
         bool pass = P.selection == nullptr || P.selection[r] != 0;
         GlobalAcc acc{&P, r};
-        for (int j = 0; j < L.A.n_null_reject && pass; ++j) pass = !acc.Null(L.A.null_reject[j]);
+        if (pass) pass = KeyNullsPass(L.A, acc);
         if (pass && P.filter_kind == 1) {
             pass = AtomsPass(P, acc);
         } else if (pass && P.filter_kind == 2) {
@@ -148,9 +163,13 @@ __global__ void __launch_bounds__(256) ProjectKernel(const __grid_constant__ Exp
 
 __global__ void __launch_bounds__(256) HashKernel(const __grid_constant__ ExprLaunch L) {
     const AggPlan& P = L.P;
+    unsigned long long kept = 0;
     for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < L.A.nrows;
          r += int64_t(gridDim.x) * blockDim.x) {
-        if (P.selection && !P.selection[r]) continue;
+        if (P.selection && !P.selection[r]) {
+            if (L.A.rf_out) L.A.rf_out[r] = 0;
+            continue;
+        }
         GlobalAcc acc{&P, r};
         uint64_t h = 0;
         for (int j = 0; j < L.A.nhash; ++j) {
@@ -166,7 +185,17 @@ __global__ void __launch_bounds__(256) HashKernel(const __grid_constant__ ExprLa
             }
             h = Combine(h, fh);
         }
-        L.A.hashes[r] = h;
+        if (L.A.rf_out) {
+            const bool keep = FilterContains(L.A.rf_kind, L.A.rf_words, L.A.rf_nwords, h);
+            L.A.rf_out[r] = keep ? 1 : 0;
+            kept += keep;
+        } else {
+            L.A.hashes[r] = h;
+        }
+    }
+    if (L.A.rf_kept) {
+        kept = WarpSumU64(kept);
+        if (LaneId() == 0 && kept) atomicAdd(L.A.rf_kept, kept);
     }
 }
 
@@ -217,9 +246,14 @@ __global__ void __launch_bounds__(256) WriteFlagsKernel(const uint8_t* flags, in
 }
 
 __global__ void __launch_bounds__(256) GatherKernel(const char* src, int width, const int64_t* idx, int stride,
-                                                    int64_t n, char* out) {
+                                                    int64_t n, char* out, const char* src2) {
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t j = idx[i * stride];
+        int64_t j = idx[i * stride];
+        if (j <= -2 && src2 != nullptr) {
+            // A row of the second source (the NULL-key arena of an ANTI join).
+            j = -j - 2;
+            src = src2;
+        }
         switch (width) {
             case 1: out[i] = j < 0 ? 0 : src[j]; break;
             case 2: reinterpret_cast<int16_t*>(out)[i] = j < 0 ? 0 : reinterpret_cast<const int16_t*>(src)[j]; break;
@@ -236,13 +270,21 @@ __global__ void __launch_bounds__(256) GatherKernel(const char* src, int width, 
 }
 
 __global__ void __launch_bounds__(256) GatherValidityKernel(const uint8_t* mask, int64_t mask_off, const int64_t* idx,
-                                                            int stride, int64_t n, uint32_t* out, int64_t out_off) {
+                                                            int stride, int64_t n, uint32_t* out, int64_t out_off,
+                                                            bool has2, const uint8_t* mask2) {
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t j = idx[i * stride];
+        int64_t j = idx[i * stride];
+        const uint8_t* m = mask;
+        int64_t moff = mask_off;
+        if (j <= -2 && has2) {
+            j = -j - 2;
+            m = mask2;
+            moff = 0;
+        }
         bool valid = j >= 0;
-        if (valid && mask) {
-            const int64_t bit = mask_off + j;
-            valid = (mask[bit >> 3] >> (bit & 7)) & 1;
+        if (valid && m) {
+            const int64_t bit = moff + j;
+            valid = (m[bit >> 3] >> (bit & 7)) & 1;
         }
         const int64_t o = out_off + i;
         if (valid) atomicOr(&out[o >> 5], 1u << (o & 31));
@@ -314,16 +356,17 @@ void CompactFlags(const uint8_t* flags, int64_t n, int64_t* out_idx, unsigned lo
 }
 
 void GatherColumn(const char* src, int width, const int64_t* idx, int idx_stride, int64_t n, char* out,
-                  cudaStream_t s) {
+                  cudaStream_t s, const char* src2) {
     if (n == 0) return;
-    GatherKernel<<<Blocks(n, 256), 256, 0, s>>>(src, width, idx, idx_stride, n, out);
+    GatherKernel<<<Blocks(n, 256), 256, 0, s>>>(src, width, idx, idx_stride, n, out, src2);
     CountLaunch();
 }
 
 void GatherValidity(const uint8_t* mask, int64_t mask_off, const int64_t* idx, int idx_stride, int64_t n,
-                    uint32_t* out_words, int64_t out_bit_off, cudaStream_t s) {
+                    uint32_t* out_words, int64_t out_bit_off, cudaStream_t s, bool has2, const uint8_t* mask2) {
     if (n == 0) return;
-    GatherValidityKernel<<<Blocks(n, 256), 256, 0, s>>>(mask, mask_off, idx, idx_stride, n, out_words, out_bit_off);
+    GatherValidityKernel<<<Blocks(n, 256), 256, 0, s>>>(mask, mask_off, idx, idx_stride, n, out_words, out_bit_off,
+                                                         has2, mask2);
     CountLaunch();
 }
 

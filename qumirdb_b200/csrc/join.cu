@@ -121,6 +121,14 @@ __device__ __forceinline__ unsigned ProbeRowMatches(const JoinProbeArgs& a, int6
                         [&](uint64_t slot, uint64_t, int) { emit(a.jt.rows[slot]); });
 }
 
+// A selected probe row with no NULL key field.
+__device__ __forceinline__ bool RowHasValidKey(const JoinProbeArgs& a, int64_t r) {
+    if (a.selection != nullptr && a.selection[r] == 0) return false;
+    bool null = false;
+    PackKeyCols(a, r, null);
+    return !null;
+}
+
 // Rows of one chunk of the pair probe (one block per chunk).
 constexpr int kPairChunk = 2048;
 constexpr int kPairThreads = 256;
@@ -134,7 +142,8 @@ __global__ void __launch_bounds__(kPairThreads) JoinPairCountKernel(const __grid
     const int64_t end = min(a.nrows, begin + kPairChunk);
     unsigned long long local = 0;
     for (int64_t r = begin + threadIdx.x; r < end; r += kPairThreads) {
-        const unsigned c = ProbeRowMatches(a, r, [](int64_t) {});
+        unsigned c = ProbeRowMatches(a, r, [](int64_t) {});
+        if (c == 0 && a.emit_unmatched && RowHasValidKey(a, r)) c = 1;   // padded with a NULL build row
         counts[r] = c;
         local += c;
     }
@@ -179,7 +188,7 @@ __global__ void __launch_bounds__(kPairThreads) JoinPairWriteKernel(const __grid
             tile += v;
         }
         __syncthreads();
-        const unsigned long long off = base + before + incl - c;
+        const unsigned long long off = a.pair_base + base + before + incl - c;
         base += tile;
         if (c == 0 || int64_t(off + c) > a.pair_cap) continue;
         int64_t* out = a.pairs + 2 * off;
@@ -191,6 +200,11 @@ __global__ void __launch_bounds__(kPairThreads) JoinPairWriteKernel(const __grid
             }
             ++k;
         });
+        if (k == 0) {   // an outer join's unmatched row (its count is 1)
+            out[0] = r;
+            out[1] = -1;
+            continue;
+        }
         // Arena order within the row (insertion sort; chains are short).
         for (unsigned x = 1; x < c; ++x) {
             const int64_t v = out[2 * x + 1];
@@ -201,6 +215,38 @@ __global__ void __launch_bounds__(kPairThreads) JoinPairWriteKernel(const __grid
             }
             out[2 * y + 1] = v;
         }
+    }
+}
+
+__global__ void __launch_bounds__(256) JoinNullKeyFlagsKernel(const __grid_constant__ JoinProbeArgs a, uint8_t* flags) {
+    for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < a.nrows; r += int64_t(gridDim.x) * blockDim.x) {
+        bool null = false;
+        if (a.selection == nullptr || a.selection[r] != 0) PackKeyCols(a, r, null);
+        flags[r] = null ? 1 : 0;
+    }
+}
+
+// Marks every build row a probe row matches; rows matched by many probe rows
+// take the same plain byte store, so no atomics are needed.
+__global__ void __launch_bounds__(256) JoinMarkKernel(const __grid_constant__ JoinProbeArgs a, uint8_t* marks) {
+    for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < a.nrows; r += int64_t(gridDim.x) * blockDim.x) {
+        ProbeRowMatches(a, r, [&](int64_t brow) {
+            if (marks[brow] == 0) marks[brow] = 1;
+        });
+    }
+}
+
+__global__ void __launch_bounds__(256) JoinMarkFlagsKernel(const uint8_t* marks, int64_t n, int want, uint8_t* flags) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        flags[i] = marks == nullptr ? 1 : uint8_t((marks[i] != 0) == (want != 0));
+    }
+}
+
+__global__ void __launch_bounds__(256) JoinWritePairsKernel(const int64_t* idx, int64_t n, int64_t* out, int mode) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t j = idx[i];
+        out[2 * i] = mode == 0 ? j : -1;
+        out[2 * i + 1] = mode == 0 ? -1 : (mode == 1 ? j : -j - 2);
     }
 }
 
@@ -493,6 +539,32 @@ void JoinProbeWrite(const JoinProbeArgs& a, const uint32_t* counts, const unsign
     ProfileBegin(s, "join_probe_pairs", a.nrows);
     JoinPairWriteKernel<<<unsigned(JoinPairChunks(a.nrows)), kPairThreads, 0, s>>>(a, counts, chunk_off);
     ProfileEnd(s);
+    CountLaunch();
+}
+
+void JoinNullKeyFlags(const JoinProbeArgs& a, uint8_t* flags, cudaStream_t s) {
+    if (a.nrows == 0) return;
+    JoinNullKeyFlagsKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(a, flags);
+    CountLaunch();
+}
+
+void JoinMarkProbe(const JoinProbeArgs& a, uint8_t* marks, cudaStream_t s) {
+    if (a.nrows == 0) return;
+    ProfileBegin(s, "join_mark_probe", a.nrows);
+    JoinMarkKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(a, marks);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
+void JoinMarkFlags(const uint8_t* marks, int64_t n, int want, uint8_t* flags, cudaStream_t s) {
+    if (n == 0) return;
+    JoinMarkFlagsKernel<<<Blocks(n, 256), 256, 0, s>>>(marks, n, want, flags);
+    CountLaunch();
+}
+
+void JoinWritePairs(const int64_t* idx, int64_t n, int64_t* out, int mode, cudaStream_t s) {
+    if (n == 0) return;
+    JoinWritePairsKernel<<<Blocks(n, 256), 256, 0, s>>>(idx, n, out, mode);
     CountLaunch();
 }
 

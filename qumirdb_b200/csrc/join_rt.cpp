@@ -34,6 +34,9 @@ struct ArenaState {
     int64_t capacity = 0;
     std::vector<ArenaCol> keys;
     std::vector<ArenaCol> payload;
+    bool want_marks = false;       // SEMI / ANTI: one mark byte per row
+    uint8_t* marks = nullptr;      // device, capacity bytes, zeroed
+    bool null_keys = false;        // the NULL-key arena of an ANTI join
 };
 
 struct TableState {
@@ -88,6 +91,7 @@ struct PairState {
     int64_t* dev = nullptr;        // (probe row, arena row) pairs
     int64_t cap = 0;
     ArenaState* arena = nullptr;
+    ArenaState* arena2 = nullptr;  // NULL-key arena (pairs name its rows -(r + 2))
     cudaStream_t s = nullptr;
 };
 
@@ -174,6 +178,14 @@ bool GrowArena(ArenaState* a, int64_t need) {
     for (auto& c : a->payload) {
         if (!grow(c)) return false;
     }
+    if (a->want_marks) {
+        auto* m = static_cast<uint8_t*>(DevAlloc(size_t(cap), a->s));
+        if (!m) return false;
+        cudaMemsetAsync(m, 0, size_t(cap), a->s);
+        if (a->marks) cudaMemcpyAsync(m, a->marks, size_t(a->rows), cudaMemcpyDeviceToDevice, a->s);
+        DevFree(a->marks, a->s);
+        a->marks = m;
+    }
     a->capacity = cap;
     return true;
 }
@@ -187,6 +199,7 @@ void DestroyArena(ArenaState* a) {
         DevFree(c.data, a->s);
         DevFree(c.valid, a->s);
     }
+    DevFree(a->marks, a->s);
     a->magic = 0;
     delete a;
 }
@@ -204,8 +217,10 @@ void DestroyTable(TableState* t) {
 }
 
 // Append: selected rows that pass the build predicate and have valid keys,
-// in input order (GenRowJoinAppendAst, qdb/kernel/join_gen.cpp:2063-2160).
-bool Append(const qdb_gpu_program* prog, ArenaState* a, qdb_rowset* batch) {
+// in input order (GenRowJoinAppendAst, qdb/kernel/join_gen.cpp:2063-2160);
+// with null_keys, the rows whose key has a NULL field instead (the
+// jr_append_null_keys variant, nullKeys = true).
+bool Append(const qdb_gpu_program* prog, ArenaState* a, qdb_rowset* batch, bool null_keys = false) {
     const JoinProgram& J = prog->join;
     const int64_t n = batch->RowCount;
     if (n == 0) return true;
@@ -229,6 +244,7 @@ bool Append(const qdb_gpu_program* prog, ArenaState* a, qdb_rowset* batch) {
     for (size_t j = 0; j < J.build_keys.size(); ++j) {
         ea.null_reject[j] = uint8_t(J.build_filter.cols.slot_of[J.build_keys[j]]);
     }
+    ea.null_keys_only = null_keys ? 1 : 0;
     FilterRows(ea, s);
     CompactFlags(flags, n, idx, dcount, scratch, s);
     unsigned long long selected = 0;
@@ -465,6 +481,47 @@ bool ProbeKeyArgs(const JoinProgram& J, qdb_rowset* batch, Staging& stg, JoinPro
     return true;
 }
 
+PairState* PairsOf(PairBuf* pairs, cudaStream_t s) {
+    if (!pairs->state || pairs->state->magic != kPairMagic) {
+        pairs->state = new PairState();
+        pairs->state->s = s;
+    }
+    return pairs->state;
+}
+
+// Room for `need` pairs; the first `keep` are kept.
+bool ReservePairs(PairState* ps, int64_t need, int64_t keep, cudaStream_t s) {
+    if (ps->cap >= need && ps->dev) return true;
+    const int64_t cap = std::max<int64_t>(need, std::max<int64_t>(1024, ps->cap * 2));
+    auto* d = static_cast<int64_t*>(DevAlloc(size_t(cap) * 16, s));
+    if (!d) return false;
+    if (keep > 0) cudaMemcpyAsync(d, ps->dev, size_t(keep) * 16, cudaMemcpyDeviceToDevice, s);
+    DevFree(ps->dev, s);
+    ps->dev = d;
+    ps->cap = cap;
+    return true;
+}
+
+// Compacts flags[0, n) into ascending indices; returns their count, < 0 on
+// a device failure.  idx has room for n entries.
+int64_t CompactCount(const uint8_t* flags, int64_t n, int64_t* idx, cudaStream_t s) {
+    if (n == 0) return 0;
+    auto* dcount = static_cast<unsigned long long*>(DevAlloc(8, s));
+    void* scratch = DevAlloc(CompactScratch(n), s);
+    if (!dcount || !scratch) {
+        DevFree(dcount, s);
+        DevFree(scratch, s);
+        return -1;
+    }
+    CompactFlags(flags, n, idx, dcount, scratch, s);
+    unsigned long long k = 0;
+    cudaMemcpyAsync(&k, dcount, 8, cudaMemcpyDeviceToHost, s);
+    const bool ok = CudaOk(cudaStreamSynchronize(s), "row join compaction");
+    DevFree(dcount, s);
+    DevFree(scratch, s);
+    return ok ? int64_t(k) : -1;
+}
+
 bool Probe(const qdb_gpu_program* prog, ArenaState* a, TableState* t, PairBuf* pairs, qdb_rowset* batch) {
     const JoinProgram& J = prog->join;
     const int64_t n = batch->RowCount;
@@ -476,51 +533,105 @@ bool Probe(const qdb_gpu_program* prog, ArenaState* a, TableState* t, PairBuf* p
     p.jkey = J.probe_jk;
     p.jt = t->dev();
     p.nrows = n;
-    if (!pairs->state || pairs->state->magic != kPairMagic) {
-        pairs->state = new PairState();
-        pairs->state->s = s;
-    }
-    PairState* ps = pairs->state;
+    PairState* ps = PairsOf(pairs, s);
     ps->arena = a;
+    if (J.marks_build) {
+        // SEMI / ANTI: mark the matched build rows; no pairs (jt_probe_and_mark).
+        JoinMarkProbe(p, a->marks, s);
+        pairs->count = 0;
+        pairs->capacity = ps->cap;
+        return CudaOk(cudaStreamSynchronize(s), "row join mark probe");
+    }
+    // An outer join pads its NULL-key rows first, in row order, as the
+    // collect pass of jr_probe_batch does (join_gen.cpp:2206-2230).
+    int64_t nnull = 0;
+    int64_t* null_idx = nullptr;
+    if (J.emit_unmatched && n > 0) {
+        auto* flags = static_cast<uint8_t*>(DevAlloc(size_t(n), s));
+        null_idx = static_cast<int64_t*>(DevAlloc(size_t(n) * 8, s));
+        if (!flags || !null_idx) {
+            DevFree(flags, s);
+            DevFree(null_idx, s);
+            return false;
+        }
+        JoinNullKeyFlags(p, flags, s);
+        nnull = CompactCount(flags, n, null_idx, s);
+        DevFree(flags, s);
+        if (nnull < 0) {
+            DevFree(null_idx, s);
+            return false;
+        }
+        p.emit_unmatched = 1;
+    }
     // Count pass, scan of the chunk totals (the last entry becomes the
     // total), then the write pass into a buffer of exactly that size.
     const int64_t nch = JoinPairChunks(n);
     auto* counts = static_cast<uint32_t*>(DevAlloc(size_t(std::max<int64_t>(n, 1)) * 4, s));
     auto* off = static_cast<unsigned long long*>(DevAlloc(size_t(nch + 1) * 8, s));
-    if (!counts || !off) {
+    auto free_scratch = [&]() {
         DevFree(counts, s);
         DevFree(off, s);
+        DevFree(null_idx, s);
+    };
+    auto fail = [&]() {
+        free_scratch();
         return false;
-    }
+    };
+    if (!counts || !off) return fail();
     cudaMemsetAsync(off, 0, size_t(nch + 1) * 8, s);
     JoinProbeCount(p, counts, off, s);
     ExclusiveScanU64(off, nch + 1, s);
-    unsigned long long total = 0;
-    cudaMemcpyAsync(&total, off + nch, 8, cudaMemcpyDeviceToHost, s);
-    if (!CudaOk(cudaStreamSynchronize(s), "row join probe count")) {
-        DevFree(counts, s);
-        DevFree(off, s);
-        return false;
-    }
-    if (ps->cap < int64_t(total) || !ps->dev) {
-        DevFree(ps->dev, s);
-        ps->cap = std::max<int64_t>(int64_t(total), 1024);
-        ps->dev = static_cast<int64_t*>(DevAlloc(size_t(ps->cap) * 16, s));
-        if (!ps->dev) {
-            ps->cap = 0;
-            DevFree(counts, s);
-            DevFree(off, s);
-            return false;
-        }
-    }
+    unsigned long long matched = 0;
+    cudaMemcpyAsync(&matched, off + nch, 8, cudaMemcpyDeviceToHost, s);
+    if (!CudaOk(cudaStreamSynchronize(s), "row join probe count")) return fail();
+    const int64_t total = nnull + int64_t(matched);
+    if (!ReservePairs(ps, total, 0, s)) return fail();
+    JoinWritePairs(null_idx, nnull, ps->dev, 0, s);
     p.pairs = ps->dev;
     p.pair_cap = ps->cap;
+    p.pair_base = nnull;
     JoinProbeWrite(p, counts, off, s);
-    DevFree(counts, s);
-    DevFree(off, s);
-    pairs->count = int64_t(total);
+    free_scratch();
+    pairs->count = total;
     pairs->capacity = ps->cap;
     return CudaOk(cudaStreamSynchronize(s), "row join probe");
+}
+
+// jr_emit_by_mark (qdb/kernel/join/join_rows.oz:199-224): appends (NULL,
+// build row) for every arena row whose mark is `marked`, in build order.  The
+// NULL-key arena of an ANTI join has no marks: all its rows are emitted.
+bool EmitByMark(const JoinProgram& J, ArenaState* a, PairBuf* pairs) {
+    cudaStream_t s = a->s;
+    PairState* ps = PairsOf(pairs, s);
+    const bool second = a->null_keys;
+    if (second) {
+        ps->arena2 = a;
+    } else {
+        ps->arena = a;
+    }
+    const int64_t have = pairs->count;
+    const int64_t n = a->rows;
+    if (n == 0) return true;
+    auto* flags = static_cast<uint8_t*>(DevAlloc(size_t(n), s));
+    auto* idx = static_cast<int64_t*>(DevAlloc(size_t(n) * 8, s));
+    if (!flags || !idx) {
+        DevFree(flags, s);
+        DevFree(idx, s);
+        return false;
+    }
+    const bool semi = J.join_type == QDB_JOIN_LEFT_SEMI;
+    JoinMarkFlags(second ? nullptr : a->marks, n, semi ? 1 : 0, flags, s);
+    const int64_t k = CompactCount(flags, n, idx, s);
+    bool ok = k >= 0 && ReservePairs(ps, have + k, have, s);
+    if (ok) {
+        JoinWritePairs(idx, k, ps->dev + 2 * have, second ? 2 : 1, s);
+        pairs->count = have + k;
+        pairs->capacity = ps->cap;
+        ok = CudaOk(cudaStreamSynchronize(s), "row join emit by mark");
+    }
+    DevFree(flags, s);
+    DevFree(idx, s);
+    return ok;
 }
 
 }  // namespace
@@ -533,11 +644,29 @@ extern "C" {
 
 qdb_gpu_program* qdb_gpu_compile_row_join(const qdb_row_join_spec* spec, char* err, size_t err_len) {
     try {
-        if (spec->join_type != QDB_JOIN_INNER) throw LowerError("only inner row joins are served");
+        // CompileRowJoin (qdb/kernel/compiler.cpp:3134-3148): an outer join
+        // streams its preserved side, so it builds the other one; a SEMI/ANTI
+        // join builds its left side and marks the rows it matches.
+        const int jt = spec->join_type;
+        const bool streams_preserved = spec->build_is_left ? jt == QDB_JOIN_RIGHT : jt == QDB_JOIN_LEFT;
+        const bool marks_build = spec->build_is_left && (jt == QDB_JOIN_LEFT_SEMI || jt == QDB_JOIN_LEFT_ANTI);
+        if (jt != QDB_JOIN_INNER && !streams_preserved && !marks_build) {
+            throw LowerError("only inner joins, outer joins that build their null-supplying side and "
+                             "semi/anti joins that build their left side are served");
+        }
+        if (marks_build) {
+            for (int k = 0; k < spec->n_out; ++k) {
+                if (spec->out_side[k] != 1) throw LowerError("a SEMI/ANTI join outputs build columns only");
+            }
+        }
         auto* p = new qdb_gpu_program();
         p->kind = PK_JOIN;
         p->flags = spec->flags;
         JoinProgram& J = p->join;
+        J.join_type = jt;
+        J.emit_unmatched = streams_preserved;
+        J.marks_build = marks_build;
+        J.keeps_null_keys = marks_build && jt == QDB_JOIN_LEFT_ANTI;
         J.build_is_left = spec->build_is_left;
         J.build_columns.assign(spec->build_columns, spec->build_columns + spec->n_build_columns);
         J.probe_columns.assign(spec->probe_columns, spec->probe_columns + spec->n_probe_columns);
@@ -619,6 +748,7 @@ qdb_gpu_program* qdb_gpu_compile_join_aggregate(const qdb_row_join_spec* join, c
     qdb_gpu_program* p = qdb_gpu_compile_row_join(join, err, err_len);
     if (!p) return nullptr;
     try {
+        if (join->join_type != QDB_JOIN_INNER) throw LowerError("a fused join-aggregate is an inner join");
         if (agg->n_columns != join->n_probe_columns + join->n_payload) {
             throw LowerError("aggregate input must be the probe columns followed by the payload columns");
         }
@@ -666,9 +796,37 @@ bool qdb_gpu_jr_dispatch(const qdb_gpu_program* prog, void* arena, void* table, 
                 col.width = Width(J.build_columns[c].type);
                 a->payload.push_back(col);
             }
+            a->want_marks = J.marks_build;
             *static_cast<ArenaState**>(arena) = a;
             static_cast<int64_t*>(arena)[5] = 0;
             return GrowArena(a, 1024);
+        }
+        case QDB_JR_OP_APPEND_NULL_KEYS: {
+            ArenaState* a = ArenaOf(arena);
+            if (!J.keeps_null_keys) {
+                SetErr("jr_dispatch(AppendNullKeys) is only served for LEFT_ANTI joins");
+                return false;
+            }
+            if (!a || !batch) {
+                SetErr("jr_dispatch(AppendNullKeys) before Init");
+                return false;
+            }
+            a->null_keys = true;
+            if (!Append(prog, a, batch, true)) return false;
+            static_cast<int64_t*>(arena)[5] = a->rows;
+            return true;
+        }
+        case QDB_JR_OP_EMIT_BY_MARK: {
+            ArenaState* a = ArenaOf(arena);
+            if (!J.marks_build) {
+                SetErr("jr_dispatch(EmitByMark) is only served for LEFT_SEMI / LEFT_ANTI joins");
+                return false;
+            }
+            if (!a || !pairs) {
+                SetErr("jr_dispatch(EmitByMark) before Init");
+                return false;
+            }
+            return EmitByMark(J, a, static_cast<PairBuf*>(pairs));
         }
         case QDB_JR_OP_APPEND: {
             ArenaState* a = ArenaOf(arena);
@@ -738,11 +896,13 @@ int64_t qdb_gpu_jr_materialize(const qdb_gpu_program* prog, void* pairs_v, qdb_r
     if (n == 0) return 0;
     cudaStream_t s = CurStream();
     PairState* ps = pairs->state;
-    if (!ps || ps->magic != kPairMagic || !ps->arena || !stream) {
+    const bool probe_cols = std::find(J.out_side.begin(), J.out_side.end(), 0) != J.out_side.end();
+    if (!ps || ps->magic != kPairMagic || (!ps->arena && !ps->arena2) || (probe_cols && !stream)) {
         SetErr("jr_materialize: the pair buffer holds no probe result");
         return -1;
     }
-    ArenaState* a = ps->arena;
+    ArenaState* a = ps->arena ? ps->arena : ps->arena2;
+    ArenaState* a2 = ps->arena2;
     Staging stg(s);
     std::vector<int> types;
     for (size_t k = 0; k < J.out_side.size(); ++k) {
@@ -766,9 +926,13 @@ int64_t qdb_gpu_jr_materialize(const qdb_gpu_program* prog, void* pairs_v, qdb_r
                                       : nullptr;
             GatherValidity(m, c.MaskBitOffset, base, 2, n, cols[k].valid, 0, s);
         } else {
+            // Build row -1 is an outer join's NULL row; -(r + 2) row r of the
+            // NULL-key arena.
             const ArenaCol& ac = a->payload[J.out_column[k]];
-            GatherColumn(ac.data, w, base + 1, 2, n, cols[k].data, s);
-            GatherValidity(reinterpret_cast<const uint8_t*>(ac.valid), 0, base + 1, 2, n, cols[k].valid, 0, s);
+            const ArenaCol* ac2 = a2 ? &a2->payload[J.out_column[k]] : nullptr;
+            GatherColumn(ac.data, w, base + 1, 2, n, cols[k].data, s, ac2 ? ac2->data : nullptr);
+            GatherValidity(reinterpret_cast<const uint8_t*>(ac.valid), 0, base + 1, 2, n, cols[k].valid, 0, s,
+                           ac2 != nullptr, ac2 ? reinterpret_cast<const uint8_t*>(ac2->valid) : nullptr);
         }
     }
     if (!EmitRowset(cols, types, n, (prog->flags & QDB_OUT_DEVICE) != 0, s, out)) return -1;

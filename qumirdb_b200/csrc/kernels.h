@@ -214,6 +214,8 @@ struct JoinProbeArgs {
     int64_t nrows;
     int64_t* pairs;          // (probe row, build row)
     int64_t pair_cap;
+    int64_t pair_base;       // pairs already written before this probe's
+    int32_t emit_unmatched;  // outer join: a valid-key row with no match pairs with -1
     int* err;
 };
 // The pair probe in two passes: per-row match counts plus per-chunk totals
@@ -224,14 +226,29 @@ int64_t JoinPairChunks(int64_t nrows);
 void JoinProbeCount(const JoinProbeArgs& a, uint32_t* counts, unsigned long long* chunk_tot, cudaStream_t s);
 void JoinProbeWrite(const JoinProbeArgs& a, const uint32_t* counts, const unsigned long long* chunk_off,
                     cudaStream_t s);
+// flags[r] = 1 for a selected probe row whose key is NULL (an outer join
+// pads those first, as jr_probe_batch's collect pass does).
+void JoinNullKeyFlags(const JoinProbeArgs& a, uint8_t* flags, cudaStream_t s);
+// SEMI / ANTI probe: marks[arena row] = 1 for every build row a selected
+// valid-key probe row matches.
+void JoinMarkProbe(const JoinProbeArgs& a, uint8_t* marks, cudaStream_t s);
+// flags[i] = (marks[i] != 0) == want over arena rows; every row when marks
+// is null.
+void JoinMarkFlags(const uint8_t* marks, int64_t n, int want, uint8_t* flags, cudaStream_t s);
+// Pair rows from compacted indices: mode 0 (idx, -1) a padded probe row;
+// mode 1 (-1, idx) a build row of the arena; mode 2 (-1, -(idx + 2)) a row
+// of the NULL-key arena.
+void JoinWritePairs(const int64_t* idx, int64_t n, int64_t* out, int mode, cudaStream_t s);
 
-// Gathers rows: out[i] = src[idx[i]] for `width`-byte values (idx < 0 -> 0).
+// Gathers rows: out[i] = src[idx[i]] for `width`-byte values (idx < 0 -> 0;
+// with src2, idx <= -2 reads src2[-idx - 2]).
 void GatherColumn(const char* src, int width, const int64_t* idx, int idx_stride, int64_t n, char* out,
-                  cudaStream_t s);
+                  cudaStream_t s, const char* src2 = nullptr);
 // Sets bit (out_bit_off + i) of out_words (pre-zeroed) for every valid
-// gathered row i.
+// gathered row i (idx == -1 is NULL; idx <= -2 reads mask2 when has2).
 void GatherValidity(const uint8_t* mask, int64_t mask_off, const int64_t* idx, int idx_stride, int64_t n,
-                    uint32_t* out_words, int64_t out_bit_off, cudaStream_t s);
+                    uint32_t* out_words, int64_t out_bit_off, cudaStream_t s, bool has2 = false,
+                    const uint8_t* mask2 = nullptr);
 
 // In-place exclusive scan of n counters (one block; n up to a few million).
 void ExclusiveScanU64(unsigned long long* counts, int64_t n, cudaStream_t s);
@@ -245,6 +262,9 @@ struct ExprArgs {
     uint8_t* out_sel = nullptr;
     int32_t n_null_reject = 0;
     uint8_t null_reject[4] = {};
+    // Set: the other way round, a selected row passes only when one of the
+    // null_reject slots IS NULL (the NULL-key rows an ANTI join keeps).
+    int32_t null_keys_only = 0;
     // Project: output k = value (src, idx) stored with type out_type[k].
     int32_t nout = 0;
     uint8_t out_src[kMaxCols] = {};
@@ -257,6 +277,15 @@ struct ExprArgs {
     int32_t hash_type[kMaxKeyParts] = {};
     uint8_t hash_nullable[kMaxKeyParts] = {};   // the key struct has a validity field
     uint64_t* hashes = nullptr;
+    // With rf_out, the hash kernel writes rf_out[r] = 1 for a selected row
+    // whose hash the runtime filter (rf_kind 1 exact / 2 Bloom over
+    // rf_words[0, rf_nwords)) may contain, else 0, and counts those rows in
+    // *rf_kept, instead of writing the hash.
+    uint8_t* rf_out = nullptr;
+    const uint64_t* rf_words = nullptr;
+    int64_t rf_kind = 0;
+    int64_t rf_nwords = 0;
+    unsigned long long* rf_kept = nullptr;
     int* err = nullptr;
 };
 void FilterRows(const ExprArgs& a, cudaStream_t s);

@@ -774,6 +774,18 @@ void Fill(char* err, size_t len, const char* msg) {
     t_error = msg;
 }
 
+// The struct rh_hash of a hash program's key slots over nrows rows.
+void HashArgs(const qdb_gpu_program* prog, const AggPlan& plan, int64_t nrows, ExprArgs& a) {
+    a.plan = &plan;
+    a.nrows = nrows;
+    a.nhash = int(prog->expr.out_types.size());
+    for (int j = 0; j < a.nhash; ++j) {
+        a.hash_slot[j] = uint8_t(prog->expr.value_idx[j]);
+        a.hash_type[j] = prog->expr.out_types[j];
+        a.hash_nullable[j] = plan.cols[a.hash_slot[j]].nullable;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1089,6 +1101,41 @@ void qdb_gpu_project(const qdb_gpu_program* prog, qdb_rowset* in, void** out_buf
     DevFree(derr, s);
 }
 
+int64_t qdb_gpu_rf_probe_rowset(const qdb_gpu_program* prog, const qdb_rf_data* data, qdb_rowset* batch,
+                                uint8_t* output) {
+    t_error.clear();
+    if (!prog || prog->kind != PK_HASH || !data || !batch || (batch->RowCount > 0 && !output) ||
+        (data->Kind != 1 && data->Kind != 2)) {
+        SetErr("rf_probe_rowset: bad arguments (a hash program, and Kind 1 exact or 2 Bloom)");
+        return -1;
+    }
+    if (!IsDevicePtr(output) || !IsDevicePtr(data->Words)) {
+        SetErr("rf_probe_rowset: the output and the filter's words must be in device memory");
+        return -1;
+    }
+    if (batch->RowCount == 0) return 0;
+    cudaStream_t s = CurStream();
+    AggPlan plan = prog->expr.plan;
+    Staging stg(s);
+    if (!ResolveColumns(plan, prog->expr.cols, prog->columns.data(), batch, stg)) return -1;
+    ExprArgs a;
+    HashArgs(prog, plan, batch->RowCount, a);
+    auto* kept = static_cast<unsigned long long*>(DevAlloc(8, s));
+    if (!kept) return -1;
+    cudaMemsetAsync(kept, 0, 8, s);
+    a.rf_out = output;
+    a.rf_words = data->Words;
+    a.rf_kind = data->Kind;
+    a.rf_nwords = data->WordCount;
+    a.rf_kept = kept;
+    HashRows(a, s);
+    unsigned long long k = 0;
+    cudaMemcpyAsync(&k, kept, 8, cudaMemcpyDeviceToHost, s);
+    const bool ok = CudaOk(cudaStreamSynchronize(s), "rf_probe_rowset");
+    DevFree(kept, s);
+    return ok ? int64_t(k) : -1;
+}
+
 bool qdb_gpu_hash(const qdb_gpu_program* prog, qdb_rowset* batch, uint64_t* hashes) {
     t_error.clear();
     if (!prog || prog->kind != PK_HASH || !batch || !hashes) {
@@ -1100,14 +1147,7 @@ bool qdb_gpu_hash(const qdb_gpu_program* prog, qdb_rowset* batch, uint64_t* hash
     Staging stg(s);
     if (!ResolveColumns(plan, prog->expr.cols, prog->columns.data(), batch, stg)) return false;
     ExprArgs a;
-    a.plan = &plan;
-    a.nrows = batch->RowCount;
-    a.nhash = int(prog->expr.out_types.size());
-    for (int j = 0; j < a.nhash; ++j) {
-        a.hash_slot[j] = uint8_t(prog->expr.value_idx[j]);
-        a.hash_type[j] = prog->expr.out_types[j];
-        a.hash_nullable[j] = plan.cols[a.hash_slot[j]].nullable;
-    }
+    HashArgs(prog, plan, batch->RowCount, a);
     const bool dev_out = IsDevicePtr(hashes);
     uint64_t* out = dev_out ? hashes : static_cast<uint64_t*>(DevAlloc(size_t(batch->RowCount) * 8, s));
     if (!dev_out && batch->Selection) {

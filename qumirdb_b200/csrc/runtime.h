@@ -107,6 +107,10 @@ bool EmitRowset(std::vector<AggOutputCol>& cols, const std::vector<int>& types, 
 
 struct JoinProgram {
     int32_t build_is_left = 0;
+    int32_t join_type = QDB_JOIN_INNER;
+    bool emit_unmatched = false;      // outer join streaming its preserved side
+    bool marks_build = false;         // LEFT_SEMI / LEFT_ANTI building the left side
+    bool keeps_null_keys = false;     // LEFT_ANTI: NULL-key build rows in a second arena
     std::vector<qdb_column_type> build_columns;
     std::vector<qdb_column_type> probe_columns;
     std::vector<int> build_keys;

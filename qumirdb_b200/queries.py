@@ -48,7 +48,7 @@ class AggSpec:
 
 class JoinSpec:
     def __init__(self, build_columns, probe_columns, build_keys, probe_keys, payload, out=(), build_eb=None,
-                 build_filter=None, flags=0):
+                 build_filter=None, flags=0, join_type=0, build_is_left=0):
         self.bcols = coltypes(build_columns)
         self.pcols = coltypes(probe_columns)
         self.bkeys = i32s(build_keys)
@@ -59,7 +59,8 @@ class JoinSpec:
         self.build_eb = build_eb
         self.bnodes = build_eb.array() if build_eb else (abi.Expr * 1)()
         s = abi.RowJoinSpec()
-        s.join_type = 0
+        s.join_type = join_type
+        s.build_is_left = build_is_left
         s.n_build_columns, s.build_columns = len(build_columns), self.bcols
         s.n_probe_columns, s.probe_columns = len(probe_columns), self.pcols
         s.n_keys, s.build_keys, s.probe_keys = len(build_keys), self.bkeys, self.pkeys
@@ -69,6 +70,7 @@ class JoinSpec:
         s.build_filter = -1 if build_filter is None else build_filter
         s.flags = flags
         self.struct = s
+        self.join_type = join_type
 
 
 # Column order of the lineitem-shaped table.
@@ -113,6 +115,9 @@ def lineitem_agg(cutoff: int, flags: int = 0) -> AggSpec:
 
 JOIN_BUILD_COLUMNS = [(abi.I64,), (abi.I64,), (abi.I32,)]
 JOIN_PROBE_COLUMNS = [(abi.I64,), (abi.I64,)]
+# The same schemas with nullable key columns.
+JOIN_BUILD_COLUMNS_NULLABLE = [(abi.I64, 0, 1), (abi.I64,), (abi.I32,)]
+JOIN_PROBE_COLUMNS_NULLABLE = [(abi.I64, 0, 1), (abi.I64,)]
 
 
 def join_sum(attr_lt: int = 20, flags: int = 0) -> tuple[JoinSpec, AggSpec]:

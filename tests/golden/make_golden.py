@@ -34,6 +34,9 @@ CASES = {
                            "big_sort_f_desc", "big_sort_i_asc", "big_sort_i_desc", "big_top_i_asc",
                            "big_top_f_desc_offset"],
     "selectivity": ["join_composite_key_filtered", "join_shared_key_range", "join_shared_key_range_independent"],
+    "outer_join": ["duplicates", "null_keys", "all_matched", "none_matched", "empty_build", "empty_probe",
+                   "right_join", "preserved_larger"],
+    "anti_join_conditions": ["exists_build_outer_side", "not_exists_filter_above"],
 }
 
 

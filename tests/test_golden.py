@@ -525,3 +525,143 @@ def test_selectivity_joins(engine, name):
         q.release(out)
     schema, want = expected(key)
     assert_rows(normalize(rows, schema), want)
+
+
+# ---------------------------------------------------------------------------
+# Outer, SEMI and ANTI row joins (jr_dispatch + jr_materialize): the pairs
+# are materialized into the selected columns, then ORDER BY is applied to
+# the output rows (NULLs last, the default for ASC).
+# ---------------------------------------------------------------------------
+def run_row_join(engine, jspec, bcols, pcols, build, probe, pbounds):
+    """Output rows of a row join: oracle pairs read back from the host
+    columns, or the device join materialized in 16384-row slices."""
+    outs = list(zip(jspec.out_side, jspec.out_col))[: jspec.struct.n_out]
+    payload = list(jspec.payload)[: jspec.struct.n_payload]
+    marks = jspec.join_type in (abi.JOIN_LEFT_SEMI, abi.JOIN_LEFT_ANTI)
+    if engine == "oracle":
+        rows = []
+        for left, right in O.row_join_typed(jspec, build, probe).tolist():
+            row = []
+            for side, c in outs:
+                if side == 0:
+                    b, r = left >> 32, left & 0xFFFFFFFF
+                    vals, valid, _ = pcols[c]
+                    g = pbounds[b][0] + r
+                else:
+                    vals, valid, _ = bcols[payload[c]]
+                    g = right
+                ok = g >= 0 and (valid is None or bool(valid[g]))
+                row.append(int(vals[g]) if ok else None)
+            rows.append(row)
+        return rows
+    types = [pcols[c][2][0] if side == 0 else bcols[payload[c]][2][0] for side, c in outs]
+    J = q.RowJoin(q.compile_row_join(jspec), keeps_null_keys=jspec.join_type == abi.JOIN_LEFT_ANTI)
+    for rs in build:
+        J.append(rs)
+    J.build()
+    rows = []
+
+    def drain(stream, n):
+        start = 0
+        while start < n:
+            k, out = J.materialize(stream, start, 16384)
+            rows.extend(gpu_rows(out, types))
+            q.release(out)
+            start += k
+
+    for rs in probe:
+        n = J.probe(rs)
+        if not marks:
+            drain(rs, n)
+    if marks:
+        drain(None, J.emit_by_mark())
+    J.release()
+    return rows
+
+
+def order_rows(rows, by):
+    """ORDER BY columns `by` ascending, NULLs last."""
+    return sorted(rows, key=lambda r: tuple((1, 0) if r[j] is None else (0, r[j]) for j in by))
+
+
+OUTER = {
+    # name: (preserved table, build table, probe grp filter, build flag filter, output, ORDER BY)
+    "duplicates": ("c", "o", None, None, ["ck", "cv", "ok", "ov"], ["cv", "ov"]),
+    "null_keys": ("c", "o", 4, None, ["ck", "cv", "ok", "ov"], ["cv", "ov"]),
+    "all_matched": ("c", "o", 1, None, ["ck", "cv", "ok", "ov"], ["cv", "ov"]),
+    "none_matched": ("c", "o", 2, None, ["ck", "cv", "ok", "ov"], ["cv", "ov"]),
+    "empty_build": ("c", "o", 3, None, ["ck", "cv", "ok", "ov"], ["cv", "ov"]),
+    "empty_probe": ("c", "o", None, 2, ["ck", "cv", "ok", "ov"], ["cv", "ov"]),
+    "right_join": ("c", "o", None, None, ["ok", "ov", "ck", "cv"], ["cv", "ov"]),
+    "preserved_larger": ("o", "c", None, None, ["ok", "ov", "ck", "cv"], ["ov", "cv"]),
+}
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("name", sorted(OUTER))
+def test_outer_join_goldens(engine, name):
+    """c LEFT JOIN o (o RIGHT JOIN c for right_join): the preserved side
+    streams through the probe, the null-supplying side is built; a WHERE on
+    the preserved side is its selection, an ON condition on the built side
+    is the build predicate."""
+    key = f"outer_join/{name}"
+    pres, bld, grp, flag, select, order = OUTER[name]
+    tp, tb = Table(case(key)["tables"][pres]), Table(case(key)["tables"][bld])
+    pnames, bnames = list(tp.cols), list(tb.cols)
+    pcols, bcols = [tp.cols[c] for c in pnames], [tb.cols[c] for c in bnames]
+    be = q.ExprBuilder()
+    bfilter = None
+    if flag is not None:
+        bfilter = be.op(abi.EQ, abi.BOOL, be.col(bnames.index("flag"), abi.I64), be.const(flag, abi.I64))
+    psel = None if grp is None else (tp.cols["grp"][0] == grp)
+    out = [(0, pnames.index(c)) if c in pnames else (1, bnames.index(c)) for c in select]
+    right = name == "right_join"
+    jspec = queries.JoinSpec(types_of(bcols), types_of(pcols), [0], [0], list(range(len(bcols))), out=out,
+                             build_eb=be if bfilter is not None else None, build_filter=bfilter,
+                             join_type=abi.JOIN_RIGHT if right else abi.JOIN_LEFT, build_is_left=1 if right else 0)
+    build = rowsets(bcols, tb.batches(), engine)
+    probe = rowsets(pcols, tp.batches(), engine, psel)
+    rows = run_row_join(engine, jspec, bcols, pcols, build, probe, tp.batches())
+    schema, want = expected(key)
+    assert_rows(normalize(order_rows(rows, [select.index(c) for c in order]), schema), want)
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("kind", ["semi", "anti"])
+def test_exists_build_outer_side(engine, kind):
+    """SELECT id FROM t WHERE [NOT] EXISTS (SELECT 1 FROM w WHERE w.k = t.a):
+    LEFT_SEMI / LEFT_ANTI building t (its NULL key kept by the ANTI join);
+    the golden's residual variants are other join programs."""
+    key = "anti_join_conditions/exists_build_outer_side"
+    t, w = Table(case(key)["tables"]["t"]), Table(case(key)["tables"]["w"])
+    tnames = list(t.cols)
+    bcols, pcols = [t.cols[c] for c in tnames], [w.cols["k"], w.cols["v"]]
+    jt = abi.JOIN_LEFT_SEMI if kind == "semi" else abi.JOIN_LEFT_ANTI
+    jspec = queries.JoinSpec(types_of(bcols), types_of(pcols), [tnames.index("a")], [0], [tnames.index("id")],
+                             out=[(1, 0)], join_type=jt, build_is_left=1)
+    rows = run_row_join(engine, jspec, bcols, pcols, rowsets(bcols, t.batches(), engine),
+                        rowsets(pcols, w.batches(), engine), w.batches())
+    schema, want = expected(key)
+    want = sorted(int(r[1]) for r in want if r[0] == kind)
+    assert sorted(r[0] for r in rows) == want
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_not_exists_filter_above(engine):
+    """SELECT id FROM t WHERE NOT EXISTS (SELECT 1 FROM s WHERE s.k = t.id
+    AND s.v > 4) AND t.b > 15: LEFT_ANTI building t with b > 15 fused into
+    Append, probing s with the selection of v > 4."""
+    key = "anti_join_conditions/not_exists_filter_above"
+    t, s = Table(case(key)["tables"]["t"]), Table(case(key)["tables"]["s"])
+    tnames = list(t.cols)
+    bcols, pcols = [t.cols[c] for c in tnames], [s.cols["k"], s.cols["v"]]
+    be = q.ExprBuilder()
+    bfilter = be.op(abi.GT, abi.BOOL, be.col(tnames.index("b"), abi.I64), be.const(15, abi.I64))
+    jspec = queries.JoinSpec(types_of(bcols), types_of(pcols), [tnames.index("id")], [0], [tnames.index("id")],
+                             out=[(1, 0)], build_eb=be, build_filter=bfilter, join_type=abi.JOIN_LEFT_ANTI,
+                             build_is_left=1)
+    psel = s.cols["v"][0] > 4
+    rows = run_row_join(engine, jspec, bcols, pcols, rowsets(bcols, t.batches(), engine),
+                        rowsets(pcols, s.batches(), engine, psel), s.batches())
+    schema, want = expected(key)
+    assert sorted(r[0] for r in rows) == sorted(int(r[0]) for r in want)

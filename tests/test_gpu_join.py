@@ -225,3 +225,123 @@ def test_join_sum_partitioned_build_and_probe_40m(attr_lt):
     assert "join_part_scatter" in names and names.count("join_agg_probe") > 1, names
     want = O.join_aggregate(jspec, aspec, [q.HostRowSet(b)], [q.HostRowSet(p)])
     assert got == want
+
+
+def _typed_join_data(seed, nb, np_, nbatches):
+    rng = np.random.default_rng(seed)
+    bk = rng.integers(0, nb // 3, nb).astype(np.int64)             # ~3 build rows per key
+    bp = np.arange(nb, dtype=np.int64) * 7 + 1                      # payload names the build row
+    ba = rng.integers(0, 100, nb).astype(np.int32)
+    bvalid = rng.random(nb) > 0.04
+    pk = rng.integers(-50, nb // 3 + 50, np_).astype(np.int64)
+    pv = rng.integers(1, 1000, np_).astype(np.int64)
+    pvalid = rng.random(np_) > 0.04
+    psel = (rng.random(np_) > 0.1).astype(np.uint8)
+    b = [bk, bp, ba]
+    p = [pk, pv]
+    bounds = [(i * np_ // nbatches, (i + 1) * np_ // nbatches) for i in range(nbatches)]
+    return b, bvalid, p, pvalid, psel, bounds
+
+
+def _canonical(pairs, lo, pvalid):
+    """The oracle's pairs in the device's order.  The reference defers a
+    probe row whose seek meets a salt collision to a later key pass; the
+    device's bucket table has no salts, so within one probe batch the NULL-key
+    pads come first (as the collect pass emits them), then rows in row
+    order, each row's build rows in chain (build) order.  A stable sort by
+    (batch, not a NULL-key pad, row) maps one order onto the other without
+    reordering any row's own pairs."""
+    def key(lr):
+        left, right = lr
+        batch, row = left >> 32, left & 0xFFFFFFFF
+        pad = right < 0 and not pvalid[lo[batch] + row]
+        return (batch, 0 if pad else 1, row)
+    return sorted(pairs, key=key)
+
+
+@pytest.mark.parametrize("join_type,build_is_left", [(abi.JOIN_LEFT, 0), (abi.JOIN_RIGHT, 1)])
+def test_outer_join_pairs_against_oracle(join_type, build_is_left):
+    """LEFT (right side built) and RIGHT (left side built): every selected
+    probe row appears, unmatched and NULL-key rows once with NULL build
+    columns; duplicate keys, NULLs on both sides, a build predicate and a
+    probe selection, over three probe batches."""
+    b, bvalid, p, pvalid, psel, bounds = _typed_join_data(11, 30_000, 120_000, 3)
+    jspec, _ = queries.join_sum(60)
+    jspec = queries.JoinSpec(queries.JOIN_BUILD_COLUMNS_NULLABLE, queries.JOIN_PROBE_COLUMNS_NULLABLE, [0], [0],
+                             [1], out=[(0, 0), (0, 1), (1, 0)], build_eb=jspec.build_eb,
+                             build_filter=jspec.struct.build_filter, join_type=join_type,
+                             build_is_left=build_is_left)
+    brs = q.HostRowSet(b, masks=[bvalid, None, None])
+    prs = [q.HostRowSet([c[lo:hi] for c in p], masks=[pvalid[lo:hi], None], selection=psel[lo:hi])
+           for lo, hi in bounds]
+    want = O.row_join_typed(jspec, [brs], prs).tolist()
+    J = q.RowJoin(q.compile_row_join(jspec))
+    J.append(brs)
+    J.build()
+    got = []
+    for bi, rs in enumerate(prs):
+        n = J.probe(rs)
+        start = 0
+        while start < n:
+            k, out = J.materialize(rs, start, 16384)
+            vals, valid = q.read_rowset(out, [abi.I64, abi.I64, abi.I64])
+            for r in range(k):
+                got.append(tuple(int(vals[c][r]) if valid[c][r] else None for c in range(3)))
+            q.release(out)
+            start += k
+    J.release()
+    lo = [b0 for b0, _ in bounds]
+    exp = []
+    for left, right in _canonical(want, lo, pvalid):
+        g = lo[left >> 32] + (left & 0xFFFFFFFF)
+        fk = int(p[0][g]) if pvalid[g] else None
+        exp.append((fk, int(p[1][g]), None if right < 0 else int(b[1][right])))
+    assert len(got) == len(exp)
+    assert got == exp
+    assert any(r[2] is None and r[0] is None for r in got) and any(r[2] is None and r[0] is not None for r in got)
+
+
+@pytest.mark.parametrize("join_type", [abi.JOIN_LEFT_SEMI, abi.JOIN_LEFT_ANTI])
+def test_semi_anti_join_against_oracle(join_type):
+    """LEFT_SEMI / LEFT_ANTI building the left side: probes mark the build
+    rows they match across three probe batches; EMIT_BY_MARK lists the
+    marked (SEMI) or unmarked (ANTI) rows in build order, then an ANTI join's
+    NULL-key rows from its second arena; only build columns come out."""
+    b, bvalid, p, pvalid, psel, bounds = _typed_join_data(12, 30_000, 60_000, 3)
+    base, _ = queries.join_sum(60)
+    jspec = queries.JoinSpec(queries.JOIN_BUILD_COLUMNS_NULLABLE, queries.JOIN_PROBE_COLUMNS_NULLABLE, [0], [0],
+                             [1, 0], out=[(1, 0), (1, 1)], build_eb=base.build_eb,
+                             build_filter=base.struct.build_filter, join_type=join_type, build_is_left=1)
+    brs = q.HostRowSet(b, masks=[bvalid, None, None])
+    prs = [q.HostRowSet([c[lo:hi] for c in p], masks=[pvalid[lo:hi], None], selection=psel[lo:hi])
+           for lo, hi in bounds]
+    want = O.row_join_typed(jspec, [brs], prs).tolist()
+    J = q.RowJoin(q.compile_row_join(jspec), keeps_null_keys=join_type == abi.JOIN_LEFT_ANTI)
+    J.append(brs)
+    J.build()
+    for rs in prs:
+        assert J.probe(rs) == 0
+    n = J.emit_by_mark()
+    got = []
+    start = 0
+    while start < n:
+        k, out = J.materialize(None, start, 16384)
+        vals, valid = q.read_rowset(out, [abi.I64, abi.I64])
+        got.extend((int(vals[0][r]), int(vals[1][r]) if valid[1][r] else None) for r in range(k))
+        q.release(out)
+        start += k
+    J.release()
+    exp = [(int(b[1][br]), int(b[0][br]) if bvalid[br] else None) for _, br in want]
+    assert got == exp
+    if join_type == abi.JOIN_LEFT_ANTI:
+        assert any(v is None for _, v in got)   # NULL-key build rows are kept
+
+
+def test_typed_join_compile_rejects_unserved_shapes():
+    base, _ = queries.join_sum(20)
+    for jt, left in [(abi.JOIN_FULL, 0), (abi.JOIN_LEFT, 1), (abi.JOIN_RIGHT, 0), (abi.JOIN_LEFT_SEMI, 0),
+                     (abi.JOIN_RIGHT_ANTI, 1)]:
+        spec = queries.JoinSpec(queries.JOIN_BUILD_COLUMNS, queries.JOIN_PROBE_COLUMNS, [0], [0], [1],
+                                out=[(1, 0)], join_type=jt, build_is_left=left)
+        with pytest.raises(q.QdbError):
+            q.compile_row_join(spec)
