@@ -579,6 +579,27 @@ int64_t qdb_gpu_rf_probe_rowset(const qdb_gpu_program* hash_program, const qdb_r
                                 qdb_rowset* batch, uint8_t* output);
 
 /* ------------------------------------------------------------------------ */
+/* Hash shuffle (THashShuffleTask, qdb/scheduler/tasks/runtime_adapter.h:444; */
+/* its scatter of one batch, runtime_adapter.cpp:998-1112).                  */
+/* ------------------------------------------------------------------------ */
+
+/* Routes every selected row of `batch` to output routes[hash % n_routes],   */
+/* or hash % n_outputs when n_routes is 0; the hash is batch->Hash when set, */
+/* else the hash program's rh_hash of its key columns (qdb_gpu_hash), so a    */
+/* row lands where the engine's shuffle sends it.  outs[0, n_outputs)         */
+/* receive each output's rows in input order with every column of the        */
+/* program's schema (fixed-width types and one-byte strings; bit-packed BOOL */
+/* is rejected) and Hash pointing at their hashes.  Outputs are device-      */
+/* resident slices of shared buffers (validity as MaskBitOffset into a shared */
+/* bitmap), freed when the last is destroyed (qdb_gpu_release_rowsets).      */
+/* Returns the rows routed, < 0 on failure — a row whose route is outside    */
+/* [0, n_outputs) included, which the engine reports as a partition routed   */
+/* nowhere.  No reference counterpart as an entry: the engine's task does    */
+/* this on the host.                                                          */
+int64_t qdb_gpu_shuffle(const qdb_gpu_program* hash_program, qdb_rowset* batch, const int64_t* routes,
+                        int64_t n_routes, int64_t n_outputs, qdb_rowset* outs);
+
+/* ------------------------------------------------------------------------ */
 /* Aggregation without device allocation.                                   */
 /* ------------------------------------------------------------------------ */
 

@@ -1843,4 +1843,26 @@ void oracle_mt19937_64(uint64_t seed, int64_t n, uint64_t* out) {
     for (int64_t i = 0; i < n; ++i) out[i] = rng();
 }
 
+
+// THashShuffleTask::OutputOf (qdb/scheduler/tasks/runtime_adapter.cpp:998-1011)
+// over a batch: dest[r] = the output of selected row r, -1 for an unselected
+// row.  Returns -1 when a row's partition is routed nowhere, else 0.
+int64_t oracle_route(const uint64_t* hashes, const uint8_t* sel, int64_t n, const int64_t* routes,
+                     int64_t n_routes, int64_t n_outputs, int64_t* dest) {
+    for (int64_t r = 0; r < n; ++r) {
+        if (sel && !sel[r]) {
+            dest[r] = -1;
+            continue;
+        }
+        if (n_routes == 0) {
+            dest[r] = int64_t(hashes[r] % uint64_t(n_outputs));
+            continue;
+        }
+        const int64_t out = routes[hashes[r] % uint64_t(n_routes)];
+        if (out < 0 || out >= n_outputs) return -1;
+        dest[r] = out;
+    }
+    return 0;
+}
+
 }  // extern "C"

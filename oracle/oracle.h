@@ -130,6 +130,11 @@ int64_t oracle_rf_probe(const qdb_rf_data* data, const uint64_t* hashes, const u
 void oracle_rf_merge(uint64_t* target, const uint64_t* source, int64_t count);
 void oracle_mt19937_64(uint64_t seed, int64_t n, uint64_t* out);
 
+/* THashShuffleTask's routing of a batch: dest[r] = output of selected row r
+   (-1 unselected); -1 when a row's partition is routed nowhere. */
+int64_t oracle_route(const uint64_t* hashes, const uint8_t* sel, int64_t n, const int64_t* routes,
+                     int64_t n_routes, int64_t n_outputs, int64_t* dest);
+
 #ifdef __cplusplus
 }
 #endif

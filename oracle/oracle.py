@@ -58,6 +58,7 @@ def lib() -> C.CDLL:
             "oracle_rf_probe": (C.c_int64, [C.POINTER(abi.RfData), P, P, P, C.c_int64]),
             "oracle_rf_merge": (None, [P, P, C.c_int64]),
             "oracle_mt19937_64": (None, [C.c_uint64, C.c_int64, P]),
+            "oracle_route": (C.c_int64, [P, P, C.c_int64, P, C.c_int64, C.c_int64, P]),
             "oracle_join_aggregate": (C.c_int, [C.POINTER(abi.RowJoinSpec), C.POINTER(abi.AggregateSpec),
                                                 C.POINTER(abi.RowSet), C.c_int32, C.POINTER(abi.RowSet), C.c_int32,
                                                 C.c_int32, C.POINTER(OracleTable), C.c_char_p, C.c_size_t]),
@@ -253,3 +254,69 @@ def sorted_row_indices(k1: np.ndarray, k2: np.ndarray, threads: int) -> np.ndarr
     out = np.empty(n, np.int64)
     lib().oracle_bench_sort(k1.ctypes.data, k2.ctypes.data, n, threads, out.ctypes.data)
     return out
+
+
+class HostStorage:
+    """The runtime filter's storage protocol over host arrays, with the
+    oracle's rf_build / rf_publish / rf_probe / rf_merge: the same host logic
+    (qumirdb_b200.rfilter) then drives the CPU restatement."""
+
+    def alloc(self, nbytes: int) -> np.ndarray:
+        return np.zeros(max(8, nbytes), dtype=np.uint8)
+
+    @staticmethod
+    def ptr(buf) -> int:
+        return buf.ctypes.data
+
+    def zero(self, buf, nbytes: int) -> None:
+        buf[:nbytes] = 0
+
+    def copy(self, dst, src, nbytes: int) -> None:
+        dst[:nbytes] = src[:nbytes]
+
+    def read_u64(self, buf, n: int) -> np.ndarray:
+        return buf[: 8 * n].view(np.uint64).copy()
+
+    def upload(self, arr: np.ndarray) -> np.ndarray:
+        buf = self.alloc(arr.nbytes)
+        buf[: arr.nbytes] = np.ascontiguousarray(arr).view(np.uint8)
+        return buf
+
+    def read_u8(self, buf, n: int) -> np.ndarray:
+        return buf[:n].copy()
+
+    def build(self, state, hashes, sel, n) -> int:
+        return lib().oracle_rf_build(C.byref(state), hashes, sel, n)
+
+    def publish(self, state, partials, n) -> int:
+        return lib().oracle_rf_publish(C.byref(state), partials, n)
+
+    def probe(self, data, hashes, sel, out, n) -> int:
+        return lib().oracle_rf_probe(C.byref(data), hashes, sel, out, n)
+
+    def merge(self, target, source, n) -> None:
+        lib().oracle_rf_merge(target, source, n)
+
+    def error(self) -> str:
+        return "oracle"
+
+
+def mt19937_64(seed: int, n: int) -> np.ndarray:
+    """std::mt19937_64(seed)'s first n outputs."""
+    out = np.zeros(max(1, n), dtype=np.uint64)
+    lib().oracle_mt19937_64(seed, n, out.ctypes.data)
+    return out[:n]
+
+
+def route(hashes: np.ndarray, selection, routes, n_outputs: int) -> np.ndarray | None:
+    """The shuffle's output per row (-1: unselected); None when a row's
+    partition is routed nowhere."""
+    h = np.ascontiguousarray(hashes, dtype=np.uint64)
+    n = len(h)
+    dest = np.zeros(max(1, n), dtype=np.int64)
+    sel = None if selection is None else np.ascontiguousarray(selection, dtype=np.uint8)
+    r = None if not routes else np.ascontiguousarray(routes, dtype=np.int64)
+    rc = lib().oracle_route(h.ctypes.data, None if sel is None else sel.ctypes.data, n,
+                            None if r is None else r.ctypes.data, 0 if r is None else len(r), n_outputs,
+                            dest.ctypes.data)
+    return None if rc < 0 else dest[:n]

@@ -292,8 +292,9 @@ def read_rowset(rs: abi.RowSet, types, on_device: bool = False) -> tuple[list[np
             vals = raw.view(dt)
         values.append(vals)
         if col.Mask and n:
-            bits = _fetch(col.Mask, (n + 7) // 8, on_device)
-            valid.append(np.unpackbits(bits, bitorder="little")[:n].astype(bool))
+            off = col.MaskBitOffset
+            bits = _fetch(col.Mask, (off + n + 7) // 8, on_device)
+            valid.append(np.unpackbits(bits, bitorder="little")[off:off + n].astype(bool))
         else:
             valid.append(np.ones(n, dtype=bool))
     return values, valid
@@ -565,6 +566,36 @@ class RowJoin:
             self.release()
         except Exception:
             pass
+
+
+def compile_hash(columns, key_columns) -> Program:
+    """The join / shuffle key hash program (TKernelCompiler::CompileJoinHash):
+    rh_hash of the key columns, as qdb_gpu_hash writes it."""
+    ct = coltypes(columns)
+    kc = i32s(key_columns)
+    err = C.create_string_buffer(512)
+    h = lib().qdb_gpu_compile_hash(len(columns), ct, len(key_columns), kc, err, 512)
+    if not h:
+        raise QdbError(err.value.decode())
+    return Program(h, keep=(ct, kc))
+
+
+def hash_rows(prog: Program, batch, out_ptr) -> None:
+    """qdb_gpu_hash: one uint64 per selected row of `batch` into out_ptr
+    (host or device memory)."""
+    if not lib().qdb_gpu_hash(prog.handle, batch.ptr, out_ptr):
+        raise QdbError(f"hash failed: {last_error()}")
+
+
+def shuffle(hash_prog: Program, batch, n_outputs: int, routes=None) -> RowSets:
+    """qdb_gpu_shuffle: the batch's selected rows split by key hash into
+    n_outputs device-resident row sets (input order kept in each)."""
+    outs = (abi.RowSet * max(1, n_outputs))()
+    r = None if not routes else (C.c_int64 * len(routes))(*routes)
+    n = lib().qdb_gpu_shuffle(hash_prog.handle, batch.ptr, r, 0 if r is None else len(routes), n_outputs, outs)
+    if n < 0:
+        raise QdbError(f"shuffle failed: {last_error()}")
+    return RowSets(outs, n_outputs)
 
 
 def compile_sort(spec) -> Program:

@@ -163,6 +163,7 @@ SIGNATURES = {
     "qdb_gpu_rf_probe": (CI64, [C.POINTER(RfData), P, P, P, CI64, CI64, P, P]),
     "qdb_gpu_rf_merge": (CI64, [P, P, CI64]),
     "qdb_gpu_rf_probe_rowset": (CI64, [P, C.POINTER(RfData), PRS, P]),
+    "qdb_gpu_shuffle": (CI64, [P, PRS, P, CI64, CI64, PRS]),
     "qdb_gpu_init": (C.c_int, [C.c_int]),
     "qdb_gpu_last_error": (C.c_char_p, []),
     "qdb_gpu_set_stream": (None, [P]),

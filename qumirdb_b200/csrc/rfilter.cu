@@ -479,7 +479,9 @@ int64_t qdb_gpu_rf_build(qdb_rf_build_state* st, const uint64_t* hashes, const u
         SetErr("rf_build: bad arguments");
         return -1;
     }
-    if (!DeviceArgs({hashes, selection, st->Keys, st->SetSlots, st->Bloom}, "rf_build")) return -1;
+    // A batch of no rows may point one past its array (the caller's next row).
+    if (count > 0 && !DeviceArgs({hashes, selection}, "rf_build")) return -1;
+    if (!DeviceArgs({st->Keys, st->SetSlots, st->Bloom}, "rf_build")) return -1;
     cudaStream_t s = CurStream();
     CallScratch sc(s);
     const int64_t max_keys = st->MaxKeys;
@@ -534,7 +536,8 @@ int64_t qdb_gpu_rf_publish(qdb_rf_publish_state* st, const qdb_rf_partial* parti
     }
     if (!DeviceArgs({st->Table, st->Bloom}, "rf_publish")) return -1;
     for (int64_t i = 0; i < n; ++i) {
-        if (!DeviceArgs({partials[i].Keys, partials[i].Bloom}, "rf_publish")) return -1;
+        if (partials[i].KeyCount > 0 && !DeviceArgs({partials[i].Keys}, "rf_publish")) return -1;
+        if (partials[i].BloomWords > 0 && !DeviceArgs({partials[i].Bloom}, "rf_publish")) return -1;
     }
     cudaStream_t s = CurStream();
     CallScratch sc(s);
@@ -608,8 +611,8 @@ int64_t qdb_gpu_rf_probe(const qdb_rf_data* data, const uint64_t* hashes, const 
         SetErr("rf_probe: bad arguments (Kind must be 1 exact or 2 Bloom)");
         return -1;
     }
-    if (!DeviceArgs({hashes, selection, output, data->Words}, "rf_probe")) return -1;
     if (count == 0) return 0;
+    if (!DeviceArgs({hashes, selection, output, data->Words}, "rf_probe")) return -1;
     cudaStream_t s = CurStream();
     CallScratch sc(s);
     auto* kept = sc.Get<unsigned long long>(1);
@@ -631,8 +634,8 @@ int64_t qdb_gpu_rf_merge(uint64_t* target, const uint64_t* source, int64_t count
         SetErr("rf_merge: bad arguments");
         return -1;
     }
-    if (!DeviceArgs({target, source}, "rf_merge")) return -1;
     if (count == 0) return 0;
+    if (!DeviceArgs({target, source}, "rf_merge")) return -1;
     cudaStream_t s = CurStream();
     RfOrKernel<<<Grid(count), 256, 0, s>>>(target, source, count);
     CountLaunch();

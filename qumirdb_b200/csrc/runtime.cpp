@@ -774,7 +774,10 @@ void Fill(char* err, size_t len, const char* msg) {
     t_error = msg;
 }
 
-// The struct rh_hash of a hash program's key slots over nrows rows.
+}  // namespace
+
+namespace qdb {
+
 void HashArgs(const qdb_gpu_program* prog, const AggPlan& plan, int64_t nrows, ExprArgs& a) {
     a.plan = &plan;
     a.nrows = nrows;
@@ -786,7 +789,7 @@ void HashArgs(const qdb_gpu_program* prog, const AggPlan& plan, int64_t nrows, E
     }
 }
 
-}  // namespace
+}  // namespace qdb
 
 extern "C" {
 

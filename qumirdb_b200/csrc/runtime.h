@@ -145,5 +145,12 @@ struct qdb_gpu_program {
 };
 
 namespace qdb {
+// The struct rh_hash of a hash program's key slots over nrows rows (the
+// plan's columns resolved for the batch).
+void HashArgs(const qdb_gpu_program* prog, const AggPlan& plan, int64_t nrows, ExprArgs& a);
+}  // namespace qdb
+
+
+namespace qdb {
 enum ProgramKind { PK_AGG = 1, PK_FILTER, PK_PROJECT, PK_HASH, PK_JOIN, PK_JOIN_AGG, PK_SORT };
 }
