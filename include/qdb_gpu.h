@@ -600,6 +600,49 @@ int64_t qdb_gpu_shuffle(const qdb_gpu_program* hash_program, qdb_rowset* batch, 
                         int64_t n_routes, int64_t n_outputs, qdb_rowset* outs);
 
 /* ------------------------------------------------------------------------ */
+/* Device column cache: host scan batches (TParquetSource::Next,             */
+/* qdb/io/parquet/source.h:89, 2^18-row batches, source.cpp:333) staged into  */
+/* HBM through pinned buffers and kept resident across queries.  No         */
+/* reference counterpart: the engine's kernels read host batches.           */
+/* ------------------------------------------------------------------------ */
+
+typedef struct qdb_gpu_column_cache qdb_gpu_column_cache;
+
+typedef struct qdb_gpu_cache_stats {
+    int64_t hits;             /* columns served from HBM                     */
+    int64_t misses;           /* columns copied in                           */
+    int64_t evictions;        /* columns dropped to stay within the budget   */
+    int64_t resident_bytes;   /* bytes of cached columns in HBM              */
+    int64_t pinned_bytes;     /* bytes of entries held by live row sets      */
+    int64_t h2d_bytes;        /* bytes copied host -> device so far          */
+    int64_t entries;          /* cached columns                              */
+} qdb_gpu_cache_stats;
+
+/* A cache holding at most budget_bytes of columns in HBM, staging copies   */
+/* from pageable host memory through two pinned buffers of staging_bytes    */
+/* each (0 picks 8 MiB), so that filling one overlaps the copy of the other. */
+/* Copies run on the stream current at creation.  NULL on failure.          */
+qdb_gpu_column_cache* qdb_gpu_cache_create(size_t budget_bytes, size_t staging_bytes);
+/* Frees every cached column; row sets it handed out must be destroyed first. */
+void qdb_gpu_cache_destroy(qdb_gpu_column_cache* cache);
+/* A device row set of batch `batch_index` of source `source_id`: columns    */
+/* columns[0, n) of `host` (typed by types[]) in that order.  A column       */
+/* already resident under (source, batch, column) is used in place; the     */
+/* others are copied in (data, and the validity bitmap when the host column  */
+/* has one) and kept, the least recently used unpinned columns evicted to    */
+/* stay within the budget.  The host batch's Selection is copied per call    */
+/* and not cached.  The entries stay pinned until out->Destroy(out).         */
+/* Returns 0, < 0 on failure (a batch larger than the budget included).      */
+/* Re-entrant across host threads.                                          */
+int64_t qdb_gpu_cache_get(qdb_gpu_column_cache* cache, uint64_t source_id, int64_t batch_index,
+                          const qdb_rowset* host, const qdb_column_type* types, const int32_t* columns,
+                          int32_t n, qdb_rowset* out);
+/* Drops the unpinned columns of one source (its file changed); returns how */
+/* many were dropped.                                                       */
+int64_t qdb_gpu_cache_invalidate(qdb_gpu_column_cache* cache, uint64_t source_id);
+void qdb_gpu_cache_get_stats(qdb_gpu_column_cache* cache, qdb_gpu_cache_stats* stats);
+
+/* ------------------------------------------------------------------------ */
 /* Aggregation without device allocation.                                   */
 /* ------------------------------------------------------------------------ */
 

@@ -598,6 +598,62 @@ def shuffle(hash_prog: Program, batch, n_outputs: int, routes=None) -> RowSets:
     return RowSets(outs, n_outputs)
 
 
+class CachedRowSet:
+    """A device row set handed out by the column cache; its columns stay
+    pinned in the cache until release()."""
+
+    def __init__(self, rs: abi.RowSet, keep):
+        self.rs = rs
+        self._keep = keep
+
+    @property
+    def ptr(self):
+        return C.byref(self.rs)
+
+    def release(self) -> None:
+        release(self.rs)
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+class ColumnCache:
+    """Device column cache between scan sources and the kernels: batches of
+    host columns staged into HBM and kept resident across queries under a
+    byte budget (qdb_gpu_cache_*)."""
+
+    def __init__(self, budget_bytes: int, staging_bytes: int = 0):
+        _ensure_init()
+        self.handle = lib().qdb_gpu_cache_create(budget_bytes, staging_bytes)
+        if not self.handle:
+            raise QdbError(f"column cache creation failed: {last_error()}")
+
+    def get(self, source_id: int, batch_index: int, host, types, columns=None) -> CachedRowSet:
+        ct = coltypes(types)
+        cols = list(range(len(types))) if columns is None else list(columns)
+        ci = i32s(cols)
+        out = abi.RowSet()
+        if lib().qdb_gpu_cache_get(self.handle, source_id, batch_index, host.ptr, ct, ci, len(cols), C.byref(out)) < 0:
+            raise QdbError(f"column cache get failed: {last_error()}")
+        return CachedRowSet(out, (ct, ci))
+
+    def invalidate(self, source_id: int) -> int:
+        return lib().qdb_gpu_cache_invalidate(self.handle, source_id)
+
+    def stats(self) -> dict:
+        st = abi.CacheStats()
+        lib().qdb_gpu_cache_get_stats(self.handle, C.byref(st))
+        return {f: getattr(st, f) for f, _ in abi.CacheStats._fields_}
+
+    def close(self) -> None:
+        if self.handle:
+            lib().qdb_gpu_cache_destroy(self.handle)
+            self.handle = None
+
+
 def compile_sort(spec) -> Program:
     err = C.create_string_buffer(512)
     h = lib().qdb_gpu_compile_sort(C.byref(spec.struct), err, 512)

@@ -121,6 +121,12 @@ class RfData(C.Structure):
     _fields_ = [("Kind", C.c_int64), ("Words", C.c_void_p), ("WordCount", C.c_int64)]
 
 
+class CacheStats(C.Structure):
+    """qdb_gpu_cache_stats."""
+    _fields_ = [("hits", C.c_int64), ("misses", C.c_int64), ("evictions", C.c_int64), ("resident_bytes", C.c_int64),
+                ("pinned_bytes", C.c_int64), ("h2d_bytes", C.c_int64), ("entries", C.c_int64)]
+
+
 class KernelTime(C.Structure):
     _fields_ = [("name", C.c_char * 48), ("ms", C.c_double), ("units", C.c_int64)]
 
@@ -164,6 +170,11 @@ SIGNATURES = {
     "qdb_gpu_rf_merge": (CI64, [P, P, CI64]),
     "qdb_gpu_rf_probe_rowset": (CI64, [P, C.POINTER(RfData), PRS, P]),
     "qdb_gpu_shuffle": (CI64, [P, PRS, P, CI64, CI64, PRS]),
+    "qdb_gpu_cache_create": (P, [SZ, SZ]),
+    "qdb_gpu_cache_destroy": (None, [P]),
+    "qdb_gpu_cache_get": (CI64, [P, CU64, CI64, PRS, C.POINTER(ColumnType), C.POINTER(CI32), CI32, PRS]),
+    "qdb_gpu_cache_invalidate": (CI64, [P, CU64]),
+    "qdb_gpu_cache_get_stats": (None, [P, C.POINTER(CacheStats)]),
     "qdb_gpu_init": (C.c_int, [C.c_int]),
     "qdb_gpu_last_error": (C.c_char_p, []),
     "qdb_gpu_set_stream": (None, [P]),
