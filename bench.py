@@ -43,9 +43,10 @@ LINEITEM_ROWS = 6_001_215
 ZIPF_ROWS = 200_000_000
 ZIPF_PARTS = 4096
 SERVE_TABLES = 16
+JOIN_PARTS = 256
 SERVE_BUDGET = 150 * 10**9
 SERVE_WORKERS = 3
-SERVE_COALESCE_ROWS = 0     # rows up to which waiting Zipf aggregations coalesce (0: off)
+SERVE_COALESCE_ROWS = 8 << 20   # rows up to which waiting Zipf aggregations coalesce (0: off)
 ZIPF_DISTINCT = 20_000_000
 SORT_ROWS = 300_000_000
 METRIC = "rows/s & HBM GB/s vs peak per operator; mixed-stream queries/s and p50/p99"
@@ -344,6 +345,107 @@ def zipf_batched_operator(q, peak):
             "l2": "inputs larger than L2", "gpu_launches": launches / 3, "autotune": q.autotune_info()}
 
 
+def join_batched_operator(q, peak, w):
+    """Config 1's join as the engine's partitioned plan: both sides split by
+    the join key's hash into JOIN_PARTS partitions with the device shuffle
+    (input preparation, untimed), then per step every partition appends its
+    build rows, all tables are built in one batched call and all probes run
+    in one persistent launch; SUM/COUNT summed over the partitions equal the
+    single join's."""
+    from qumirdb_b200 import abi
+    hprog_b = q.compile_hash([(abi.I64,), (abi.I64,), (abi.I32,)], [0])
+    hprog_p = q.compile_hash([(abi.I64,), (abi.I64,)], [0])
+    bparts = q.shuffle(hprog_b, w.dev_build, JOIN_PARTS)
+    pparts = q.shuffle(hprog_p, w.dev_probe, JOIN_PARTS)
+
+    class View:
+        def __init__(self, rs):
+            self.rs = rs
+            self.ptr = C.byref(rs)
+
+    bviews = [View(bparts[i]) for i in range(JOIN_PARTS)]
+    pviews = [View(pparts[i]) for i in range(JOIN_PARTS)]
+    res = []
+
+    def step():
+        jb = q.RowJoinBatch(w.prog, JOIN_PARTS)
+        for i in range(JOIN_PARTS):
+            jb.append(i, bviews[i])
+        jb.build()
+        jb.probe_aggregate(pviews)
+        s = c = 0
+        for out in jb.finish():
+            vals, _ = q.read_rowset(out, [abi.I64, abi.I64])
+            s += int(vals[0][0])
+            c += int(vals[1][0])
+            q.release(out)
+        jb.release()
+        res.append((s, c))
+
+    ms, _, launches, _ = timed(q, step, 3, 2)
+    _, _, _, kernels = timed(q, step, 2, 0, profile=True)
+    kms, _ = kernel_avg(kernels, "join_agg_probe_batch", 2)
+    bms, _ = kernel_avg(kernels, "join_build_batch", 2)
+    alg = PROBE_ROWS * 16
+    bparts.release()
+    pparts.release()
+    return {"workload": f"the 2M x 120M join split by key hash into {JOIN_PARTS} partitions (device shuffle), "
+                        "per-partition appends, one batched build, one batched probe launch",
+            "rows_per_s": w.rows / (ms / 1e3), "ms_per_query": ms, "result": list(res[-1]),
+            "kernel": "join_agg_probe_batch", "kernel_ms": kms, "build_batch_ms": bms,
+            "frac_of_measured_hbm": (alg / (kms / 1e3) / 1e9) / peak if kms else None,
+            "gpu_launches": launches / 3}
+
+
+def serving_cpu_arm(tables, sample_rows: int = 4 << 20) -> dict:
+    """The CPU arm of the serving stream: each table's query through the CPU
+    restatement's threaded plans on all host threads, timed on a prefix of
+    at most `sample_rows` rows of the same seeded table (the generators are
+    deterministic per row) and scaled to the table's rows (these plans are
+    linear in rows); queries/s is the table count over the summed service
+    times (one query at a time, the engine's executor shape), p50/p99 the
+    service times'."""
+    from oracle import oracle as O
+    from qumirdb_b200 import HostRowSet, queries
+    threads = os.cpu_count() or 1
+    secs = []
+    for t in tables:
+        m = min(t.rows, sample_rows)
+        if t.template == "lineitem":
+            cols = [np.empty(m, np.int64), np.empty(m, np.int64), np.empty(m, np.int64), np.empty(m, np.int64),
+                    np.empty(m, np.uint8), np.empty(m, np.uint8), np.empty(m, np.int32)]
+            O.lib().qdb_gen_lineitem(t.seed, m, *[c.ctypes.data for c in cols])
+            spec = queries.lineitem_agg(t.cutoff)
+            sec = O.lib().oracle_bench_aggregate(C.byref(spec.struct), HostRowSet(cols).ptr, threads, None)
+        elif t.template == "zipf":
+            cols = [np.empty(m, np.int64), np.empty(m, np.int64), np.empty(m, np.float64)]
+            O.lib().qdb_gen_zipf(t.seed, m, max(1, t.rows // 10), 1.1, *[c.ctypes.data for c in cols])
+            spec = queries.zipf_agg(expected_groups=max(1, m // 10))
+            sec = O.lib().oracle_bench_aggregate(C.byref(spec.struct), HostRowSet(cols).ptr, threads, None)
+        elif t.template == "join":
+            nb = max(1, t.rows // 60)
+            b = [np.empty(nb, np.int64), np.empty(nb, np.int64), np.empty(nb, np.int32)]
+            p = [np.empty(m, np.int64), np.empty(m, np.int64)]
+            O.lib().qdb_gen_join(t.seed, nb, m, nb + nb // 4, *[x.ctypes.data for x in b + p])
+            s_, c_ = C.c_int64(), C.c_int64()
+            sec = O.lib().oracle_bench_join_sum(b[0].ctypes.data, b[1].ctypes.data, b[2].ctypes.data, nb, 20,
+                                                p[0].ctypes.data, p[1].ctypes.data, m, threads, C.byref(s_),
+                                                C.byref(c_))
+        else:
+            k1, k2 = np.empty(m, np.int64), np.empty(m, np.int32)
+            O.lib().qdb_gen_sort(t.seed, m, k1.ctypes.data, k2.ctypes.data, None)
+            spec = queries.sort_k1_desc_k2()
+            rs = HostRowSet([k1, k2, np.arange(m, dtype=np.int64)])
+            t0 = time.perf_counter()
+            O.top_k(spec, [rs], np.arange(m, dtype=np.int64), min(1000, m))
+            sec = time.perf_counter() - t0
+        secs.append(sec * t.rows / m)
+    arr = np.array(secs)
+    return {"queries_per_s": len(arr) / arr.sum(), "p50_ms": float(np.percentile(arr, 50)) * 1e3,
+            "p99_ms": float(np.percentile(arr, 99)) * 1e3, "cores": threads,
+            "sample": f"each table's query on a prefix of at most {sample_rows:,} rows, scaled to its rows"}
+
+
 def serving_operator(q):
     """The mixed serving stream: Poisson arrivals of queries drawn uniformly
     from the four templates, each over its own resident seeded tables of
@@ -399,6 +501,11 @@ def serving_operator(q):
         out[mode] = {k: best[k] for k in ("rate", "queries_per_s", "p50_ms", "p99_ms")}
     srv.close()
     out["serving_over_plain_qps"] = out["serving"]["queries_per_s"] / out["plain"]["queries_per_s"]
+    best = max((r for r in out["sweeps"]["serving"] if r["sustained"]), key=lambda r: r["queries_per_s"],
+               default=out["sweeps"]["serving"][0])
+    out["coalesced_queries"] = best.get("coalesced_queries", 0)
+    out["batched_launches"] = best.get("batched_launches", 0)
+    out["cpu"] = serving_cpu_arm(tables)
     return out
 
 
@@ -686,7 +793,7 @@ def compact_operators(ops: dict) -> dict:
         return None if x is None else float(f"{x:.{nd}g}")
 
     out = {}
-    for name in ("lineitem", "zipf", "zipf_batched", "sort"):
+    for name in ("lineitem", "zipf", "zipf_batched", "join_batched", "sort"):
         o = ops.get(name)
         if not o:
             continue
@@ -704,6 +811,9 @@ def compact_operators(ops: dict) -> dict:
             c["groups"] = o.get("groups")
         if "finalize_ms" in o:
             c["finalize_ms"] = r(o.get("finalize_ms"))
+        if "build_batch_ms" in o:
+            c["build_batch_ms"] = r(o.get("build_batch_ms"))
+            c["result"] = o.get("result")
         cb = o.get("cpu_baseline")
         if cb:
             c["cpu_baseline"] = {"rows_per_s": r(cb["value"]), "cores": cb["cores"], "kind": cb["kind"]}
@@ -836,7 +946,8 @@ def main() -> None:
         ops = {}
         try:
             ops = {"lineitem": lineitem_operator(q, peak), "zipf": zipf_operator(q, peak),
-                   "zipf_batched": zipf_batched_operator(q, peak), "sort": sort_operator(q, peak),
+                   "zipf_batched": zipf_batched_operator(q, peak), "join_batched": join_batched_operator(q, peak, w),
+                   "sort": sort_operator(q, peak),
                    "serving": serving_operator(q)}
             if not args.no_cpu_baseline:
                 ops["sort"]["cpu_baseline"] = {

@@ -403,6 +403,23 @@ int64_t qdb_gpu_join_aggregate_probe(const qdb_gpu_program* program,
                                      void* arena, void* table, void* ht,
                                      qdb_rowset* batch);
 
+/* Many joins of one program at once (the per-partition row tables of a     */
+/* partitioned join, qdb/exec/row_join_exec.cpp:93-220, or the joins of many  */
+/* queries of one template).  No reference counterpart as entries.           */
+/* jr_build_batch: Build (jr_dispatch op 2) for n appended arenas in one     */
+/* launch that clears every table and one that inserts every arena's rows;   */
+/* these tables carry no Bloom filter or direct index (a table larger than   */
+/* L2 still gets its own partitioned build).  Returns false on failure.      */
+bool qdb_gpu_jr_build_batch(const qdb_gpu_program* program, void* const* arenas, void* const* tables, int64_t n);
+/* join_aggregate_probe_batch: qdb_gpu_join_aggregate_probe of batches[i]    */
+/* into hts[i] for every i, in one persistent launch when the program has   */
+/* the keyless join-sum shape (COUNT / SUM of products of the build payload */
+/* and one probe column) and no batch has a selection; one by one otherwise. */
+/* Returns the total matched pairs, < 0 on failure.                          */
+int64_t qdb_gpu_join_aggregate_probe_batch(const qdb_gpu_program* program, void* const* arenas,
+                                           void* const* tables, void* const* hts, qdb_rowset* const* batches,
+                                           int64_t n);
+
 /* qdb_sort_run (qdb/kernel/compiler.h:522-541, compiler.cpp:1165-1218).     */
 /* With do_sort, sorts the n packed row ids (batch << 32 | row) in place by  */
 /* the keys, stable in input order; then materializes [start, start+limit)   */

@@ -654,6 +654,46 @@ class ColumnCache:
             self.handle = None
 
 
+class RowJoinBatch:
+    """Many fused join-aggregates of one program (the partitions of a
+    partitioned join, or the joins of many queries of one template): each
+    join appends its own build rows, then every table is built in one batched
+    call and every probe folded in one persistent launch."""
+
+    def __init__(self, prog: Program, n: int):
+        self.prog = prog
+        self.n = n
+        self.joins = [RowJoin(prog) for _ in range(n)]
+        self.aggs = [Aggregate(prog) for _ in range(n)]
+
+    def _ptrs(self, bufs):
+        return (C.c_void_p * max(1, self.n))(*[C.cast(b, C.c_void_p) for b in bufs])
+
+    def append(self, i: int, batch) -> None:
+        self.joins[i].append(batch)
+
+    def build(self) -> None:
+        if not lib().qdb_gpu_jr_build_batch(self.prog.handle, self._ptrs([j.arena for j in self.joins]),
+                                            self._ptrs([j.table for j in self.joins]), self.n):
+            raise QdbError(f"batched join build failed: {last_error()}")
+
+    def probe_aggregate(self, batches) -> int:
+        rs = RowSetPointers(batches)
+        m = lib().qdb_gpu_join_aggregate_probe_batch(self.prog.handle, self._ptrs([j.arena for j in self.joins]),
+                                                      self._ptrs([j.table for j in self.joins]),
+                                                      self._ptrs([a.ht for a in self.aggs]), rs.arr, self.n)
+        if m < 0:
+            raise QdbError(f"batched join probe failed: {last_error()}")
+        return m
+
+    def finish(self) -> list[abi.RowSet]:
+        return [a.finish() for a in self.aggs]
+
+    def release(self) -> None:
+        for j in self.joins:
+            j.release()
+
+
 def compile_sort(spec) -> Program:
     err = C.create_string_buffer(512)
     h = lib().qdb_gpu_compile_sort(C.byref(spec.struct), err, 512)

@@ -559,6 +559,8 @@ bool JoinSumPartitioned(const JoinSumShape& shape, const JTableDev& jt, int64_t 
 
 }  // namespace
 
+bool JoinSumProbeColumn(const JoinSumShape& shape, const int64_t*& vcol) { return SingleProbeColumn(shape, vcol); }
+
 void JoinSumRun(const JoinSumShape& shape, const JTableDev& jt, int64_t nrows, uint64_t* group_states,
                 AggCounters* counters, cudaStream_t s) {
     if (nrows == 0) return;
@@ -571,6 +573,99 @@ void JoinSumRun(const JoinSumShape& shape, const JTableDev& jt, int64_t nrows, u
         return;
     }
     JoinSumLaunch(shape, jt, nrows, group_states, counters, s);
+}
+
+// ---------------------------------------------------------------------------
+// Batched join-sum probe: many small joins of one program (the partitions of
+// a partitioned join, or the joins of many queries of one template) in one
+// persistent launch.  A warp pulls a work item (join, range of at most
+// kJsBatchItemRows probe rows), probes one row per lane per step against that
+// join's bucket table (left in L2: small tables, no staging or Bloom filter),
+// and ends the item with a warp reduction and one atomic add per state word.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct JsBatchLaunch {
+    JoinSumShape S;
+    const JsBatchJoin* joins;
+    const JoinBatchItem* items;
+    int64_t nitems;
+    unsigned* next;
+};
+
+__device__ __forceinline__ uint64_t JsBatchTerm(const JsState& st, uint64_t pay, int64_t sv) {
+    uint64_t v = 1;
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+        if (f >= st.nf) break;
+        const JsFactor& jf = st.f[f];
+        v *= uint64_t(jf.c) + uint64_t(jf.d) * (jf.side == 1 ? pay : uint64_t(sv));
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(256) JoinSumBatchKernel(const __grid_constant__ JsBatchLaunch L) {
+    const int lane = LaneId();
+    for (;;) {
+        unsigned it = 0;
+        if (lane == 0) it = atomicAdd(L.next, 1u);
+        it = __shfl_sync(kFull, it, 0);
+        if (int64_t(it) >= L.nitems) return;
+        const JoinBatchItem item = L.items[it];
+        const JsBatchJoin& J = L.joins[item.join];
+        const JTableDev& jt = J.jt;
+        const int64_t nspecial = int64_t(*jt.nspecial);
+        uint64_t v[kJsMaxStates];
+#pragma unroll
+        for (int s = 0; s < kJsMaxStates; ++s) v[s] = 0;
+        unsigned long long matched = 0;
+        auto fold = [&](uint64_t pay, int64_t sv) {
+            ++matched;
+#pragma unroll
+            for (int s = 0; s < kJsMaxStates; ++s) {
+                if (s < L.S.nstates) v[s] += JsBatchTerm(L.S.states[s], pay, sv);
+            }
+        };
+        for (int64_t r = item.lo + lane; r < item.hi; r += 32) {
+            const uint64_t key = uint64_t(__ldcs(&J.key[r]));
+            const int64_t sv = J.vcol ? __ldcs(&J.vcol[r]) : 0;
+            if (key == kEmptyKey) {
+                for (int64_t q = 0; q < nspecial; ++q) fold(uint64_t(jt.special_rows[2 * q + 1]), sv);
+                continue;
+            }
+            const uint64_t b = Fmix64(key) & jt.bmask;
+            VisitMatches(jt, key, b, BucketKeys(jt, b), [&](uint64_t, uint64_t bk, int jj) {
+                fold(L.S.need_pay ? jt.buckets[4 * bk + 2 + jj] : 0, sv);
+            });
+        }
+#pragma unroll
+        for (int s = 0; s < kJsMaxStates; ++s) {
+            if (s >= L.S.nstates) break;
+            const uint64_t t = WarpSumU64(v[s]);
+            if (lane == 0 && t) atomicAdd(reinterpret_cast<unsigned long long*>(J.states + L.S.states[s].word), t);
+        }
+        const uint64_t m = WarpSumU64(matched);
+        if (lane == 0 && m) atomicAdd(J.matched, (unsigned long long)m);
+    }
+}
+
+}  // namespace
+
+void JoinSumBatchRun(const JoinSumShape& shape, const JsBatchJoin* joins, const JoinBatchItem* items,
+                     int64_t nitems, unsigned* next, cudaStream_t s) {
+    if (nitems == 0) return;
+    JsBatchLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    L.S = shape;
+    L.joins = joins;
+    L.items = items;
+    L.nitems = nitems;
+    L.next = next;
+    const int warps = int(std::min<int64_t>(nitems, int64_t(DeviceSMs()) * 64));
+    ProfileBegin(s, "join_agg_probe_batch", nitems);
+    JoinSumBatchKernel<<<(warps + 7) / 8, 256, 0, s>>>(L);
+    ProfileEnd(s);
+    CountLaunch();
 }
 
 }  // namespace qdb

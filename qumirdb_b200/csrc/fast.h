@@ -48,4 +48,23 @@ bool MatchFast(const AggPlan& plan, FastPlan& F);
 void JoinSumRun(const JoinSumShape& shape, const JTableDev& jt, int64_t nrows, uint64_t* group_states,
                 AggCounters* counters, cudaStream_t s);
 
+// The probe column every probe factor reads (nullptr: none); false when the
+// factors read two probe columns or a build column through the arena row.
+bool JoinSumProbeColumn(const JoinSumShape& shape, const int64_t*& vcol);
+
+// One join of a batched join-sum probe.
+struct JsBatchJoin {
+    JTableDev jt;
+    const int64_t* key;             // probe key column
+    const int64_t* vcol;            // the probe column the factors read (side 3), or nullptr
+    uint64_t* states;               // state words of the join's keyless group
+    unsigned long long* matched;    // the join's matched-row counter
+};
+// Probes many joins of one program in one persistent launch: warps pull work
+// items (join, probe-row range) from `next` (zeroed); `shape`'s factors read
+// the bucket payload (side 1) or the join's vcol (side 3) only.  joins,
+// items and next are device memory.
+void JoinSumBatchRun(const JoinSumShape& shape, const JsBatchJoin* joins, const JoinBatchItem* items,
+                     int64_t nitems, unsigned* next, cudaStream_t s);
+
 }  // namespace qdb

@@ -73,32 +73,53 @@ __global__ void JoinInitKernel(uint64_t* buckets, int64_t nbuckets) {
     }
 }
 
+// Inserts arena row r: one slot of its key's bucket sequence claimed by CAS.
+__device__ __forceinline__ void BuildRow(const JoinBuildArgs& a, int64_t r) {
+    bool null = false;
+    const uint64_t key = PackKeyCols(a, r, null);
+    if (null) return;
+    const uint64_t pay = a.pay0 ? uint64_t(a.pay0[r]) : 0;
+    if (a.jkey.full64 && key == kEmptyKey) {
+        const unsigned long long k = atomicAdd(a.nspecial, 1ull);
+        a.special_rows[2 * k] = a.row_base + r;
+        a.special_rows[2 * k + 1] = int64_t(pay);
+        return;
+    }
+    uint64_t b = Fmix64(key) & a.bmask;
+    for (uint64_t p = 0; p <= a.bmask; ++p) {
+        for (int j = 0; j < 2; ++j) {
+            auto* kp = reinterpret_cast<unsigned long long*>(&a.buckets[4 * b + j]);
+            if (*reinterpret_cast<volatile unsigned long long*>(kp) == kEmptyKey &&
+                atomicCAS(kp, kEmptyKey, key) == kEmptyKey) {
+                a.buckets[4 * b + 2 + j] = pay;
+                a.rows[2 * b + j] = a.row_base + r;
+                return;
+            }
+        }
+        b = (b + 1) & a.bmask;
+    }
+}
+
 __global__ void __launch_bounds__(256) JoinBuildKernel(const __grid_constant__ JoinBuildArgs a) {
     for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < a.nrows; r += int64_t(gridDim.x) * blockDim.x) {
-        bool null = false;
-        const uint64_t key = PackKeyCols(a, r, null);
-        if (null) continue;
-        const uint64_t pay = a.pay0 ? uint64_t(a.pay0[r]) : 0;
-        if (a.jkey.full64 && key == kEmptyKey) {
-            const unsigned long long k = atomicAdd(a.nspecial, 1ull);
-            a.special_rows[2 * k] = a.row_base + r;
-            a.special_rows[2 * k + 1] = int64_t(pay);
-            continue;
-        }
-        uint64_t b = Fmix64(key) & a.bmask;
-        bool placed = false;
-        for (uint64_t p = 0; p <= a.bmask && !placed; ++p) {
-            for (int j = 0; j < 2; ++j) {
-                auto* kp = reinterpret_cast<unsigned long long*>(&a.buckets[4 * b + j]);
-                if (*reinterpret_cast<volatile unsigned long long*>(kp) == kEmptyKey &&
-                    atomicCAS(kp, kEmptyKey, key) == kEmptyKey) {
-                    a.buckets[4 * b + 2 + j] = pay;
-                    a.rows[2 * b + j] = a.row_base + r;
-                    placed = true;
-                    break;
-                }
+        BuildRow(a, r);
+    }
+}
+
+// Many tables in one launch: item = (table, range); `init` clears bucket
+// ranges, otherwise arena-row ranges are inserted.
+__global__ void __launch_bounds__(256) JoinBatchKernel(const JoinBuildArgs* args, const JoinBatchItem* items,
+                                                       int64_t nitems, int init) {
+    for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const JoinBatchItem item = items[it];
+        const JoinBuildArgs& a = args[item.join];
+        for (int64_t r = item.lo + threadIdx.x; r < item.hi; r += blockDim.x) {
+            if (init) {
+                reinterpret_cast<ulonglong2*>(a.buckets)[2 * r] = make_ulonglong2(kEmptyKey, kEmptyKey);
+                reinterpret_cast<ulonglong2*>(a.buckets)[2 * r + 1] = make_ulonglong2(0, 0);
+            } else {
+                BuildRow(a, r);
             }
-            b = (b + 1) & a.bmask;
         }
     }
 }
@@ -565,6 +586,16 @@ void JoinMarkFlags(const uint8_t* marks, int64_t n, int want, uint8_t* flags, cu
 void JoinWritePairs(const int64_t* idx, int64_t n, int64_t* out, int mode, cudaStream_t s) {
     if (n == 0) return;
     JoinWritePairsKernel<<<Blocks(n, 256), 256, 0, s>>>(idx, n, out, mode);
+    CountLaunch();
+}
+
+void JoinBuildBatch(const JoinBuildArgs* args, const JoinBatchItem* items, int64_t nitems, bool init,
+                    cudaStream_t s) {
+    if (nitems == 0) return;
+    ProfileBegin(s, init ? "join_init_batch" : "join_build_batch", nitems);
+    JoinBatchKernel<<<int(std::min<int64_t>(nitems, int64_t(DeviceSMs()) * 8)), 256, 0, s>>>(args, items, nitems,
+                                                                                            init ? 1 : 0);
+    ProfileEnd(s);
     CountLaunch();
 }
 

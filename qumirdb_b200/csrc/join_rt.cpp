@@ -382,10 +382,9 @@ bool BuildDense(const JoinProgram& J, const ArenaState* a, const JoinBuildArgs& 
     return true;
 }
 
-bool Build(const qdb_gpu_program* prog, ArenaState* a, void* table) {
-    const JoinProgram& J = prog->join;
-    TableState* old = TableOf(table);
-    if (old) DestroyTable(old);
+// Sizes and allocates the bucket table of arena `a` (not yet initialised)
+// and fills its build arguments; nullptr on an allocation failure.
+TableState* NewTable(const JoinProgram& J, const ArenaState* a, JoinBuildArgs& b) {
     auto* t = new TableState();
     t->s = a->s;
     // Slots: a power of two >= 2x the rows; >= 4x while the buckets stay
@@ -400,11 +399,9 @@ bool Build(const qdb_gpu_program* prog, ArenaState* a, void* table) {
     t->nspecial_d = static_cast<unsigned long long*>(DevAlloc(8, t->s));
     if (!t->buckets || !t->rows || !t->special || !t->nspecial_d) {
         DestroyTable(t);
-        return false;
+        return nullptr;
     }
     cudaMemsetAsync(t->nspecial_d, 0, 8, t->s);
-    JoinInitTable(t->buckets, cap / 2, t->s);
-    JoinBuildArgs b;
     std::memset(&b, 0, sizeof(b));
     for (size_t j = 0; j < J.build_keys.size(); ++j) {
         const int ty = J.build_columns[J.build_keys[j]].type;
@@ -425,6 +422,26 @@ bool Build(const qdb_gpu_program* prog, ArenaState* a, void* table) {
     b.special_rows = t->special;
     b.nspecial = t->nspecial_d;
     b.row_base = 0;
+    return t;
+}
+
+void PublishTable(void* table, TableState* t, int64_t rows) {
+    *static_cast<TableState**>(table) = t;
+    int64_t* w = static_cast<int64_t*>(table);
+    w[1] = t->slots;   // Capacity
+    w[4] = rows;       // Rows
+    w[5] = rows;       // Keys (rows indexed)
+}
+
+bool Build(const qdb_gpu_program* prog, ArenaState* a, void* table) {
+    const JoinProgram& J = prog->join;
+    TableState* old = TableOf(table);
+    if (old) DestroyTable(old);
+    JoinBuildArgs b;
+    TableState* t = NewTable(J, a, b);
+    if (!t) return false;
+    const int64_t cap = t->slots;
+    JoinInitTable(t->buckets, cap / 2, t->s);
     int part_shift = 0;
     const int parts = JoinPartsFor(cap / 2, part_shift);
     if (parts == 1) {
@@ -450,11 +467,7 @@ bool Build(const qdb_gpu_program* prog, ArenaState* a, void* table) {
         DestroyTable(t);
         return false;
     }
-    *static_cast<TableState**>(table) = t;
-    int64_t* w = static_cast<int64_t*>(table);
-    w[1] = cap;        // Capacity
-    w[4] = a->rows;    // Rows
-    w[5] = a->rows;    // Keys (rows indexed)
+    PublishTable(table, t, a->rows);
     return true;
 }
 
@@ -985,6 +998,226 @@ int64_t qdb_gpu_join_aggregate_probe(const qdb_gpu_program* prog, void* arena, v
     }
     AggMirrorHeader(ht, st, prog->agg.plan);
     return AggStateMatched(st) - before;
+}
+
+}  // extern "C"
+
+namespace qdb {
+
+namespace {
+
+constexpr int64_t kBatchItemRows = 65536;
+
+void AddItems(std::vector<JoinBatchItem>& items, int32_t join, int64_t n) {
+    for (int64_t lo = 0; lo < n; lo += kBatchItemRows) {
+        JoinBatchItem it;
+        it.join = join;
+        it.pad = 0;
+        it.lo = lo;
+        it.hi = std::min(n, lo + kBatchItemRows);
+        items.push_back(it);
+    }
+}
+
+// Device copy of a host vector on stream s (freed by the caller).
+template <class T>
+T* ToDevice(const std::vector<T>& v, cudaStream_t s) {
+    auto* d = static_cast<T*>(DevAlloc(std::max<size_t>(v.size(), 1) * sizeof(T), s));
+    if (d && !v.empty()) cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+    return d;
+}
+
+// The fused join-aggregate plan of one probe batch (as
+// qdb_gpu_join_aggregate_probe resolves it) and its join-sum shape; false
+// when it has none (then `plan` is still resolved).
+bool ResolveJoinSum(const qdb_gpu_program* prog, const ArenaState* a, qdb_rowset* batch, Staging& stg,
+                    AggPlan& plan, int& inline_slot, JoinSumShape& shape, bool& is_sum) {
+    const JoinProgram& J = prog->join;
+    plan = prog->agg.plan;
+    if (!ResolveColumns(plan, prog->agg.cols, prog->columns.data(), batch, stg)) return false;
+    const int np = int(J.probe_columns.size());
+    for (int slot = 0; slot < plan.ncols; ++slot) {
+        ColDesc& cd = plan.cols[slot];
+        if (!cd.build) continue;
+        const ArenaCol& ac = a->payload[prog->agg.cols.input_of[slot] - np];
+        cd.data = ac.data;
+        cd.mask = reinterpret_cast<const uint8_t*>(ac.valid);
+        cd.mask_off = 0;
+        cd.bit_off = 0;
+    }
+    inline_slot = -1;
+    if (!J.payload.empty() && a->payload[0].width == 8) {
+        const int s0 = prog->agg.cols.slot_of[np];
+        if (s0 >= 0 && (plan.cols[s0].kind == LK_SIGNED || plan.cols[s0].kind == LK_F64)) inline_slot = s0;
+    }
+    std::memset(&shape, 0, sizeof(shape));
+    is_sum = MatchJoinSum(plan, J.agg_jk, inline_slot, shape);
+    return true;
+}
+
+}  // namespace
+
+}  // namespace qdb
+
+extern "C" {
+
+bool qdb_gpu_jr_build_batch(const qdb_gpu_program* prog, void* const* arenas, void* const* tables, int64_t n) {
+    t_error.clear();
+    if (!prog || (prog->kind != PK_JOIN && prog->kind != PK_JOIN_AGG) || n < 0 || (n > 0 && (!arenas || !tables))) {
+        SetErr("jr_build_batch: bad arguments");
+        return false;
+    }
+    const JoinProgram& J = prog->join;
+    cudaStream_t s = CurStream();
+    std::vector<JoinBuildArgs> args;
+    std::vector<JoinBatchItem> init_items, build_items;
+    std::vector<std::pair<TableState*, int64_t>> made;   // table, index
+    std::vector<cudaStream_t> streams;
+    for (int64_t i = 0; i < n; ++i) {
+        ArenaState* a = ArenaOf(arenas[i]);
+        if (!a || !tables[i]) {
+            SetErr("jr_build_batch: state %lld is not initialised", (long long)i);
+            return false;
+        }
+        if (TableState* old = TableOf(tables[i])) DestroyTable(old);
+        int64_t cap = 1024;   // NewTable's slot count
+        while (cap < a->rows * 2) cap *= 2;
+        if (cap * 2 * 16 <= (int64_t(32) << 20)) cap *= 2;
+        int part_shift = 0;
+        if (JoinPartsFor(cap / 2, part_shift) > 1) {   // a table larger than L2 takes the partitioned build
+            if (!Build(prog, a, tables[i])) return false;
+            continue;
+        }
+        JoinBuildArgs b;
+        TableState* t = NewTable(J, a, b);
+        if (!t) return false;
+        if (std::find(streams.begin(), streams.end(), t->s) == streams.end()) streams.push_back(t->s);
+        AddItems(init_items, int32_t(args.size()), t->slots / 2);
+        AddItems(build_items, int32_t(args.size()), a->rows);
+        args.push_back(b);
+        made.emplace_back(t, i);
+    }
+    // Appends and allocations ran on the arenas' streams.
+    for (cudaStream_t st : streams) {
+        if (st != s && !CudaOk(cudaStreamSynchronize(st), "jr_build_batch")) return false;
+    }
+    auto* dargs = ToDevice(args, s);
+    auto* dinit = ToDevice(init_items, s);
+    auto* dbuild = ToDevice(build_items, s);
+    bool ok = dargs && dinit && dbuild;
+    if (ok) {
+        JoinBuildBatch(dargs, dinit, int64_t(init_items.size()), true, s);
+        JoinBuildBatch(dargs, dbuild, int64_t(build_items.size()), false, s);
+        ok = CudaOk(cudaStreamSynchronize(s), "jr_build_batch");
+    }
+    DevFree(dargs, s);
+    DevFree(dinit, s);
+    DevFree(dbuild, s);
+    for (auto& m : made) {
+        if (ok) {
+            PublishTable(tables[m.second], m.first, ArenaOf(arenas[m.second])->rows);
+        } else {
+            DestroyTable(m.first);
+        }
+    }
+    return ok;
+}
+
+int64_t qdb_gpu_join_aggregate_probe_batch(const qdb_gpu_program* prog, void* const* arenas, void* const* tables,
+                                           void* const* hts, qdb_rowset* const* batches, int64_t n) {
+    t_error.clear();
+    if (!prog || prog->kind != PK_JOIN_AGG || n < 0 || (n > 0 && (!arenas || !tables || !hts || !batches))) {
+        SetErr("join_aggregate_probe_batch: bad arguments");
+        return -1;
+    }
+    cudaStream_t s = CurStream();
+    Staging stg(s);
+    std::vector<JsBatchJoin> joins;
+    std::vector<JoinBatchItem> items;
+    std::vector<AggTableState*> sts;
+    std::vector<cudaStream_t> streams;
+    JoinSumShape common;
+    bool batched = true;
+    for (int64_t i = 0; i < n && batched; ++i) {
+        ArenaState* a = ArenaOf(arenas[i]);
+        TableState* t = TableOf(tables[i]);
+        AggTableState* st = AggStateOf(hts[i]);
+        if (!a || !t || !st || !batches[i]) {
+            SetErr("join_aggregate_probe_batch: state %lld is not initialised and built", (long long)i);
+            return -1;
+        }
+        AggPlan plan;
+        int inline_slot = -1;
+        JoinSumShape shape;
+        bool is_sum = false;
+        if (!ResolveJoinSum(prog, a, batches[i], stg, plan, inline_slot, shape, is_sum)) return -1;
+        const int64_t* vcol = nullptr;
+        // The batched kernel reads the bucket payload and one probe column.
+        batched = is_sum && !batches[i]->Selection && JoinSumProbeColumn(shape, vcol);
+        if (!batched) break;
+        for (int k = 0; k < shape.nstates; ++k) {
+            for (int f = 0; f < shape.states[k].nf; ++f) {
+                JsFactor& jf = shape.states[k].f[f];
+                if (jf.side == 0) jf.side = 3;
+                jf.data = nullptr;
+            }
+        }
+        if (i == 0) {
+            common = shape;
+        } else if (std::memcmp(common.states, shape.states, sizeof(shape.states)) != 0 ||
+                   common.nstates != shape.nstates || common.need_pay != shape.need_pay) {
+            batched = false;
+            break;
+        }
+        JsBatchJoin j;
+        std::memset(&j, 0, sizeof(j));
+        j.jt = t->dev();
+        j.key = shape.probe_key;
+        j.vcol = vcol;
+        AggJoinSumTargets(st, &j.states, &j.matched);
+        if (std::find(streams.begin(), streams.end(), st->s) == streams.end()) streams.push_back(st->s);
+        AddItems(items, int32_t(joins.size()), batches[i]->RowCount);
+        joins.push_back(j);
+        sts.push_back(st);
+    }
+    if (!batched) {
+        // Another shape (a grouped aggregate, a selection): one by one.
+        int64_t total = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            const int64_t m = qdb_gpu_join_aggregate_probe(prog, arenas[i], tables[i], hts[i], batches[i]);
+            if (m < 0) return -1;
+            total += m;
+        }
+        return total;
+    }
+    // Biggest joins' items first: the tail of the launch is small items.
+    std::stable_sort(items.begin(), items.end(), [&](const JoinBatchItem& x, const JoinBatchItem& y) {
+        return batches[x.join]->RowCount > batches[y.join]->RowCount;
+    });
+    for (cudaStream_t st : streams) {
+        if (st != s && !CudaOk(cudaStreamSynchronize(st), "join_aggregate_probe_batch")) return -1;
+    }
+    auto* djoins = ToDevice(joins, s);
+    auto* ditems = ToDevice(items, s);
+    auto* next = static_cast<unsigned*>(DevAlloc(4, s));
+    bool ok = djoins && ditems && next;
+    if (ok) {
+        cudaMemsetAsync(next, 0, 4, s);
+        JoinSumBatchRun(common, djoins, ditems, int64_t(items.size()), next, s);
+        ok = CudaOk(cudaStreamSynchronize(s), "join_aggregate_probe_batch");
+    }
+    DevFree(djoins, s);
+    DevFree(ditems, s);
+    DevFree(next, s);
+    if (!ok) return -1;
+    int64_t total = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t before = AggStateMatched(sts[size_t(i)]);
+        if (!AggJoinSumCommit(sts[size_t(i)])) return -1;
+        AggMirrorHeader(hts[i], sts[size_t(i)], prog->agg.plan);
+        total += AggStateMatched(sts[size_t(i)]) - before;
+    }
+    return total;
 }
 
 }  // extern "C"

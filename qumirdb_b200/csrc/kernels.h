@@ -155,6 +155,17 @@ struct JoinBuildArgs {
 };
 void JoinInitTable(uint64_t* buckets, int64_t nbuckets, cudaStream_t s);
 void JoinBuild(const JoinBuildArgs& a, cudaStream_t s);
+// Work item of a launch over many tables: table `join`, range [lo, hi).
+struct JoinBatchItem {
+    int32_t join;
+    int32_t pad;
+    int64_t lo;
+    int64_t hi;
+};
+// Many tables in one launch (args and items in device memory): with init,
+// item ranges are bucket ranges to clear; otherwise arena-row ranges to insert.
+void JoinBuildBatch(const JoinBuildArgs* args, const JoinBatchItem* items, int64_t nitems, bool init,
+                    cudaStream_t s);
 // Radix partitioning of join rows for tables larger than L2: partition =
 // home bucket (Fmix64(key) & bmask) >> part_shift, so partition p's rows
 // touch only bucket slice p (and the slot after a full bucket).

@@ -501,6 +501,19 @@ bool AggRunJoinSum(AggTableState* st, const JoinSumShape& shape, const JTableDev
     return true;
 }
 
+void AggJoinSumTargets(AggTableState* st, uint64_t** states, unsigned long long** matched) {
+    const int64_t slot = int64_t(Fmix64(0) & uint64_t(st->t.capacity - 1));
+    *states = st->t.slots + slot * st->t.slot_words + st->t.state_off;
+    *matched = &st->dc->matched;
+    ResetCounters(st);
+}
+
+bool AggJoinSumCommit(AggTableState* st) {
+    if (!ReadCounters(st)) return false;
+    st->matched += int64_t(st->hc->matched);
+    return true;
+}
+
 int64_t AggStateGroups(const AggTableState* st) { return st ? st->groups : 0; }
 int64_t AggStateMatched(const AggTableState* st) { return st ? st->matched : 0; }
 AggTableState* AggStateOf(void* ht) { return StateOf(ht); }

@@ -95,6 +95,11 @@ bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyP
 int64_t AggFinish(AggTableState* st, const AggLowering& lw, uint32_t flags, qdb_rowset* out);
 struct JoinSumShape;
 bool AggRunJoinSum(AggTableState* st, const JoinSumShape& shape, const JTableDev& jt, int64_t nrows);
+// Batched join-sum: the keyless group's state words and matched counter of a
+// state (its counters reset on its stream), then the read-back that adds
+// the matched rows once the batch has run.
+void AggJoinSumTargets(AggTableState* st, uint64_t** states, unsigned long long** matched);
+bool AggJoinSumCommit(AggTableState* st);
 int64_t AggStateGroups(const AggTableState* st);
 int64_t AggStateMatched(const AggTableState* st);
 AggTableState* AggStateOf(void* ht);

@@ -345,3 +345,38 @@ def test_typed_join_compile_rejects_unserved_shapes():
                                 out=[(1, 0)], join_type=jt, build_is_left=left)
         with pytest.raises(q.QdbError):
             q.compile_row_join(spec)
+
+
+@pytest.mark.parametrize("with_selection", [False, True])
+def test_batched_joins_match_each_join(with_selection):
+    """Many uneven joins of the join-sum program: one batched build and one
+    persistent probe launch give every join the oracle's SUM / COUNT (a
+    selection on a probe batch takes the one-by-one path, same results)."""
+    rng = np.random.default_rng(21)
+    jspec, aspec = queries.join_sum(40)
+    prog = q.compile_join_aggregate(jspec, aspec)
+    n = 200
+    jb = q.RowJoinBatch(prog, n)
+    builds, probes = [], []
+    for i in range(n):
+        nb = int(rng.integers(10, 20_000))
+        npr = int(rng.integers(1, 200_000))
+        b, p = join_data(nb, npr, int(nb * 1.3) + 1)
+        if i % 17 == 0:
+            b[0][: nb // 3] = b[0][0]            # duplicate build keys
+        if i % 23 == 0:
+            p[0][::7] = -1                       # the empty-key marker of the table, as a key
+        sel = (rng.random(npr) > 0.5).astype(np.uint8) if with_selection and i == 5 else None
+        brs, prs = q.HostRowSet(b), q.DeviceRowSet(p, selection=sel)
+        jb.append(i, brs)
+        builds.append(brs)
+        probes.append((prs, q.HostRowSet(p, selection=sel)))
+    jb.build()
+    jb.probe_aggregate([p for p, _ in probes])
+    outs = jb.finish()
+    for i, out in enumerate(outs):
+        got = gpu_rows(out, [abi.I64, abi.I64])
+        q.release(out)
+        want = O.join_aggregate(jspec, aspec, [builds[i]], [probes[i][1]])
+        assert got == want, i
+    jb.release()
