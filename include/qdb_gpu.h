@@ -411,6 +411,10 @@ int64_t qdb_gpu_join_aggregate_probe(const qdb_gpu_program* program,
 /* these tables carry no Bloom filter or direct index (a table larger than   */
 /* L2 still gets its own partitioned build).  Returns false on failure.      */
 bool qdb_gpu_jr_build_batch(const qdb_gpu_program* program, void* const* arenas, void* const* tables, int64_t n);
+/* jr_append_batch: Append (jr_dispatch op 1) of batches[i] to arenas[i] for  */
+/* every i, waiting on the device once for all of them.  false on failure.   */
+bool qdb_gpu_jr_append_batch(const qdb_gpu_program* program, void* const* arenas, qdb_rowset* const* batches,
+                             int64_t n);
 /* join_aggregate_probe_batch: qdb_gpu_join_aggregate_probe of batches[i]    */
 /* into hts[i] for every i, in one persistent launch when the program has   */
 /* the keyless join-sum shape (COUNT / SUM of products of the build payload */

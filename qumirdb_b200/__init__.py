@@ -672,6 +672,13 @@ class RowJoinBatch:
     def append(self, i: int, batch) -> None:
         self.joins[i].append(batch)
 
+    def append_all(self, batches) -> None:
+        """Every join's build batch at once (one device wait for all)."""
+        rs = RowSetPointers(batches)
+        if not lib().qdb_gpu_jr_append_batch(self.prog.handle, self._ptrs([j.arena for j in self.joins]), rs.arr,
+                                             self.n):
+            raise QdbError(f"batched join append failed: {last_error()}")
+
     def build(self) -> None:
         if not lib().qdb_gpu_jr_build_batch(self.prog.handle, self._ptrs([j.arena for j in self.joins]),
                                             self._ptrs([j.table for j in self.joins]), self.n):
@@ -686,8 +693,13 @@ class RowJoinBatch:
             raise QdbError(f"batched join probe failed: {last_error()}")
         return m
 
-    def finish(self) -> list[abi.RowSet]:
-        return [a.finish() for a in self.aggs]
+    def finish(self) -> "RowSets":
+        """Every join's aggregate finished in one batched finalize (slices of
+        shared output buffers; release each, or all with release())."""
+        outs = (abi.RowSet * max(1, self.n))()
+        if lib().qdb_gpu_agg_finish_batch(self.prog.handle, self._ptrs([a.ht for a in self.aggs]), self.n, outs) < 0:
+            raise QdbError(f"batched join finish failed: {last_error()}")
+        return RowSets(outs, self.n)
 
     def release(self) -> None:
         for j in self.joins:

@@ -171,6 +171,7 @@ SIGNATURES = {
     "qdb_gpu_rf_probe_rowset": (CI64, [P, C.POINTER(RfData), PRS, P]),
     "qdb_gpu_shuffle": (CI64, [P, PRS, P, CI64, CI64, PRS]),
     "qdb_gpu_jr_build_batch": (BOOLC, [P, C.POINTER(P), C.POINTER(P), CI64]),
+    "qdb_gpu_jr_append_batch": (BOOLC, [P, C.POINTER(P), C.POINTER(PRS), CI64]),
     "qdb_gpu_join_aggregate_probe_batch": (CI64, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(PRS), CI64]),
     "qdb_gpu_cache_create": (P, [SZ, SZ]),
     "qdb_gpu_cache_destroy": (None, [P]),

@@ -838,7 +838,7 @@ extern "C" {
 
 int64_t qdb_gpu_agg_finish_batch(const qdb_gpu_program* prog, void* const* hts, int64_t n, qdb_rowset* outs) {
     t_error.clear();
-    if (!prog || prog->kind != PK_AGG || (n > 0 && (!hts || !outs))) {
+    if (!prog || (prog->kind != PK_AGG && prog->kind != PK_JOIN_AGG) || (n > 0 && (!hts || !outs))) {
         SetErr("agg_finish_batch: not an aggregate program, or no states");
         return -1;
     }

@@ -585,6 +585,8 @@ void JoinSumRun(const JoinSumShape& shape, const JTableDev& jt, int64_t nrows, u
 // ---------------------------------------------------------------------------
 namespace {
 
+constexpr int kJsBatchRows = 4;   // rows per lane per step
+
 struct JsBatchLaunch {
     JoinSumShape S;
     const JsBatchJoin* joins;
@@ -626,17 +628,46 @@ __global__ void __launch_bounds__(256) JoinSumBatchKernel(const __grid_constant_
                 if (s < L.S.nstates) v[s] += JsBatchTerm(L.S.states[s], pay, sv);
             }
         };
-        for (int64_t r = item.lo + lane; r < item.hi; r += 32) {
-            const uint64_t key = uint64_t(__ldcs(&J.key[r]));
-            const int64_t sv = J.vcol ? __ldcs(&J.vcol[r]) : 0;
-            if (key == kEmptyKey) {
-                for (int64_t q = 0; q < nspecial; ++q) fold(uint64_t(jt.special_rows[2 * q + 1]), sv);
-                continue;
+        // Four coalesced 32-row slabs per step: every lane's four key loads,
+        // then its four bucket reads, are in flight together.
+        for (int64_t r0 = item.lo + lane; r0 < item.hi; r0 += 32 * kJsBatchRows) {
+            uint64_t key[kJsBatchRows];
+            int64_t sv[kJsBatchRows];
+            bool on[kJsBatchRows];
+#pragma unroll
+            for (int j = 0; j < kJsBatchRows; ++j) {
+                const int64_t r = r0 + 32 * j;
+                on[j] = r < item.hi;
+                key[j] = on[j] ? uint64_t(__ldcs(&J.key[r])) : 0;
+                sv[j] = (on[j] && J.vcol) ? __ldcs(&J.vcol[r]) : 0;
             }
-            const uint64_t b = Fmix64(key) & jt.bmask;
-            VisitMatches(jt, key, b, BucketKeys(jt, b), [&](uint64_t, uint64_t bk, int jj) {
-                fold(L.S.need_pay ? jt.buckets[4 * bk + 2 + jj] : 0, sv);
-            });
+            uint64_t b[kJsBatchRows];
+            ulonglong2 k[kJsBatchRows], p[kJsBatchRows];
+#pragma unroll
+            for (int j = 0; j < kJsBatchRows; ++j) {
+                const bool probe = on[j] && key[j] != kEmptyKey;
+                b[j] = Fmix64(key[j]) & jt.bmask;
+                k[j] = probe ? BucketKeys(jt, b[j]) : make_ulonglong2(kEmptyKey, kEmptyKey);
+                p[j] = (probe && L.S.need_pay) ? BucketPays(jt, b[j]) : make_ulonglong2(0, 0);
+            }
+#pragma unroll
+            for (int j = 0; j < kJsBatchRows; ++j) {
+                if (!on[j]) continue;
+                if (key[j] == kEmptyKey) {   // the one key equal to the empty marker lives in the side list
+                    for (int64_t q = 0; q < nspecial; ++q) fold(uint64_t(jt.special_rows[2 * q + 1]), sv[j]);
+                    continue;
+                }
+                if (k[j].x == kEmptyKey) continue;
+                if (k[j].x == key[j]) fold(p[j].x, sv[j]);
+                if (k[j].y == kEmptyKey) continue;
+                if (k[j].y == key[j]) fold(p[j].y, sv[j]);
+                // Both slots taken: the key's sequence goes on.
+                const uint64_t nb = (b[j] + 1) & jt.bmask;
+                const int64_t v = sv[j];
+                VisitMatches(jt, key[j], nb, BucketKeys(jt, nb), [&](uint64_t, uint64_t bk, int jj) {
+                    fold(L.S.need_pay ? jt.buckets[4 * bk + 2 + jj] : 0, v);
+                });
+            }
         }
 #pragma unroll
         for (int s = 0; s < kJsMaxStates; ++s) {

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstring>
+#include <memory>
 
 #include "fast.h"
 #include "runtime.h"
@@ -216,60 +217,113 @@ void DestroyTable(TableState* t) {
     delete t;
 }
 
-// Append: selected rows that pass the build predicate and have valid keys,
-// in input order (GenRowJoinAppendAst, qdb/kernel/join_gen.cpp:2063-2160);
-// with null_keys, the rows whose key has a NULL field instead (the
-// jr_append_null_keys variant, nullKeys = true).
-bool Append(const qdb_gpu_program* prog, ArenaState* a, qdb_rowset* batch, bool null_keys = false) {
+// One Append in two halves, so that a batch of appends waits on the device
+// once: Start filters and compacts the batch's rows and queues the read-back
+// of their count; Finish (after the stream has drained) grows the arena and
+// gathers the rows.
+struct AppendJob {
+    ArenaState* a = nullptr;
+    std::unique_ptr<Staging> stg;
+    AggPlan plan;
+    int64_t n = 0;
+    uint8_t* flags = nullptr;
+    int64_t* idx = nullptr;
+    unsigned long long* dcount = nullptr;
+    void* scratch = nullptr;
+    int* derr = nullptr;
+    unsigned long long* hcount = nullptr;   // page-locked: count, then error
+    void Free() {
+        cudaStream_t s = a->s;
+        DevFree(flags, s);
+        DevFree(idx, s);
+        DevFree(dcount, s);
+        DevFree(scratch, s);
+        DevFree(derr, s);
+        flags = nullptr;
+        idx = nullptr;
+        dcount = nullptr;
+        scratch = nullptr;
+        derr = nullptr;
+    }
+};
+
+bool AppendStart(const qdb_gpu_program* prog, ArenaState* a, qdb_rowset* batch, bool null_keys, AppendJob& job,
+                 unsigned long long* hcount) {
     const JoinProgram& J = prog->join;
-    const int64_t n = batch->RowCount;
-    if (n == 0) return true;
+    job.a = a;
+    job.n = batch->RowCount;
+    job.hcount = hcount;
+    hcount[0] = 0;
+    hcount[1] = 0;
+    if (job.n == 0) return true;
     cudaStream_t s = a->s;
-    Staging stg(s);
-    AggPlan plan = J.build_filter.plan;
-    if (!ResolveColumns(plan, J.build_filter.cols, J.build_columns.data(), batch, stg)) return false;
-    uint8_t* flags = static_cast<uint8_t*>(DevAlloc(size_t(n), s));
-    int64_t* idx = static_cast<int64_t*>(DevAlloc(size_t(n) * 8, s));
-    unsigned long long* dcount = static_cast<unsigned long long*>(DevAlloc(8, s));
-    void* scratch = DevAlloc(CompactScratch(n), s);
-    int* derr = static_cast<int*>(DevAlloc(sizeof(int), s));
-    if (!flags || !idx || !dcount || !scratch || !derr) return false;
-    cudaMemsetAsync(derr, 0, sizeof(int), s);
+    job.stg.reset(new Staging(s));
+    job.plan = J.build_filter.plan;
+    if (!ResolveColumns(job.plan, J.build_filter.cols, J.build_columns.data(), batch, *job.stg)) return false;
+    const int64_t n = job.n;
+    job.flags = static_cast<uint8_t*>(DevAlloc(size_t(n), s));
+    job.idx = static_cast<int64_t*>(DevAlloc(size_t(n) * 8, s));
+    job.dcount = static_cast<unsigned long long*>(DevAlloc(8, s));
+    job.scratch = DevAlloc(CompactScratch(n), s);
+    job.derr = static_cast<int*>(DevAlloc(sizeof(int), s));
+    if (!job.flags || !job.idx || !job.dcount || !job.scratch || !job.derr) return false;
+    cudaMemsetAsync(job.derr, 0, sizeof(int), s);
     ExprArgs ea;
-    ea.plan = &plan;
+    ea.plan = &job.plan;
     ea.nrows = n;
-    ea.out_sel = flags;
-    ea.err = derr;
+    ea.out_sel = job.flags;
+    ea.err = job.derr;
     ea.n_null_reject = int(J.build_keys.size());
     for (size_t j = 0; j < J.build_keys.size(); ++j) {
         ea.null_reject[j] = uint8_t(J.build_filter.cols.slot_of[J.build_keys[j]]);
     }
     ea.null_keys_only = null_keys ? 1 : 0;
     FilterRows(ea, s);
-    CompactFlags(flags, n, idx, dcount, scratch, s);
-    unsigned long long selected = 0;
-    int herr = 0;
-    cudaMemcpyAsync(&selected, dcount, 8, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s);
-    if (!CudaOk(cudaStreamSynchronize(s), "row join append")) return false;
+    CompactFlags(job.flags, n, job.idx, job.dcount, job.scratch, s);
+    cudaMemcpyAsync(hcount, job.dcount, 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hcount + 1, job.derr, sizeof(int), cudaMemcpyDeviceToHost, s);
+    return true;
+}
+
+bool AppendFinish(const qdb_gpu_program* prog, AppendJob& job) {
+    if (job.n == 0) return true;
+    const JoinProgram& J = prog->join;
+    ArenaState* a = job.a;
+    cudaStream_t s = a->s;
+    const unsigned long long selected = job.hcount[0];
+    const int herr = int(job.hcount[1]);
     bool ok = herr == 0;
     if (!ok) SetErr("row join append: device error %d", herr);
     if (ok && selected > 0) {
         ok = GrowArena(a, a->rows + int64_t(selected));
         auto gather = [&](ArenaCol& c, int input) {
-            const ColDesc& cd = plan.cols[J.build_filter.cols.slot_of[input]];
-            GatherColumn(cd.data, c.width, idx, 1, int64_t(selected), c.data + a->rows * c.width, s);
-            if (c.valid) GatherValidity(cd.mask, cd.mask_off, idx, 1, int64_t(selected), c.valid, a->rows, s);
+            const ColDesc& cd = job.plan.cols[J.build_filter.cols.slot_of[input]];
+            GatherColumn(cd.data, c.width, job.idx, 1, int64_t(selected), c.data + a->rows * c.width, s);
+            if (c.valid) GatherValidity(cd.mask, cd.mask_off, job.idx, 1, int64_t(selected), c.valid, a->rows, s);
         };
         for (size_t j = 0; ok && j < J.build_keys.size(); ++j) gather(a->keys[j], J.build_keys[j]);
         for (size_t j = 0; ok && j < J.payload.size(); ++j) gather(a->payload[j], J.payload[j]);
         a->rows += int64_t(selected);
     }
-    DevFree(flags, s);
-    DevFree(idx, s);
-    DevFree(dcount, s);
-    DevFree(scratch, s);
-    DevFree(derr, s);
+    job.Free();
+    return ok;
+}
+
+// Append: selected rows that pass the build predicate and have valid keys,
+// in input order (GenRowJoinAppendAst, qdb/kernel/join_gen.cpp:2063-2160);
+// with null_keys, the rows whose key has a NULL field instead (the
+// jr_append_null_keys variant, nullKeys = true).
+bool Append(const qdb_gpu_program* prog, ArenaState* a, qdb_rowset* batch, bool null_keys = false) {
+    unsigned long long* hc = static_cast<unsigned long long*>(HostOutAlloc(16));
+    if (!hc) return false;
+    AppendJob job;
+    bool ok = AppendStart(prog, a, batch, null_keys, job, hc) && CudaOk(cudaStreamSynchronize(a->s), "row join append");
+    if (ok) {
+        ok = AppendFinish(prog, job);
+    } else if (job.a) {
+        job.Free();
+    }
+    HostOutFree(hc);
     return ok;
 }
 
@@ -1204,6 +1258,7 @@ int64_t qdb_gpu_join_aggregate_probe_batch(const qdb_gpu_program* prog, void* co
     if (ok) {
         cudaMemsetAsync(next, 0, 4, s);
         JoinSumBatchRun(common, djoins, ditems, int64_t(items.size()), next, s);
+        for (AggTableState* st : sts) AggJoinSumFetch(st, s);
         ok = CudaOk(cudaStreamSynchronize(s), "join_aggregate_probe_batch");
     }
     DevFree(djoins, s);
@@ -1218,6 +1273,43 @@ int64_t qdb_gpu_join_aggregate_probe_batch(const qdb_gpu_program* prog, void* co
         total += AggStateMatched(sts[size_t(i)]) - before;
     }
     return total;
+}
+
+bool qdb_gpu_jr_append_batch(const qdb_gpu_program* prog, void* const* arenas, qdb_rowset* const* batches,
+                             int64_t n) {
+    t_error.clear();
+    if (!prog || (prog->kind != PK_JOIN && prog->kind != PK_JOIN_AGG) || n < 0 || (n > 0 && (!arenas || !batches))) {
+        SetErr("jr_append_batch: bad arguments");
+        return false;
+    }
+    auto* hc = static_cast<unsigned long long*>(HostOutAlloc(size_t(std::max<int64_t>(n, 1)) * 16));
+    if (!hc) return false;
+    std::vector<AppendJob> jobs(static_cast<size_t>(n));
+    std::vector<cudaStream_t> streams;
+    bool ok = true;
+    for (int64_t i = 0; i < n && ok; ++i) {
+        ArenaState* a = ArenaOf(arenas[i]);
+        if (!a || !batches[i]) {
+            SetErr("jr_append_batch: arena %lld is not initialised", (long long)i);
+            ok = false;
+            break;
+        }
+        ok = AppendStart(prog, a, batches[i], false, jobs[size_t(i)], hc + 2 * i);
+        if (std::find(streams.begin(), streams.end(), a->s) == streams.end()) streams.push_back(a->s);
+    }
+    for (cudaStream_t st : streams) ok = CudaOk(cudaStreamSynchronize(st), "jr_append_batch") && ok;
+    for (int64_t i = 0; i < n; ++i) {
+        AppendJob& job = jobs[size_t(i)];
+        if (!job.a) continue;
+        if (ok) {
+            ok = AppendFinish(prog, job);
+            static_cast<int64_t*>(arenas[i])[5] = job.a->rows;
+        } else {
+            job.Free();
+        }
+    }
+    HostOutFree(hc);
+    return ok;
 }
 
 }  // extern "C"

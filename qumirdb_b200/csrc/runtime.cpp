@@ -508,8 +508,15 @@ void AggJoinSumTargets(AggTableState* st, uint64_t** states, unsigned long long*
     ResetCounters(st);
 }
 
+void AggJoinSumFetch(AggTableState* st, cudaStream_t s) {
+    cudaMemcpyAsync(st->hc, st->dc, sizeof(AggCounters), cudaMemcpyDeviceToHost, s);
+}
+
 bool AggJoinSumCommit(AggTableState* st) {
-    if (!ReadCounters(st)) return false;
+    if (st->hc->error) {
+        SetErr("aggregate kernel reported device error %d", st->hc->error);
+        return false;
+    }
     st->matched += int64_t(st->hc->matched);
     return true;
 }

@@ -96,9 +96,11 @@ int64_t AggFinish(AggTableState* st, const AggLowering& lw, uint32_t flags, qdb_
 struct JoinSumShape;
 bool AggRunJoinSum(AggTableState* st, const JoinSumShape& shape, const JTableDev& jt, int64_t nrows);
 // Batched join-sum: the keyless group's state words and matched counter of a
-// state (its counters reset on its stream), then the read-back that adds
-// the matched rows once the batch has run.
+// state (its counters reset on its stream); once the batch has run, Fetch
+// queues the counters' read-back on stream s and, after s has drained,
+// Commit adds the matched rows.
 void AggJoinSumTargets(AggTableState* st, uint64_t** states, unsigned long long** matched);
+void AggJoinSumFetch(AggTableState* st, cudaStream_t s);
 bool AggJoinSumCommit(AggTableState* st);
 int64_t AggStateGroups(const AggTableState* st);
 int64_t AggStateMatched(const AggTableState* st);

@@ -368,9 +368,13 @@ def test_batched_joins_match_each_join(with_selection):
             p[0][::7] = -1                       # the empty-key marker of the table, as a key
         sel = (rng.random(npr) > 0.5).astype(np.uint8) if with_selection and i == 5 else None
         brs, prs = q.HostRowSet(b), q.DeviceRowSet(p, selection=sel)
-        jb.append(i, brs)
+        if i % 2:
+            jb.append(i, brs)
         builds.append(brs)
         probes.append((prs, q.HostRowSet(p, selection=sel)))
+    empty = q.HostRowSet([np.empty(0, np.int64), np.empty(0, np.int64), np.empty(0, np.int32)])
+    # Even joins take their build rows in one batched append (odd ones were appended one by one).
+    jb.append_all([builds[i] if i % 2 == 0 else empty for i in range(n)])
     jb.build()
     jb.probe_aggregate([p for p, _ in probes])
     outs = jb.finish()
