@@ -345,7 +345,7 @@ def zipf_batched_operator(q, peak):
             "l2": "inputs larger than L2", "gpu_launches": launches / 3, "autotune": q.autotune_info()}
 
 
-def join_batched_operator(q, peak, w):
+def join_batched_operator(q, peak, w, steps: int = 3):
     """Config 1's join as the engine's partitioned plan: both sides split by
     the join key's hash into JOIN_PARTS partitions with the device shuffle
     (input preparation, untimed), then per step the partitions' build rows
@@ -381,7 +381,7 @@ def join_batched_operator(q, peak, w):
         jb.release()
         res.append((s, c))
 
-    ms, _, launches, _ = timed(q, step, 3, 2)
+    ms, _, launches, _ = timed(q, step, steps, 2 if steps > 1 else 0)
     _, _, _, kernels = timed(q, step, 2, 0, profile=True)
     kms, _ = kernel_avg(kernels, "join_agg_probe_batch", 2)
     bms, _ = kernel_avg(kernels, "join_build_batch", 2)
@@ -729,6 +729,10 @@ def profile_case(name: str, rows: int) -> None:
             agg = q.Aggregate(prog)
             J.probe_aggregate(agg, dp)
             q.release(agg.finish())
+    elif name == "join_batched":
+        w = JoinWorkload(q, 0)
+        for _ in range(2):
+            join_batched_operator(q, 1.0, w, steps=1)
     elif name == "zipf":
         n = rows or ZIPF_ROWS
         cols = [np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.float64)]
@@ -836,7 +840,8 @@ def main() -> None:
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--no-operators", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-case", choices=["join", "sort", "topk", "lineitem", "zipf", "zipf_batched"],
+    ap.add_argument("--profile-case", choices=["join", "join_batched", "sort", "topk", "lineitem", "zipf",
+                                               "zipf_batched"],
                     help="run one workload twice at --rows rows (for profiler captures) and exit")
     ap.add_argument("--rows", type=int, default=0)
     ap.add_argument("--detail", help="write every operator's full figures (serving sweeps included) to this file")
