@@ -476,8 +476,11 @@ int64_t qdb_gpu_top_sort_update(const qdb_gpu_program* program, qdb_rowset* stat
 /* taken from a device arena shared by the batch.  Block shape and work item */
 /* size come from an autotuner (set QDB_AUTOTUNE=0 to keep the defaults); the */
 /* launch sequence is replayed as a CUDA graph while the batch keeps its     */
-/* structure.  States whose program shape has no batched kernel are updated  */
-/* one by one.  Returns n, or < 0 on failure.                                */
+/* structure.  High-cardinality programs run a shared tier in front of each  */
+/* aggregate's table; keyless ones and ones whose hint is <= 64 groups fold  */
+/* into lane-private accumulators per work item.  States whose program shape */
+/* has no batched kernel (or whose columns are not on a four-value boundary, */
+/* for the latter) are updated one by one.  Returns n, or < 0 on failure.    */
 int64_t qdb_gpu_agg_dispatch_batch(const qdb_gpu_program* program, void* const* states,
                                    qdb_rowset* const* batches, int64_t n);
 

@@ -2011,6 +2011,26 @@ __device__ __forceinline__ void QuadRow(RegRow<SH::Cols::n>& row,
     }
 }
 
+// L2 prefetch of 128-row tile `t` of a range of n rows: the tile's w lines
+// of a w-byte column (and its selection bytes), one line per lane.  Rows
+// past the range are not touched.
+constexpr int kPrefetchTiles = 16;   // two tiles ahead for each of a CTA's eight warps
+
+template <class SH, int K = 0>
+__device__ __forceinline__ void QuadPrefetchTile(const char* const* cb, const uint8_t* sel, int64_t t, int64_t n,
+                                                 int lane) {
+    constexpr int kTileRows = 32 * kQuadRows;
+    if constexpr (K < SH::Cols::n) {
+        constexpr int w = SH::cw(K);
+        const int64_t r = t * kTileRows + int64_t(lane) * (128 / w);
+        if (lane < w && r < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(cb[K] + r * w));
+        QuadPrefetchTile<SH, K + 1>(cb, sel, t, n, lane);
+    } else {
+        const int64_t r = t * kTileRows;
+        if (sel && lane == 0 && r < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(sel + r));
+    }
+}
+
 template <class SIG>
 __global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid_constant__ AggLaunch L) {
     unsigned char* smem = DynSmem();
@@ -2027,6 +2047,7 @@ __global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid
         misc[1] = 0;
         misc[2] = 0;
         misc[4] = 0;
+        misc[5] = 0;   // next 128-row tile of the range
     }
     for (int i = tid; i < sm.S; i += bd) {
         sm.keys[i] = kEmptyKey;
@@ -2078,8 +2099,22 @@ __global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid
     }
     const uint8_t* sel = P.selection ? P.selection + row0 : nullptr;
     constexpr int NC = SIG::Cols::n > 0 ? SIG::Cols::n : 1;
+    // The warps of the CTA take the range's 128-row tiles from a shared
+    // counter, so that none idles at the closing barrier while another still
+    // has tiles; each asks the L2 for the tile kPrefetchTiles ahead of the one
+    // it takes (every tile is asked for once), so that the tile's loads meet
+    // it in L2 rather than in HBM.
+    const int64_t ntiles = (n + kWarpRows - 1) / kWarpRows;
+    unsigned* next_tile = misc + 5;
 #pragma unroll 1
-    for (int64_t r4 = int64_t(tid >> 5) * kWarpRows + lane * kQuadRows; r4 < n; r4 += (bd >> 5) * kWarpRows) {
+    for (;;) {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(next_tile, 1u);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (int64_t(t) >= ntiles) break;
+        QuadPrefetchTile<SIG>(cb, sel, int64_t(t) + kPrefetchTiles, n, lane);
+        const int64_t r4 = int64_t(t) * kWarpRows + lane * kQuadRows;
+        if (r4 >= n) continue;
         const int nvalid = int(min(int64_t(kQuadRows), n - r4));
         int64_t q[NC][kQuadRows];
         LoadQuad<SIG>(q, cb, r4, nvalid);
@@ -2184,6 +2219,235 @@ __global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid
     }
     __syncthreads();
     if (tid == 0 && sm.fresh[0]) atomicAdd(&L.counters->new_groups, (unsigned long long)sm.fresh[0]);
+}
+
+// ---------------------------------------------------------------------------
+// Many low-cardinality aggregates of one program in one persistent launch
+// (batched aggregation of the QDB_SHAPE_LIST shapes): a CTA pulls work items
+// (aggregate, row range) from the queue; for each it walks the rows four per
+// lane as AggSigQuadKernel does, folding the item's first kPrivGroups groups
+// into lane-private accumulators and any others into the shared tier, then
+// merges both into that aggregate's table — spilling tagged entries when the
+// table is full, for the replay into a grown table — and clears them for the
+// next item.  A row whose group finds no room in the tier goes to the table
+// at once; one that the full table turns away is deferred for the replay.
+// ---------------------------------------------------------------------------
+template <class SIG>
+__global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadBatchKernel(const __grid_constant__ AggLaunch L,
+                                                                         const __grid_constant__ HighBatch B) {
+    unsigned char* smem = DynSmem();
+    unsigned* misc = reinterpret_cast<unsigned*>(smem + L.off_misc);
+    const SmemTable sm = MakeSmem(L, false, true);
+    const AggPlan& P = L.P;
+    const FastPlan& F = L.F;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    constexpr int bd = kQuadThreads;
+    constexpr int kWarpRows = 32 * kQuadRows;
+    constexpr int NC = SIG::Cols::n > 0 ? SIG::Cols::n : 1;
+    uint64_t* pacc = reinterpret_cast<uint64_t*>(smem + L.off_pacc);
+    __shared__ long long item_at;
+    for (;;) {
+        // Clear the tiers for the next item.
+        if (tid == 0) {
+            misc[0] = 0;
+            misc[1] = 0;
+            misc[2] = 0;
+            misc[4] = 0;
+            item_at = (long long)atomicAdd(&B.counters->next_item, 1ull);
+        }
+        for (int i = tid; i < sm.S; i += bd) {
+            sm.keys[i] = kEmptyKey;
+            sm.gid[i] = -1;
+            for (int st = 0; st < P.nstates; ++st) {
+                const StateDesc sd = P.states[st];
+                sm.st[int64_t(sd.word) * sm.S + i] = StateIdentity(sd.kind);
+                if (sd.kind == ST_SUM_I128) sm.st[int64_t(sd.word + 1) * sm.S + i] = 0;
+            }
+        }
+        for (int i = tid; i < kPrivGroups * SIG::words * bd; i += bd) pacc[i] = 0;
+        __syncthreads();
+        const int64_t it = item_at;
+        if (it >= B.nitems) return;
+        if (P.nkeyparts == 0 && tid == 0 && sm.S > 0) {
+            const int i = int(uint32_t(Fmix64(0)) & uint32_t(sm.S - 1));
+            sm.keys[i] = 0;
+            sm.gid[i] = 0;
+            sm.gid_slot[0] = i;
+            misc[0] = 1;
+            misc[2] = 1;
+        }
+        __syncthreads();
+        const HighItem item = B.items[it];
+        const HighTask& tk = B.tasks[item.task];
+        HighDst D;
+        D.T = tk.T;
+        D.cap_mask = uint64_t(tk.T.capacity - 1);
+        D.deferred = B.deferred;
+        D.deferred_cap = B.deferred_cap;
+        D.ndeferred = &B.counters->ndeferred;
+        D.spill = B.spill;
+        D.spill_cap = B.spill_cap;
+        D.nspill = &B.counters->nspill;
+        D.error = &B.counters->error;
+        D.tag = item.task;
+
+        uint64_t ckey[kPrivGroups];
+        int cgid[kPrivGroups];
+#pragma unroll
+        for (int j = 0; j < kPrivGroups; ++j) {
+            ckey[j] = kEmptyKey;
+            cgid[j] = -1;
+        }
+        int ncache = 0;
+        if (P.nkeyparts == 0) {
+            ckey[0] = 0;
+            cgid[0] = 0;
+            ncache = 1;
+        }
+        const char* cb[kFastCols];
+#pragma unroll
+        for (int c = 0; c < kFastCols; ++c) {
+            cb[c] = nullptr;
+            if (c < SIG::Cols::n) cb[c] = tk.cols[c] + item.row0 * SIG::cw(c);
+        }
+        const uint8_t* sel = tk.sel ? tk.sel + item.row0 : nullptr;
+        const int64_t n = item.nrows;
+        // Columns of every task start on a four-value boundary and selections
+        // on a four-byte one (checked by the host), so full quads take vector
+        // loads; items start on a multiple of four rows.
+#pragma unroll 1
+        for (int64_t r4 = int64_t(tid >> 5) * kWarpRows + lane * kQuadRows; r4 < n; r4 += (bd >> 5) * kWarpRows) {
+            const int nvalid = int(min(int64_t(kQuadRows), n - r4));
+            int64_t q[NC][kQuadRows];
+            LoadQuad<SIG>(q, cb, r4, nvalid);
+            uint32_t selq = nvalid == kQuadRows ? 0x01010101u : 0u;
+            if (nvalid < kQuadRows) {
+                for (int j = 0; j < nvalid; ++j) selq |= 1u << (8 * j);
+            }
+            if (sel) {
+                if (nvalid == kQuadRows) {
+                    selq = __ldcs(reinterpret_cast<const unsigned int*>(sel + r4));
+                } else {
+                    uint32_t m = 0;
+                    for (int j = 0; j < nvalid; ++j) m |= uint32_t(sel[r4 + j]) << (8 * j);
+                    selq = m;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kQuadRows; ++j) {
+                if (((selq >> (8 * j)) & 0xffu) == 0) continue;
+                RegRow<SIG::Cols::n> cur;
+                QuadRow<SIG>(cur, q, j);
+                if (SIG::Atoms::n && ShapeHeld<SIG>(P, F, cur) != F.clause_mask) continue;
+                const uint64_t key = ShapeKey<SIG>(cur);
+                int g = -1;
+#pragma unroll
+                for (int k = 0; k < kPrivGroups; ++k) g = ckey[k] == key ? cgid[k] : g;
+                const bool special = P.key_full64 && key == kEmptyKey;
+                int slot = -1;
+                if (g < 0 && !special) {
+                    slot = sm.Find(key);
+                    if (slot >= 0) {
+                        const int gg = *reinterpret_cast<volatile int*>(&sm.gid[slot]);
+                        if (gg >= 0 && gg < kPrivGroups && ncache < kPrivGroups) {
+                            g = gg;
+#pragma unroll
+                            for (int k = 0; k < kPrivGroups; ++k) {
+                                if (k == ncache) {
+                                    ckey[k] = key;
+                                    cgid[k] = gg;
+                                }
+                            }
+                            ++ncache;
+                        }
+                    }
+                }
+                if (g >= 0) {
+                    ShapeFoldP<SIG, kQuadThreads>(pacc + g * SIG::words * kQuadThreads + tid, F, cur);
+                } else if (slot >= 0) {
+                    ShapeVals<SIG> v;
+                    ShapeRowVals<SIG>(v, F, cur);
+                    ShapeSmemAtomics<SIG>(sm.st + slot, sm.S, v);
+                } else {
+                    // The tier is full, or the key is the empty marker: the
+                    // aggregate's own table (its flag slot for the marker).
+                    ShapeVals<SIG> v;
+                    ShapeRowVals<SIG>(v, F, cur);
+                    uint64_t* gw = D.T.slots + D.T.capacity * D.T.slot_words;
+                    if (special) {
+                        auto* flag = reinterpret_cast<unsigned long long*>(gw + D.T.key_off);
+                        if (*reinterpret_cast<volatile unsigned long long*>(flag) == 0 && atomicExch(flag, 1ull) == 0)
+                            atomicAdd(sm.fresh, 1u);
+                        ShapeAtomics<SIG>(gw + D.T.state_off, 1, v);
+                    } else {
+                        int is_new = 0;
+                        const int64_t gs = GlobalFindH(D.T, D.cap_mask, Fmix64(key), key, is_new);
+                        if (is_new) atomicAdd(sm.fresh, 1u);
+                        if (gs < 0) {
+                            DeferTo(D, item.row0 + r4 + j);   // replayed after the table grows
+                        } else {
+                            ShapeAtomics<SIG>(D.T.slots + gs * D.T.slot_words + D.T.state_off, 1, v);
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // Lane-private accumulators -> shared tier.
+        const int ng = int(min(*reinterpret_cast<volatile unsigned*>(sm.ngid), unsigned(kPrivGroups)));
+        constexpr int nwarps = bd >> 5;
+        for (int w = tid >> 5; w < ng * SIG::n; w += nwarps) {
+            const int qg = w / SIG::n;
+            const int st2 = w - qg * SIG::n;
+            const int o = SIG::off(st2);
+            const bool wide2 = SIG::width(st2) == 2;
+            uint64_t lo = 0, hi = 0;
+            for (int t2 = lane; t2 < bd; t2 += 32) {
+                const uint64_t* src = pacc + int64_t(qg * SIG::words + o) * bd + t2;
+                Add128(lo, hi, src[0], wide2 ? src[bd] : 0ull);
+            }
+            WarpSum128(lo, hi);
+            if (lane == 0 && (lo | hi)) {
+                const int slot = *reinterpret_cast<volatile int*>(&sm.gid_slot[qg]);
+                const StateDesc sd = P.states[st2];
+                uint64_t* dst = sm.st + int64_t(sd.word) * sm.S + slot;
+                ApplyState(dst, dst + sm.S, sd.kind, lo, hi, 0.0);
+            }
+        }
+        __syncthreads();
+        // Shared tier -> the aggregate's table (tagged spill when it is full).
+        const int rec_words = 2 + P.state_words;
+        for (int i = tid; i < sm.S; i += bd) {
+            const uint64_t key = sm.keys[i];
+            if (key == kEmptyKey) continue;
+            int is_new = 0;
+            const int64_t g = GlobalFindH(D.T, D.cap_mask, Fmix64(key), key, is_new);
+            if (is_new) atomicAdd(sm.fresh, 1u);
+            if (g < 0) {
+                const unsigned long long e = atomicAdd(D.nspill, 1ull);
+                if (int64_t(e) >= D.spill_cap) {
+                    SetError(D.error, DE_SPILL_FULL);
+                    continue;
+                }
+                uint64_t* rec = D.spill + int64_t(e) * rec_words;
+                rec[0] = key;
+                for (int w = 0; w < P.state_words; ++w) rec[1 + w] = sm.st[int64_t(w) * sm.S + i];
+                rec[1 + P.state_words] = uint64_t(D.tag);
+                continue;
+            }
+            uint64_t* gbase = D.T.slots + g * D.T.slot_words + D.T.state_off;
+            for (int st2 = 0; st2 < P.nstates; ++st2) {
+                const StateDesc sd = P.states[st2];
+                const uint64_t lo = sm.st[int64_t(sd.word) * sm.S + i];
+                const uint64_t hi = sd.kind == ST_SUM_I128 ? sm.st[int64_t(sd.word + 1) * sm.S + i] : 0;
+                if (IsIdentity(sd.kind, lo, hi)) continue;
+                ApplyState(gbase + sd.word, gbase + sd.word + 1, sd.kind, lo, hi, 0.0);
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && sm.fresh[0]) atomicAdd(&B.new_groups[item.task], (unsigned long long)sm.fresh[0]);
+    }
 }
 
 // The instantiated query shapes.  QDB_C(w, u): a fast column of w bytes
@@ -3158,21 +3422,45 @@ struct BatchFns {
     void (*replay)(AggLaunch, HighBatch, const int64_t*, int64_t) = nullptr;
 };
 
-BatchFns FindBatchKernels(const AggPlan& P, const FastPlan& F) {
+// High-cardinality programs take AggHighBatchKernel (a shared tier in front
+// of each aggregate's table); low-cardinality ones AggSigQuadBatchKernel,
+// whose lane-private accumulators keep a handful of groups from piling every
+// row's atomics onto a few shared slots.
+BatchFns FindBatchKernels(const AggPlan& P, const FastPlan& F, bool low) {
     BatchFns b;
     const std::vector<int> key = ShapeKeyOf(P, F);
     if (key.empty()) return b;
-#define QDB_SHAPE_FIND(...)                                                           \
+#define QDB_SHAPE_FIND(KERNEL, ...)                                                   \
     if (!b.update && ShapeMatches<__VA_ARGS__>(key) && ShapeWordsMatch<__VA_ARGS__>(F)) { \
-        b.update = AggHighBatchKernel<__VA_ARGS__>;                                   \
+        b.update = KERNEL<__VA_ARGS__>;                                               \
         b.replay = AggBatchReplayKernel<__VA_ARGS__>;                                 \
     }
-    // High-cardinality shapes only: the few groups of a low-cardinality
-    // program would pile every row's atomics onto a handful of shared slots;
-    // its states take the one-state path (lane-private accumulators).
-    QDB_HIGH_SHAPE_LIST(QDB_SHAPE_FIND)
+#define QDB_SHAPE_FIND_HIGH(...) QDB_SHAPE_FIND(AggHighBatchKernel, __VA_ARGS__)
+#define QDB_SHAPE_FIND_LOW(...) QDB_SHAPE_FIND(AggSigQuadBatchKernel, __VA_ARGS__)
+    if (low) {
+        QDB_SHAPE_LIST(QDB_SHAPE_FIND_LOW)
+    } else {
+        QDB_HIGH_SHAPE_LIST(QDB_SHAPE_FIND_HIGH)
+    }
+#undef QDB_SHAPE_FIND_LOW
+#undef QDB_SHAPE_FIND_HIGH
 #undef QDB_SHAPE_FIND
     return b;
+}
+
+// Shared memory of AggSigQuadBatchKernel: misc words, the kQuadSlots-slot
+// tier (keys, states, group ids), then kPrivGroups groups of lane-private
+// words per thread.  Sets the launch's offsets; returns the bytes.
+constexpr int kQuadSlots = 64;
+
+size_t QuadBatchLayout(AggLaunch& L) {
+    const int S = kQuadSlots;
+    L.off_misc = 0;
+    L.off_skeys = 128;
+    L.off_sst = L.off_skeys + S * 8;
+    L.off_gid = L.off_sst + S * L.P.state_words * 8;
+    L.off_pacc = int(Align(L.off_gid + S * 4, 16));
+    return size_t(L.off_pacc) + size_t(kPrivGroups) * L.P.state_words * kQuadThreads * 8;
 }
 
 AggLaunch& BatchLaunchOf(const AggPlan& p, const FastPlan& f, int smem_slots) {
@@ -3188,23 +3476,34 @@ AggLaunch& BatchLaunchOf(const AggPlan& p, const FastPlan& f, int smem_slots) {
     return L;
 }
 
+// The launch's block shape: the low-cardinality kernel has a fixed one.
+size_t BatchSmemOf(AggLaunch& L, bool low, int smem_slots, int& threads) {
+    if (!low) return size_t(HighLayoutOf(smem_slots, L.P.state_words).bytes);
+    threads = kQuadThreads;
+    L.smem_slots = kQuadSlots;
+    L.smem_limit = kQuadSlots / 2;
+    L.priv = 1;
+    return QuadBatchLayout(L);
+}
+
 }  // namespace
 
-std::string AggBatchShapeKey(const AggPlan& p, const FastPlan& f) {
-    std::string k;
+std::string AggBatchShapeKey(const AggPlan& p, const FastPlan& f, bool low) {
+    std::string k = low ? "low:" : "high:";
     for (int v : ShapeKeyOf(p, f)) k += std::to_string(v) + ",";
     return k;
 }
 
-bool AggBatchSupported(const AggPlan& p, const FastPlan& f) {
-    return p.key_words <= 1 && FindBatchKernels(p, f).update != nullptr;
+bool AggBatchSupported(const AggPlan& p, const FastPlan& f, bool low) {
+    return p.key_words <= 1 && FindBatchKernels(p, f, low).update != nullptr;
 }
 
-int AggBatchOccupancy(const AggPlan& p, const FastPlan& f, int threads, int smem_slots) {
+int AggBatchOccupancy(const AggPlan& p, const FastPlan& f, int threads, int smem_slots, bool low) {
     EnsureDeviceInfo();
-    const BatchFns fns = FindBatchKernels(p, f);
+    const BatchFns fns = FindBatchKernels(p, f, low);
     if (!fns.update) return 0;
-    const size_t bytes = size_t(HighLayoutOf(smem_slots, p.state_words).bytes) + 64;
+    AggLaunch& L = BatchLaunchOf(p, f, smem_slots);
+    const size_t bytes = BatchSmemOf(L, low, smem_slots, threads) + 64;
     if (bytes > g_smem_optin) return 0;
     SetSmem(fns.update, bytes);
     int n = 0;
@@ -3216,22 +3515,22 @@ int AggBatchOccupancy(const AggPlan& p, const FastPlan& f, int threads, int smem
 }
 
 void AggBatchUpdate(const AggPlan& p, const FastPlan& f, const HighBatch& b, int threads, int smem_slots, int grid,
-                    cudaStream_t s) {
+                    cudaStream_t s, bool low) {
     EnsureDeviceInfo();
-    const BatchFns fns = FindBatchKernels(p, f);
+    const BatchFns fns = FindBatchKernels(p, f, low);
     AggLaunch& L = BatchLaunchOf(p, f, smem_slots);
-    const size_t bytes = size_t(HighLayoutOf(smem_slots, p.state_words).bytes);
+    const size_t bytes = BatchSmemOf(L, low, smem_slots, threads);
     SetSmem(fns.update, bytes + 64);
-    ProfileBegin(s, "agg_batch_update", b.nitems);
+    ProfileBegin(s, low ? "agg_batch_update_low" : "agg_batch_update", b.nitems);
     fns.update<<<grid, threads, bytes, s>>>(L, b);
     ProfileEnd(s);
     CountLaunch();
 }
 
 void AggBatchReplay(const AggPlan& p, const FastPlan& f, const HighBatch& b, const int64_t* pairs, int64_t n,
-                    cudaStream_t s) {
+                    cudaStream_t s, bool low) {
     if (n <= 0) return;
-    const BatchFns fns = FindBatchKernels(p, f);
+    const BatchFns fns = FindBatchKernels(p, f, low);
     AggLaunch& L = BatchLaunchOf(p, f, 0);
     ProfileBegin(s, "agg_batch_replay", n);
     fns.replay<<<int((n + 255) / 256), 256, 0, s>>>(L, b, pairs, n);

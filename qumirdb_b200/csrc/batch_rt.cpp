@@ -48,6 +48,17 @@ struct BatchConfig {
     int64_t chunk_rows = int64_t(1) << 17;
 };
 
+// The low-cardinality kernel's block shape is fixed: 256 threads, a 64-slot
+// shared tier.
+BatchConfig DefaultConfig(bool low) {
+    BatchConfig c;
+    if (low) {
+        c.threads = 256;
+        c.smem_slots = 64;
+    }
+    return c;
+}
+
 constexpr int64_t kTuneMinRows = int64_t(16) << 20;   // rows in a batch worth a search
 
 int SizeClass(int64_t rows) {
@@ -65,6 +76,8 @@ struct Tuner {
     int64_t trials = 0;     // candidate launches timed
     int64_t reused = 0;     // batches served from a stored choice
     int64_t resized = 0;    // launches run again with tables for one group per row
+    int64_t states_low = 0;   // states updated by the low-cardinality batched kernel
+    int64_t states_high = 0;  // ... and by the high-cardinality one
 };
 
 Tuner& Tune() {
@@ -188,29 +201,30 @@ void BuildItems(const std::vector<int64_t>& rows, const std::vector<int>& order,
     }
 }
 
-int GridFor(const AggPlan& p, const FastPlan& f, const BatchConfig& c, int64_t nitems) {
-    const int occ = std::max(1, AggBatchOccupancy(p, f, c.threads, c.smem_slots));
+int GridFor(const AggPlan& p, const FastPlan& f, const BatchConfig& c, int64_t nitems, bool low) {
+    const int occ = std::max(1, AggBatchOccupancy(p, f, c.threads, c.smem_slots, low));
     return int(std::max<int64_t>(1, std::min<int64_t>(nitems, int64_t(DeviceSMs()) * occ)));
 }
 
 // Runs one batched update of `nitems` items whose tasks and items are
 // already in the context's device buffers.
 void LaunchUpdate(BatchContext& cx, const AggPlan& p, const FastPlan& f, const BatchConfig& c, int64_t ntasks,
-                  int64_t nitems, int grid, cudaStream_t s) {
+                  int64_t nitems, int grid, cudaStream_t s, bool low) {
     HighBatch b = cx.Desc(nitems);
     b.spill_cap = cx.spill_cap / (2 + p.state_words);
     cudaMemsetAsync(cx.d_counters, 0, sizeof(BatchCounters), s);
     cudaMemsetAsync(cx.d_new, 0, size_t(ntasks) * 8, s);
-    AggBatchUpdate(p, f, b, c.threads, c.smem_slots, grid, s);
+    AggBatchUpdate(p, f, b, c.threads, c.smem_slots, grid, s, low);
 }
 
 // Chooses the block shape and item size for a batch: coordinate search
-// over item size, shared-tier slots and threads per CTA, each candidate
+// over item size, shared-tier slots and threads per CTA (item size only for
+// the low-cardinality kernel, whose block shape is fixed), each candidate
 // timed (best of two) on a sample of the batch's states folded into
 // scratch tables sized like theirs.
 BatchConfig Search(const AggPlan& p, const FastPlan& f, const std::vector<HighTask>& tasks,
-                   const std::vector<int64_t>& caps, cudaStream_t s) {
-    BatchConfig best;
+                   const std::vector<int64_t>& caps, cudaStream_t s, bool low) {
+    BatchConfig best = DefaultConfig(low);
     // Sample: states spread over the size order, up to 64 states / 32M rows.
     std::vector<int> order(tasks.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = int(i);
@@ -270,7 +284,8 @@ BatchConfig Search(const AggPlan& p, const FastPlan& f, const std::vector<HighTa
         for (int rep = 0; rep < 2; ++rep) {
             AggBatchInitTables(p, all, cx.d_tasks, int(st.size()), s);
             cudaEventRecord(e0, s);
-            LaunchUpdate(cx, p, f, c, int64_t(st.size()), int64_t(items.size()), GridFor(p, f, c, int64_t(items.size())), s);
+            LaunchUpdate(cx, p, f, c, int64_t(st.size()), int64_t(items.size()),
+                         GridFor(p, f, c, int64_t(items.size()), low), s, low);
             cudaEventRecord(e1, s);
             cudaEventSynchronize(e1);
             float ms = 0.f;
@@ -291,19 +306,20 @@ BatchConfig Search(const AggPlan& p, const FastPlan& f, const std::vector<HighTa
         }
     }
     for (int S : {1024, 4096}) {
+        if (low) break;
         BatchConfig c = best;
         c.smem_slots = S;
-        if (AggBatchOccupancy(p, f, c.threads, S) < 1) continue;
+        if (AggBatchOccupancy(p, f, c.threads, S, low) < 1) continue;
         const float ms = trial(c);
         if (ms < cur) {
             cur = ms;
             best = c;
         }
     }
-    {
+    if (!low) {
         BatchConfig c = best;
         c.threads = 512;
-        if (AggBatchOccupancy(p, f, c.threads, c.smem_slots) >= 1) {
+        if (AggBatchOccupancy(p, f, c.threads, c.smem_slots, low) >= 1) {
             const float ms = trial(c);
             if (ms < cur) best = c;
         }
@@ -470,6 +486,18 @@ int64_t DispatchBatch(const qdb_gpu_program* prog, void* const* hts, qdb_rowset*
     FastPlan fast{};
     bool have_fast = false;
     AggPlan P0 = lw.plan;
+    // A few groups per aggregate (the planner's hint, or none at all): the
+    // low-cardinality kernel, whose typed columns must start on a boundary of
+    // four values (and a selection on one of four bytes).
+    const bool low = lw.plan.nkeyparts == 0 || (prog->expected_groups > 0 && prog->expected_groups <= 64);
+    auto typed_ok = [&](const HighTask& t) {
+        if (!low) return true;
+        for (int c = 0; c < fast.ncols && c < kFastCols; ++c) {
+            const int w = int(P0.cols[fast.col_slot[c]].width);
+            if (reinterpret_cast<uintptr_t>(t.cols[c]) % uintptr_t(std::min(16, 4 * w))) return false;
+        }
+        return (reinterpret_cast<uintptr_t>(t.sel) & 3) == 0;
+    };
     for (int64_t i = 0; i < n; ++i) {
         if (!hts[i] || !batches[i]) {
             SetErr("agg_dispatch_batch: state or batch %lld is NULL", (long long)i);
@@ -478,18 +506,18 @@ int64_t DispatchBatch(const qdb_gpu_program* prog, void* const* hts, qdb_rowset*
         rows[size_t(i)] = batches[i]->RowCount;
         if (have_fast) {
             typed[size_t(i)] = ResolveShapeColumns(P0, fast, lw.cols, prog->columns.data(), batches[i], stg,
-                                                   resolved[size_t(i)]) ? 1 : 0;
+                                                   resolved[size_t(i)]) && typed_ok(resolved[size_t(i)]) ? 1 : 0;
             continue;
         }
         AggPlan pi = lw.plan;
         if (!ResolveColumns(pi, lw.cols, prog->columns.data(), batches[i], stg)) return -1;
         FastPlan fi{};
-        if (MatchFast(pi, fi) && AggBatchSupported(pi, fi)) {
+        if (MatchFast(pi, fi) && AggBatchSupported(pi, fi, low)) {
             fast = fi;
             have_fast = true;
             P0 = pi;
             typed[size_t(i)] = ResolveShapeColumns(P0, fast, lw.cols, prog->columns.data(), batches[i], stg,
-                                                   resolved[size_t(i)]) ? 1 : 0;
+                                                   resolved[size_t(i)]) && typed_ok(resolved[size_t(i)]) ? 1 : 0;
         }
     }
     // States outside the batched kernel (no compiled shape, nullable columns)
@@ -512,7 +540,12 @@ int64_t DispatchBatch(const qdb_gpu_program* prog, void* const* hts, qdb_rowset*
         MirrorHeader(hts[i], st, lw.plan);
     }
     if (members.empty()) return n;
-    const std::string shape = AggBatchShapeKey(P0, fast);
+    const std::string shape = AggBatchShapeKey(P0, fast, low);
+    {
+        Tuner& tn = Tune();
+        std::lock_guard<std::mutex> lk(tn.mu);
+        (low ? tn.states_low : tn.states_high) += int64_t(members.size());
+    }
     const int sw = SlotWords(lw.plan, false);
     const int64_t m = int64_t(members.size());
 
@@ -603,7 +636,7 @@ int64_t DispatchBatch(const qdb_gpu_program* prog, void* const* hts, qdb_rowset*
     // nearest size class of the shape (a search costs tens of launches, so
     // a shape is searched once and its later batches, of whatever mix, reuse
     // the nearest choice); a shape never searched is searched now.
-    BatchConfig cfg;
+    BatchConfig cfg = DefaultConfig(low);
     bool found = false;
     {
         Tuner& tn = Tune();
@@ -630,7 +663,7 @@ int64_t DispatchBatch(const qdb_gpu_program* prog, void* const* hts, qdb_rowset*
     if (!found && TuningEnabled() && worth_tuning) {
         // Fresh tables must be initialised before the search reuses the
         // context's device buffers; it runs on scratch tables of its own.
-        cfg = Search(P0, fast, tasks, caps, s);
+        cfg = Search(P0, fast, tasks, caps, s, low);
         Tuner& tn = Tune();
         std::lock_guard<std::mutex> lk(tn.mu);
         tn.best[{shape, rows_class, states_class}] = cfg;
@@ -670,11 +703,11 @@ int64_t DispatchBatch(const qdb_gpu_program* prog, void* const* hts, qdb_rowset*
 
     // The launch sequence: as a replayed graph while the batch's structure
     // holds, else eagerly (and always eagerly while kernels are timed).
-    const int grid = GridFor(P0, fast, cfg, nitems);
+    const int grid = GridFor(P0, fast, cfg, nitems, low);
     auto record = [&](cudaStream_t st) {
         cudaMemcpyAsync(cx.d_tasks, cx.h_tasks, size_t(m) * sizeof(HighTask), cudaMemcpyHostToDevice, st);
         if (nitems) cudaMemcpyAsync(cx.d_items, cx.h_items, size_t(nitems) * sizeof(HighItem), cudaMemcpyHostToDevice, st);
-        LaunchUpdate(cx, P0, fast, cfg, m, nitems, grid, st);
+        LaunchUpdate(cx, P0, fast, cfg, m, nitems, grid, st, low);
         cudaMemcpyAsync(cx.h_new, cx.d_new, size_t(m) * 8, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(cx.h_counters, cx.d_counters, sizeof(BatchCounters), cudaMemcpyDeviceToHost, st);
     };
@@ -988,13 +1021,16 @@ int64_t qdb_gpu_autotune_info(char* buf, int64_t cap) {
     std::string js = "{\"searches\": " + std::to_string(t.tuned) + ", \"trials\": " + std::to_string(t.trials) +
                      ", \"reused\": " + std::to_string(t.reused) +
                      ", \"resized\": " + std::to_string(t.resized) +
-                     ", \"graph_replays\": " + std::to_string(Ctx().graph_replays) + ", \"configs\": [";
+                     ", \"graph_replays\": " + std::to_string(Ctx().graph_replays) +
+                     ", \"batched_states\": {\"low\": " + std::to_string(t.states_low) +
+                     ", \"high\": " + std::to_string(t.states_high) + "}, \"configs\": [";
     bool first = true;
     for (auto& kv : t.best) {
         char e[256];
-        std::snprintf(e, sizeof(e), "%s{\"rows_class\": %d, \"states_class\": %d, \"threads\": %d, \"smem_slots\": %d, "
-                                    "\"chunk_rows\": %lld}",
-                      first ? "" : ", ", std::get<1>(kv.first), std::get<2>(kv.first), kv.second.threads,
+        const bool low = std::get<0>(kv.first).rfind("low:", 0) == 0;
+        std::snprintf(e, sizeof(e), "%s{\"class\": \"%s\", \"rows_class\": %d, \"states_class\": %d, \"threads\": %d, "
+                                    "\"smem_slots\": %d, \"chunk_rows\": %lld}",
+                      first ? "" : ", ", low ? "low" : "high", std::get<1>(kv.first), std::get<2>(kv.first), kv.second.threads,
                       kv.second.smem_slots, (long long)kv.second.chunk_rows);
         js += e;
         first = false;
@@ -1014,6 +1050,7 @@ void qdb_gpu_autotune_reset(void) {
     t.best.clear();
     t.ratio.clear();
     t.tuned = t.trials = t.reused = t.resized = 0;
+    t.states_low = t.states_high = 0;
 }
 
 }  // extern "C"

@@ -579,13 +579,13 @@ void JoinSumRun(const JoinSumShape& shape, const JTableDev& jt, int64_t nrows, u
 // Batched join-sum probe: many small joins of one program (the partitions of
 // a partitioned join, or the joins of many queries of one template) in one
 // persistent launch.  A warp pulls a work item (join, range of at most
-// kJsBatchItemRows probe rows), probes one row per lane per step against that
+// 16K probe rows), probes two rows per lane per step against that
 // join's bucket table (left in L2: small tables, no staging or Bloom filter),
 // and ends the item with a warp reduction and one atomic add per state word.
 // ---------------------------------------------------------------------------
 namespace {
 
-constexpr int kJsBatchRows = 4;   // rows per lane per step
+constexpr int kJsBatchRows = 2;   // rows per lane per step
 
 struct JsBatchLaunch {
     JoinSumShape S;
@@ -606,7 +606,7 @@ __device__ __forceinline__ uint64_t JsBatchTerm(const JsState& st, uint64_t pay,
     return v;
 }
 
-__global__ void __launch_bounds__(256) JoinSumBatchKernel(const __grid_constant__ JsBatchLaunch L) {
+__global__ void __launch_bounds__(256, 4) JoinSumBatchKernel(const __grid_constant__ JsBatchLaunch L) {
     const int lane = LaneId();
     for (;;) {
         unsigned it = 0;
@@ -628,8 +628,9 @@ __global__ void __launch_bounds__(256) JoinSumBatchKernel(const __grid_constant_
                 if (s < L.S.nstates) v[s] += JsBatchTerm(L.S.states[s], pay, sv);
             }
         };
-        // Four coalesced 32-row slabs per step: every lane's four key loads,
-        // then its four bucket reads, are in flight together.
+        // Two coalesced 32-row slabs per step: every lane's key loads, then
+        // its bucket reads, are in flight together (two rows per lane keep
+        // 60 registers, so that four CTAs fit an SM).
         for (int64_t r0 = item.lo + lane; r0 < item.hi; r0 += 32 * kJsBatchRows) {
             uint64_t key[kJsBatchRows];
             int64_t sv[kJsBatchRows];
@@ -692,7 +693,9 @@ void JoinSumBatchRun(const JoinSumShape& shape, const JsBatchJoin* joins, const 
     L.items = items;
     L.nitems = nitems;
     L.next = next;
-    const int warps = int(std::min<int64_t>(nitems, int64_t(DeviceSMs()) * 64));
+    // Four CTAs of eight warps per SM (64 registers each), fewer when there
+    // are fewer items than warps.
+    const int warps = int(std::min<int64_t>(nitems, int64_t(DeviceSMs()) * 32));
     ProfileBegin(s, "join_agg_probe_batch", nitems);
     JoinSumBatchKernel<<<(warps + 7) / 8, 256, 0, s>>>(L);
     ProfileEnd(s);

@@ -1060,7 +1060,9 @@ namespace qdb {
 
 namespace {
 
-constexpr int64_t kBatchItemRows = 65536;
+// Rows per work item of the batched launches: enough items to keep every
+// warp of the persistent probe busy on a partitioned 120M-row probe.
+constexpr int64_t kBatchItemRows = 16384;
 
 void AddItems(std::vector<JoinBatchItem>& items, int32_t join, int64_t n) {
     for (int64_t lo = 0; lo < n; lo += kBatchItemRows) {

@@ -341,16 +341,21 @@ struct HighBatch {
     uint64_t* spill;                  // [key, states..., aggregate] records
     int64_t spill_cap;
 };
-// The program's batched kernel exists when its typed shape was compiled in.
-bool AggBatchSupported(const AggPlan& p, const FastPlan& f);
-// A name of the program's typed shape (the autotuner's key).
-std::string AggBatchShapeKey(const AggPlan& p, const FastPlan& f);
+// The program's batched kernel exists when its typed shape was compiled in
+// for its cardinality class (`low`: a few groups per aggregate, folded into
+// lane-private accumulators; else a shared tier in front of the table).  The
+// low-cardinality kernel has a fixed block shape (threads and shared-tier
+// slots are ignored) and wants every task's columns on a four-value boundary
+// and its selection on a four-byte one.
+bool AggBatchSupported(const AggPlan& p, const FastPlan& f, bool low);
+// A name of the program's typed shape and class (the autotuner's key).
+std::string AggBatchShapeKey(const AggPlan& p, const FastPlan& f, bool low);
 // Resident CTAs per SM of the batched kernel at this block shape.
-int AggBatchOccupancy(const AggPlan& p, const FastPlan& f, int threads, int smem_slots);
+int AggBatchOccupancy(const AggPlan& p, const FastPlan& f, int threads, int smem_slots, bool low);
 void AggBatchUpdate(const AggPlan& p, const FastPlan& f, const HighBatch& b, int threads, int smem_slots, int grid,
-                    cudaStream_t s);
+                    cudaStream_t s, bool low);
 void AggBatchReplay(const AggPlan& p, const FastPlan& f, const HighBatch& b, const int64_t* pairs, int64_t n,
-                    cudaStream_t s);
+                    cudaStream_t s, bool low);
 void AggBatchSpill(const AggPlan& p, const HighBatch& b, const uint64_t* recs, int64_t n, cudaStream_t s);
 // Initialises `total` slots laid out like the tables of `tasks` (contiguous
 // tables of one slot layout), then marks each table's one-word-key flag slot

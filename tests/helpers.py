@@ -7,7 +7,7 @@ import math
 import numpy as np
 
 import qumirdb_b200 as q
-from qumirdb_b200 import abi
+from qumirdb_b200 import abi, queries
 
 F64_REL = 1e-12
 
@@ -68,3 +68,32 @@ def zipf_data(n: int, distinct: int, seed: int = 2):
     cols = [np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.float64)]
     q.lib().qdb_gen_zipf(seed, n, distinct, 1.1, *[c.ctypes.data for c in cols])
     return cols
+
+
+def shape_case(shape, groups, n, rng):
+    """(columns, spec, output types) of a plan whose shape is compiled in the
+    listed-row kernel's catalogue."""
+    k = rng.integers(0, groups, n).astype(np.int64) * 1009 + 5
+    a = rng.integers(-10**12, 10**12, n).astype(np.int64)
+    e = q.ExprBuilder()
+    if shape == "count":
+        kc = e.col(0, abi.I64)
+        spec = queries.AggSpec([(abi.I64,)], e, None, [kc], [(abi.COUNT_STAR, -1)], expected_groups=64)
+        return [k], spec, [abi.I64, abi.I64]
+    if shape == "sum_count":
+        kc, ac = e.col(0, abi.I64), e.col(1, abi.I64)
+        spec = queries.AggSpec([(abi.I64,), (abi.I64,)], e, None, [kc], [(abi.SUM, ac), (abi.COUNT_STAR, -1)],
+                               expected_groups=64)
+        return [k, a], spec, [abi.I64, abi.I64, abi.I64]
+    if shape == "q6":
+        x = rng.integers(0, 1000, n).astype(np.int64)
+        xc, ac = e.col(0, abi.I64), e.col(1, abi.I64)
+        filt = e.op(abi.BETWEEN, abi.BOOL, xc, e.const(100, abi.I64), e.const(700, abi.I64))
+        spec = queries.AggSpec([(abi.I64,), (abi.I64,)], e, filt, [], [(abi.SUM, e.op(abi.MUL, abi.I64, xc, ac))],
+                               expected_groups=1)
+        return [x, a], spec, [abi.I64]
+    # lineitem shape with `groups` flag codes (two one-byte keys).
+    cols = lineitem(n, seed=9)
+    cols[4] = (rng.integers(0, groups, n) + 65).astype(np.uint8)
+    spec = queries.lineitem_agg(int(cols[6].max()) - 90)
+    return cols, spec, queries.LINEITEM_OUT_TYPES

@@ -6,7 +6,7 @@ import qumirdb_b200 as q
 from oracle import oracle as O
 from qumirdb_b200 import abi, queries
 
-from .helpers import assert_same_groups, gpu_rows, lineitem, zipf_data
+from .helpers import assert_same_groups, gpu_rows, lineitem, shape_case, zipf_data
 
 pytestmark = pytest.mark.gpu
 
@@ -169,35 +169,6 @@ def test_device_output_stays_resident():
     q.release(out)
 
 
-def _shape_case(shape, groups, n, rng):
-    """(columns, spec, output types) of a plan whose shape is compiled in the
-    listed-row kernel's catalogue."""
-    k = rng.integers(0, groups, n).astype(np.int64) * 1009 + 5
-    a = rng.integers(-10**12, 10**12, n).astype(np.int64)
-    e = q.ExprBuilder()
-    if shape == "count":
-        kc = e.col(0, abi.I64)
-        spec = queries.AggSpec([(abi.I64,)], e, None, [kc], [(abi.COUNT_STAR, -1)], expected_groups=64)
-        return [k], spec, [abi.I64, abi.I64]
-    if shape == "sum_count":
-        kc, ac = e.col(0, abi.I64), e.col(1, abi.I64)
-        spec = queries.AggSpec([(abi.I64,), (abi.I64,)], e, None, [kc], [(abi.SUM, ac), (abi.COUNT_STAR, -1)],
-                               expected_groups=64)
-        return [k, a], spec, [abi.I64, abi.I64, abi.I64]
-    if shape == "q6":
-        x = rng.integers(0, 1000, n).astype(np.int64)
-        xc, ac = e.col(0, abi.I64), e.col(1, abi.I64)
-        filt = e.op(abi.BETWEEN, abi.BOOL, xc, e.const(100, abi.I64), e.const(700, abi.I64))
-        spec = queries.AggSpec([(abi.I64,), (abi.I64,)], e, filt, [], [(abi.SUM, e.op(abi.MUL, abi.I64, xc, ac))],
-                               expected_groups=1)
-        return [x, a], spec, [abi.I64]
-    # lineitem shape with `groups` flag codes (two one-byte keys).
-    cols = lineitem(n, seed=9)
-    cols[4] = (rng.integers(0, groups, n) + 65).astype(np.uint8)
-    spec = queries.lineitem_agg(int(cols[6].max()) - 90)
-    return cols, spec, queries.LINEITEM_OUT_TYPES
-
-
 @pytest.mark.parametrize("groups", [1, 3, 40])
 @pytest.mark.parametrize("shape", ["count", "sum_count", "q6", "lineitem"])
 def test_shape_kernels(shape, groups):
@@ -207,7 +178,7 @@ def test_shape_kernels(shape, groups):
     last ending in a partial tile."""
     rng = np.random.default_rng(7 + groups)
     n = 150_001
-    cols, spec, types = _shape_case(shape, groups, n, rng)
+    cols, spec, types = shape_case(shape, groups, n, rng)
     bounds = [(0, 70_000), (70_000, 140_000), (140_000, n)]
     q.profile(True)
     q.profile_read()

@@ -10,7 +10,7 @@ import qumirdb_b200 as q
 from oracle import oracle as O
 from qumirdb_b200 import abi, queries
 
-from .helpers import assert_same_groups, gpu_rows, lineitem, zipf_data
+from .helpers import assert_same_groups, gpu_rows, lineitem, shape_case, zipf_data
 
 pytestmark = pytest.mark.gpu
 
@@ -177,3 +177,39 @@ def test_same_shape_programs_with_other_literals_do_not_share_a_graph(form):
         for i in range(len(parts)):
             assert_same_groups(gpu_rows(outs[i], types), want[c][i], types, nkeys=1)
         outs.release()
+
+
+@pytest.mark.parametrize("shape,groups", [("lineitem", 6), ("q6", 1), ("count", 3), ("sum_count", 40),
+                                          ("sum_count", 5000)])
+def test_batch_low_cardinality_partitions(shape, groups):
+    """Uneven partitions (empty, a partial quad, up to 400K rows) of each
+    compiled low-cardinality shape in one batched launch of the
+    low-cardinality kernel: the first four groups of a work item in
+    lane-private accumulators, the next ones in the shared tier, the rest
+    (and, with 5000 groups against a hint of 64, the rows the full tables
+    turn away) through the tables and the replay.  Two updates per state;
+    every partition's groups equal the oracle's."""
+    rng = np.random.default_rng(31 + groups)
+    sizes = [0, 3, 4, 129, 5000] + [int(x) for x in np.exp(rng.uniform(np.log(1000), np.log(400_000), 27))]
+    cols, spec, types = shape_case(shape, groups, sum(sizes), rng)
+    bounds = np.concatenate([[0], np.cumsum(sizes)])
+    parts = [[c[lo:hi] for c in cols] for lo, hi in zip(bounds[:-1], bounds[1:])]
+    halves = ([[c[: len(p[0]) // 2 // 4 * 4] for c in p] for p in parts],
+              [[c[len(p[0]) // 2 // 4 * 4:] for c in p] for p in parts])
+    prog = q.compile_aggregate(spec)
+    before = q.autotune_info()["batched_states"]["low"]
+    q.profile(True)
+    q.profile_read()
+    batch = q.AggregateBatch(prog, len(parts))
+    for h in halves:
+        batch.add([q.DeviceRowSet(c) for c in h])
+    outs = batch.finish()
+    names = {k[0] for k in q.profile_read()}
+    q.profile(False)
+    assert "agg_batch_update_low" in names, names
+    assert q.autotune_info()["batched_states"]["low"] - before == 2 * len(parts)
+    nkeys = 0 if shape == "q6" else (2 if shape == "lineitem" else 1)
+    for p, o in zip(parts, outs):
+        want = O.aggregate(spec, [q.HostRowSet(p)])
+        assert_same_groups(gpu_rows(o, types), want, types, nkeys=nkeys)
+    outs.release()
