@@ -85,6 +85,8 @@ struct AggLaunch {
     JoinKeyPlan jk;
     JTableDev jt;
     FastPlan F;               // typed row shape (FAST kernels)
+    const uint64_t* seeds;    // high-cardinality kernel: keys pre-loaded into the shared tier
+    const int* nseed;         // their count (device), or seeds == nullptr
 };
 
 // ---------------------------------------------------------------------------
@@ -993,6 +995,13 @@ struct Shape {
         return o;
     }
     static constexpr int words = off(n);
+    // Word of the first COUNT state (every folded row adds one), or -1.
+    __host__ __device__ static constexpr int count_off() {
+        for (int s = 0; s < n; ++s) {
+            if (kind(s) == SK_COUNT) return off(s);
+        }
+        return -1;
+    }
     __host__ __device__ static constexpr int cw(int k) { return Cols::at(k) >> 1; }
     __host__ __device__ static constexpr bool cu(int k) { return (Cols::at(k) & 1) != 0; }
 };
@@ -1539,6 +1548,13 @@ __device__ __forceinline__ void ShapeFlush(const AggPlan& P, const HighDst& D, c
     for (int i = threadIdx.x; i < sm.S; i += blockDim.x) {
         const uint64_t key = sm.keys[i];
         if (key == kEmptyKey) continue;
+        if constexpr (SH::count_off() >= 0) {
+            // A seeded slot that no row of the range reached.
+            if (sm.st[int64_t(SH::count_off()) * sm.S + i] == 0) {
+                if (reset) sm.keys[i] = kEmptyKey;
+                continue;
+            }
+        }
         int is_new = 0;
         const int64_t g = GlobalFindH(D.T, D.cap_mask, Fmix64(key), key, is_new);
         if (is_new) atomicAdd(sm.fresh, 1u);
@@ -1611,6 +1627,19 @@ __global__ void __launch_bounds__(kHighThreads, 1) AggHighKernel(const __grid_co
     const HighSmem sm = HighSmemOf(L, hl);
     HighInit(L, sm);
     __syncthreads();
+    if (L.seeds) {
+        // The aggregate's most frequent keys take the tier first, so that the
+        // rows of the distribution's head fold in shared memory instead of
+        // each going to the global table before the tier fills with whatever
+        // came first.  A seed that none of this CTA's rows reached has a
+        // COUNT of 0 and is skipped at the flush (seeded shapes count rows).
+        const int ns = min(*L.nseed, sm.limit);
+        for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+            const uint64_t key = L.seeds[i];
+            sm.Find(Fmix64(key), key);
+        }
+        __syncthreads();
+    }
     const int64_t per = (L.nrows + gridDim.x - 1) / gridDim.x;
     const int64_t row0 = int64_t(blockIdx.x) * per;
     const int n = int(max(int64_t(0), min(per, L.nrows - row0)));
@@ -2014,7 +2043,7 @@ __device__ __forceinline__ void QuadRow(RegRow<SH::Cols::n>& row,
 // L2 prefetch of 128-row tile `t` of a range of n rows: the tile's w lines
 // of a w-byte column (and its selection bytes), one line per lane.  Rows
 // past the range are not touched.
-constexpr int kPrefetchTiles = 16;   // two tiles ahead for each of a CTA's eight warps
+constexpr int kQuadChunkTiles = 4;   // tiles a warp takes from the queue at a time
 
 template <class SH, int K = 0>
 __device__ __forceinline__ void QuadPrefetchTile(const char* const* cb, const uint8_t* sel, int64_t t, int64_t n,
@@ -2047,7 +2076,6 @@ __global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid
         misc[1] = 0;
         misc[2] = 0;
         misc[4] = 0;
-        misc[5] = 0;   // next 128-row tile of the range
     }
     for (int i = tid; i < sm.S; i += bd) {
         sm.keys[i] = kEmptyKey;
@@ -2085,12 +2113,12 @@ __global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid
         ncache = 1;
     }
 
-    // Contiguous range per CTA, a multiple of the 128-row warp tile.
+    // Every warp of the grid takes chunks of kQuadChunkTiles 128-row tiles
+    // from one queue, so that no SM idles at the end while another still has
+    // rows (a static split left the slowest SMs 20% behind the median).
     constexpr int kWarpRows = 32 * kQuadRows;
-    int64_t per = (L.nrows + gridDim.x - 1) / gridDim.x;
-    per = (per + kWarpRows - 1) / kWarpRows * kWarpRows;
-    const int64_t row0 = int64_t(blockIdx.x) * per;
-    const int64_t n = max(int64_t(0), min(per, L.nrows - row0));
+    constexpr int64_t row0 = 0;
+    const int64_t n = L.nrows;
     const char* cb[kFastCols];
 #pragma unroll
     for (int c = 0; c < kFastCols; ++c) {
@@ -2099,70 +2127,73 @@ __global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid
     }
     const uint8_t* sel = P.selection ? P.selection + row0 : nullptr;
     constexpr int NC = SIG::Cols::n > 0 ? SIG::Cols::n : 1;
-    // The warps of the CTA take the range's 128-row tiles from a shared
-    // counter, so that none idles at the closing barrier while another still
-    // has tiles; each asks the L2 for the tile kPrefetchTiles ahead of the one
-    // it takes (every tile is asked for once), so that the tile's loads meet
-    // it in L2 rather than in HBM.
-    const int64_t ntiles = (n + kWarpRows - 1) / kWarpRows;
-    unsigned* next_tile = misc + 5;
+    // Each warp asks the L2 for the chunk one round of the grid's warps ahead
+    // of the one it takes (every chunk is asked for once), so that the
+    // chunk's loads meet it in L2 rather than in HBM.
+    const int64_t nchunks = (n + kQuadChunkTiles * kWarpRows - 1) / (kQuadChunkTiles * kWarpRows);
+    const int64_t ahead = int64_t(gridDim.x) * (bd >> 5);
 #pragma unroll 1
     for (;;) {
-        unsigned t = 0;
-        if (lane == 0) t = atomicAdd(next_tile, 1u);
-        t = __shfl_sync(0xffffffffu, t, 0);
-        if (int64_t(t) >= ntiles) break;
-        QuadPrefetchTile<SIG>(cb, sel, int64_t(t) + kPrefetchTiles, n, lane);
-        const int64_t r4 = int64_t(t) * kWarpRows + lane * kQuadRows;
-        if (r4 >= n) continue;
-        const int nvalid = int(min(int64_t(kQuadRows), n - r4));
-        int64_t q[NC][kQuadRows];
-        LoadQuad<SIG>(q, cb, r4, nvalid);
-        uint32_t selq = nvalid == kQuadRows ? 0x01010101u : 0u;
-        if (nvalid < kQuadRows) {
-            for (int j = 0; j < nvalid; ++j) selq |= 1u << (8 * j);
-        }
-        if (sel) {
-            if (nvalid == kQuadRows) {
-                selq = __ldcs(reinterpret_cast<const unsigned int*>(sel + r4));
-            } else {
-                uint32_t m = 0;
-                for (int j = 0; j < nvalid; ++j) m |= uint32_t(sel[r4 + j]) << (8 * j);
-                selq = m;
+        unsigned c = 0;
+        if (lane == 0) c = atomicAdd(&L.counters->next_chunk, 1u);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (int64_t(c) >= nchunks) break;
+#pragma unroll 1
+        for (int k = 0; k < kQuadChunkTiles; ++k)
+            QuadPrefetchTile<SIG>(cb, sel, (int64_t(c) + ahead) * kQuadChunkTiles + k, n, lane);
+#pragma unroll 1
+        for (int k = 0; k < kQuadChunkTiles; ++k) {
+            const int64_t r4 = (int64_t(c) * kQuadChunkTiles + k) * kWarpRows + lane * kQuadRows;
+            if (r4 >= n) break;
+            const int nvalid = int(min(int64_t(kQuadRows), n - r4));
+            int64_t q[NC][kQuadRows];
+            LoadQuad<SIG>(q, cb, r4, nvalid);
+            uint32_t selq = nvalid == kQuadRows ? 0x01010101u : 0u;
+            if (nvalid < kQuadRows) {
+                for (int j = 0; j < nvalid; ++j) selq |= 1u << (8 * j);
             }
-        }
-#pragma unroll
-        for (int j = 0; j < kQuadRows; ++j) {
-            if (((selq >> (8 * j)) & 0xffu) == 0) continue;
-            RegRow<SIG::Cols::n> cur;
-            QuadRow<SIG>(cur, q, j);
-            if (SIG::Atoms::n && ShapeHeld<SIG>(P, F, cur) != F.clause_mask) continue;
-            const uint64_t key = ShapeKey<SIG>(cur);
-            int g = -1;
-#pragma unroll
-            for (int k = 0; k < kPrivGroups; ++k) g = ckey[k] == key ? cgid[k] : g;
-            if (g < 0 && !(P.key_full64 && key == kEmptyKey)) {
-                const int slot = sm.Find(key);
-                if (slot >= 0) {
-                    const int gg = *reinterpret_cast<volatile int*>(&sm.gid[slot]);
-                    if (gg >= 0 && gg < kPrivGroups && ncache < kPrivGroups) {
-                        g = gg;
-#pragma unroll
-                        for (int k = 0; k < kPrivGroups; ++k) {
-                            if (k == ncache) {
-                                ckey[k] = key;
-                                cgid[k] = gg;
-                            }
-                        }
-                        ++ncache;
-                    }
+            if (sel) {
+                if (nvalid == kQuadRows) {
+                    selq = __ldcs(reinterpret_cast<const unsigned int*>(sel + r4));
+                } else {
+                    uint32_t m = 0;
+                    for (int j = 0; j < nvalid; ++j) m |= uint32_t(sel[r4 + j]) << (8 * j);
+                    selq = m;
                 }
             }
-            if (g >= 0) {
-                ShapeFoldP<SIG, kQuadThreads>(pacc + g * SIG::words * kQuadThreads + tid, F, cur);
-            } else {
-                RowAcc acc{&P, nullptr, 0, row0 + r4 + j, 0, -1, 0};
-                FoldRowFast<false>(L, acc);
+    #pragma unroll
+            for (int j = 0; j < kQuadRows; ++j) {
+                if (((selq >> (8 * j)) & 0xffu) == 0) continue;
+                RegRow<SIG::Cols::n> cur;
+                QuadRow<SIG>(cur, q, j);
+                if (SIG::Atoms::n && ShapeHeld<SIG>(P, F, cur) != F.clause_mask) continue;
+                const uint64_t key = ShapeKey<SIG>(cur);
+                int g = -1;
+    #pragma unroll
+                for (int k = 0; k < kPrivGroups; ++k) g = ckey[k] == key ? cgid[k] : g;
+                if (g < 0 && !(P.key_full64 && key == kEmptyKey)) {
+                    const int slot = sm.Find(key);
+                    if (slot >= 0) {
+                        const int gg = *reinterpret_cast<volatile int*>(&sm.gid[slot]);
+                        if (gg >= 0 && gg < kPrivGroups && ncache < kPrivGroups) {
+                            g = gg;
+    #pragma unroll
+                            for (int k = 0; k < kPrivGroups; ++k) {
+                                if (k == ncache) {
+                                    ckey[k] = key;
+                                    cgid[k] = gg;
+                                }
+                            }
+                            ++ncache;
+                        }
+                    }
+                }
+                if (g >= 0) {
+                    ShapeFoldP<SIG, kQuadThreads>(pacc + g * SIG::words * kQuadThreads + tid, F, cur);
+                } else {
+                    RowAcc acc{&P, nullptr, 0, row0 + r4 + j, 0, -1, 0};
+                    FoldRowFast<false>(L, acc);
+                }
             }
         }
     }
@@ -2448,6 +2479,97 @@ __global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadBatchKernel(const _
         __syncthreads();
         if (tid == 0 && sm.fresh[0]) atomicAdd(&B.new_groups[item.task], (unsigned long long)sm.fresh[0]);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Heavy hitters of a high-cardinality aggregate: its keys counted over an
+// evenly strided sample of rows in a scratch table, then the most frequent
+// (sampled at least twice, at most k of them) kept as the shared tier's seeds.
+// ---------------------------------------------------------------------------
+struct SeedSlot {
+    unsigned long long key;
+    unsigned count;
+    unsigned pad;
+};
+
+constexpr int kSeedSampleRows = 1 << 18;
+constexpr int kSeedTableSlots = 1 << 19;   // twice the sample: at most half full
+constexpr int kSeedProbe = 64;
+constexpr int kSeedHistBins = 1024;
+
+__global__ void SeedInitKernel(SeedSlot* tab, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        tab[i].key = kEmptyKey;
+        tab[i].count = 0;
+        tab[i].pad = 0;
+    }
+}
+
+template <class SH>
+__global__ void __launch_bounds__(256) SeedSampleKernel(const __grid_constant__ AggLaunch L, SeedSlot* tab,
+                                                        int64_t stride, int64_t nsample) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nsample) return;
+    const char* cb[kFastCols];
+#pragma unroll
+    for (int c = 0; c < kFastCols; ++c) cb[c] = c < SH::Cols::n ? L.P.cols[L.F.col_slot[c]].data : nullptr;
+    const TileRow row{cb, int(i * stride)};
+    const uint64_t key = ShapeKey<SH>(row);
+    if (key == kEmptyKey) return;
+    uint32_t h = uint32_t(Fmix64(key)) & uint32_t(kSeedTableSlots - 1);
+    for (int p = 0; p < kSeedProbe; ++p) {
+        auto* kp = &tab[h].key;
+        const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(kp);
+        if (cur == key) {
+            atomicAdd(&tab[h].count, 1u);
+            return;
+        }
+        if (cur == kEmptyKey) {
+            const unsigned long long old = atomicCAS(kp, kEmptyKey, key);
+            if (old == kEmptyKey || old == key) {
+                atomicAdd(&tab[h].count, 1u);
+                return;
+            }
+        }
+        h = (h + 1) & uint32_t(kSeedTableSlots - 1);
+    }
+}
+
+// One CTA: a histogram of the sampled counts picks the smallest count c >= 2
+// whose keys sampled at least c times number at most k; those keys are the
+// seeds (in table order).
+__global__ void __launch_bounds__(1024) SeedSelectKernel(const SeedSlot* tab, int k, uint64_t* seeds, int* nseed) {
+    __shared__ unsigned hist[kSeedHistBins];
+    __shared__ unsigned thr;
+    __shared__ unsigned taken;
+    for (int i = threadIdx.x; i < kSeedHistBins; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < kSeedTableSlots; i += blockDim.x) {
+        const unsigned c = tab[i].count;
+        if (c >= 2) atomicAdd(&hist[min(c, unsigned(kSeedHistBins - 1))], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned cum = 0, t = kSeedHistBins;
+        for (int b = kSeedHistBins - 1; b >= 2; --b) {
+            if (cum + hist[b] > unsigned(k)) break;
+            cum += hist[b];
+            t = unsigned(b);
+        }
+        thr = t;
+        taken = 0;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kSeedTableSlots; i += blockDim.x) {
+        const unsigned c = tab[i].count;
+        if (c >= 2 && min(c, unsigned(kSeedHistBins - 1)) >= thr) {
+            const unsigned at = atomicAdd(&taken, 1u);
+            if (at < unsigned(k)) seeds[at] = tab[i].key;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *nseed = int(min(taken, unsigned(k)));
 }
 
 // The instantiated query shapes.  QDB_C(w, u): a fast column of w bytes
@@ -3025,6 +3147,20 @@ SigKernelFn FindHighKernel(const AggPlan& P, const FastPlan& F) {
     return nullptr;
 }
 
+using SeedKernelFn = void (*)(AggLaunch, SeedSlot*, int64_t, int64_t);
+
+SeedKernelFn FindSeedKernel(const AggPlan& P, const FastPlan& F) {
+    const std::vector<int> key = ShapeKeyOf(P, F);
+    if (key.empty()) return nullptr;
+    // Seeds need a COUNT state: the flush skips the seeded slots it is 0 in.
+#define QDB_SHAPE_FIND(...)                                                             \
+    if (ShapeMatches<__VA_ARGS__>(key) && ShapeWordsMatch<__VA_ARGS__>(F))               \
+        return __VA_ARGS__::count_off() >= 0 ? SeedSampleKernel<__VA_ARGS__> : nullptr;
+    QDB_HIGH_SHAPE_LIST(QDB_SHAPE_FIND)
+#undef QDB_SHAPE_FIND
+    return nullptr;
+}
+
 SigKernelFn FindSigKernel(const AggPlan& P, const FastPlan& F, bool quad) {
     const std::vector<int> key = ShapeKeyOf(P, F);
     if (key.empty()) return nullptr;
@@ -3063,6 +3199,8 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
     L.jk = a.jkey;
     L.jt = a.jt;
     L.inline_slot = a.join ? a.inline_slot : -1;
+    L.seeds = a.seeds;
+    L.nseed = a.nseed;
     const bool wide = a.table.wide != 0;
 
     if (a.index) {
@@ -3268,6 +3406,34 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
     }
     ProfileEnd(s);
     CountLaunch();
+}
+
+bool AggHighSeedable(const AggPlan& p, const FastPlan& f) {
+    return p.nkeyparts > 0 && p.key_words <= 1 && FindHighKernel(p, f) != nullptr && FindSeedKernel(p, f) != nullptr;
+}
+
+size_t AggSeedScratch() { return size_t(kSeedTableSlots) * sizeof(SeedSlot); }
+
+bool AggSeedHeavy(const AggPlan& p, const FastPlan& f, int64_t nrows, uint64_t* seeds, int* nseed, int k,
+                  void* scratch, cudaStream_t s) {
+    const SeedKernelFn fn = FindSeedKernel(p, f);
+    if (!fn || nrows <= 0 || k <= 0 || !scratch) return false;
+    auto* tab = static_cast<SeedSlot*>(scratch);
+    static thread_local AggLaunch* Lp = nullptr;
+    if (!Lp) Lp = new AggLaunch();
+    AggLaunch& L = *Lp;
+    std::memset(&L, 0, sizeof(L));
+    L.P = p;
+    L.F = f;
+    const int64_t nsample = std::min<int64_t>(nrows, kSeedSampleRows);
+    const int64_t stride = nrows / nsample;
+    ProfileBegin(s, "agg_seed", nsample);
+    SeedInitKernel<<<kSeedTableSlots / 256, 256, 0, s>>>(tab, kSeedTableSlots);
+    fn<<<int((nsample + 255) / 256), 256, 0, s>>>(L, tab, stride, nsample);
+    SeedSelectKernel<<<1, 1024, 0, s>>>(tab, k, seeds, nseed);
+    ProfileEnd(s);
+    CountLaunch(3);
+    return true;
 }
 
 void AggRehash(const AggPlan& p, const GTableDev& from, const GTableDev& to, AggCounters* c, cudaStream_t s) {

@@ -20,7 +20,7 @@ struct AggCounters {
     unsigned long long spilled;
     unsigned long long matched;     // fused join: joined rows folded in
     int error;
-    int pad;
+    unsigned next_chunk;            // work queue head of the listed-row kernel (zeroed with the rest)
 };
 
 // Global open-addressing group table in HBM: capacity slots plus one slot for
@@ -102,6 +102,8 @@ struct AggUpdateArgs {
     bool join = false;
     JoinKeyPlan jkey;
     JTableDev jt;
+    const uint64_t* seeds = nullptr;  // high-cardinality kernel: shared-tier seeds (device)
+    const int* nseed = nullptr;       // their count (device)
 };
 
 struct AggOutputCol {
@@ -118,6 +120,15 @@ size_t MaxSmemOptin();
 void AggInitTable(const AggPlan& p, const GTableDev& t, cudaStream_t s);
 // Returns the shared-memory slots actually used by the launch.
 void AggUpdate(const AggUpdateArgs& a, cudaStream_t s);
+// Heavy-hitter seeds of a high-cardinality typed plan (a key column and a
+// COUNT state): the up-to-k most frequent keys of an evenly strided sample of
+// its rows (filter and selection aside) go to seeds[0, *nseed) on stream s (`scratch`: device,
+// AggSeedScratch() bytes, free once s has passed the call).  The
+// high-cardinality kernel pre-loads them into its shared tier.
+bool AggHighSeedable(const AggPlan& p, const FastPlan& f);
+size_t AggSeedScratch();
+bool AggSeedHeavy(const AggPlan& p, const FastPlan& f, int64_t nrows, uint64_t* seeds, int* nseed, int k,
+                  void* scratch, cudaStream_t s);
 void AggRehash(const AggPlan& p, const GTableDev& from, const GTableDev& to, AggCounters* c,
                cudaStream_t s);
 void AggMergeSpill(const AggPlan& p, const uint64_t* spill, int64_t n, const GTableDev& t,

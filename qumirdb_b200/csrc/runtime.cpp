@@ -534,11 +534,15 @@ void AggStateDestroy(AggTableState* st) {
     DevFree(st->deferred[0], st->s);
     DevFree(st->deferred[1], st->s);
     DevFree(st->spill, st->s);
+    DevFree(st->seeds, st->s);
     // Every readback into the mirror was synchronised when it was read.
     PinnedCountersPut(st->hc);
     st->magic = 0;
     delete st;
 }
+
+constexpr int64_t kSeedMinRows = int64_t(4) << 20;   // updates worth a heavy-hitter sample
+constexpr int kSeedKeys = 2048;                        // seeds kept (the tier takes up to half its slots)
 
 // Runs the fused kernel over `rows` rows of a resolved plan, then replays
 // deferred rows and spilled entries after growing the table.
@@ -575,6 +579,20 @@ bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyP
         }
         const int64_t groups_before = st->groups;
         const AggPlan chunk = OffsetPlan(plan, begin);
+        // A large high-cardinality update samples its keys once; the most
+        // frequent seed the kernel's shared tier from then on.
+        if (!priv && use_fast && !st->seeded && rows >= kSeedMinRows && AggHighSeedable(chunk, fast)) {
+            st->seeded = true;
+            st->seeds = static_cast<uint64_t*>(DevAlloc(size_t(kSeedKeys) * 8 + 16, st->s));
+            void* scratch = st->seeds ? DevAlloc(AggSeedScratch(), st->s) : nullptr;
+            if (!scratch || !AggSeedHeavy(chunk, fast, n, st->seeds, reinterpret_cast<int*>(st->seeds + kSeedKeys),
+                                          kSeedKeys, scratch, st->s)) {
+                DevFree(st->seeds, st->s);
+                st->seeds = nullptr;
+            }
+            DevFree(scratch, st->s);
+            cudaGetLastError();
+        }
         AggUpdateArgs a;
         a.plan = &chunk;
         a.nrows = n;
@@ -587,6 +605,10 @@ bool AggRun(AggTableState* st, const AggPlan& plan, int64_t rows, const JoinKeyP
         a.smem_slots = st->smem_slots;
         a.priv = priv;
         a.fast = use_fast ? &fast : nullptr;
+        if (st->seeds && !priv) {
+            a.seeds = st->seeds;
+            a.nseed = reinterpret_cast<const int*>(st->seeds + kSeedKeys);
+        }
         if (jk) {
             a.join = true;
             a.jkey = *jk;

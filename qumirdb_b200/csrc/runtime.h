@@ -74,6 +74,8 @@ struct AggTableState {
     AggArena* arena = nullptr;      // batch-created: table and counters may live here
     bool table_in_arena = false;
     bool dc_in_arena = false;
+    uint64_t* seeds = nullptr;      // heavy-hitter keys of the shared tier (device), then their count
+    bool seeded = false;            // sampled once, from the first large update
 };
 
 AggTableState* StateOf(void* ht);

@@ -210,6 +210,30 @@ def test_lineitem_runs_the_signature_kernel():
     assert_same_groups(got, want, queries.LINEITEM_OUT_TYPES, nkeys=2)
 
 
+def test_high_cardinality_heavy_hitter_seeds():
+    """An update of at least 4M rows samples its keys and seeds the shared
+    tier with the most frequent; a later update (with a selection, and rows
+    whose keys include none of some seeds) reuses them.  Rows of key -1 (the
+    empty marker) take the table's flag slot.  Every group equals the
+    oracle's."""
+    n = 6_000_000
+    first = zipf_data(n, 200_000, 11)
+    first[0][::997] = -1
+    second = zipf_data(1_000_000, 400_000, 12)
+    sel = (np.random.default_rng(3).random(len(second[0])) > 0.4).astype(np.uint8)
+    spec = queries.zipf_agg(expected_groups=200_000)
+    q.profile(True)
+    q.profile_read()
+    out = run_gpu(spec, [q.DeviceRowSet(first), q.DeviceRowSet(second, selection=sel)])
+    names = [kk[0] for kk in q.profile_read()]
+    q.profile(False)
+    got = gpu_rows(out, queries.ZIPF_OUT_TYPES)
+    q.release(out)
+    assert names.count("agg_seed") == 1 and "agg_update_high" in names, names
+    want = O.aggregate(spec, [q.HostRowSet(first), q.HostRowSet(second, selection=sel)])
+    assert_same_groups(got, want, queries.ZIPF_OUT_TYPES, nkeys=1)
+
+
 @pytest.mark.parametrize("shape", ["zipf", "count", "sum_count"])
 def test_high_cardinality_shape_kernels(shape):
     """The high-cardinality shape kernel (shared tier for hot keys, global
