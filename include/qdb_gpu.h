@@ -81,8 +81,14 @@ typedef enum qdb_type {
     QDB_TYPE_DATE32 = 12,     /* i32 days since 1970-01-01 (qdb/plan/types/date.h:14-29) */
     QDB_TYPE_DECIMAL64 = 13,  /* unscaled i64, precision <= 18 (qdb/plan/types/decimal.h:80-99) */
     QDB_TYPE_DECIMAL128 = 14, /* unscaled i128 "BinInt", precision 19..38     */
-    QDB_TYPE_CHAR1 = 15       /* a string column whose values are one byte,
+    QDB_TYPE_CHAR1 = 15,      /* a string column whose values are one byte,
                                  staged as one code byte per row             */
+    QDB_TYPE_STRING = 16      /* a string column as Arrow lays it out: row r's
+                                 bytes are Data[Offsets[r] .. Offsets[r+1]),
+                                 Offsets of OffsetWidth 4 (utf8) or 8
+                                 (large_utf8) bytes each.  Served as a key
+                                 column of hash programs (qdb_gpu_hash and
+                                 the runtime-filter probe of a row set).     */
 } qdb_type;
 
 typedef struct qdb_column_type {

@@ -45,6 +45,8 @@ struct Val {
     i128 i = 0;
     double f = 0.0;
     bool null = false;
+    const uint8_t* s = nullptr;   // strings: the row's bytes
+    int64_t n = 0;                // and their count
 };
 
 bool IsFloat(int t) { return t == QDB_TYPE_F32 || t == QDB_TYPE_F64; }
@@ -118,6 +120,21 @@ Val ReadCell(const qdb_column& c, const qdb_column_type& t, int64_t row) {
         case QDB_TYPE_DECIMAL128: {
             const uint64_t* w = reinterpret_cast<const uint64_t*>(d) + 2 * row;
             v.i = i128((u128(uint64_t(w[1])) << 64) | w[0]);
+            break;
+        }
+        case QDB_TYPE_STRING: {   // Arrow utf8 / large_utf8: Data[Offsets[r] .. Offsets[r+1])
+            int64_t b, e;
+            if (c.OffsetWidth == 8) {
+                b = static_cast<const int64_t*>(c.Offsets)[row];
+                e = static_cast<const int64_t*>(c.Offsets)[row + 1];
+            } else if (c.OffsetWidth == 4) {
+                b = static_cast<const int32_t*>(c.Offsets)[row];
+                e = static_cast<const int32_t*>(c.Offsets)[row + 1];
+            } else {
+                throw Error("string column without offsets of width 4 or 8");
+            }
+            v.s = reinterpret_cast<const uint8_t*>(d) + b;
+            v.n = e - b;
             break;
         }
         default: throw Error("unsupported column type");
@@ -334,8 +351,8 @@ void EvalAll(const Expr& e, int32_t root, const std::function<Val(int32_t)>& lea
 
 // ---------------------------------------------------------------------------
 // Key hashing: HashKeyValue (qdb/kernel/gen.cpp:233-379), rh_hash(i64)
-// (qdb/kernel/aggregation/key_ops_i64.oz:4-11) and qdb_string_hash_bytes for
-// short strings (qdb/modules/qumirdb_runtime.cpp:270-300).
+// (qdb/kernel/aggregation/key_ops_i64.oz:4-11) and qdb_string_hash_bytes
+// (qdb/modules/qumirdb_runtime.cpp:270-300).
 // ---------------------------------------------------------------------------
 uint64_t MixU64(uint64_t h) {
     h ^= h >> 12;
@@ -345,6 +362,111 @@ uint64_t MixU64(uint64_t h) {
 }
 
 uint64_t ByteSwap(uint64_t x) { return __builtin_bswap64(x); }
+
+// Strings above 16 bytes: XXH3-64 (xxHash 0.8, as vendored by Apache Arrow
+// and called by qdb_string_hash_bytes) with seed 0 and the engine's own
+// 136-byte secret, qdb/modules/qumirdb_runtime.cpp:253-299.  A restatement
+// of the published algorithm: the 17-128, 129-240 and long (stripes of 64
+// bytes, blocks of (secret - 64) / 8 stripes) paths.
+const uint8_t kStringSecret[] = {
+    0xe7, 0x8b, 0x13, 0xf9, 0xfc, 0xb5, 0x8e, 0xef, 0x81, 0x48, 0x2c, 0xbf, 0xf9, 0x9f,
+    0xc1, 0x1e, 0x43, 0x6d, 0xbf, 0xa6, 0x6d, 0xb5, 0x72, 0xbc, 0x97, 0xd8, 0x61, 0x24,
+    0x0f, 0x12, 0xe3, 0x05, 0x21, 0xf7, 0x5c, 0x66, 0x67, 0xa5, 0x65, 0x03, 0x96, 0x26,
+    0x69, 0xd8, 0x29, 0x20, 0xf8, 0xc7, 0xb0, 0x3d, 0xdd, 0x7d, 0x18, 0xa0, 0x60, 0x75,
+    0x92, 0xa4, 0xce, 0xba, 0xc0, 0x77, 0xf4, 0xac, 0xb7, 0x03, 0x53, 0xf0, 0x98, 0xce,
+    0xe6, 0x2b, 0x20, 0xc7, 0x82, 0x91, 0xab, 0xbf, 0x68, 0x5c, 0x62, 0x4d, 0x33, 0xa3,
+    0xe1, 0xb3, 0xff, 0x97, 0x54, 0x4c, 0x44, 0x34, 0xb5, 0xb9, 0x32, 0x4c, 0x75, 0x42,
+    0x89, 0x53, 0x94, 0xd4, 0x9f, 0x2b, 0x76, 0x4d, 0x4e, 0xe6, 0xfa, 0x15, 0x3e, 0xc1,
+    0xdb, 0x71, 0x4b, 0x2c, 0x94, 0xf5, 0xfc, 0x8c, 0x89, 0x4b, 0xfb, 0xc1, 0x82, 0xa5,
+    0x6a, 0x53, 0xf9, 0x4a, 0xba, 0xce, 0x1f, 0xc0, 0x97, 0x1a,
+};
+constexpr int64_t kStringSecretBytes = 136;
+static_assert(sizeof(kStringSecret) == kStringSecretBytes, "secret size");
+
+constexpr uint64_t kXxP32_1 = 0x9E3779B1ULL, kXxP32_2 = 0x85EBCA77ULL, kXxP32_3 = 0xC2B2AE3DULL;
+constexpr uint64_t kXxP64_1 = 0x9E3779B185EBCA87ULL, kXxP64_2 = 0xC2B2AE3D27D4EB4FULL;
+constexpr uint64_t kXxP64_3 = 0x165667B19E3779F9ULL, kXxP64_4 = 0x85EBCA77C2B2AE63ULL;
+constexpr uint64_t kXxP64_5 = 0x27D4EB2F165667C5ULL;
+
+uint64_t XxLe64(const uint8_t* p) {
+    uint64_t v = 0;
+    for (int k = 7; k >= 0; --k) v = (v << 8) | p[k];
+    return v;
+}
+
+uint64_t XxFold(uint64_t a, uint64_t b) {
+    const unsigned __int128 p = (unsigned __int128)a * b;
+    return uint64_t(p) ^ uint64_t(p >> 64);
+}
+
+uint64_t XxAvalanche(uint64_t h) {
+    h ^= h >> 37;
+    h *= 0x165667919E3779F9ULL;
+    return h ^ (h >> 32);
+}
+
+uint64_t XxMix16(const uint8_t* in, const uint8_t* sec) {
+    return XxFold(XxLe64(in) ^ XxLe64(sec), XxLe64(in + 8) ^ XxLe64(sec + 8));
+}
+
+void XxStripe(uint64_t* acc, const uint8_t* in, const uint8_t* sec) {
+    for (int i = 0; i < 8; ++i) {
+        const uint64_t v = XxLe64(in + 8 * i);
+        const uint64_t k = v ^ XxLe64(sec + 8 * i);
+        acc[i ^ 1] += v;
+        acc[i] += (k & 0xffffffffULL) * (k >> 32);
+    }
+}
+
+uint64_t Xxh3WithSecret(const uint8_t* d, int64_t n, const uint8_t* sec, int64_t sec_n) {
+    const uint64_t len = uint64_t(n);
+    if (n <= 128) {   // 17..128
+        uint64_t acc = len * kXxP64_1;
+        if (n > 32) {
+            if (n > 64) {
+                if (n > 96) {
+                    acc += XxMix16(d + 48, sec + 96);
+                    acc += XxMix16(d + n - 64, sec + 112);
+                }
+                acc += XxMix16(d + 32, sec + 64);
+                acc += XxMix16(d + n - 48, sec + 80);
+            }
+            acc += XxMix16(d + 16, sec + 32);
+            acc += XxMix16(d + n - 32, sec + 48);
+        }
+        acc += XxMix16(d, sec);
+        acc += XxMix16(d + n - 16, sec + 16);
+        return XxAvalanche(acc);
+    }
+    if (n <= 240) {
+        uint64_t acc = len * kXxP64_1;
+        for (int i = 0; i < 8; ++i) acc += XxMix16(d + 16 * i, sec + 16 * i);
+        acc = XxAvalanche(acc);
+        const int rounds = int(n / 16);
+        for (int i = 8; i < rounds; ++i) acc += XxMix16(d + 16 * i, sec + 16 * (i - 8) + 3);
+        acc += XxMix16(d + n - 16, sec + 136 - 17);
+        return XxAvalanche(acc);
+    }
+    uint64_t acc[8] = {kXxP32_3, kXxP64_1, kXxP64_2, kXxP64_3, kXxP64_4, kXxP32_2, kXxP64_5, kXxP32_1};
+    const int64_t stripes_per_block = (sec_n - 64) / 8;
+    const int64_t block = 64 * stripes_per_block;
+    const int64_t blocks = (n - 1) / block;
+    for (int64_t b = 0; b < blocks; ++b) {
+        for (int64_t s = 0; s < stripes_per_block; ++s) XxStripe(acc, d + b * block + 64 * s, sec + 8 * s);
+        for (int i = 0; i < 8; ++i) {   // scramble
+            uint64_t a = acc[i];
+            a ^= a >> 47;
+            a ^= XxLe64(sec + sec_n - 64 + 8 * i);
+            acc[i] = a * kXxP32_1;
+        }
+    }
+    const int64_t tail_stripes = ((n - 1) - block * blocks) / 64;
+    for (int64_t s = 0; s < tail_stripes; ++s) XxStripe(acc, d + blocks * block + 64 * s, sec + 8 * s);
+    XxStripe(acc, d + n - 64, sec + sec_n - 64 - 7);
+    uint64_t r = len * kXxP64_1;
+    for (int i = 0; i < 4; ++i) r += XxFold(acc[2 * i] ^ XxLe64(sec + 11 + 16 * i), acc[2 * i + 1] ^ XxLe64(sec + 11 + 16 * i + 8));
+    return XxAvalanche(r);
+}
 
 uint64_t StringHash(const uint8_t* d, int64_t n) {
     const uint64_t mul0 = 11400714785074694791ULL, mul1 = 14029467366897019727ULL;
@@ -366,7 +488,7 @@ uint64_t StringHash(const uint8_t* d, int64_t n) {
         std::memcpy(&y, d, 8);
         return uint64_t(n) ^ ByteSwap(mul0 * x) ^ ByteSwap(mul1 * y);
     }
-    throw Error("strings above 16 bytes hash with XXH3; not restated");
+    return Xxh3WithSecret(d, n, kStringSecret, kStringSecretBytes);
 }
 
 // Canonical float bits: -0 -> +0, every NaN -> one quiet NaN
@@ -382,6 +504,7 @@ uint64_t LeafHash(const Val& v, int t) {
     switch (t) {
         case QDB_TYPE_BOOL: return uint64_t(v.i != 0) * 2685821657736338717ULL;
         case QDB_TYPE_CHAR1: { const uint8_t b = uint8_t(v.i); return StringHash(&b, 1); }
+        case QDB_TYPE_STRING: return StringHash(v.s, v.n);
         case QDB_TYPE_F64: return MixU64(CanonicalF64Bits(v.f));
         case QDB_TYPE_F32: {
             float f = float(v.f);
@@ -1838,6 +1961,10 @@ void oracle_rf_merge(uint64_t* target, const uint64_t* source, int64_t count) { 
 
 // std::mt19937_64 output (the generator the reference's runtime-filter
 // tests draw their hashes from, test/test_runtime_filter.cpp:31-39).
+uint64_t oracle_string_hash(const uint8_t* data, int64_t size) { return StringHash(data, size); }
+
+const uint8_t* oracle_string_secret(void) { return kStringSecret; }
+
 void oracle_mt19937_64(uint64_t seed, int64_t n, uint64_t* out) {
     std::mt19937_64 rng(seed);
     for (int64_t i = 0; i < n; ++i) out[i] = rng();

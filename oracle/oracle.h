@@ -135,6 +135,11 @@ void oracle_mt19937_64(uint64_t seed, int64_t n, uint64_t* out);
 int64_t oracle_route(const uint64_t* hashes, const uint8_t* sel, int64_t n, const int64_t* routes,
                      int64_t n_routes, int64_t n_outputs, int64_t* dest);
 
+/* qdb_string_hash_bytes (qdb/modules/qumirdb_runtime.cpp:270-300) of one
+   string, and the 136-byte XXH3 secret it hashes strings above 16 bytes with. */
+uint64_t oracle_string_hash(const uint8_t* data, int64_t size);
+const uint8_t* oracle_string_secret(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,8 @@ def lib() -> C.CDLL:
             "oracle_rf_probe": (C.c_int64, [C.POINTER(abi.RfData), P, P, P, C.c_int64]),
             "oracle_rf_merge": (None, [P, P, C.c_int64]),
             "oracle_mt19937_64": (None, [C.c_uint64, C.c_int64, P]),
+            "oracle_string_hash": (C.c_uint64, [P, C.c_int64]),
+            "oracle_string_secret": (C.c_void_p, []),
             "oracle_route": (C.c_int64, [P, P, C.c_int64, P, C.c_int64, C.c_int64, P]),
             "oracle_join_aggregate": (C.c_int, [C.POINTER(abi.RowJoinSpec), C.POINTER(abi.AggregateSpec),
                                                 C.POINTER(abi.RowSet), C.c_int32, C.POINTER(abi.RowSet), C.c_int32,
@@ -320,3 +322,14 @@ def route(hashes: np.ndarray, selection, routes, n_outputs: int) -> np.ndarray |
                             None if r is None else r.ctypes.data, 0 if r is None else len(r), n_outputs,
                             dest.ctypes.data)
     return None if rc < 0 else dest[:n]
+
+
+def string_hash(b: bytes) -> int:
+    """qdb_string_hash_bytes of one string (the oracle's restatement)."""
+    buf = C.create_string_buffer(b, len(b)) if b else None
+    return int(lib().oracle_string_hash(buf, len(b)))
+
+
+def string_secret() -> bytes:
+    """The engine's 136-byte XXH3 secret for strings above 16 bytes."""
+    return C.string_at(lib().oracle_string_secret(), 136)

@@ -132,17 +132,49 @@ def _bitmap(valid: np.ndarray) -> np.ndarray:
     return np.packbits(valid.astype(np.uint8), bitorder="little")
 
 
+class StringColumn:
+    """A QDB_TYPE_STRING column in Arrow's layout: row r is
+    data[offsets[r]:offsets[r + 1]], offsets int32 (utf8) or int64
+    (large_utf8)."""
+
+    def __init__(self, offsets, data):
+        self.offsets = np.ascontiguousarray(offsets)
+        if self.offsets.dtype not in (np.int32, np.int64):
+            raise ValueError("string offsets must be int32 or int64")
+        self.data = np.ascontiguousarray(data, dtype=np.uint8)
+
+    @classmethod
+    def of(cls, values, large: bool = False) -> "StringColumn":
+        bs = [v if isinstance(v, bytes) else str(v).encode() for v in values]
+        off = np.zeros(len(bs) + 1, np.int64 if large else np.int32)
+        np.cumsum([len(b) for b in bs], out=off[1:])
+        return cls(off, np.frombuffer(b"".join(bs), np.uint8).copy())
+
+    def __len__(self) -> int:
+        return len(self.offsets) - 1
+
+
+def _host_column(col: "abi.Column", a) -> None:
+    if isinstance(a, StringColumn):
+        col.Data = a.data.ctypes.data if a.data.size else None
+        col.Offsets = a.offsets.ctypes.data
+        col.OffsetWidth = a.offsets.itemsize
+    else:
+        col.Data = a.ctypes.data if a.size else None
+
+
 class HostRowSet:
-    """A TRowSet over host numpy columns (kept alive by this object)."""
+    """A TRowSet over host numpy columns (kept alive by this object);
+    string columns are StringColumn."""
 
     def __init__(self, columns, masks=None, selection=None, rows=None):
-        self.arrays = [np.ascontiguousarray(c) for c in columns]
+        self.arrays = [c if isinstance(c, StringColumn) else np.ascontiguousarray(c) for c in columns]
         n = rows if rows is not None else (len(self.arrays[0]) if self.arrays else 0)
         self.masks = [None if m is None else _bitmap(np.asarray(m, dtype=bool)) for m in (masks or [None] * len(columns))]
         self.selection = None if selection is None else np.ascontiguousarray(selection, dtype=np.uint8)
         self.cols = (abi.Column * max(1, len(self.arrays)))()
         for k, a in enumerate(self.arrays):
-            self.cols[k].Data = a.ctypes.data if a.size else None
+            _host_column(self.cols[k], a)
             if self.masks[k] is not None:
                 self.cols[k].Mask = self.masks[k].ctypes.data
         self.rs = abi.RowSet()
@@ -203,10 +235,18 @@ class DeviceRowSet:
     def __init__(self, columns, masks=None, selection=None, rows=None):
         host = HostRowSet(columns, masks, selection, rows)
         self.rows = host.rs.RowCount
-        self.widths = [a.dtype.itemsize for a in host.arrays]
+        self.widths = [0 if isinstance(a, StringColumn) else a.dtype.itemsize for a in host.arrays]
         self.bufs = []
         self.cols = (abi.Column * max(1, len(host.arrays)))()
         for k, a in enumerate(host.arrays):
+            if isinstance(a, StringColumn):
+                ob = DeviceBuffer(a.offsets.nbytes).upload(a.offsets, stream_sync=False)
+                db = DeviceBuffer(a.data.nbytes).upload(a.data, stream_sync=False)
+                self.bufs += [ob, db]
+                self.cols[k].Data = db.ptr
+                self.cols[k].Offsets = ob.ptr
+                self.cols[k].OffsetWidth = a.offsets.itemsize
+                continue
             b = DeviceBuffer(a.nbytes).upload(a, stream_sync=False)
             self.bufs.append(b)
             self.cols[k].Data = b.ptr

@@ -10,6 +10,7 @@ from pathlib import Path
 
 # qdb_type
 BOOL, I8, I16, I32, I64, U8, U16, U32, U64, F32, F64, DATE32, DECIMAL64, DECIMAL128, CHAR1 = range(1, 16)
+STRING = 16   # Arrow layout: offsets (int32 / int64) into the bytes; hash-program keys
 # qdb_expr_op
 (COLUMN, CONST, NULL, ADD, SUB, MUL, DIV, NEG, CAST, EQ, NE, LT, LE, GT, GE, AND, OR, NOT, BETWEEN, IN_LIST,
  CASE, IS_NULL, IS_NOT_NULL, MOD) = range(1, 25)

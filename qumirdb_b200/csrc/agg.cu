@@ -89,6 +89,37 @@ struct AggLaunch {
     const int* nseed;         // their count (device), or seeds == nullptr
 };
 
+// Launch arguments of the listed-row kernel (AggSigQuadKernel): the typed
+// plan and the fields of AggLaunch it reads, under a fifth of AggLaunch's
+// bytes — a launch's parameter block travels with it, and ~11 KB of it cost
+// about 6 us per launch on B200 against a small block.
+struct QuadLaunch {
+    FastPlan F;
+    const char* cols[kFastCols];   // the typed columns, at row 0
+    const uint8_t* selection;
+    int64_t nrows;
+    GTableDev T;
+    uint64_t cap_mask;
+    AggCounters* counters;
+    int64_t* deferred;
+    int64_t deferred_cap;
+    uint64_t* spill;
+    int64_t spill_cap;
+    StateDesc states[kMaxStates];
+    int32_t nstates;
+    int32_t state_words;
+    int32_t nkeyparts;
+    int32_t key_full64;
+    int32_t smem_slots;
+    int32_t smem_limit;
+    int32_t off_misc;
+    int32_t off_skeys;
+    int32_t off_sst;
+    int32_t off_gid;
+    int32_t off_pacc;
+    int64_t list[kMaxList];        // IN-list constants of the filter atoms
+};
+
 // ---------------------------------------------------------------------------
 // Row accessor over staged tiles, global columns and gathered build rows.
 // ---------------------------------------------------------------------------
@@ -411,7 +442,8 @@ __device__ __forceinline__ unsigned char* DynSmem() {
 }
 
 // The shared-memory tier of this CTA, located by the launch's offsets.
-__device__ __forceinline__ SmemTable MakeSmem(const AggLaunch& L, bool wide, bool priv) {
+template <class LT>
+__device__ __forceinline__ SmemTable MakeSmem(const LT& L, bool wide, bool priv) {
     unsigned char* smem = DynSmem();
     unsigned* misc = reinterpret_cast<unsigned*>(smem + L.off_misc);
     SmemTable sm;
@@ -1115,8 +1147,8 @@ __device__ __forceinline__ void ShapeFoldP(uint64_t* p, const FastPlan& F, const
 }
 
 // Clauses held by the row's filter atoms (AND of OR clauses).
-template <class SH, int J = 0, class A>
-__device__ __forceinline__ uint32_t ShapeHeld(const AggPlan& P, const FastPlan& F, const A& row) {
+template <class SH, int J = 0, class PL, class A>
+__device__ __forceinline__ uint32_t ShapeHeld(const PL& P, const FastPlan& F, const A& row) {
     if constexpr (J < SH::Atoms::n) {
         constexpr int op = SH::Atoms::at(J) >> 3;
         constexpr int col = SH::Atoms::at(J) & 7;
@@ -1141,7 +1173,7 @@ __device__ __forceinline__ uint32_t ShapeHeld(const AggPlan& P, const FastPlan& 
         } else {
             ok = v >= t.c0;
         }
-        return (ok ? (1u << t.clause) : 0u) | ShapeHeld<SH, J + 1>(P, F, row);
+        return (ok ? (1u << t.clause) : 0u) | ShapeHeld<SH, J + 1, PL>(P, F, row);
     } else {
         return 0u;
     }
@@ -2060,12 +2092,43 @@ __device__ __forceinline__ void QuadPrefetchTile(const char* const* cb, const ui
     }
 }
 
+// A row of the listed-row kernel that neither the lanes' groups nor the
+// shared tier took (the tier is full, or the key is the empty marker): the
+// table itself — its flag slot for the marker — or the replay list when the
+// table is full.
 template <class SIG>
-__global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid_constant__ AggLaunch L) {
+__device__ __forceinline__ void QuadGlobalRow(const QuadLaunch& L, const SmemTable& sm, uint64_t key, bool special,
+                                              const ShapeVals<SIG>& v, int64_t row) {
+    uint64_t* flag_slot = L.T.slots + L.T.capacity * L.T.slot_words;
+    if (special) {
+        auto* flag = reinterpret_cast<unsigned long long*>(flag_slot + L.T.key_off);
+        if (*reinterpret_cast<volatile unsigned long long*>(flag) == 0 && atomicExch(flag, 1ull) == 0)
+            atomicAdd(sm.fresh, 1u);
+        ShapeAtomics<SIG>(flag_slot + L.T.state_off, 1, v);
+        return;
+    }
+    int is_new = 0;
+    const int64_t g = GlobalFindH(L.T, L.cap_mask, Fmix64(key), key, is_new);
+    if (is_new) atomicAdd(sm.fresh, 1u);
+    if (g >= 0) {
+        ShapeAtomics<SIG>(L.T.slots + g * L.T.slot_words + L.T.state_off, 1, v);
+        return;
+    }
+    const unsigned long long k = atomicAdd(&L.counters->deferred, 1ull);
+    if (int64_t(k) < L.deferred_cap) {
+        L.deferred[2 * k] = row;
+        L.deferred[2 * k + 1] = 0;
+    } else {
+        SetError(&L.counters->error, DE_DEFER_FULL);
+    }
+}
+
+template <class SIG>
+__global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid_constant__ QuadLaunch L) {
     unsigned char* smem = DynSmem();
     unsigned* misc = reinterpret_cast<unsigned*>(smem + L.off_misc);
     const SmemTable sm = MakeSmem(L, false, true);
-    const AggPlan& P = L.P;
+    const QuadLaunch& P = L;
     const FastPlan& F = L.F;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -2123,7 +2186,7 @@ __global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid
 #pragma unroll
     for (int c = 0; c < kFastCols; ++c) {
         cb[c] = nullptr;
-        if (c < SIG::Cols::n) cb[c] = P.cols[F.col_slot[c]].data + row0 * SIG::cw(c);
+        if (c < SIG::Cols::n) cb[c] = L.cols[c] + row0 * SIG::cw(c);
     }
     const uint8_t* sel = P.selection ? P.selection + row0 : nullptr;
     constexpr int NC = SIG::Cols::n > 0 ? SIG::Cols::n : 1;
@@ -2161,7 +2224,7 @@ __global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid
                     selq = m;
                 }
             }
-    #pragma unroll
+#pragma unroll
             for (int j = 0; j < kQuadRows; ++j) {
                 if (((selq >> (8 * j)) & 0xffu) == 0) continue;
                 RegRow<SIG::Cols::n> cur;
@@ -2169,15 +2232,17 @@ __global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid
                 if (SIG::Atoms::n && ShapeHeld<SIG>(P, F, cur) != F.clause_mask) continue;
                 const uint64_t key = ShapeKey<SIG>(cur);
                 int g = -1;
-    #pragma unroll
+#pragma unroll
                 for (int k = 0; k < kPrivGroups; ++k) g = ckey[k] == key ? cgid[k] : g;
-                if (g < 0 && !(P.key_full64 && key == kEmptyKey)) {
-                    const int slot = sm.Find(key);
+                const bool special = P.key_full64 && key == kEmptyKey;
+                int slot = -1;
+                if (g < 0 && !special) {
+                    slot = sm.Find(key);
                     if (slot >= 0) {
                         const int gg = *reinterpret_cast<volatile int*>(&sm.gid[slot]);
                         if (gg >= 0 && gg < kPrivGroups && ncache < kPrivGroups) {
                             g = gg;
-    #pragma unroll
+#pragma unroll
                             for (int k = 0; k < kPrivGroups; ++k) {
                                 if (k == ncache) {
                                     ckey[k] = key;
@@ -2191,8 +2256,13 @@ __global__ void __launch_bounds__(kQuadThreads, 2) AggSigQuadKernel(const __grid
                 if (g >= 0) {
                     ShapeFoldP<SIG, kQuadThreads>(pacc + g * SIG::words * kQuadThreads + tid, F, cur);
                 } else {
-                    RowAcc acc{&P, nullptr, 0, row0 + r4 + j, 0, -1, 0};
-                    FoldRowFast<false>(L, acc);
+                    ShapeVals<SIG> v;
+                    ShapeRowVals<SIG>(v, F, cur);
+                    if (slot >= 0) {
+                        ShapeSmemAtomics<SIG>(sm.st + slot, sm.S, v);   // a group past the lanes' four
+                    } else {
+                        QuadGlobalRow<SIG>(L, sm, key, special, v, row0 + r4 + j);
+                    }
                 }
             }
         }
@@ -3161,12 +3231,54 @@ SeedKernelFn FindSeedKernel(const AggPlan& P, const FastPlan& F) {
     return nullptr;
 }
 
-SigKernelFn FindSigKernel(const AggPlan& P, const FastPlan& F, bool quad) {
+using QuadKernelFn = void (*)(QuadLaunch);
+
+QuadKernelFn FindQuadKernel(const AggPlan& P, const FastPlan& F) {
     const std::vector<int> key = ShapeKeyOf(P, F);
     if (key.empty()) return nullptr;
-#define QDB_SHAPE_FIND(...)                                                            \
-    if (ShapeMatches<__VA_ARGS__>(key) && ShapeWordsMatch<__VA_ARGS__>(F))             \
-        return quad ? AggSigQuadKernel<__VA_ARGS__> : AggSigDirectKernel<__VA_ARGS__>;
+#define QDB_SHAPE_FIND(...) \
+    if (ShapeMatches<__VA_ARGS__>(key) && ShapeWordsMatch<__VA_ARGS__>(F)) return AggSigQuadKernel<__VA_ARGS__>;
+    QDB_SHAPE_LIST(QDB_SHAPE_FIND)
+#undef QDB_SHAPE_FIND
+    return nullptr;
+}
+
+// The listed-row kernel's arguments, from a launch laid out for it.
+void QuadLaunchOf(const AggLaunch& L, QuadLaunch& Q) {
+    std::memset(&Q, 0, sizeof(Q));
+    Q.F = L.F;
+    for (int c = 0; c < L.F.ncols && c < kFastCols; ++c) Q.cols[c] = L.P.cols[L.F.col_slot[c]].data;
+    Q.selection = L.P.selection;
+    Q.nrows = L.nrows;
+    Q.T = L.T;
+    Q.cap_mask = L.cap_mask;
+    Q.counters = L.counters;
+    Q.deferred = L.deferred;
+    Q.deferred_cap = L.deferred_cap;
+    Q.spill = L.spill;
+    Q.spill_cap = L.spill_cap;
+    static_assert(sizeof(Q.states) == sizeof(L.P.states), "state table sizes");
+    std::memcpy(Q.states, L.P.states, sizeof(Q.states));
+    Q.nstates = L.P.nstates;
+    Q.state_words = L.P.state_words;
+    Q.nkeyparts = L.P.nkeyparts;
+    Q.key_full64 = L.P.key_full64;
+    Q.smem_slots = L.smem_slots;
+    Q.smem_limit = L.smem_limit;
+    Q.off_misc = L.off_misc;
+    Q.off_skeys = L.off_skeys;
+    Q.off_sst = L.off_sst;
+    Q.off_gid = L.off_gid;
+    Q.off_pacc = L.off_pacc;
+    static_assert(sizeof(Q.list) == sizeof(L.P.list), "IN-list sizes");
+    std::memcpy(Q.list, L.P.list, sizeof(Q.list));
+}
+
+SigKernelFn FindSigKernel(const AggPlan& P, const FastPlan& F) {
+    const std::vector<int> key = ShapeKeyOf(P, F);
+    if (key.empty()) return nullptr;
+#define QDB_SHAPE_FIND(...) \
+    if (ShapeMatches<__VA_ARGS__>(key) && ShapeWordsMatch<__VA_ARGS__>(F)) return AggSigDirectKernel<__VA_ARGS__>;
     QDB_SHAPE_LIST(QDB_SHAPE_FIND)
 #undef QDB_SHAPE_FIND
     if (std::getenv("QDB_SHAPE_DEBUG")) {
@@ -3306,7 +3418,7 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
         }
         if (L.P.selection && (reinterpret_cast<uintptr_t>(L.P.selection) & 3)) quad = false;
         if (quad) {
-            if (SigKernelFn fn = FindSigKernel(L.P, *a.fast, true)) {
+            if (QuadKernelFn fn = FindQuadKernel(L.P, *a.fast)) {
                 L.F = *a.fast;
                 layout(16, 1, 64);
                 const size_t bytes = size_t(L.off_pacc) + size_t(kPrivGroups) * sw * kQuadThreads * 8;
@@ -3314,6 +3426,9 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
                     L.smem_slots = 64;
                     L.smem_limit = 32;
                     L.priv = 1;
+                    static thread_local QuadLaunch* Qp = nullptr;
+                    if (!Qp) Qp = new QuadLaunch();
+                    QuadLaunchOf(L, *Qp);
                     SetSmem(fn, bytes);
                     int per_sm = 1;
                     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kQuadThreads, bytes) != cudaSuccess) {
@@ -3325,7 +3440,7 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
                     const int64_t nt = (a.nrows + (int64_t(1) << 14) - 1) >> 14;
                     const int g2 = int(std::max<int64_t>(1, std::min<int64_t>(nt, int64_t(g_sms) * std::max(1, per_sm))));
                     ProfileBegin(s, "agg_update_sig", a.nrows);
-                    fn<<<g2, kQuadThreads, bytes, s>>>(L);
+                    fn<<<g2, kQuadThreads, bytes, s>>>(*Qp);
                     ProfileEnd(s);
                     CountLaunch();
                     return;
@@ -3333,7 +3448,7 @@ void AggUpdate(const AggUpdateArgs& a, cudaStream_t s) {
                 layout(T, stages, S);
             }
         }
-        if (SigKernelFn fn = FindSigKernel(L.P, *a.fast, false)) {
+        if (SigKernelFn fn = FindSigKernel(L.P, *a.fast)) {
             L.F = *a.fast;
             // The kernel stages nothing: a token stage keeps the layout's offsets.
             layout(16, 1, 64);

@@ -161,6 +161,143 @@ __global__ void __launch_bounds__(256) ProjectKernel(const __grid_constant__ Exp
     }
 }
 
+// ---------------------------------------------------------------------------
+// qdb_string_hash_bytes (qdb/modules/qumirdb_runtime.cpp:270-300) on the
+// device: the engine's short-string mix up to 16 bytes, XXH3-64 (xxHash
+// 0.8, seed 0) with the engine's 136-byte secret above.  A restatement of
+// the published XXH3 steps; bytes are read one at a time (a string starts
+// anywhere).
+// ---------------------------------------------------------------------------
+__constant__ uint8_t kStrSecret[136] = {
+    0xe7, 0x8b, 0x13, 0xf9, 0xfc, 0xb5, 0x8e, 0xef, 0x81, 0x48, 0x2c, 0xbf, 0xf9, 0x9f,
+    0xc1, 0x1e, 0x43, 0x6d, 0xbf, 0xa6, 0x6d, 0xb5, 0x72, 0xbc, 0x97, 0xd8, 0x61, 0x24,
+    0x0f, 0x12, 0xe3, 0x05, 0x21, 0xf7, 0x5c, 0x66, 0x67, 0xa5, 0x65, 0x03, 0x96, 0x26,
+    0x69, 0xd8, 0x29, 0x20, 0xf8, 0xc7, 0xb0, 0x3d, 0xdd, 0x7d, 0x18, 0xa0, 0x60, 0x75,
+    0x92, 0xa4, 0xce, 0xba, 0xc0, 0x77, 0xf4, 0xac, 0xb7, 0x03, 0x53, 0xf0, 0x98, 0xce,
+    0xe6, 0x2b, 0x20, 0xc7, 0x82, 0x91, 0xab, 0xbf, 0x68, 0x5c, 0x62, 0x4d, 0x33, 0xa3,
+    0xe1, 0xb3, 0xff, 0x97, 0x54, 0x4c, 0x44, 0x34, 0xb5, 0xb9, 0x32, 0x4c, 0x75, 0x42,
+    0x89, 0x53, 0x94, 0xd4, 0x9f, 0x2b, 0x76, 0x4d, 0x4e, 0xe6, 0xfa, 0x15, 0x3e, 0xc1,
+    0xdb, 0x71, 0x4b, 0x2c, 0x94, 0xf5, 0xfc, 0x8c, 0x89, 0x4b, 0xfb, 0xc1, 0x82, 0xa5,
+    0x6a, 0x53, 0xf9, 0x4a, 0xba, 0xce, 0x1f, 0xc0, 0x97, 0x1a,
+};
+constexpr int kStrSecretBytes = 136;
+
+__device__ __forceinline__ uint64_t StrLe64(const uint8_t* p) {
+    uint64_t v = 0;
+#pragma unroll
+    for (int k = 7; k >= 0; --k) v = (v << 8) | p[k];
+    return v;
+}
+
+__device__ __forceinline__ uint32_t StrLe32(const uint8_t* p) {
+    return uint32_t(p[0]) | (uint32_t(p[1]) << 8) | (uint32_t(p[2]) << 16) | (uint32_t(p[3]) << 24);
+}
+
+__device__ __forceinline__ uint64_t XxFold(uint64_t a, uint64_t b) { return a * b ^ __umul64hi(a, b); }
+
+__device__ __forceinline__ uint64_t XxAvalanche(uint64_t h) {
+    h ^= h >> 37;
+    h *= 0x165667919E3779F9ull;
+    return h ^ (h >> 32);
+}
+
+__device__ __forceinline__ uint64_t XxMix16(const uint8_t* in, int so) {
+    return XxFold(StrLe64(in) ^ StrLe64(kStrSecret + so), StrLe64(in + 8) ^ StrLe64(kStrSecret + so + 8));
+}
+
+__device__ __forceinline__ void XxStripe(uint64_t (&acc)[8], const uint8_t* in, int so) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint64_t v = StrLe64(in + 8 * i);
+        const uint64_t k = v ^ StrLe64(kStrSecret + so + 8 * i);
+        acc[i ^ 1] += v;
+        acc[i] += (k & 0xffffffffull) * (k >> 32);
+    }
+}
+
+__device__ __noinline__ uint64_t Xxh3Long(const uint8_t* d, int64_t n) {
+    uint64_t acc[8] = {0xC2B2AE3Dull, 0x9E3779B185EBCA87ull, 0xC2B2AE3D27D4EB4Full, 0x165667B19E3779F9ull,
+                       0x85EBCA77C2B2AE63ull, 0x85EBCA77ull, 0x27D4EB2F165667C5ull, 0x9E3779B1ull};
+    constexpr int kStripes = (kStrSecretBytes - 64) / 8;
+    constexpr int64_t kBlock = 64 * kStripes;
+    const int64_t blocks = (n - 1) / kBlock;
+    for (int64_t b = 0; b < blocks; ++b) {
+        for (int s = 0; s < kStripes; ++s) XxStripe(acc, d + b * kBlock + 64 * s, 8 * s);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            uint64_t a = acc[i];
+            a ^= a >> 47;
+            a ^= StrLe64(kStrSecret + kStrSecretBytes - 64 + 8 * i);
+            acc[i] = a * 0x9E3779B1ull;
+        }
+    }
+    const int64_t tail = ((n - 1) - kBlock * blocks) / 64;
+    for (int64_t s = 0; s < tail; ++s) XxStripe(acc, d + blocks * kBlock + 64 * s, int(8 * s));
+    XxStripe(acc, d + n - 64, kStrSecretBytes - 64 - 7);
+    uint64_t r = uint64_t(n) * 0x9E3779B185EBCA87ull;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        r += XxFold(acc[2 * i] ^ StrLe64(kStrSecret + 11 + 16 * i), acc[2 * i + 1] ^ StrLe64(kStrSecret + 19 + 16 * i));
+    return XxAvalanche(r);
+}
+
+__device__ __forceinline__ uint64_t StringHashDev(const uint8_t* d, int64_t n) {
+    constexpr uint64_t m0 = 11400714785074694791ull, m1 = 14029467366897019727ull;
+    if (n == 0) return 1;
+    if (n <= 3) {
+        const uint32_t x = (uint32_t(n) << 24) ^ (uint32_t(d[0]) << 16) ^ (uint32_t(d[n / 2]) << 8) ^ d[n - 1];
+        return ByteSwap64(m0 * x);
+    }
+    if (n <= 8) return uint64_t(n) ^ ByteSwap64(m0 * StrLe32(d + n - 4)) ^ ByteSwap64(m1 * StrLe32(d));
+    if (n <= 16) return uint64_t(n) ^ ByteSwap64(m0 * StrLe64(d + n - 8)) ^ ByteSwap64(m1 * StrLe64(d));
+    const uint64_t len = uint64_t(n);
+    if (n <= 128) {
+        uint64_t acc = len * 0x9E3779B185EBCA87ull;
+        if (n > 32) {
+            if (n > 64) {
+                if (n > 96) {
+                    acc += XxMix16(d + 48, 96);
+                    acc += XxMix16(d + n - 64, 112);
+                }
+                acc += XxMix16(d + 32, 64);
+                acc += XxMix16(d + n - 48, 80);
+            }
+            acc += XxMix16(d + 16, 32);
+            acc += XxMix16(d + n - 32, 48);
+        }
+        acc += XxMix16(d, 0);
+        acc += XxMix16(d + n - 16, 16);
+        return XxAvalanche(acc);
+    }
+    if (n <= 240) {
+        uint64_t acc = len * 0x9E3779B185EBCA87ull;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc += XxMix16(d + 16 * i, 16 * i);
+        acc = XxAvalanche(acc);
+        const int rounds = int(n / 16);
+        for (int i = 8; i < rounds; ++i) acc += XxMix16(d + 16 * i, 16 * (i - 8) + 3);
+        acc += XxMix16(d + n - 16, kStrSecretBytes - 17);
+        return XxAvalanche(acc);
+    }
+    return Xxh3Long(d, n);
+}
+
+// The string of row r of a string column (offsets of 4 or 8 bytes).
+__device__ __forceinline__ uint64_t StringCellHash(const ColDesc& cd, int64_t r) {
+    int64_t b, e;
+    if (cd.offset_width == 8) {
+        b = reinterpret_cast<const int64_t*>(cd.offsets)[r];
+        e = reinterpret_cast<const int64_t*>(cd.offsets)[r + 1];
+    } else {
+        b = reinterpret_cast<const int32_t*>(cd.offsets)[r];
+        e = reinterpret_cast<const int32_t*>(cd.offsets)[r + 1];
+    }
+    return StringHashDev(reinterpret_cast<const uint8_t*>(cd.data) + b, e - b);
+}
+
+// STR: some key column is a string (the string hash is compiled in only then,
+// so that integer keys keep the lean kernel).
+template <bool STR>
 __global__ void __launch_bounds__(256) HashKernel(const __grid_constant__ ExprLaunch L) {
     const AggPlan& P = L.P;
     unsigned long long kept = 0;
@@ -179,7 +316,9 @@ __global__ void __launch_bounds__(256) HashKernel(const __grid_constant__ ExprLa
             // A nullable key is two struct fields: its BOOL validity, then the value.
             if (L.A.hash_nullable[j]) h = Combine(h, null ? 0 : LeafHashOf(QDB_TYPE_BOOL, 1, 0.0));
             uint64_t fh = 0;
-            if (!null) {
+            if (STR && !null && t == QDB_TYPE_STRING) {
+                fh = StringCellHash(P.cols[c], r);
+            } else if (!null) {
                 const bool fl = t == QDB_TYPE_F32 || t == QDB_TYPE_F64;
                 fh = LeafHashOf(t, fl ? i128(0) : acc.Int(c), fl ? acc.F64(c) : 0.0);
             }
@@ -331,8 +470,11 @@ void HashRows(const ExprArgs& a, cudaStream_t s) {
     ExprLaunch& L = *ThreadLaunch();
     L.P = *a.plan;
     L.A = a;
+    bool str = false;
+    for (int j = 0; j < a.nhash; ++j) str = str || a.hash_type[j] == QDB_TYPE_STRING;
     ProfileBegin(s, "hash", a.nrows);
-    HashKernel<<<Blocks(a.nrows, 256), 256, 0, s>>>(L);
+    if (str) HashKernel<true><<<Blocks(a.nrows, 256), 256, 0, s>>>(L);
+    else HashKernel<false><<<Blocks(a.nrows, 256), 256, 0, s>>>(L);
     ProfileEnd(s);
     CountLaunch();
 }

@@ -51,6 +51,8 @@ struct ColDesc {
     int32_t smem_off;        // byte offset of its tile inside a stage
     int32_t scale;           // decimal scale (F64() divides by 10^scale)
     int32_t build;           // fused join: value comes from the matched build row
+    const char* offsets;     // QDB_TYPE_STRING: device offsets (row 0 of the range), `data` the bytes
+    int32_t offset_width;    // 4 or 8 (0: not a string column)
 };
 
 // Value kinds of the fast path and of state words.

@@ -312,6 +312,47 @@ Staging::~Staging() {
 }
 
 // Resolves the plan's probe/scan column slots against a row set.
+// A string column's offsets and bytes on the device.  Host offsets give the
+// byte count to stage; device offsets need device bytes.
+bool ResolveStrings(ColDesc& cd, const qdb_column& c, int64_t n, Staging& st, int input) {
+    const int ow = c.OffsetWidth;
+    if ((ow != 4 && ow != 8) || (n > 0 && (!c.Offsets || !c.Data))) {
+        SetErr("string column %d needs offsets of width 4 or 8 and data", input);
+        return false;
+    }
+    cd.offset_width = ow;
+    if (n == 0) {
+        cd.offsets = nullptr;
+        cd.data = nullptr;
+        return true;
+    }
+    if (IsDevicePtr(c.Offsets)) {
+        if (!IsDevicePtr(c.Data)) {
+            SetErr("string column %d: device offsets with host bytes", input);
+            return false;
+        }
+        cd.offsets = static_cast<const char*>(c.Offsets);
+        cd.data = c.Data;
+        return true;
+    }
+    // Host offsets are checked here (non-decreasing from a non-negative
+    // start), so that the kernel reads only the staged bytes; device offsets
+    // are taken as Arrow guarantees them.
+    int64_t prev = 0, end = 0;
+    for (int64_t r = 0; r <= n; ++r) {
+        const int64_t o = ow == 8 ? static_cast<const int64_t*>(c.Offsets)[r] : static_cast<const int32_t*>(c.Offsets)[r];
+        if (o < prev) {
+            SetErr("string column %d: offsets decrease at row %lld", input, (long long)r);
+            return false;
+        }
+        prev = end = o;
+    }
+    cd.offsets = static_cast<const char*>(st.Device(c.Offsets, size_t(n + 1) * size_t(ow)));
+    // No bytes at all (every string empty): no byte is ever read.
+    cd.data = end > 0 ? static_cast<const char*>(st.Device(c.Data, size_t(end))) : cd.offsets;
+    return cd.offsets != nullptr && cd.data != nullptr;
+}
+
 bool ResolveColumns(AggPlan& P, const ColumnMap& cm, const qdb_column_type* types, const qdb_rowset* rs,
                     Staging& st) {
     const int64_t n = rs->RowCount;
@@ -325,7 +366,11 @@ bool ResolveColumns(AggPlan& P, const ColumnMap& cm, const qdb_column_type* type
         }
         const qdb_column& c = rs->Columns[input];
         const int t = types[input].type;
-        if (t == QDB_TYPE_BOOL) {
+        cd.offsets = nullptr;
+        cd.offset_width = 0;
+        if (t == QDB_TYPE_STRING) {
+            if (!ResolveStrings(cd, c, n, st, input)) return false;
+        } else if (t == QDB_TYPE_BOOL) {
             const size_t bytes = size_t((c.DataBitOffset + n + 7) / 8);
             cd.data = static_cast<const char*>(st.Device(c.Data, bytes));
             cd.bit_off = c.DataBitOffset;
@@ -354,8 +399,13 @@ AggPlan OffsetPlan(const AggPlan& P, int64_t begin) {
     for (int slot = 0; slot < q.ncols; ++slot) {
         ColDesc& cd = q.cols[slot];
         if (cd.build) continue;
-        if (cd.kind == LK_BOOLBIT) cd.bit_off += begin;
-        else cd.data += begin * cd.width;
+        if (cd.offset_width) {
+            if (cd.offsets) cd.offsets += begin * cd.offset_width;   // the offsets index the bytes from 0
+        } else if (cd.kind == LK_BOOLBIT) {
+            cd.bit_off += begin;
+        } else {
+            cd.data += begin * cd.width;
+        }
         if (cd.mask) cd.mask_off += begin;
     }
     if (q.selection) q.selection += begin;
@@ -957,11 +1007,19 @@ qdb_gpu_program* qdb_gpu_compile_hash(int32_t n_columns, const qdb_column_type* 
                                       const int32_t* key_columns, char* err, size_t err_len) {
     try {
         if (n_keys < 1 || n_keys > kMaxKeyParts) throw LowerError("hash needs 1..6 key columns");
+        if (n_columns < 1 || !columns) throw LowerError("hash needs an input schema");
+        // A string key is lowered as a 64-bit slot (its offsets and bytes are
+        // resolved per batch from the true schema kept on the program), and
+        // the hash kernel reads it as a string.
+        std::vector<qdb_column_type> lowered(columns, columns + n_columns);
+        for (qdb_column_type& ct : lowered) {
+            if (ct.type == QDB_TYPE_STRING) ct.type = QDB_TYPE_U64;
+        }
         std::vector<qdb_expr> nodes(n_keys);
         std::vector<int32_t> exprs(n_keys);
         for (int j = 0; j < n_keys; ++j) {
             if (key_columns[j] < 0 || key_columns[j] >= n_columns) throw LowerError("key column out of range");
-            const qdb_column_type& ct = columns[key_columns[j]];
+            const qdb_column_type& ct = lowered[size_t(key_columns[j])];
             std::memset(&nodes[j], 0, sizeof(qdb_expr));
             nodes[j].op = QDB_EXPR_COLUMN;
             nodes[j].type = ct.type;
@@ -972,7 +1030,7 @@ qdb_gpu_program* qdb_gpu_compile_hash(int32_t n_columns, const qdb_column_type* 
         auto* p = new qdb_gpu_program();
         p->kind = PK_HASH;
         p->columns.assign(columns, columns + n_columns);
-        p->expr = LowerProject(n_columns, columns, n_keys, nodes.data(), n_keys, exprs.data());
+        p->expr = LowerProject(n_columns, lowered.data(), n_keys, nodes.data(), n_keys, exprs.data());
         for (int j = 0; j < n_keys; ++j) {
             p->expr.value_idx[j] = p->expr.cols.slot_of[key_columns[j]];
             p->expr.out_types[j] = columns[key_columns[j]].type;

@@ -203,6 +203,10 @@ int64_t qdb_gpu_shuffle(const qdb_gpu_program* prog, qdb_rowset* batch, const in
             SetErr("shuffle: bit-packed BOOL columns are not served");
             return -1;
         }
+        if (t.type == QDB_TYPE_STRING) {
+            SetErr("shuffle: string columns are hashed (qdb_gpu_hash) but not gathered");
+            return -1;
+        }
     }
     const int64_t n = batch->RowCount;
     cudaStream_t s = CurStream();

@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(kExtractThreads) SortExtractKernel(const __gri
 // ---------------------------------------------------------------------------
 // Onesweep pass.
 // ---------------------------------------------------------------------------
-constexpr int kPassThreads = 512;
+constexpr int kPassThreads = 256;   // 16 keys per thread; three CTAs per SM
 constexpr int kPassItems = kSortTile / kPassThreads;
 constexpr int kPassWarps = kPassThreads / 32;
 constexpr unsigned long long kFlagAgg = 1ull << 62;
@@ -480,7 +480,7 @@ __device__ __forceinline__ void PassTile(const PassLaunch<K>& a, PassShared& sh,
 }
 
 template <typename K>
-__global__ void __launch_bounds__(kPassThreads, 2) SortPassKernel(const __grid_constant__ PassLaunch<K> a) {
+__global__ void __launch_bounds__(kPassThreads, 3) SortPassKernel(const __grid_constant__ PassLaunch<K> a) {
     extern __shared__ __align__(16) unsigned char dyn[];
     K* skeys = reinterpret_cast<K*>(dyn);
     uint32_t* sidx = reinterpret_cast<uint32_t*>(dyn + size_t(kSortTile) * sizeof(K));
