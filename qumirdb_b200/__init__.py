@@ -246,10 +246,10 @@ class DeviceRowSet:
                 self.cols[k].Data = db.ptr
                 self.cols[k].Offsets = ob.ptr
                 self.cols[k].OffsetWidth = a.offsets.itemsize
-                continue
-            b = DeviceBuffer(a.nbytes).upload(a, stream_sync=False)
-            self.bufs.append(b)
-            self.cols[k].Data = b.ptr
+            else:
+                b = DeviceBuffer(a.nbytes).upload(a, stream_sync=False)
+                self.bufs.append(b)
+                self.cols[k].Data = b.ptr
             if host.masks[k] is not None:
                 mb = DeviceBuffer(host.masks[k].nbytes).upload(host.masks[k], stream_sync=False)
                 self.bufs.append(mb)
