@@ -1198,12 +1198,79 @@ Val StoreCell(const qdb_sort_spec& s, const qdb_rowset* store, int64_t packed, i
     return ReadCell(store[batch].Columns[col], s.columns[col], row);
 }
 
+// sr_sort_compare (qdb/kernel/sort/sort_rowids.oz:616-650): memcmp over the
+// common length, then the shorter first.
+int StringCompare(const Val& a, const Val& b) {
+    const int64_t m = std::min(a.n, b.n);
+    for (int64_t i = 0; i < m; ++i) {
+        if (a.s[i] != b.s[i]) return a.s[i] < b.s[i] ? -1 : 1;
+    }
+    return a.n < b.n ? -1 : (a.n > b.n ? 1 : 0);
+}
+
+// sort_string_rowids / sort_string_rowids_nullable (sort_rowids.oz:876-1060):
+// (8-byte big-endian prefix, row id) pairs through eight stable byte passes
+// (DESC walks the buckets downwards; NULLs in bucket 0 or 256 by
+// nulls_first), then every run of equal prefixes among the valid rows is
+// ordered stably by the full comparison (sr_pair_tiebreak_runs, :818-846).
+void SortStringKey(const qdb_sort_spec& s, const qdb_rowset* store, std::vector<int64_t>& ids, int col, bool desc,
+                   bool nulls_first) {
+    const size_t n = ids.size();
+    std::vector<Val> cell(n);
+    std::vector<uint64_t> prefix(n, 0);
+    for (size_t i = 0; i < n; ++i) {
+        cell[i] = StoreCell(s, store, ids[i], col);
+        if (cell[i].null) continue;
+        const int64_t lim = std::min<int64_t>(cell[i].n, 8);
+        uint64_t p = 0;
+        for (int64_t j = 0; j < lim; ++j) p = (p << 8) | cell[i].s[j];
+        prefix[i] = p << (8 * (8 - lim));
+    }
+    std::vector<size_t> order(n), tmp(n);
+    for (size_t i = 0; i < n; ++i) order[i] = i;
+    for (int digit = 0; digit < 64; digit += 8) {
+        std::vector<size_t> count(259, 0);   // buckets 0 .. 257, shifted by one
+        auto bucket = [&](size_t i) -> size_t {
+            if (cell[i].null) return nulls_first ? 0 : 257;
+            size_t b = size_t((prefix[i] >> digit) & 255);
+            if (desc) b = 255 - b;
+            return b + 1;
+        };
+        for (size_t i : order) ++count[bucket(i) + 1];
+        for (size_t b = 1; b < count.size(); ++b) count[b] += count[b - 1];
+        for (size_t i : order) tmp[count[bucket(i)]++] = i;
+        order.swap(tmp);
+    }
+    size_t lo = 0, hi = n;
+    while (lo < hi && cell[order[lo]].null) ++lo;
+    while (lo < hi && cell[order[hi - 1]].null) --hi;
+    for (size_t a = lo; a < hi;) {
+        size_t b = a + 1;
+        while (b < hi && prefix[order[b]] == prefix[order[a]]) ++b;
+        if (b - a > 1) {
+            std::stable_sort(order.begin() + std::ptrdiff_t(a), order.begin() + std::ptrdiff_t(b),
+                             [&](size_t x, size_t y) {
+                                 const int c = StringCompare(cell[x], cell[y]);
+                                 return desc ? c > 0 : c < 0;
+                             });
+        }
+        a = b;
+    }
+    std::vector<int64_t> out(n);
+    for (size_t i = 0; i < n; ++i) out[i] = ids[order[i]];
+    ids.swap(out);
+}
+
 // sort_fixed_rowids(_nullable) for one key: NULL rows keep input order at
-// the chosen end, valid rows are LSD-sorted.
+// the chosen end, valid rows are LSD-sorted (strings: SortStringKey).
 void SortOneKey(const qdb_sort_spec& s, const qdb_rowset* store, std::vector<int64_t>& ids,
                 int col, bool desc, bool nulls_first) {
     const int t = s.columns[col].type;
     if (t == QDB_TYPE_DECIMAL128) throw Error("DECIMAL128 sort keys are not restated");
+    if (t == QDB_TYPE_STRING) {
+        SortStringKey(s, store, ids, col, desc, nulls_first);
+        return;
+    }
     std::vector<uint64_t> keys;
     std::vector<int64_t> valid_ids, null_ids;
     for (int64_t id : ids) {

@@ -2562,8 +2562,8 @@ struct SeedSlot {
     unsigned pad;
 };
 
-constexpr int kSeedSampleRows = 1 << 18;
-constexpr int kSeedTableSlots = 1 << 19;   // twice the sample: at most half full
+constexpr int kSeedSampleRows = 1 << 16;
+constexpr int kSeedTableSlots = 1 << 17;   // twice the sample: at most half full
 constexpr int kSeedProbe = 64;
 constexpr int kSeedHistBins = 1024;
 

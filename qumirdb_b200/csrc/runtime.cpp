@@ -591,7 +591,7 @@ void AggStateDestroy(AggTableState* st) {
     delete st;
 }
 
-constexpr int64_t kSeedMinRows = int64_t(4) << 20;   // updates worth a heavy-hitter sample
+constexpr int64_t kSeedMinRows = int64_t(16) << 20;  // updates worth a heavy-hitter sample (~60 us)
 constexpr int kSeedKeys = 2048;                        // seeds kept (the tier takes up to half its slots)
 
 // Runs the fused kernel over `rows` rows of a resolved plan, then replays

@@ -210,6 +210,36 @@ __device__ __forceinline__ void StageKeys(const StoreTable& st, const SortStage&
         db[u] = (sc.width == 0 && c[u] >= 0) ? st.data_bit[c[u]] : 0;
     }
     uint64_t raw[U];
+    if (sg.src == SS_STR_CHUNK || sg.src == SS_STR_LEN) {
+        // NULL strings take key 0: their order is the NULL rank stage's.
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            uint64_t key = 0;
+            if (valid[u]) {
+                const char* off = st.offsets[c[u]];
+                int64_t b, e;
+                if (sc.width == 8) {
+                    b = reinterpret_cast<const int64_t*>(off)[row[u]];
+                    e = reinterpret_cast<const int64_t*>(off)[row[u] + 1];
+                } else {
+                    b = reinterpret_cast<const int32_t*>(off)[row[u]];
+                    e = reinterpret_cast<const int32_t*>(off)[row[u] + 1];
+                }
+                const int64_t len = e - b;
+                if (sg.src == SS_STR_LEN) {
+                    key = uint64_t(len);
+                } else {
+                    const uint8_t* p = reinterpret_cast<const uint8_t*>(d[u]) + b;
+                    const int64_t at = 8 * int64_t(sg.chunk);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) key = (key << 8) | (at + j < len ? p[at + j] : 0u);
+                }
+                key ^= sc.dmask;
+            }
+            k[u] = key;
+        }
+        return;
+    }
     if (sg.src == SS_NULL_RANK) {
 #pragma unroll
         for (int u = 0; u < U; ++u) k[u] = valid[u] ? sc.rank_valid : sc.rank_null;
@@ -987,6 +1017,11 @@ KeyCodec CodecOf(const SortStage& sg) {
 // The codec of a stage (StageKey's arithmetic).
 StageCodec StageCodecOf(const SortStage& sg) {
     StageCodec c{};
+    if (sg.src == SS_STR_CHUNK || sg.src == SS_STR_LEN) {
+        c.width = sg.owidth;
+        c.dmask = sg.desc ? ~0ull : 0ull;
+        return c;
+    }
     const int bits = SortKeyBits(sg.type);
     c.width = SortKeyWidth(sg.type) < 0 ? 8 : SortKeyWidth(sg.type);
     c.flt = sg.type == QDB_TYPE_F32 ? 4 : (sg.type == QDB_TYPE_F64 ? 8 : 0);
@@ -1017,9 +1052,50 @@ int Blocks(int64_t n, int threads, int per_sm) {
 
 }  // namespace
 
+__global__ void __launch_bounds__(256) SortStringMaxLenKernel(const int64_t* ids, int64_t n, StoreTable st, int tcol,
+                                                              int owidth, unsigned long long* out, int* err) {
+    unsigned long long m = 0;
+    bool bad = false;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const uint32_t batch = uint32_t(uint64_t(ids[i]) >> 32);
+        const int64_t row = int64_t(uint32_t(uint64_t(ids[i])));
+        if (batch >= uint32_t(st.nbatches)) {
+            bad = true;
+            continue;
+        }
+        const char* off = st.offsets[int64_t(batch) * st.ncols + tcol];
+        const int64_t len = owidth == 8 ? reinterpret_cast<const int64_t*>(off)[row + 1] -
+                                              reinterpret_cast<const int64_t*>(off)[row]
+                                        : int64_t(reinterpret_cast<const int32_t*>(off)[row + 1]) -
+                                              int64_t(reinterpret_cast<const int32_t*>(off)[row]);
+        m = max(m, (unsigned long long)max(len, int64_t(0)));
+    }
+    m = WarpMaxU64(m);
+    if (LaneId() == 0 && m) atomicMax(out, m);
+    if (bad) SetError(err, DE_BAD_ROW_ID);
+}
+
+void SortStringMaxLen(const int64_t* ids, int64_t n, const StoreTable& st, int tcol, int owidth,
+                      unsigned long long* out, int* err, cudaStream_t s) {
+    if (n == 0) return;
+    ProfileBegin(s, "sort_string_len", n);
+    SortStringMaxLenKernel<<<Blocks(n, 256, 4), 256, 0, s>>>(ids, n, st, tcol, owidth, out, err);
+    ProfileEnd(s);
+    CountLaunch();
+}
+
 void SortExtract(const int64_t* ids, int64_t n, const StoreTable& st, const SortStage* stages, int nstages,
                  void* const* keys, unsigned long long* hist, int* err, cudaStream_t s) {
     if (n == 0 || nstages == 0) return;
+    // At most kMaxSortStages stages per launch (their histograms live in
+    // shared memory); more go in further launches.
+    if (nstages > kMaxSortStages) {
+        for (int g = 0; g < nstages; g += kMaxSortStages) {
+            const int m = std::min(kMaxSortStages, nstages - g);
+            SortExtract(ids, n, st, stages + g, m, keys + g, hist + size_t(g) * kSortDigits * 256, err, s);
+        }
+        return;
+    }
     static thread_local ExtractLaunch L;
     L = ExtractLaunch{};
     L.ids = ids;

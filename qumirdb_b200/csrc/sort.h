@@ -12,7 +12,8 @@ namespace qdb {
 // entry b * ncols + c is column slot c of batch b).  A packed row id is
 // (batch << 32) | row (qdb/exec/join_exec.h:25-36).
 struct StoreTable {
-    const char* const* data = nullptr;
+    const char* const* data = nullptr;      // string columns: the bytes
+    const char* const* offsets = nullptr;   // string columns: Arrow offsets (4 or 8 bytes each)
     const uint8_t* const* mask = nullptr;   // validity bitmaps (nullptr entries: all valid)
     const int64_t* data_bit = nullptr;      // DataBitOffset (bit-packed BOOL)
     const int64_t* mask_bit = nullptr;      // MaskBitOffset
@@ -24,7 +25,11 @@ struct StoreTable {
 // of a column (DESC inverted, NULL rank packed above keys of <= 32 bits), the
 // NULL rank of a 64-bit key (a separate, more significant stage), or the
 // packed row id itself (top-K tie break).
-enum SortStageSrc : int32_t { SS_KEY = 0, SS_NULL_RANK = 1, SS_ROW_ID = 2 };
+// A string key is ordered by the bytes, shorter first on a common prefix
+// (sr_sort_compare): stages of its 8-byte big-endian chunks, zero-padded
+// (chunk 0 most significant), and below them its length, which breaks the
+// ties that the padding leaves; its NULL rank is a stage above them all.
+enum SortStageSrc : int32_t { SS_KEY = 0, SS_NULL_RANK = 1, SS_ROW_ID = 2, SS_STR_CHUNK = 3, SS_STR_LEN = 4 };
 
 struct SortStage {
     int32_t src = SS_KEY;
@@ -34,10 +39,13 @@ struct SortStage {
     int32_t nulls_first = 0;
     int32_t nullable = 0;
     int32_t wide = 0;          // u64 stage keys (else u32)
+    int32_t chunk = 0;         // SS_STR_CHUNK: bytes [8 * chunk, 8 * chunk + 8)
+    int32_t owidth = 0;        // string stages: offset bytes (4 or 8)
     int32_t pad = 0;
 };
 
-constexpr int kMaxSortStages = 16;
+constexpr int kMaxSortStages = 16;                 // stages one extraction launch writes
+constexpr int kMaxSortStagesTotal = 48;            // stages of one sort (string keys add a stage per 8 bytes)
 constexpr int kSortDigits = 8;                     // 8-bit digits of a u64 key
 constexpr int kSortTile = 4096;                    // keys per onesweep tile
 
@@ -51,6 +59,11 @@ __host__ __device__ inline int SortKeyBits(int type) {
         default: return 0;
     }
 }
+
+// Longest string (bytes) of column slot `tcol` (offsets of `owidth` bytes)
+// among the rows ids[0, n), into *out (device, pre-zeroed).
+void SortStringMaxLen(const int64_t* ids, int64_t n, const StoreTable& st, int tcol, int owidth,
+                      unsigned long long* out, int* err, cudaStream_t s);
 
 // Writes every stage's keys (input order, u32 or u64 by stage.wide) and
 // adds their digit histograms (stage-major, kSortDigits x 256 counters) to

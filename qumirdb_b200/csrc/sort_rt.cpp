@@ -29,7 +29,8 @@ constexpr int64_t kTopKSamples = 32768;
 struct StoreView {
     StoreTable t;
     std::vector<int> cols;   // slot -> store column
-    void* dev = nullptr;     // one allocation holding the four tables
+    std::vector<int> owidth; // slot -> string offset bytes (0: not a string column)
+    void* dev = nullptr;     // one allocation holding the five tables
     cudaStream_t s = nullptr;
     ~StoreView() { DevFree(dev, s); }
     int Slot(int col) const {
@@ -40,13 +41,51 @@ struct StoreView {
     }
 };
 
+// A batch's string column on the device: its offsets and bytes (host
+// offsets are checked to be non-decreasing, so that only staged bytes are
+// read); every batch of a column must use one offset width.
+bool StageStrings(const qdb_column& c, int64_t rows, Staging& stg, int64_t b, int col, int& owidth,
+                  const char*& data, const char*& offs) {
+    const int ow = c.OffsetWidth;
+    if ((ow != 4 && ow != 8) || (owidth && owidth != ow) || (rows > 0 && (!c.Offsets || !c.Data))) {
+        SetErr("sort: string column %d of batch %lld needs offsets of one width (4 or 8) and data", col, (long long)b);
+        return false;
+    }
+    owidth = ow;
+    data = offs = nullptr;
+    if (rows == 0) return true;
+    if (IsDevicePtr(c.Offsets)) {
+        if (!IsDevicePtr(c.Data)) {
+            SetErr("sort: string column %d of batch %lld has device offsets and host bytes", col, (long long)b);
+            return false;
+        }
+        offs = static_cast<const char*>(c.Offsets);
+        data = c.Data;
+        return true;
+    }
+    int64_t prev = 0;
+    for (int64_t r = 0; r <= rows; ++r) {
+        const int64_t o = ow == 8 ? static_cast<const int64_t*>(c.Offsets)[r] : static_cast<const int32_t*>(c.Offsets)[r];
+        if (o < prev) {
+            SetErr("sort: string column %d of batch %lld: offsets decrease at row %lld", col, (long long)b,
+                   (long long)r);
+            return false;
+        }
+        prev = o;
+    }
+    offs = static_cast<const char*>(stg.Device(c.Offsets, size_t(rows + 1) * size_t(ow)));
+    data = prev > 0 ? static_cast<const char*>(stg.Device(c.Data, size_t(prev))) : offs;
+    return offs != nullptr && data != nullptr;
+}
+
 bool BuildStoreView(const SortProgram& P, const qdb_rowset* store, int64_t nbatches, Staging& stg, StoreView& v) {
     v.s = stg.s;
     const int nc = int(v.cols.size());
     const size_t cells = size_t(nbatches) * nc;
-    std::vector<const char*> data(cells);
+    std::vector<const char*> data(cells), offs(cells, nullptr);
     std::vector<const uint8_t*> mask(cells);
     std::vector<int64_t> dbit(cells), mbit(cells);
+    v.owidth.assign(size_t(nc), 0);
     for (int64_t b = 0; b < nbatches; ++b) {
         const qdb_rowset& rs = store[b];
         for (int j = 0; j < nc; ++j) {
@@ -61,9 +100,16 @@ bool BuildStoreView(const SortProgram& P, const qdb_rowset* store, int64_t nbatc
             const size_t i = size_t(b) * nc + j;
             const int64_t rows = rs.RowCount;
             size_t bytes;
-            if (type == QDB_TYPE_BOOL) bytes = size_t((c.DataBitOffset + rows + 7) / 8);
-            else bytes = size_t(rows) * size_t(type == QDB_TYPE_DECIMAL128 ? 16 : SortKeyBits(type) / 8);
-            data[i] = rows > 0 ? static_cast<const char*>(stg.Device(c.Data, std::max<size_t>(bytes, 1))) : nullptr;
+            if (type == QDB_TYPE_STRING) {
+                if (!StageStrings(c, rows, stg, b, col, v.owidth[size_t(j)], data[i], offs[i])) return false;
+                bytes = 0;
+            } else if (type == QDB_TYPE_BOOL) {
+                bytes = size_t((c.DataBitOffset + rows + 7) / 8);
+            } else {
+                bytes = size_t(rows) * size_t(type == QDB_TYPE_DECIMAL128 ? 16 : SortKeyBits(type) / 8);
+            }
+            if (type != QDB_TYPE_STRING)
+                data[i] = rows > 0 ? static_cast<const char*>(stg.Device(c.Data, std::max<size_t>(bytes, 1))) : nullptr;
             mask[i] = (c.Mask && rows > 0)
                           ? static_cast<const uint8_t*>(stg.Device(c.Mask, size_t((c.MaskBitOffset + rows + 7) / 8)))
                           : nullptr;
@@ -73,7 +119,7 @@ bool BuildStoreView(const SortProgram& P, const qdb_rowset* store, int64_t nbatc
         }
     }
     const size_t part = std::max<size_t>(cells, 1) * 8;
-    v.dev = DevAlloc(4 * part, stg.s);
+    v.dev = DevAlloc(5 * part, stg.s);
     if (!v.dev) return false;
     char* base = static_cast<char*>(v.dev);
     if (cells) {
@@ -81,7 +127,9 @@ bool BuildStoreView(const SortProgram& P, const qdb_rowset* store, int64_t nbatc
         cudaMemcpyAsync(base + part, mask.data(), cells * 8, cudaMemcpyHostToDevice, stg.s);
         cudaMemcpyAsync(base + 2 * part, dbit.data(), cells * 8, cudaMemcpyHostToDevice, stg.s);
         cudaMemcpyAsync(base + 3 * part, mbit.data(), cells * 8, cudaMemcpyHostToDevice, stg.s);
+        cudaMemcpyAsync(base + 4 * part, offs.data(), cells * 8, cudaMemcpyHostToDevice, stg.s);
     }
+    v.t.offsets = reinterpret_cast<const char* const*>(base + 4 * part);
     v.t.data = reinterpret_cast<const char* const*>(base);
     v.t.mask = reinterpret_cast<const uint8_t* const*>(base + part);
     v.t.data_bit = reinterpret_cast<const int64_t*>(base + 2 * part);
@@ -141,8 +189,11 @@ bool ReadError(int* derr, cudaStream_t s, const char* what) {
 // Stages of an ORDER BY, least significant first: key k from the last to the
 // first (compiler.cpp:595-599), a 64-bit nullable key followed by its NULL
 // rank.  With `id_first`, the packed row id is the least significant stage.
+// `chunks[k]`: 8-byte chunks of string key k (its longest string, rounded
+// up), known once the store view is built; without it a string key gets its
+// length stage only (enough to register its column in the view).
 std::vector<SortStage> MakeStages(const SortProgram& P, const bool* descs, const bool* nulls_firsts, bool id_first,
-                                  StoreView& v) {
+                                  StoreView& v, const std::vector<int>* chunks = nullptr) {
     std::vector<SortStage> st;
     if (id_first) {
         SortStage g;
@@ -165,6 +216,29 @@ std::vector<SortStage> MakeStages(const SortProgram& P, const bool* descs, const
         g.desc = descs ? descs[k] : P.keys[k].desc;
         g.nulls_first = nulls_firsts ? nulls_firsts[k] : P.keys[k].nulls_first;
         g.nullable = ct.nullable ? 1 : 0;
+        if (ct.type == QDB_TYPE_STRING) {
+            // Least significant first: the length, then the chunks from the
+            // last to the first, then the NULL rank.
+            g.wide = 1;
+            g.owidth = size_t(slot) < v.owidth.size() ? v.owidth[size_t(slot)] : 0;
+            SortStage len = g;
+            len.src = SS_STR_LEN;
+            st.push_back(len);
+            const int nch = chunks ? (*chunks)[size_t(k)] : 0;
+            for (int c = nch - 1; c >= 0; --c) {
+                SortStage ch = g;
+                ch.src = SS_STR_CHUNK;
+                ch.chunk = c;
+                st.push_back(ch);
+            }
+            if (g.nullable) {
+                SortStage r = g;
+                r.src = SS_NULL_RANK;
+                r.wide = 0;
+                st.push_back(r);
+            }
+            continue;
+        }
         const int bits = SortKeyBits(ct.type);
         g.wide = (bits > 32 || g.nullable) ? 1 : 0;
         st.push_back(g);
@@ -185,8 +259,9 @@ bool SortIds(int64_t* ids, int64_t n, const std::vector<SortStage>& stages, cons
     cudaStream_t s = sc.s;
     const int ns = int(stages.size());
     if (n <= 1 || ns == 0) return true;
-    if (ns > kMaxSortStages) {
-        SetErr("sort: at most %d key stages are served", kMaxSortStages);
+    if (ns > kMaxSortStagesTotal) {
+        SetErr("sort: at most %d key stages are served (a string key takes one per 8 bytes of its longest value)",
+               kMaxSortStagesTotal);
         return false;
     }
     bool any_wide = false;
@@ -266,6 +341,36 @@ bool SortIds(int64_t* ids, int64_t n, const std::vector<SortStage>& stages, cons
     }
     SortGatherIds(orig, idx, n, id_tiles, ids, s);
     return ReadError(derr, s, "sort: radix passes");
+}
+
+bool HasStringKey(const SortProgram& P) {
+    for (const qdb_sort_key& k : P.keys) {
+        if (P.columns[k.column].type == QDB_TYPE_STRING) return true;
+    }
+    return false;
+}
+
+// 8-byte chunks of every string key (of its longest value among the rows);
+// 0 for other keys.
+bool StringChunks(const SortProgram& P, const int64_t* ids, int64_t n, const StoreView& v, Scratch& sc,
+                  std::vector<int>& chunks) {
+    chunks.assign(P.keys.size(), 0);
+    auto* dmax = static_cast<unsigned long long*>(sc.Get(P.keys.size() * 8));
+    int* derr = static_cast<int*>(sc.Get(sizeof(int)));
+    if (!dmax || !derr) return false;
+    cudaMemsetAsync(dmax, 0, P.keys.size() * 8, sc.s);
+    cudaMemsetAsync(derr, 0, sizeof(int), sc.s);
+    for (size_t k = 0; k < P.keys.size(); ++k) {
+        const int col = P.keys[k].column;
+        if (P.columns[col].type != QDB_TYPE_STRING) continue;
+        const int slot = v.Slot(col);
+        SortStringMaxLen(ids, n, v.t, slot, v.owidth[size_t(slot)], dmax + k, derr, sc.s);
+    }
+    std::vector<unsigned long long> h(P.keys.size());
+    cudaMemcpyAsync(h.data(), dmax, h.size() * 8, cudaMemcpyDeviceToHost, sc.s);
+    if (!ReadError(derr, sc.s, "sort: string lengths")) return false;
+    for (size_t k = 0; k < h.size(); ++k) chunks[k] = int((h[k] + 7) / 8);
+    return true;
 }
 
 // Materializes the out columns of ids[0, rows) into `out`.
@@ -430,9 +535,10 @@ qdb_gpu_program* qdb_gpu_compile_sort(const qdb_sort_spec* spec, char* err, size
             delete p;
             return fail("sort: key column out of range");
         }
-        if (SortKeyBits(P.columns[k.column].type) == 0) {
+        if (SortKeyBits(P.columns[k.column].type) == 0 && P.columns[k.column].type != QDB_TYPE_STRING) {
             delete p;
-            return fail("sort: key type is not served (fixed-width integer, decimal64, date, float, bool, char1)");
+            return fail("sort: key type is not served (fixed-width integer, decimal64, date, float, bool, char1, "
+                        "string)");
         }
     }
     for (int c : P.out_columns) {
@@ -448,11 +554,13 @@ qdb_gpu_program* qdb_gpu_compile_sort(const qdb_sort_spec* spec, char* err, size
     }
     // Stages: every key plus a NULL rank per nullable 64-bit key, plus the row
     // id stage top-K adds.
+    // (A string key's stages depend on its longest value: checked per sort.)
     int stages = 1;
     for (const qdb_sort_key& k : P.keys) {
-        stages += 1 + ((P.columns[k.column].nullable && SortKeyBits(P.columns[k.column].type) == 64) ? 1 : 0);
+        const int t = P.columns[k.column].type;
+        stages += 1 + ((P.columns[k.column].nullable && (SortKeyBits(t) == 64 || t == QDB_TYPE_STRING)) ? 1 : 0);
     }
-    if (stages > kMaxSortStages) {
+    if (stages > kMaxSortStagesTotal) {
         delete p;
         return fail("sort: too many keys");
     }
@@ -491,8 +599,13 @@ int64_t qdb_gpu_sort_run(const qdb_gpu_program* program, qdb_rowset* store, int6
         int64_t nbatches = 0, sparse = 0;
         if (!BatchCount(ids, n, sc, nbatches, tiles, &sparse)) return -1;
         StoreView v;
-        const std::vector<SortStage> stages = MakeStages(prog->sort, descs, nulls_firsts, false, v);
+        std::vector<SortStage> stages = MakeStages(prog->sort, descs, nulls_firsts, false, v);
         if (!BuildStoreView(prog->sort, store, nbatches, stg, v)) return -1;
+        if (HasStringKey(prog->sort)) {
+            std::vector<int> chunks;
+            if (!StringChunks(prog->sort, ids, n, v, sc, chunks)) return -1;
+            stages = MakeStages(prog->sort, descs, nulls_firsts, false, v, &chunks);
+        }
         if (!SortIds(ids, n, stages, v.t, sc, tiles, sparse)) return -1;
         if (!dev_ids) {
             cudaMemcpyAsync(row_ids, ids, size_t(n) * 8, cudaMemcpyDeviceToHost, s);
@@ -522,6 +635,10 @@ int64_t qdb_gpu_top_k_select(const qdb_gpu_program* program, qdb_rowset* store, 
     t_error.clear();
     const qdb_gpu_program* prog = SortProgramOf(program);
     if (!prog) return -1;
+    if (HasStringKey(prog->sort)) {
+        SetErr("top-K: string keys are served by qdb_sort_run (then a slice), not by the top-K entries");
+        return -1;
+    }
     const int64_t k = std::min(limit, size);
     if (k <= 0) return 0;
     if (!store || !row_ids) {
@@ -564,6 +681,10 @@ int64_t qdb_gpu_top_sort_update(const qdb_gpu_program* program, qdb_rowset* stat
     t_error.clear();
     const qdb_gpu_program* prog = SortProgramOf(program);
     if (!prog) return -1;
+    if (HasStringKey(prog->sort)) {
+        SetErr("top-K: string keys are served by qdb_sort_run (then a slice), not by the top-K entries");
+        return -1;
+    }
     const SortProgram& P = prog->sort;
     if (!state || !batch || !out || (n > 0 && !row_ids) || n < 0) {
         SetErr("top-sort: state, batch, output and row ids are needed");

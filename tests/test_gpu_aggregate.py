@@ -211,12 +211,12 @@ def test_lineitem_runs_the_signature_kernel():
 
 
 def test_high_cardinality_heavy_hitter_seeds():
-    """An update of at least 4M rows samples its keys and seeds the shared
+    """An update of at least 16M rows samples its keys and seeds the shared
     tier with the most frequent; a later update (with a selection, and rows
     whose keys include none of some seeds) reuses them.  Rows of key -1 (the
     empty marker) take the table's flag slot.  Every group equals the
     oracle's."""
-    n = 6_000_000
+    n = 17_000_000
     first = zipf_data(n, 200_000, 11)
     first[0][::997] = -1
     second = zipf_data(1_000_000, 400_000, 12)
