@@ -229,10 +229,20 @@ __device__ __forceinline__ void StageKeys(const StoreTable& st, const SortStage&
                 if (sg.src == SS_STR_LEN) {
                     key = uint64_t(len);
                 } else {
-                    const uint8_t* p = reinterpret_cast<const uint8_t*>(d[u]) + b;
+                    // The chunk's bytes inside the string (0..8 of them);
+                    // every load reads one of the string's own bytes, and
+                    // the bytes past its end are masked to zero.
                     const int64_t at = 8 * int64_t(sg.chunk);
+                    const int64_t nb = min(int64_t(8), len - at);
+                    if (nb > 0) {
+                        const uint8_t* p = reinterpret_cast<const uint8_t*>(d[u]) + b + at;
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) key = (key << 8) | (at + j < len ? p[at + j] : 0u);
+                        for (int j = 0; j < 8; ++j) {
+                            const uint64_t byte = uint64_t(p[min(int64_t(j), nb - 1)]);
+                            const uint64_t keep = j < nb ? 0xffull : 0ull;
+                            key |= (byte & keep) << (56 - 8 * j);
+                        }
+                    }
                 }
                 key ^= sc.dmask;
             }
