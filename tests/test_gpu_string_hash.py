@@ -75,7 +75,7 @@ def test_nullable_string_beside_integer_keys_with_selection(where):
     k = rng.integers(-10**12, 10**12, N)
     valid = rng.random(N) > 0.15
     sel = (rng.random(N) > 0.3).astype(np.uint8)
-    schema = [(abi.I64,), (abi.STRING, 0, 0, 1)]
+    schema = [(abi.I64,), (abi.STRING, 0, 1)]
     for keys in ([1], [0, 1], [1, 0]):
         got, want = run([k, s], schema, keys, masks=[None, valid], sel=sel, where=where)
         np.testing.assert_array_equal(got[sel != 0], want[sel != 0])

@@ -64,7 +64,7 @@ def test_string_sort_matches_oracle(device, large, nullable, desc, nulls_first):
     rng = np.random.default_rng(4)
     valid = rng.random(n) > 0.2 if nullable else np.ones(n, bool)
     k = rng.integers(0, 5, n).astype(np.int64)
-    types = [(abi.STRING, 0, 0, 1 if nullable else 0), (abi.I64,)]
+    types = [(abi.STRING, 0, 1 if nullable else 0), (abi.I64,)]
     st = store(vals, k, valid, nullable, device, large)
     host = store(vals, k, valid, nullable, False, large)
     for keys in ([(0, desc, nulls_first)], [(1, 0, 0), (0, desc, nulls_first)], [(0, desc, nulls_first), (1, 1, 0)]):

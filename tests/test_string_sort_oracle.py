@@ -43,7 +43,7 @@ def test_string_sort_order(desc, nulls_first, nullable):
     rng = np.random.default_rng(9)
     valid = rng.random(n) > 0.2 if nullable else np.ones(n, bool)
     k2 = rng.integers(0, 4, n).astype(np.int64)
-    types = [(abi.STRING, 0, 0, 1 if nullable else 0), (abi.I64,)]
+    types = [(abi.STRING, 0, 1 if nullable else 0), (abi.I64,)]
     batches = store(vals, k2, valid, nullable)
     ids = np.concatenate([(np.int64(b) << 32) | np.arange(1000, dtype=np.int64) for b in range(3)])
     rng.shuffle(ids)
