@@ -268,6 +268,57 @@ def lineitem_operator(q, peak):
             "l2": "flushed between queries (256 MiB write)", "gpu_launches": launches / 10}
 
 
+def lineitem_batched_operator(q, peak):
+    """The config-0 lineitem table split into 64 contiguous partitions, each
+    its own aggregate of the Q1-shaped program, all in one
+    qdb_gpu_agg_dispatch_batch (the low-cardinality batched kernel) and one
+    batched finalize per query; L2 flushed between queries."""
+    from qumirdb_b200 import abi, queries
+    n = LINEITEM_ROWS
+    parts = 64
+    cols = [np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64),
+            np.empty(n, np.uint8), np.empty(n, np.uint8), np.empty(n, np.int32)]
+    q.lib().qdb_gen_lineitem(0, n, *[c.ctypes.data for c in cols])
+    prog = q.compile_aggregate(queries.lineitem_agg(int(cols[6].max()) - 90, flags=abi.OUT_DEVICE))
+    bounds = np.linspace(0, n, parts + 1).astype(np.int64)
+    rowsets = [q.DeviceRowSet([c[lo:hi] for c in cols]) for lo, hi in zip(bounds[:-1], bounds[1:])]
+    flush = q.DeviceBuffer(256 << 20)
+
+    import torch
+    stream = torch.cuda.ExternalStream(q.lib().qdb_gpu_get_stream())
+
+    def query():
+        b = q.AggregateBatch(prog, parts)
+        b.add(rowsets)
+        b.finish().release()
+
+    for _ in range(3):
+        flush_l2(q, flush)
+        query()
+    q.synchronize()
+    q.profile(True)
+    q.profile_read()
+    times = []
+    for _ in range(10):
+        flush_l2(q, flush)
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        query()
+        e.record(stream)
+        e.synchronize()
+        times.append(a.elapsed_time(e))
+    kernels = q.profile_read()
+    q.profile(False)
+    ms = statistics.median(times)
+    kms, _ = kernel_avg(kernels, "agg_batch_update_low", 10)
+    alg = n * 38
+    return {"workload": "lineitem scan-filter-aggregate, 6,001,215 rows as 64 partitions, one batched launch",
+            "rows_per_s": n / (ms / 1e3), "ms_per_query": ms, "kernel": "agg_batch_update_low", "kernel_ms": kms,
+            "algorithmic_bytes": alg, "kernel_gbs": alg / (kms / 1e3) / 1e9 if kms else None,
+            "frac_of_measured_hbm": (alg / (kms / 1e3) / 1e9) / peak if kms else None,
+            "l2": "flushed between queries (256 MiB write)"}
+
+
 def flush_l2(q, buf):
     q.lib().qdb_gpu_memset(buf.ptr, 0, buf.nbytes)
 
@@ -796,7 +847,7 @@ def compact_operators(ops: dict) -> dict:
         return None if x is None else float(f"{x:.{nd}g}")
 
     out = {}
-    for name in ("lineitem", "zipf", "zipf_batched", "join_batched", "sort"):
+    for name in ("lineitem", "lineitem_batched", "zipf", "zipf_batched", "join_batched", "sort"):
         o = ops.get(name)
         if not o:
             continue
@@ -845,14 +896,15 @@ def main() -> None:
                     help="run one workload twice at --rows rows (for profiler captures) and exit")
     ap.add_argument("--rows", type=int, default=0)
     ap.add_argument("--detail", help="write every operator's full figures (serving sweeps included) to this file")
-    ap.add_argument("--only", choices=["lineitem", "zipf", "zipf_batched", "sort", "serving"],
+    ap.add_argument("--only", choices=["lineitem", "lineitem_batched", "zipf", "zipf_batched", "sort", "serving"],
                     help="run one operator's measurement and print its JSON")
     args = ap.parse_args()
     if args.only:
         import qumirdb_b200 as q
         q.init(0)
         peak, _ = peaks()
-        fn = {"lineitem": lambda: lineitem_operator(q, peak), "zipf": lambda: zipf_operator(q, peak),
+        fn = {"lineitem": lambda: lineitem_operator(q, peak),
+              "lineitem_batched": lambda: lineitem_batched_operator(q, peak), "zipf": lambda: zipf_operator(q, peak),
               "zipf_batched": lambda: zipf_batched_operator(q, peak), "sort": lambda: sort_operator(q, peak),
               "serving": lambda: serving_operator(q)}[args.only]
         print(json.dumps({args.only: fn()}), flush=True)
@@ -949,7 +1001,8 @@ def main() -> None:
     if rank == 0 and world == 1 and not args.no_operators:
         ops = {}
         try:
-            ops = {"lineitem": lineitem_operator(q, peak), "zipf": zipf_operator(q, peak),
+            ops = {"lineitem": lineitem_operator(q, peak), "lineitem_batched": lineitem_batched_operator(q, peak),
+                   "zipf": zipf_operator(q, peak),
                    "zipf_batched": zipf_batched_operator(q, peak), "join_batched": join_batched_operator(q, peak, w),
                    "sort": sort_operator(q, peak),
                    "serving": serving_operator(q)}

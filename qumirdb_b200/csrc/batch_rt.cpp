@@ -668,6 +668,14 @@ int64_t DispatchBatch(const qdb_gpu_program* prog, void* const* hts, qdb_rowset*
         std::lock_guard<std::mutex> lk(tn.mu);
         tn.best[{shape, rows_class, states_class}] = cfg;
         tn.tuned++;
+    } else if (!found && low) {
+        // Untuned low-cardinality batches: items small enough (16K-128K
+        // rows) that the launch has about four per SM; with one big item per
+        // aggregate, a batch of fewer aggregates than SMs left SMs idle.
+        const int64_t per = total_rows / (int64_t(DeviceSMs()) * 4);
+        int64_t c = int64_t(1) << 14;
+        while (c < per && c < (int64_t(1) << 17)) c <<= 1;
+        cfg.chunk_rows = c;
     }
 
     std::vector<int> order(static_cast<size_t>(m));
