@@ -765,6 +765,18 @@ def profile_case(name: str, rows: int) -> None:
             a = q.Aggregate(prog)
             a.add(drs)
             q.release(a.finish())
+    elif name == "lineitem_batched":
+        n = rows or LINEITEM_ROWS
+        cols = [np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64), np.empty(n, np.int64),
+                np.empty(n, np.uint8), np.empty(n, np.uint8), np.empty(n, np.int32)]
+        q.lib().qdb_gen_lineitem(0, n, *[c.ctypes.data for c in cols])
+        prog = q.compile_aggregate(queries.lineitem_agg(int(cols[6].max()) - 90))
+        bounds = np.linspace(0, n, 65).astype(np.int64)
+        rowsets = [q.DeviceRowSet([c[lo:hi] for c in cols]) for lo, hi in zip(bounds[:-1], bounds[1:])]
+        for _ in range(2):
+            b = q.AggregateBatch(prog, 64)
+            b.add(rowsets)
+            b.finish().release()
     elif name == "join":
         n = rows or PROBE_ROWS
         b = [np.empty(BUILD_ROWS, np.int64), np.empty(BUILD_ROWS, np.int64), np.empty(BUILD_ROWS, np.int32)]
@@ -891,8 +903,8 @@ def main() -> None:
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--no-operators", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-case", choices=["join", "join_batched", "sort", "topk", "lineitem", "zipf",
-                                               "zipf_batched"],
+    ap.add_argument("--profile-case", choices=["join", "join_batched", "sort", "topk", "lineitem",
+                                               "lineitem_batched", "zipf", "zipf_batched"],
                     help="run one workload twice at --rows rows (for profiler captures) and exit")
     ap.add_argument("--rows", type=int, default=0)
     ap.add_argument("--detail", help="write every operator's full figures (serving sweeps included) to this file")

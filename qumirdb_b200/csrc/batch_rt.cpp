@@ -201,6 +201,47 @@ void BuildItems(const std::vector<int64_t>& rows, const std::vector<int>& order,
     }
 }
 
+// Work items for a launch of `grid` CTAs: about `target` items in all, each
+// state's share of them in proportion to its rows (largest remainders round
+// up), a state's items of equal size on four-row boundaries, and the queue
+// ordered biggest item first.  With a target that is a multiple of the grid,
+// every CTA draws the same number of near-equal items and none waits out a
+// partial last wave, which a fixed item size leaves whenever a state's rows
+// are not a multiple of it.
+void BuildItemsBalanced(const std::vector<int64_t>& rows, int64_t target, std::vector<HighItem>& items) {
+    items.clear();
+    const size_t m = rows.size();
+    int64_t total = 0;
+    for (int64_t r : rows) total += r;
+    if (total == 0) return;
+    std::vector<int64_t> n(m, 0);
+    std::vector<std::pair<double, int>> frac;
+    int64_t given = 0;
+    for (size_t t = 0; t < m; ++t) {
+        if (rows[t] == 0) continue;
+        const double want = double(target) * double(rows[t]) / double(total);
+        n[t] = std::max<int64_t>(1, int64_t(want));
+        given += n[t];
+        frac.push_back({want - double(int64_t(want)), int(t)});
+    }
+    std::stable_sort(frac.begin(), frac.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+        return a.first > b.first;
+    });
+    for (size_t k = 0; k < frac.size() && given < target; ++k, ++given) n[size_t(frac[k].second)]++;
+    for (size_t t = 0; t < m; ++t) {
+        if (rows[t] == 0) continue;
+        const int64_t q = ((rows[t] + n[t] - 1) / n[t] + 3) & ~int64_t(3);
+        for (int64_t r0 = 0; r0 < rows[t]; r0 += q) {
+            HighItem it;
+            it.task = int32_t(t);
+            it.nrows = int32_t(std::min<int64_t>(q, rows[t] - r0));
+            it.row0 = r0;
+            items.push_back(it);
+        }
+    }
+    std::stable_sort(items.begin(), items.end(), [](const HighItem& a, const HighItem& b) { return a.nrows > b.nrows; });
+}
+
 int GridFor(const AggPlan& p, const FastPlan& f, const BatchConfig& c, int64_t nitems, bool low) {
     const int occ = std::max(1, AggBatchOccupancy(p, f, c.threads, c.smem_slots, low));
     return int(std::max<int64_t>(1, std::min<int64_t>(nitems, int64_t(DeviceSMs()) * occ)));
@@ -668,25 +709,31 @@ int64_t DispatchBatch(const qdb_gpu_program* prog, void* const* hts, qdb_rowset*
         std::lock_guard<std::mutex> lk(tn.mu);
         tn.best[{shape, rows_class, states_class}] = cfg;
         tn.tuned++;
-    } else if (!found && low) {
-        // Untuned low-cardinality batches: items small enough (16K-128K
-        // rows) that the launch has about four per SM; with one big item per
-        // aggregate, a batch of fewer aggregates than SMs left SMs idle.
-        const int64_t per = total_rows / (int64_t(DeviceSMs()) * 4);
-        int64_t c = int64_t(1) << 14;
-        while (c < per && c < (int64_t(1) << 17)) c <<= 1;
-        cfg.chunk_rows = c;
     }
 
-    std::vector<int> order(static_cast<size_t>(m));
-    for (int64_t k = 0; k < m; ++k) order[size_t(k)] = int(k);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return tasks[size_t(a)].nrows > tasks[size_t(b)].nrows; });
+    std::vector<int64_t> task_rows(static_cast<size_t>(m));
+    for (int64_t k = 0; k < m; ++k) task_rows[size_t(k)] = tasks[size_t(k)].nrows;
     std::vector<HighItem> items;
-    BuildItems([&] {
-        std::vector<int64_t> r(static_cast<size_t>(m));
-        for (int64_t k = 0; k < m; ++k) r[size_t(k)] = tasks[size_t(k)].nrows;
-        return r;
-    }(), order, cfg.chunk_rows, items);
+    if (!found && low) {
+        // Untuned low-cardinality batches: two items per resident CTA while
+        // they stay above 8K rows (an item's claim, clear and merge cost a
+        // few microseconds), up to about 128K rows each for long batches;
+        // tiny batches take fewer CTAs.
+        const int64_t grid = int64_t(DeviceSMs()) *
+                             std::max(1, AggBatchOccupancy(P0, fast, cfg.threads, cfg.smem_slots, true));
+        const int64_t min_rows = int64_t(1) << 13;
+        int64_t target = total_rows / min_rows;
+        if (target >= 2 * grid) {
+            const int64_t k = std::max<int64_t>(2, (total_rows / grid + (int64_t(1) << 17) - 1) >> 17);
+            target = k * grid;
+        }
+        BuildItemsBalanced(task_rows, std::max<int64_t>(target, 1), items);
+    } else {
+        std::vector<int> order(static_cast<size_t>(m));
+        for (int64_t k = 0; k < m; ++k) order[size_t(k)] = int(k);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return task_rows[size_t(a)] > task_rows[size_t(b)]; });
+        BuildItems(task_rows, order, cfg.chunk_rows, items);
+    }
     const int64_t nitems = int64_t(items.size());
     const int64_t spill_words = int64_t(DeviceSMs()) * 4 * cfg.smem_slots * (2 + lw.plan.state_words);
     const int64_t defer_cap = std::max<int64_t>(total_rows / 4, int64_t(1) << 20);
