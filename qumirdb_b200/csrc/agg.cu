@@ -30,8 +30,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "common.cuh"
@@ -3594,6 +3596,11 @@ void ExclusiveScanU64(unsigned long long* counts, int64_t n, cudaStream_t s) {
 // instead of one atomic per row.
 static void PresetValidity(const AggPlan& p, const OutputPlan& out, FinLaunch& L, int64_t rows, cudaStream_t s) {
     if (!out.identity) return;
+    const size_t words = size_t((rows + 31) / 32);
+    // Runs of never-NULL columns whose validity words lie side by side (a
+    // packed output block) take one memset each.
+    uint32_t* run = nullptr;
+    size_t run_words = 0;
     for (int k = 0; k < L.ncols; ++k) {
         AggOutputCol& c = L.cols[k];
         if (!c.valid) continue;
@@ -3602,9 +3609,16 @@ static void PresetValidity(const AggPlan& p, const OutputPlan& out, FinLaunch& L
         else if (k - p.nkeyparts < p.naggs) never_null = p.aggs[k - p.nkeyparts].valid_state == 0xFF;
         else never_null = false;
         if (!never_null) continue;
-        cudaMemsetAsync(c.valid, 0xFF, size_t((rows + 31) / 32) * 4, s);
+        if (run && c.valid == run + run_words) {
+            run_words += words;
+        } else {
+            if (run) cudaMemsetAsync(run, 0xFF, run_words * 4, s);
+            run = c.valid;
+            run_words = words;
+        }
         c.valid = nullptr;
     }
+    if (run) cudaMemsetAsync(run, 0xFF, run_words * 4, s);
 }
 
 // Copy plan of an identity output whose columns are all never NULL and are
@@ -3786,12 +3800,24 @@ int AggBatchOccupancy(const AggPlan& p, const FastPlan& f, int threads, int smem
     AggLaunch& L = BatchLaunchOf(p, f, smem_slots);
     const size_t bytes = BatchSmemOf(L, low, smem_slots, threads) + 64;
     if (bytes > g_smem_optin) return 0;
+    // The answer depends only on the kernel and its block shape; the driver
+    // query costs microseconds on every batched dispatch, so it is kept.
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, int, size_t>, int> seen;
+    const auto key = std::make_tuple(reinterpret_cast<const void*>(fns.update), threads, bytes);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = seen.find(key);
+        if (it != seen.end()) return it->second;
+    }
     SetSmem(fns.update, bytes);
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fns.update, threads, bytes) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
+    std::lock_guard<std::mutex> lk(mu);
+    seen[key] = n;
     return n;
 }
 

@@ -374,8 +374,17 @@ BatchConfig Search(const AggPlan& p, const FastPlan& f, const std::vector<HighTa
 
 // FNV-1a over a plan's bytes.
 uint64_t PlanBytesHash(const void* p, size_t n, uint64_t h = 1469598103934665603ull) {
+    // Eight bytes a step (plans run to kilobytes and are hashed per dispatch);
+    // each step's product is folded back so every input bit reaches all 64.
     const auto* b = static_cast<const unsigned char*>(p);
-    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    size_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+        uint64_t w;
+        std::memcpy(&w, b + i, 8);
+        h = (h ^ w) * 0x9e3779b97f4a7c15ull;
+        h ^= h >> 29;
+    }
+    for (; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
     return h;
 }
 
@@ -491,6 +500,21 @@ void DestroySlice(qdb_rowset* rs) {
 namespace {
 int64_t DispatchBatch(const qdb_gpu_program* prog, void* const* hts, qdb_rowset* const* batches, int64_t n,
                       bool every_row_a_group);
+
+// Pinned staging of one host thread's batched finalize (its block list and
+// table descriptors up, its error word down); it only grows, and each use
+// ends with a stream synchronise before the next can write it.
+char* FinishStaging(size_t bytes) {
+    thread_local char* p = nullptr;
+    thread_local size_t cap = 0;
+    if (bytes > cap) {
+        HostOutFree(p);
+        cap = std::max(bytes, cap * 2);
+        p = static_cast<char*>(HostOutAlloc(cap));
+        if (!p) cap = 0;
+    }
+    return p;
+}
 }
 
 extern "C" {
@@ -743,7 +767,13 @@ int64_t DispatchBatch(const qdb_gpu_program* prog, void* const* hts, qdb_rowset*
     }
     std::memcpy(cx.h_tasks, tasks.data(), size_t(m) * sizeof(HighTask));
     if (nitems) std::memcpy(cx.h_items, items.data(), size_t(nitems) * sizeof(HighItem));
-    if (!fresh.empty()) {
+    if (!fresh.empty() && fresh.size() == size_t(m)) {
+        // Every state fresh: the tables are initialised and their flag slots
+        // marked from the tasks uploaded from pinned staging, in stream order
+        // before the update (no wait on the host).
+        cudaMemcpyAsync(cx.d_tasks, cx.h_tasks, size_t(m) * sizeof(HighTask), cudaMemcpyHostToDevice, s);
+        AggBatchInitTables(lw.plan, all, cx.d_tasks, int(m), s);
+    } else if (!fresh.empty()) {
         // The fresh tables' flag slots are marked through the uploaded tasks
         // of the fresh states only.
         std::vector<HighTask> ft(fresh.size());
@@ -967,19 +997,24 @@ int64_t qdb_gpu_agg_finish_batch(const qdb_gpu_program* prog, void* const* hts, 
     std::vector<int> types;
     for (int k = 0; k < lw.out.n; ++k) types.push_back(lw.out.out_type[k]);
     std::vector<AggOutputCol> cols;
-    if (!AllocOutputCols(types, std::max<int64_t>(out_rows, 64), true, cols, s)) {
+    void* out_block = AllocOutputColsPacked(types, std::max<int64_t>(out_rows, 64), cols, s);
+    if (!out_block) {
         SetErr("output allocation failed");
         return -1;
     }
     auto owner = std::make_shared<BatchOutputs>();
     owner->s = s;
-    for (auto& c : cols) {
-        owner->dev.push_back(c.data);
-        if (c.valid) owner->dev.push_back(c.valid);
-        if (c.offsets) owner->dev.push_back(c.offsets);
-    }
+    owner->dev.push_back(out_block);
     const int64_t nblocks = int64_t(blocks.size());
     const size_t scratch_bytes = AggFinalizeBatchScratch(nblocks);
+    const size_t up_bytes = blocks.size() * sizeof(FinBlock) + tables.size() * sizeof(GTableDev);
+    char* h_up = FinishStaging(up_bytes + 16);
+    if (!h_up) {
+        SetErr("pinned allocation failed");
+        return -1;
+    }
+    std::memcpy(h_up, blocks.data(), blocks.size() * sizeof(FinBlock));
+    std::memcpy(h_up + blocks.size() * sizeof(FinBlock), tables.data(), tables.size() * sizeof(GTableDev));
     char* dev = static_cast<char*>(DevAlloc(scratch_bytes + blocks.size() * sizeof(FinBlock) +
                                                 tables.size() * sizeof(GTableDev) + 16, s));
     if (!dev) return -1;
@@ -987,14 +1022,15 @@ int64_t qdb_gpu_agg_finish_batch(const qdb_gpu_program* prog, void* const* hts, 
     auto* d_tables = reinterpret_cast<GTableDev*>(dev + scratch_bytes + blocks.size() * sizeof(FinBlock));
     int* d_err = reinterpret_cast<int*>(dev + scratch_bytes + blocks.size() * sizeof(FinBlock) +
                                         tables.size() * sizeof(GTableDev));
-    cudaMemcpyAsync(d_blocks, blocks.data(), blocks.size() * sizeof(FinBlock), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_tables, tables.data(), tables.size() * sizeof(GTableDev), cudaMemcpyHostToDevice, s);
+    // Blocks and tables sit side by side on both ends: one upload.
+    cudaMemcpyAsync(d_blocks, h_up, up_bytes, cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(d_err, 0, sizeof(int), s);
     AggFinalizeBatch(lw.plan, lw.out, tables[0], d_tables, d_blocks, nblocks, cols.data(), int(cols.size()),
                      out_rows, dev, d_err, s);
-    int herr = 0;
-    cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    int* h_err = reinterpret_cast<int*>(h_up + ((up_bytes + 7) & ~size_t(7)));
+    cudaMemcpyAsync(h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (!CudaOk(cudaStreamSynchronize(s), "batched finalize")) return -1;
+    const int herr = *h_err;
     DevFree(dev, s);
     if (herr) {
         SetErr("batched finalize reported device error %d", herr);

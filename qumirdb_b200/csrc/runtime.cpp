@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -283,12 +284,30 @@ AddrRangeFn AddrRange() {
 
 }  // namespace
 
+// Live allocations of qdb_gpu_alloc, [begin, end) by begin: a column inside
+// one is on the device without a driver query (a batch of many row sets meets
+// hundreds of distinct buffers, and two driver queries per buffer cost more
+// host time than the batched launch saves).
+namespace {
+std::mutex g_alloc_mu;
+std::map<uintptr_t, uintptr_t> g_allocs;
+
+bool InOwnAllocation(uintptr_t a, size_t bytes) {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    auto it = g_allocs.upper_bound(a);
+    if (it == g_allocs.begin()) return false;
+    --it;
+    return a + bytes <= it->second;
+}
+}  // namespace
+
 const void* Staging::Device(const void* p, size_t bytes) {
     if (!p) return nullptr;
     const uintptr_t a = reinterpret_cast<uintptr_t>(p);
     for (const auto& r : dev_ranges) {
         if (a >= r.first && a + bytes <= r.second) return p;
     }
+    if (InOwnAllocation(a, bytes)) return p;
     if (IsDevicePtr(p)) {
         unsigned long long base = 0;
         size_t size = 0;
@@ -833,6 +852,39 @@ bool AllocOutputCols(const std::vector<int>& types, int64_t rows, bool with_vali
     return true;
 }
 
+void* AllocOutputColsPacked(const std::vector<int>& types, int64_t rows, std::vector<AggOutputCol>& cols,
+                            cudaStream_t s) {
+    cols.resize(types.size());
+    for (auto& c : cols) std::memset(&c, 0, sizeof(c));
+    const size_t words = size_t((std::max<int64_t>(rows, 1) + 31) / 32);
+    auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+    size_t data_bytes = 0, off_bytes = 0;
+    for (int t : types) {
+        data_bytes += up(std::max<size_t>(16, size_t(rows) * size_t(StorageWidth(t))));
+        if (t == QDB_TYPE_CHAR1) off_bytes += up(size_t(rows + 1) * 4);
+    }
+    const size_t valid_bytes = types.size() * words * 4;
+    char* block = static_cast<char*>(DevAlloc(data_bytes + off_bytes + valid_bytes + 16, s));
+    if (!block) return nullptr;
+    char* d = block;
+    char* o = block + data_bytes;
+    auto* v = reinterpret_cast<uint32_t*>(block + data_bytes + off_bytes);
+    for (size_t k = 0; k < types.size(); ++k) {
+        AggOutputCol& c = cols[k];
+        c.type = types[k];
+        c.data = d;
+        d += up(std::max<size_t>(16, size_t(rows) * size_t(StorageWidth(types[k]))));
+        c.valid = v + k * words;
+        if (types[k] == QDB_TYPE_CHAR1) {
+            c.offsets = reinterpret_cast<int32_t*>(o);
+            o += up(size_t(rows + 1) * 4);
+            cudaMemsetAsync(c.offsets, 0, 4, s);
+        }
+    }
+    cudaMemsetAsync(v, 0, valid_bytes, s);
+    return block;
+}
+
 int64_t AggFinish(AggTableState* st, const AggLowering& lw, uint32_t flags, qdb_rowset* out) {
     const int64_t groups = st->groups;
     std::vector<int> types;
@@ -905,12 +957,20 @@ int qdb_gpu_synchronize(void) { return CudaOk(cudaStreamSynchronize(CurStream())
 
 void* qdb_gpu_alloc(size_t bytes) {
     void* p = nullptr;
-    if (!CudaOk(cudaMalloc(&p, std::max<size_t>(bytes, 16)), "cudaMalloc")) return nullptr;
+    bytes = std::max<size_t>(bytes, 16);
+    if (!CudaOk(cudaMalloc(&p, bytes), "cudaMalloc")) return nullptr;
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    g_allocs[reinterpret_cast<uintptr_t>(p)] = reinterpret_cast<uintptr_t>(p) + bytes;
     return p;
 }
 
 void qdb_gpu_free(void* ptr) {
-    if (ptr) cudaFree(ptr);
+    if (!ptr) return;
+    {
+        std::lock_guard<std::mutex> lk(g_alloc_mu);
+        g_allocs.erase(reinterpret_cast<uintptr_t>(ptr));
+    }
+    cudaFree(ptr);
 }
 
 void* qdb_gpu_host_alloc(size_t bytes) {

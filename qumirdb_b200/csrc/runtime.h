@@ -111,6 +111,11 @@ void AggMirrorHeader(void* ht, const AggTableState* st, const AggPlan& p);
 
 bool AllocOutputCols(const std::vector<int>& types, int64_t rows, bool with_valid, std::vector<AggOutputCol>& cols,
                      cudaStream_t s);
+// The same columns carved from one device block (returned; freed as one):
+// the validity words of all columns side by side after the data, cleared by
+// one memset, so never-NULL columns can be preset by one memset per run.
+void* AllocOutputColsPacked(const std::vector<int>& types, int64_t rows, std::vector<AggOutputCol>& cols,
+                            cudaStream_t s);
 bool EmitRowset(std::vector<AggOutputCol>& cols, const std::vector<int>& types, int64_t rows, bool on_device,
                 cudaStream_t s, qdb_rowset* out);
 
