@@ -3594,11 +3594,14 @@ void ExclusiveScanU64(unsigned long long* counts, int64_t n, cudaStream_t s) {
 // Output columns of an identity output that no group can leave NULL (keys
 // and aggregates over non-nullable inputs) get an all-valid bitmap up front
 // instead of one atomic per row.
-static void PresetValidity(const AggPlan& p, const OutputPlan& out, FinLaunch& L, int64_t rows, cudaStream_t s) {
+static void PresetValidity(const AggPlan& p, const OutputPlan& out, FinLaunch& L, int64_t rows, cudaStream_t s,
+                           bool packed) {
     if (!out.identity) return;
     const size_t words = size_t((rows + 31) / 32);
-    // Runs of never-NULL columns whose validity words lie side by side (a
-    // packed output block) take one memset each.
+    // Runs of never-NULL columns whose validity words lie side by side in one
+    // packed output block take one memset each.  Only there: the masks of
+    // caller-owned outputs may be separate allocations that merely abut, and
+    // a memset may not run across an allocation's end.
     uint32_t* run = nullptr;
     size_t run_words = 0;
     for (int k = 0; k < L.ncols; ++k) {
@@ -3609,7 +3612,7 @@ static void PresetValidity(const AggPlan& p, const OutputPlan& out, FinLaunch& L
         else if (k - p.nkeyparts < p.naggs) never_null = p.aggs[k - p.nkeyparts].valid_state == 0xFF;
         else never_null = false;
         if (!never_null) continue;
-        if (run && c.valid == run + run_words) {
+        if (packed && run && c.valid == run + run_words) {
             run_words += words;
         } else {
             if (run) cudaMemsetAsync(run, 0xFF, run_words * 4, s);
@@ -3667,7 +3670,7 @@ static void PlanCopy(const AggPlan& p, const OutputPlan& out, const GTableDev& t
 size_t AggFinalizeScratch(const GTableDev&) { return sizeof(unsigned long long); }
 
 void AggFinalize(const AggPlan& p, const OutputPlan& out, const GTableDev& t, AggOutputCol* cols, int ncols,
-                 int64_t groups, void* scratch, int* err, cudaStream_t s) {
+                 int64_t groups, void* scratch, int* err, cudaStream_t s, bool packed) {
     static thread_local FinLaunch* Lp = nullptr;
     if (!Lp) Lp = new FinLaunch();
     FinLaunch& L = *Lp;
@@ -3680,7 +3683,7 @@ void AggFinalize(const AggPlan& p, const OutputPlan& out, const GTableDev& t, Ag
     L.groups = groups;
     L.row_counters = static_cast<unsigned long long*>(scratch);
     L.err = err;
-    PresetValidity(p, out, L, groups, s);
+    PresetValidity(p, out, L, groups, s, packed);
     PlanCopy(p, out, t, L);
     const int64_t blocks = (t.capacity + 1 + kFinChunk - 1) / kFinChunk;
     cudaMemsetAsync(L.row_counters, 0, sizeof(unsigned long long), s);
@@ -3874,7 +3877,7 @@ void AggFinalizeBatch(const AggPlan& p, const OutputPlan& out, const GTableDev& 
     L.err = err;
     L.tables = tables;
     L.blocks = blocks;
-    PresetValidity(p, out, L, out_rows, s);
+    PresetValidity(p, out, L, out_rows, s, true);
     PlanCopy(p, out, layout, L);
     cudaMemsetAsync(L.row_counters, 0, AggFinalizeBatchScratch(nblocks), s);
     ProfileBegin(s, "agg_finalize_batch", nblocks);

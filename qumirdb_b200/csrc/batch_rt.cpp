@@ -997,14 +997,14 @@ int64_t qdb_gpu_agg_finish_batch(const qdb_gpu_program* prog, void* const* hts, 
     std::vector<int> types;
     for (int k = 0; k < lw.out.n; ++k) types.push_back(lw.out.out_type[k]);
     std::vector<AggOutputCol> cols;
-    void* out_block = AllocOutputColsPacked(types, std::max<int64_t>(out_rows, 64), cols, s);
-    if (!out_block) {
+    OutBlock blk;
+    if (!AllocOutputCols(types, std::max<int64_t>(out_rows, 64), true, cols, s, &blk)) {
         SetErr("output allocation failed");
         return -1;
     }
     auto owner = std::make_shared<BatchOutputs>();
     owner->s = s;
-    owner->dev.push_back(out_block);
+    owner->dev.push_back(blk.p);
     const int64_t nblocks = int64_t(blocks.size());
     const size_t scratch_bytes = AggFinalizeBatchScratch(nblocks);
     const size_t up_bytes = blocks.size() * sizeof(FinBlock) + tables.size() * sizeof(GTableDev);
@@ -1046,28 +1046,24 @@ int64_t qdb_gpu_agg_finish_batch(const qdb_gpu_program* prog, void* const* hts, 
         obase[k] = cols[k].offsets;
     }
     if (!on_device) {
-        // One copy of each combined column to the host; the slices point there.
+        // One copy of the whole block to the host; the slices point there, at
+        // the same offsets.
         auto host = std::make_shared<BatchOutputs>();
+        char* h = static_cast<char*>(HostOutAlloc(std::max<size_t>(blk.bytes, 16)));
+        if (!h) {
+            SetErr("pinned allocation failed");
+            return -1;
+        }
+        host->host.push_back(h);
+        cudaMemcpyAsync(h, blk.p, blk.bytes, cudaMemcpyDeviceToHost, s);
+        const char* b = static_cast<const char*>(blk.p);
         for (size_t k = 0; k < cols.size(); ++k) {
-            const size_t w = size_t(StorageWidth(types[k]));
-            const size_t db = size_t(std::max<int64_t>(out_rows, 1)) * w;
-            base[k] = static_cast<char*>(HostOutAlloc(db));
-            host->host.push_back(base[k]);
-            cudaMemcpyAsync(base[k], cols[k].data, db, cudaMemcpyDeviceToHost, s);
-            if (cols[k].valid) {
-                const size_t mb = size_t((out_rows + 31) / 32) * 4 + 4;
-                vbase[k] = static_cast<uint32_t*>(HostOutAlloc(mb));
-                host->host.push_back(vbase[k]);
-                cudaMemcpyAsync(vbase[k], cols[k].valid, mb - 4, cudaMemcpyDeviceToHost, s);
-            }
-            if (cols[k].offsets) {
-                obase[k] = static_cast<int32_t*>(HostOutAlloc(size_t(out_rows + 1) * 4));
-                host->host.push_back(obase[k]);
-                cudaMemcpyAsync(obase[k], cols[k].offsets, size_t(out_rows + 1) * 4, cudaMemcpyDeviceToHost, s);
-            }
+            base[k] = h + (cols[k].data - b);
+            if (cols[k].valid) vbase[k] = reinterpret_cast<uint32_t*>(h + (reinterpret_cast<const char*>(cols[k].valid) - b));
+            if (cols[k].offsets) obase[k] = reinterpret_cast<int32_t*>(h + (reinterpret_cast<const char*>(cols[k].offsets) - b));
         }
         if (!CudaOk(cudaStreamSynchronize(s), "batched finalize read-back")) return -1;
-        owner = host;   // the device buffers go back to the pool now
+        owner = host;   // the device block goes back to the pool now
     }
     for (int64_t i = 0; i < n; ++i) {
         auto* sl = new SliceRowset();

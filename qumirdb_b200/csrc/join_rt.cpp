@@ -977,7 +977,8 @@ int64_t qdb_gpu_jr_materialize(const qdb_gpu_program* prog, void* pairs_v, qdb_r
                                            : J.build_columns[J.payload[J.out_column[k]]].type);
     }
     std::vector<AggOutputCol> cols;
-    if (!AllocOutputCols(types, n, true, cols, s)) {
+    OutBlock blk;
+    if (!AllocOutputCols(types, n, true, cols, s, &blk)) {
         SetErr("jr_materialize: allocation failed");
         return -1;
     }
@@ -1002,7 +1003,7 @@ int64_t qdb_gpu_jr_materialize(const qdb_gpu_program* prog, void* pairs_v, qdb_r
                            ac2 != nullptr, ac2 ? reinterpret_cast<const uint8_t*>(ac2->valid) : nullptr);
         }
     }
-    if (!EmitRowset(cols, types, n, (prog->flags & QDB_OUT_DEVICE) != 0, s, out)) return -1;
+    if (!EmitRowset(cols, types, n, (prog->flags & QDB_OUT_DEVICE) != 0, s, out, &blk)) return -1;
     return n;
 }
 

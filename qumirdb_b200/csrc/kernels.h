@@ -135,10 +135,13 @@ void AggMergeSpill(const AggPlan& p, const uint64_t* spill, int64_t n, const GTa
                    AggCounters* c, cudaStream_t s);
 // Writes every group of `t` into `cols`; `scratch` holds >= AggFinalizeScratch
 // bytes.  `out` describes the output projection (see lower.h OutputPlan).
+// `packed`: the columns' validity words were carved side by side from one
+// allocation (AllocOutputCols with a block), so abutting masks are preset by
+// one memset.
 struct OutputPlan;
 size_t AggFinalizeScratch(const GTableDev& t);
 void AggFinalize(const AggPlan& p, const OutputPlan& out, const GTableDev& t, AggOutputCol* cols,
-                 int ncols, int64_t groups, void* scratch, int* err, cudaStream_t s);
+                 int ncols, int64_t groups, void* scratch, int* err, cudaStream_t s, bool packed = false);
 
 // One whole aggregate in the file-scope scratch array of agg.cu (no device
 // allocation): returns the group count, or -1 with `err` set.

@@ -753,10 +753,53 @@ void DestroyOwned(qdb_rowset* rs) {
 
 // Moves device output columns into `out` (copying to host unless on_device).
 bool EmitRowset(std::vector<AggOutputCol>& cols, const std::vector<int>& types, int64_t rows, bool on_device,
-                cudaStream_t s, qdb_rowset* out) {
+                cudaStream_t s, qdb_rowset* out, const OutBlock* blk) {
     auto* o = new OwnedRowset();
     o->s = s;
     o->cols.resize(cols.size());
+    if (blk && blk->p) {
+        // One block: the rowset owns it on the device, or one copy of it
+        // (columns at the same offsets) on the host.
+        char* h = nullptr;
+        if (on_device) {
+            o->dev.push_back(blk->p);
+        } else {
+            h = static_cast<char*>(HostOutAlloc(std::max<size_t>(blk->bytes, 16)));
+            if (!h) {
+                delete o;
+                SetErr("pinned allocation failed");
+                return false;
+            }
+            o->host.push_back(h);
+            cudaMemcpyAsync(h, blk->p, blk->bytes, cudaMemcpyDeviceToHost, s);
+        }
+        char* b = static_cast<char*>(blk->p);
+        auto at = [&](void* d) -> char* { return on_device ? static_cast<char*>(d) : h + (static_cast<char*>(d) - b); };
+        for (size_t k = 0; k < cols.size(); ++k) {
+            qdb_column& c = o->cols[k];
+            std::memset(&c, 0, sizeof(c));
+            c.Data = at(cols[k].data);
+            if (cols[k].valid) c.Mask = reinterpret_cast<const uint8_t*>(at(cols[k].valid));
+            if (cols[k].offsets) {
+                c.Offsets = at(cols[k].offsets);
+                c.OffsetWidth = 4;
+            }
+        }
+        if (!CudaOk(cudaStreamSynchronize(s), "output")) {
+            for (void* p : o->host) HostOutFree(p);
+            delete o;
+            return false;
+        }
+        if (!on_device) DevFree(blk->p, s);
+        std::memset(out, 0, sizeof(*out));
+        out->Columns = o->cols.data();
+        out->ColumnCount = int64_t(cols.size());
+        out->RowCount = rows;
+        out->Destroy = DestroyOwned;
+        out->Private = o;
+        out->RefCount = 1;
+        return true;
+    }
     for (size_t k = 0; k < cols.size(); ++k) {
         qdb_column& c = o->cols[k];
         std::memset(&c, 0, sizeof(c));
@@ -819,8 +862,47 @@ bool EmitRowset(std::vector<AggOutputCol>& cols, const std::vector<int>& types, 
     return true;
 }
 
+namespace {
+bool AllocOutputBlock(const std::vector<int>& types, int64_t rows, std::vector<AggOutputCol>& cols, cudaStream_t s,
+                      OutBlock& blk) {
+    cols.resize(types.size());
+    for (auto& c : cols) std::memset(&c, 0, sizeof(c));
+    const size_t words = size_t((std::max<int64_t>(rows, 1) + 31) / 32);
+    auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+    size_t data_bytes = 0, off_bytes = 0;
+    for (int t : types) {
+        data_bytes += up(std::max<size_t>(16, size_t(rows) * size_t(StorageWidth(t))));
+        if (t == QDB_TYPE_CHAR1) off_bytes += up(size_t(rows + 1) * 4);
+    }
+    const size_t valid_bytes = types.size() * words * 4;
+    blk.bytes = data_bytes + off_bytes + valid_bytes;
+    char* block = static_cast<char*>(DevAlloc(blk.bytes + 16, s));
+    blk.p = block;
+    if (!block) return false;
+    char* d = block;
+    char* o = block + data_bytes;
+    auto* v = reinterpret_cast<uint32_t*>(block + data_bytes + off_bytes);
+    for (size_t k = 0; k < types.size(); ++k) {
+        AggOutputCol& c = cols[k];
+        c.type = types[k];
+        c.data = d;
+        d += up(std::max<size_t>(16, size_t(rows) * size_t(StorageWidth(types[k]))));
+        c.valid = v + k * words;
+        if (types[k] == QDB_TYPE_CHAR1) {
+            c.offsets = reinterpret_cast<int32_t*>(o);
+            o += up(size_t(rows + 1) * 4);
+            cudaMemsetAsync(c.offsets, 0, 4, s);
+        }
+    }
+    cudaMemsetAsync(v, 0, valid_bytes, s);
+    return true;
+}
+}  // namespace
+
+
 bool AllocOutputCols(const std::vector<int>& types, int64_t rows, bool with_valid, std::vector<AggOutputCol>& cols,
-                     cudaStream_t s) {
+                     cudaStream_t s, OutBlock* blk) {
+    if (blk && with_valid) return AllocOutputBlock(types, rows, cols, s, *blk);
     cols.resize(types.size());
     for (auto& c : cols) std::memset(&c, 0, sizeof(c));
     auto fail = [&]() {
@@ -852,55 +934,24 @@ bool AllocOutputCols(const std::vector<int>& types, int64_t rows, bool with_vali
     return true;
 }
 
-void* AllocOutputColsPacked(const std::vector<int>& types, int64_t rows, std::vector<AggOutputCol>& cols,
-                            cudaStream_t s) {
-    cols.resize(types.size());
-    for (auto& c : cols) std::memset(&c, 0, sizeof(c));
-    const size_t words = size_t((std::max<int64_t>(rows, 1) + 31) / 32);
-    auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
-    size_t data_bytes = 0, off_bytes = 0;
-    for (int t : types) {
-        data_bytes += up(std::max<size_t>(16, size_t(rows) * size_t(StorageWidth(t))));
-        if (t == QDB_TYPE_CHAR1) off_bytes += up(size_t(rows + 1) * 4);
-    }
-    const size_t valid_bytes = types.size() * words * 4;
-    char* block = static_cast<char*>(DevAlloc(data_bytes + off_bytes + valid_bytes + 16, s));
-    if (!block) return nullptr;
-    char* d = block;
-    char* o = block + data_bytes;
-    auto* v = reinterpret_cast<uint32_t*>(block + data_bytes + off_bytes);
-    for (size_t k = 0; k < types.size(); ++k) {
-        AggOutputCol& c = cols[k];
-        c.type = types[k];
-        c.data = d;
-        d += up(std::max<size_t>(16, size_t(rows) * size_t(StorageWidth(types[k]))));
-        c.valid = v + k * words;
-        if (types[k] == QDB_TYPE_CHAR1) {
-            c.offsets = reinterpret_cast<int32_t*>(o);
-            o += up(size_t(rows + 1) * 4);
-            cudaMemsetAsync(c.offsets, 0, 4, s);
-        }
-    }
-    cudaMemsetAsync(v, 0, valid_bytes, s);
-    return block;
-}
-
 int64_t AggFinish(AggTableState* st, const AggLowering& lw, uint32_t flags, qdb_rowset* out) {
     const int64_t groups = st->groups;
     std::vector<int> types;
     for (int k = 0; k < lw.out.n; ++k) types.push_back(lw.out.out_type[k]);
     std::vector<AggOutputCol> cols;
-    if (!AllocOutputCols(types, groups, true, cols, st->s)) {
+    OutBlock blk;
+    if (!AllocOutputCols(types, groups, true, cols, st->s, &blk)) {
         SetErr("output allocation failed");
         return -1;
     }
     void* scratch = DevAlloc(AggFinalizeScratch(st->t), st->s);
     if (!scratch) return -1;
     ResetCounters(st);
-    AggFinalize(lw.plan, lw.out, st->t, cols.data(), int(cols.size()), groups, scratch, &st->dc->error, st->s);
+    AggFinalize(lw.plan, lw.out, st->t, cols.data(), int(cols.size()), groups, scratch, &st->dc->error, st->s,
+                true);
     DevFree(scratch, st->s);
     if (!ReadCounters(st)) return -1;
-    if (!EmitRowset(cols, types, groups, (flags & QDB_OUT_DEVICE) != 0, st->s, out)) return -1;
+    if (!EmitRowset(cols, types, groups, (flags & QDB_OUT_DEVICE) != 0, st->s, out, &blk)) return -1;
     return groups;
 }
 

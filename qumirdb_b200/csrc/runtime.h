@@ -109,15 +109,19 @@ int64_t AggStateMatched(const AggTableState* st);
 AggTableState* AggStateOf(void* ht);
 void AggMirrorHeader(void* ht, const AggTableState* st, const AggPlan& p);
 
+// Output columns of `rows` rows.  With `blk` (and validity) they are carved
+// from one device block: data, then string offsets, then the validity words
+// of all columns side by side, cleared by one memset (so runs of never-NULL
+// columns are preset by one memset each); EmitRowset given the same block
+// hands it to the row set whole, or copies it to the host in one transfer.
+struct OutBlock {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
 bool AllocOutputCols(const std::vector<int>& types, int64_t rows, bool with_valid, std::vector<AggOutputCol>& cols,
-                     cudaStream_t s);
-// The same columns carved from one device block (returned; freed as one):
-// the validity words of all columns side by side after the data, cleared by
-// one memset, so never-NULL columns can be preset by one memset per run.
-void* AllocOutputColsPacked(const std::vector<int>& types, int64_t rows, std::vector<AggOutputCol>& cols,
-                            cudaStream_t s);
+                     cudaStream_t s, OutBlock* blk = nullptr);
 bool EmitRowset(std::vector<AggOutputCol>& cols, const std::vector<int>& types, int64_t rows, bool on_device,
-                cudaStream_t s, qdb_rowset* out);
+                cudaStream_t s, qdb_rowset* out, const OutBlock* blk = nullptr);
 
 struct JoinProgram {
     int32_t build_is_left = 0;

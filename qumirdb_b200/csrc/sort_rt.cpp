@@ -385,7 +385,8 @@ int64_t Materialize(const qdb_gpu_program* prog, qdb_rowset* store, const int64_
     std::vector<int> types;
     for (int c : P.out_columns) types.push_back(P.columns[c].type);
     std::vector<AggOutputCol> cols;
-    if (!AllocOutputCols(types, rows, true, cols, sc.s)) {
+    OutBlock blk;
+    if (!AllocOutputCols(types, rows, true, cols, sc.s, &blk)) {
         SetErr("sort materialize: allocation failed");
         return -1;
     }
@@ -396,7 +397,7 @@ int64_t Materialize(const qdb_gpu_program* prog, qdb_rowset* store, const int64_
         SortMaterialize(v.t, int(j), types[j], ids, rows, cols[j].data, cols[j].valid, derr, sc.s);
     }
     if (!ReadError(derr, sc.s, "sort materialize")) return -1;
-    if (!EmitRowset(cols, types, rows, (prog->flags & QDB_OUT_DEVICE) != 0, sc.s, out)) return -1;
+    if (!EmitRowset(cols, types, rows, (prog->flags & QDB_OUT_DEVICE) != 0, sc.s, out, &blk)) return -1;
     return rows;
 }
 
