@@ -424,11 +424,12 @@ def join_batched_operator(q, peak, w, steps: int = 3):
         jb.build()
         jb.probe_aggregate(pviews)
         s = c = 0
-        for out in jb.finish():
+        outs = jb.finish()
+        for out in outs:
             vals, _ = q.read_rowset(out, [abi.I64, abi.I64])
             s += int(vals[0][0])
             c += int(vals[1][0])
-            q.release(out)
+        outs.release()
         jb.release()
         res.append((s, c))
 
